@@ -1,0 +1,168 @@
+"""Build recipes for the CPU oracle.
+
+TEST INFRASTRUCTURE ONLY: the checker of the CUDA path, never the product.
+
+* ``build_port()`` compiles the C restatement (fdo_setup.c, fdo_port.c,
+  fdo_driver.c) into ``oracle/_build/libfdo_port.so``.  It needs only gcc and
+  runs anywhere, including the GPU box.
+* ``build_ref(cfg)`` compiles the reference's own kernel sources *in place*
+  from the reference tree (``SEISCL_REF_SRC`` or /root/reference/src) with the
+  same -D constants the reference passes at run time (src/clprogram.c:449-571),
+  links them with ref_glue.c and the restated time loop, and writes
+  ``oracle/_ref/libfdo_ref_<key>.so``.  Nothing from the reference tree is
+  copied.  Each grid needs its own build because the reference fixes sizes at
+  compile time.
+
+Both builds use -O2 -ffp-contract=off so the two agree bit for bit.
+"""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import json
+import os
+import subprocess
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+REF_OUT = os.path.join(HERE, "_ref")
+REF_SRC = os.environ.get("SEISCL_REF_SRC", "/root/reference/src")
+CFLAGS = ["-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-std=gnu17", "-w"]
+PORT_SOURCES = ["fdo_setup.c", "fdo_port.c", "fdo_driver.c"]
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed: %s\n%s" % (" ".join(cmd), r.stderr[-4000:]))
+
+
+def port_lib_path() -> str:
+    return os.path.join(BUILD, "libfdo_port.so")
+
+
+def build_port(force: bool = False) -> str:
+    out = port_lib_path()
+    srcs = [os.path.join(HERE, s) for s in PORT_SOURCES + ["fdo.h"]]
+    if not force and os.path.exists(out):
+        if os.path.getmtime(out) >= max(os.path.getmtime(s) for s in srcs):
+            return out
+    os.makedirs(BUILD, exist_ok=True)
+    tmp = out + ".tmp%d" % os.getpid()
+    _run(["gcc", *CFLAGS, "-shared", "-o", tmp, *[os.path.join(HERE, s) for s in PORT_SOURCES], "-lm"])
+    os.replace(tmp, out)
+    return out
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(REF_SRC, "update_v2D.cl"))
+
+
+def _literal(v: float) -> str:
+    return "%9.9f" % v
+
+
+def ref_defines(cfg: dict, nbnd: int, hc: list) -> list:
+    """The -D constants of src/clprogram.c:449-571 for a single device."""
+    nd = cfg["nd"]
+    F = cfg["fdorder"] // 2
+    f32 = lambda x: float(ctypes.c_float(x).value)
+    dt = f32(cfg["dt"])
+    dh = f32(cfg["dh"])
+    d = {
+        "NZ": cfg["nz"] + 2 * F,
+        "NX": cfg["nx"] + 2 * F,
+        "FDOH": F,
+        "NAB": cfg["nab"],
+        "LVE": cfg.get("L", 0),
+        "ND": nd,
+        "NDIM": 3 if nd == 3 else 2,
+        "ABS_TYPE": cfg.get("abs_type", 1),
+        "FREESURF": cfg.get("freesurf", 0),
+        "DT": _literal(dt),
+        "DT2": _literal(dt / 2.0),
+        "DH": _literal(dh),
+        "DTDH": _literal(f32(dt / dh)),
+        "NT": cfg["nt"],
+        "OFFSET": 0,
+        "DEVID": 0,
+        "NUM_DEVICES": 1,
+        "MYLOCALID": 0,
+        "NLOCALP": 1,
+        "LCOMM": 0,
+        "COMM12": 0,
+        "BACK_PROP_TYPE": 1,
+        "RESTYPE": cfg.get("restype", 0),
+        "HOUT": 0,
+        "GRADSRCOUT": 0,
+        "GRADOUT": 1,
+        "FP16": 0,
+        "NFREQS": 0,
+        "NBND": nbnd,
+        "NTNYQ": 0,
+        "DTNYQ": 0,
+    }
+    if nd == 3:
+        d["NY"] = cfg["ny"] + 2 * F
+    for i in range(6):
+        d["HC%d" % (i + 1)] = _literal(hc[i + 1])
+    return ["-D%s=%s" % (k, v) for k, v in d.items()]
+
+
+KERNELS = {
+    2: [("update_v2D.cl", "update_v", 1, False), ("update_s2D.cl", "update_s", 1, False),
+        ("surface2D.cl", "freesurface", 0, False), ("update_adjv2D.cl", "update_adjv", 1, True),
+        ("update_adjs2D.cl", "update_adjs", 1, True), ("surface2D_adj.cl", "surface_adj", 0, False),
+        ("savebnd2D.cl", "savebnd", 1, False)],
+    3: [("update_v3D.cl", "update_v", 1, False), ("update_s3D.cl", "update_s", 1, False),
+        ("surface3D.cl", "freesurface", 0, False), ("update_adjv3D.cl", "update_adjv", 1, True),
+        ("update_adjs3D.cl", "update_adjs", 1, True), ("surface3D_adj.cl", "surface_adj", 0, False),
+        ("savebnd3D.cl", "savebnd", 1, False)],
+}
+
+
+def ref_key(cfg: dict) -> str:
+    keys = ["nd", "nz", "ny", "nx", "fdorder", "maxrelerror", "nab", "freesurf", "abs_type", "L", "nt",
+            "dt", "dh", "restype"]
+    blob = json.dumps({k: cfg.get(k) for k in keys}, sort_keys=True)
+    return hashlib.sha1(blob.encode()).hexdigest()[:16]
+
+
+def ref_lib_path(cfg: dict) -> str:
+    return os.path.join(REF_OUT, "libfdo_ref_%s.so" % ref_key(cfg))
+
+
+def build_ref(cfg: dict, nbnd: int, hc: list) -> str:
+    """Compile the reference kernels for this grid (needs the reference tree)."""
+    out = ref_lib_path(cfg)
+    if os.path.exists(out):
+        return out
+    if not ref_available():
+        raise FileNotFoundError("reference kernel sources not found at %s" % REF_SRC)
+    os.makedirs(REF_OUT, exist_ok=True)
+    nd = 3 if cfg["nd"] == 3 else 2
+    defs = ref_defines(cfg, nbnd, hc)
+    with tempfile.TemporaryDirectory() as td:
+        objs = []
+        for fname, entry, local_off, inject in KERNELS[nd]:
+            obj = os.path.join(td, entry + ".o")
+            cmd = ["gcc", *CFLAGS, "-c", "-o", obj, os.path.join(HERE, "ref_tu.c"), "-I" + HERE,
+                   "-I" + REF_SRC, *defs, "-DLOCAL_OFF=%d" % local_off,
+                   "-DREF_KERNEL_FILE=%s" % fname, "-D%s=ref_%s" % (entry, entry)]
+            if inject:
+                cmd += ["-DREF_WITH_INJECT=1", "-Dinject_ind=inject_ind_%s" % entry]
+            _run(cmd)
+            objs.append(obj)
+        glue = os.path.join(td, "glue.o")
+        gdefs = [d for d in defs if d.split("=")[0] in ("-DND", "-DNX", "-DNY", "-DNZ", "-DFDOH")]
+        _run(["gcc", *CFLAGS, "-c", "-o", glue, os.path.join(HERE, "ref_glue.c"), "-I" + HERE, *gdefs])
+        tmp = out + ".tmp%d" % os.getpid()
+        _run(["gcc", *CFLAGS, "-shared", "-o", tmp, glue, *objs,
+              *[os.path.join(HERE, s) for s in PORT_SOURCES], "-lm"])
+        os.replace(tmp, out)
+    return out
+
+
+if __name__ == "__main__":
+    print(build_port(force=True))

@@ -1,0 +1,269 @@
+"""ctypes binding of the CPU oracle.
+
+TEST INFRASTRUCTURE ONLY.  This is the checker of the CUDA product path: only
+tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use it.
+
+``Oracle(cfg)`` runs the C restatement (fdo_port.c); ``Oracle(cfg, ref=True)``
+runs the reference's own kernel sources compiled in place (oracle/_ref), with
+the same restated time loop.  Inputs and outputs follow SeisCL's host
+conventions: models are [nx][nz] (2D) or [nx][ny][nz] (3D) arrays with z
+fastest; src_pos is [nsrc][5], rec_pos [nrec][8], src [nsrc][NT]; seismograms
+are [nrec][NT] per recorded variable.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+OUT_NAMES = ["vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "syz", "sxz", "p"]
+WAVE_IDS = {"vx": 0, "vy": 1, "vz": 2, "sxx": 3, "syy": 4, "szz": 5, "sxy": 6, "syz": 7, "sxz": 8}
+MEM_IDS = {"rxx": 0, "ryy": 1, "rzz": 2, "rxy": 3, "ryz": 4, "rxz": 5}
+PARAM_IDS = {"M": 0, "mu": 1, "rho": 2, "taup": 3, "taus": 4, "rip": 5, "rjp": 6, "rkp": 7, "muipkp": 8,
+             "muipjp": 9, "mujpkp": 10, "tausipkp": 11, "tausipjp": 12, "tausjpkp": 13}
+PSI_IDS = {n: i for i, n in enumerate(
+    ["psi_vx_x", "psi_vy_x", "psi_vz_x", "psi_vx_y", "psi_vy_y", "psi_vz_y", "psi_vx_z", "psi_vy_z",
+     "psi_vz_z", "psi_sxx_x", "psi_sxy_x", "psi_sxz_x", "psi_sxy_y", "psi_syy_y", "psi_syz_y",
+     "psi_sxz_z", "psi_syz_z", "psi_szz_z"])}
+
+
+class fdo_cfg(C.Structure):
+    _fields_ = [("nd", C.c_int), ("nz", C.c_int), ("ny", C.c_int), ("nx", C.c_int),
+                ("fdorder", C.c_int), ("fdoh", C.c_int), ("maxrelerror", C.c_int),
+                ("nab", C.c_int), ("freesurf", C.c_int), ("abs_type", C.c_int), ("L", C.c_int),
+                ("nt", C.c_int), ("tmin", C.c_int), ("tmax", C.c_int),
+                ("dt", C.c_float), ("dh", C.c_float), ("f0", C.c_float), ("fl", C.c_float * 8),
+                ("vppml", C.c_float), ("fpml", C.c_float), ("npower", C.c_float),
+                ("k_max_cpml", C.c_float), ("abpc", C.c_float),
+                ("param_type", C.c_int), ("restype", C.c_int)]
+
+
+DEFAULTS = dict(nd=2, ny=1, fdorder=8, maxrelerror=1, nab=16, freesurf=0, abs_type=1, L=0, tmin=0,
+                tmax=0, f0=15.0, fl=(15.0,), vppml=3500.0, fpml=15.0, npower=2.0, k_max_cpml=2.0,
+                abpc=6.0, param_type=0, restype=0)
+
+
+def make_cfg(cfg: dict) -> fdo_cfg:
+    d = dict(DEFAULTS)
+    d.update(cfg)
+    c = fdo_cfg()
+    for k in ["nd", "nz", "ny", "nx", "fdorder", "maxrelerror", "nab", "freesurf", "abs_type", "L", "nt",
+              "tmin", "tmax", "param_type", "restype"]:
+        setattr(c, k, int(d[k]))
+    c.fdoh = int(d["fdorder"]) // 2
+    if c.nd != 3:
+        c.ny = 1
+    for k in ["dt", "dh", "f0", "vppml", "fpml", "npower", "k_max_cpml", "abpc"]:
+        setattr(c, k, float(d[k]))
+    fl = list(np.atleast_1d(d["fl"]).astype(float))
+    for i in range(8):
+        c.fl[i] = fl[i] if i < len(fl) else 0.0
+    return c
+
+
+def _lib(path):
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    FP = C.POINTER(C.c_float)
+    lib.fdo_create.restype = P
+    lib.fdo_create.argtypes = [C.POINTER(fdo_cfg), C.c_int, C.POINTER(C.c_int)]
+    lib.fdo_destroy.argtypes = [P]
+    lib.fdo_model.argtypes = [P, FP, FP, FP, FP, FP]
+    lib.fdo_run_forward.argtypes = [P, C.c_int, FP, FP, C.c_int, FP, C.POINTER(C.c_int), C.c_int,
+                                    C.POINTER(FP), C.c_int]
+    lib.fdo_run_adjoint.argtypes = [P, C.c_int, FP, FP, C.c_int, FP, C.POINTER(C.c_int), C.c_int,
+                                    C.POINTER(FP)]
+    lib.fdo_get_grad.argtypes = [P, FP, FP, FP, FP, FP, FP]
+    lib.fdo_clear_grad.argtypes = [P]
+    lib.fdo_array.restype = FP
+    lib.fdo_array.argtypes = [P, C.c_int, C.c_int]
+    lib.fdo_info.argtypes = [P, C.POINTER(C.c_int64)]
+    lib.fdo_run_steps.argtypes = [P, C.c_int]
+    lib.fdo_holberg.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+    lib.fdo_source_targets.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
+    lib.fdo_inject_ind.argtypes = [P, C.c_int, C.c_int, C.c_int]
+    lib.fdo_savebnd_cell.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    return lib
+
+
+_PORT = None
+
+
+def port_lib():
+    global _PORT
+    if _PORT is None:
+        _PORT = _lib(_build.build_port())
+    return _PORT
+
+
+def _fptr(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def source_type_mask(src_pos: np.ndarray) -> int:
+    """Bit t for source types 0..3 and bit 4 for type 100, over all shots
+    (the reference scans every source of the acquisition,
+    src/automatic_kernels.c:416-437)."""
+    m = 0
+    for t in np.asarray(src_pos).reshape(-1, 5)[:, 4].astype(np.int32):
+        if 0 <= t < 4:
+            m |= 1 << int(t)
+        if t == 100:
+            m |= 1 << 4
+    return m
+
+
+class Oracle:
+    def __init__(self, cfg: dict, ref: bool = False):
+        self.cfg = dict(DEFAULTS)
+        self.cfg.update(cfg)
+        if self.cfg["nd"] != 3:
+            self.cfg["ny"] = 1
+        self._c = make_cfg(self.cfg)
+        self.lib = port_lib()
+        if ref:
+            h0 = self._make(self.lib, False)
+            info = self._info(self.lib, h0)
+            self.lib.fdo_destroy(h0)
+            hc = (C.c_double * 7)()
+            self.lib.fdo_holberg(self._c.fdorder, self._c.maxrelerror, hc)
+            path = _build.build_ref(self.cfg, int(info[5]), list(hc))
+            self.lib = _lib(path)
+        self.h = self._make(self.lib, ref)
+        self.info = self._info(self.lib, self.h)
+        self.NZp, self.NYp, self.NXp, self.nvol, self.npar, self.nbnd = [int(v) for v in self.info]
+
+    def _make(self, lib, ref):
+        err = C.c_int(0)
+        h = lib.fdo_create(C.byref(self._c), 1 if ref else 0, C.byref(err))
+        if err.value != 0:
+            lib.fdo_destroy(h)
+            raise RuntimeError("oracle init failed (%d)" % err.value)
+        return h
+
+    @staticmethod
+    def _info(lib, h):
+        out = (C.c_int64 * 6)()
+        lib.fdo_info(h, out)
+        return list(out)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.fdo_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        c = self.cfg
+        return (c["nx"], c["ny"], c["nz"]) if c["nd"] == 3 else (c["nx"], c["nz"])
+
+    def set_model(self, vp, vs, rho, taup=None, taus=None) -> int:
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float32).reshape(self.shape)
+                for a in (vp, vs, rho, taup, taus)]
+        self._keep = arrs
+        return self.lib.fdo_model(self.h, *[_fptr(a) for a in arrs])
+
+    def _outsel(self, outputs):
+        sel = (C.c_int * 10)()
+        for n in outputs:
+            sel[OUT_NAMES.index(n)] = 1
+        return sel
+
+    def forward(self, src_pos, src, rec_pos, outputs, mask=None, save_boundaries=False):
+        src_pos = np.ascontiguousarray(src_pos, np.float32).reshape(-1, 5)
+        rec_pos = np.ascontiguousarray(rec_pos, np.float32).reshape(-1, 8)
+        nt = self.cfg["nt"]
+        src = np.ascontiguousarray(src, np.float32).reshape(src_pos.shape[0], nt)
+        if mask is None:
+            mask = source_type_mask(src_pos)
+        nrec = rec_pos.shape[0]
+        outs = {n: np.zeros((nrec, nt), np.float32) for n in outputs}
+        ptrs = (C.POINTER(C.c_float) * 10)()
+        for n, a in outs.items():
+            ptrs[OUT_NAMES.index(n)] = _fptr(a)
+        rc = self.lib.fdo_run_forward(self.h, src_pos.shape[0], _fptr(src_pos), _fptr(src), nrec,
+                                      _fptr(rec_pos), self._outsel(outputs), mask, ptrs,
+                                      1 if save_boundaries else 0)
+        if rc:
+            raise RuntimeError("oracle forward failed (%d)" % rc)
+        return outs
+
+    def adjoint(self, src_pos, src, rec_pos, residuals: dict, mask=None):
+        src_pos = np.ascontiguousarray(src_pos, np.float32).reshape(-1, 5)
+        rec_pos = np.ascontiguousarray(rec_pos, np.float32).reshape(-1, 8)
+        nt = self.cfg["nt"]
+        src = np.ascontiguousarray(src, np.float32).reshape(src_pos.shape[0], nt)
+        if mask is None:
+            mask = source_type_mask(src_pos)
+        res = {n: np.ascontiguousarray(r, np.float32).reshape(rec_pos.shape[0], nt) for n, r in residuals.items()}
+        ptrs = (C.POINTER(C.c_float) * 10)()
+        for n, a in res.items():
+            ptrs[OUT_NAMES.index(n)] = _fptr(a)
+        rc = self.lib.fdo_run_adjoint(self.h, src_pos.shape[0], _fptr(src_pos), _fptr(src), rec_pos.shape[0],
+                                      _fptr(rec_pos), self._outsel(list(res)), mask, ptrs)
+        if rc:
+            raise RuntimeError("oracle adjoint failed (%d)" % rc)
+
+    def gradients(self):
+        n = self.npar
+        g = [np.zeros(n, np.float32) for _ in range(6)]
+        self.lib.fdo_get_grad(self.h, *[_fptr(a) for a in g])
+        sh = self.shape
+        return {"vp": g[0].reshape(sh), "vs": g[1].reshape(sh), "rho": g[2].reshape(sh),
+                "rawM": g[3].reshape(sh), "rawmu": g[4].reshape(sh), "rawrho": g[5].reshape(sh)}
+
+    def clear_gradients(self):
+        self.lib.fdo_clear_grad(self.h)
+
+    def array(self, kind: str, name: str) -> np.ndarray:
+        """Copy of an internal array (for field-level comparisons)."""
+        c = self.cfg
+        nab = c["nab"]
+        if kind in ("wave", "adj"):
+            k, i, n = (0 if kind == "wave" else 1), WAVE_IDS[name], self.nvol
+        elif kind in ("mem", "adjmem"):
+            k, i, n = (2 if kind == "mem" else 3), MEM_IDS[name], self.nvol * c["L"]
+        elif kind == "psi":
+            k, i = 4, PSI_IDS[name]
+            ny = c["ny"]
+            axis = name[-1]
+            n = {"x": 2 * nab * ny * c["nz"], "y": c["nx"] * 2 * nab * c["nz"], "z": c["nx"] * ny * 2 * nab}[axis]
+        elif kind == "param":
+            k, i, n = 5, PARAM_IDS[name], self.npar
+        elif kind in ("cpml_x", "cpml_y", "cpml_z"):
+            k = {"cpml_x": 6, "cpml_y": 7, "cpml_z": 8}[kind]
+            i = ["K", "a", "b", "K_half", "a_half", "b_half"].index(name)
+            n = 2 * nab
+        elif kind == "taper":
+            k, i, n = 9, 0, nab
+        elif kind == "eta":
+            k, i, n = 10, 0, c["L"]
+        elif kind == "bnd":
+            k, i, n = 11, WAVE_IDS[name], self.nbnd * c["nt"]
+        else:
+            raise KeyError(kind)
+        p = self.lib.fdo_array(self.h, k, i)
+        if not p:
+            return None
+        return np.ctypeslib.as_array(p, shape=(int(n),)).copy()
+
+    def run_steps(self, n):
+        self.lib.fdo_run_steps(self.h, n)
+
+
+def holberg(fdorder: int, maxrelerror: int):
+    hc = (C.c_double * 7)()
+    if port_lib().fdo_holberg(fdorder, maxrelerror, hc):
+        raise ValueError("bad FD order / error level")
+    return list(hc)
