@@ -1,0 +1,175 @@
+/*
+ * seiscl_b200.h -- C ABI of the B200 staggered-grid FDTD engine.
+ *
+ * One plan = one grid, one physics case and one set of device buffers on the
+ * current CUDA device.  All arrays crossing this boundary are plain host or
+ * device pointers with sizes; nothing here depends on PyTorch.
+ *
+ * The entry points replace the single-device path of SeisCL:
+ *   - sfd_plan_create/sfd_set_model replace readhdf5 + assign_modeling_case +
+ *     Init_cst + Init_model + Init_CUDA (src/read_hdf5.c:554,
+ *     src/assign_modeling_case.c:871, src/Init_cst.c:24, src/Init_model.c:40,
+ *     src/Init_OpenCL.c:326);
+ *   - sfd_forward replaces the forward half of
+ *     int time_stepping(model*, device**, struct filenames)
+ *     (src/time_stepping.c:692, loop at :747-860);
+ *   - sfd_adjoint replaces its gradient half (src/time_stepping.c:862-940)
+ *     for BACK_PROP_TYPE=1 (boundary-saving reconstruction);
+ *   - sfd_get_gradient replaces transf_grad (src/calc_grad.c:975-1107).
+ *
+ * Layout conventions are the reference host's (src/read_hdf5.c:606-625):
+ * model parameters are [nx][ny][nz] (3D) or [nx][nz] (2D) with z fastest;
+ * src_pos is [nsrc][5] = (x, y, z, srcid, type); rec_pos is [nrec][8] =
+ * (x, y, z, srcid, recid, ...); src is [nsrc][NT]; a seismogram is
+ * [nrec][NT] (src/writehdf5.c:209-220).
+ *
+ * Errors: every call returns 0 or a negative SFD_ERR_* code and leaves a
+ * message in sfd_last_error(plan).  Nothing calls exit().  A plan must not
+ * be used from two host threads at once; distinct plans are independent.
+ */
+#ifndef SEISCL_B200_H
+#define SEISCL_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SFD_OK 0
+#define SFD_ERR_ARG (-1)       /* invalid argument or configuration */
+#define SFD_ERR_CUDA (-2)      /* a CUDA call failed */
+#define SFD_ERR_CFL (-3)       /* dt above the stability limit (assign_modeling_case.c:819) */
+#define SFD_ERR_MEMORY (-4)    /* device memory exhausted or above the plan budget */
+#define SFD_ERR_STATE (-5)     /* call out of order (e.g. adjoint without forward) */
+#define SFD_ERR_UNSTABLE (-6)  /* non-finite wavefield detected (residuals.c:444-448) */
+#define SFD_ERR_UNSUPPORTED (-7)
+
+/* Output variable indices for the outsel/seis arrays. */
+enum {
+    SFD_OUT_VX = 0, SFD_OUT_VY, SFD_OUT_VZ, SFD_OUT_SXX, SFD_OUT_SYY, SFD_OUT_SZZ,
+    SFD_OUT_SXY, SFD_OUT_SYZ, SFD_OUT_SXZ, SFD_OUT_P, SFD_NOUT
+};
+
+/* Storage precision of wave fields / saved boundaries (arithmetic is FP32). */
+enum { SFD_PREC_FP32 = 0, SFD_PREC_FP16 = 1, SFD_PREC_BF16 = 2 };
+
+/* The csts keys of SeisCL.py:23-30 that the single-device path reads
+ * (src/read_hdf5.c:461-552). */
+typedef struct sfd_config {
+    int nd;            /* 2: P-SV, 3: 3D */
+    int n[3];          /* N as in SeisCL: [NZ, NX] in 2D, [NZ, NY, NX] in 3D */
+    int nt;            /* NT */
+    int fdorder;       /* FDORDER: 2..12 */
+    int maxrelerror;   /* MAXRELERROR: 0..4 */
+    int L;             /* relaxation mechanisms (0 = elastic) */
+    int freesurf;
+    int abs_type;      /* 1: CPML, 2: Cerjan taper */
+    int nab;
+    float dt, dh, f0;
+    float fl[8];       /* FL, L values */
+    float vppml, fpml, npower, k_max_cpml, abpc;
+    int tmin, tmax;    /* adjoint time window in steps; tmax <= 0 means NT */
+    int param_type;    /* 0: vp,vs,rho  1: M,mu,rho  2: Ip,Is,rho */
+    int restype;       /* 0: L2 (full gradient), 1: M only */
+    int precision;     /* SFD_PREC_*: storage of the saved boundaries */
+    int reserved[7];
+} sfd_config;
+
+typedef struct sfd_shot {
+    int nsrc, nrec;
+    const float *src_pos;  /* [nsrc][5] */
+    const float *src;      /* [nsrc][NT] */
+    const float *rec_pos;  /* [nrec][8] */
+} sfd_shot;
+
+typedef struct sfd_plan sfd_plan;
+
+/* Create a plan for `cfg` on the current CUDA device.  No device memory is
+ * allocated for the model until sfd_set_model. */
+int sfd_plan_create(const sfd_config *cfg, sfd_plan **out);
+void sfd_plan_destroy(sfd_plan *plan);
+const char *sfd_last_error(const sfd_plan *plan);
+
+/* Upload the model.  params = {vp, vs, rho} (param_type 0), plus {taup, taus}
+ * when L > 0, each a host array of nz*ny*nx floats in [nx][ny][nz] order.
+ * vs may be NULL for zero shear.  Applies the reference transforms
+ * (assign_modeling_case.c:305-535) and the CFL check (:730-827). */
+int sfd_set_model(sfd_plan *plan, const float *const *params);
+
+/* Bit t (t = 0..3) for each source type and bit 4 for type 100 over the
+ * whole acquisition (automatic_kernels.c:416-437 scans all shots). */
+int sfd_source_type_mask(const float *src_pos, int nsrc_all);
+
+/* Forward modelling of one shot (time_stepping.c:747-835).  outsel[SFD_NOUT]
+ * selects the recorded variables; seis[k] receives [nrec][NT] floats for each
+ * selected k (host pointers).  save_boundaries != 0 keeps the boundary shells
+ * and final state on the device for a following sfd_adjoint.  stream may be
+ * NULL (the plan's own stream). */
+int sfd_forward(sfd_plan *plan, const sfd_shot *shot, int srctype_mask, const int *outsel,
+                float *const *seis, int save_boundaries, void *stream);
+
+/* Adjoint of the shot last run by sfd_forward(save_boundaries=1):
+ * residuals[k] are [nrec][NT] host arrays already scaled as adjoint sources
+ * (see sfd_residual_scale); gradients accumulate in FP64 on the device. */
+int sfd_adjoint(sfd_plan *plan, const sfd_shot *shot, int srctype_mask, const int *outsel,
+                const float *const *residuals, void *stream);
+
+/* Zero the gradient accumulators (gradinit, automatic_kernels.c:840-930). */
+int sfd_zero_gradient(sfd_plan *plan);
+
+/* Gradients [nx][ny][nz] as floats: transformed (transform=1: gradvp,
+ * gradvs, gradrho for param_type 0, calc_grad.c:975-1107) or raw
+ * (transform=0: grad M, grad mu, grad rho of the stored parameters). */
+int sfd_get_gradient(sfd_plan *plan, int transform, float *g0, float *g1, float *g2);
+
+/* res_scale (residuals.c:452-568): scale residuals in place into adjoint
+ * sources.  res[k] are [nrec][NT] host arrays for the selected outputs. */
+int sfd_residual_scale(sfd_plan *plan, const sfd_shot *shot, const int *outsel, float *const *res);
+
+/* ---- host-only set-up (no device needed) ---- */
+
+/* The 14 transformed parameter arrays of sfd_set_model (M, mu, rho_b, taup,
+ * taus, rip, rjp, rkp, muipkp, muipjp, mujpkp, tausipkp, tausipjp, tausjpkp;
+ * src/assign_modeling_case.c:305-535), each nz*ny*nx floats.  out[k] may be
+ * NULL.  Returns SFD_ERR_CFL when dt is above the stability limit. */
+int sfd_host_transform(const sfd_config *cfg, const float *const *params, float *const *out);
+
+/* Padded linear cell index ((i*NYp + j)*NZp + k) of n source or receiver rows
+ * of `stride` floats, i = (int)(x/DH) + FDOH as the generated kernels compute
+ * it (src/automatic_kernels.c:95-105, 501-511); -1 for rows dropped because
+ * i is outside [FDOH, NXp-FDOH-1].  Returns the number kept. */
+int sfd_host_point_cells(const sfd_config *cfg, const float *pos, int n, int stride, int64_t *cells);
+
+/* Wave fields fed by a source of `type` under the acquisition's type mask
+ * (src/automatic_kernels.c:416-614): fields[3] receive indices in
+ * SFD_OUT_VX..SFD_OUT_SXZ order, div[3] the divisor (0 = none). */
+int sfd_host_source_targets(int nd, int mask, int type, int *fields, float *div);
+
+/* CPML profiles of one axis: 6 arrays of 2*nab floats (K, a, b, K_half,
+ * a_half, b_half; src/third_party/SOFI3D/CPML_COEFF.c:26-200). */
+int sfd_host_cpml(const sfd_config *cfg, float *out);
+
+/* Introspection for tests: padded dims, counts, boundary cells. */
+int sfd_plan_info(const sfd_plan *plan, int64_t *out8);
+
+/* Copy a device array of the plan to the host (tests): kind 0 wave field,
+ * 1 adjoint wave field, 2 memory variable, 3 transformed parameter,
+ * 4 CPML constants of axis id (6 arrays of 2*nab), 5 psi array.  Returns the
+ * number of floats written, or a negative error. */
+int64_t sfd_debug_copy(sfd_plan *plan, int kind, int id, float *dst, int64_t cap);
+
+/* Kernel timing for benchmarks: runs the velocity update, the stress update
+ * and (with a free surface) the surface kernel `nrep` times each on the
+ * plan's stream, bracketed by CUDA events, and writes the mean milliseconds
+ * per launch to out_ms[0..2].  The wave fields are modified. */
+int sfd_bench_kernels(sfd_plan *plan, int nrep, float *out_ms);
+
+/* Milliseconds spent in the device time loop of the last sfd_forward /
+ * sfd_adjoint (CUDA events on the plan's stream). */
+float sfd_last_loop_ms(const sfd_plan *plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

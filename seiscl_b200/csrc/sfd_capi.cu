@@ -1,0 +1,692 @@
+// sfd_capi.cu -- the C ABI of the engine: plans, model upload, the forward
+// and adjoint time loops (src/time_stepping.c:692-1012, single device).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "seiscl_b200.h"
+#include "sfd_internal.h"
+#include "sfd_kernels.h"
+#include "sfd_setup.h"
+
+using namespace sfd;
+
+namespace {
+
+int fail(sfd_plan *p, int code, const std::string &msg)
+{
+    if (p) p->err = msg;
+    return code;
+}
+
+#define CKC(call)                                                                                     \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return fail(p, e_ == cudaErrorMemoryAllocation ? SFD_ERR_MEMORY : SFD_ERR_CUDA,           \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                           \
+    } while (0)
+
+void *dalloc(sfd_plan *p, size_t bytes, cudaError_t *err)
+{
+    void *ptr = nullptr;
+    *err = cudaMalloc(&ptr, bytes ? bytes : 16);
+    if (*err != cudaSuccess) return nullptr;
+    p->allocs.push_back(ptr);
+    return ptr;
+}
+
+bool is_wave_used(const Grid &g, int w)
+{
+    if (g.nd == 3) return true;
+    return w == VX || w == VZ || w == SXX || w == SZZ || w == SXZ;
+}
+bool is_mem_used(const Grid &g, int r)
+{
+    if (g.L == 0) return false;
+    if (g.nd == 3) return true;
+    return r == RXX || r == RZZ || r == RXZ;
+}
+
+unsigned outmask_of(const int *outsel, int nd, int *nsel)
+{
+    unsigned m = 0;
+    int n = 0;
+    for (int o = 0; o < SFD_NOUT; o++)
+        if (outsel && outsel[o]) {
+            m |= 1u << o;
+            n++;
+        }
+    *nsel = n;
+    return m;
+}
+
+int check_outsel(sfd_plan *p, const int *outsel)
+{
+    for (int o = 0; o < SFD_NOUT; o++) {
+        if (!outsel || !outsel[o]) continue;
+        if (o == SFD_OUT_P) continue;
+        if (!is_wave_used(p->g, o)) return fail(p, SFD_ERR_ARG, "requested output variable does not exist in 2D P-SV");
+    }
+    return SFD_OK;
+}
+
+// grow the per-shot device buffers
+int ensure_shot_buffers(sfd_plan *p, int nsrc, int nrec, int nsel)
+{
+    cudaError_t e;
+    if (nsrc > p->cap_src) {
+        int cap = std::max(nsrc, 16);
+        p->d_src_cell = (int64_t *)dalloc(p, sizeof(int64_t) * cap, &e); if (e) goto oom;
+        p->d_src_nt = (int *)dalloc(p, sizeof(int) * cap, &e); if (e) goto oom;
+        p->d_src_kz = (int *)dalloc(p, sizeof(int) * cap, &e); if (e) goto oom;
+        p->d_src_field = (int *)dalloc(p, sizeof(int) * 3 * cap, &e); if (e) goto oom;
+        p->d_src_div = (float *)dalloc(p, sizeof(float) * 3 * cap, &e); if (e) goto oom;
+        p->d_src = (float *)dalloc(p, sizeof(float) * (size_t)cap * p->cfg.nt, &e); if (e) goto oom;
+        p->cap_src = cap;
+    }
+    if ((int64_t)nrec * std::max(nsel, 1) > p->cap_rec) {
+        int64_t cap = std::max<int64_t>((int64_t)nrec * std::max(nsel, 1), 16);
+        p->d_rec_cell = (int64_t *)dalloc(p, sizeof(int64_t) * cap, &e); if (e) goto oom;
+        p->d_seis = (float *)dalloc(p, sizeof(float) * (size_t)cap * p->cfg.nt, &e); if (e) goto oom;
+        p->d_res = (float *)dalloc(p, sizeof(float) * (size_t)cap * p->cfg.nt, &e); if (e) goto oom;
+        p->cap_rec = (int)cap;
+    }
+    return SFD_OK;
+oom:
+    return fail(p, SFD_ERR_MEMORY, std::string("device allocation failed: ") + cudaGetErrorString(e));
+}
+
+// host-side mapping of a shot's sources and receivers, uploaded to the device
+int upload_shot(sfd_plan *p, const sfd_shot *shot, int mask, PointSet &S, PointSet &R, cudaStream_t st)
+{
+    const Grid &g = p->g;
+    int nsrc = shot->nsrc, nrec = shot->nrec, F = g.F;
+    std::vector<int64_t> scell(nsrc), rcell(nrec);
+    std::vector<int> snt(nsrc), sfield(3 * nsrc), skz(nsrc);
+    std::vector<float> sdiv(3 * nsrc);
+    for (int s = 0; s < nsrc; s++) {
+        int i, j, k;
+        point_cell(shot->src_pos + 5 * s, p->DH_lit, F, i, j, k);
+        if (g.nd != 3) j = 0;  // 2D kernels index [(i)*NZ+k] (automatic_kernels.c:536-543)
+        // sources outside [F, NX-F-1] along x are dropped (automatic_kernels.c:506-511)
+        if (i < F || i > g.NX - F - 1) { scell[s] = -1; snt[s] = 0; continue; }
+        if (j < 0 || j >= g.NY || k < 0 || k >= g.NZ)
+            return fail(p, SFD_ERR_ARG, "source position outside the padded grid");
+        scell[s] = ((int64_t)i * g.NY + j) * g.NZ + k;
+        skz[s] = k;
+        int type = (int)shot->src_pos[5 * s + 4];
+        snt[s] = source_targets(g.nd, mask, type, &sfield[3 * s], &sdiv[3 * s]);
+    }
+    for (int r = 0; r < nrec; r++) {
+        int i, j, k;
+        point_cell(shot->rec_pos + 8 * r, p->DH_lit, F, i, j, k);
+        if (g.nd != 3) j = 0;
+        if (i < F || i > g.NX - F - 1) { rcell[r] = -1; continue; }
+        if (j < 0 || j >= g.NY || k < 0 || k >= g.NZ)
+            return fail(p, SFD_ERR_ARG, "receiver position outside the padded grid");
+        rcell[r] = ((int64_t)i * g.NY + j) * g.NZ + k;
+    }
+    {
+        if (nsrc) {
+            CKC(cudaMemcpyAsync(p->d_src_cell, scell.data(), sizeof(int64_t) * nsrc, cudaMemcpyHostToDevice, st));
+            CKC(cudaMemcpyAsync(p->d_src_nt, snt.data(), sizeof(int) * nsrc, cudaMemcpyHostToDevice, st));
+            CKC(cudaMemcpyAsync(p->d_src_kz, skz.data(), sizeof(int) * nsrc, cudaMemcpyHostToDevice, st));
+            CKC(cudaMemcpyAsync(p->d_src_field, sfield.data(), sizeof(int) * 3 * nsrc, cudaMemcpyHostToDevice, st));
+            CKC(cudaMemcpyAsync(p->d_src_div, sdiv.data(), sizeof(float) * 3 * nsrc, cudaMemcpyHostToDevice, st));
+            CKC(cudaMemcpyAsync(p->d_src, shot->src, sizeof(float) * (size_t)nsrc * p->cfg.nt,
+                                cudaMemcpyHostToDevice, st));
+        }
+        if (nrec) CKC(cudaMemcpyAsync(p->d_rec_cell, rcell.data(), sizeof(int64_t) * nrec, cudaMemcpyHostToDevice, st));
+        // pageable sources: wait so the host vectors may go out of scope
+        CKC(cudaStreamSynchronize(st));
+    }
+    S = PointSet{nsrc, p->d_src_cell, p->d_src_nt, p->d_src_field, p->d_src_div, p->d_src_kz};
+    R = PointSet{nrec, p->d_rec_cell, nullptr, nullptr, nullptr, nullptr};
+    return SFD_OK;
+}
+
+int alloc_model(sfd_plan *p)
+{
+    const Grid &g = p->g;
+    cudaError_t e;
+    for (int w = 0; w < NW; w++) {
+        p->f.w[w] = nullptr;
+        if (!is_wave_used(g, w)) continue;
+        p->f.w[w] = (float *)dalloc(p, sizeof(float) * g.nvol, &e);
+        if (e) return fail(p, SFD_ERR_MEMORY, "wave field allocation failed");
+    }
+    for (int r = 0; r < NR; r++) {
+        p->f.r[r] = nullptr;
+        if (!is_mem_used(g, r)) continue;
+        p->f.r[r] = (float *)dalloc(p, sizeof(float) * g.nvol * g.L, &e);
+        if (e) return fail(p, SFD_ERR_MEMORY, "memory-variable allocation failed");
+    }
+    int64_t nab2 = 2 * (int64_t)g.nab;
+    int64_t sx = nab2 * g.ny * g.nz, sy = (int64_t)g.nx * nab2 * g.nz, sz = (int64_t)g.nx * g.ny * nab2;
+    int64_t sizes[NPSI] = {sx, sx, sx, sy, sy, sy, sz, sz, sz, sx, sx, sx, sy, sy, sy, sz, sz, sz};
+    int64_t tot = 0;
+    for (int i = 0; i < NPSI; i++) {
+        bool used = g.abs_type == 1 && g.nab > 0 && (g.nd == 3 || (i != PVY_X && i != PVX_Y && i != PVY_Y &&
+                    i != PVZ_Y && i != PVY_Z && i != PSXY_X && i != PSXY_Y && i != PSYY_Y && i != PSYZ_Y && i != PSYZ_Z));
+        p->psi_size[i] = used ? sizes[i] : 0;
+        tot += p->psi_size[i];
+    }
+    p->d_psi_all = tot ? (float *)dalloc(p, sizeof(float) * tot, &e) : nullptr;
+    if (tot && e) return fail(p, SFD_ERR_MEMORY, "CPML allocation failed");
+    int64_t off = 0;
+    for (int i = 0; i < NPSI; i++) {
+        p->f.psi[i] = p->psi_size[i] ? p->d_psi_all + off : nullptr;
+        off += p->psi_size[i];
+    }
+    int64_t npar = (int64_t)g.nz * g.ny * g.nx;
+    for (int k = 0; k < NPAR; k++) {
+        p->f.p[k] = (const float *)dalloc(p, sizeof(float) * npar, &e);
+        if (e) return fail(p, SFD_ERR_MEMORY, "parameter allocation failed");
+    }
+    int nc = std::max(2 * g.nab, 1);
+    float *cst = (float *)dalloc(p, sizeof(float) * (3 * NC * nc + nc), &e);
+    if (e) return fail(p, SFD_ERR_MEMORY, "constant allocation failed");
+    for (int k = 0; k < NC; k++) {
+        p->f.cx[k] = cst + (0 * NC + k) * nc;
+        p->f.cy[k] = cst + (1 * NC + k) * nc;
+        p->f.cz[k] = cst + (2 * NC + k) * nc;
+    }
+    p->f.taper = cst + 3 * NC * nc;
+    return SFD_OK;
+}
+
+int upload_constants(sfd_plan *p)
+{
+    const Grid &g = p->g;
+    const sfd_config &c = p->cfg;
+    int nc = std::max(2 * g.nab, 1);
+    std::vector<float> h(3 * NC * nc + nc, 0.0f);
+    if (g.abs_type == 1 && g.nab > 0) {
+        for (int ax = 0; ax < 3; ax++) {
+            float *b = h.data() + ax * NC * nc;
+            if (!cpml_profiles(c.npower, c.k_max_cpml, c.fpml, c.vppml, c.dh, c.dt, g.nab, b + CK * nc, b + CA * nc,
+                               b + CB * nc, b + CKH * nc, b + CAH * nc, b + CBH * nc))
+                return fail(p, SFD_ERR_ARG, "invalid CPML parameters");
+        }
+    }
+    if (g.abs_type == 2) cerjan_taper(c.abpc, g.nab, h.data() + 3 * NC * nc);
+    CKC(cudaMemcpy((void *)p->f.cx[0], h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
+    return SFD_OK;
+}
+
+int zero_forward_state(sfd_plan *p, cudaStream_t st)
+{
+    const Grid &g = p->g;
+    for (int w = 0; w < NW; w++)
+        if (p->f.w[w]) CKC(cudaMemsetAsync(p->f.w[w], 0, sizeof(float) * g.nvol, st));
+    for (int r = 0; r < NR; r++)
+        if (p->f.r[r]) CKC(cudaMemsetAsync(p->f.r[r], 0, sizeof(float) * g.nvol * g.L, st));
+    int64_t tot = 0;
+    for (int i = 0; i < NPSI; i++) tot += p->psi_size[i];
+    if (tot) CKC(cudaMemsetAsync(p->d_psi_all, 0, sizeof(float) * tot, st));
+    return SFD_OK;
+}
+
+int alloc_adjoint(sfd_plan *p)
+{
+    const Grid &g = p->g;
+    cudaError_t e;
+    if (p->a.grad[0]) return SFD_OK;
+    for (int w = 0; w < NW; w++) {
+        p->a.wr[w] = nullptr;
+        if (!is_wave_used(g, w)) continue;
+        p->a.wr[w] = (float *)dalloc(p, sizeof(float) * g.nvol, &e);
+        if (e) return fail(p, SFD_ERR_MEMORY, "adjoint field allocation failed");
+    }
+    for (int r = 0; r < NR; r++) {
+        p->a.rr[r] = nullptr;
+        if (!is_mem_used(g, r)) continue;
+        p->a.rr[r] = (float *)dalloc(p, sizeof(float) * g.nvol * g.L, &e);
+        if (e) return fail(p, SFD_ERR_MEMORY, "adjoint memory-variable allocation failed");
+    }
+    int64_t npar = (int64_t)g.nz * g.ny * g.nx;
+    for (int k = 0; k < NG; k++) {
+        p->a.grad[k] = (double *)dalloc(p, sizeof(double) * npar, &e);
+        if (e) return fail(p, SFD_ERR_MEMORY, "gradient allocation failed");
+        CKC(cudaMemset(p->a.grad[k], 0, sizeof(double) * npar));
+    }
+    int64_t nq = (int64_t)g.nx * g.ny;
+    p->d_surf_q = (float *)dalloc(p, sizeof(float) * nq, &e);
+    if (e) return fail(p, SFD_ERR_MEMORY, "scratch allocation failed");
+    return SFD_OK;
+}
+
+}  // namespace
+
+// ====================================================================== ABI
+extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
+{
+    if (!cfg || !out) return SFD_ERR_ARG;
+    *out = nullptr;
+    const sfd_config &c = *cfg;
+    if (c.nd != 2 && c.nd != 3) return SFD_ERR_UNSUPPORTED;
+    if (c.fdorder < 2 || c.fdorder > 12 || c.fdorder % 2) return SFD_ERR_ARG;
+    if (c.maxrelerror < 0 || c.maxrelerror > 4) return SFD_ERR_ARG;
+    if (c.L < 0 || c.L > 8 || c.nt <= 0 || !(c.dt > 0) || !(c.dh > 0) || c.nab < 0) return SFD_ERR_ARG;
+    if (c.abs_type != 1 && c.abs_type != 2 && c.abs_type != 0) return SFD_ERR_ARG;
+    for (int i = 0; i < (c.nd == 3 ? 3 : 2); i++)
+        if (c.n[i] <= 0) return SFD_ERR_ARG;
+    // N[0] must be even (read_hdf5.c:535-540)
+    if (c.n[0] % 2) return SFD_ERR_ARG;
+    if (c.precision < 0 || c.precision > 2) return SFD_ERR_ARG;
+
+    sfd_plan *p = new sfd_plan();
+    p->cfg = c;
+    Grid &g = p->g;
+    memset(&g, 0, sizeof g);
+    g.nd = c.nd;
+    g.F = c.fdorder / 2;
+    g.nz = c.n[0];
+    if (c.nd == 3) { g.ny = c.n[1]; g.nx = c.n[2]; }
+    else { g.ny = 1; g.nx = c.n[1]; }
+    g.NZ = g.nz + 2 * g.F;
+    g.NX = g.nx + 2 * g.F;
+    g.NY = c.nd == 3 ? g.ny + 2 * g.F : 1;
+    g.nab = c.abs_type == 0 ? 0 : c.nab;
+    g.abs_type = g.nab < 1 ? 0 : c.abs_type;  // NAB<1 disables absorption (assign_modeling_case.c:1045)
+    g.L = c.L;
+    g.freesurf = c.freesurf ? 1 : 0;
+    g.restype = c.restype;
+    g.nvol = (int64_t)g.NZ * g.NY * g.NX;
+    double hc[6];
+    holberg(c.fdorder, c.maxrelerror, hc);
+    for (int i = 0; i < 6; i++) g.hc[i] = (float)hc[i];
+    g.dt = c.dt;
+    g.dt2 = (float)((double)c.dt / 2.0);
+    for (int l = 0; l < 8; l++) g.eta[l] = l < c.L ? (float)(2.0 * 3.141592653589793238462643 * c.fl[l] * (double)c.dt) : 0.0f;
+    g.nbnd = nbnd_cells(g.nd, g.nz, g.ny, g.nx, g.F, g.nab, g.freesurf);
+    if (p->cfg.tmax <= 0 || p->cfg.tmax > c.nt) p->cfg.tmax = c.nt;
+    if (p->cfg.tmin < 0) p->cfg.tmin = 0;
+    p->DH_lit = literal9((double)c.dh);
+    p->DT_lit = literal9((double)c.dt);
+    p->model_set = false;
+    p->have_forward = false;
+    p->d_psi_all = nullptr;
+    for (int w = 0; w < NW; w++) p->d_bnd[w] = nullptr;
+    p->bnd_elem = c.precision == SFD_PREC_FP32 ? 4 : 2;
+    p->cap_src = p->cap_rec = 0;
+    p->d_surf_q = nullptr;
+    memset(&p->f, 0, sizeof p->f);
+    memset(&p->a, 0, sizeof p->a);
+    p->last_ms = 0.0f;
+    if (cudaGetDevice(&p->device) != cudaSuccess) { delete p; return SFD_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) { delete p; return SFD_ERR_CUDA; }
+    p->own_stream = true;
+    cudaEventCreate(&p->ev0);
+    cudaEventCreate(&p->ev1);
+    *out = p;
+    return SFD_OK;
+}
+
+extern "C" void sfd_plan_destroy(sfd_plan *p)
+{
+    if (!p) return;
+    cudaStreamSynchronize(p->stream);
+    for (void *ptr : p->allocs) cudaFree(ptr);
+    for (int w = 0; w < NW; w++)
+        if (p->d_bnd[w]) cudaFree(p->d_bnd[w]);
+    cudaEventDestroy(p->ev0);
+    cudaEventDestroy(p->ev1);
+    if (p->own_stream) cudaStreamDestroy(p->stream);
+    delete p;
+}
+
+extern "C" const char *sfd_last_error(const sfd_plan *p) { return p ? p->err.c_str() : "null plan"; }
+
+extern "C" int sfd_set_model(sfd_plan *p, const float *const *params)
+{
+    if (!p || !params) return SFD_ERR_ARG;
+    int rc = transform_model(p->cfg, p->g.nz, p->g.ny, p->g.nx, params, p->hp, p->err);
+    if (rc) return rc;
+    if (!p->model_set) {
+        if ((rc = alloc_model(p))) return rc;
+        if ((rc = upload_constants(p))) return rc;
+    }
+    int64_t npar = (int64_t)p->g.nz * p->g.ny * p->g.nx;
+    for (int k = 0; k < NPAR; k++)
+        CKC(cudaMemcpy((void *)p->f.p[k], p->hp[k].data(), sizeof(float) * npar, cudaMemcpyHostToDevice));
+    p->model_set = true;
+    p->have_forward = false;
+    return SFD_OK;
+}
+
+extern "C" int sfd_source_type_mask(const float *src_pos, int nsrc_all)
+{
+    int m = 0;
+    for (int s = 0; s < nsrc_all; s++) {
+        int t = (int)src_pos[5 * s + 4];
+        if (t >= 0 && t < 4) m |= 1 << t;
+        if (t == 100) m |= 1 << 4;
+    }
+    return m;
+}
+
+extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const int *outsel, float *const *seis,
+                           int save_boundaries, void *stream)
+{
+    if (!p || !shot) return SFD_ERR_ARG;
+    if (!p->model_set) return fail(p, SFD_ERR_STATE, "sfd_set_model must be called first");
+    int rc;
+    if ((rc = check_outsel(p, outsel))) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+    const Grid &g = p->g;
+    int nsel;
+    unsigned omask = outmask_of(outsel, g.nd, &nsel);
+    if ((rc = ensure_shot_buffers(p, shot->nsrc, shot->nrec, nsel))) return rc;
+    PointSet S, R;
+    if ((rc = upload_shot(p, shot, mask, S, R, st))) return rc;
+    if ((rc = zero_forward_state(p, st))) return rc;
+    if (nsel) CKC(cudaMemsetAsync(p->d_seis, 0, sizeof(float) * (size_t)nsel * shot->nrec * p->cfg.nt, st));
+    BndSlot bs;
+    memset(&bs, 0, sizeof bs);
+    if (save_boundaries) {
+        if (g.nab <= 0 || g.nbnd <= 0) return fail(p, SFD_ERR_ARG, "boundary saving needs an absorbing layer");
+        for (int w = 0; w < NW; w++) {
+            if (!p->f.w[w]) continue;
+            if (!p->d_bnd[w]) {
+                cudaError_t e = cudaMalloc(&p->d_bnd[w], p->bnd_elem * (size_t)p->cfg.nt * g.nbnd);
+                if (e != cudaSuccess) {
+                    p->d_bnd[w] = nullptr;
+                    return fail(p, SFD_ERR_MEMORY, "saved-boundary store does not fit in device memory");
+                }
+            }
+            bs.p[w] = p->d_bnd[w];
+            bs.fields[bs.nfield++] = w;
+        }
+    }
+    p->have_forward = false;
+    const int NT = p->cfg.nt, tmax = p->cfg.tmax;
+    CKC(cudaEventRecord(p->ev0, st));
+    for (int t = 0; t < tmax; t++) {
+        launch_sources(g, p->f, S, p->d_src, NT, t, 1, st);
+        launch_update_v(g, p->f, st);
+        launch_update_s(g, p->f, st);
+        if (save_boundaries) launch_savebnd(g, p->f, bs, p->cfg.precision, (int64_t)t * g.nbnd, st);
+        if (g.freesurf) launch_surface(g, p->f, 1, st);
+        launch_record(g, p->f, R, p->d_seis, NT, t, omask, st);
+    }
+    CKC(cudaEventRecord(p->ev1, st));
+    CKC(cudaGetLastError());
+    int slot = 0;
+    for (int o = 0; o < SFD_NOUT; o++) {
+        if (!(omask & (1u << o))) continue;
+        if (seis && seis[o])
+            CKC(cudaMemcpyAsync(seis[o], p->d_seis + (size_t)slot * shot->nrec * NT,
+                                sizeof(float) * (size_t)shot->nrec * NT, cudaMemcpyDeviceToHost, st));
+        slot++;
+    }
+    CKC(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1);
+    p->have_forward = save_boundaries != 0;
+    return SFD_OK;
+}
+
+extern "C" int sfd_adjoint(sfd_plan *p, const sfd_shot *shot, int mask, const int *outsel,
+                           const float *const *residuals, void *stream)
+{
+    if (!p || !shot) return SFD_ERR_ARG;
+    if (!p->have_forward) return fail(p, SFD_ERR_STATE, "sfd_adjoint needs a preceding sfd_forward with saved boundaries");
+    int rc;
+    if ((rc = check_outsel(p, outsel))) return rc;
+    if ((rc = alloc_adjoint(p))) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+    const Grid &g = p->g;
+    int nsel;
+    unsigned omask = outmask_of(outsel, g.nd, &nsel);
+    if ((rc = ensure_shot_buffers(p, shot->nsrc, shot->nrec, nsel))) return rc;
+    PointSet S, R;
+    if ((rc = upload_shot(p, shot, mask, S, R, st))) return rc;
+    const int NT = p->cfg.nt;
+    int slot = 0;
+    for (int o = 0; o < SFD_NOUT; o++) {
+        if (!(omask & (1u << o))) continue;
+        if (!residuals || !residuals[o]) return fail(p, SFD_ERR_ARG, "missing residual array");
+        CKC(cudaMemcpyAsync(p->d_res + (size_t)slot * shot->nrec * NT, residuals[o],
+                            sizeof(float) * (size_t)shot->nrec * NT, cudaMemcpyHostToDevice, st));
+        slot++;
+    }
+    // adjoint fields start at zero; the CPML memory carries over from the
+    // forward run (the reference binds the forward psi buffers by name)
+    for (int w = 0; w < NW; w++)
+        if (p->a.wr[w]) CKC(cudaMemsetAsync(p->a.wr[w], 0, sizeof(float) * g.nvol, st));
+    for (int r = 0; r < NR; r++)
+        if (p->a.rr[r]) CKC(cudaMemsetAsync(p->a.rr[r], 0, sizeof(float) * g.nvol * g.L, st));
+    AdjFields a = p->a;
+    CKC(cudaEventRecord(p->ev0, st));
+    for (int t = p->cfg.tmax - 1; t > p->cfg.tmin; t--) {
+        for (int w = 0; w < NW; w++)
+            a.bnd[w] = p->d_bnd[w] ? (const char *)p->d_bnd[w] + p->bnd_elem * (size_t)(t - 1) * g.nbnd : nullptr;
+        if (g.freesurf) launch_surface_adj(g, p->f, a, p->d_surf_q, st);
+        launch_residuals(g, a, R, p->d_res, NT, t, omask, st);
+        launch_update_adj(g, p->f, a, true, p->cfg.precision, st);
+        launch_update_adj(g, p->f, a, false, p->cfg.precision, st);
+        launch_sources(g, p->f, S, p->d_src, NT, t, -1, st);
+    }
+    CKC(cudaEventRecord(p->ev1, st));
+    CKC(cudaGetLastError());
+    CKC(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1);
+    p->have_forward = false;
+    return SFD_OK;
+}
+
+extern "C" int sfd_zero_gradient(sfd_plan *p)
+{
+    if (!p) return SFD_ERR_ARG;
+    int rc;
+    if ((rc = alloc_adjoint(p))) return rc;
+    int64_t npar = (int64_t)p->g.nz * p->g.ny * p->g.nx;
+    for (int k = 0; k < NG; k++) CKC(cudaMemset(p->a.grad[k], 0, sizeof(double) * npar));
+    return SFD_OK;
+}
+
+extern "C" int sfd_get_gradient(sfd_plan *p, int transform, float *g0, float *g1, float *g2)
+{
+    if (!p) return SFD_ERR_ARG;
+    if (!p->a.grad[0]) return fail(p, SFD_ERR_STATE, "no gradient has been accumulated");
+    int64_t n = (int64_t)p->g.nz * p->g.ny * p->g.nx;
+    std::vector<double> gr(n), gM(n), gmu(n);
+    CKC(cudaMemcpy(gr.data(), p->a.grad[GRHO], sizeof(double) * n, cudaMemcpyDeviceToHost));
+    CKC(cudaMemcpy(gM.data(), p->a.grad[GM], sizeof(double) * n, cudaMemcpyDeviceToHost));
+    CKC(cudaMemcpy(gmu.data(), p->a.grad[GMU], sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (!transform) {
+        for (int64_t i = 0; i < n; i++) {
+            if (g0) g0[i] = (float)gM[i];
+            if (g1) g1[i] = (float)gmu[i];
+            if (g2) g2[i] = (float)gr[i];
+        }
+        return SFD_OK;
+    }
+    // src/calc_grad.c:975-1107
+    const double dt = p->cfg.dt, dh = p->cfg.dh;
+    const int pt = p->cfg.param_type;
+    for (int64_t i = 0; i < n; i++) {
+        double rho = 1.0 / p->hp[PRHO][i] * dt / dh;
+        double M = p->hp[PM][i] * dh / dt, mu = p->hp[PMU][i] * dh / dt;
+        double grho = gr[i] / dt, gm = gM[i] / dt, gs = gmu[i] / dt;
+        if (pt == 0 || pt == 2) {
+            grho += M / rho * gm;
+            if (mu > 0) grho += mu / rho * gs;
+        }
+        if (pt == 0) {
+            gm = 2.0 * std::sqrt(rho * M) * gm;
+            gs = 2.0 * std::sqrt(rho * mu) * gs;
+        } else if (pt == 2) {
+            gm = 2.0 * std::sqrt(M / rho) * gm;
+            gs = 2.0 * std::sqrt(mu / rho) * gs;
+        }
+        if (g0) g0[i] = (float)gm;
+        if (g1) g1[i] = (float)gs;
+        if (g2) g2[i] = (float)grho;
+    }
+    return SFD_OK;
+}
+
+extern "C" int sfd_residual_scale(sfd_plan *p, const sfd_shot *shot, const int *outsel, float *const *res)
+{
+    // src/residuals.c:452-568 in FP32 (par_scale 0).  For velocity outputs
+    // the reference reads x, y and z from the first column of rec_pos
+    // (:487-489); that index is kept.
+    if (!p || !shot) return SFD_ERR_ARG;
+    if (!p->model_set) return fail(p, SFD_ERR_STATE, "no model");
+    const Grid &g = p->g;
+    const int NT = p->cfg.nt, tmax = p->cfg.tmax;
+    const float dh = p->cfg.dh, dt = p->cfg.dt;
+    int64_t npar = (int64_t)g.nz * g.ny * g.nx;
+    for (int o = 0; o < SFD_NOUT; o++) {
+        if (!outsel || !outsel[o] || !res || !res[o]) continue;
+        if (o != SFD_OUT_VX && o != SFD_OUT_VY && o != SFD_OUT_VZ && o != SFD_OUT_P) continue;
+        for (int r = 0; r < shot->nrec; r++) {
+            const float *rp = shot->rec_pos + 8 * r;
+            int x, y, z;
+            if (o == SFD_OUT_P) { x = (int)(rp[0] / dh); y = (int)(rp[1] / dh); z = (int)(rp[2] / dh); }
+            else { x = (int)(rp[0] / dh); y = x; z = x; }
+            int64_t pos = g.nd == 3 ? ((int64_t)x * g.ny + y) * g.nz + z : (int64_t)x * g.nz + z;
+            if (pos < 0 || pos >= npar) return fail(p, SFD_ERR_ARG, "residual scaling index outside the model");
+            float *row = res[o] + (int64_t)r * NT;
+            if (o == SFD_OUT_P) {
+                float parscal = -2.0 * (p->hp[PM][pos] - p->hp[PMU][pos]) * dh / dt;
+                for (int t = 0; t < tmax; t++) row[t] *= parscal * dt;
+            } else {
+                int id = o == SFD_OUT_VX ? PRIP : (o == SFD_OUT_VY ? PRJP : PRKP);
+                float parscal = 1.0 / p->hp[id][pos] * dh / dt;
+                for (int t = 0; t < tmax; t++) row[t] *= 1.0 / parscal * dt;
+            }
+        }
+    }
+    return SFD_OK;
+}
+
+extern "C" int sfd_plan_info(const sfd_plan *p, int64_t *o)
+{
+    if (!p || !o) return SFD_ERR_ARG;
+    o[0] = p->g.NZ; o[1] = p->g.NY; o[2] = p->g.NX; o[3] = p->g.nvol;
+    o[4] = (int64_t)p->g.nz * p->g.ny * p->g.nx; o[5] = p->g.nbnd; o[6] = p->g.F; o[7] = p->cfg.tmax;
+    return SFD_OK;
+}
+
+extern "C" int64_t sfd_debug_copy(sfd_plan *p, int kind, int id, float *dst, int64_t cap)
+{
+    if (!p || !dst) return SFD_ERR_ARG;
+    const Grid &g = p->g;
+    const void *src = nullptr;
+    int64_t n = 0;
+    if (kind == 0 && id >= 0 && id < NW) { src = p->f.w[id]; n = g.nvol; }
+    else if (kind == 1 && id >= 0 && id < NW) { src = p->a.wr[id]; n = g.nvol; }
+    else if (kind == 2 && id >= 0 && id < NR) { src = p->f.r[id]; n = g.nvol * g.L; }
+    else if (kind == 3 && id >= 0 && id < NPAR) { src = p->f.p[id]; n = (int64_t)g.nz * g.ny * g.nx; }
+    else if (kind == 4 && id >= 0 && id < 3) {
+        src = id == 0 ? p->f.cx[0] : (id == 1 ? p->f.cy[0] : p->f.cz[0]);
+        n = (int64_t)NC * std::max(2 * g.nab, 1);
+    } else if (kind == 5 && id >= 0 && id < NPSI) { src = p->f.psi[id]; n = p->psi_size[id]; }
+    if (!src) return fail(p, SFD_ERR_ARG, "array not allocated");
+    if (n > cap) return fail(p, SFD_ERR_ARG, "destination too small");
+    cudaDeviceSynchronize();
+    if (cudaMemcpy(dst, src, sizeof(float) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(p, SFD_ERR_CUDA, "copy failed");
+    return n;
+}
+
+extern "C" float sfd_last_loop_ms(const sfd_plan *p) { return p ? p->last_ms : 0.0f; }
+
+extern "C" int sfd_bench_kernels(sfd_plan *p, int nrep, float *out_ms)
+{
+    if (!p || !out_ms || nrep <= 0) return SFD_ERR_ARG;
+    if (!p->model_set) return fail(p, SFD_ERR_STATE, "no model");
+    cudaStream_t st = p->stream;
+    const Grid &g = p->g;
+    for (int k = 0; k < 3; k++) out_ms[k] = 0.0f;
+    for (int which = 0; which < 3; which++) {
+        if (which == 2 && !g.freesurf) break;
+        CKC(cudaEventRecord(p->ev0, st));
+        for (int r = 0; r < nrep; r++) {
+            if (which == 0) launch_update_v(g, p->f, st);
+            else if (which == 1) launch_update_s(g, p->f, st);
+            else launch_surface(g, p->f, 1, st);
+        }
+        CKC(cudaEventRecord(p->ev1, st));
+        CKC(cudaEventSynchronize(p->ev1));
+        CKC(cudaGetLastError());
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p->ev0, p->ev1);
+        out_ms[which] = ms / nrep;
+    }
+    return SFD_OK;
+}
+
+// ------------------------------------------------------------ host-only
+namespace {
+int host_grid(const sfd_config *c, Grid &g)
+{
+    if (!c || (c->nd != 2 && c->nd != 3) || c->fdorder < 2 || c->fdorder > 12 || c->fdorder % 2) return SFD_ERR_ARG;
+    memset(&g, 0, sizeof g);
+    g.nd = c->nd;
+    g.F = c->fdorder / 2;
+    g.nz = c->n[0];
+    if (c->nd == 3) { g.ny = c->n[1]; g.nx = c->n[2]; }
+    else { g.ny = 1; g.nx = c->n[1]; }
+    if (g.nz <= 0 || g.ny <= 0 || g.nx <= 0) return SFD_ERR_ARG;
+    g.NZ = g.nz + 2 * g.F;
+    g.NX = g.nx + 2 * g.F;
+    g.NY = c->nd == 3 ? g.ny + 2 * g.F : 1;
+    return SFD_OK;
+}
+}  // namespace
+
+extern "C" int sfd_host_transform(const sfd_config *cfg, const float *const *params, float *const *out)
+{
+    Grid g;
+    int rc = host_grid(cfg, g);
+    if (rc) return rc;
+    std::vector<float> tmp[NPAR];
+    std::string err;
+    rc = transform_model(*cfg, g.nz, g.ny, g.nx, params, tmp, err);
+    if (rc) return rc;
+    for (int k = 0; k < NPAR; k++)
+        if (out && out[k]) memcpy(out[k], tmp[k].data(), sizeof(float) * tmp[k].size());
+    return SFD_OK;
+}
+
+extern "C" int sfd_host_point_cells(const sfd_config *cfg, const float *pos, int n, int stride, int64_t *cells)
+{
+    Grid g;
+    int rc = host_grid(cfg, g);
+    if (rc) return rc;
+    double DH = literal9((double)cfg->dh);
+    int kept = 0;
+    for (int r = 0; r < n; r++) {
+        int i, j, k;
+        point_cell(pos + (int64_t)stride * r, DH, g.F, i, j, k);
+        if (g.nd != 3) j = 0;
+        if (i < g.F || i > g.NX - g.F - 1) { cells[r] = -1; continue; }
+        cells[r] = ((int64_t)i * g.NY + j) * g.NZ + k;
+        kept++;
+    }
+    return kept;
+}
+
+extern "C" int sfd_host_source_targets(int nd, int mask, int type, int *fields, float *div)
+{
+    return source_targets(nd, mask, type, fields, div);
+}
+
+extern "C" int sfd_host_cpml(const sfd_config *c, float *out)
+{
+    if (!c || !out || c->nab <= 0) return SFD_ERR_ARG;
+    int n = 2 * c->nab;
+    if (!cpml_profiles(c->npower, c->k_max_cpml, c->fpml, c->vppml, c->dh, c->dt, c->nab, out, out + n, out + 2 * n,
+                       out + 3 * n, out + 4 * n, out + 5 * n))
+        return SFD_ERR_ARG;
+    return SFD_OK;
+}

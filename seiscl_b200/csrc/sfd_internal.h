@@ -1,0 +1,105 @@
+// sfd_internal.h -- plan state and kernel argument blocks of the B200 FDTD
+// engine (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "seiscl_b200.h"
+
+namespace sfd {
+
+// wave fields; the order doubles as the bit layout of masks
+enum { VX, VY, VZ, SXX, SYY, SZZ, SXY, SYZ, SXZ, NW };
+// memory variables
+enum { RXX, RYY, RZZ, RXY, RYZ, RXZ, NR };
+// CPML memory arrays psi_<field>_<axis>
+enum {
+    PVX_X, PVY_X, PVZ_X, PVX_Y, PVY_Y, PVZ_Y, PVX_Z, PVY_Z, PVZ_Z,
+    PSXX_X, PSXY_X, PSXZ_X, PSXY_Y, PSYY_Y, PSYZ_Y, PSXZ_Z, PSYZ_Z, PSZZ_Z, NPSI
+};
+// transformed parameters
+enum {
+    PM, PMU, PRHO, PTAUP, PTAUS, PRIP, PRJP, PRKP, PMUIPKP, PMUIPJP, PMUJPKP,
+    PTAUSIPKP, PTAUSIPJP, PTAUSJPKP, NPAR
+};
+// CPML constants per axis
+enum { CK, CA, CB, CKH, CAH, CBH, NC };
+enum { GRHO, GM, GMU, NG };
+
+// Everything a stencil kernel needs, passed by value (a few hundred bytes of
+// kernel parameter space).
+struct Grid {
+    int nd;                 // 2 or 3
+    int F;                  // stencil half width
+    int nz, ny, nx;         // physical sizes (ny = 1 in 2D)
+    int NZ, NY, NX;         // padded sizes
+    int nab, L, freesurf, abs_type;
+    int64_t nvol;           // padded cell count
+    float hc[6];            // FD coefficients
+    float dt, dt2;          // dt and dt/2
+    float eta[8];           // 2 pi FL dt
+    int nbnd;               // saved-boundary cells per field per step
+    int restype;
+};
+
+struct Fields {
+    float *w[NW];
+    float *r[NR];           // [L][nvol]
+    float *psi[NPSI];
+    const float *p[NPAR];
+    const float *cx[NC], *cy[NC], *cz[NC];
+    const float *taper;
+};
+
+struct AdjFields {
+    float *wr[NW];
+    float *rr[NR];
+    double *grad[NG];
+    const void *bnd[NW];    // slice t-1 of the saved boundaries
+};
+
+struct PointSet {           // sources or receivers of one shot, device side
+    int n;
+    const int64_t *cell;    // padded linear index, -1 when dropped
+    const int *ntarget;     // sources: number of fed fields
+    const int *field;       // sources: [n][3] wave-field ids
+    const float *div;       // sources: [n][3] divisor (0 = none)
+    const int *kz;          // z cell index (free-surface adjoint skip)
+};
+
+}  // namespace sfd
+
+struct sfd_plan {
+    sfd_config cfg;
+    sfd::Grid g;
+    int device;
+    cudaStream_t stream;
+    bool own_stream;
+    std::string err;
+    double DH_lit;          // the reference's "%9.9f" dh literal
+    double DT_lit;
+    // host copies of the transformed parameters (for transf_grad, res_scale)
+    std::vector<float> hp[sfd::NPAR];
+    bool model_set;
+    // device memory
+    std::vector<void *> allocs;
+    sfd::Fields f;
+    sfd::AdjFields a;
+    float *d_psi_all;
+    int64_t psi_size[sfd::NPSI];
+    void *d_bnd[sfd::NW];   // [nt][nbnd]
+    size_t bnd_elem;        // bytes per stored value
+    bool have_forward;      // boundaries of a forward run are on the device
+    // per-shot device buffers (grown on demand)
+    int cap_src, cap_rec;
+    int64_t *d_src_cell, *d_rec_cell;
+    int *d_src_nt, *d_src_field, *d_src_kz;
+    float *d_src_div, *d_src, *d_seis, *d_res;
+    float *d_surf_q;        // surface-adjoint scratch [nx][ny]
+    cudaEvent_t ev0, ev1;
+    float last_ms;
+};

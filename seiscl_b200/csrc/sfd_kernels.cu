@@ -1,0 +1,1274 @@
+// sfd_kernels.cu -- general sm_100a kernels of the staggered-grid FDTD engine.
+//
+// One thread per grid cell; z (fastest) runs along the warp so every stencil
+// tap is a coalesced row load served from L1/L2.  These kernels cover every
+// configuration the engine accepts (2D P-SV and 3D, FDORDER 2..12, elastic
+// and viscoelastic, CPML or Cerjan taper, free surface) and are the
+// reference implementation inside the product; sfd_kernels3d_fast.cu holds
+// the register-blocked 3D kernels used on the hot configurations.
+//
+// Semantics follow the reference kernels cell for cell:
+//   update_v  src/update_v2D.cl:32-246,  src/update_v3D.cl:34-369
+//   update_s  src/update_s2D.cl:30-327,  src/update_s3D.cl:35-489
+//   surface   src/surface2D.cl:30-193,   src/surface3D.cl:39-271
+//   adjoint   src/update_adj{v,s}{2D,3D}.cl, src/surface{2D,3D}_adj.cl
+//   boundary  src/savebnd{2D,3D}.cl, src/header_injectbnd.cl
+// Arithmetic is FP32 with FMA; gradients accumulate in FP64.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "sfd_internal.h"
+#include "sfd_kernels.h"
+
+namespace sfd {
+
+typedef int64_t i64;
+
+// ---------------------------------------------------------------- helpers
+// forward difference c1 (v[i+1]-v[i]) + c2 (v[i+2]-v[i-1]) + ...  (Dxp)
+template <int F>
+__device__ __forceinline__ float dfw(const float *__restrict__ v, i64 i, i64 st, const float *hc)
+{
+    float acc = hc[0] * (__ldg(v + i + st) - __ldg(v + i));
+#pragma unroll
+    for (int m = 2; m <= F; m++) acc = fmaf(hc[m - 1], __ldg(v + i + m * st) - __ldg(v + i - (m - 1) * st), acc);
+    return acc;
+}
+// backward difference c1 (v[i]-v[i-1]) + c2 (v[i+1]-v[i-2]) + ...  (Dxm)
+template <int F>
+__device__ __forceinline__ float dbw(const float *__restrict__ v, i64 i, i64 st, const float *hc)
+{
+    float acc = hc[0] * (__ldg(v + i) - __ldg(v + i - st));
+#pragma unroll
+    for (int m = 2; m <= F; m++) acc = fmaf(hc[m - 1], __ldg(v + i + (m - 1) * st) - __ldg(v + i - m * st), acc);
+    return acc;
+}
+// non-cached variants for arrays written by the same kernel
+template <int F>
+__device__ __forceinline__ float dfw_rw(const float *v, i64 i, i64 st, const float *hc)
+{
+    float acc = hc[0] * (v[i + st] - v[i]);
+#pragma unroll
+    for (int m = 2; m <= F; m++) acc = fmaf(hc[m - 1], v[i + m * st] - v[i - (m - 1) * st], acc);
+    return acc;
+}
+template <int F>
+__device__ __forceinline__ float dbw_rw(const float *v, i64 i, i64 st, const float *hc)
+{
+    float acc = hc[0] * (v[i] - v[i - st]);
+#pragma unroll
+    for (int m = 2; m <= F; m++) acc = fmaf(hc[m - 1], v[i + (m - 1) * st] - v[i - m * st], acc);
+    return acc;
+}
+
+// psi = b psi + a d ; d = d/K + psi    (the CPML recursion of every kernel)
+__device__ __forceinline__ void cpml(float *psi, i64 q, const float *K, const float *a, const float *b, int ci,
+                                     float &d)
+{
+    float ps = __ldg(b + ci) * psi[q] + __ldg(a + ci) * d;
+    psi[q] = ps;
+    d = d / __ldg(K + ci) + ps;
+}
+
+template <typename T> __device__ __forceinline__ float to_f(T v);
+template <> __device__ __forceinline__ float to_f<float>(float v) { return v; }
+template <> __device__ __forceinline__ float to_f<__half>(__half v) { return __half2float(v); }
+template <> __device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <typename T> __device__ __forceinline__ T from_f(float v);
+template <> __device__ __forceinline__ float from_f<float>(float v) { return v; }
+template <> __device__ __forceinline__ __half from_f<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+// ------------------------------------------------------- boundary shells
+struct BndDims {
+    int NXbnd, NYbnd, NZbnd, lbnd, lbnds;
+};
+__device__ __host__ inline BndDims bnd_dims(const Grid &g)
+{
+    BndDims b;
+    b.NXbnd = g.NX - 2 * g.F - 2 * g.nab;
+    b.NYbnd = g.nd == 3 ? g.NY - 2 * g.F - 2 * g.nab : 1;
+    if (!g.freesurf) {
+        b.NZbnd = g.NZ - 2 * g.F - 2 * g.nab;
+        b.lbnd = g.F + g.nab;
+        b.lbnds = g.F + g.nab;
+    } else {
+        b.NZbnd = g.NZ - 2 * g.F - g.nab;
+        b.lbnd = g.F + g.nab;
+        b.lbnds = g.F;
+    }
+    return b;
+}
+
+// index of cell (k, i) in the saved shell, -1 if not a shell cell
+// (src/header_injectbnd.cl:238-283)
+__device__ __forceinline__ int inject_ind2d(const Grid &g, int k, int i)
+{
+    BndDims b = bnd_dims(g);
+    int F = g.F, m = -1;
+    i -= b.lbnd;
+    k -= b.lbnds;
+    if ((k > F - 1 && k < b.NZbnd - F) && (i > F - 1 && i < b.NXbnd - F)) m = -1;
+    else if (k < 0 || k > b.NZbnd - 1 || i < 0 || i > b.NXbnd - 1) m = -1;
+    else if (i < F) m = i * b.NZbnd + k;
+    else if (i > b.NXbnd - 1 - F) { i = i - b.NXbnd + F; m = b.NZbnd * F + i * b.NZbnd + k; }
+    else if (k < F) { i = i - F; m = b.NZbnd * F * 2 + (b.NXbnd - 2 * F) * F + i + k * (b.NXbnd - 2 * F); }
+    else { i = i - F; k = k - b.NZbnd + F; m = b.NZbnd * F * 2 + i + k * (b.NXbnd - 2 * F); }
+    return m;
+}
+// (src/header_injectbnd.cl:25-84)
+__device__ __forceinline__ int inject_ind3d(const Grid &g, int k, int j, int i)
+{
+    BndDims b = bnd_dims(g);
+    int F = g.F, m = -1;
+    i -= b.lbnd; j -= b.lbnd; k -= b.lbnds;
+    int NX = b.NXbnd, NY = b.NYbnd, NZ = b.NZbnd;
+    if ((k > F - 1 && k < NZ - F) && (j > F - 1 && j < NY - F) && (i > F - 1 && i < NX - F)) m = -1;
+    else if (k < 0 || k > NZ - 1 || j < 0 || j > NY - 1 || i < 0 || i > NX - 1) m = -1;
+    else if (i < F) m = i * NY * NZ + j * NZ + k;
+    else if (i > NX - 1 - F) { i = i - NX + F; m = NY * NZ * F + i * NY * NZ + j * NZ + k; }
+    else if (j < F) { i = i - F; m = NY * NZ * F * 2 + i * F * NZ + j * NZ + k; }
+    else if (j > NY - 1 - F) { i = i - F; j = j - NY + F; m = NY * NZ * F * 2 + (NX - 2 * F) * NZ * F + i * F * NZ + j * NZ + k; }
+    else if (k < F) {
+        i = i - F; j = j - F;
+        m = NY * NZ * F * 2 + (NX - 2 * F) * NZ * F * 2 + (NX - 2 * F) * (NY - 2 * F) * F + i * (NY - 2 * F) * F + j * F + k;
+    } else {
+        i = i - F; j = j - F; k = k - NZ + F;
+        m = NY * NZ * F * 2 + (NX - 2 * F) * NZ * F * 2 + i * (NY - 2 * F) * F + j * F + k;
+    }
+    return m;
+}
+
+// shell cell of saved index gid (src/savebnd2D.cl:52-93, savebnd3D.cl:46-103)
+__device__ __forceinline__ bool shell_cell(const Grid &g, int gid, int &i, int &j, int &k)
+{
+    BndDims b = bnd_dims(g);
+    int F = g.F, NAB = g.nab, gidf;
+    if (g.nd != 3) {
+        j = 0;
+        int NZ = b.NZbnd, NX = b.NXbnd;
+        if (gid < NZ * F) { gidf = gid; i = gidf / NZ + b.lbnd; k = gidf % NZ + b.lbnds; }
+        else if (gid < NZ * F * 2) { gidf = gid - NZ * F; i = gidf / NZ + NX + NAB; k = gidf % NZ + b.lbnds; }
+        else if (gid < NZ * F * 2 + (NX - 2 * F) * F) {
+            gidf = gid - NZ * F * 2; i = gidf % (NX - 2 * F) + b.lbnd + F; k = gidf / (NX - 2 * F) + NZ + b.lbnds - F;
+        } else if (gid < NZ * F * 2 + (NX - 2 * F) * 2 * F) {
+            gidf = gid - NZ * F * 2 - (NX - 2 * F) * F; i = gidf % (NX - 2 * F) + b.lbnd + F; k = gidf / (NX - 2 * F) + b.lbnds;
+        } else return false;
+        return true;
+    }
+    int NX = b.NXbnd, NY = b.NYbnd, NZ = b.NZbnd;
+    int a0 = NY * NZ * F, a1 = NZ * (NX - 2 * F) * F, a2 = (NY - 2 * F) * (NX - 2 * F) * F;
+    if (gid < a0) { gidf = gid; i = gidf / (NY * NZ) + b.lbnd; j = (gidf / NZ) % NY + b.lbnd; k = gidf % NZ + b.lbnds; }
+    else if (gid < 2 * a0) { gidf = gid - a0; i = gidf / (NY * NZ) + NX + NAB; j = (gidf / NZ) % NY + b.lbnd; k = gidf % NZ + b.lbnds; }
+    else if (gid < 2 * a0 + a1) { gidf = gid - 2 * a0; i = gidf / (NZ * F) + b.lbnd + F; j = (gidf / NZ) % F + b.lbnd; k = gidf % NZ + b.lbnds; }
+    else if (gid < 2 * a0 + 2 * a1) { gidf = gid - 2 * a0 - a1; i = gidf / (NZ * F) + b.lbnd + F; j = (gidf / NZ) % F + NY + NAB; k = gidf % NZ + b.lbnds; }
+    else if (gid < 2 * a0 + 2 * a1 + a2) {
+        gidf = gid - 2 * a0 - 2 * a1;
+        i = gidf / (F * (NY - 2 * F)) + b.lbnd + F; j = (gidf / F) % (NY - 2 * F) + b.lbnd + F; k = gidf % F + NZ + b.lbnds - F;
+    } else if (gid < 2 * a0 + 2 * a1 + 2 * a2) {
+        gidf = gid - 2 * a0 - 2 * a1 - a2;
+        i = gidf / (F * (NY - 2 * F)) + b.lbnd + F; j = (gidf / F) % (NY - 2 * F) + b.lbnd + F; k = gidf % F + b.lbnds;
+    } else return false;
+    return true;
+}
+
+// ------------------------------------------------------------------ taper
+template <int NF>
+__device__ __forceinline__ void apply_taper(const Grid &g, const float *taper, int gz, int gy, int gx,
+                                            float *const *fs, i64 iv)
+{
+    int F = g.F, NAB = g.nab;
+    if (!g.freesurf && gz - F < NAB) { float t = __ldg(taper + gz - F); for (int q = 0; q < NF; q++) fs[q][iv] *= t; }
+    if (gz > g.NZ - NAB - F - 1) { float t = __ldg(taper + g.NZ - F - gz - 1); for (int q = 0; q < NF; q++) fs[q][iv] *= t; }
+    if (g.nd == 3) {
+        if (gy - F < NAB) { float t = __ldg(taper + gy - F); for (int q = 0; q < NF; q++) fs[q][iv] *= t; }
+        if (gy > g.NY - NAB - F - 1) { float t = __ldg(taper + g.NY - F - gy - 1); for (int q = 0; q < NF; q++) fs[q][iv] *= t; }
+    }
+    if (gx - F < NAB) { float t = __ldg(taper + gx - F); for (int q = 0; q < NF; q++) fs[q][iv] *= t; }
+    if (gx > g.NX - NAB - F - 1) { float t = __ldg(taper + g.NX - F - gx - 1); for (int q = 0; q < NF; q++) fs[q][iv] *= t; }
+}
+
+// ===================================================================== 2D
+// CPML on the stress derivatives (update_v2D.cl:146-207)
+__device__ __forceinline__ void cpml_v2d(const Grid &g, const Fields &f, int gz, int gx, float &sxx_x,
+                                         float &szz_z, float &sxz_x, float &sxz_z)
+{
+    int F = g.F, NAB = g.nab, NZ = g.NZ, NX = g.NX;
+    if (gz > NZ - NAB - F - 1) {
+        int i = gx - F, k = gz - NZ + NAB + F + NAB, ind = 2 * NAB - 1 - k;
+        i64 q = (i64)i * (2 * NAB) + k;
+        cpml(f.psi[PSXZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, sxz_z);
+        cpml(f.psi[PSZZ_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, szz_z);
+    } else if (!g.freesurf && gz - F < NAB) {
+        int i = gx - F, k = gz - F;
+        i64 q = (i64)i * (2 * NAB) + k;
+        cpml(f.psi[PSXZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], k, sxz_z);
+        cpml(f.psi[PSZZ_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], k, szz_z);
+    }
+    if (gx - F < NAB) {
+        int i = gx - F, k = gz - F;
+        i64 q = (i64)i * g.nz + k;
+        cpml(f.psi[PSXX_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], i, sxx_x);
+        cpml(f.psi[PSXZ_X], q, f.cx[CK], f.cx[CA], f.cx[CB], i, sxz_x);
+    }
+    if (gx > NX - NAB - F - 1) {
+        int i = gx - NX + NAB + F + NAB, k = gz - F, ind = 2 * NAB - 1 - i;
+        i64 q = (i64)i * g.nz + k;
+        cpml(f.psi[PSXX_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, sxx_x);
+        cpml(f.psi[PSXZ_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, sxz_x);
+    }
+}
+
+// CPML on the velocity derivatives (update_s2D.cl:145-208)
+__device__ __forceinline__ void cpml_s2d(const Grid &g, const Fields &f, int gz, int gx, float &vxx, float &vxz,
+                                         float &vzx, float &vzz)
+{
+    int F = g.F, NAB = g.nab, NZ = g.NZ, NX = g.NX;
+    if (gz > NZ - NAB - F - 1) {
+        int i = gx - F, k = gz - NZ + NAB + F + NAB, ind = 2 * NAB - 1 - k;
+        i64 q = (i64)i * (2 * NAB) + k;
+        cpml(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, vxz);
+        cpml(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, vzz);
+    } else if (!g.freesurf && gz - F < NAB) {
+        int i = gx - F, k = gz - F;
+        i64 q = (i64)i * (2 * NAB) + k;
+        cpml(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], k, vxz);
+        cpml(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], k, vzz);
+    }
+    if (gx - F < NAB) {
+        int i = gx - F, k = gz - F;
+        i64 q = (i64)i * g.nz + k;
+        cpml(f.psi[PVX_X], q, f.cx[CK], f.cx[CA], f.cx[CB], i, vxx);
+        cpml(f.psi[PVZ_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], i, vzx);
+    }
+    if (gx > NX - NAB - F - 1) {
+        int i = gx - NX + NAB + F + NAB, k = gz - F, ind = 2 * NAB - 1 - i;
+        i64 q = (i64)i * g.nz + k;
+        cpml(f.psi[PVX_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, vxx);
+        cpml(f.psi[PVZ_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, vzx);
+    }
+}
+
+template <int F>
+__global__ void __launch_bounds__(256) k_v2d(Grid g, Fields f)
+{
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
+    i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
+    const float *hc = g.hc;
+    float sxx_x = dfw<F>(f.w[SXX], iv, g.NZ, hc);
+    float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc);
+    float sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
+    float sxz_x = dbw<F>(f.w[SXZ], iv, g.NZ, hc);
+    if (g.abs_type == 1) cpml_v2d(g, f, gz, gx, sxx_x, szz_z, sxz_x, sxz_z);
+    f.w[VX][iv] += (sxx_x + sxz_z) * __ldg(f.p[PRIP] + ip);
+    f.w[VZ][iv] += (szz_z + sxz_x) * __ldg(f.p[PRKP] + ip);
+    if (g.abs_type == 2) {
+        float *fs[2] = {f.w[VX], f.w[VZ]};
+        apply_taper<2>(g, f.taper, gz, 0, gx, fs, iv);
+    }
+}
+
+template <int F>
+__global__ void __launch_bounds__(256) k_s2d(Grid g, Fields f)
+{
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
+    i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
+    const float *hc = g.hc;
+    float vxx = dbw<F>(f.w[VX], iv, g.NZ, hc);
+    float vxz = dfw<F>(f.w[VX], iv, 1, hc);
+    float vzz = dbw<F>(f.w[VZ], iv, 1, hc);
+    float vzx = dfw<F>(f.w[VZ], iv, g.NZ, hc);
+    if (g.abs_type == 1) cpml_s2d(g, f, gz, gx, vxx, vxz, vzx, vzz);
+    const int L = g.L;
+    if (L == 0) {
+        float fipkp = __ldg(f.p[PMUIPKP] + ip);
+        float fm = 2.0f * __ldg(f.p[PMU] + ip);
+        float gm = __ldg(f.p[PM] + ip);
+        f.w[SXZ][iv] += fipkp * (vxz + vzx);
+        f.w[SXX][iv] += gm * (vxx + vzz) - fm * vzz;
+        f.w[SZZ][iv] += gm * (vxx + vzz) - fm * vxx;
+    } else {
+        float lM = __ldg(f.p[PM] + ip), lmu = __ldg(f.p[PMU] + ip), lmuipkp = __ldg(f.p[PMUIPKP] + ip);
+        float ltaup = __ldg(f.p[PTAUP] + ip), ltaus = __ldg(f.p[PTAUS] + ip), ltausipkp = __ldg(f.p[PTAUSIPKP] + ip);
+        float fipkp = lmuipkp * (1.0f + (float)L * ltausipkp);
+        float gm = lM * (1.0f + (float)L * ltaup);
+        float fm = 2.0f * lmu * (1.0f + (float)L * ltaus);
+        float dipkp = lmuipkp * ltausipkp / g.dt;
+        float d = 2.0f * lmu * ltaus / g.dt;
+        float e = lM * ltaup / g.dt;
+        float *rxx = f.r[RXX], *rzz = f.r[RZZ], *rxz = f.r[RXZ];
+        float sxz_ = 0, sxx_ = 0, szz_ = 0;
+        for (int l = 0; l < L; l++) {
+            i64 ir = l * g.nvol + iv;
+            sxz_ += rxz[ir]; sxx_ += rxx[ir]; szz_ += rzz[ir];
+        }
+        float lsxz = fipkp * (vxz + vzx) + g.dt2 * sxz_;
+        float lsxx = (gm * (vxx + vzz) - fm * vzz) + g.dt2 * sxx_;
+        float lszz = (gm * (vxx + vzz) - fm * vxx) + g.dt2 * szz_;
+        sxz_ = sxx_ = szz_ = 0;
+        for (int l = 0; l < L; l++) {
+            float el = g.eta[l];
+            float b = 1.0f / (1.0f + el * 0.5f), c = 1.0f - el * 0.5f;
+            i64 ir = l * g.nvol + iv;
+            float a1 = b * (rxz[ir] * c - el * (dipkp * (vxz + vzx)));
+            float a2 = b * (rxx[ir] * c - el * (e * (vxx + vzz) - d * vzz));
+            float a3 = b * (rzz[ir] * c - el * (e * (vxx + vzz) - d * vxx));
+            rxz[ir] = a1; rxx[ir] = a2; rzz[ir] = a3;
+            sxz_ += a1; sxx_ += a2; szz_ += a3;
+        }
+        f.w[SXZ][iv] += lsxz + g.dt2 * sxz_;
+        f.w[SXX][iv] += lsxx + g.dt2 * sxx_;
+        f.w[SZZ][iv] += lszz + g.dt2 * szz_;
+    }
+    if (g.abs_type == 2) {
+        float *fs[3] = {f.w[SXX], f.w[SZZ], f.w[SXZ]};
+        apply_taper<3>(g, f.taper, gz, 0, gx, fs, iv);
+    }
+}
+
+// free surface, one thread per surface column (surface2D.cl:30-193)
+template <int F>
+__global__ void k_surf2d(Grid g, Fields f, int pdir)
+{
+    int gx = blockIdx.x * blockDim.x + threadIdx.x + F;
+    if (gx > g.NX - F - 1) return;
+    int gz = F, NZ = g.NZ, L = g.L, NAB = g.nab;
+    i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * NZ + gz;
+    float *vx = f.w[VX], *vz = f.w[VZ], *sxx = f.w[SXX], *szz = f.w[SZZ], *sxz = f.w[SXZ];
+    szz[iv] = 0.0f;
+    for (int l = 0; l < L; l++) f.r[RZZ][l * g.nvol + iv] = 0.0f;
+#pragma unroll
+    for (int m = 1; m <= F; m++) {
+        szz[iv - m] = -szz[iv + m];
+        sxz[iv - m] = -sxz[iv + m - 1];
+    }
+    float vxx = dbw_rw<F>(vx, iv, NZ, g.hc);
+    float vzz = dbw_rw<F>(vz, iv, 1, g.hc);
+    if (g.abs_type == 1) {
+        if (gx - F < NAB) {
+            int i = gx - F;
+            vxx = vxx / f.cx[CK][i] + f.psi[PVX_X][(i64)i * g.nz + (gz - F)];
+        }
+        if (gx > g.NX - NAB - F - 1) {
+            int i = gx - g.NX + NAB + F + NAB, ind = 2 * NAB - 1 - i;
+            vxx = vxx / f.cx[CK][ind + 1] + f.psi[PVX_X][(i64)i * g.nz + (gz - F)];
+        }
+    }
+    if (L == 0) {
+        float fm = f.p[PMU][ip] * 2.0f, gm = f.p[PM][ip];
+        float h = -((gm - fm) * (gm - fm) * vxx / gm) - ((gm - fm) * vzz);
+        sxx[iv] += pdir * h;
+    } else {
+        float taus = f.p[PTAUS][ip], taup = f.p[PTAUP][ip], mu = f.p[PMU][ip], M = f.p[PM][ip];
+        float fm = mu * 2.0f * (1.0f + L * taus);
+        float gm = M * (1.0f + L * taup);
+        float h = -((gm - fm) * (gm - fm) * vxx / gm) - ((gm - fm) * vzz);
+        float sump = 0;
+        for (int l = 0; l < L; l++) sump += f.r[RXX][l * g.nvol + iv];
+        h += -g.dt2 * sump;
+        sxx[iv] += pdir * h;
+        float d = 2.0f * mu * taus / g.dt, e = M * taup / g.dt;
+        sump = 0;
+        for (int l = 0; l < L; l++) {
+            float b = g.eta[l] / (1.0f + g.eta[l] * 0.5f);
+            float hh = b * (((d - e) * ((fm / gm) - 1.0f) * vxx) - ((d - e) * vzz));
+            float r = f.r[RXX][l * g.nvol + iv] + pdir * hh;
+            f.r[RXX][l * g.nvol + iv] = r;
+            sump += r;
+        }
+        sxx[iv] += pdir * (g.dt2 * sump);
+    }
+}
+
+// ===================================================================== 3D
+__device__ __forceinline__ void cpml_v3d(const Grid &g, const Fields &f, int gz, int gy, int gx, float &sxx_x,
+                                         float &syy_y, float &szz_z, float &sxy_y, float &sxy_x, float &syz_y,
+                                         float &syz_z, float &sxz_x, float &sxz_z)
+{
+    int F = g.F, NAB = g.nab, NZ = g.NZ, NY = g.NY, NX = g.NX;
+    i64 nz = g.nz, ny = g.ny;
+    if (gz > NZ - NAB - F - 1) {
+        i64 i = gx - F, j = gy - F, k = gz - NZ + NAB + F + NAB;
+        int ind = 2 * NAB - 1 - (int)k;
+        i64 q = (i * ny + j) * (2 * NAB) + k;
+        cpml(f.psi[PSXZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, sxz_z);
+        cpml(f.psi[PSYZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, syz_z);
+        cpml(f.psi[PSZZ_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, szz_z);
+    } else if (!g.freesurf && gz - F < NAB) {
+        i64 i = gx - F, j = gy - F, k = gz - F;
+        i64 q = (i * ny + j) * (2 * NAB) + k;
+        cpml(f.psi[PSXZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, sxz_z);
+        cpml(f.psi[PSYZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, syz_z);
+        cpml(f.psi[PSZZ_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, szz_z);
+    }
+    if (gy - F < NAB) {
+        i64 i = gx - F, j = gy - F, k = gz - F;
+        i64 q = (i * (2 * NAB) + j) * nz + k;
+        cpml(f.psi[PSXY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], (int)j, sxy_y);
+        cpml(f.psi[PSYY_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, syy_y);
+        cpml(f.psi[PSYZ_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], (int)j, syz_y);
+    } else if (gy > NY - NAB - F - 1) {
+        i64 i = gx - F, j = gy - NY + NAB + F + NAB, k = gz - F;
+        int ind = 2 * NAB - 1 - (int)j;
+        i64 q = (i * (2 * NAB) + j) * nz + k;
+        cpml(f.psi[PSXY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], ind + 1, sxy_y);
+        cpml(f.psi[PSYY_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, syy_y);
+        cpml(f.psi[PSYZ_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], ind + 1, syz_y);
+    }
+    if (gx - F < NAB) {
+        i64 i = gx - F, j = gy - F, k = gz - F;
+        i64 q = (i * ny + j) * nz + k;
+        cpml(f.psi[PSXX_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, sxx_x);
+        cpml(f.psi[PSXY_X], q, f.cx[CK], f.cx[CA], f.cx[CB], (int)i, sxy_x);
+        cpml(f.psi[PSXZ_X], q, f.cx[CK], f.cx[CA], f.cx[CB], (int)i, sxz_x);
+    }
+    if (gx > NX - NAB - F - 1) {
+        i64 i = gx - NX + NAB + F + NAB, j = gy - F, k = gz - F;
+        int ind = 2 * NAB - 1 - (int)i;
+        i64 q = (i * ny + j) * nz + k;
+        cpml(f.psi[PSXX_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, sxx_x);
+        cpml(f.psi[PSXY_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, sxy_x);
+        cpml(f.psi[PSXZ_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, sxz_x);
+    }
+}
+
+// update_s3D.cl:190-298 (plain "if"s); the adjoint form uses "else if" for the
+// z-top and y-far branches (update_adjs3D.cl)
+__device__ __forceinline__ void cpml_s3d(const Grid &g, const Fields &f, int gz, int gy, int gx, float &vxx,
+                                         float &vxy, float &vxz, float &vyx, float &vyy, float &vyz, float &vzx,
+                                         float &vzy, float &vzz, bool adjoint_form)
+{
+    int F = g.F, NAB = g.nab, NZ = g.NZ, NY = g.NY, NX = g.NX;
+    i64 nz = g.nz, ny = g.ny;
+    bool zb = gz > NZ - NAB - F - 1;
+    if (zb) {
+        i64 i = gx - F, j = gy - F, k = gz - NZ + NAB + F + NAB;
+        int ind = 2 * NAB - 1 - (int)k;
+        i64 q = (i * ny + j) * (2 * NAB) + k;
+        cpml(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, vxz);
+        cpml(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, vyz);
+        cpml(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, vzz);
+    }
+    if (!g.freesurf && gz - F < NAB && !(adjoint_form && zb)) {
+        i64 i = gx - F, j = gy - F, k = gz - F;
+        i64 q = (i * ny + j) * (2 * NAB) + k;
+        cpml(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, vxz);
+        cpml(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, vyz);
+        cpml(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, vzz);
+    }
+    bool yb = gy - F < NAB;
+    if (yb) {
+        i64 i = gx - F, j = gy - F, k = gz - F;
+        i64 q = (i * (2 * NAB) + j) * nz + k;
+        cpml(f.psi[PVX_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, vxy);
+        cpml(f.psi[PVY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], (int)j, vyy);
+        cpml(f.psi[PVZ_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, vzy);
+    }
+    if (gy > NY - NAB - F - 1 && !(adjoint_form && yb)) {
+        i64 i = gx - F, j = gy - NY + NAB + F + NAB, k = gz - F;
+        int ind = 2 * NAB - 1 - (int)j;
+        i64 q = (i * (2 * NAB) + j) * nz + k;
+        cpml(f.psi[PVX_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, vxy);
+        cpml(f.psi[PVY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], ind + 1, vyy);
+        cpml(f.psi[PVZ_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, vzy);
+    }
+    if (gx - F < NAB) {
+        i64 i = gx - F, j = gy - F, k = gz - F;
+        i64 q = (i * ny + j) * nz + k;
+        cpml(f.psi[PVX_X], q, f.cx[CK], f.cx[CA], f.cx[CB], (int)i, vxx);
+        cpml(f.psi[PVY_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, vyx);
+        cpml(f.psi[PVZ_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, vzx);
+    }
+    if (gx > NX - NAB - F - 1) {
+        i64 i = gx - NX + NAB + F + NAB, j = gy - F, k = gz - F;
+        int ind = 2 * NAB - 1 - (int)i;
+        i64 q = (i * ny + j) * nz + k;
+        cpml(f.psi[PVX_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, vxx);
+        cpml(f.psi[PVY_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, vyx);
+        cpml(f.psi[PVZ_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, vzx);
+    }
+}
+
+#define CELL3D                                                                         \
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;                                \
+    int gy = blockIdx.y * blockDim.y + threadIdx.y + F;                                \
+    int gx = blockIdx.z * blockDim.z + threadIdx.z + F;                                \
+    if (gz > g.NZ - F - 1 || gy > g.NY - F - 1 || gx > g.NX - F - 1) return;           \
+    const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;                                        \
+    i64 iv = gx * sx + (i64)gy * sy + gz;                                              \
+    i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz - F);
+
+template <int F>
+__global__ void __launch_bounds__(256) k_v3d(Grid g, Fields f)
+{
+    CELL3D
+    const float *hc = g.hc;
+    float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc);
+    float sxx_x = dfw<F>(f.w[SXX], iv, sx, hc);
+    float sxz_x = dbw<F>(f.w[SXZ], iv, sx, hc);
+    float sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
+    float syz_y = dbw<F>(f.w[SYZ], iv, sy, hc);
+    float syz_z = dbw<F>(f.w[SYZ], iv, 1, hc);
+    float syy_y = dfw<F>(f.w[SYY], iv, sy, hc);
+    float sxy_x = dbw<F>(f.w[SXY], iv, sx, hc);
+    float sxy_y = dbw<F>(f.w[SXY], iv, sy, hc);
+    if (g.abs_type == 1) cpml_v3d(g, f, gz, gy, gx, sxx_x, syy_y, szz_z, sxy_y, sxy_x, syz_y, syz_z, sxz_x, sxz_z);
+    f.w[VX][iv] += (sxx_x + sxy_y + sxz_z) * __ldg(f.p[PRIP] + ip);
+    f.w[VY][iv] += (syy_y + sxy_x + syz_z) * __ldg(f.p[PRJP] + ip);
+    f.w[VZ][iv] += (szz_z + sxz_x + syz_y) * __ldg(f.p[PRKP] + ip);
+    if (g.abs_type == 2) {
+        float *fs[3] = {f.w[VX], f.w[VY], f.w[VZ]};
+        apply_taper<3>(g, f.taper, gz, gy, gx, fs, iv);
+    }
+}
+
+template <int F>
+__global__ void __launch_bounds__(256) k_s3d(Grid g, Fields f)
+{
+    CELL3D
+    const float *hc = g.hc;
+    float vzx = dfw<F>(f.w[VZ], iv, sx, hc), vzy = dfw<F>(f.w[VZ], iv, sy, hc), vzz = dbw<F>(f.w[VZ], iv, 1, hc);
+    float vyx = dfw<F>(f.w[VY], iv, sx, hc), vyy = dbw<F>(f.w[VY], iv, sy, hc), vyz = dfw<F>(f.w[VY], iv, 1, hc);
+    float vxx = dbw<F>(f.w[VX], iv, sx, hc), vxy = dfw<F>(f.w[VX], iv, sy, hc), vxz = dfw<F>(f.w[VX], iv, 1, hc);
+    if (g.abs_type == 1) cpml_s3d(g, f, gz, gy, gx, vxx, vxy, vxz, vyx, vyy, vyz, vzx, vzy, vzz, false);
+    float vxyyx = vxy + vyx, vyzzy = vyz + vzy, vxzzx = vxz + vzx;
+    float vxxyyzz = vxx + vyy + vzz, vyyzz = vyy + vzz, vxxzz = vxx + vzz, vxxyy = vxx + vyy;
+    const int L = g.L;
+    if (L == 0) {
+        float fipjp = __ldg(f.p[PMUIPJP] + ip), fjpkp = __ldg(f.p[PMUJPKP] + ip), fipkp = __ldg(f.p[PMUIPKP] + ip);
+        float gm = __ldg(f.p[PM] + ip), fm = 2.0f * __ldg(f.p[PMU] + ip);
+        f.w[SXY][iv] += fipjp * vxyyx;
+        f.w[SYZ][iv] += fjpkp * vyzzy;
+        f.w[SXZ][iv] += fipkp * vxzzx;
+        f.w[SXX][iv] += gm * vxxyyzz - fm * vyyzz;
+        f.w[SYY][iv] += gm * vxxyyzz - fm * vxxzz;
+        f.w[SZZ][iv] += gm * vxxyyzz - fm * vxxyy;
+    } else {
+        float lM = __ldg(f.p[PM] + ip), lmu = __ldg(f.p[PMU] + ip);
+        float lmuipkp = __ldg(f.p[PMUIPKP] + ip), lmuipjp = __ldg(f.p[PMUIPJP] + ip), lmujpkp = __ldg(f.p[PMUJPKP] + ip);
+        float ltaup = __ldg(f.p[PTAUP] + ip), ltaus = __ldg(f.p[PTAUS] + ip);
+        float ltausipkp = __ldg(f.p[PTAUSIPKP] + ip), ltausipjp = __ldg(f.p[PTAUSIPJP] + ip),
+              ltausjpkp = __ldg(f.p[PTAUSJPKP] + ip);
+        float fipjp = lmuipjp * (1.0f + (float)L * ltausipjp);
+        float fjpkp = lmujpkp * (1.0f + (float)L * ltausjpkp);
+        float fipkp = lmuipkp * (1.0f + (float)L * ltausipkp);
+        float gm = lM * (1.0f + (float)L * ltaup);
+        float fm = 2.0f * lmu * (1.0f + (float)L * ltaus);
+        float dipjp = lmuipjp * ltausipjp / g.dt, djpkp = lmujpkp * ltausjpkp / g.dt, dipkp = lmuipkp * ltausipkp / g.dt;
+        float d = 2.0f * lmu * ltaus / g.dt, e = lM * ltaup / g.dt;
+        float a[6] = {0, 0, 0, 0, 0, 0};
+        float *const *r = f.r;
+        for (int l = 0; l < L; l++) {
+            i64 ir = l * g.nvol + iv;
+            a[0] += r[RXY][ir]; a[1] += r[RYZ][ir]; a[2] += r[RXZ][ir];
+            a[3] += r[RXX][ir]; a[4] += r[RYY][ir]; a[5] += r[RZZ][ir];
+        }
+        float lsxy = fipjp * vxyyx + g.dt2 * a[0];
+        float lsyz = fjpkp * vyzzy + g.dt2 * a[1];
+        float lsxz = fipkp * vxzzx + g.dt2 * a[2];
+        float lsxx = (gm * vxxyyzz - fm * vyyzz) + g.dt2 * a[3];
+        float lsyy = (gm * vxxyyzz - fm * vxxzz) + g.dt2 * a[4];
+        float lszz = (gm * vxxyyzz - fm * vxxyy) + g.dt2 * a[5];
+        for (int q = 0; q < 6; q++) a[q] = 0;
+        for (int l = 0; l < L; l++) {
+            float el = g.eta[l];
+            float b = 1.0f / (1.0f + el * 0.5f), c = 1.0f - el * 0.5f;
+            i64 ir = l * g.nvol + iv;
+            float n0 = b * (r[RXY][ir] * c - el * (dipjp * vxyyx));
+            float n1 = b * (r[RYZ][ir] * c - el * (djpkp * vyzzy));
+            float n2 = b * (r[RXZ][ir] * c - el * (dipkp * vxzzx));
+            float n3 = b * (r[RXX][ir] * c - el * (e * vxxyyzz - d * vyyzz));
+            float n4 = b * (r[RYY][ir] * c - el * (e * vxxyyzz - d * vxxzz));
+            float n5 = b * (r[RZZ][ir] * c - el * (e * vxxyyzz - d * vxxyy));
+            r[RXY][ir] = n0; r[RYZ][ir] = n1; r[RXZ][ir] = n2; r[RXX][ir] = n3; r[RYY][ir] = n4; r[RZZ][ir] = n5;
+            a[0] += n0; a[1] += n1; a[2] += n2; a[3] += n3; a[4] += n4; a[5] += n5;
+        }
+        f.w[SXY][iv] += lsxy + g.dt2 * a[0];
+        f.w[SYZ][iv] += lsyz + g.dt2 * a[1];
+        f.w[SXZ][iv] += lsxz + g.dt2 * a[2];
+        f.w[SXX][iv] += lsxx + g.dt2 * a[3];
+        f.w[SYY][iv] += lsyy + g.dt2 * a[4];
+        f.w[SZZ][iv] += lszz + g.dt2 * a[5];
+    }
+    if (g.abs_type == 2) {
+        float *fs[6] = {f.w[SXY], f.w[SYZ], f.w[SXZ], f.w[SXX], f.w[SYY], f.w[SZZ]};
+        apply_taper<6>(g, f.taper, gz, gy, gx, fs, iv);
+    }
+}
+
+// free surface 3D, one thread per (y, x) column (surface3D.cl:39-271)
+template <int F>
+__global__ void k_surf3d(Grid g, Fields f, int pdir)
+{
+    int gy = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gy > g.NY - F - 1 || gx > g.NX - F - 1) return;
+    int gz = F, NAB = g.nab, L = g.L;
+    const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;
+    i64 iv = gx * sx + (i64)gy * sy + gz;
+    i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz - F);
+    float *sxx = f.w[SXX], *syy = f.w[SYY], *szz = f.w[SZZ], *syz = f.w[SYZ], *sxz = f.w[SXZ];
+    szz[iv] = 0.0f;
+    for (int l = 0; l < L; l++) f.r[RZZ][l * g.nvol + iv] = 0.0f;
+#pragma unroll
+    for (int m = 1; m <= F; m++) {
+        szz[iv - m] = -szz[iv + m];
+        sxz[iv - m] = -sxz[iv + m - 1];
+        syz[iv - m] = -syz[iv + m - 1];
+    }
+    float vxx = dbw_rw<F>(f.w[VX], iv, sx, g.hc);
+    float vyy = dbw_rw<F>(f.w[VY], iv, sy, g.hc);
+    float vzz = dbw_rw<F>(f.w[VZ], iv, 1, g.hc);
+    if (g.abs_type == 1) {
+        i64 nz = g.nz, ny = g.ny;
+        if (gy - F < NAB) {
+            i64 i = gx - F, j = gy - F;
+            vyy = vyy / f.cy[CK][j] + f.psi[PVY_Y][(i * (2 * NAB) + j) * nz];
+        } else if (gy > g.NY - NAB - F - 1) {
+            i64 i = gx - F, j = gy - g.NY + NAB + F + NAB;
+            int ind = 2 * NAB - 1 - (int)j;
+            vyy = vyy / f.cy[CK][ind + 1] + f.psi[PVY_Y][(i * (2 * NAB) + j) * nz];
+        }
+        if (gx - F < NAB) {
+            i64 i = gx - F, j = gy - F;
+            vxx = vxx / f.cx[CK][i] + f.psi[PVX_X][(i * ny + j) * nz];
+        }
+        if (gx > g.NX - NAB - F - 1) {
+            i64 i = gx - g.NX + NAB + F + NAB, j = gy - F;
+            int ind = 2 * NAB - 1 - (int)i;
+            vxx = vxx / f.cx[CK][ind + 1] + f.psi[PVX_X][(i * ny + j) * nz];
+        }
+    }
+    if (L == 0) {
+        float fm = f.p[PMU][ip] * 2.0f, gm = f.p[PM][ip];
+        float h = -((gm - fm) * (gm - fm) * (vxx + vyy) / gm) - ((gm - fm) * vzz);
+        // the reference adds h without the propagation direction (surface3D.cl:172-173)
+        sxx[iv] += h;
+        syy[iv] += h;
+    } else {
+        float taus = f.p[PTAUS][ip], taup = f.p[PTAUP][ip], mu = f.p[PMU][ip], M = f.p[PM][ip];
+        float fm = mu * 2.0f * (1.0f + L * taus);
+        float gm = M * (1.0f + L * taup);
+        float h = -((gm - fm) * (gm - fm) * (vxx + vyy) / gm) - ((gm - fm) * vzz);
+        float sumx = 0, sumy = 0;
+        for (int l = 0; l < L; l++) { sumx += f.r[RXX][l * g.nvol + iv]; sumy += f.r[RYY][l * g.nvol + iv]; }
+        sxx[iv] += pdir * (h - g.dt2 * sumx);
+        syy[iv] += pdir * (h - g.dt2 * sumy);
+        float d = 2.0f * mu * taus / g.dt, e = M * taup / g.dt;
+        sumx = 0; sumy = 0;
+        for (int l = 0; l < L; l++) {
+            float b = g.eta[l] / (1.0f + g.eta[l] * 0.5f);
+            float hh = b * (((d - e) * ((fm / gm) - 1.0f) * (vxx + vyy)) - ((d - e) * vzz));
+            float rx = f.r[RXX][l * g.nvol + iv] + hh, ry = f.r[RYY][l * g.nvol + iv] + hh;
+            f.r[RXX][l * g.nvol + iv] = rx;
+            f.r[RYY][l * g.nvol + iv] = ry;
+            sumx += rx; sumy += ry;
+        }
+        sxx[iv] += g.dt2 * sumx;
+        syy[iv] += g.dt2 * sumy;
+    }
+}
+
+// ---------------------------------------------------- boundary save (forward)
+template <typename T>
+__global__ void k_savebnd(Grid g, Fields f, BndSlot b, i64 tofs)
+{
+    int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= g.nbnd) return;
+    int i, j, k;
+    if (!shell_cell(g, gid, i, j, k)) return;
+    i64 iv = ((i64)i * g.NY + j) * g.NZ + k;
+    for (int q = 0; q < b.nfield; q++) {
+        int w = b.fields[q];
+        ((T *)b.p[w])[tofs + gid] = from_f<T>(f.w[w][iv]);
+    }
+}
+
+// ------------------------------------------------------- adjoint kernels 2D
+template <int F, typename T>
+__global__ void __launch_bounds__(256) k_adjv2d(Grid g, Fields f, AdjFields a)
+{
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
+    i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
+    const float *hc = g.hc;
+    float sxx_x = dfw<F>(f.w[SXX], iv, g.NZ, hc);
+    float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc);
+    float sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
+    float sxz_x = dbw<F>(f.w[SXZ], iv, g.NZ, hc);
+    float sxx_xr = dfw<F>(a.wr[SXX], iv, g.NZ, hc);
+    float szz_zr = dfw<F>(a.wr[SZZ], iv, 1, hc);
+    float sxz_zr = dbw<F>(a.wr[SXZ], iv, 1, hc);
+    float sxz_xr = dbw<F>(a.wr[SXZ], iv, g.NZ, hc);
+    float rip = __ldg(f.p[PRIP] + ip), rkp = __ldg(f.p[PRKP] + ip);
+    float lvx = (sxx_x + sxz_z) * rip, lvz = (szz_z + sxz_x) * rkp;
+    float vx = f.w[VX][iv] - lvx, vz = f.w[VZ][iv] - lvz;
+    int m = inject_ind2d(g, gz, gx);
+    if (m != -1) {
+        vx = to_f<T>(((const T *)a.bnd[VX])[m]);
+        vz = to_f<T>(((const T *)a.bnd[VZ])[m]);
+    }
+    f.w[VX][iv] = vx;
+    f.w[VZ][iv] = vz;
+    if (g.abs_type == 1) cpml_v2d(g, f, gz, gx, sxx_xr, szz_zr, sxz_xr, sxz_zr);
+    lvx = (sxx_xr + sxz_zr) * rip;
+    lvz = (szz_zr + sxz_xr) * rkp;
+    a.wr[VX][iv] += lvx;
+    a.wr[VZ][iv] += lvz;
+    if (g.abs_type == 2) {
+        float *fs[2] = {a.wr[VX], a.wr[VZ]};
+        apply_taper<2>(g, f.taper, gz, 0, gx, fs, iv);
+    }
+    a.grad[GRHO][ip] += (double)(-vx * lvx - vz * lvz);
+}
+
+template <int F, typename T>
+__global__ void __launch_bounds__(256) k_adjs2d(Grid g, Fields f, AdjFields a)
+{
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
+    i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
+    const float *hc = g.hc;
+    float vxx = dbw<F>(f.w[VX], iv, g.NZ, hc), vxz = dfw<F>(f.w[VX], iv, 1, hc);
+    float vzz = dbw<F>(f.w[VZ], iv, 1, hc), vzx = dfw<F>(f.w[VZ], iv, g.NZ, hc);
+    float vxxr = dbw<F>(a.wr[VX], iv, g.NZ, hc), vxzr = dfw<F>(a.wr[VX], iv, 1, hc);
+    float vzzr = dbw<F>(a.wr[VZ], iv, 1, hc), vzxr = dfw<F>(a.wr[VZ], iv, g.NZ, hc);
+    const int L = g.L;
+    float lM = __ldg(f.p[PM] + ip), lmu = __ldg(f.p[PMU] + ip), fipkp, fm, gm, dipkp = 0, d = 0, e = 0;
+    if (L == 0) {
+        fipkp = __ldg(f.p[PMUIPKP] + ip);
+        fm = 2.0f * lmu;
+        gm = lM;
+    } else {
+        float lmuipkp = __ldg(f.p[PMUIPKP] + ip), ltaup = __ldg(f.p[PTAUP] + ip), ltaus = __ldg(f.p[PTAUS] + ip);
+        float ltausipkp = __ldg(f.p[PTAUSIPKP] + ip);
+        fipkp = lmuipkp * (1.0f + (float)L * ltausipkp);
+        gm = lM * (1.0f + (float)L * ltaup);
+        fm = 2.0f * lmu * (1.0f + (float)L * ltaus);
+        dipkp = lmuipkp * ltausipkp / g.dt;
+        d = 2.0f * lmu * ltaus / g.dt;
+        e = lM * ltaup / g.dt;
+    }
+    float sxx = f.w[SXX][iv], szz = f.w[SZZ][iv], sxz = f.w[SXZ][iv];
+    // reconstruct the forward stresses (update_adjs2D.cl:222-278)
+    if (L == 0) {
+        sxz -= fipkp * (vxz + vzx);
+        sxx -= gm * (vxx + vzz) - fm * vzz;
+        szz -= gm * (vxx + vzz) - fm * vxx;
+    } else {
+        float *rxx = f.r[RXX], *rzz = f.r[RZZ], *rxz = f.r[RXZ];
+        float s1 = 0, s2 = 0, s3 = 0;
+        for (int l = 0; l < L; l++) { i64 ir = l * g.nvol + iv; s1 += rxz[ir]; s2 += rxx[ir]; s3 += rzz[ir]; }
+        float lsxz = fipkp * (vxz + vzx) + g.dt2 * s1;
+        float lsxx = (gm * (vxx + vzz) - fm * vzz) + g.dt2 * s2;
+        float lszz = (gm * (vxx + vzz) - fm * vxx) + g.dt2 * s3;
+        s1 = s2 = s3 = 0;
+        for (int l = 0; l < L; l++) {
+            float el = g.eta[l];
+            float b = 1.0f / (1.0f - el * 0.5f), c = 1.0f + el * 0.5f;
+            i64 ir = l * g.nvol + iv;
+            float n1 = b * (rxz[ir] * c - el * (dipkp * (vxz + vzx)));
+            float n2 = b * (rxx[ir] * c - el * (e * (vxx + vzz) - d * vzz));
+            float n3 = b * (rzz[ir] * c - el * (e * (vxx + vzz) - d * vxx));
+            rxz[ir] = n1; rxx[ir] = n2; rzz[ir] = n3;
+            s1 += n1; s2 += n2; s3 += n3;
+        }
+        sxz -= lsxz + g.dt2 * s1;
+        sxx -= lsxx + g.dt2 * s2;
+        szz -= lszz + g.dt2 * s3;
+    }
+    int m = inject_ind2d(g, gz, gx);
+    if (m != -1) {
+        sxx = to_f<T>(((const T *)a.bnd[SXX])[m]);
+        szz = to_f<T>(((const T *)a.bnd[SZZ])[m]);
+        sxz = to_f<T>(((const T *)a.bnd[SXZ])[m]);
+    }
+    f.w[SXX][iv] = sxx; f.w[SZZ][iv] = szz; f.w[SXZ][iv] = sxz;
+    if (g.abs_type == 1) cpml_s2d(g, f, gz, gx, vxxr, vxzr, vzxr, vzzr);
+    float lsxz, lsxx, lszz;
+    if (L == 0) {
+        lsxz = fipkp * (vxzr + vzxr);
+        lsxx = gm * (vxxr + vzzr) - fm * vzzr;
+        lszz = gm * (vxxr + vzzr) - fm * vxxr;
+        a.wr[SXZ][iv] += lsxz;
+        a.wr[SXX][iv] += lsxx;
+        a.wr[SZZ][iv] += lszz;
+    } else {
+        float *rxxr = a.rr[RXX], *rzzr = a.rr[RZZ], *rxzr = a.rr[RXZ];
+        float s1 = 0, s2 = 0, s3 = 0;
+        for (int l = 0; l < L; l++) { i64 ir = l * g.nvol + iv; s1 += rxzr[ir]; s2 += rxxr[ir]; s3 += rzzr[ir]; }
+        lsxz = fipkp * (vxzr + vzxr) + g.dt2 * s1;
+        lsxx = (gm * (vxxr + vzzr) - fm * vzzr) + g.dt2 * s2;
+        lszz = (gm * (vxxr + vzzr) - fm * vxxr) + g.dt2 * s3;
+        s1 = s2 = s3 = 0;
+        // every iteration updates the last mechanism's slot, as the reference
+        // does (update_adjs2D.cl:379-391)
+        i64 ir = (L - 1) * g.nvol + iv;
+        for (int l = 0; l < L; l++) {
+            float el = g.eta[l];
+            float b = 1.0f / (1.0f + el * 0.5f), c = 1.0f - el * 0.5f;
+            float n1 = b * (rxzr[ir] * c - el * (dipkp * (vxzr + vzxr)));
+            float n2 = b * (rxxr[ir] * c - el * (e * (vxxr + vzzr) - d * vzzr));
+            float n3 = b * (rzzr[ir] * c - el * (e * (vxxr + vzzr) - d * vxxr));
+            rxzr[ir] = n1; rxxr[ir] = n2; rzzr[ir] = n3;
+            s1 += n1; s2 += n2; s3 += n3;
+        }
+        a.wr[SXZ][iv] += lsxz + g.dt2 * s1;
+        a.wr[SXX][iv] += lsxx + g.dt2 * s2;
+        a.wr[SZZ][iv] += lszz + g.dt2 * s3;
+    }
+    if (g.abs_type == 2) {
+        float *fs[3] = {a.wr[SXZ], a.wr[SXX], a.wr[SZZ]};
+        apply_taper<3>(g, f.taper, gz, 0, gx, fs, iv);
+    }
+    if (g.restype == 0) {
+        float c1 = 1.0f / ((2.0f * lM - 2.0f * lmu) * (2.0f * lM - 2.0f * lmu));
+        float c3 = 1.0f / (lmu * lmu);
+        float c5 = 0.25f * c3;
+        float dM = c1 * (sxx + szz) * (lsxx + lszz);
+        a.grad[GM][ip] += (double)(-dM);
+        a.grad[GMU][ip] += (double)(-c3 * (sxz * lsxz) + dM - c5 * ((sxx - szz) * (lsxx - lszz)));
+    } else {
+        float dM = (sxx + szz) * (lsxx + lszz);
+        a.grad[GM][ip] += (double)(-dM);
+    }
+}
+
+// surface adjoint, split in two passes so no thread updates another
+// column's cell (surface2D_adj.cl:35-148 lets neighbouring work-items add
+// into the same vxr cells).  Pass 1: per column, the L transform, the vzr
+// update of its own column, and q = hx * lsxx for pass 2.
+template <int F>
+__global__ void k_surfadj2d_a(Grid g, Fields f, AdjFields a, float *q)
+{
+    int gx = blockIdx.x * blockDim.x + threadIdx.x + F;
+    if (gx > g.NX - F - 1) return;
+    int gz = F;
+    i64 iv = (i64)gx * g.NZ + gz, ip = (i64)(gx - F) * g.nz + (gz - F);
+    float lszz = a.wr[SZZ][iv], lsxx = a.wr[SXX][iv];
+    float lmu = f.p[PMU][ip], lM = f.p[PM][ip];
+    float t1 = lsxx, t2 = lszz;
+    float aa = 1.0f / (4.0f * lM * lmu - 4.0f * lmu * lmu);
+    lsxx = -aa * (lM * t1 + (-lM + 2.0f * lmu) * t2);
+    lszz = 0.0f;
+    float hx = -((lM - lmu * 2.0f) * (lM - lmu * 2.0f) / lM);
+    float hz = -(lM - lmu * 2.0f);
+    for (int m = 0; m < F; m++)
+        a.wr[VZ][iv + m] += g.hc[m] * hz * lsxx * f.p[PRKP][ip + m];
+    q[gx - F] = hx * lsxx;
+    a.wr[SZZ][iv] = -(lM * lszz + (lM - 2.0f * lmu) * lsxx);
+    a.wr[SXX][iv] = -(lM * lsxx + (lM - 2.0f * lmu) * lszz);
+}
+// Pass 2: each column gathers the contributions of its neighbours.
+template <int F>
+__global__ void k_surfadj2d_b(Grid g, Fields f, AdjFields a, const float *q)
+{
+    int gx = blockIdx.x * blockDim.x + threadIdx.x + F;
+    if (gx > g.NX - F - 1) return;
+    int gz = F, x = gx - F, nx = g.nx;
+    i64 iv = (i64)gx * g.NZ + gz, ip = (i64)(gx - F) * g.nz + (gz - F);
+    float rip = f.p[PRIP][ip], acc = 0.0f;
+    for (int m = 0; m < F; m++) {
+        if (x - m >= 0) acc += g.hc[m] * q[x - m];
+        if (x + m + 1 < nx) acc -= g.hc[m] * q[x + m + 1];
+    }
+    a.wr[VX][iv] += acc * rip;
+}
+
+// ------------------------------------------------------- adjoint kernels 3D
+template <int F, typename T>
+__global__ void __launch_bounds__(256) k_adjv3d(Grid g, Fields f, AdjFields a)
+{
+    CELL3D
+    const float *hc = g.hc;
+    float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc), sxx_x = dfw<F>(f.w[SXX], iv, sx, hc);
+    float sxz_x = dbw<F>(f.w[SXZ], iv, sx, hc), sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
+    float syz_y = dbw<F>(f.w[SYZ], iv, sy, hc), syz_z = dbw<F>(f.w[SYZ], iv, 1, hc);
+    float syy_y = dfw<F>(f.w[SYY], iv, sy, hc);
+    float sxy_x = dbw<F>(f.w[SXY], iv, sx, hc), sxy_y = dbw<F>(f.w[SXY], iv, sy, hc);
+    float szz_zr = dfw<F>(a.wr[SZZ], iv, 1, hc), sxx_xr = dfw<F>(a.wr[SXX], iv, sx, hc);
+    float sxz_xr = dbw<F>(a.wr[SXZ], iv, sx, hc), sxz_zr = dbw<F>(a.wr[SXZ], iv, 1, hc);
+    float syz_yr = dbw<F>(a.wr[SYZ], iv, sy, hc), syz_zr = dbw<F>(a.wr[SYZ], iv, 1, hc);
+    float syy_yr = dfw<F>(a.wr[SYY], iv, sy, hc);
+    float sxy_xr = dbw<F>(a.wr[SXY], iv, sx, hc), sxy_yr = dbw<F>(a.wr[SXY], iv, sy, hc);
+    float rip = __ldg(f.p[PRIP] + ip), rjp = __ldg(f.p[PRJP] + ip), rkp = __ldg(f.p[PRKP] + ip);
+    float lvx = (sxx_x + sxy_y + sxz_z) * rip;
+    float lvy = (syy_y + sxy_x + syz_z) * rjp;
+    float lvz = (szz_z + sxz_x + syz_y) * rkp;
+    float vx = f.w[VX][iv] - lvx, vy = f.w[VY][iv] - lvy, vz = f.w[VZ][iv] - lvz;
+    int m = inject_ind3d(g, gz, gy, gx);
+    if (m != -1) {
+        vx = to_f<T>(((const T *)a.bnd[VX])[m]);
+        vy = to_f<T>(((const T *)a.bnd[VY])[m]);
+        vz = to_f<T>(((const T *)a.bnd[VZ])[m]);
+    }
+    f.w[VX][iv] = vx; f.w[VY][iv] = vy; f.w[VZ][iv] = vz;
+    if (g.abs_type == 1)
+        cpml_v3d(g, f, gz, gy, gx, sxx_xr, syy_yr, szz_zr, sxy_yr, sxy_xr, syz_yr, syz_zr, sxz_xr, sxz_zr);
+    lvx = (sxx_xr + sxy_yr + sxz_zr) * rip;
+    lvy = (syy_yr + sxy_xr + syz_zr) * rjp;
+    lvz = (szz_zr + sxz_xr + syz_yr) * rkp;
+    a.wr[VX][iv] += lvx; a.wr[VY][iv] += lvy; a.wr[VZ][iv] += lvz;
+    if (g.abs_type == 2) {
+        float *fs[3] = {a.wr[VX], a.wr[VY], a.wr[VZ]};
+        apply_taper<3>(g, f.taper, gz, gy, gx, fs, iv);
+    }
+    a.grad[GRHO][ip] += (double)(-vx * lvx - vy * lvy - vz * lvz);
+}
+
+template <int F, typename T>
+__global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
+{
+    CELL3D
+    const float *hc = g.hc;
+    float vzx = dfw<F>(f.w[VZ], iv, sx, hc), vzy = dfw<F>(f.w[VZ], iv, sy, hc), vzz = dbw<F>(f.w[VZ], iv, 1, hc);
+    float vyx = dfw<F>(f.w[VY], iv, sx, hc), vyy = dbw<F>(f.w[VY], iv, sy, hc), vyz = dfw<F>(f.w[VY], iv, 1, hc);
+    float vxx = dbw<F>(f.w[VX], iv, sx, hc), vxy = dfw<F>(f.w[VX], iv, sy, hc), vxz = dfw<F>(f.w[VX], iv, 1, hc);
+    float vzxr = dfw<F>(a.wr[VZ], iv, sx, hc), vzyr = dfw<F>(a.wr[VZ], iv, sy, hc), vzzr = dbw<F>(a.wr[VZ], iv, 1, hc);
+    float vyxr = dfw<F>(a.wr[VY], iv, sx, hc), vyyr = dbw<F>(a.wr[VY], iv, sy, hc), vyzr = dfw<F>(a.wr[VY], iv, 1, hc);
+    float vxxr = dbw<F>(a.wr[VX], iv, sx, hc), vxyr = dfw<F>(a.wr[VX], iv, sy, hc), vxzr = dfw<F>(a.wr[VX], iv, 1, hc);
+    const int L = g.L;
+    float lM = __ldg(f.p[PM] + ip), lmu = __ldg(f.p[PMU] + ip);
+    float fipjp, fjpkp, fipkp, gm, fm, dipjp = 0, djpkp = 0, dipkp = 0, d = 0, e = 0;
+    if (L == 0) {
+        fipjp = __ldg(f.p[PMUIPJP] + ip); fjpkp = __ldg(f.p[PMUJPKP] + ip); fipkp = __ldg(f.p[PMUIPKP] + ip);
+        gm = lM; fm = 2.0f * lmu;
+    } else {
+        float lmuipkp = __ldg(f.p[PMUIPKP] + ip), lmuipjp = __ldg(f.p[PMUIPJP] + ip), lmujpkp = __ldg(f.p[PMUJPKP] + ip);
+        float ltaup = __ldg(f.p[PTAUP] + ip), ltaus = __ldg(f.p[PTAUS] + ip);
+        float ltausipkp = __ldg(f.p[PTAUSIPKP] + ip), ltausipjp = __ldg(f.p[PTAUSIPJP] + ip),
+              ltausjpkp = __ldg(f.p[PTAUSJPKP] + ip);
+        fipjp = lmuipjp * (1.0f + (float)L * ltausipjp);
+        fjpkp = lmujpkp * (1.0f + (float)L * ltausjpkp);
+        fipkp = lmuipkp * (1.0f + (float)L * ltausipkp);
+        gm = lM * (1.0f + (float)L * ltaup);
+        fm = 2.0f * lmu * (1.0f + (float)L * ltaus);
+        dipjp = lmuipjp * ltausipjp / g.dt; djpkp = lmujpkp * ltausjpkp / g.dt; dipkp = lmuipkp * ltausipkp / g.dt;
+        d = 2.0f * lmu * ltaus / g.dt; e = lM * ltaup / g.dt;
+    }
+    float vxyyx = vxy + vyx, vyzzy = vyz + vzy, vxzzx = vxz + vzx;
+    float vxxyyzz = vxx + vyy + vzz, vyyzz = vyy + vzz, vxxzz = vxx + vzz, vxxyy = vxx + vyy;
+    float s[6] = {f.w[SXY][iv], f.w[SYZ][iv], f.w[SXZ][iv], f.w[SXX][iv], f.w[SYY][iv], f.w[SZZ][iv]};
+    float *const *r = f.r;
+    if (L == 0) {
+        s[0] -= fipjp * vxyyx; s[1] -= fjpkp * vyzzy; s[2] -= fipkp * vxzzx;
+        s[3] -= gm * vxxyyzz - fm * vyyzz; s[4] -= gm * vxxyyzz - fm * vxxzz; s[5] -= gm * vxxyyzz - fm * vxxyy;
+    } else {
+        float aa[6] = {0, 0, 0, 0, 0, 0};
+        for (int l = 0; l < L; l++) {
+            i64 ir = l * g.nvol + iv;
+            aa[0] += r[RXY][ir]; aa[1] += r[RYZ][ir]; aa[2] += r[RXZ][ir];
+            aa[3] += r[RXX][ir]; aa[4] += r[RYY][ir]; aa[5] += r[RZZ][ir];
+        }
+        float ls[6] = {fipjp * vxyyx + g.dt2 * aa[0], fjpkp * vyzzy + g.dt2 * aa[1], fipkp * vxzzx + g.dt2 * aa[2],
+                       (gm * vxxyyzz - fm * vyyzz) + g.dt2 * aa[3], (gm * vxxyyzz - fm * vxxzz) + g.dt2 * aa[4],
+                       (gm * vxxyyzz - fm * vxxyy) + g.dt2 * aa[5]};
+        for (int q = 0; q < 6; q++) aa[q] = 0;
+        // 3D reconstruction keeps the forward-time coefficients (update_adjs3D.cl:357-359)
+        for (int l = 0; l < L; l++) {
+            float el = g.eta[l];
+            float b = 1.0f / (1.0f + el * 0.5f), c = 1.0f - el * 0.5f;
+            i64 ir = l * g.nvol + iv;
+            float n0 = b * (r[RXY][ir] * c - el * (dipjp * vxyyx));
+            float n1 = b * (r[RYZ][ir] * c - el * (djpkp * vyzzy));
+            float n2 = b * (r[RXZ][ir] * c - el * (dipkp * vxzzx));
+            float n3 = b * (r[RXX][ir] * c - el * (e * vxxyyzz - d * vyyzz));
+            float n4 = b * (r[RYY][ir] * c - el * (e * vxxyyzz - d * vxxzz));
+            float n5 = b * (r[RZZ][ir] * c - el * (e * vxxyyzz - d * vxxyy));
+            r[RXY][ir] = n0; r[RYZ][ir] = n1; r[RXZ][ir] = n2; r[RXX][ir] = n3; r[RYY][ir] = n4; r[RZZ][ir] = n5;
+            aa[0] += n0; aa[1] += n1; aa[2] += n2; aa[3] += n3; aa[4] += n4; aa[5] += n5;
+        }
+        for (int q = 0; q < 6; q++) s[q] -= ls[q] + g.dt2 * aa[q];
+    }
+    int m = inject_ind3d(g, gz, gy, gx);
+    if (m != -1) {
+        s[3] = to_f<T>(((const T *)a.bnd[SXX])[m]); s[4] = to_f<T>(((const T *)a.bnd[SYY])[m]);
+        s[5] = to_f<T>(((const T *)a.bnd[SZZ])[m]); s[0] = to_f<T>(((const T *)a.bnd[SXY])[m]);
+        s[1] = to_f<T>(((const T *)a.bnd[SYZ])[m]); s[2] = to_f<T>(((const T *)a.bnd[SXZ])[m]);
+    }
+    f.w[SXY][iv] = s[0]; f.w[SYZ][iv] = s[1]; f.w[SXZ][iv] = s[2];
+    f.w[SXX][iv] = s[3]; f.w[SYY][iv] = s[4]; f.w[SZZ][iv] = s[5];
+    if (g.abs_type == 1) cpml_s3d(g, f, gz, gy, gx, vxxr, vxyr, vxzr, vyxr, vyyr, vyzr, vzxr, vzyr, vzzr, true);
+    float vxyyxr = vxyr + vyxr, vyzzyr = vyzr + vzyr, vxzzxr = vxzr + vzxr;
+    float vxxyyzzr = vxxr + vyyr + vzzr, vyyzzr = vyyr + vzzr, vxxzzr = vxxr + vzzr, vxxyyr = vxxr + vyyr;
+    float ls[6];
+    ls[0] = fipjp * vxyyxr; ls[1] = fjpkp * vyzzyr; ls[2] = fipkp * vxzzxr;
+    ls[3] = gm * vxxyyzzr - fm * vyyzzr; ls[4] = gm * vxxyyzzr - fm * vxxzzr; ls[5] = gm * vxxyyzzr - fm * vxxyyr;
+    float *const *wr = a.wr;
+    const int sid[6] = {SXY, SYZ, SXZ, SXX, SYY, SZZ};
+    if (L == 0) {
+        for (int q = 0; q < 6; q++) wr[sid[q]][iv] += ls[q];
+    } else {
+        float *const *rr = a.rr;
+        const int rid[6] = {RXY, RYZ, RXZ, RXX, RYY, RZZ};
+        float aa[6] = {0, 0, 0, 0, 0, 0};
+        for (int l = 0; l < L; l++) {
+            i64 ir = l * g.nvol + iv;
+            for (int q = 0; q < 6; q++) aa[q] += rr[rid[q]][ir];
+        }
+        for (int q = 0; q < 6; q++) ls[q] += g.dt2 * aa[q];
+        // the reference stores these into the forward memory variables and
+        // keeps only the last adjoint value of each sum (update_adjs3D.cl:566-583)
+        for (int l = 0; l < L; l++) {
+            float el = g.eta[l];
+            float b = 1.0f / (1.0f + el * 0.5f), c = 1.0f - el * 0.5f;
+            i64 ir = l * g.nvol + iv;
+            r[RXY][ir] = b * (rr[RXY][ir] * c - el * (dipjp * vxyyxr));
+            r[RYZ][ir] = b * (rr[RYZ][ir] * c - el * (djpkp * vyzzyr));
+            r[RXZ][ir] = b * (rr[RXZ][ir] * c - el * (dipkp * vxzzxr));
+            r[RXX][ir] = b * (rr[RXX][ir] * c - el * (e * vxxyyzzr - d * vyyzzr));
+            r[RYY][ir] = b * (rr[RYY][ir] * c - el * (e * vxxyyzzr - d * vxxzzr));
+            r[RZZ][ir] = b * (rr[RZZ][ir] * c - el * (e * vxxyyzzr - d * vxxyyr));
+            for (int q = 0; q < 6; q++) aa[q] = rr[rid[q]][ir];
+        }
+        for (int q = 0; q < 6; q++) wr[sid[q]][iv] += ls[q] + g.dt2 * aa[q];
+    }
+    if (g.abs_type == 2) {
+        float *fs[6] = {wr[SXY], wr[SYZ], wr[SXZ], wr[SXX], wr[SYY], wr[SZZ]};
+        apply_taper<6>(g, f.taper, gz, gy, gx, fs, iv);
+    }
+    float sxx = s[3], syy = s[4], szz = s[5], sxy = s[0], syz = s[1], sxz = s[2];
+    float lsxy = ls[0], lsyz = ls[1], lsxz = ls[2], lsxx = ls[3], lsyy = ls[4], lszz = ls[5];
+    if (g.restype == 0) {
+        float c1 = 1.0f / (3.0f * lM - 4.0f * lmu) / (3.0f * lM - 4.0f * lmu);
+        float c3 = 1.0f / lmu / lmu;
+        float c5 = 1.0f / 6.0f * c3;
+        float dM = c1 * (sxx + syy + szz) * (lsxx + lsyy + lszz);
+        a.grad[GM][ip] += (double)(-dM);
+        a.grad[GMU][ip] += (double)(-c3 * (sxz * lsxz + sxy * lsxy + syz * lsyz) + 4.0f / 3.0f * dM -
+                                    c5 * (lsxx * (2.0f * sxx - syy - szz) + lsyy * (2.0f * syy - sxx - szz) +
+                                          lszz * (2.0f * szz - sxx - syy)));
+    } else {
+        float dM = (sxx + syy + szz) * (lsxx + lsyy + lszz);
+        a.grad[GM][ip] += (double)(-dM);
+    }
+}
+
+// surface adjoint 3D (surface3D_adj.cl:29-116), two passes like 2D.  The
+// reference reads the syy component from sxxr (:62).
+template <int F>
+__global__ void k_surfadj3d_a(Grid g, Fields f, AdjFields a, float *q)
+{
+    int gy = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gy > g.NY - F - 1 || gx > g.NX - F - 1) return;
+    int gz = F;
+    const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;
+    i64 iv = gx * sx + (i64)gy * sy + gz;
+    i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz - F);
+    float lszz = -a.wr[SZZ][iv], lsxx = -a.wr[SXX][iv], lsyy = -a.wr[SXX][iv];
+    float lmu = f.p[PMU][ip], lM = f.p[PM][ip];
+    float t1 = lsxx, t2 = lsyy, t3 = lszz;
+    float aa = 1.0f / (6.0f * lM * lmu - 8.0f * lmu * lmu);
+    lsxx = aa * (2.0f * (lM - lmu) * t1 + (-lM + 2.0f * lmu) * (t2 + t3));
+    lsyy = aa * (2.0f * (lM - lmu) * t2 + (-lM + 2.0f * lmu) * (t1 + t3));
+    lszz = 0.0f;
+    float h = -((lM - lmu * 2.0f) * (lM - lmu * 2.0f) / lM);
+    float hz = -(lM - lmu * 2.0f);
+    for (int m = 0; m < F; m++) a.wr[VZ][iv + m] += g.hc[m] * hz * (lsxx + lsyy) * f.p[PRKP][ip + m];
+    q[(i64)(gx - F) * g.ny + (gy - F)] = h * (lsxx + lsyy);
+    a.wr[SXX][iv] = -(lM * lsxx + (lM - 2.0f * lmu) * (lsyy + lszz));
+    a.wr[SYY][iv] = -(lM * lsyy + (lM - 2.0f * lmu) * (lsxx + lszz));
+    a.wr[SZZ][iv] = -(lM * lszz + (lM - 2.0f * lmu) * (lsxx + lsyy));
+}
+template <int F>
+__global__ void k_surfadj3d_b(Grid g, Fields f, AdjFields a, const float *q)
+{
+    int gy = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gy > g.NY - F - 1 || gx > g.NX - F - 1) return;
+    int gz = F, x = gx - F, y = gy - F, nx = g.nx, ny = g.ny;
+    const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;
+    i64 iv = gx * sx + (i64)gy * sy + gz;
+    i64 ip = ((i64)x * g.ny + y) * g.nz;
+    float accx = 0.0f, accy = 0.0f;
+    for (int m = 0; m < F; m++) {
+        if (x - m >= 0) accx += g.hc[m] * q[(i64)(x - m) * ny + y];
+        if (x + m + 1 < nx) accx -= g.hc[m] * q[(i64)(x + m + 1) * ny + y];
+        if (y - m >= 0) accy += g.hc[m] * q[(i64)x * ny + (y - m)];
+        if (y + m + 1 < ny) accy -= g.hc[m] * q[(i64)x * ny + (y + m + 1)];
+    }
+    a.wr[VX][iv] += accx * f.p[PRIP][ip];
+    a.wr[VY][iv] += accy * f.p[PRJP][ip];
+}
+
+// ------------------------------------------------ point kernels (per shot)
+// src/automatic_kernels.c:394-629; several sources may share a cell
+__global__ void k_sources(Fields f, PointSet s, const float *src, int nt_total, int t, int pdir, float dt,
+                          int freesurf, int F)
+{
+    int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= s.n) return;
+    i64 cell = s.cell[gid];
+    if (cell < 0) return;
+    if (freesurf && pdir == -1 && s.kz[gid] < 2 * F) return;
+    float amp = (float)pdir * (dt * src[(i64)gid * nt_total + t]);
+    for (int q = 0; q < s.ntarget[gid]; q++) {
+        float dv = s.div[gid * 3 + q];
+        float val = dv == 0.0f ? amp : amp / dv;
+        atomicAdd(f.w[s.field[gid * 3 + q]] + cell, val);
+    }
+}
+
+// src/automatic_kernels.c:22-219; out is [nsel][nrec][NT]
+__global__ void k_record(Fields f, PointSet r, float *out, int nt_total, int t, unsigned outmask, int nd)
+{
+    int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= r.n) return;
+    i64 cell = r.cell[gid];
+    if (cell < 0) return;
+    int slot = 0;
+    for (int o = 0; o < SFD_NOUT; o++) {
+        if (!(outmask & (1u << o))) continue;
+        float v;
+        if (o == SFD_OUT_P) {
+            if (nd == 3) v = (f.w[SXX][cell] + f.w[SZZ][cell] + f.w[SYY][cell]) / 3.0f;
+            else v = (f.w[SXX][cell] + f.w[SZZ][cell]) / 2.0f;
+        } else {
+            v = f.w[o][cell];
+        }
+        out[((i64)slot * r.n + gid) * nt_total + t] = v;
+        slot++;
+    }
+}
+
+// src/automatic_kernels.c:631-836; res is [nsel][nrec][NT]
+__global__ void k_residuals(AdjFields a, PointSet r, const float *res, int nt_total, int t, unsigned outmask, int nd)
+{
+    int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= r.n) return;
+    i64 cell = r.cell[gid];
+    if (cell < 0) return;
+    int slot = 0;
+    for (int o = 0; o < SFD_NOUT; o++) {
+        if (!(outmask & (1u << o))) continue;
+        float v = res[((i64)slot * r.n + gid) * nt_total + t];
+        if (o == SFD_OUT_P) {
+            float n2 = nd == 3 ? 3.0f : 2.0f;
+            atomicAdd(a.wr[SXX] + cell, v / n2);
+            atomicAdd(a.wr[SZZ] + cell, v / n2);
+            if (nd == 3) atomicAdd(a.wr[SYY] + cell, v / n2);
+        } else {
+            atomicAdd(a.wr[o] + cell, v);
+        }
+        slot++;
+    }
+}
+
+// ------------------------------------------------------------- launchers
+static inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
+
+#define DISPATCH_F(F, ...)                                                      \
+    switch (F) {                                                               \
+    case 1: { constexpr int FF = 1; __VA_ARGS__; } break;                      \
+    case 2: { constexpr int FF = 2; __VA_ARGS__; } break;                      \
+    case 3: { constexpr int FF = 3; __VA_ARGS__; } break;                      \
+    case 4: { constexpr int FF = 4; __VA_ARGS__; } break;                      \
+    case 5: { constexpr int FF = 5; __VA_ARGS__; } break;                      \
+    case 6: { constexpr int FF = 6; __VA_ARGS__; } break;                      \
+    default: break;                                                            \
+    }
+
+void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
+{
+    if (g.nd == 3) {
+        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
+        DISPATCH_F(g.F, k_v3d<FF><<<gr, b, 0, st>>>(g, f));
+    } else {
+        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
+        DISPATCH_F(g.F, k_v2d<FF><<<gr, b, 0, st>>>(g, f));
+    }
+}
+
+void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
+{
+    if (g.nd == 3) {
+        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
+        DISPATCH_F(g.F, k_s3d<FF><<<gr, b, 0, st>>>(g, f));
+    } else {
+        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
+        DISPATCH_F(g.F, k_s2d<FF><<<gr, b, 0, st>>>(g, f));
+    }
+}
+
+void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st)
+{
+    if (g.nd == 3) {
+        dim3 b(32, 4), gr(cdiv(g.ny, 32), cdiv(g.nx, 4));
+        DISPATCH_F(g.F, k_surf3d<FF><<<gr, b, 0, st>>>(g, f, pdir));
+    } else {
+        DISPATCH_F(g.F, k_surf2d<FF><<<cdiv(g.nx, 128), 128, 0, st>>>(g, f, pdir));
+    }
+}
+
+void launch_savebnd(const Grid &g, const Fields &f, const BndSlot &b, int prec, int64_t tofs, cudaStream_t st)
+{
+    unsigned gr = cdiv(g.nbnd, 256);
+    if (gr == 0) return;
+    if (prec == SFD_PREC_FP16) k_savebnd<__half><<<gr, 256, 0, st>>>(g, f, b, tofs);
+    else if (prec == SFD_PREC_BF16) k_savebnd<__nv_bfloat16><<<gr, 256, 0, st>>>(g, f, b, tofs);
+    else k_savebnd<float><<<gr, 256, 0, st>>>(g, f, b, tofs);
+}
+
+template <typename T>
+static void launch_adj_t(const Grid &g, const Fields &f, const AdjFields &a, bool stress, cudaStream_t st)
+{
+    if (g.nd == 3) {
+        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
+        if (stress) DISPATCH_F(g.F, k_adjs3d<FF, T><<<gr, b, 0, st>>>(g, f, a))
+        else DISPATCH_F(g.F, k_adjv3d<FF, T><<<gr, b, 0, st>>>(g, f, a))
+    } else {
+        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
+        if (stress) DISPATCH_F(g.F, k_adjs2d<FF, T><<<gr, b, 0, st>>>(g, f, a))
+        else DISPATCH_F(g.F, k_adjv2d<FF, T><<<gr, b, 0, st>>>(g, f, a))
+    }
+}
+
+void launch_update_adj(const Grid &g, const Fields &f, const AdjFields &a, bool stress, int prec, cudaStream_t st)
+{
+    if (prec == SFD_PREC_FP16) launch_adj_t<__half>(g, f, a, stress, st);
+    else if (prec == SFD_PREC_BF16) launch_adj_t<__nv_bfloat16>(g, f, a, stress, st);
+    else launch_adj_t<float>(g, f, a, stress, st);
+}
+
+void launch_surface_adj(const Grid &g, const Fields &f, const AdjFields &a, float *q, cudaStream_t st)
+{
+    if (g.nd == 3) {
+        dim3 b(32, 4), gr(cdiv(g.ny, 32), cdiv(g.nx, 4));
+        DISPATCH_F(g.F, k_surfadj3d_a<FF><<<gr, b, 0, st>>>(g, f, a, q));
+        DISPATCH_F(g.F, k_surfadj3d_b<FF><<<gr, b, 0, st>>>(g, f, a, q));
+    } else {
+        DISPATCH_F(g.F, k_surfadj2d_a<FF><<<cdiv(g.nx, 128), 128, 0, st>>>(g, f, a, q));
+        DISPATCH_F(g.F, k_surfadj2d_b<FF><<<cdiv(g.nx, 128), 128, 0, st>>>(g, f, a, q));
+    }
+}
+
+void launch_sources(const Grid &g, const Fields &f, const PointSet &s, const float *src, int nt_total, int t,
+                    int pdir, cudaStream_t st)
+{
+    if (s.n == 0) return;
+    k_sources<<<cdiv(s.n, 128), 128, 0, st>>>(f, s, src, nt_total, t, pdir, g.dt, g.freesurf, g.F);
+}
+
+void launch_record(const Grid &g, const Fields &f, const PointSet &r, float *out, int nt_total, int t,
+                   unsigned outmask, cudaStream_t st)
+{
+    if (r.n == 0 || outmask == 0) return;
+    k_record<<<cdiv(r.n, 128), 128, 0, st>>>(f, r, out, nt_total, t, outmask, g.nd);
+}
+
+void launch_residuals(const Grid &g, const AdjFields &a, const PointSet &r, const float *res, int nt_total, int t,
+                      unsigned outmask, cudaStream_t st)
+{
+    if (r.n == 0 || outmask == 0) return;
+    k_residuals<<<cdiv(r.n, 128), 128, 0, st>>>(a, r, res, nt_total, t, outmask, g.nd);
+}
+
+}  // namespace sfd

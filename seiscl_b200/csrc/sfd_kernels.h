@@ -1,0 +1,29 @@
+// sfd_kernels.h -- launchers of the FDTD kernels (host side).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "sfd_internal.h"
+
+namespace sfd {
+
+struct BndSlot {            // saved-boundary stores, by value
+    void *p[NW];
+    int nfield;
+    int fields[NW];
+};
+
+void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st);
+void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st);
+void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st);
+void launch_savebnd(const Grid &g, const Fields &f, const BndSlot &b, int prec, int64_t tofs, cudaStream_t st);
+void launch_update_adj(const Grid &g, const Fields &f, const AdjFields &a, bool stress, int prec, cudaStream_t st);
+void launch_surface_adj(const Grid &g, const Fields &f, const AdjFields &a, float *q, cudaStream_t st);
+void launch_sources(const Grid &g, const Fields &f, const PointSet &s, const float *src, int nt_total, int t,
+                    int pdir, cudaStream_t st);
+void launch_record(const Grid &g, const Fields &f, const PointSet &r, float *out, int nt_total, int t,
+                   unsigned outmask, cudaStream_t st);
+void launch_residuals(const Grid &g, const AdjFields &a, const PointSet &r, const float *res, int nt_total, int t,
+                      unsigned outmask, cudaStream_t st);
+
+}  // namespace sfd

@@ -1,0 +1,340 @@
+"""ctypes binding of libseiscl_b200.so (the C ABI in include/seiscl_b200.h).
+
+The product path: every call goes to the CUDA library.  There is no CPU
+fallback; if the library cannot be loaded, or no CUDA device is present,
+the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libseiscl_b200.so")
+
+OUT_NAMES = ["vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "syz", "sxz", "p"]
+PREC = {"fp32": 0, "fp16": 1, "bf16": 2}
+ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "CFL violated", -4: "out of device memory",
+          -5: "call out of order", -6: "unstable", -7: "unsupported"}
+
+
+class SeisCLEngineError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (ERRORS.get(code, "error"), code, msg))
+        self.code = code
+
+
+class sfd_config(C.Structure):
+    _fields_ = [("nd", C.c_int), ("n", C.c_int * 3), ("nt", C.c_int), ("fdorder", C.c_int),
+                ("maxrelerror", C.c_int), ("L", C.c_int), ("freesurf", C.c_int), ("abs_type", C.c_int),
+                ("nab", C.c_int), ("dt", C.c_float), ("dh", C.c_float), ("f0", C.c_float),
+                ("fl", C.c_float * 8), ("vppml", C.c_float), ("fpml", C.c_float), ("npower", C.c_float),
+                ("k_max_cpml", C.c_float), ("abpc", C.c_float), ("tmin", C.c_int), ("tmax", C.c_int),
+                ("param_type", C.c_int), ("restype", C.c_int), ("precision", C.c_int),
+                ("reserved", C.c_int * 7)]
+
+
+class sfd_shot(C.Structure):
+    _fields_ = [("nsrc", C.c_int), ("nrec", C.c_int), ("src_pos", C.POINTER(C.c_float)),
+                ("src", C.POINTER(C.c_float)), ("rec_pos", C.POINTER(C.c_float))]
+
+
+FP = C.POINTER(C.c_float)
+EXPORTS = {
+    "sfd_plan_create": (C.c_int, [C.POINTER(sfd_config), C.POINTER(C.c_void_p)]),
+    "sfd_plan_destroy": (None, [C.c_void_p]),
+    "sfd_last_error": (C.c_char_p, [C.c_void_p]),
+    "sfd_set_model": (C.c_int, [C.c_void_p, C.POINTER(FP)]),
+    "sfd_source_type_mask": (C.c_int, [FP, C.c_int]),
+    "sfd_forward": (C.c_int, [C.c_void_p, C.POINTER(sfd_shot), C.c_int, C.POINTER(C.c_int), C.POINTER(FP),
+                              C.c_int, C.c_void_p]),
+    "sfd_adjoint": (C.c_int, [C.c_void_p, C.POINTER(sfd_shot), C.c_int, C.POINTER(C.c_int), C.POINTER(FP),
+                              C.c_void_p]),
+    "sfd_zero_gradient": (C.c_int, [C.c_void_p]),
+    "sfd_get_gradient": (C.c_int, [C.c_void_p, C.c_int, FP, FP, FP]),
+    "sfd_residual_scale": (C.c_int, [C.c_void_p, C.POINTER(sfd_shot), C.POINTER(C.c_int), C.POINTER(FP)]),
+    "sfd_plan_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "sfd_debug_copy": (C.c_int64, [C.c_void_p, C.c_int, C.c_int, FP, C.c_int64]),
+    "sfd_last_loop_ms": (C.c_float, [C.c_void_p]),
+    "sfd_bench_kernels": (C.c_int, [C.c_void_p, C.c_int, FP]),
+    "sfd_host_transform": (C.c_int, [C.POINTER(sfd_config), C.POINTER(FP), C.POINTER(FP)]),
+    "sfd_host_point_cells": (C.c_int, [C.POINTER(sfd_config), FP, C.c_int, C.c_int, C.POINTER(C.c_int64)]),
+    "sfd_host_source_targets": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
+    "sfd_host_cpml": (C.c_int, [C.POINTER(sfd_config), FP]),
+}
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the CUDA library.  Raises if it is missing: there is no fallback."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise FileNotFoundError("libseiscl_b200.so not built (run __graft_entry__.build()): %s" % path)
+    lib = C.CDLL(path)
+    for name, (res, args) in EXPORTS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None:
+        a = a.reshape(shape)
+    return a
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(FP)
+
+
+def source_type_mask(src_pos) -> int:
+    sp = _f32(src_pos).reshape(-1, 5)
+    return int(load_library().sfd_source_type_mask(_ptr(sp), sp.shape[0]))
+
+
+@dataclass
+class Config:
+    """The csts keys of SeisCL.py:23-30 used by the single-device path.
+
+    ``N`` is [NZ, NX] (2D) or [NZ, NY, NX] (3D) as in SeisCL."""
+    N: Sequence[int]
+    ND: int = 2
+    dh: float = 10.0
+    dt: float = 0.0008
+    NT: int = 875
+    L: int = 0
+    f0: float = 15.0
+    FL: Sequence[float] = (15.0,)
+    FDORDER: int = 8
+    MAXRELERROR: int = 1
+    freesurf: int = 0
+    abs_type: int = 1
+    VPPML: float = 3500.0
+    NPOWER: float = 2.0
+    FPML: float = 15.0
+    K_MAX_CPML: float = 2.0
+    nab: int = 16
+    abpc: float = 6.0
+    tmin: int = 0
+    tmax: int = 0
+    param_type: int = 0
+    restype: int = 0
+    precision: str = "fp32"
+
+    def to_c(self) -> sfd_config:
+        c = sfd_config()
+        c.nd = int(self.ND)
+        n = list(self.N)
+        for i in range(3):
+            c.n[i] = int(n[i]) if i < len(n) else 0
+        c.nt = int(self.NT)
+        c.fdorder = int(self.FDORDER)
+        c.maxrelerror = int(self.MAXRELERROR)
+        c.L = int(self.L)
+        c.freesurf = int(self.freesurf)
+        c.abs_type = int(self.abs_type)
+        c.nab = int(self.nab)
+        c.dt = float(self.dt)
+        c.dh = float(self.dh)
+        c.f0 = float(self.f0)
+        fl = list(np.atleast_1d(self.FL).astype(float))
+        for i in range(8):
+            c.fl[i] = fl[i] if i < len(fl) else 0.0
+        c.vppml = float(self.VPPML)
+        c.fpml = float(self.FPML)
+        c.npower = float(self.NPOWER)
+        c.k_max_cpml = float(self.K_MAX_CPML)
+        c.abpc = float(self.abpc)
+        c.tmin = int(self.tmin)
+        c.tmax = int(self.tmax)
+        c.param_type = int(self.param_type)
+        c.restype = int(self.restype)
+        c.precision = PREC[self.precision]
+        return c
+
+    @property
+    def model_shape(self):
+        """Host layout of a parameter array: [nx][nz] or [nx][ny][nz]."""
+        n = list(self.N)
+        return (n[2], n[1], n[0]) if self.ND == 3 else (n[1], n[0])
+
+
+class Plan:
+    """One grid on the current CUDA device (a thin wrapper of sfd_plan)."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        self.lib = load_library()
+        self._c = cfg.to_c()
+        h = C.c_void_p()
+        rc = self.lib.sfd_plan_create(C.byref(self._c), C.byref(h))
+        if rc:
+            raise SeisCLEngineError(rc, "sfd_plan_create rejected the configuration")
+        self.h = h
+        info = (C.c_int64 * 8)()
+        self.lib.sfd_plan_info(self.h, info)
+        self.NZp, self.NYp, self.NXp, self.nvol, self.npar, self.nbnd, self.F, self.tmax = [int(v) for v in info]
+
+    def _check(self, rc):
+        if rc:
+            raise SeisCLEngineError(rc, self.lib.sfd_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sfd_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_model(self, vp, vs, rho, taup=None, taus=None):
+        """Parameters in host layout [nx][(ny)][nz], z fastest."""
+        sh = self.cfg.model_shape
+        arrs = [None if a is None else _f32(a, sh) for a in (vp, vs, rho, taup, taus)]
+        ptrs = (FP * 5)(*[_ptr(a) for a in arrs])
+        self._check(self.lib.sfd_set_model(self.h, ptrs))
+
+    @staticmethod
+    def _shot(src_pos, src, rec_pos, nt):
+        sp = _f32(src_pos).reshape(-1, 5)
+        rp = _f32(rec_pos).reshape(-1, 8)
+        s = _f32(src).reshape(sp.shape[0], nt)
+        shot = sfd_shot(sp.shape[0], rp.shape[0], _ptr(sp), _ptr(s), _ptr(rp))
+        return shot, (sp, s, rp)
+
+    def forward(self, src_pos, src, rec_pos, outputs, mask=None, save_boundaries=False) -> Dict[str, np.ndarray]:
+        nt = self.cfg.NT
+        shot, keep = self._shot(src_pos, src, rec_pos, nt)
+        if mask is None:
+            mask = source_type_mask(src_pos)
+        sel = (C.c_int * 10)()
+        outs = {}
+        ptrs = (FP * 10)()
+        for n in outputs:
+            i = OUT_NAMES.index(n)
+            sel[i] = 1
+            outs[n] = np.zeros((shot.nrec, nt), np.float32)
+            ptrs[i] = _ptr(outs[n])
+        self._check(self.lib.sfd_forward(self.h, C.byref(shot), int(mask), sel, ptrs,
+                                         1 if save_boundaries else 0, None))
+        return outs
+
+    def adjoint(self, src_pos, src, rec_pos, residuals: Dict[str, np.ndarray], mask=None):
+        nt = self.cfg.NT
+        shot, keep = self._shot(src_pos, src, rec_pos, nt)
+        if mask is None:
+            mask = source_type_mask(src_pos)
+        sel = (C.c_int * 10)()
+        ptrs = (FP * 10)()
+        res = {}
+        for n, r in residuals.items():
+            i = OUT_NAMES.index(n)
+            sel[i] = 1
+            res[n] = _f32(r, (shot.nrec, nt))
+            ptrs[i] = _ptr(res[n])
+        self._check(self.lib.sfd_adjoint(self.h, C.byref(shot), int(mask), sel, ptrs, None))
+
+    def residual_scale(self, rec_pos, residuals: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
+        nt = self.cfg.NT
+        rp = _f32(rec_pos).reshape(-1, 8)
+        shot = sfd_shot(0, rp.shape[0], None, None, _ptr(rp))
+        sel = (C.c_int * 10)()
+        ptrs = (FP * 10)()
+        out = {}
+        for n, r in residuals.items():
+            i = OUT_NAMES.index(n)
+            sel[i] = 1
+            out[n] = np.array(r, dtype=np.float32, copy=True).reshape(rp.shape[0], nt)
+            ptrs[i] = _ptr(out[n])
+        self._check(self.lib.sfd_residual_scale(self.h, C.byref(shot), sel, ptrs))
+        return out
+
+    def zero_gradient(self):
+        self._check(self.lib.sfd_zero_gradient(self.h))
+
+    def gradient(self, transform=True):
+        sh = self.cfg.model_shape
+        g = [np.zeros(sh, np.float32) for _ in range(3)]
+        self._check(self.lib.sfd_get_gradient(self.h, 1 if transform else 0, *[_ptr(a) for a in g]))
+        if transform:
+            names = {0: ("vp", "vs", "rho"), 1: ("M", "mu", "rho"), 2: ("Ip", "Is", "rho")}[self.cfg.param_type]
+        else:
+            names = ("M", "mu", "rho")
+        return dict(zip(names, g))
+
+    def debug_array(self, kind: int, idx: int, n: int) -> np.ndarray:
+        out = np.zeros(n, np.float32)
+        got = self.lib.sfd_debug_copy(self.h, kind, idx, _ptr(out), n)
+        if got < 0:
+            self._check(int(got))
+        return out[:got]
+
+    def bench_kernels(self, nrep: int = 20):
+        """Mean ms per launch of (velocity, stress, surface) kernels."""
+        out = (C.c_float * 3)()
+        self._check(self.lib.sfd_bench_kernels(self.h, int(nrep), out))
+        return list(out)
+
+    @property
+    def last_loop_ms(self) -> float:
+        return float(self.lib.sfd_last_loop_ms(self.h))
+
+
+# ---------------------------------------------------------------- host-only
+PARAM_NAMES = ["M", "mu", "rho", "taup", "taus", "rip", "rjp", "rkp", "muipkp", "muipjp", "mujpkp",
+               "tausipkp", "tausipjp", "tausjpkp"]
+
+
+def host_transform(cfg: Config, vp, vs, rho, taup=None, taus=None) -> Dict[str, np.ndarray]:
+    """Transformed parameters exactly as sfd_set_model uploads them."""
+    lib = load_library()
+    sh = cfg.model_shape
+    arrs = [None if a is None else _f32(a, sh) for a in (vp, vs, rho, taup, taus)]
+    outs = [np.zeros(sh, np.float32) for _ in PARAM_NAMES]
+    c = cfg.to_c()
+    rc = lib.sfd_host_transform(C.byref(c), (FP * 5)(*[_ptr(a) for a in arrs]), (FP * 14)(*[_ptr(o) for o in outs]))
+    if rc:
+        raise SeisCLEngineError(rc, "host transform failed")
+    return dict(zip(PARAM_NAMES, outs))
+
+
+def host_point_cells(cfg: Config, pos, stride: int) -> np.ndarray:
+    lib = load_library()
+    p = _f32(pos).reshape(-1, stride)
+    cells = np.zeros(p.shape[0], np.int64)
+    c = cfg.to_c()
+    rc = lib.sfd_host_point_cells(C.byref(c), _ptr(p), p.shape[0], stride, cells.ctypes.data_as(C.POINTER(C.c_int64)))
+    if rc < 0:
+        raise SeisCLEngineError(rc, "point mapping failed")
+    return cells
+
+
+def host_source_targets(nd: int, mask: int, stype: int):
+    lib = load_library()
+    f = (C.c_int * 3)()
+    d = (C.c_float * 3)()
+    n = lib.sfd_host_source_targets(nd, mask, stype, f, d)
+    return [(OUT_NAMES[f[i]], float(d[i])) for i in range(n)]
+
+
+def host_cpml(cfg: Config) -> np.ndarray:
+    lib = load_library()
+    out = np.zeros((6, 2 * cfg.nab), np.float32)
+    c = cfg.to_c()
+    rc = lib.sfd_host_cpml(C.byref(c), _ptr(out))
+    if rc:
+        raise SeisCLEngineError(rc, "cpml failed")
+    return out

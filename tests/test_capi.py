@@ -1,0 +1,60 @@
+"""The C-ABI library loads on a machine without a GPU and exports every
+function declared in include/*.h."""
+import glob
+import os
+import re
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"\b(sfd_[a-z0-9_]+)\s*\(", src):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    from seiscl_b200.engine import load_library
+
+    lib = load_library()
+    names = declared_functions()
+    assert len(names) >= 15
+    for n in sorted(names):
+        assert hasattr(lib, n), n
+
+
+def test_plan_create_without_gpu_fails_cleanly():
+    """Without a device the plan cannot be created; the call returns an error
+    code instead of crashing."""
+    import torch
+
+    from seiscl_b200.engine import Config, Plan, SeisCLEngineError
+
+    if torch.cuda.is_available():
+        return
+    try:
+        Plan(Config(N=[40, 40], ND=2, NT=10, nab=8))
+    except SeisCLEngineError as e:
+        assert e.code == -2
+    else:
+        raise AssertionError("plan creation should fail without a CUDA device")
+
+
+def test_invalid_configs_rejected():
+    import ctypes as C
+
+    from seiscl_b200.engine import Config, load_library
+
+    lib = load_library()
+    for bad in (dict(N=[41, 40]), dict(N=[40, 40], FDORDER=7), dict(N=[40, 40], MAXRELERROR=5),
+                dict(N=[40, 40], ND=5), dict(N=[40, 40], L=9)):
+        kw = dict(ND=2, NT=10, nab=8)
+        kw.update(bad)
+        c = Config(**kw).to_c()
+        h = C.c_void_p()
+        rc = lib.sfd_plan_create(C.byref(c), C.byref(h))
+        assert rc in (-1, -7), bad

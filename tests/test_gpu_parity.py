@@ -1,0 +1,120 @@
+"""CUDA path vs the CPU oracle on the same seeded inputs.
+
+Forward seismograms and adjoint gradients go through the C ABI
+(libseiscl_b200.so).  The oracle is the C restatement in oracle/ (pinned
+bit-exact to the reference kernels by tests/test_oracle_pin.py).
+
+Tolerances (relative L2 over each output):
+  forward seismograms   2e-5   (FP32 with FMA vs the reference's
+                                 double-accumulated stencils)
+  raw gradients         2e-4   (FP64 accumulation here, FP32 in the reference)
+"""
+import numpy as np
+import pytest
+
+from tests._cases import engine_config, make_case, rel_l2
+
+FWD_TOL = 2e-5
+GRAD_TOL = 2e-4
+
+FORWARD_CASES = [
+    dict(nd=2, freesurf=1, L=0, abs_type=1, src_type=100),
+    dict(nd=2, freesurf=0, L=1, abs_type=1, src_type=2),
+    dict(nd=2, freesurf=1, L=2, abs_type=1, src_type=100),
+    dict(nd=2, freesurf=0, L=0, abs_type=2, src_type=0),
+    dict(nd=2, freesurf=1, L=0, abs_type=1, src_type=100, fdorder=4),
+    dict(nd=2, freesurf=0, L=0, abs_type=1, src_type=100, fdorder=12, nz=50, nx=46),
+    dict(nd=3, freesurf=1, L=0, abs_type=1, src_type=100, nz=36, ny=34, nx=38, nt=120, nab=8),
+    dict(nd=3, freesurf=1, L=2, abs_type=1, src_type=2, nz=36, ny=34, nx=38, nt=120, nab=8),
+    dict(nd=3, freesurf=0, L=1, abs_type=2, src_type=1, nz=36, ny=34, nx=38, nt=120, nab=8),
+]
+
+
+def _outputs(nd):
+    return ["vx", "vy", "vz", "p"] if nd == 3 else ["vx", "vz", "p"]
+
+
+def _run_pair(kw, grad=False):
+    from oracle.oracle import Oracle
+    from seiscl_b200.engine import Plan
+
+    cfg, model, acq = make_case(**kw)
+    outs = _outputs(cfg["nd"])
+    ora = Oracle(cfg)
+    assert ora.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"]) == 0
+    d_ref = ora.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs, save_boundaries=grad)
+    plan = Plan(engine_config(cfg))
+    plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+    d_gpu = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs, save_boundaries=grad)
+    return cfg, model, acq, ora, plan, d_ref, d_gpu
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", FORWARD_CASES, ids=lambda k: "-".join("%s%s" % (a, b) for a, b in k.items()))
+def test_forward_matches_oracle(kw, cuda_device):
+    cfg, model, acq, ora, plan, d_ref, d_gpu = _run_pair(kw)
+    for name in d_ref:
+        ref = d_ref[name]
+        assert np.abs(ref).max() > 0, name
+        err = rel_l2(d_gpu[name], ref)
+        assert err < FWD_TOL, (name, err)
+
+
+GRAD_CASES = [
+    dict(nd=2, freesurf=1, L=0, abs_type=1, src_type=100),
+    dict(nd=2, freesurf=0, L=0, abs_type=1, src_type=2),
+    dict(nd=2, freesurf=0, L=0, abs_type=2, src_type=100),
+    dict(nd=3, freesurf=1, L=0, abs_type=1, src_type=100, nz=36, ny=34, nx=38, nt=100, nab=8),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", GRAD_CASES, ids=lambda k: "-".join("%s%s" % (a, b) for a, b in k.items()))
+def test_gradient_matches_oracle(kw, cuda_device):
+    cfg, model, acq, ora, plan, d_ref, d_gpu = _run_pair(kw, grad=True)
+    # residuals: a fixed fraction of the recorded data, as adjoint sources
+    res = {k: (0.3 * v).astype(np.float32) for k, v in d_ref.items() if k != "p"}
+    ora.clear_gradients()
+    ora.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], res)
+    g_ref = ora.gradients()
+    plan.zero_gradient()
+    plan.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], res)
+    g_raw = plan.gradient(transform=False)
+    for ours, theirs in (("M", "rawM"), ("mu", "rawmu"), ("rho", "rawrho")):
+        assert np.abs(g_ref[theirs]).max() > 0, theirs
+        err = rel_l2(g_raw[ours], g_ref[theirs])
+        assert err < GRAD_TOL, (ours, err)
+    g_t = plan.gradient(transform=True)
+    for name in ("vp", "vs", "rho"):
+        err = rel_l2(g_t[name], g_ref[name])
+        assert err < GRAD_TOL, (name, err)
+
+
+@pytest.mark.gpu
+def test_gradient_accumulates_over_shots(cuda_device):
+    from seiscl_b200.engine import Plan
+
+    cfg, model, acq = make_case(nd=2, nt=120)
+    plan = Plan(engine_config(cfg))
+    plan.set_model(model["vp"], model["vs"], model["rho"])
+    d = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], ["vx", "vz"], save_boundaries=True)
+    plan.zero_gradient()
+    plan.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], d)
+    g1 = plan.gradient(transform=False)
+    plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], ["vx", "vz"], save_boundaries=True)
+    plan.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], d)
+    g2 = plan.gradient(transform=False)
+    for k in g1:
+        assert rel_l2(g2[k], 2 * g1[k]) < 1e-6
+
+
+@pytest.mark.gpu
+def test_adjoint_requires_forward(cuda_device):
+    from seiscl_b200.engine import Plan, SeisCLEngineError
+
+    cfg, model, acq = make_case(nd=2, nt=20)
+    plan = Plan(engine_config(cfg))
+    plan.set_model(model["vp"], model["vs"], model["rho"])
+    with pytest.raises(SeisCLEngineError) as e:
+        plan.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], {"vx": np.zeros((len(acq["rec_pos"]), 20))})
+    assert e.value.code == -5
