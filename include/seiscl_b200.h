@@ -127,6 +127,38 @@ int sfd_get_gradient(sfd_plan *plan, int transform, float *g0, float *g1, float 
  * sources.  res[k] are [nrec][NT] host arrays for the selected outputs. */
 int sfd_residual_scale(sfd_plan *plan, const sfd_shot *shot, const int *outsel, float *const *res);
 
+/* ---- forward modelling without allocation ----
+ *
+ * This entry point has no counterpart in the reference; SeisCL always
+ * allocates its buffers per run.  It is for callers that cannot call
+ * cudaMalloc when they run a shot -- a serving process that reserved its
+ * device memory budget at start-up and must not grow it per request, or a
+ * host application whose own allocator owns the device.  It runs the same
+ * forward time loop as sfd_forward, but keeps its working memory (wave
+ * fields, memory variables, CPML memory, source/receiver maps) in one fixed
+ * array of SFD_NOALLOC_SCRATCH_BYTES compiled into the library, which every
+ * GPU that loads the library holds until the process exits.  It calls no
+ * cudaMalloc, cudaFree or other allocating routine.
+ *
+ * - The plan must hold a model (sfd_set_model, done beforehand) and its
+ *   device must be current.  The shot's working memory must fit in the
+ *   array; a larger grid is rejected with SFD_ERR_MEMORY and a message
+ *   naming the size it needed.
+ * - Inputs and outputs are caller-owned DEVICE buffers: src_pos [nsrc][5],
+ *   src [nsrc][NT], rec_pos [nrec][8], and seis [nsel][nrec][NT] for the
+ *   nsel selected outputs in SFD_OUT_* order.
+ * - The first call on a device looks up the array's device address
+ *   (cudaGetSymbolAddress) with that device current; make that first call
+ *   before any stream capture.
+ * - Every call on a device shares the one array.  Each call clears what must
+ *   start at zero, but calls that overlap on the GPU (different streams or
+ *   threads at once) race on it: issue them one after another.
+ * - The call returns after the shot has finished on `stream` (or the plan's
+ *   stream when NULL). */
+#define SFD_NOALLOC_SCRATCH_BYTES (16u << 20)
+int sfd_forward_noalloc(sfd_plan *plan, const float *src_pos, const float *src, int nsrc, const float *rec_pos,
+                        int nrec, int srctype_mask, const int *outsel, float *seis, void *stream);
+
 /* ---- host-only set-up (no device needed) ---- */
 
 /* The 14 transformed parameter arrays of sfd_set_model (M, mu, rho_b, taup,
