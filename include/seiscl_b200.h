@@ -73,7 +73,8 @@ typedef struct sfd_config {
     int param_type;    /* 0: vp,vs,rho  1: M,mu,rho  2: Ip,Is,rho */
     int restype;       /* 0: L2 (full gradient), 1: M only */
     int precision;     /* SFD_PREC_*: storage of the saved boundaries */
-    int reserved[7];
+    int kernels;       /* 0: fastest kernels available, 1: general kernels only */
+    int reserved[6];
 } sfd_config;
 
 typedef struct sfd_shot {

@@ -119,6 +119,11 @@ KERNELS = {
         ("surface3D.cl", "freesurface", 0, False), ("update_adjv3D.cl", "update_adjv", 1, True),
         ("update_adjs3D.cl", "update_adjs", 1, True), ("surface3D_adj.cl", "surface_adj", 0, False),
         ("savebnd3D.cl", "savebnd", 1, False)],
+    # SH: the reference's stress kernel does not compile for L>0 and its
+    # surface kernel cannot be loaded (named "surface"), so only v and s
+    21: [("update_v2D_SH.cl", "update_v", 1, False), ("update_s2D_SH.cl", "update_s", 1, False)],
+    # acoustic: forward only in the reference
+    22: [("update_v2D_acc.cl", "update_v", 1, False), ("update_s2D_acc.cl", "update_s", 1, False)],
 }
 
 
@@ -141,7 +146,7 @@ def build_ref(cfg: dict, nbnd: int, hc: list) -> str:
     if not ref_available():
         raise FileNotFoundError("reference kernel sources not found at %s" % REF_SRC)
     os.makedirs(REF_OUT, exist_ok=True)
-    nd = 3 if cfg["nd"] == 3 else 2
+    nd = cfg["nd"]
     defs = ref_defines(cfg, nbnd, hc)
     with tempfile.TemporaryDirectory() as td:
         objs = []

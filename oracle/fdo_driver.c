@@ -32,9 +32,13 @@ int fdo_source_targets(int nd, int mask, int type, int *fields, float *div)
     /* model variable list order, src/assign_modeling_case.c:1049-1076 */
     static const int vl2[] = {W_VX, W_VZ, W_SXX, W_SZZ, W_SXZ};
     static const int vl3[] = {W_VX, W_VY, W_VZ, W_SXX, W_SZZ, W_SXZ, W_SXY, W_SYZ, W_SYY};
-    static const int name_of_type[4] = {W_VX, W_VY, W_VZ, -1};
-    const int *vl = nd == 3 ? vl3 : vl2;
-    int nvl = nd == 3 ? 9 : 5;
+    static const int vl21[] = {W_VY, W_SXY, W_SYZ};
+    static const int vl22[] = {W_VX, W_VZ, W_SXX}; /* vx, vz, p */
+    /* the acoustic model has a variable named p; the others average p */
+    int name_of_type[4] = {W_VX, W_VY, W_VZ, nd == 22 ? W_SXX : -1};
+    const int *vl = nd == 3 ? vl3 : (nd == 21 ? vl21 : (nd == 22 ? vl22 : vl2));
+    int nvl = nd == 3 ? 9 : (nd == 21 || nd == 22 ? 3 : 5);
+    int has_p_average = nd == 2 || nd == 3;
     int tos[9] = {0};
     int tos_p = 0;
     for (int t = 0; t < 4; t++) {
@@ -42,9 +46,9 @@ int fdo_source_targets(int nd, int mask, int type, int *fields, float *div)
         if (name_of_type[t] >= 0)
             for (int j = 0; j < nvl; j++)
                 if (vl[j] == name_of_type[t]) tos[j] = 1;
-        if (t == 3) tos_p = 1;
+        if (t == 3 && has_p_average) tos_p = 1;
     }
-    if (mask & (1 << 4)) tos_p = 1;
+    if ((mask & (1 << 4)) && has_p_average) tos_p = 1;
     int ntypes = tos_p;
     for (int j = 0; j < nvl; j++) ntypes += tos[j];
     int n = 0;
@@ -109,6 +113,7 @@ static void record(fdo_state *s, const fdo_shot *sh, const int outsel[O_N], floa
             float v;
             if (o == O_P) {
                 if (s->c.nd == 3) v = (s->w[W_SXX][ix] + s->w[W_SZZ][ix] + s->w[W_SYY][ix]) / 3.0;
+                else if (s->c.nd == 22) v = s->w[W_SXX][ix];
                 else v = (s->w[W_SXX][ix] + s->w[W_SZZ][ix]) / 2.0;
             } else v = s->w[out_field[o]][ix];
             seis[o][(i64)NT * g + t] = v;

@@ -1277,9 +1277,244 @@ static void port_surface_adj3d(fdo_state *s)
 #undef INDP3
 }
 
-static void port_update_v(fdo_state *s) { if (s->c.nd == 3) port_update_v3d(s); else port_update_v2d(s); }
-static void port_update_s(fdo_state *s) { if (s->c.nd == 3) port_update_s3d(s); else port_update_s2d(s); }
-static void port_surface(fdo_state *s, int pdir) { if (s->c.nd == 3) port_surface3d(s, pdir); else port_surface2d(s, pdir); }
+
+/* ======================================================================
+ * 2D acoustic (ND=22): src/update_v2D_acc.cl:80-324, update_s2D_acc.cl:79-402.
+ * The pressure lives in the W_SXX slot, its memory variable in R_XX, and
+ * psi_p_x / psi_p_z in the PS_SXX_X / PS_SZZ_Z slots.
+ * ====================================================================== */
+static void port_update_v_acc(fdo_state *s)
+{
+    const fdo_cfg *c = &s->c;
+    int F = c->fdoh, NZ = s->NZp, NX = s->NXp, nz = c->nz, NAB = c->nab;
+    const double *hc = s->hc;
+    float *vx = s->w[W_VX], *vz = s->w[W_VZ];
+    const float *p = s->w[W_SXX], *rip = s->p[P_RIP], *rkp = s->p[P_RKP];
+    float **ps = s->psi;
+#pragma omp parallel for schedule(static)
+    for (int gx = F; gx < NX - F; gx++)
+        for (int gz = F; gz < NZ - F; gz++) {
+            i64 ip = (i64)(gx - F) * nz + (gz - F), iv = (i64)gx * NZ + gz;
+            float p_x = dfw(p, iv, NZ, hc, F);
+            float p_z = dfw(p, iv, 1, hc, F);
+            if (c->abs_type == 1) {
+                if (gz > NZ - NAB - F - 1) {
+                    int i = gx - F, k = gz - NZ + NAB + F + NAB, ind = 2 * NAB - 1 - k;
+                    CPML(ps[PS_SZZ_Z], (i64)i * (2 * NAB) + k, s->cz[C_KH], s->cz[C_AH], s->cz[C_BH], ind, p_z);
+                } else if (!c->freesurf && gz - F < NAB) {
+                    int i = gx - F, k = gz - F;
+                    CPML(ps[PS_SZZ_Z], (i64)i * (2 * NAB) + k, s->cz[C_KH], s->cz[C_AH], s->cz[C_BH], k, p_z);
+                }
+                if (gx - F < NAB) {
+                    int i = gx - F, k = gz - F;
+                    CPML(ps[PS_SXX_X], (i64)i * nz + k, s->cx[C_KH], s->cx[C_AH], s->cx[C_BH], i, p_x);
+                }
+                if (gx > NX - NAB - F - 1) {
+                    int i = gx - NX + NAB + F + NAB, k = gz - F, ind = 2 * NAB - 1 - i;
+                    CPML(ps[PS_SXX_X], (i64)i * nz + k, s->cx[C_KH], s->cx[C_AH], s->cx[C_BH], ind, p_x);
+                }
+            }
+            vx[iv] += (p_x * rip[ip]);
+            vz[iv] += (p_z * rkp[ip]);
+            if (c->abs_type == 2) {
+                /* the acoustic kernels taper the top even with a free surface */
+                float *f[2] = {vx, vz};
+                if (gz - F < NAB) for (int q = 0; q < 2; q++) f[q][iv] *= s->taper[gz - F];
+                if (gz > NZ - NAB - F - 1) for (int q = 0; q < 2; q++) f[q][iv] *= s->taper[NZ - F - gz - 1];
+                if (gx - F < NAB) for (int q = 0; q < 2; q++) f[q][iv] *= s->taper[gx - F];
+                if (gx > NX - NAB - F - 1) for (int q = 0; q < 2; q++) f[q][iv] *= s->taper[NX - F - gx - 1];
+            }
+        }
+}
+
+static void port_update_s_acc(fdo_state *s)
+{
+    const fdo_cfg *c = &s->c;
+    int F = c->fdoh, NZ = s->NZp, NX = s->NXp, nz = c->nz, NAB = c->nab, L = c->L;
+    const double *hc = s->hc;
+    const double DT2 = s->DT2;
+    const float *vx = s->w[W_VX], *vz = s->w[W_VZ];
+    float *p = s->w[W_SXX], *rp = s->r[R_XX];
+    const float *M = s->p[P_M], *taup = s->p[P_TAUP];
+    float **ps = s->psi;
+    const i64 NXNZ = (i64)NX * NZ;
+#pragma omp parallel for schedule(static)
+    for (int gx = F; gx < NX - F; gx++)
+        for (int gz = F; gz < NZ - F; gz++) {
+            i64 ip = (i64)(gx - F) * nz + (gz - F), iv = (i64)gx * NZ + gz;
+            float vxx = dbw(vx, iv, NZ, hc, F);
+            float vzz = dbw(vz, iv, 1, hc, F);
+            if (c->abs_type == 1) {
+                if (gz > NZ - NAB - F - 1) {
+                    int i = gx - F, k = gz - NZ + NAB + F + NAB, ind = 2 * NAB - 1 - k;
+                    CPML(ps[PS_VZ_Z], (i64)i * (2 * NAB) + k, s->cz[C_K], s->cz[C_A], s->cz[C_B], ind + 1, vzz);
+                } else if (!c->freesurf && gz - F < NAB) {
+                    int i = gx - F, k = gz - F;
+                    CPML(ps[PS_VZ_Z], (i64)i * (2 * NAB) + k, s->cz[C_K], s->cz[C_A], s->cz[C_B], k, vzz);
+                }
+                if (gx - F < NAB) {
+                    int i = gx - F, k = gz - F;
+                    CPML(ps[PS_VX_X], (i64)i * nz + k, s->cx[C_K], s->cx[C_A], s->cx[C_B], i, vxx);
+                }
+                if (gx > NX - NAB - F - 1) {
+                    int i = gx - NX + NAB + F + NAB, k = gz - F, ind = 2 * NAB - 1 - i;
+                    CPML(ps[PS_VX_X], (i64)i * nz + k, s->cx[C_K], s->cx[C_A], s->cx[C_B], ind + 1, vxx);
+                }
+            }
+            if (L == 0) {
+                float g = M[ip];
+                p[iv] += (g * (vxx + vzz));
+            } else {
+                float lM = M[ip], ltaup = taup[ip];
+                float g = lM * (1.0 + (float)L * ltaup);
+                /* no 1/DT here, unlike the elastic kernels (update_s2D_acc.cl:333) */
+                float e = lM * ltaup;
+                float sumrp = 0;
+                for (int l = 0; l < L; l++) sumrp += rp[l * NXNZ + iv];
+                float lp = (g * (vxx + vzz)) + (DT2 * sumrp);
+                sumrp = 0;
+                for (int l = 0; l < L; l++) {
+                    float el = s->eta[l];
+                    float b = 1.0 / (1.0 + (el * 0.5));
+                    float cc = 1.0 - (el * 0.5);
+                    i64 ir = l * NXNZ + iv;
+                    rp[ir] = b * (rp[ir] * cc - el * e * (vxx + vzz));
+                    sumrp += rp[ir];
+                }
+                p[iv] += lp + (DT2 * sumrp);
+            }
+            if (c->abs_type == 2) {
+                if (gz - F < NAB) p[iv] *= s->taper[gz - F];
+                if (gz > NZ - NAB - F - 1) p[iv] *= s->taper[NZ - F - gz - 1];
+                if (gx - F < NAB) p[iv] *= s->taper[gx - F];
+                if (gx > NX - NAB - F - 1) p[iv] *= s->taper[NX - F - gx - 1];
+            }
+        }
+}
+
+/* ======================================================================
+ * 2D SH (ND=21): src/update_v2D_SH.cl:106-356, update_s2D_SH.cl:109-421.
+ * Buoyancy and shear modulus are used at the cell, unaveraged, as the
+ * reference does; at FDOH=1 the stress kernel's differences carry no
+ * coefficient (update_s2D_SH.cl:204-205); stresses are not tapered (the
+ * reference tests the lower-case macro abstype).  The reference binds the
+ * stress kernel's CPML arrays under names no buffer has (psi_vyx, psi_vyz);
+ * here they are psi_vy_x / psi_vy_z.
+ * ====================================================================== */
+static void port_update_v_sh(fdo_state *s)
+{
+    const fdo_cfg *c = &s->c;
+    int F = c->fdoh, NZ = s->NZp, NX = s->NXp, nz = c->nz, NAB = c->nab;
+    const double *hc = s->hc;
+    float *vy = s->w[W_VY];
+    const float *sxy = s->w[W_SXY], *syz = s->w[W_SYZ], *rho = s->p[P_RHO];
+    float **ps = s->psi;
+#pragma omp parallel for schedule(static)
+    for (int gx = F; gx < NX - F; gx++)
+        for (int gz = F; gz < NZ - F; gz++) {
+            i64 ip = (i64)(gx - F) * nz + (gz - F), iv = (i64)gx * NZ + gz;
+            float sxy_x = dbw(sxy, iv, NZ, hc, F);
+            float syz_z = dbw(syz, iv, 1, hc, F);
+            if (c->abs_type == 1) {
+                if (gz > NZ - NAB - F - 1) {
+                    int i = gx - F, k = gz - NZ + NAB + F + NAB, ind = 2 * NAB - 1 - k;
+                    CPML(ps[PS_SYZ_Z], (i64)i * (2 * NAB) + k, s->cz[C_K], s->cz[C_A], s->cz[C_B], ind + 1, syz_z);
+                } else if (!c->freesurf && gz - F < NAB) {
+                    int i = gx - F, k = gz - F;
+                    CPML(ps[PS_SYZ_Z], (i64)i * (2 * NAB) + k, s->cz[C_K], s->cz[C_A], s->cz[C_B], k, syz_z);
+                }
+                if (gx - F < NAB) {
+                    int i = gx - F, k = gz - F;
+                    CPML(ps[PS_SXY_X], (i64)i * nz + k, s->cx[C_K], s->cx[C_A], s->cx[C_B], i, sxy_x);
+                }
+                if (gx > NX - NAB - F - 1) {
+                    /* full-node coefficients at ind, not ind+1 (update_v2D_SH.cl:309-310) */
+                    int i = gx - NX + NAB + F + NAB, k = gz - F, ind = 2 * NAB - 1 - i;
+                    CPML(ps[PS_SXY_X], (i64)i * nz + k, s->cx[C_K], s->cx[C_A], s->cx[C_B], ind, sxy_x);
+                }
+            }
+            vy[iv] += ((sxy_x + syz_z) * rho[ip]);
+            if (c->abs_type == 2) {
+                if (!c->freesurf && gz - F < NAB) vy[iv] *= s->taper[gz - F];
+                if (gz > NZ - NAB - F - 1) vy[iv] *= s->taper[NZ - F - gz - 1];
+                if (gx - F < NAB) vy[iv] *= s->taper[gx - F];
+                if (gx > NX - NAB - F - 1) vy[iv] *= s->taper[NX - F - gx - 1];
+            }
+        }
+}
+
+static void port_update_s_sh(fdo_state *s)
+{
+    const fdo_cfg *c = &s->c;
+    int F = c->fdoh, NZ = s->NZp, NX = s->NXp, nz = c->nz, NAB = c->nab;
+    const double *hc = s->hc;
+    const float *vy = s->w[W_VY];
+    float *sxy = s->w[W_SXY], *syz = s->w[W_SYZ];
+    const float *mu = s->p[P_MU];
+    float **ps = s->psi;
+    double one[7] = {0, 1, 0, 0, 0, 0, 0};
+    const double *h = F == 1 ? one : hc;
+#pragma omp parallel for schedule(static)
+    for (int gx = F; gx < NX - F; gx++)
+        for (int gz = F; gz < NZ - F; gz++) {
+            i64 ip = (i64)(gx - F) * nz + (gz - F), iv = (i64)gx * NZ + gz;
+            float vyx = dfw(vy, iv, NZ, h, F);
+            float vyz = dfw(vy, iv, 1, h, F);
+            if (c->abs_type == 1) {
+                if (gz > NZ - NAB - F - 1) {
+                    int i = gx - F, k = gz - NZ + NAB + F + NAB, ind = 2 * NAB - 1 - k;
+                    CPML(ps[PS_VY_Z], (i64)i * (2 * NAB) + k, s->cz[C_KH], s->cz[C_AH], s->cz[C_BH], ind, vyz);
+                } else if (!c->freesurf && gz - F < NAB) {
+                    int i = gx - F, k = gz - F;
+                    CPML(ps[PS_VY_Z], (i64)i * (2 * NAB) + k, s->cz[C_KH], s->cz[C_AH], s->cz[C_BH], k, vyz);
+                }
+                if (gx - F < NAB) {
+                    int i = gx - F, k = gz - F;
+                    CPML(ps[PS_VY_X], (i64)i * nz + k, s->cx[C_KH], s->cx[C_AH], s->cx[C_BH], i, vyx);
+                }
+                if (gx > NX - NAB - F - 1) {
+                    int i = gx - NX + NAB + F + NAB, k = gz - F, ind = 2 * NAB - 1 - i;
+                    CPML(ps[PS_VY_X], (i64)i * nz + k, s->cx[C_KH], s->cx[C_AH], s->cx[C_BH], ind, vyx);
+                }
+            }
+            float f = mu[ip];
+            sxy[iv] += (f * vyx);
+            syz[iv] += (f * vyz);
+        }
+}
+
+/* free surface for SH: image syz above the surface.  The reference's SH
+ * kernel is named "surface" while the loader asks for "freesurface"
+ * (src/surface2D_SH.cl:23, assign_modeling_case.c:989); this is its body. */
+static void port_surface_sh(fdo_state *s, int pdir)
+{
+    (void)pdir;
+    int F = s->c.fdoh, NZ = s->NZp, NX = s->NXp;
+    float *syz = s->w[W_SYZ];
+    for (int gx = F; gx <= NX - F - 1; gx++)
+        for (int m = 1; m <= F; m++) syz[(i64)gx * NZ + F - m] = -syz[(i64)gx * NZ + F + m - 1];
+}
+
+static void port_update_v(fdo_state *s)
+{
+    if (s->c.nd == 3) port_update_v3d(s);
+    else if (s->c.nd == 22) port_update_v_acc(s);
+    else if (s->c.nd == 21) port_update_v_sh(s);
+    else port_update_v2d(s);
+}
+static void port_update_s(fdo_state *s)
+{
+    if (s->c.nd == 3) port_update_s3d(s);
+    else if (s->c.nd == 22) port_update_s_acc(s);
+    else if (s->c.nd == 21) port_update_s_sh(s);
+    else port_update_s2d(s);
+}
+static void port_surface(fdo_state *s, int pdir)
+{
+    if (s->c.nd == 3) port_surface3d(s, pdir);
+    else if (s->c.nd == 21) port_surface_sh(s, pdir);
+    else if (s->c.nd == 2) port_surface2d(s, pdir);
+}
 static void port_update_adjv(fdo_state *s) { if (s->c.nd == 3) port_update_adjv3d(s); else port_update_adjv2d(s); }
 static void port_update_adjs(fdo_state *s) { if (s->c.nd == 3) port_update_adjs3d(s); else port_update_adjs2d(s); }
 static void port_surface_adj(fdo_state *s) { if (s->c.nd == 3) port_surface_adj3d(s); else port_surface_adj2d(s); }

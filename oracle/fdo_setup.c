@@ -175,9 +175,17 @@ int fdo_state_init(fdo_state *s, const fdo_cfg *c)
     int ids2[] = {W_VX, W_VZ, W_SXX, W_SZZ, W_SXZ};
     int rid3[] = {R_XX, R_YY, R_ZZ, R_XY, R_YZ, R_XZ};
     int rid2[] = {R_XX, R_ZZ, R_XZ};
+    int ids22[] = {W_VX, W_VZ, W_SXX}, rid22[] = {R_XX};     /* acoustic: p, rp */
+    int ids21[] = {W_VY, W_SXY, W_SYZ}, rid21[] = {R_XY, R_YZ}; /* SH */
     if (c->nd == 3) {
         s->nwave = 9; memcpy(s->wave_ids, ids3, sizeof ids3);
         s->nmem = 6; memcpy(s->mem_ids, rid3, sizeof rid3);
+    } else if (c->nd == 22) {
+        s->nwave = 3; memcpy(s->wave_ids, ids22, sizeof ids22);
+        s->nmem = 1; memcpy(s->mem_ids, rid22, sizeof rid22);
+    } else if (c->nd == 21) {
+        s->nwave = 3; memcpy(s->wave_ids, ids21, sizeof ids21);
+        s->nmem = 2; memcpy(s->mem_ids, rid21, sizeof rid21);
     } else {
         s->nwave = 5; memcpy(s->wave_ids, ids2, sizeof ids2);
         s->nmem = 3; memcpy(s->mem_ids, rid2, sizeof rid2);

@@ -44,12 +44,16 @@ void *dalloc(sfd_plan *p, size_t bytes, cudaError_t *err)
 bool is_wave_used(const Grid &g, int w)
 {
     if (g.nd == 3) return true;
+    if (g.nd == 21) return w == VY || w == SXY || w == SYZ;
+    if (g.nd == 22) return w == VX || w == VZ || w == SXX;  // SXX holds the acoustic pressure
     return w == VX || w == VZ || w == SXX || w == SZZ || w == SXZ;
 }
 bool is_mem_used(const Grid &g, int r)
 {
     if (g.L == 0) return false;
     if (g.nd == 3) return true;
+    if (g.nd == 21) return r == RXY || r == RYZ;
+    if (g.nd == 22) return r == RXX;
     return r == RXX || r == RZZ || r == RXZ;
 }
 
@@ -70,8 +74,12 @@ int check_outsel(sfd_plan *p, const int *outsel)
 {
     for (int o = 0; o < SFD_NOUT; o++) {
         if (!outsel || !outsel[o]) continue;
-        if (o == SFD_OUT_P) continue;
-        if (!is_wave_used(p->g, o)) return fail(p, SFD_ERR_ARG, "requested output variable does not exist in 2D P-SV");
+        if (o == SFD_OUT_P) {
+            if (p->g.nd == 21) return fail(p, SFD_ERR_ARG, "Cannot output pressure for SH modeling");
+            continue;
+        }
+        if (p->g.nd == 22 && o == SFD_OUT_SXX) return fail(p, SFD_ERR_ARG, "acoustic modeling records p, not sxx");
+        if (!is_wave_used(p->g, o)) return fail(p, SFD_ERR_ARG, "requested output variable does not exist in this physics");
     }
     return SFD_OK;
 }
@@ -172,8 +180,12 @@ int alloc_model(sfd_plan *p)
     int64_t sizes[NPSI] = {sx, sx, sx, sy, sy, sy, sz, sz, sz, sx, sx, sx, sy, sy, sy, sz, sz, sz};
     int64_t tot = 0;
     for (int i = 0; i < NPSI; i++) {
-        bool used = g.abs_type == 1 && g.nab > 0 && (g.nd == 3 || (i != PVY_X && i != PVX_Y && i != PVY_Y &&
-                    i != PVZ_Y && i != PVY_Z && i != PSXY_X && i != PSXY_Y && i != PSYY_Y && i != PSYZ_Y && i != PSYZ_Z));
+        bool used2 = i == PVX_X || i == PVZ_X || i == PVX_Z || i == PVZ_Z || i == PSXX_X || i == PSXZ_X ||
+                     i == PSXZ_Z || i == PSZZ_Z;
+        bool used21 = i == PSXY_X || i == PSYZ_Z || i == PVY_X || i == PVY_Z;
+        bool used22 = i == PVX_X || i == PVZ_Z || i == PSXX_X || i == PSZZ_Z;  // + psi_p_x / psi_p_z
+        bool used = g.abs_type == 1 && g.nab > 0 &&
+                    (g.nd == 3 || (g.nd == 2 && used2) || (g.nd == 21 && used21) || (g.nd == 22 && used22));
         p->psi_size[i] = used ? sizes[i] : 0;
         tot += p->psi_size[i];
     }
@@ -270,7 +282,11 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     if (!cfg || !out) return SFD_ERR_ARG;
     *out = nullptr;
     const sfd_config &c = *cfg;
-    if (c.nd != 2 && c.nd != 3) return SFD_ERR_UNSUPPORTED;
+    if (c.nd != 2 && c.nd != 3 && c.nd != 21 && c.nd != 22) return SFD_ERR_UNSUPPORTED;
+    // the reference has no acoustic free surface (assign_modeling_case.c:957-970) and its
+    // viscoelastic SH stress kernel does not compile (update_s2D_SH.cl:290)
+    if (c.nd == 22 && c.freesurf) return SFD_ERR_UNSUPPORTED;
+    if (c.nd == 21 && c.L > 0) return SFD_ERR_UNSUPPORTED;
     if (c.fdorder < 2 || c.fdorder > 12 || c.fdorder % 2) return SFD_ERR_ARG;
     if (c.maxrelerror < 0 || c.maxrelerror > 4) return SFD_ERR_ARG;
     if (c.L < 0 || c.L > 8 || c.nt <= 0 || !(c.dt > 0) || !(c.dh > 0) || c.nab < 0) return SFD_ERR_ARG;
@@ -280,6 +296,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     // N[0] must be even (read_hdf5.c:535-540)
     if (c.n[0] % 2) return SFD_ERR_ARG;
     if (c.precision < 0 || c.precision > 2) return SFD_ERR_ARG;
+    if (c.kernels < 0 || c.kernels > 1) return SFD_ERR_ARG;
 
     sfd_plan *p = new sfd_plan();
     p->cfg = c;
@@ -298,6 +315,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     g.L = c.L;
     g.freesurf = c.freesurf ? 1 : 0;
     g.restype = c.restype;
+    g.kernels = c.kernels == 1 ? 1 : 0;
     g.nvol = (int64_t)g.NZ * g.NY * g.NX;
     double hc[6];
     holberg(c.fdorder, c.maxrelerror, hc);
@@ -391,6 +409,8 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
     BndSlot bs;
     memset(&bs, 0, sizeof bs);
     if (save_boundaries) {
+        if (g.nd == 21 || g.nd == 22)
+            return fail(p, SFD_ERR_UNSUPPORTED, "the adjoint path covers P-SV and 3D elastic/viscoelastic media");
         if (g.nab <= 0 || g.nbnd <= 0) return fail(p, SFD_ERR_ARG, "boundary saving needs an absorbing layer");
         for (int w = 0; w < NW; w++) {
             if (!p->f.w[w]) continue;
@@ -436,6 +456,8 @@ extern "C" int sfd_adjoint(sfd_plan *p, const sfd_shot *shot, int mask, const in
                            const float *const *residuals, void *stream)
 {
     if (!p || !shot) return SFD_ERR_ARG;
+    if (p->g.nd == 21 || p->g.nd == 22)
+        return fail(p, SFD_ERR_UNSUPPORTED, "the adjoint path covers P-SV and 3D elastic/viscoelastic media");
     if (!p->have_forward) return fail(p, SFD_ERR_STATE, "sfd_adjoint needs a preceding sfd_forward with saved boundaries");
     int rc;
     if ((rc = check_outsel(p, outsel))) return rc;
@@ -629,7 +651,9 @@ extern "C" int sfd_bench_kernels(sfd_plan *p, int nrep, float *out_ms)
 namespace {
 int host_grid(const sfd_config *c, Grid &g)
 {
-    if (!c || (c->nd != 2 && c->nd != 3) || c->fdorder < 2 || c->fdorder > 12 || c->fdorder % 2) return SFD_ERR_ARG;
+    if (!c || (c->nd != 2 && c->nd != 3 && c->nd != 21 && c->nd != 22) || c->fdorder < 2 || c->fdorder > 12 ||
+        c->fdorder % 2)
+        return SFD_ERR_ARG;
     memset(&g, 0, sizeof g);
     g.nd = c->nd;
     g.F = c->fdorder / 2;

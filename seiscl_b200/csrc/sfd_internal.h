@@ -44,6 +44,7 @@ struct Grid {
     float eta[8];           // 2 pi FL dt
     int nbnd;               // saved-boundary cells per field per step
     int restype;
+    int kernels;            // 0: register-blocked 3D kernels where available, 1: general only
 };
 
 struct Fields {

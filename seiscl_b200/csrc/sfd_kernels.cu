@@ -674,6 +674,198 @@ __global__ void k_surf3d(Grid g, Fields f, int pdir)
     }
 }
 
+
+// ============================================================ 2D acoustic
+// src/update_v2D_acc.cl:80-324, src/update_s2D_acc.cl:79-402; the pressure
+// lives in the SXX slot, its memory variable in RXX, psi_p_x / psi_p_z in the
+// PSXX_X / PSZZ_Z slots.
+template <int F>
+__global__ void __launch_bounds__(256) k_v2d_acc(Grid g, Fields f)
+{
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
+    i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
+    int NAB = g.nab, NZ = g.NZ, NX = g.NX;
+    float p_x = dfw<F>(f.w[SXX], iv, NZ, g.hc);
+    float p_z = dfw<F>(f.w[SXX], iv, 1, g.hc);
+    if (g.abs_type == 1) {
+        if (gz > NZ - NAB - F - 1) {
+            int i = gx - F, k = gz - NZ + NAB + F + NAB, ind = 2 * NAB - 1 - k;
+            cpml(f.psi[PSZZ_Z], (i64)i * (2 * NAB) + k, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, p_z);
+        } else if (!g.freesurf && gz - F < NAB) {
+            int i = gx - F, k = gz - F;
+            cpml(f.psi[PSZZ_Z], (i64)i * (2 * NAB) + k, f.cz[CKH], f.cz[CAH], f.cz[CBH], k, p_z);
+        }
+        if (gx - F < NAB) {
+            int i = gx - F, k = gz - F;
+            cpml(f.psi[PSXX_X], (i64)i * g.nz + k, f.cx[CKH], f.cx[CAH], f.cx[CBH], i, p_x);
+        }
+        if (gx > NX - NAB - F - 1) {
+            int i = gx - NX + NAB + F + NAB, k = gz - F, ind = 2 * NAB - 1 - i;
+            cpml(f.psi[PSXX_X], (i64)i * g.nz + k, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, p_x);
+        }
+    }
+    float vx = f.w[VX][iv] + p_x * __ldg(f.p[PRIP] + ip);
+    float vz = f.w[VZ][iv] + p_z * __ldg(f.p[PRKP] + ip);
+    if (g.abs_type == 2) {
+        // the acoustic kernels taper the top even with a free surface
+        const float *tp = f.taper;
+        if (gz - F < NAB) { vx *= tp[gz - F]; vz *= tp[gz - F]; }
+        if (gz > NZ - NAB - F - 1) { vx *= tp[NZ - F - gz - 1]; vz *= tp[NZ - F - gz - 1]; }
+        if (gx - F < NAB) { vx *= tp[gx - F]; vz *= tp[gx - F]; }
+        if (gx > NX - NAB - F - 1) { vx *= tp[NX - F - gx - 1]; vz *= tp[NX - F - gx - 1]; }
+    }
+    f.w[VX][iv] = vx;
+    f.w[VZ][iv] = vz;
+}
+
+template <int F>
+__global__ void __launch_bounds__(256) k_s2d_acc(Grid g, Fields f)
+{
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
+    i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
+    int NAB = g.nab, NZ = g.NZ, NX = g.NX, L = g.L;
+    float vxx = dbw<F>(f.w[VX], iv, NZ, g.hc);
+    float vzz = dbw<F>(f.w[VZ], iv, 1, g.hc);
+    if (g.abs_type == 1) {
+        if (gz > NZ - NAB - F - 1) {
+            int i = gx - F, k = gz - NZ + NAB + F + NAB, ind = 2 * NAB - 1 - k;
+            cpml(f.psi[PVZ_Z], (i64)i * (2 * NAB) + k, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, vzz);
+        } else if (!g.freesurf && gz - F < NAB) {
+            int i = gx - F, k = gz - F;
+            cpml(f.psi[PVZ_Z], (i64)i * (2 * NAB) + k, f.cz[CK], f.cz[CA], f.cz[CB], k, vzz);
+        }
+        if (gx - F < NAB) {
+            int i = gx - F, k = gz - F;
+            cpml(f.psi[PVX_X], (i64)i * g.nz + k, f.cx[CK], f.cx[CA], f.cx[CB], i, vxx);
+        }
+        if (gx > NX - NAB - F - 1) {
+            int i = gx - NX + NAB + F + NAB, k = gz - F, ind = 2 * NAB - 1 - i;
+            cpml(f.psi[PVX_X], (i64)i * g.nz + k, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, vxx);
+        }
+    }
+    float p = f.w[SXX][iv];
+    if (L == 0) {
+        p += __ldg(f.p[PM] + ip) * (vxx + vzz);
+    } else {
+        float lM = __ldg(f.p[PM] + ip), ltaup = __ldg(f.p[PTAUP] + ip);
+        float gm = lM * (1.0f + (float)L * ltaup);
+        float e = lM * ltaup;  // no 1/dt, as update_s2D_acc.cl:333
+        float sumrp = 0;
+        for (int l = 0; l < L; l++) sumrp += f.r[RXX][l * g.nvol + iv];
+        float lp = gm * (vxx + vzz) + g.dt2 * sumrp;
+        sumrp = 0;
+        for (int l = 0; l < L; l++) {
+            float el = g.eta[l];
+            float b = 1.0f / (1.0f + el * 0.5f), c = 1.0f - el * 0.5f;
+            i64 ir = l * g.nvol + iv;
+            float r = b * (f.r[RXX][ir] * c - el * e * (vxx + vzz));
+            f.r[RXX][ir] = r;
+            sumrp += r;
+        }
+        p += lp + g.dt2 * sumrp;
+    }
+    if (g.abs_type == 2) {
+        const float *tp = f.taper;
+        if (gz - F < NAB) p *= tp[gz - F];
+        if (gz > NZ - NAB - F - 1) p *= tp[NZ - F - gz - 1];
+        if (gx - F < NAB) p *= tp[gx - F];
+        if (gx > NX - NAB - F - 1) p *= tp[NX - F - gx - 1];
+    }
+    f.w[SXX][iv] = p;
+}
+
+// ================================================================== 2D SH
+// src/update_v2D_SH.cl:106-356, src/update_s2D_SH.cl:109-421 (elastic).
+// Buoyancy and shear modulus at the cell, unaveraged; the far-x CPML of the
+// velocity uses the full-node coefficients at ind; at FDOH=1 the stress
+// differences carry no coefficient; stresses are not tapered.
+template <int F>
+__global__ void __launch_bounds__(256) k_v2d_sh(Grid g, Fields f)
+{
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
+    i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
+    int NAB = g.nab, NZ = g.NZ, NX = g.NX;
+    float sxy_x = dbw<F>(f.w[SXY], iv, NZ, g.hc);
+    float syz_z = dbw<F>(f.w[SYZ], iv, 1, g.hc);
+    if (g.abs_type == 1) {
+        if (gz > NZ - NAB - F - 1) {
+            int i = gx - F, k = gz - NZ + NAB + F + NAB, ind = 2 * NAB - 1 - k;
+            cpml(f.psi[PSYZ_Z], (i64)i * (2 * NAB) + k, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, syz_z);
+        } else if (!g.freesurf && gz - F < NAB) {
+            int i = gx - F, k = gz - F;
+            cpml(f.psi[PSYZ_Z], (i64)i * (2 * NAB) + k, f.cz[CK], f.cz[CA], f.cz[CB], k, syz_z);
+        }
+        if (gx - F < NAB) {
+            int i = gx - F, k = gz - F;
+            cpml(f.psi[PSXY_X], (i64)i * g.nz + k, f.cx[CK], f.cx[CA], f.cx[CB], i, sxy_x);
+        }
+        if (gx > NX - NAB - F - 1) {
+            int i = gx - NX + NAB + F + NAB, k = gz - F, ind = 2 * NAB - 1 - i;
+            cpml(f.psi[PSXY_X], (i64)i * g.nz + k, f.cx[CK], f.cx[CA], f.cx[CB], ind, sxy_x);
+        }
+    }
+    float vy = f.w[VY][iv] + (sxy_x + syz_z) * __ldg(f.p[PRHO] + ip);
+    if (g.abs_type == 2) {
+        const float *tp = f.taper;
+        if (!g.freesurf && gz - F < NAB) vy *= tp[gz - F];
+        if (gz > NZ - NAB - F - 1) vy *= tp[NZ - F - gz - 1];
+        if (gx - F < NAB) vy *= tp[gx - F];
+        if (gx > NX - NAB - F - 1) vy *= tp[NX - F - gx - 1];
+    }
+    f.w[VY][iv] = vy;
+}
+
+template <int F>
+__global__ void __launch_bounds__(256) k_s2d_sh(Grid g, Fields f)
+{
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
+    i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
+    int NAB = g.nab, NZ = g.NZ, NX = g.NX;
+    float hone[6] = {1.0f, 0, 0, 0, 0, 0};
+    const float *h = F == 1 ? hone : g.hc;
+    float vyx = dfw<F>(f.w[VY], iv, NZ, h);
+    float vyz = dfw<F>(f.w[VY], iv, 1, h);
+    if (g.abs_type == 1) {
+        if (gz > NZ - NAB - F - 1) {
+            int i = gx - F, k = gz - NZ + NAB + F + NAB, ind = 2 * NAB - 1 - k;
+            cpml(f.psi[PVY_Z], (i64)i * (2 * NAB) + k, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, vyz);
+        } else if (!g.freesurf && gz - F < NAB) {
+            int i = gx - F, k = gz - F;
+            cpml(f.psi[PVY_Z], (i64)i * (2 * NAB) + k, f.cz[CKH], f.cz[CAH], f.cz[CBH], k, vyz);
+        }
+        if (gx - F < NAB) {
+            int i = gx - F, k = gz - F;
+            cpml(f.psi[PVY_X], (i64)i * g.nz + k, f.cx[CKH], f.cx[CAH], f.cx[CBH], i, vyx);
+        }
+        if (gx > NX - NAB - F - 1) {
+            int i = gx - NX + NAB + F + NAB, k = gz - F, ind = 2 * NAB - 1 - i;
+            cpml(f.psi[PVY_X], (i64)i * g.nz + k, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, vyx);
+        }
+    }
+    float mu = __ldg(f.p[PMU] + ip);
+    f.w[SXY][iv] += mu * vyx;
+    f.w[SYZ][iv] += mu * vyz;
+}
+
+// SH free surface: image syz above the surface (src/surface2D_SH.cl:37-39)
+template <int F>
+__global__ void k_surf_sh(Grid g, Fields f)
+{
+    int gx = blockIdx.x * blockDim.x + threadIdx.x + F;
+    if (gx > g.NX - F - 1) return;
+    i64 iv = (i64)gx * g.NZ + F;
+#pragma unroll
+    for (int m = 1; m <= F; m++) f.w[SYZ][iv - m] = -f.w[SYZ][iv + m - 1];
+}
+
 // ---------------------------------------------------- boundary save (forward)
 template <typename T>
 __global__ void k_savebnd(Grid g, Fields f, BndSlot b, i64 tofs)
@@ -1130,6 +1322,7 @@ __global__ void k_record(Fields f, PointSet r, float *out, int nt_total, int t, 
         float v;
         if (o == SFD_OUT_P) {
             if (nd == 3) v = (f.w[SXX][cell] + f.w[SZZ][cell] + f.w[SYY][cell]) / 3.0f;
+            else if (nd == 22) v = f.w[SXX][cell];
             else v = (f.w[SXX][cell] + f.w[SZZ][cell]) / 2.0f;
         } else {
             v = f.w[o][cell];
@@ -1178,6 +1371,13 @@ static inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b)
 
 void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
 {
+    if (g.kernels == 0 && launch_update_v_fast(g, f, st)) return;
+    if (g.nd == 21 || g.nd == 22) {
+        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
+        if (g.nd == 21) DISPATCH_F(g.F, k_v2d_sh<FF><<<gr, b, 0, st>>>(g, f))
+        else DISPATCH_F(g.F, k_v2d_acc<FF><<<gr, b, 0, st>>>(g, f))
+        return;
+    }
     if (g.nd == 3) {
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
         DISPATCH_F(g.F, k_v3d<FF><<<gr, b, 0, st>>>(g, f));
@@ -1189,6 +1389,13 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
 
 void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
 {
+    if (g.kernels == 0 && launch_update_s_fast(g, f, st)) return;
+    if (g.nd == 21 || g.nd == 22) {
+        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
+        if (g.nd == 21) DISPATCH_F(g.F, k_s2d_sh<FF><<<gr, b, 0, st>>>(g, f))
+        else DISPATCH_F(g.F, k_s2d_acc<FF><<<gr, b, 0, st>>>(g, f))
+        return;
+    }
     if (g.nd == 3) {
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
         DISPATCH_F(g.F, k_s3d<FF><<<gr, b, 0, st>>>(g, f));
@@ -1200,6 +1407,11 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
 
 void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st)
 {
+    if (g.nd == 21) {
+        DISPATCH_F(g.F, k_surf_sh<FF><<<cdiv(g.nx, 128), 128, 0, st>>>(g, f));
+        return;
+    }
+    if (g.nd == 22) return;
     if (g.nd == 3) {
         dim3 b(32, 4), gr(cdiv(g.ny, 32), cdiv(g.nx, 4));
         DISPATCH_F(g.F, k_surf3d<FF><<<gr, b, 0, st>>>(g, f, pdir));

@@ -14,6 +14,9 @@ struct BndSlot {            // saved-boundary stores, by value
 };
 
 void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st);
+bool launch_update_v_fast(const Grid &g, const Fields &f, cudaStream_t st);
+bool launch_update_s_fast(const Grid &g, const Fields &f, cudaStream_t st);
+int fast3d_xchunk(const Grid &g);
 void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st);
 void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st);
 void launch_savebnd(const Grid &g, const Fields &f, const BndSlot &b, int prec, int64_t tofs, cudaStream_t st);

@@ -106,9 +106,9 @@ extern "C" int sfd_forward_noalloc(sfd_plan *p, const float *src_pos, const floa
     int nsel = 0;
     for (int o = 0; o < SFD_NOUT; o++) {
         if (!outsel || !outsel[o]) continue;
-        if (o != SFD_OUT_P && g.nd != 3 && !(o == SFD_OUT_VX || o == SFD_OUT_VZ || o == SFD_OUT_SXX ||
-                                              o == SFD_OUT_SZZ || o == SFD_OUT_SXZ)) {
-            p->err = "requested output variable does not exist in 2D P-SV";
+        bool ok = o == SFD_OUT_P ? g.nd != 21 : (p->f.w[o] != nullptr && !(g.nd == 22 && o == SFD_OUT_SXX));
+        if (!ok) {
+            p->err = "requested output variable does not exist in this physics";
             return SFD_ERR_ARG;
         }
         omask |= 1u << o;
@@ -116,9 +116,13 @@ extern "C" int sfd_forward_noalloc(sfd_plan *p, const float *src_pos, const floa
     }
     if (nsel && !seis) { p->err = "missing seismogram buffer"; return SFD_ERR_ARG; }
 
-    // carve the scratch: wave fields, memory variables, CPML memory, maps
-    const int nwave = g.nd == 3 ? 9 : 5;
-    const int nmem = g.L == 0 ? 0 : (g.nd == 3 ? 6 : 3);
+    // carve the scratch: the plan's own set of wave fields and memory
+    // variables (which depends on the physics), CPML memory, maps
+    int ids[NW], rids[NR], nwave = 0, nmem = 0;
+    for (int w = 0; w < NW; w++)
+        if (p->f.w[w]) ids[nwave++] = w;
+    for (int r = 0; r < NR; r++)
+        if (p->f.r[r]) rids[nmem++] = r;
     size_t need = 0;
     size_t off_w = need; need += align256(sizeof(float) * g.nvol * nwave);
     size_t off_r = need; need += align256(sizeof(float) * g.nvol * g.L * nmem);
@@ -150,14 +154,8 @@ extern "C" int sfd_forward_noalloc(sfd_plan *p, const float *src_pos, const floa
     cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
 
     Fields f = p->f;  // parameters, CPML constants and taper stay the plan's
-    static const int ids3[] = {VX, VY, VZ, SXX, SYY, SZZ, SXY, SYZ, SXZ};
-    static const int ids2[] = {VX, VZ, SXX, SZZ, SXZ};
-    const int *ids = g.nd == 3 ? ids3 : ids2;
     for (int w = 0; w < NW; w++) f.w[w] = nullptr;
     for (int q = 0; q < nwave; q++) f.w[ids[q]] = (float *)(base + off_w) + (int64_t)q * g.nvol;
-    static const int rid3[] = {RXX, RYY, RZZ, RXY, RYZ, RXZ};
-    static const int rid2[] = {RXX, RZZ, RXZ};
-    const int *rids = g.nd == 3 ? rid3 : rid2;
     for (int r = 0; r < NR; r++) f.r[r] = nullptr;
     for (int q = 0; q < nmem; q++) f.r[rids[q]] = (float *)(base + off_r) + (int64_t)q * g.nvol * g.L;
     int64_t poff = 0;

@@ -190,11 +190,17 @@ int transform_model(const sfd_config &c, int nz, int ny, int nx, const float *co
     const double dt = c.dt, dh = c.dh;
     std::vector<double> M(n), mu(n), rho(n), taup(n, 0.0), taus(n, 0.0);
     const float *pa = params[0], *pb = params[1], *prho = params[2];
-    if (!pa || !prho) { err = "vp (or M / Ip) and rho are required"; return SFD_ERR_ARG; }
+    // SH reads only vs and rho, acoustic only vp and rho (assign_modeling_case.c:1004-1016)
+    if (c.nd == 21) pa = nullptr;
+    if (c.nd == 22) pb = nullptr;
+    if ((c.nd != 21 && !pa) || (c.nd == 21 && !pb) || !prho) {
+        err = c.nd == 21 ? "vs (or mu / Is) and rho are required" : "vp (or M / Ip) and rho are required";
+        return SFD_ERR_ARG;
+    }
     for (int64_t i = 0; i < n; i++) {
         double r = prho[i];
         if (!(r > 0)) { err = "rho must be positive everywhere"; return SFD_ERR_ARG; }
-        double a = pa[i], b = pb ? pb[i] : 0.0;
+        double a = pa ? pa[i] : 0.0, b = pb ? pb[i] : 0.0;
         if (c.param_type == 0) { M[i] = a * a * r * dt / dh; mu[i] = b * b * r * dt / dh; }
         else if (c.param_type == 1) { M[i] = a * dt / dh; mu[i] = b * dt / dh; }
         else if (c.param_type == 2) { M[i] = (a / r) * (a / r) * r * dt / dh; mu[i] = (b / r) * (b / r) * r * dt / dh; }
@@ -289,17 +295,22 @@ int source_targets(int nd, int mask, int type, int fields[3], float div[3])
 {
     static const int vl2[] = {VX, VZ, SXX, SZZ, SXZ};
     static const int vl3[] = {VX, VY, VZ, SXX, SZZ, SXZ, SXY, SYZ, SYY};
-    static const int by_type[4] = {VX, VY, VZ, -1};
-    const int *vl = nd == 3 ? vl3 : vl2;
-    int nvl = nd == 3 ? 9 : 5;
+    static const int vl21[] = {VY, SXY, SYZ};
+    static const int vl22[] = {VX, VZ, SXX};  // vx, vz, p (acoustic pressure in the SXX slot)
+    // type 3 is a variable named p in the acoustic model, the average of the
+    // normal stresses in P-SV and 3D; SH and acoustic have no averaged p
+    const int by_type[4] = {VX, VY, VZ, nd == 22 ? SXX : -1};
+    const int *vl = nd == 3 ? vl3 : (nd == 21 ? vl21 : (nd == 22 ? vl22 : vl2));
+    int nvl = nd == 3 ? 9 : (nd == 21 || nd == 22 ? 3 : 5);
+    bool has_avg = nd == 2 || nd == 3;
     bool fed[9] = {false};
-    bool fed_p = (mask & (1 << 4)) != 0;
+    bool fed_p = has_avg && (mask & (1 << 4)) != 0;
     for (int t = 0; t < 4; t++) {
         if (!(mask & (1 << t))) continue;
         if (by_type[t] >= 0)
             for (int j = 0; j < nvl; j++)
                 if (vl[j] == by_type[t]) fed[j] = true;
-        if (t == 3) fed_p = true;
+        if (t == 3 && has_avg) fed_p = true;
     }
     int ntypes = fed_p ? 1 : 0;
     for (int j = 0; j < nvl; j++) ntypes += fed[j];

@@ -35,7 +35,7 @@ class sfd_config(C.Structure):
                 ("fl", C.c_float * 8), ("vppml", C.c_float), ("fpml", C.c_float), ("npower", C.c_float),
                 ("k_max_cpml", C.c_float), ("abpc", C.c_float), ("tmin", C.c_int), ("tmax", C.c_int),
                 ("param_type", C.c_int), ("restype", C.c_int), ("precision", C.c_int),
-                ("reserved", C.c_int * 7)]
+                ("kernels", C.c_int), ("reserved", C.c_int * 6)]
 
 
 class sfd_shot(C.Structure):
@@ -130,6 +130,7 @@ class Config:
     param_type: int = 0
     restype: int = 0
     precision: str = "fp32"
+    kernels: str = "fast"  # "fast": register-blocked 3D kernels where available; "general"
 
     def to_c(self) -> sfd_config:
         c = sfd_config()
@@ -160,6 +161,7 @@ class Config:
         c.param_type = int(self.param_type)
         c.restype = int(self.restype)
         c.precision = PREC[self.precision]
+        c.kernels = {"fast": 0, "general": 1}[self.kernels]
         return c
 
     @property

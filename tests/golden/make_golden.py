@@ -27,6 +27,8 @@ CASES = {
     "psv2d_taper_fd4": dict(nd=2, freesurf=0, L=0, abs_type=2, src_type=100, fdorder=4),
     "el3d_fs_elastic": dict(nd=3, freesurf=1, L=0, abs_type=1, src_type=100, nz=36, ny=34, nx=38, nt=100, nab=8),
     "el3d_visco_l2": dict(nd=3, freesurf=1, L=2, abs_type=1, src_type=2, nz=36, ny=34, nx=38, nt=100, nab=8),
+    "acoustic2d_l1": dict(nd=22, freesurf=0, L=1, abs_type=1, src_type=3),
+    "sh2d_elastic": dict(nd=21, freesurf=0, L=0, abs_type=2, src_type=1),
 }
 
 
@@ -41,15 +43,19 @@ def input_hash(model, acq):
 
 
 def outputs_of(nd):
-    return ["vx", "vy", "vz", "p"] if nd == 3 else ["vx", "vz", "p"]
+    return {3: ["vx", "vy", "vz", "p"], 21: ["vy", "sxy", "syz"]}.get(nd, ["vx", "vz", "p"])
 
 
 def run(kw, ref=True):
     cfg, model, acq = make_case(**kw)
     o = Oracle(cfg, ref=ref)
-    rc = o.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+    nd = cfg["nd"]
+    rc = o.set_model(model["vp"] if nd != 21 else None, model["vs"] if nd != 22 else None, model["rho"],
+                     model["taup"], model["taus"])
     assert rc == 0
-    outs = outputs_of(cfg["nd"])
+    outs = outputs_of(nd)
+    if nd in (21, 22):  # forward only in the reference
+        return cfg, model, acq, o.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs), {}
     d = o.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs, save_boundaries=True)
     res = {k: (0.3 * v).astype(np.float32) for k, v in d.items() if k != "p"}
     o.clear_gradients()

@@ -118,3 +118,69 @@ def test_adjoint_requires_forward(cuda_device):
     with pytest.raises(SeisCLEngineError) as e:
         plan.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], {"vx": np.zeros((len(acq["rec_pos"]), 20))})
     assert e.value.code == -5
+
+
+FAST_CASES = [
+    dict(nd=3, freesurf=1, L=2, abs_type=1, src_type=100, nz=38, ny=29, nx=31, nt=80, nab=6),
+    dict(nd=3, freesurf=0, L=1, abs_type=2, src_type=2, nz=70, ny=35, nx=22, nt=60, nab=5),
+    dict(nd=3, freesurf=1, L=0, abs_type=1, src_type=0, nz=34, ny=18, nx=40, nt=60, nab=6, fdorder=12),
+    dict(nd=3, freesurf=0, L=3, abs_type=1, src_type=100, nz=36, ny=20, nx=24, nt=60, nab=6, fdorder=4),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", FAST_CASES, ids=lambda k: "-".join("%s%s" % (a, b) for a, b in k.items()))
+def test_fast_3d_kernels_match_general(kw, cuda_device):
+    """The register-blocked 3D kernels against the general ones (ragged
+    tiles, CPML and taper, viscoelastic, FDORDER 4/8/12) and the oracle."""
+    import dataclasses
+
+    from oracle.oracle import Oracle
+    from seiscl_b200.engine import Plan
+
+    cfg, model, acq = make_case(**kw)
+    outs = _outputs(3)
+    res = {}
+    for variant in ("fast", "general"):
+        ec = dataclasses.replace(engine_config(cfg), kernels=variant)
+        plan = Plan(ec)
+        plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+        res[variant] = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
+    ora = Oracle(cfg)
+    ora.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+    ref = ora.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
+    for n in outs:
+        assert rel_l2(res["fast"][n], res["general"][n]) < 1e-6, n
+        assert rel_l2(res["fast"][n], ref[n]) < FWD_TOL, n
+
+
+OTHER_PHYSICS = [
+    dict(nd=22, freesurf=0, L=0, abs_type=1, src_type=3),
+    dict(nd=22, freesurf=0, L=1, abs_type=2, src_type=3),
+    dict(nd=22, freesurf=0, L=0, abs_type=1, src_type=0, fdorder=4),
+    dict(nd=21, freesurf=0, L=0, abs_type=1, src_type=1),
+    dict(nd=21, freesurf=1, L=0, abs_type=2, src_type=1),
+    dict(nd=21, freesurf=0, L=0, abs_type=1, src_type=1, fdorder=2),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", OTHER_PHYSICS, ids=lambda k: "-".join("%s%s" % (a, b) for a, b in k.items()))
+def test_acoustic_and_sh_forward_match_oracle(kw, cuda_device):
+    """2D acoustic (ND=22) and SH (ND=21) forward modelling."""
+    from oracle.oracle import Oracle
+    from seiscl_b200.engine import Plan
+
+    cfg, model, acq = make_case(**kw)
+    outs = ["vx", "vz", "p"] if cfg["nd"] == 22 else ["vy", "sxy", "syz"]
+    vp = model["vp"] if cfg["nd"] != 21 else None
+    vs = model["vs"] if cfg["nd"] != 22 else None
+    ora = Oracle(cfg)
+    assert ora.set_model(vp, vs, model["rho"], model["taup"], model["taus"]) == 0
+    ref = ora.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
+    plan = Plan(engine_config(cfg))
+    plan.set_model(vp, vs, model["rho"], model["taup"], model["taus"])
+    got = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
+    for n in outs:
+        assert np.abs(ref[n]).max() > 0, n
+        assert rel_l2(got[n], ref[n]) < FWD_TOL, (n, rel_l2(got[n], ref[n]))

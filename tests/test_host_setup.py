@@ -70,7 +70,7 @@ def test_point_cells_bit_exact():
             assert cells[r] == want, (dh, r, pos[r, :3])
 
 
-@pytest.mark.parametrize("nd", [2, 3])
+@pytest.mark.parametrize("nd", [2, 3, 21, 22])
 def test_source_targets_match_oracle(nd):
     import ctypes as C
 

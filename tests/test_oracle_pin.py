@@ -36,8 +36,12 @@ def _run(kw, ref=False):
 
     cfg, model, acq = make_case(**kw)
     o = Oracle(cfg, ref=ref)
-    assert o.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"]) == 0
-    outs = ["vx", "vy", "vz", "p"] if cfg["nd"] == 3 else ["vx", "vz", "p"]
+    nd = cfg["nd"]
+    assert o.set_model(model["vp"] if nd != 21 else None, model["vs"] if nd != 22 else None, model["rho"],
+                       model["taup"], model["taus"]) == 0
+    outs = {3: ["vx", "vy", "vz", "p"], 21: ["vy", "sxy", "syz"]}.get(nd, ["vx", "vz", "p"])
+    if nd in (21, 22):
+        return cfg, model, acq, o.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs), {}, o
     d = o.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs, save_boundaries=True)
     res = {k: (0.3 * v).astype(np.float32) for k, v in d.items() if k != "p"}
     o.clear_gradients()
@@ -54,7 +58,7 @@ def test_port_reproduces_golden(name):
     for k, v in d.items():
         assert np.array_equal(v, gold["seis_" + k]), k
     for k, v in g.items():
-        if cfg["nd"] == 2:
+        if cfg["nd"] in (2, 21, 22):
             assert np.array_equal(v, gold["grad_" + k]), k
         else:
             v64 = v.astype(np.float64)
@@ -65,6 +69,34 @@ def _ref_available():
     from oracle import build
 
     return build.ref_available()
+
+
+LIVE_2D_OTHER = [
+    dict(nd=22, freesurf=0, L=0, abs_type=1, src_type=3, nt=80, seed=6),
+    dict(nd=22, freesurf=0, L=2, abs_type=2, src_type=0, nt=80, seed=7),
+    dict(nd=21, freesurf=0, L=0, abs_type=1, src_type=1, nt=80, seed=8),
+    dict(nd=21, freesurf=0, L=0, abs_type=2, src_type=1, nt=80, seed=9, fdorder=2),
+]
+
+
+@pytest.mark.skipif(not _ref_available(), reason="reference tree not present")
+@pytest.mark.parametrize("kw", LIVE_2D_OTHER, ids=lambda k: "-".join("%s%s" % (a, b) for a, b in k.items()))
+def test_acoustic_sh_port_matches_reference_build(kw):
+    """Acoustic (ND=22) and SH (ND=21) forward kernels, compiled in place."""
+    from oracle.oracle import Oracle
+
+    cfg, model, acq = make_case(**kw)
+    outs = ["vx", "vz", "p"] if cfg["nd"] == 22 else ["vy", "sxy", "syz"]
+    vp = model["vp"] if cfg["nd"] != 21 else None
+    vs = model["vs"] if cfg["nd"] != 22 else None
+    res = []
+    for ref in (False, True):
+        o = Oracle(cfg, ref=ref)
+        assert o.set_model(vp, vs, model["rho"], model["taup"], model["taus"]) == 0
+        res.append(o.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs))
+    for k in outs:
+        assert np.abs(res[0][k]).max() > 0
+        assert np.array_equal(res[0][k], res[1][k]), k
 
 
 LIVE = [
