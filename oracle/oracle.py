@@ -258,6 +258,48 @@ class Oracle:
             return None
         return np.ctypeslib.as_array(p, shape=(int(n),)).copy()
 
+    def residual_scale(self, rec_pos, residuals: dict) -> dict:
+        """Adjoint-source scaling of src/residuals.c:452-568 (res_scale,
+        FP16=0): velocity residuals times dt / (b * dh / dt) with b the
+        buoyancy (rip/rjp/rkp) of the receiver's cell, whose x, y and z are
+        all taken from rec_pos column 0 (residuals.c:487-489); pressure
+        residuals times -2 (M - mu) dh / dt * dt, with the reference's mix of
+        FP32 and double intermediates."""
+        c = self.cfg
+        rec_pos = np.ascontiguousarray(rec_pos, np.float32).reshape(-1, 8)
+        nt = c["nt"]
+        tmax = c.get("tmax", 0) or nt
+        dh = np.float32(c["dh"])
+        dt = np.float32(c["dt"])
+        nz, ny = c["nz"], c["ny"]
+        out = {}
+        for name, r in residuals.items():
+            r = np.array(r, dtype=np.float32, copy=True).reshape(rec_pos.shape[0], nt)
+            if name in ("vx", "vy", "vz"):
+                par = self.array("param", {"vx": "rip", "vy": "rjp", "vz": "rkp"}[name])
+            elif name == "p":
+                M = self.array("param", "M")
+                mu = self.array("param", "mu")
+            else:
+                out[name] = r
+                continue
+            for g in range(rec_pos.shape[0]):
+                if name == "p":
+                    x, y, z = (int(rec_pos[g, k] / dh) for k in range(3))
+                else:
+                    x = y = z = int(rec_pos[g, 0] / dh)
+                pos = (x * ny + y) * nz + z if c["nd"] == 3 else x * nz + z
+                if name == "p":
+                    # FP32 difference, double product, FP32 factor parscal*dt
+                    parscal = np.float32(-2.0 * float(M[pos] - mu[pos]) * float(dh) / float(dt))
+                    r[g, :tmax] *= np.float32(parscal * dt)
+                else:
+                    parscal = np.float32(1.0 / float(par[pos]) * float(dh) / float(dt))
+                    f = 1.0 / float(parscal) * float(dt)
+                    r[g, :tmax] = (r[g, :tmax].astype(np.float64) * f).astype(np.float32)
+            out[name] = r
+        return out
+
     def run_steps(self, n):
         self.lib.fdo_run_steps(self.h, n)
 
