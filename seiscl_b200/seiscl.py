@@ -37,6 +37,7 @@ from typing import Dict, List, Optional
 import numpy as np
 
 from . import engine
+from . import shots as shots_mod
 
 # Seismogram variables of each modelling case (assign_modeling_case.c:1242-1322);
 # "p" is a transformed variable of the elastic cases and a field in acoustics.
@@ -667,6 +668,9 @@ class SeisCL:
             raise SeisCLError("Error: Cannot input and output residuals simultaneously")
         outs = self._outputs(din, resin)
         shots = self._shots()
+        # shots of this rank when running one process per GPU (time_stepping.c:705-722)
+        rank, world, _ = shots_mod.dist_context()
+        smin, smax = shots_mod.shot_range(len(shots), rank, world)
         sp_all = np.asarray(self.src_pos, dtype=np.float32).T
         src_all = np.asarray(self.src, dtype=np.float32).T
         rp_all = np.asarray(self.rec_pos, dtype=np.float32).T
@@ -678,7 +682,7 @@ class SeisCL:
         if self.gradout:
             plan.zero_gradient()
         try:
-            for sid, si, gi in shots:
+            for sid, si, gi in shots[smin:smax]:
                 sp, src, rp = sp_all[si], src_all[si], rp_all[gi]
                 if self.inputres and self.gradout:
                     res = {k: np.ascontiguousarray(np.transpose(resin[k + "res"]), dtype=np.float32)[
@@ -703,6 +707,17 @@ class SeisCL:
                 plan.adjoint(sp, src, rp, res)
         except engine.SeisCLEngineError as exc:
             raise SeisCLError(str(exc)) from exc
+        if world > 1:
+            # every rank filled only its own traces: one sum gives all of them
+            # (Out_MPI.c:70-160); the gradient is summed after the chain rule,
+            # which is linear in the accumulated kernels
+            red = {"seis_" + k: v for k, v in seis.items()}
+            red.update({"res_" + k: v for k, v in resid.items()})
+            red["rms"] = np.array([rms, rmsnorm])
+            red = shots_mod.allreduce_sum(red)
+            seis = {k: red["seis_" + k] for k in seis}
+            resid = {k: red["res_" + k] for k in resid}
+            rms, rmsnorm = (float(v) for v in red["rms"])
         if not (self.inputres and self.gradout):
             dout = {k + "out": np.ascontiguousarray(seis[k].T) for k in outs}
             if self.resout and not self.inputres:
@@ -716,6 +731,8 @@ class SeisCL:
                                           "rms_norm": np.array([np.sqrt(rmsnorm)], np.float32)}
         if self.gradout:
             g = plan.gradient(transform=True)
+            if world > 1:
+                g = shots_mod.allreduce_sum(g)
             shape = tuple(int(v) for v in np.atleast_1d(self.N))
             names = {0: ("vp", "vs"), 1: ("M", "mu"), 2: ("Ip", "Is")}[self.param_type]
             gout = {}
@@ -727,7 +744,8 @@ class SeisCL:
                 gout["grad" + name] = np.ascontiguousarray(np.transpose(g[name])).reshape(shape)
             self._files[self.file_gout] = gout
         ms = (time.perf_counter() - t0) * 1e3
-        return "%d shot(s), %d trace(s), %d time steps: %.1f ms\n" % (len(shots), ntr, NT, ms)
+        return "%d shot(s) (%d on rank %d of %d), %d trace(s), %d time steps: %.1f ms\n" % (
+            len(shots), smax - smin, rank, world, ntr, NT, ms)
 
     def close(self):
         if self._plan is not None:
