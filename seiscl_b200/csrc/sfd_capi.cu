@@ -296,7 +296,8 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     // N[0] must be even (read_hdf5.c:535-540)
     if (c.n[0] % 2) return SFD_ERR_ARG;
     if (c.precision < 0 || c.precision > 2) return SFD_ERR_ARG;
-    if (c.kernels < 0 || c.kernels > 1) return SFD_ERR_ARG;
+    if (c.kernels < 0 || c.kernels > 2) return SFD_ERR_ARG;
+    if (c.adjoint_reset_psi < 0 || c.adjoint_reset_psi > 1) return SFD_ERR_ARG;
 
     sfd_plan *p = new sfd_plan();
     p->cfg = c;
@@ -315,7 +316,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     g.L = c.L;
     g.freesurf = c.freesurf ? 1 : 0;
     g.restype = c.restype;
-    g.kernels = c.kernels == 1 ? 1 : 0;
+    g.kernels = c.kernels;
     g.nvol = (int64_t)g.NZ * g.NY * g.NX;
     double hc[6];
     holberg(c.fdorder, c.maxrelerror, hc);
@@ -448,6 +449,8 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
     }
     CKC(cudaStreamSynchronize(st));
     cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1);
+    if (tma_take_status())
+        return fail(p, SFD_ERR_CUDA, "a TMA stage of the 3D stencil kernels did not arrive within its time bound");
     p->have_forward = save_boundaries != 0;
     return SFD_OK;
 }
@@ -484,6 +487,12 @@ extern "C" int sfd_adjoint(sfd_plan *p, const sfd_shot *shot, int mask, const in
         if (p->a.wr[w]) CKC(cudaMemsetAsync(p->a.wr[w], 0, sizeof(float) * g.nvol, st));
     for (int r = 0; r < NR; r++)
         if (p->a.rr[r]) CKC(cudaMemsetAsync(p->a.rr[r], 0, sizeof(float) * g.nvol * g.L, st));
+    if (p->cfg.adjoint_reset_psi) {
+        // optional: start the adjoint with clean CPML memory instead
+        int64_t tot = 0;
+        for (int i = 0; i < NPSI; i++) tot += p->psi_size[i];
+        if (tot) CKC(cudaMemsetAsync(p->d_psi_all, 0, sizeof(float) * tot, st));
+    }
     AdjFields a = p->a;
     CKC(cudaEventRecord(p->ev0, st));
     for (int t = p->cfg.tmax - 1; t > p->cfg.tmin; t--) {
@@ -596,6 +605,13 @@ extern "C" int sfd_plan_info(const sfd_plan *p, int64_t *o)
     o[0] = p->g.NZ; o[1] = p->g.NY; o[2] = p->g.NX; o[3] = p->g.nvol;
     o[4] = (int64_t)p->g.nz * p->g.ny * p->g.nx; o[5] = p->g.nbnd; o[6] = p->g.F; o[7] = p->cfg.tmax;
     return SFD_OK;
+}
+
+extern "C" int sfd_plan_uses_tma(const sfd_plan *p)
+{
+    if (!p) return SFD_ERR_ARG;
+    if (cudaSetDevice(p->device) != cudaSuccess) return SFD_ERR_CUDA;
+    return tma_ready(p->g, p->f) ? 1 : 0;
 }
 
 extern "C" int64_t sfd_debug_copy(sfd_plan *p, int kind, int id, float *dst, int64_t cap)

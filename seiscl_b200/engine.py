@@ -35,7 +35,7 @@ class sfd_config(C.Structure):
                 ("fl", C.c_float * 8), ("vppml", C.c_float), ("fpml", C.c_float), ("npower", C.c_float),
                 ("k_max_cpml", C.c_float), ("abpc", C.c_float), ("tmin", C.c_int), ("tmax", C.c_int),
                 ("param_type", C.c_int), ("restype", C.c_int), ("precision", C.c_int),
-                ("kernels", C.c_int), ("reserved", C.c_int * 6)]
+                ("kernels", C.c_int), ("adjoint_reset_psi", C.c_int), ("reserved", C.c_int * 5)]
 
 
 class sfd_shot(C.Structure):
@@ -58,6 +58,7 @@ EXPORTS = {
     "sfd_get_gradient": (C.c_int, [C.c_void_p, C.c_int, FP, FP, FP]),
     "sfd_residual_scale": (C.c_int, [C.c_void_p, C.POINTER(sfd_shot), C.POINTER(C.c_int), C.POINTER(FP)]),
     "sfd_plan_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "sfd_plan_uses_tma": (C.c_int, [C.c_void_p]),
     "sfd_debug_copy": (C.c_int64, [C.c_void_p, C.c_int, C.c_int, FP, C.c_int64]),
     "sfd_last_loop_ms": (C.c_float, [C.c_void_p]),
     "sfd_bench_kernels": (C.c_int, [C.c_void_p, C.c_int, FP]),
@@ -130,7 +131,8 @@ class Config:
     param_type: int = 0
     restype: int = 0
     precision: str = "fp32"
-    kernels: str = "fast"  # "fast": register-blocked 3D kernels where available; "general"
+    kernels: str = "fast"  # "fast": TMA-pipelined 3D kernels where eligible; "general"; "register"
+    adjoint_reset_psi: bool = False  # True: the adjoint starts from zeroed CPML memory (not the reference's)
 
     def to_c(self) -> sfd_config:
         c = sfd_config()
@@ -161,7 +163,8 @@ class Config:
         c.param_type = int(self.param_type)
         c.restype = int(self.restype)
         c.precision = PREC[self.precision]
-        c.kernels = {"fast": 0, "general": 1}[self.kernels]
+        c.kernels = {"fast": 0, "general": 1, "register": 2}[self.kernels]
+        c.adjoint_reset_psi = 1 if self.adjoint_reset_psi else 0
         return c
 
     @property
@@ -289,6 +292,14 @@ class Plan:
         out = (C.c_float * 3)()
         self._check(self.lib.sfd_bench_kernels(self.h, int(nrep), out))
         return list(out)
+
+    @property
+    def uses_tma(self) -> bool:
+        """True when the 3D updates of this plan run on the TMA-pipelined kernels."""
+        rc = int(self.lib.sfd_plan_uses_tma(self.h))
+        if rc < 0:
+            self._check(rc)
+        return rc == 1
 
     @property
     def last_loop_ms(self) -> float:
