@@ -1371,7 +1371,8 @@ static inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b)
 
 void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
 {
-    if (g.kernels == 0 && launch_update_v_fast(g, f, st)) return;
+    if (g.kernels == 0 && launch_update_v_tma(g, f, st)) return;
+    if (g.kernels == 2 && launch_update_v_fast(g, f, st)) return;
     if (g.nd == 21 || g.nd == 22) {
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
         if (g.nd == 21) DISPATCH_F(g.F, k_v2d_sh<FF><<<gr, b, 0, st>>>(g, f))
@@ -1389,7 +1390,8 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
 
 void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
 {
-    if (g.kernels == 0 && launch_update_s_fast(g, f, st)) return;
+    if (g.kernels == 0 && launch_update_s_tma(g, f, st)) return;
+    if (g.kernels == 2 && launch_update_s_fast(g, f, st)) return;
     if (g.nd == 21 || g.nd == 22) {
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
         if (g.nd == 21) DISPATCH_F(g.F, k_s2d_sh<FF><<<gr, b, 0, st>>>(g, f))

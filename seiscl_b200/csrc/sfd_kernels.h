@@ -17,6 +17,10 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st);
 bool launch_update_v_fast(const Grid &g, const Fields &f, cudaStream_t st);
 bool launch_update_s_fast(const Grid &g, const Fields &f, cudaStream_t st);
 int fast3d_xchunk(const Grid &g);
+bool launch_update_v_tma(const Grid &g, const Fields &f, cudaStream_t st);
+bool launch_update_s_tma(const Grid &g, const Fields &f, cudaStream_t st);
+bool tma_ready(const Grid &g, const Fields &f);  // the TMA kernels will run for this plan
+int tma_take_status();      // 1 if a TMA stage of the last launches never arrived (and clears it)
 void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st);
 void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st);
 void launch_savebnd(const Grid &g, const Fields &f, const BndSlot &b, int prec, int64_t tofs, cudaStream_t st);

@@ -121,6 +121,12 @@ def test_adjoint_requires_forward(cuda_device):
 
 
 FAST_CASES = [
+    # TMA-eligible (8th order, nz % 4 == 0): ragged y/x tiles, several x chunks
+    dict(nd=3, freesurf=1, L=2, abs_type=1, src_type=100, nz=36, ny=29, nx=31, nt=80, nab=6),
+    dict(nd=3, freesurf=0, L=0, abs_type=1, src_type=2, nz=68, ny=35, nx=22, nt=60, nab=5),
+    dict(nd=3, freesurf=0, L=1, abs_type=2, src_type=0, nz=40, ny=20, nx=44, nt=60, nab=6),
+    dict(nd=3, freesurf=1, L=3, abs_type=1, src_type=100, nz=36, ny=18, nx=40, nt=60, nab=6),
+    # not eligible (odd nz tiles, other orders): register-blocked kernels only
     dict(nd=3, freesurf=1, L=2, abs_type=1, src_type=100, nz=38, ny=29, nx=31, nt=80, nab=6),
     dict(nd=3, freesurf=0, L=1, abs_type=2, src_type=2, nz=70, ny=35, nx=22, nt=60, nab=5),
     dict(nd=3, freesurf=1, L=0, abs_type=1, src_type=0, nz=34, ny=18, nx=40, nt=60, nab=6, fdorder=12),
@@ -131,8 +137,9 @@ FAST_CASES = [
 @pytest.mark.gpu
 @pytest.mark.parametrize("kw", FAST_CASES, ids=lambda k: "-".join("%s%s" % (a, b) for a, b in k.items()))
 def test_fast_3d_kernels_match_general(kw, cuda_device):
-    """The register-blocked 3D kernels against the general ones (ragged
-    tiles, CPML and taper, viscoelastic, FDORDER 4/8/12) and the oracle."""
+    """The TMA-pipelined and register-blocked 3D kernels against the general
+    ones (ragged tiles, CPML and taper, free surface, L = 0..3, FDORDER
+    4/8/12) and the oracle.  Eligible cases must actually take the TMA path."""
     import dataclasses
 
     from oracle.oracle import Oracle
@@ -141,17 +148,23 @@ def test_fast_3d_kernels_match_general(kw, cuda_device):
     cfg, model, acq = make_case(**kw)
     outs = _outputs(3)
     res = {}
-    for variant in ("fast", "general"):
+    for variant in ("fast", "register", "general"):
         ec = dataclasses.replace(engine_config(cfg), kernels=variant)
         plan = Plan(ec)
         plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+        if variant == "fast":
+            eligible = kw.get("fdorder", 8) == 8 and kw["nz"] % 4 == 0
+            assert plan.uses_tma == eligible
+        else:
+            assert not plan.uses_tma
         res[variant] = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
     ora = Oracle(cfg)
     ora.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
     ref = ora.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
     for n in outs:
-        assert rel_l2(res["fast"][n], res["general"][n]) < 1e-6, n
-        assert rel_l2(res["fast"][n], ref[n]) < FWD_TOL, n
+        for v in ("fast", "register"):
+            assert rel_l2(res[v][n], res["general"][n]) < 1e-6, (v, n)
+            assert rel_l2(res[v][n], ref[n]) < FWD_TOL, (v, n)
 
 
 OTHER_PHYSICS = [
