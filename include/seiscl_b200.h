@@ -73,9 +73,11 @@ typedef struct sfd_config {
     int param_type;    /* 0: vp,vs,rho  1: M,mu,rho  2: Ip,Is,rho */
     int restype;       /* 0: L2 (full gradient), 1: M only */
     int precision;     /* SFD_PREC_*: storage of the saved boundaries */
-    int kernels;       /* 0: fastest available (TMA-pipelined 3D kernels where eligible),
+    int kernels;       /* 0: fastest measured: TMA-pipelined 3D stress update where
+                             eligible, general velocity update,
                           1: general one-thread-per-cell kernels only,
-                          2: register-blocked 3D kernels where available */
+                          2: register-blocked 3D kernels where available,
+                          3: TMA-pipelined 3D velocity and stress updates */
     int adjoint_reset_psi; /* 0: the adjoint continues with the forward run's CPML memory
                               (reference behaviour, src/clprogram.c:806-811); 1: it starts
                               from zeroed CPML memory.  With sources whose wave field is
@@ -193,9 +195,9 @@ int sfd_host_cpml(const sfd_config *cfg, float *out);
 /* Introspection for tests: padded dims, counts, boundary cells. */
 int sfd_plan_info(const sfd_plan *plan, int64_t *out8);
 
-/* 1 when the plan's 3D velocity and stress updates run on the TMA-pipelined
- * kernels (kernels = 0, 8th order, nz a multiple of 4), 0 when they run on
- * the other kernel families; negative on error.  No counterpart in the
+/* 1 when the plan's 3D stress update (and with kernels = 3 the velocity
+ * update) runs on the TMA-pipelined kernels (kernels = 0 or 3, 8th order, nz a
+ * multiple of 4), 0 otherwise; negative on error.  No counterpart in the
  * reference (kernel selection is internal to this engine). */
 int sfd_plan_uses_tma(const sfd_plan *plan);
 

@@ -202,7 +202,7 @@ int alloc_model(sfd_plan *p)
         if (e) return fail(p, SFD_ERR_MEMORY, "parameter allocation failed");
     }
     int nc = std::max(2 * g.nab, 1);
-    float *cst = (float *)dalloc(p, sizeof(float) * (3 * NC * nc + nc), &e);
+    float *cst = (float *)dalloc(p, sizeof(float) * (3 * NC * nc + nc + 6 * nc), &e);
     if (e) return fail(p, SFD_ERR_MEMORY, "constant allocation failed");
     for (int k = 0; k < NC; k++) {
         p->f.cx[k] = cst + (0 * NC + k) * nc;
@@ -210,6 +210,8 @@ int alloc_model(sfd_plan *p)
         p->f.cz[k] = cst + (2 * NC + k) * nc;
     }
     p->f.taper = cst + 3 * NC * nc;
+    for (int ax = 0; ax < 3; ax++)
+        for (int h = 0; h < 2; h++) p->f.kinv[ax][h] = cst + 3 * NC * nc + nc + (2 * ax + h) * nc;
     return SFD_OK;
 }
 
@@ -218,7 +220,7 @@ int upload_constants(sfd_plan *p)
     const Grid &g = p->g;
     const sfd_config &c = p->cfg;
     int nc = std::max(2 * g.nab, 1);
-    std::vector<float> h(3 * NC * nc + nc, 0.0f);
+    std::vector<float> h(3 * NC * nc + nc + 6 * nc, 0.0f);
     if (g.abs_type == 1 && g.nab > 0) {
         for (int ax = 0; ax < 3; ax++) {
             float *b = h.data() + ax * NC * nc;
@@ -228,6 +230,13 @@ int upload_constants(sfd_plan *p)
         }
     }
     if (g.abs_type == 2) cerjan_taper(c.abpc, g.nab, h.data() + 3 * NC * nc);
+    // reciprocals of K and K_half for kernels that multiply instead of divide
+    for (int ax = 0; ax < 3; ax++)
+        for (int hh = 0; hh < 2; hh++) {
+            const float *K = h.data() + ax * NC * nc + (hh ? CKH : CK) * nc;
+            float *ki = h.data() + 3 * NC * nc + nc + (2 * ax + hh) * nc;
+            for (int i = 0; i < nc; i++) ki[i] = K[i] != 0.0f ? 1.0f / K[i] : 0.0f;
+        }
     CKC(cudaMemcpy((void *)p->f.cx[0], h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice));
     return SFD_OK;
 }
@@ -296,7 +305,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     // N[0] must be even (read_hdf5.c:535-540)
     if (c.n[0] % 2) return SFD_ERR_ARG;
     if (c.precision < 0 || c.precision > 2) return SFD_ERR_ARG;
-    if (c.kernels < 0 || c.kernels > 2) return SFD_ERR_ARG;
+    if (c.kernels < 0 || c.kernels > 3) return SFD_ERR_ARG;
     if (c.adjoint_reset_psi < 0 || c.adjoint_reset_psi > 1) return SFD_ERR_ARG;
 
     sfd_plan *p = new sfd_plan();
@@ -324,6 +333,12 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     g.dt = c.dt;
     g.dt2 = (float)((double)c.dt / 2.0);
     for (int l = 0; l < 8; l++) g.eta[l] = l < c.L ? (float)(2.0 * 3.141592653589793238462643 * c.fl[l] * (double)c.dt) : 0.0f;
+    for (int l = 0; l < 8; l++) {
+        volatile float half = g.eta[l] * 0.5f;   // FP32 steps, as a kernel would form them
+        g.eta_b[l] = 1.0f / (1.0f + half);
+        g.eta_c[l] = 1.0f - half;
+    }
+    g.inv_dt = 1.0f / c.dt;
     g.nbnd = nbnd_cells(g.nd, g.nz, g.ny, g.nx, g.F, g.nab, g.freesurf);
     if (p->cfg.tmax <= 0 || p->cfg.tmax > c.nt) p->cfg.tmax = c.nt;
     if (p->cfg.tmin < 0) p->cfg.tmin = 0;

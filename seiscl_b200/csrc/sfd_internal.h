@@ -42,6 +42,8 @@ struct Grid {
     float hc[6];            // FD coefficients
     float dt, dt2;          // dt and dt/2
     float eta[8];           // 2 pi FL dt
+    float eta_b[8], eta_c[8];  // 1/(1+eta/2) and 1-eta/2, FP32 as the kernels would form them
+    float inv_dt;           // 1/dt rounded to FP32
     int nbnd;               // saved-boundary cells per field per step
     int restype;
     int kernels;            // 0: register-blocked 3D kernels where available, 1: general only
@@ -53,6 +55,7 @@ struct Fields {
     float *psi[NPSI];
     const float *p[NPAR];
     const float *cx[NC], *cy[NC], *cz[NC];
+    const float *kinv[3][2];  // 1/K and 1/K_half per axis (x, y, z), FP32-rounded on the host
     const float *taper;
 };
 

@@ -182,21 +182,39 @@ __device__ __forceinline__ void cpml(float *psi, i64 q, const float *K, const fl
 // exactly one role, and each role evaluates its outputs with the operation
 // order of the general kernels.
 //
-// rp[m] points at the ring slot of plane x-F+m; c is the thread's centre in
-// a haloed tile; C points at the thread's cell in the centre tiles of x.
+// rs[m] is the offset in shared memory of the ring slot of plane x-F+m; c is
+// the thread's centre in a haloed tile; C points at the thread's cell in the
+// centre tiles of plane x.
 
+// One thread's cell on plane x.  The z and y slab memberships do not change
+// along the thread's march in x and are computed once; the x memberships are
+// uniform over the CTA and recomputed per plane.
 struct Cell {
     int x, gz, gy;        // padded coordinates
     i64 iv;               // padded linear index
+    unsigned zy;          // bit 0: z low slab, 1: z high, 2: y low, 3: y high
+    unsigned xs;          // bit 0: x low slab, 1: x high
 };
 
-// CPML slab tests of the reference kernels (update_v3D.cl / update_s3D.cl)
-__device__ __forceinline__ bool in_zlo(const Grid &g, int gz) { return !g.freesurf && gz - TF < g.nab; }
-__device__ __forceinline__ bool in_zhi(const Grid &g, int gz) { return gz > g.NZ - g.nab - TF - 1; }
-__device__ __forceinline__ bool in_ylo(const Grid &g, int gy) { return gy - TF < g.nab; }
-__device__ __forceinline__ bool in_yhi(const Grid &g, int gy) { return gy > g.NY - g.nab - TF - 1; }
-__device__ __forceinline__ bool in_xlo(const Grid &g, int x) { return x - TF < g.nab; }
-__device__ __forceinline__ bool in_xhi(const Grid &g, int x) { return x > g.NX - g.nab - TF - 1; }
+// slab tests of the reference kernels (update_v3D.cl / update_s3D.cl)
+__device__ __forceinline__ unsigned zy_slabs(const Grid &g, int gz, int gy)
+{
+    return (unsigned)(!g.freesurf && gz - TF < g.nab) | (unsigned)(gz > g.NZ - g.nab - TF - 1) << 1 |
+           (unsigned)(gy - TF < g.nab) << 2 | (unsigned)(gy > g.NY - g.nab - TF - 1) << 3;
+}
+__device__ __forceinline__ unsigned x_slabs(const Grid &g, int x)
+{
+    return (unsigned)(x - TF < g.nab) | (unsigned)(x > g.NX - g.nab - TF - 1) << 1;
+}
+
+// psi = b psi + a d;  d = d / K + psi, with 1/K precomputed
+__device__ __forceinline__ void cpml_k(float *psi, i64 q, const float *Ki, const float *a, const float *b, int ci,
+                                       float &d)
+{
+    float ps = __ldg(b + ci) * psi[q] + __ldg(a + ci) * d;
+    psi[q] = ps;
+    d = d * __ldg(Ki + ci) + ps;
+}
 
 // CPML update of derivative d in the z (or y) slabs; H selects the half-node
 // profile, X that the two slabs are tested as if / else if (velocity kernel)
@@ -205,47 +223,47 @@ template <bool H, bool X>
 __device__ __forceinline__ void cpml_z(const Grid &g, const Fields &f, int psi, const Cell &e, float &d)
 {
     const int NAB = g.nab;
-    const float *K = f.cz[H ? CKH : CK], *A = f.cz[H ? CAH : CA], *B = f.cz[H ? CBH : CB];
-    if (in_zhi(g, e.gz)) {
+    const float *Ki = f.kinv[2][H], *A = f.cz[H ? CAH : CA], *B = f.cz[H ? CBH : CB];
+    if (e.zy & 2u) {
         i64 i = e.x - TF, j = e.gy - TF, kk = e.gz - g.NZ + NAB + TF + NAB;
         int ind = 2 * NAB - 1 - (int)kk;
-        cpml(f.psi[psi], (i * g.ny + j) * (2 * NAB) + kk, K, A, B, H ? ind : ind + 1, d);
+        cpml_k(f.psi[psi], (i * g.ny + j) * (2 * NAB) + kk, Ki, A, B, H ? ind : ind + 1, d);
         if (X) return;
     }
-    if (in_zlo(g, e.gz)) {
+    if (e.zy & 1u) {
         i64 i = e.x - TF, j = e.gy - TF, kk = e.gz - TF;
-        cpml(f.psi[psi], (i * g.ny + j) * (2 * NAB) + kk, K, A, B, (int)kk, d);
+        cpml_k(f.psi[psi], (i * g.ny + j) * (2 * NAB) + kk, Ki, A, B, (int)kk, d);
     }
 }
 template <bool H, bool X>
 __device__ __forceinline__ void cpml_y(const Grid &g, const Fields &f, int psi, const Cell &e, float &d)
 {
     const int NAB = g.nab;
-    const float *K = f.cy[H ? CKH : CK], *A = f.cy[H ? CAH : CA], *B = f.cy[H ? CBH : CB];
-    if (in_ylo(g, e.gy)) {
+    const float *Ki = f.kinv[1][H], *A = f.cy[H ? CAH : CA], *B = f.cy[H ? CBH : CB];
+    if (e.zy & 4u) {
         i64 i = e.x - TF, j = e.gy - TF, kk = e.gz - TF;
-        cpml(f.psi[psi], (i * (2 * NAB) + j) * g.nz + kk, K, A, B, (int)j, d);
+        cpml_k(f.psi[psi], (i * (2 * NAB) + j) * g.nz + kk, Ki, A, B, (int)j, d);
         if (X) return;
     }
-    if (in_yhi(g, e.gy)) {
+    if (e.zy & 8u) {
         i64 i = e.x - TF, j = e.gy - g.NY + NAB + TF + NAB, kk = e.gz - TF;
         int ind = 2 * NAB - 1 - (int)j;
-        cpml(f.psi[psi], (i * (2 * NAB) + j) * g.nz + kk, K, A, B, H ? ind : ind + 1, d);
+        cpml_k(f.psi[psi], (i * (2 * NAB) + j) * g.nz + kk, Ki, A, B, H ? ind : ind + 1, d);
     }
 }
 template <bool H>
 __device__ __forceinline__ void cpml_x(const Grid &g, const Fields &f, int psi, const Cell &e, float &d)
 {
     const int NAB = g.nab;
-    const float *K = f.cx[H ? CKH : CK], *A = f.cx[H ? CAH : CA], *B = f.cx[H ? CBH : CB];
-    if (in_xlo(g, e.x)) {
+    const float *Ki = f.kinv[0][H], *A = f.cx[H ? CAH : CA], *B = f.cx[H ? CBH : CB];
+    if (e.xs & 1u) {
         i64 i = e.x - TF, j = e.gy - TF, kk = e.gz - TF;
-        cpml(f.psi[psi], (i * g.ny + j) * g.nz + kk, K, A, B, (int)i, d);
+        cpml_k(f.psi[psi], (i * g.ny + j) * g.nz + kk, Ki, A, B, (int)i, d);
     }
-    if (in_xhi(g, e.x)) {
+    if (e.xs & 2u) {
         i64 i = e.x - g.NX + NAB + TF + NAB, j = e.gy - TF, kk = e.gz - TF;
         int ind = 2 * NAB - 1 - (int)i;
-        cpml(f.psi[psi], (i * g.ny + j) * g.nz + kk, K, A, B, H ? ind : ind + 1, d);
+        cpml_k(f.psi[psi], (i * g.ny + j) * g.nz + kk, Ki, A, B, H ? ind : ind + 1, d);
     }
 }
 
@@ -258,31 +276,32 @@ __device__ __forceinline__ void taper(const Grid &g, const Fields &f, const Cell
 #pragma unroll
         for (int i = 0; i < N; i++) v[i] *= t;
     };
-    if (in_zlo(g, e.gz)) mul(tp[e.gz - TF]);
-    if (in_zhi(g, e.gz)) mul(tp[g.NZ - TF - e.gz - 1]);
-    if (in_ylo(g, e.gy)) mul(tp[e.gy - TF]);
-    if (in_yhi(g, e.gy)) mul(tp[g.NY - TF - e.gy - 1]);
-    if (in_xlo(g, e.x)) mul(tp[e.x - TF]);
-    if (in_xhi(g, e.x)) mul(tp[g.NX - TF - e.x - 1]);
+    if (e.zy & 1u) mul(tp[e.gz - TF]);
+    if (e.zy & 2u) mul(tp[g.NZ - TF - e.gz - 1]);
+    if (e.zy & 4u) mul(tp[e.gy - TF]);
+    if (e.zy & 8u) mul(tp[g.NY - TF - e.gy - 1]);
+    if (e.xs & 1u) mul(tp[e.x - TF]);
+    if (e.xs & 2u) mul(tp[g.NX - TF - e.x - 1]);
 }
 
-__device__ __forceinline__ void column(const float *const *rp, int off, float *q)
+// the 2F+1 ring values at tile offset `off`; rs[m] = slot offset of plane x-F+m
+__device__ __forceinline__ void column(const float *sm, const int *rs, int off, float *q)
 {
 #pragma unroll
-    for (int m = 0; m <= 2 * TF; m++) q[m] = rp[m][off];
+    for (int m = 0; m <= 2 * TF; m++) q[m] = sm[rs[m] + off];
 }
 
 // velocity: ring sxx, sxy, sxz; plane (P) syy, szz, syz; centre vx, vy, vz, rip, rjp, rkp
 template <int ROLE>
-__device__ __forceinline__ void cell_v(const Grid &g, const Fields &f, const float *const *rp, const float *P,
+__device__ __forceinline__ void cell_v(const Grid &g, const Fields &f, const float *sm, const int *rs, const float *P,
                                        const float *C, int c, const Cell &e, const float *hc)
 {
-    const float *Rx = rp[TF];  // plane x of the ring fields
-    const bool cp = g.abs_type == 1;
+    const float *Rx = sm + rs[TF];  // plane x of the ring fields
+    const bool cp = g.abs_type == 1 && (e.zy | e.xs);
     float q[2 * TF + 1];
     float v;
     if (ROLE == 0) {           // vx = vx + (sxx_x + sxy_y + sxz_z) * rip
-        column(rp, c, q);
+        column(sm, rs, c, q);
         float sxx_x = dxf(q, hc), sxy_y = dyb(Rx + HALO + c, hc), sxz_z = dzb(Rx + 2 * HALO + c, hc);
         if (cp) {
             cpml_z<false, true>(g, f, PSXZ_Z, e, sxz_z);
@@ -291,7 +310,7 @@ __device__ __forceinline__ void cell_v(const Grid &g, const Fields &f, const flo
         }
         v = C[0 * CT] + (sxx_x + sxy_y + sxz_z) * C[3 * CT];
     } else if (ROLE == 1) {    // vy = vy + (syy_y + sxy_x + syz_z) * rjp
-        column(rp, HALO + c, q);
+        column(sm, rs, HALO + c, q);
         float syy_y = dyf(P + c, hc), sxy_x = dxb(q, hc), syz_z = dzb(P + 2 * HALO + c, hc);
         if (cp) {
             cpml_z<false, true>(g, f, PSYZ_Z, e, syz_z);
@@ -300,7 +319,7 @@ __device__ __forceinline__ void cell_v(const Grid &g, const Fields &f, const flo
         }
         v = C[1 * CT] + (syy_y + sxy_x + syz_z) * C[4 * CT];
     } else {                   // vz = vz + (szz_z + sxz_x + syz_y) * rkp
-        column(rp, 2 * HALO + c, q);
+        column(sm, rs, 2 * HALO + c, q);
         float szz_z = dzf(P + HALO + c, hc), sxz_x = dxb(q, hc), syz_y = dyb(P + 2 * HALO + c, hc);
         if (cp) {
             cpml_z<true, true>(g, f, PSZZ_Z, e, szz_z);
@@ -309,7 +328,7 @@ __device__ __forceinline__ void cell_v(const Grid &g, const Fields &f, const flo
         }
         v = C[2 * CT] + (szz_z + sxz_x + syz_y) * C[5 * CT];
     }
-    if (g.abs_type == 2) {
+    if (g.abs_type == 2 && (e.zy | e.xs)) {
         float t[1] = {v};
         taper<1>(g, f, e, t);
         v = t[0];
@@ -317,20 +336,92 @@ __device__ __forceinline__ void cell_v(const Grid &g, const Fields &f, const flo
     f.w[VX + ROLE][e.iv] = v;
 }
 
+// One shear stress Q (0: sxy, 1: syz, 2: sxz) and its memory variables, with
+// the two cross derivatives it needs; the general kernels' expressions.
+template <int L, int Q>
+__device__ __forceinline__ void shear(const Grid &g, const Fields &f, const float *sm, const int *rs, const float *C,
+                                      int c, const Cell &e, const float *hc)
+{
+    constexpr int CP = 6 + 6 * L;
+    const float *R = sm + rs[TF];
+    float q[2 * TF + 1];
+    float d1, d2;  // the two derivatives, in the order of the general kernels' sums
+    if (Q == 0) {         // vxy + vyx
+        column(sm, rs, HALO + c, q);
+        d1 = dyf(R + c, hc);
+        d2 = dxf(q, hc);
+        if (g.abs_type == 1 && (e.zy | e.xs)) {
+            cpml_y<true, false>(g, f, PVX_Y, e, d1);
+            cpml_x<true>(g, f, PVY_X, e, d2);
+        }
+    } else if (Q == 1) {  // vyz + vzy
+        d1 = dzf(R + HALO + c, hc);
+        d2 = dyf(R + 2 * HALO + c, hc);
+        if (g.abs_type == 1 && (e.zy | e.xs)) {
+            cpml_z<true, false>(g, f, PVY_Z, e, d1);
+            cpml_y<true, false>(g, f, PVZ_Y, e, d2);
+        }
+    } else {              // vxz + vzx
+        column(sm, rs, 2 * HALO + c, q);
+        d1 = dzf(R + c, hc);
+        d2 = dxf(q, hc);
+        if (g.abs_type == 1 && (e.zy | e.xs)) {
+            cpml_z<true, false>(g, f, PVX_Z, e, d1);
+            cpml_x<true>(g, f, PVZ_X, e, d2);
+        }
+    }
+    const float v = d1 + d2;
+    float s = C[Q * CT];
+    // elastic parameters: muipjp, mujpkp, muipkp; viscoelastic: mu?p at CP+{3,4,2}, taus?p at CP+{8,9,7}
+    if (L == 0) {
+        s += C[(CP + Q) * CT] * v;
+    } else {
+        constexpr int PM = Q == 0 ? 3 : (Q == 1 ? 4 : 2);
+        constexpr int PT = Q == 0 ? 8 : (Q == 1 ? 9 : 7);
+        const float lmu = C[(CP + PM) * CT], ltaus = C[(CP + PT) * CT];
+        const float fm = lmu * (1.0f + (float)L * ltaus);
+        const float dm = lmu * ltaus * g.inv_dt;
+        float r[L > 0 ? L : 1];
+        float a = 0;
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            r[l] = C[(6 + 6 * l + Q) * CT];
+            a += r[l];
+        }
+        const float ls = fm * v + g.dt2 * a;
+        a = 0;
+        constexpr int RQ = Q == 0 ? RXY : (Q == 1 ? RYZ : RXZ);
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            r[l] = g.eta_b[l] * (r[l] * g.eta_c[l] - g.eta[l] * (dm * v));
+            a += r[l];
+            f.r[RQ][l * g.nvol + e.iv] = r[l];
+        }
+        s += ls + g.dt2 * a;
+    }
+    if (g.abs_type == 2 && (e.zy | e.xs)) {
+        float t[1] = {s};
+        taper<1>(g, f, e, t);
+        s = t[0];
+    }
+    f.w[Q == 0 ? SXY : (Q == 1 ? SYZ : SXZ)][e.iv] = s;
+}
+
 // stress: ring vx, vy, vz; centre sxy, syz, sxz, sxx, syy, szz, r[l][xy, yz, xz, xx, yy, zz], parameters
-// role 0: normal stresses and their memory variables; role 1: shear stresses.
+// role 0: normal stresses and their memory variables; role 1: sxy and sxz;
+// role 2: syz (the shear stresses through shear<>).
 template <int L, int ROLE>
-__device__ __forceinline__ void cell_s(const Grid &g, const Fields &f, const float *const *rp, const float *C, int c,
+__device__ __forceinline__ void cell_s(const Grid &g, const Fields &f, const float *sm, const int *rs, const float *C, int c,
                                        const Cell &e, const float *hc)
 {
     constexpr int CP = 6 + 6 * L;  // first parameter stream
-    const float *R = rp[TF];       // plane x of vx, vy, vz
+    const float *R = sm + rs[TF];       // plane x of vx, vy, vz
     const float *Vx = R + c, *Vy = R + HALO + c, *Vz = R + 2 * HALO + c;
-    const bool cp = g.abs_type == 1;
+    const bool cp = g.abs_type == 1 && (e.zy | e.xs);
     float q[2 * TF + 1];
     float s[3];
     if (ROLE == 0) {
-        column(rp, c, q);
+        column(sm, rs, c, q);
         float vxx = dxb(q, hc), vyy = dyb(Vy, hc), vzz = dzb(Vz, hc);
         if (cp) {
             cpml_z<false, false>(g, f, PVZ_Z, e, vzz);
@@ -351,7 +442,7 @@ __device__ __forceinline__ void cell_s(const Grid &g, const Fields &f, const flo
             float ltaup = C[(CP + 5) * CT], ltaus = C[(CP + 6) * CT];
             float gm = lM * (1.0f + (float)L * ltaup);
             float fm = 2.0f * lmu * (1.0f + (float)L * ltaus);
-            float d = 2.0f * lmu * ltaus / g.dt, ee = lM * ltaup / g.dt;
+            float d = 2.0f * lmu * ltaus * g.inv_dt, ee = lM * ltaup * g.inv_dt;
             float r[3][L > 0 ? L : 1];
 #pragma unroll
             for (int l = 0; l < L; l++)
@@ -370,7 +461,7 @@ __device__ __forceinline__ void cell_s(const Grid &g, const Fields &f, const flo
 #pragma unroll
             for (int l = 0; l < L; l++) {
                 float el = g.eta[l];
-                float b = 1.0f / (1.0f + el * 0.5f), cc = 1.0f - el * 0.5f;
+                float b = g.eta_b[l], cc = g.eta_c[l];
                 r[0][l] = b * (r[0][l] * cc - el * (ee * vxxyyzz - d * vyyzz));
                 r[1][l] = b * (r[1][l] * cc - el * (ee * vxxyyzz - d * vxxzz));
                 r[2][l] = b * (r[2][l] * cc - el * (ee * vxxyyzz - d * vxxyy));
@@ -383,70 +474,13 @@ __device__ __forceinline__ void cell_s(const Grid &g, const Fields &f, const flo
             s[1] += lsyy + g.dt2 * a[1];
             s[2] += lszz + g.dt2 * a[2];
         }
-        if (g.abs_type == 2) taper<3>(g, f, e, s);
+        if (g.abs_type == 2 && (e.zy | e.xs)) taper<3>(g, f, e, s);
         f.w[SXX][e.iv] = s[0]; f.w[SYY][e.iv] = s[1]; f.w[SZZ][e.iv] = s[2];
+    } else if (ROLE == 1) {
+        shear<L, 0>(g, f, sm, rs, C, c, e, hc);   // sxy
+        shear<L, 2>(g, f, sm, rs, C, c, e, hc);   // sxz
     } else {
-        float qz[2 * TF + 1];
-        column(rp, HALO + c, q);       // vy
-        column(rp, 2 * HALO + c, qz);  // vz
-        float vyx = dxf(q, hc), vzx = dxf(qz, hc);
-        float vxy = dyf(Vx, hc), vxz = dzf(Vx, hc), vyz = dzf(Vy, hc), vzy = dyf(Vz, hc);
-        if (cp) {
-            cpml_z<true, false>(g, f, PVX_Z, e, vxz);
-            cpml_z<true, false>(g, f, PVY_Z, e, vyz);
-            cpml_y<true, false>(g, f, PVX_Y, e, vxy);
-            cpml_y<true, false>(g, f, PVZ_Y, e, vzy);
-            cpml_x<true>(g, f, PVY_X, e, vyx);
-            cpml_x<true>(g, f, PVZ_X, e, vzx);
-        }
-        float vxyyx = vxy + vyx, vyzzy = vyz + vzy, vxzzx = vxz + vzx;
-        s[0] = C[0 * CT]; s[1] = C[1 * CT]; s[2] = C[2 * CT];
-        if (L == 0) {
-            float fipjp = C[(CP + 0) * CT], fjpkp = C[(CP + 1) * CT], fipkp = C[(CP + 2) * CT];
-            s[0] += fipjp * vxyyx;
-            s[1] += fjpkp * vyzzy;
-            s[2] += fipkp * vxzzx;
-        } else {
-            float lmuipkp = C[(CP + 2) * CT], lmuipjp = C[(CP + 3) * CT], lmujpkp = C[(CP + 4) * CT];
-            float ltausipkp = C[(CP + 7) * CT], ltausipjp = C[(CP + 8) * CT], ltausjpkp = C[(CP + 9) * CT];
-            float fipjp = lmuipjp * (1.0f + (float)L * ltausipjp);
-            float fjpkp = lmujpkp * (1.0f + (float)L * ltausjpkp);
-            float fipkp = lmuipkp * (1.0f + (float)L * ltausipkp);
-            float dipjp = lmuipjp * ltausipjp / g.dt, djpkp = lmujpkp * ltausjpkp / g.dt,
-                  dipkp = lmuipkp * ltausipkp / g.dt;
-            float r[3][L > 0 ? L : 1];
-#pragma unroll
-            for (int l = 0; l < L; l++)
-#pragma unroll
-                for (int k = 0; k < 3; k++) r[k][l] = C[(6 + 6 * l + k) * CT];
-            float a[3] = {0, 0, 0};
-#pragma unroll
-            for (int l = 0; l < L; l++)
-#pragma unroll
-                for (int k = 0; k < 3; k++) a[k] += r[k][l];
-            float lsxy = fipjp * vxyyx + g.dt2 * a[0];
-            float lsyz = fjpkp * vyzzy + g.dt2 * a[1];
-            float lsxz = fipkp * vxzzx + g.dt2 * a[2];
-#pragma unroll
-            for (int k = 0; k < 3; k++) a[k] = 0;
-#pragma unroll
-            for (int l = 0; l < L; l++) {
-                float el = g.eta[l];
-                float b = 1.0f / (1.0f + el * 0.5f), cc = 1.0f - el * 0.5f;
-                r[0][l] = b * (r[0][l] * cc - el * (dipjp * vxyyx));
-                r[1][l] = b * (r[1][l] * cc - el * (djpkp * vyzzy));
-                r[2][l] = b * (r[2][l] * cc - el * (dipkp * vxzzx));
-#pragma unroll
-                for (int k = 0; k < 3; k++) a[k] += r[k][l];
-                const i64 ir = l * g.nvol + e.iv;
-                f.r[RXY][ir] = r[0][l]; f.r[RYZ][ir] = r[1][l]; f.r[RXZ][ir] = r[2][l];
-            }
-            s[0] += lsxy + g.dt2 * a[0];
-            s[1] += lsyz + g.dt2 * a[1];
-            s[2] += lsxz + g.dt2 * a[2];
-        }
-        if (g.abs_type == 2) taper<3>(g, f, e, s);
-        f.w[SXY][e.iv] = s[0]; f.w[SYZ][e.iv] = s[1]; f.w[SXZ][e.iv] = s[2];
+        shear<L, 1>(g, f, sm, rs, C, c, e, hc);   // syz
     }
 }
 
@@ -473,7 +507,53 @@ __device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity)
 
 // consumer warps: one per tile row and role
 template <int KIND>
-constexpr int nwc() { return TY * (KIND == 0 ? 3 : 2); }
+constexpr int nwc() { return TY * 3; }
+
+// Plane loop of one consumer warp: wait for stage k, update this thread's
+// cell of plane xs+k, release the stage.  Per-thread quantities (tile
+// offsets, slab memberships, linear index) are set up once and advanced per
+// plane.
+template <int KIND, int L, int DPF, int ROLE>
+__device__ __forceinline__ void consume(const Grid &g, const Fields &f, const float *sm, int xs, int nst, int z0,
+                                        int y0, int tz, int ty, uint64_t *full, uint64_t *empty)
+{
+    constexpr int NVR = 2 * TF + 1 + DPF, NCR = DPF + 1;
+    constexpr int NCF = KIND == 0 ? 6 : 6 + 6 * L + (L > 0 ? 10 : 5);
+    constexpr int NPL = KIND == 0 ? 3 : 0;
+    constexpr int PRING = NVR * 3 * HALO;              // offsets (floats) of the slot arrays in sm
+    constexpr int CRING = PRING + NCR * NPL * HALO;
+    const int lane = tz;
+    const int gz = z0 + tz, gy = y0 + ty;
+    const bool active = gz <= g.NZ - TF - 1 && gy <= g.NY - TF - 1;
+    const int c = (ty + TF) * HZ + tz + TF;           // this thread's centre in a haloed tile
+    const int cc = ty * TZ + tz;                      // and in a centre tile
+    const float *hc = g.hc;
+    const i64 plane = (i64)g.NY * g.NZ;
+    Cell e;
+    e.gz = gz;
+    e.gy = gy;
+    e.zy = zy_slabs(g, gz, gy);
+    e.iv = ((i64)xs * g.NY + gy) * g.NZ + gz;
+    int s0 = (xs - TF) % NVR;                         // ring slot of plane x - F
+    for (int k = 0; k < nst; k++) {
+        const int sl = k % NCR;
+        if (!warp_wait(&full[sl], (k / NCR) & 1)) return;
+        e.x = xs + k;
+        e.xs = x_slabs(g, e.x);
+        if (active) {
+            int rs[2 * TF + 1];
+#pragma unroll
+            for (int m = 0; m <= 2 * TF; m++) rs[m] = (s0 + m < NVR ? s0 + m : s0 + m - NVR) * 3 * HALO;
+            const float *C = sm + CRING + sl * NCF * CT + cc;
+            if (KIND == 0) cell_v<ROLE>(g, f, sm, rs, sm + PRING + sl * NPL * HALO, C, c, e, hc);
+            else cell_s<L, ROLE>(g, f, sm, rs, C, c, e, hc);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[sl]);
+        e.iv += plane;
+        s0 = s0 + 1 == NVR ? 0 : s0 + 1;
+    }
+}
 
 // KIND 0: velocity update, KIND 1: stress update with L mechanisms.
 // Warp NWC is the producer: it issues the TMA copies of stage j once every
@@ -561,39 +641,16 @@ __global__ void __launch_bounds__(32 * (nwc<KIND>() + 1), 1) k_tma(const __grid_
         return;
     }
     const int tz = lane, ty = warp % TY, role = warp / TY;
-    const int gz = z0 + tz, gy = y0 + ty;
-    const bool active = gz <= g.NZ - TF - 1 && gy <= g.NY - TF - 1;
-    const int c = (ty + TF) * HZ + tz + TF;   // this thread's centre in a haloed tile
-    const float *hc = g.hc;
     if (!warp_wait(pro, 0)) return;
-    for (int k = 0; k < nst; k++) {
-        const int sl = k % NCR;
-        if (!warp_wait(&full[sl], (k / NCR) & 1)) return;
-        const int x = xs + k;
-        if (active) {
-            const float *rp[2 * TF + 1];
-            int s = (x - TF) % NVR;
-#pragma unroll
-            for (int m = 0; m <= 2 * TF; m++) {
-                rp[m] = vring + s * 3 * HALO;
-                s = s + 1 == NVR ? 0 : s + 1;
-            }
-            const float *C = cring + sl * NCF * CT + ty * TZ + tz;
-            Cell e;
-            e.x = x; e.gz = gz; e.gy = gy;
-            e.iv = ((i64)x * g.NY + gy) * g.NZ + gz;
-            if (KIND == 0) {
-                const float *P = pring + sl * NPL * HALO;
-                if (role == 0) cell_v<0>(g, f, rp, P, C, c, e, hc);
-                else if (role == 1) cell_v<1>(g, f, rp, P, C, c, e, hc);
-                else cell_v<2>(g, f, rp, P, C, c, e, hc);
-            } else {
-                if (role == 0) cell_s<L, 0>(g, f, rp, C, c, e, hc);
-                else cell_s<L, 1>(g, f, rp, C, c, e, hc);
-            }
-        }
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[sl]);
+    // one specialised plane loop per role (the role is uniform over a warp)
+    if (KIND == 0) {
+        if (role == 0) consume<KIND, L, DPF, 0>(g, f, sm, xs, nst, z0, y0, tz, ty, full, empty);
+        else if (role == 1) consume<KIND, L, DPF, 1>(g, f, sm, xs, nst, z0, y0, tz, ty, full, empty);
+        else consume<KIND, L, DPF, 2>(g, f, sm, xs, nst, z0, y0, tz, ty, full, empty);
+    } else {
+        if (role == 0) consume<KIND, L, DPF, 0>(g, f, sm, xs, nst, z0, y0, tz, ty, full, empty);
+        else if (role == 1) consume<KIND, L, DPF, 1>(g, f, sm, xs, nst, z0, y0, tz, ty, full, empty);
+        else consume<KIND, L, DPF, 2>(g, f, sm, xs, nst, z0, y0, tz, ty, full, empty);
     }
 }
 
@@ -663,7 +720,8 @@ std::vector<CacheEntry> g_cache;
 
 bool eligible(const Grid &g)
 {
-    return g.nd == 3 && g.F == TF && g.kernels == 0 && g.nz % 4 == 0 && g.NZ % 4 == 0 && g.L >= 0 && g.L <= 3;
+    return g.nd == 3 && g.F == TF && (g.kernels == 0 || g.kernels == 3) && g.nz % 4 == 0 && g.NZ % 4 == 0 &&
+           g.L >= 0 && g.L <= 3;
 }
 
 bool build_maps(const Grid &g, const Fields &f, CacheEntry &e)

@@ -131,7 +131,7 @@ class Config:
     param_type: int = 0
     restype: int = 0
     precision: str = "fp32"
-    kernels: str = "fast"  # "fast": TMA-pipelined 3D kernels where eligible; "general"; "register"
+    kernels: str = "fast"  # "fast" (TMA stress + general velocity in 3D), "general", "register", "tma"
     adjoint_reset_psi: bool = False  # True: the adjoint starts from zeroed CPML memory (not the reference's)
 
     def to_c(self) -> sfd_config:
@@ -163,7 +163,7 @@ class Config:
         c.param_type = int(self.param_type)
         c.restype = int(self.restype)
         c.precision = PREC[self.precision]
-        c.kernels = {"fast": 0, "general": 1, "register": 2}[self.kernels]
+        c.kernels = {"fast": 0, "general": 1, "register": 2, "tma": 3}[self.kernels]
         c.adjoint_reset_psi = 1 if self.adjoint_reset_psi else 0
         return c
 
@@ -295,7 +295,7 @@ class Plan:
 
     @property
     def uses_tma(self) -> bool:
-        """True when the 3D updates of this plan run on the TMA-pipelined kernels."""
+        """True when the 3D stress update of this plan runs on the TMA-pipelined kernels."""
         rc = int(self.lib.sfd_plan_uses_tma(self.h))
         if rc < 0:
             self._check(rc)

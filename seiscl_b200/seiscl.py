@@ -503,6 +503,9 @@ class SeisCL:
         N = [int(v) for v in np.atleast_1d(self.N)]
         if self.back_prop_type != 1 and self.gradout:
             raise SeisCLError("Error: only back_prop_type=1 (boundary-saving backpropagation) is supported")
+        for flag in ("Hout", "gradsrcout", "movout"):
+            if getattr(self, flag):
+                raise SeisCLError("Error: %s is not provided by this engine" % flag)
         return engine.Config(
             N=N, ND=int(self.ND), dh=float(self.dh), dt=float(self.dt), NT=int(self.NT), L=int(self.L),
             f0=float(self.f0), FL=tuple(np.atleast_1d(self.FL).astype(float)), FDORDER=int(self.FDORDER),

@@ -15,6 +15,10 @@ import pytest
 from tests._cases import engine_config, make_case, rel_l2
 
 FWD_TOL = 2e-5
+# TMA kernels vs general kernels: same operation order except that the TMA
+# kernels multiply by FP32 reciprocals of dt, 1 + eta/2 and the CPML K where
+# the general kernels divide (a last-bit difference per coefficient)
+FAST_TOL = 5e-6
 GRAD_TOL = 2e-4
 
 FORWARD_CASES = [
@@ -148,11 +152,11 @@ def test_fast_3d_kernels_match_general(kw, cuda_device):
     cfg, model, acq = make_case(**kw)
     outs = _outputs(3)
     res = {}
-    for variant in ("fast", "register", "general"):
+    for variant in ("fast", "tma", "register", "general"):
         ec = dataclasses.replace(engine_config(cfg), kernels=variant)
         plan = Plan(ec)
         plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
-        if variant == "fast":
+        if variant in ("fast", "tma"):
             eligible = kw.get("fdorder", 8) == 8 and kw["nz"] % 4 == 0
             assert plan.uses_tma == eligible
         else:
@@ -162,9 +166,9 @@ def test_fast_3d_kernels_match_general(kw, cuda_device):
     ora.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
     ref = ora.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
     for n in outs:
-        for v in ("fast", "register"):
-            assert rel_l2(res[v][n], res["general"][n]) < 1e-6, (v, n)
-            assert rel_l2(res[v][n], ref[n]) < FWD_TOL, (v, n)
+        for v in ("fast", "tma", "register"):
+            e_gen, e_ref = rel_l2(res[v][n], res["general"][n]), rel_l2(res[v][n], ref[n])
+            assert e_gen < FAST_TOL and e_ref < FWD_TOL, (v, n, e_gen, e_ref)
 
 
 OTHER_PHYSICS = [
