@@ -347,6 +347,8 @@ def main():
     v_gbs = ab["v"] / (kv / 1e3) / 1e9
     step_ms = loop_ms / args.steps / w["nt"]
     fused_gbs = ab["fused"] / (step_ms / 1e3) / 1e9
+    skern = ("stress update, TMA-pipelined (k_tma<1,%d,*>)" % w["L"]) if plan.uses_tma else \
+        ("stress update, general (k_s%dd)" % (3 if w["nd"] == 3 else 2))
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic_%s.json" % args.workload)
     if os.path.exists(tpath):
@@ -378,7 +380,7 @@ def main():
                    "l2": "inputs larger than L2 (%.2f GB of fields)" % (cells * 4 * (9 + 6 * w["L"]) / 1e9)},
         "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
-        "roofline": {"bound": "hbm", "kernel": "stress update (k_s3d)", "achieved": round(s_gbs, 1),
+        "roofline": {"bound": "hbm", "kernel": skern, "achieved": round(s_gbs, 1),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(s_gbs / peak, 4),
                      "traffic": traffic, "bytes_per_cell": round(ab["s"] / cells, 2),
                      "velocity_kernel_gbs": round(v_gbs, 1), "kernel_ms": [round(kv, 4), round(ks, 4),
