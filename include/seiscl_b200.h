@@ -73,11 +73,13 @@ typedef struct sfd_config {
     int param_type;    /* 0: vp,vs,rho  1: M,mu,rho  2: Ip,Is,rho */
     int restype;       /* 0: L2 (full gradient), 1: M only */
     int precision;     /* SFD_PREC_*: storage of the saved boundaries */
-    int kernels;       /* 0: fastest measured: TMA-pipelined 3D stress update where
-                             eligible, general velocity update,
+    int kernels;       /* 0: fastest measured: in 3D the streaming velocity update and
+                             the TMA-pipelined stress update where eligible (else the
+                             streaming one); general kernels in 2D,
                           1: general one-thread-per-cell kernels only,
                           2: register-blocked 3D kernels where available,
-                          3: TMA-pipelined 3D velocity and stress updates */
+                          3: TMA-pipelined 3D velocity and stress updates,
+                          4: streaming one-thread-per-cell 3D kernels (per-cell loads first) */
     int adjoint_reset_psi; /* 0: the adjoint continues with the forward run's CPML memory
                               (reference behaviour, src/clprogram.c:806-811); 1: it starts
                               from zeroed CPML memory.  With sources whose wave field is

@@ -305,7 +305,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     // N[0] must be even (read_hdf5.c:535-540)
     if (c.n[0] % 2) return SFD_ERR_ARG;
     if (c.precision < 0 || c.precision > 2) return SFD_ERR_ARG;
-    if (c.kernels < 0 || c.kernels > 3) return SFD_ERR_ARG;
+    if (c.kernels < 0 || c.kernels > 4) return SFD_ERR_ARG;
     if (c.adjoint_reset_psi < 0 || c.adjoint_reset_psi > 1) return SFD_ERR_ARG;
 
     sfd_plan *p = new sfd_plan();

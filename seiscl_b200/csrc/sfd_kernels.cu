@@ -601,6 +601,137 @@ __global__ void __launch_bounds__(256) k_s3d(Grid g, Fields f)
     }
 }
 
+// ----------------------------------------------------- streaming 3D kernels
+// Same arithmetic as k_v3d / k_s3d, one thread per cell, but every per-cell
+// stream (the updated fields, memory variables and parameters) is loaded
+// into registers before the stencil work starts, so each thread has all of
+// its independent DRAM loads in flight at once; the updated values are
+// stored once at the end (taper applied in registers, in the reference's
+// factor order).  L is a template parameter so the memory variables stay in
+// registers.  The stencil taps go through the read-only cache as in the
+// general kernels.
+template <int NF>
+__device__ __forceinline__ void taper_regs(const Grid &g, const float *taper, int gz, int gy, int gx, float (&v)[NF])
+{
+    const int F = g.F, NAB = g.nab;
+    auto mul = [&](float t) {
+#pragma unroll
+        for (int q = 0; q < NF; q++) v[q] *= t;
+    };
+    if (!g.freesurf && gz - F < NAB) mul(__ldg(taper + gz - F));
+    if (gz > g.NZ - NAB - F - 1) mul(__ldg(taper + g.NZ - F - gz - 1));
+    if (gy - F < NAB) mul(__ldg(taper + gy - F));
+    if (gy > g.NY - NAB - F - 1) mul(__ldg(taper + g.NY - F - gy - 1));
+    if (gx - F < NAB) mul(__ldg(taper + gx - F));
+    if (gx > g.NX - NAB - F - 1) mul(__ldg(taper + g.NX - F - gx - 1));
+}
+
+template <int F>
+__global__ void __launch_bounds__(256, 3) k_v3d_stream(Grid g, Fields f)
+{
+    CELL3D
+    const float *hc = g.hc;
+    float v[3] = {__ldg(f.w[VX] + iv), __ldg(f.w[VY] + iv), __ldg(f.w[VZ] + iv)};
+    const float rip = __ldg(f.p[PRIP] + ip), rjp = __ldg(f.p[PRJP] + ip), rkp = __ldg(f.p[PRKP] + ip);
+    float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc);
+    float sxx_x = dfw<F>(f.w[SXX], iv, sx, hc);
+    float sxz_x = dbw<F>(f.w[SXZ], iv, sx, hc);
+    float sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
+    float syz_y = dbw<F>(f.w[SYZ], iv, sy, hc);
+    float syz_z = dbw<F>(f.w[SYZ], iv, 1, hc);
+    float syy_y = dfw<F>(f.w[SYY], iv, sy, hc);
+    float sxy_x = dbw<F>(f.w[SXY], iv, sx, hc);
+    float sxy_y = dbw<F>(f.w[SXY], iv, sy, hc);
+    if (g.abs_type == 1) cpml_v3d(g, f, gz, gy, gx, sxx_x, syy_y, szz_z, sxy_y, sxy_x, syz_y, syz_z, sxz_x, sxz_z);
+    v[0] += (sxx_x + sxy_y + sxz_z) * rip;
+    v[1] += (syy_y + sxy_x + syz_z) * rjp;
+    v[2] += (szz_z + sxz_x + syz_y) * rkp;
+    if (g.abs_type == 2) taper_regs<3>(g, f.taper, gz, gy, gx, v);
+    f.w[VX][iv] = v[0];
+    f.w[VY][iv] = v[1];
+    f.w[VZ][iv] = v[2];
+}
+
+template <int F, int L>
+__global__ void __launch_bounds__(256, 2) k_s3d_stream(Grid g, Fields f)
+{
+    CELL3D
+    const float *hc = g.hc;
+    // per-cell streams first: stresses, memory variables, parameters
+    float s[6] = {__ldg(f.w[SXY] + iv), __ldg(f.w[SYZ] + iv), __ldg(f.w[SXZ] + iv),
+                  __ldg(f.w[SXX] + iv), __ldg(f.w[SYY] + iv), __ldg(f.w[SZZ] + iv)};
+    float r[6][L > 0 ? L : 1];
+#pragma unroll
+    for (int l = 0; l < L; l++) {
+        const i64 ir = l * g.nvol + iv;
+        r[0][l] = __ldg(f.r[RXY] + ir); r[1][l] = __ldg(f.r[RYZ] + ir); r[2][l] = __ldg(f.r[RXZ] + ir);
+        r[3][l] = __ldg(f.r[RXX] + ir); r[4][l] = __ldg(f.r[RYY] + ir); r[5][l] = __ldg(f.r[RZZ] + ir);
+    }
+    const float lM = __ldg(f.p[PM] + ip), lmu = __ldg(f.p[PMU] + ip);
+    const float lmuipkp = __ldg(f.p[PMUIPKP] + ip), lmuipjp = __ldg(f.p[PMUIPJP] + ip),
+                lmujpkp = __ldg(f.p[PMUJPKP] + ip);
+    float ltaup = 0, ltaus = 0, ltausipkp = 0, ltausipjp = 0, ltausjpkp = 0;
+    if (L > 0) {
+        ltaup = __ldg(f.p[PTAUP] + ip); ltaus = __ldg(f.p[PTAUS] + ip);
+        ltausipkp = __ldg(f.p[PTAUSIPKP] + ip); ltausipjp = __ldg(f.p[PTAUSIPJP] + ip);
+        ltausjpkp = __ldg(f.p[PTAUSJPKP] + ip);
+    }
+    float vzx = dfw<F>(f.w[VZ], iv, sx, hc), vzy = dfw<F>(f.w[VZ], iv, sy, hc), vzz = dbw<F>(f.w[VZ], iv, 1, hc);
+    float vyx = dfw<F>(f.w[VY], iv, sx, hc), vyy = dbw<F>(f.w[VY], iv, sy, hc), vyz = dfw<F>(f.w[VY], iv, 1, hc);
+    float vxx = dbw<F>(f.w[VX], iv, sx, hc), vxy = dfw<F>(f.w[VX], iv, sy, hc), vxz = dfw<F>(f.w[VX], iv, 1, hc);
+    if (g.abs_type == 1) cpml_s3d(g, f, gz, gy, gx, vxx, vxy, vxz, vyx, vyy, vyz, vzx, vzy, vzz, false);
+    float vxyyx = vxy + vyx, vyzzy = vyz + vzy, vxzzx = vxz + vzx;
+    float vxxyyzz = vxx + vyy + vzz, vyyzz = vyy + vzz, vxxzz = vxx + vzz, vxxyy = vxx + vyy;
+    if (L == 0) {
+        float gm = lM, fm = 2.0f * lmu;
+        s[0] += lmuipjp * vxyyx;
+        s[1] += lmujpkp * vyzzy;
+        s[2] += lmuipkp * vxzzx;
+        s[3] += gm * vxxyyzz - fm * vyyzz;
+        s[4] += gm * vxxyyzz - fm * vxxzz;
+        s[5] += gm * vxxyyzz - fm * vxxyy;
+    } else {
+        float fipjp = lmuipjp * (1.0f + (float)L * ltausipjp);
+        float fjpkp = lmujpkp * (1.0f + (float)L * ltausjpkp);
+        float fipkp = lmuipkp * (1.0f + (float)L * ltausipkp);
+        float gm = lM * (1.0f + (float)L * ltaup);
+        float fm = 2.0f * lmu * (1.0f + (float)L * ltaus);
+        float dipjp = lmuipjp * ltausipjp / g.dt, djpkp = lmujpkp * ltausjpkp / g.dt, dipkp = lmuipkp * ltausipkp / g.dt;
+        float d = 2.0f * lmu * ltaus / g.dt, e = lM * ltaup / g.dt;
+        float a[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int l = 0; l < L; l++)
+#pragma unroll
+            for (int q = 0; q < 6; q++) a[q] += r[q][l];
+        float ls[6] = {fipjp * vxyyx + g.dt2 * a[0], fjpkp * vyzzy + g.dt2 * a[1], fipkp * vxzzx + g.dt2 * a[2],
+                       (gm * vxxyyzz - fm * vyyzz) + g.dt2 * a[3], (gm * vxxyyzz - fm * vxxzz) + g.dt2 * a[4],
+                       (gm * vxxyyzz - fm * vxxyy) + g.dt2 * a[5]};
+#pragma unroll
+        for (int q = 0; q < 6; q++) a[q] = 0;
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            float el = g.eta[l];
+            float b = 1.0f / (1.0f + el * 0.5f), c = 1.0f - el * 0.5f;
+            r[0][l] = b * (r[0][l] * c - el * (dipjp * vxyyx));
+            r[1][l] = b * (r[1][l] * c - el * (djpkp * vyzzy));
+            r[2][l] = b * (r[2][l] * c - el * (dipkp * vxzzx));
+            r[3][l] = b * (r[3][l] * c - el * (e * vxxyyzz - d * vyyzz));
+            r[4][l] = b * (r[4][l] * c - el * (e * vxxyyzz - d * vxxzz));
+            r[5][l] = b * (r[5][l] * c - el * (e * vxxyyzz - d * vxxyy));
+#pragma unroll
+            for (int q = 0; q < 6; q++) a[q] += r[q][l];
+            const i64 ir = l * g.nvol + iv;
+            f.r[RXY][ir] = r[0][l]; f.r[RYZ][ir] = r[1][l]; f.r[RXZ][ir] = r[2][l];
+            f.r[RXX][ir] = r[3][l]; f.r[RYY][ir] = r[4][l]; f.r[RZZ][ir] = r[5][l];
+        }
+#pragma unroll
+        for (int q = 0; q < 6; q++) s[q] += ls[q] + g.dt2 * a[q];
+    }
+    if (g.abs_type == 2) taper_regs<6>(g, f.taper, gz, gy, gx, s);
+    f.w[SXY][iv] = s[0]; f.w[SYZ][iv] = s[1]; f.w[SXZ][iv] = s[2];
+    f.w[SXX][iv] = s[3]; f.w[SYY][iv] = s[4]; f.w[SZZ][iv] = s[5];
+}
+
 // free surface 3D, one thread per (y, x) column (surface3D.cl:39-271)
 template <int F>
 __global__ void k_surf3d(Grid g, Fields f, int pdir)
@@ -1371,8 +1502,8 @@ static inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b)
 
 void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
 {
-    // kernels 0: the general velocity kernel measures faster than the TMA one
-    // at 256^3 (0.58 vs 0.63 ms), so only kernels 3 takes the TMA path here
+    // kernels 0 takes the streaming velocity kernel (0.52 ms at 256^3, against
+    // 0.58 general and 0.63 TMA); only kernels 3 takes the TMA path here
     if (g.kernels == 3 && launch_update_v_tma(g, f, st)) return;
     if (g.kernels == 2 && launch_update_v_fast(g, f, st)) return;
     if (g.nd == 21 || g.nd == 22) {
@@ -1383,6 +1514,10 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
     }
     if (g.nd == 3) {
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
+        if (g.kernels == 0 || g.kernels == 4) {
+            DISPATCH_F(g.F, k_v3d_stream<FF><<<gr, b, 0, st>>>(g, f));
+            return;
+        }
         DISPATCH_F(g.F, k_v3d<FF><<<gr, b, 0, st>>>(g, f));
     } else {
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
@@ -1402,6 +1537,15 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
     }
     if (g.nd == 3) {
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
+        if ((g.kernels == 0 || g.kernels == 4) && g.L <= 3) {
+            switch (g.L) {
+            case 0: DISPATCH_F(g.F, k_s3d_stream<FF, 0><<<gr, b, 0, st>>>(g, f)); break;
+            case 1: DISPATCH_F(g.F, k_s3d_stream<FF, 1><<<gr, b, 0, st>>>(g, f)); break;
+            case 2: DISPATCH_F(g.F, k_s3d_stream<FF, 2><<<gr, b, 0, st>>>(g, f)); break;
+            default: DISPATCH_F(g.F, k_s3d_stream<FF, 3><<<gr, b, 0, st>>>(g, f)); break;
+            }
+            return;
+        }
         DISPATCH_F(g.F, k_s3d<FF><<<gr, b, 0, st>>>(g, f));
     } else {
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));

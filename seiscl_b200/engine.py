@@ -131,7 +131,8 @@ class Config:
     param_type: int = 0
     restype: int = 0
     precision: str = "fp32"
-    kernels: str = "fast"  # "fast" (TMA stress + general velocity in 3D), "general", "register", "tma"
+    kernels: str = "fast"  # "fast" (3D: streaming velocity, TMA or streaming stress), "general", "register",
+    #                        "tma", "stream"
     adjoint_reset_psi: bool = False  # True: the adjoint starts from zeroed CPML memory (not the reference's)
 
     def to_c(self) -> sfd_config:
@@ -163,7 +164,7 @@ class Config:
         c.param_type = int(self.param_type)
         c.restype = int(self.restype)
         c.precision = PREC[self.precision]
-        c.kernels = {"fast": 0, "general": 1, "register": 2, "tma": 3}[self.kernels]
+        c.kernels = {"fast": 0, "general": 1, "register": 2, "tma": 3, "stream": 4}[self.kernels]
         c.adjoint_reset_psi = 1 if self.adjoint_reset_psi else 0
         return c
 

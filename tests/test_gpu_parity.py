@@ -152,7 +152,7 @@ def test_fast_3d_kernels_match_general(kw, cuda_device):
     cfg, model, acq = make_case(**kw)
     outs = _outputs(3)
     res = {}
-    for variant in ("fast", "tma", "register", "general"):
+    for variant in ("fast", "tma", "stream", "register", "general"):
         ec = dataclasses.replace(engine_config(cfg), kernels=variant)
         plan = Plan(ec)
         plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
@@ -166,7 +166,7 @@ def test_fast_3d_kernels_match_general(kw, cuda_device):
     ora.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
     ref = ora.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
     for n in outs:
-        for v in ("fast", "tma", "register"):
+        for v in ("fast", "tma", "stream", "register"):
             e_gen, e_ref = rel_l2(res[v][n], res["general"][n]), rel_l2(res[v][n], ref[n])
             assert e_gen < FAST_TOL and e_ref < FWD_TOL, (v, n, e_gen, e_ref)
 
