@@ -40,6 +40,84 @@ WORKLOADS = {
 }
 
 
+# Gradient workloads (one "step" = one shot: forward with saved boundaries,
+# L2 residual against observed data, res_scale, adjoint, gradient accumulation)
+GRADIENT_WORKLOADS = {
+    # 2D acoustic FWI gradient, run as 2D P-SV with vs = 0 (the reference's acoustic
+    # kernels have no adjoint): 300 x 1000, 4th order, 32 shots, 500 receivers
+    "fwi2d": dict(nd=2, nz=300, ny=1, nx=1000, nt=3000, dh=10.0, dt=1e-3, L=0, fdorder=4, nab=20, freesurf=0,
+                  f0=8.0, src_type=100, src_f=8.0, precision="fp32", nshots=32, outputs=["p"]),
+    # 3D elastic FWI gradient: 200 x 400 x 400, 8th order, saved boundaries in BF16
+    # (91.8 GB; FP32 would need 183.5 GB), 16 force shots, 100 x 100 receivers
+    "fwi3d": dict(nd=3, nz=200, ny=400, nx=400, nt=2500, dh=12.5, dt=1e-3, L=0, fdorder=8, nab=20, freesurf=1,
+                  f0=12.0, src_type=2, src_f=12.0, precision="bf16", nshots=16, outputs=["vx", "vy", "vz"]),
+}
+
+
+def build_gradient_workload(name, nshots):
+    """Seeded true and starting models and the first ``nshots`` shots."""
+    from scipy.ndimage import gaussian_filter
+
+    w = dict(GRADIENT_WORKLOADS[name])
+    w["fl"] = [w["f0"]]
+    nd, nz, ny, nx, dh = w["nd"], w["nz"], w["ny"], w["nx"], w["dh"]
+    z = np.arange(nz, dtype=np.float64)
+    if nd == 2:
+        vp = np.broadcast_to(1500.0 + 2500.0 * z / (nz - 1), (nx, nz)).copy()
+        rng = np.random.default_rng(301)
+        xx, zz = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+        for sgn in (1.0, -1.0):
+            cx, cz = rng.uniform(0.25 * nx, 0.75 * nx), rng.uniform(0.3 * nz, 0.7 * nz)
+            vp *= 1.0 + 0.1 * sgn * np.exp(-((xx - cx) ** 2 + (zz - cz) ** 2) / (2 * 20.0 ** 2))
+        vs = np.zeros_like(vp)
+        xs = np.linspace(w["nab"] + 5, nx - w["nab"] - 5, w["nshots"])
+        gx = np.linspace(w["nab"], nx - w["nab"] - 1, 500).astype(int)
+        shots = []
+        for i in range(nshots):
+            sp = np.array([[xs[i] * dh, 0, 5 * dh, i, w["src_type"]]], np.float32)
+            rp = np.zeros((len(gx), 8), np.float32)
+            rp[:, 0] = gx * dh
+            rp[:, 2] = 5 * dh
+            rp[:, 3] = i
+            rp[:, 4] = np.arange(1, len(gx) + 1)
+            shots.append((sp, ricker(w["src_f"], w["nt"], w["dt"])[None, :], rp))
+    else:
+        depths = np.sort(np.random.default_rng(401).choice(np.arange(10, nz - 10), 5, replace=False))
+        vps = np.sort(np.random.default_rng(401).uniform(1800.0, 4500.0, 6))
+        vp1 = np.empty(nz)
+        edges = [0] + list(depths) + [nz]
+        for l in range(6):
+            vp1[edges[l]:edges[l + 1]] = vps[l]
+        vp = np.broadcast_to(vp1, (nx, ny, nz)).copy()
+        rng = np.random.default_rng(402)
+        xx, yy, zz = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij", sparse=True)
+        for k in range(3):
+            c = rng.uniform(0.3, 0.7, 3) * np.array([nx, ny, nz])
+            vp *= 1.0 + 0.08 * (1 if k % 2 == 0 else -1) * np.exp(
+                -((xx - c[0]) ** 2 + (yy - c[1]) ** 2 + (zz - c[2]) ** 2) / (2 * 15.0 ** 2))
+        vs = vp / 1.8
+        g = np.arange(100) * 4 + (nx - 400) // 2 + 2
+        gxx, gyy = np.meshgrid(g, g, indexing="ij")
+        shots = []
+        for i in range(nshots):
+            cx, cy = (2 * (i % 4) + 1) / 8.0 * nx, (2 * (i // 4) + 1) / 8.0 * ny
+            sp = np.array([[cx * dh, cy * dh, 5 * dh, i, w["src_type"]]], np.float32)
+            rp = np.zeros((gxx.size, 8), np.float32)
+            rp[:, 0] = gxx.ravel() * dh
+            rp[:, 1] = gyy.ravel() * dh
+            rp[:, 2] = 5 * dh
+            rp[:, 3] = i
+            rp[:, 4] = np.arange(1, gxx.size + 1)
+            shots.append((sp, ricker(w["src_f"], w["nt"], w["dt"])[None, :], rp))
+    rho = 310.0 * vp ** 0.25
+    true = {k: np.ascontiguousarray(v, dtype=np.float32) for k, v in (("vp", vp), ("vs", vs), ("rho", rho))}
+    sig = 15.0 if nd == 2 else 8.0
+    start = {k: np.ascontiguousarray(gaussian_filter(v, sig), dtype=np.float32) for k, v in true.items()}
+    if nd == 2:
+        start["vs"][:] = 0.0
+    return w, true, start, shots
+
+
 def ricker(f0, nt, dt):
     t = np.linspace(-1.5 / f0, (nt - 1) * dt - 1.5 / f0, num=int(nt))
     return ((1.0 - 2.0 * (np.pi ** 2) * (f0 ** 2) * (t ** 2)) * np.exp(-(np.pi ** 2) * (f0 ** 2) * (t ** 2))).astype(
@@ -139,7 +217,7 @@ def build_workload_light(name):
     return w, None, None
 
 
-def algorithmic_bytes(w):
+def algorithmic_bytes(w, state_bytes=4):
     """Minimum DRAM bytes of one time step of the two stencil kernels (FP32).
 
     Velocity kernel: read 6 stresses, read+write 3 velocities, read 3
@@ -164,9 +242,10 @@ def algorithmic_bytes(w):
         psi_cells_axis = 2 * nab * nz + nx * zlayers
         psi_v = 2 * psi_cells_axis
         psi_s = 2 * psi_cells_axis
-    v_bytes = n * 4 * (ns + 2 * nv + nv) + 8 * psi_v
-    s_bytes = n * 4 * (nv + 2 * ns + 2 * ns * L + npar_s) + 8 * psi_s
-    fused = n * 4 * (2 * (nv + ns + ns * L) + nv + npar_s) + 8 * (psi_v + psi_s)
+    sb = state_bytes  # bytes per stored wave-field / memory-variable value; parameters and psi stay FP32
+    v_bytes = n * (sb * (ns + 2 * nv) + 4 * nv) + 8 * psi_v
+    s_bytes = n * (sb * (nv + 2 * ns + 2 * ns * L) + 4 * npar_s) + 8 * psi_s
+    fused = n * (sb * 2 * (nv + ns + ns * L) + 4 * (nv + npar_s)) + 8 * (psi_v + psi_s)
     return dict(v=v_bytes, s=s_bytes, fused=fused, cells=n)
 
 
@@ -276,19 +355,175 @@ def run_reference_arm(args, w, model, acq):
     print(json.dumps(line))
 
 
+def run_gradient(args):
+    """Gradient workloads: per step one shot of forward (saving boundaries),
+    L2 residual against observed data, res_scale and adjoint.  Metric counts
+    both sweeps: cells * NT * 2 per shot."""
+    import dataclasses
+
+    import torch
+
+    from seiscl_b200.engine import Plan
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if world > 1:
+        raise SystemExit("gradient workloads run on one GPU per process without torchrun")
+    nuse = args.warmup + args.steps
+    w, true, start, shots = build_gradient_workload(args.workload, nuse)
+    if args.nt > 0:
+        w["nt"] = args.nt
+        shots = [(sp, src[:, :args.nt].copy(), rp) for sp, src, rp in shots]
+    outs = w["outputs"]
+    cfg = dataclasses.replace(engine_config(w), precision=w["precision"])
+    plan = Plan(cfg)
+    plan.set_model(true["vp"], true["vs"], true["rho"])
+    obs = [plan.forward(sp, src, rp, outs) for sp, src, rp in shots]   # observed data, untimed
+    plan.set_model(start["vp"], start["vs"], start["rho"])
+    plan.zero_gradient()
+
+    def one(i):
+        sp, src, rp = shots[i]
+        d = plan.forward(sp, src, rp, outs, save_boundaries=True)
+        ms = plan.last_loop_ms
+        res = {k: d[k] - obs[i][k] for k in outs}
+        plan.adjoint(sp, src, rp, plan.residual_scale(rp, res))
+        return ms + plan.last_loop_ms
+
+    for i in range(args.warmup):
+        one(i)
+    torch.cuda.synchronize()
+    clk = ClockSampler(os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
+                                    else "/tmp", "clocks_bench_r%d.csv" % rank))
+    loop_ms = 0.0
+    with clk:
+        t0 = time.perf_counter()
+        for i in range(args.warmup, nuse):
+            loop_ms += one(i)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    g = plan.gradient(transform=True)
+    cells = w["nz"] * w["ny"] * w["nx"]
+    updates = cells * w["nt"] * 2 * args.steps
+    rec = shots[0][2].shape[0]
+    print(json.dumps({
+        "metric": "Gcell-updates/s", "value": round(updates / (loop_ms / 1e3) / 1e9, 3), "unit": "Gcell-updates/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(loop_ms / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": [w["nz"], w["ny"], w["nx"]], "nt": w["nt"],
+                   "fdorder": w["fdorder"], "boundaries": w["precision"], "outputs": outs,
+                   "step": "one shot: forward + residual + res_scale + adjoint (2 sweeps counted)"},
+        "e2e": {"value": round(updates / wall / 1e9, 3), "unit": "Gcell-updates/s",
+                "h2d_bytes_per_step": int(sum(a.nbytes for a in shots[0]) + len(outs) * rec * w["nt"] * 4),
+                "d2h_bytes_per_step": int(len(outs) * rec * w["nt"] * 4)},
+        "gradient_finite": bool(all(np.isfinite(v).all() for k, v in g.items() if k in ("vp", "rho"))),
+        "gpu_launches": None,
+        "clocks": clk.summary(0),
+    }))
+
+
+def run_serving(args):
+    """Service mix: Poisson arrivals of forward (70 %) and gradient (30 %)
+    requests with random 2D and small 3D grids, orders 4/8, elastic or
+    viscoelastic, on a pool of workers sharing one GPU.  Reports requests
+    and shots per second and latency percentiles."""
+    import dataclasses
+
+    import torch
+
+    from seiscl_b200 import serving
+    from seiscl_b200.engine import Config
+    from seiscl_b200.qfit import band_frequencies, q_to_tau
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rng = np.random.default_rng(501)
+    nreq = max(args.steps, 1)
+    reqs, arrivals = [], np.cumsum(rng.exponential(1.0 / args.rate, nreq))
+    for i in range(nreq):
+        three = rng.uniform() < 0.2
+        L = int(rng.integers(0, 3))
+        order = int(rng.choice([4, 8]))
+        nt = int(rng.integers(500, 1500))
+        f0 = float(rng.uniform(5, 20))
+        if three:
+            n = int(rng.integers(64, 129)) // 2 * 2
+            N, shape = [n, n, n], (n, n, n)
+        else:
+            nz, nx = int(rng.integers(100, 400)) // 2 * 2, int(rng.integers(200, 1000))
+            N, shape = [nz, nx], (nx, nz)
+        fl = band_frequencies(L, 0.5 * f0, 2.5 * f0) if L else [f0]
+        cfg = Config(N=N, ND=3 if three else 2, dh=10.0, dt=8e-4, NT=nt, L=L, f0=f0, FL=fl, FDORDER=order,
+                     freesurf=1, nab=16)
+        vp = np.full(shape, 3000.0, np.float32) * (1 + 0.1 * rng.uniform(-1, 1, shape)).astype(np.float32)
+        m = {"vp": vp, "vs": (vp / 1.8).astype(np.float32), "rho": np.full(shape, 2000.0, np.float32)}
+        if L:
+            tau = q_to_tau(50.0, fl, 0.5 * f0, 2.5 * f0)
+            m["taup"] = np.full(shape, tau, np.float32)
+            m["taus"] = np.full(shape, tau, np.float32)
+        nx_ = shape[0]
+        shots = []
+        for k in range(int(rng.integers(1, 5))):
+            x = float(rng.uniform(20, nx_ - 20)) * 10.0
+            y = shape[1] // 2 * 10.0 if three else 0.0
+            sp = np.array([[x, y, 50.0, k, 100]], np.float32)
+            rp = np.zeros((64, 8), np.float32)
+            rp[:, 0] = np.linspace(200.0, (nx_ - 20) * 10.0, 64)
+            rp[:, 1] = y
+            rp[:, 2] = 50.0
+            rp[:, 4] = np.arange(1, 65)
+            shots.append((sp, ricker(f0, nt, cfg.dt)[None, :], rp))
+        kind = "gradient" if rng.uniform() < 0.3 else "forward"
+        obs = [{"vx": np.zeros((64, nt), np.float32), "vz": np.zeros((64, nt), np.float32)} for _ in shots] \
+            if kind == "gradient" else None
+        reqs.append(serving.Request(cfg, m, shots, ("vx", "vz"), kind, obs, rid=i))
+    with serving.Server(workers=args.workers) as srv:
+        futs = []
+        t0 = time.perf_counter()
+        for a, q in zip(arrivals, reqs):
+            dt = t0 + a - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            futs.append(srv.submit(q))
+        res = [f.result() for f in futs]
+        wall = time.perf_counter() - t0
+    lat = [r.latency for r in res]
+    p = serving.percentiles(lat)
+    nshots = sum(len(q.shots) for q in reqs)
+    print(json.dumps({
+        "metric": "shots/s", "value": round(nshots / wall, 3), "unit": "shots/s", "n_gpus": 1,
+        "steps": nreq, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serving", "requests": nreq, "arrival_rate_per_s": args.rate, "workers": args.workers,
+                   "mix": "70 % forward / 30 % gradient; 80 % 2D (100-400 x 200-1000), 20 % 3D (64-128^3); "
+                          "order 4/8; L 0-2; NT 500-1500; 1-4 shots"},
+        "requests_per_s": round(nreq / wall, 3), "latency_s": {k: round(v, 3) for k, v in p.items()},
+        "wall_s": round(wall, 2),
+    }))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="visco3d", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="visco3d",
+                    choices=sorted(WORKLOADS) + sorted(GRADIENT_WORKLOADS) + ["serving"])
+    ap.add_argument("--fields", default="fp32", choices=["fp32", "fp16"],
+                    help="storage of wave fields and memory variables (arithmetic is FP32 either way)")
+    ap.add_argument("--rate", type=float, default=20.0, help="serving: request arrival rate (1/s)")
+    ap.add_argument("--workers", type=int, default=4, help="serving: worker threads")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--ref-budget", type=float, default=15.0)
     ap.add_argument("--kernel-reps", type=int, default=20)
     ap.add_argument("--nt", type=int, default=0, help="override NT (profiling runs only)")
     args = ap.parse_args()
+    if args.workload in GRADIENT_WORKLOADS:
+        return run_gradient(args)
+    if args.workload == "serving":
+        return run_serving(args)
 
     w, model, acq = build_workload(args.workload)
     if args.nt > 0:
@@ -312,7 +547,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from seiscl_b200.engine import Plan
 
-    plan = Plan(engine_config(w))
+    import dataclasses
+
+    plan = Plan(dataclasses.replace(engine_config(w), field_precision=args.fields))
     plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
     sp, src, rp, outs = acq["src_pos"], acq["src"], acq["rec_pos"], acq["outputs"]
     for _ in range(args.warmup):
@@ -341,17 +578,18 @@ def main():
     e2e = total_updates / wall / 1e9
     # kernel-level roofline (dominant kernel = stress update)
     kv, ks, ksurf = plan.bench_kernels(args.kernel_reps)
-    ab = algorithmic_bytes(w)
+    ab = algorithmic_bytes(w, 2 if args.fields == "fp16" else 4)
     peak, peak_kind = measured_peaks()
     s_gbs = ab["s"] / (ks / 1e3) / 1e9
     v_gbs = ab["v"] / (kv / 1e3) / 1e9
     step_ms = loop_ms / args.steps / w["nt"]
     fused_gbs = ab["fused"] / (step_ms / 1e3) / 1e9
-    skern = ("stress update, TMA-pipelined (k_tma<1,%d,*>)" % w["L"]) if plan.uses_tma else \
+    skern = ("stress update, streaming, FP16 storage (k_s3d_stream<4,%d,half>)" % w["L"]) if args.fields == "fp16" \
+        else ("stress update, TMA-pipelined (k_tma<1,%d,*>)" % w["L"]) if plan.uses_tma else \
         ("stress update, general (k_s%dd)" % (3 if w["nd"] == 3 else 2))
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic_%s.json" % args.workload)
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and args.fields == "fp32":
         traffic = json.load(open(tpath)).get("stress_kernel_bytes_per_launch")
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -375,7 +613,7 @@ def main():
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": args.workload, "grid": [w["nz"], w["ny"], w["nx"]], "nt": w["nt"], "L": w["L"],
+        "config": {"workload": args.workload, "field_storage": args.fields, "grid": [w["nz"], w["ny"], w["nx"]], "nt": w["nt"], "L": w["L"],
                    "fdorder": w["fdorder"], "nab": w["nab"], "freesurf": w["freesurf"], "shots_per_gpu": args.steps,
                    "l2": "inputs larger than L2 (%.2f GB of fields)" % (cells * 4 * (9 + 6 * w["L"]) / 1e9)},
         "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": int(h2d),

@@ -85,7 +85,12 @@ typedef struct sfd_config {
                               from zeroed CPML memory.  With sources whose wave field is
                               large (forces), the carried-over memory dominates the adjoint
                               field inside the absorbing layers; 1 removes that. */
-    int reserved[5];
+    int field_precision;   /* 0: wave fields and memory variables in FP32; 1: in FP16,
+                              scaled by powers of two per shot (3D forward modelling
+                              only; arithmetic stays FP32).  No reference counterpart
+                              in this form: the reference's FP16=2 mode also scales
+                              by powers of two (src/assign_modeling_case.c:829-866). */
+    int reserved[4];
 } sfd_config;
 
 typedef struct sfd_shot {

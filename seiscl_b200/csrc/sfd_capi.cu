@@ -159,6 +159,9 @@ int upload_shot(sfd_plan *p, const sfd_shot *shot, int mask, PointSet &S, PointS
     return SFD_OK;
 }
 
+// bytes per stored wave-field / memory-variable value
+size_t wave_elem(const Grid &g) { return g.fhalf ? 2 : sizeof(float); }
+
 int alloc_model(sfd_plan *p)
 {
     const Grid &g = p->g;
@@ -166,13 +169,13 @@ int alloc_model(sfd_plan *p)
     for (int w = 0; w < NW; w++) {
         p->f.w[w] = nullptr;
         if (!is_wave_used(g, w)) continue;
-        p->f.w[w] = (float *)dalloc(p, sizeof(float) * g.nvol, &e);
+        p->f.w[w] = (float *)dalloc(p, wave_elem(g) * g.nvol, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "wave field allocation failed");
     }
     for (int r = 0; r < NR; r++) {
         p->f.r[r] = nullptr;
         if (!is_mem_used(g, r)) continue;
-        p->f.r[r] = (float *)dalloc(p, sizeof(float) * g.nvol * g.L, &e);
+        p->f.r[r] = (float *)dalloc(p, wave_elem(g) * g.nvol * g.L, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "memory-variable allocation failed");
     }
     int64_t nab2 = 2 * (int64_t)g.nab;
@@ -245,9 +248,9 @@ int zero_forward_state(sfd_plan *p, cudaStream_t st)
 {
     const Grid &g = p->g;
     for (int w = 0; w < NW; w++)
-        if (p->f.w[w]) CKC(cudaMemsetAsync(p->f.w[w], 0, sizeof(float) * g.nvol, st));
+        if (p->f.w[w]) CKC(cudaMemsetAsync(p->f.w[w], 0, wave_elem(g) * g.nvol, st));
     for (int r = 0; r < NR; r++)
-        if (p->f.r[r]) CKC(cudaMemsetAsync(p->f.r[r], 0, sizeof(float) * g.nvol * g.L, st));
+        if (p->f.r[r]) CKC(cudaMemsetAsync(p->f.r[r], 0, wave_elem(g) * g.nvol * g.L, st));
     int64_t tot = 0;
     for (int i = 0; i < NPSI; i++) tot += p->psi_size[i];
     if (tot) CKC(cudaMemsetAsync(p->d_psi_all, 0, sizeof(float) * tot, st));
@@ -307,6 +310,8 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     if (c.precision < 0 || c.precision > 2) return SFD_ERR_ARG;
     if (c.kernels < 0 || c.kernels > 4) return SFD_ERR_ARG;
     if (c.adjoint_reset_psi < 0 || c.adjoint_reset_psi > 1) return SFD_ERR_ARG;
+    if (c.field_precision < 0 || c.field_precision > 1) return SFD_ERR_ARG;
+    if (c.field_precision == 1 && (c.nd != 3 || c.L > 3)) return SFD_ERR_UNSUPPORTED;
 
     sfd_plan *p = new sfd_plan();
     p->cfg = c;
@@ -339,6 +344,8 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
         g.eta_c[l] = 1.0f - half;
     }
     g.inv_dt = 1.0f / c.dt;
+    g.fhalf = c.field_precision == 1;
+    for (int w = 0; w < NW; w++) g.ws.w[w] = 1.0f;
     g.nbnd = nbnd_cells(g.nd, g.nz, g.ny, g.nx, g.F, g.nab, g.freesurf);
     if (p->cfg.tmax <= 0 || p->cfg.tmax > c.nt) p->cfg.tmax = c.nt;
     if (p->cfg.tmin < 0) p->cfg.tmin = 0;
@@ -354,6 +361,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     memset(&p->f, 0, sizeof p->f);
     memset(&p->a, 0, sizeof p->a);
     p->last_ms = 0.0f;
+    p->kshift = 0;
     if (cudaGetDevice(&p->device) != cudaSuccess) { delete p; return SFD_ERR_CUDA; }
     if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) { delete p; return SFD_ERR_CUDA; }
     p->own_stream = true;
@@ -388,8 +396,31 @@ extern "C" int sfd_set_model(sfd_plan *p, const float *const *params)
         if ((rc = upload_constants(p))) return rc;
     }
     int64_t npar = (int64_t)p->g.nz * p->g.ny * p->g.nx;
-    for (int k = 0; k < NPAR; k++)
-        CKC(cudaMemcpy((void *)p->f.p[k], p->hp[k].data(), sizeof(float) * npar, cudaMemcpyHostToDevice));
+    if (p->g.fhalf) {
+        // FP16 storage keeps velocities as v * 2^b and stresses as s * 2^a with
+        // b - a = kshift ~ log2 of the impedance, so both stay near the same
+        // magnitude; the moduli carry 2^-kshift and the buoyancies 2^kshift
+        // (exact power-of-two scalings of the FP32 parameters).
+        double acc = 0.0;
+        int64_t n = 0, step = std::max<int64_t>(1, npar / 4096);
+        for (int64_t i = 0; i < npar; i += step) {
+            const double z = std::sqrt((double)p->hp[PM][i] / (double)p->hp[PRIP][i]);
+            if (z > 0 && std::isfinite(z)) { acc += std::log2(z); n++; }
+        }
+        p->kshift = n ? (int)std::lround(acc / n) : 0;
+        const int up[3] = {PRIP, PRJP, PRKP}, down[5] = {PM, PMU, PMUIPKP, PMUIPJP, PMUJPKP};
+        std::vector<float> tmp(npar);
+        for (int k = 0; k < NPAR; k++) {
+            int e = 0;
+            for (int q : up) if (q == k) e = p->kshift;
+            for (int q : down) if (q == k) e = -p->kshift;
+            for (int64_t i = 0; i < npar; i++) tmp[i] = std::ldexp(p->hp[k][i], e);
+            CKC(cudaMemcpy((void *)p->f.p[k], tmp.data(), sizeof(float) * npar, cudaMemcpyHostToDevice));
+        }
+    } else {
+        for (int k = 0; k < NPAR; k++)
+            CKC(cudaMemcpy((void *)p->f.p[k], p->hp[k].data(), sizeof(float) * npar, cudaMemcpyHostToDevice));
+    }
     p->model_set = true;
     p->have_forward = false;
     return SFD_OK;
@@ -424,6 +455,22 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
     if (nsel) CKC(cudaMemsetAsync(p->d_seis, 0, sizeof(float) * (size_t)nsel * shot->nrec * p->cfg.nt, st));
     BndSlot bs;
     memset(&bs, 0, sizeof bs);
+    if (g.fhalf) {
+        if (save_boundaries)
+            return fail(p, SFD_ERR_UNSUPPORTED, "FP16 wave-field storage covers forward modelling only");
+        // the source injects about 2^4 per step into the field it feeds
+        float smax = 0.0f;
+        bool force_only = shot->nsrc > 0;
+        for (int i = 0; i < shot->nsrc; i++) {
+            const int ty = (int)shot->src_pos[5 * i + 4];
+            if (ty != 0 && ty != 1 && ty != 2) force_only = false;
+            for (int t = 0; t < p->cfg.nt; t++) smax = std::max(smax, std::fabs(shot->src[(int64_t)i * p->cfg.nt + t]));
+        }
+        const double inj = (double)smax * p->cfg.dt;
+        const int e0 = inj > 0 ? (int)std::lround(4.0 - std::log2(inj)) : 0;
+        const int a = force_only ? e0 - p->kshift : e0, b = a + p->kshift;
+        for (int w = 0; w < NW; w++) p->g.ws.w[w] = std::ldexp(1.0f, w <= VZ ? b : a);
+    }
     if (save_boundaries) {
         if (g.nd == 21 || g.nd == 22)
             return fail(p, SFD_ERR_UNSUPPORTED, "the adjoint path covers P-SV and 3D elastic/viscoelastic media");
@@ -476,6 +523,7 @@ extern "C" int sfd_adjoint(sfd_plan *p, const sfd_shot *shot, int mask, const in
     if (!p || !shot) return SFD_ERR_ARG;
     if (p->g.nd == 21 || p->g.nd == 22)
         return fail(p, SFD_ERR_UNSUPPORTED, "the adjoint path covers P-SV and 3D elastic/viscoelastic media");
+    if (p->g.fhalf) return fail(p, SFD_ERR_UNSUPPORTED, "FP16 wave-field storage covers forward modelling only");
     if (!p->have_forward) return fail(p, SFD_ERR_STATE, "sfd_adjoint needs a preceding sfd_forward with saved boundaries");
     int rc;
     if ((rc = check_outsel(p, outsel))) return rc;
@@ -635,6 +683,7 @@ extern "C" int64_t sfd_debug_copy(sfd_plan *p, int kind, int id, float *dst, int
     const Grid &g = p->g;
     const void *src = nullptr;
     int64_t n = 0;
+    if (g.fhalf && kind >= 0 && kind <= 2) return fail(p, SFD_ERR_UNSUPPORTED, "wave fields are stored in FP16");
     if (kind == 0 && id >= 0 && id < NW) { src = p->f.w[id]; n = g.nvol; }
     else if (kind == 1 && id >= 0 && id < NW) { src = p->a.wr[id]; n = g.nvol; }
     else if (kind == 2 && id >= 0 && id < NR) { src = p->f.r[id]; n = g.nvol * g.L; }

@@ -30,6 +30,12 @@ enum {
 enum { CK, CA, CB, CKH, CAH, CBH, NC };
 enum { GRHO, GM, GMU, NG };
 
+// Stored value = field x w[field]: 1 for FP32 storage; powers of two for
+// FP16 storage (set per shot from the source amplitude).
+struct WScale {
+    float w[NW];
+};
+
 // Everything a stencil kernel needs, passed by value (a few hundred bytes of
 // kernel parameter space).
 struct Grid {
@@ -44,6 +50,8 @@ struct Grid {
     float eta[8];           // 2 pi FL dt
     float eta_b[8], eta_c[8];  // 1/(1+eta/2) and 1-eta/2, FP32 as the kernels would form them
     float inv_dt;           // 1/dt rounded to FP32
+    int fhalf;              // 1: wave fields and memory variables stored in FP16 (3D forward)
+    WScale ws;              // storage scale per wave field (all 1 for FP32)
     int nbnd;               // saved-boundary cells per field per step
     int restype;
     int kernels;            // 0: register-blocked 3D kernels where available, 1: general only
@@ -105,5 +113,6 @@ struct sfd_plan {
     float *d_src_div, *d_src, *d_seis, *d_res;
     float *d_surf_q;        // surface-adjoint scratch [nx][ny]
     cudaEvent_t ev0, ev1;
+    int kshift;             // FP16 storage: log2 ratio of velocity to stress scales
     float last_ms;
 };

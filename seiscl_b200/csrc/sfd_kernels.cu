@@ -62,6 +62,44 @@ __device__ __forceinline__ float dbw_rw(const float *v, i64 i, i64 st, const flo
     return acc;
 }
 
+// Wave-field storage access: FP32, or FP16 holding the field times a power
+// of two (the kernels compute in FP32 either way).
+template <class T> __device__ __forceinline__ float ldv(const T *p);
+template <> __device__ __forceinline__ float ldv<float>(const float *p) { return *p; }
+template <> __device__ __forceinline__ float ldv<__half>(const __half *p) { return __half2float(*p); }
+template <class T> __device__ __forceinline__ float ldgv(const T *p);
+template <> __device__ __forceinline__ float ldgv<float>(const float *p) { return __ldg(p); }
+template <> __device__ __forceinline__ float ldgv<__half>(const __half *p) { return __half2float(__ldg(p)); }
+template <class T> __device__ __forceinline__ void stv(T *p, float v);
+template <> __device__ __forceinline__ void stv<float>(float *p, float v) { *p = v; }
+template <> __device__ __forceinline__ void stv<__half>(__half *p, float v) { *p = __float2half_rn(v); }
+template <class T> __device__ __forceinline__ T *fld(float *p) { return reinterpret_cast<T *>(p); }
+
+template <int F, class T>
+__device__ __forceinline__ float dfwT(const T *__restrict__ v, i64 i, i64 st, const float *hc)
+{
+    float acc = hc[0] * (ldgv(v + i + st) - ldgv(v + i));
+#pragma unroll
+    for (int m = 2; m <= F; m++) acc = fmaf(hc[m - 1], ldgv(v + i + m * st) - ldgv(v + i - (m - 1) * st), acc);
+    return acc;
+}
+template <int F, class T>
+__device__ __forceinline__ float dbwT(const T *__restrict__ v, i64 i, i64 st, const float *hc)
+{
+    float acc = hc[0] * (ldgv(v + i) - ldgv(v + i - st));
+#pragma unroll
+    for (int m = 2; m <= F; m++) acc = fmaf(hc[m - 1], ldgv(v + i + (m - 1) * st) - ldgv(v + i - m * st), acc);
+    return acc;
+}
+template <int F, class T>
+__device__ __forceinline__ float dbw_rwT(const T *v, i64 i, i64 st, const float *hc)
+{
+    float acc = hc[0] * (ldv(v + i) - ldv(v + i - st));
+#pragma unroll
+    for (int m = 2; m <= F; m++) acc = fmaf(hc[m - 1], ldv(v + i + (m - 1) * st) - ldv(v + i - m * st), acc);
+    return acc;
+}
+
 // psi = b psi + a d ; d = d/K + psi    (the CPML recursion of every kernel)
 __device__ __forceinline__ void cpml(float *psi, i64 q, const float *K, const float *a, const float *b, int ci,
                                      float &d)
@@ -626,46 +664,54 @@ __device__ __forceinline__ void taper_regs(const Grid &g, const float *taper, in
     if (gx > g.NX - NAB - F - 1) mul(__ldg(taper + g.NX - F - gx - 1));
 }
 
-template <int F>
+template <int F, class T = float>
 __global__ void __launch_bounds__(256, 3) k_v3d_stream(Grid g, Fields f)
 {
     CELL3D
     const float *hc = g.hc;
-    float v[3] = {__ldg(f.w[VX] + iv), __ldg(f.w[VY] + iv), __ldg(f.w[VZ] + iv)};
+    T *wvx = fld<T>(f.w[VX]), *wvy = fld<T>(f.w[VY]), *wvz = fld<T>(f.w[VZ]);
+    float v[3] = {ldgv(wvx + iv), ldgv(wvy + iv), ldgv(wvz + iv)};
     const float rip = __ldg(f.p[PRIP] + ip), rjp = __ldg(f.p[PRJP] + ip), rkp = __ldg(f.p[PRKP] + ip);
-    float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc);
-    float sxx_x = dfw<F>(f.w[SXX], iv, sx, hc);
-    float sxz_x = dbw<F>(f.w[SXZ], iv, sx, hc);
-    float sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
-    float syz_y = dbw<F>(f.w[SYZ], iv, sy, hc);
-    float syz_z = dbw<F>(f.w[SYZ], iv, 1, hc);
-    float syy_y = dfw<F>(f.w[SYY], iv, sy, hc);
-    float sxy_x = dbw<F>(f.w[SXY], iv, sx, hc);
-    float sxy_y = dbw<F>(f.w[SXY], iv, sy, hc);
+    const T *Sxx = fld<T>(f.w[SXX]), *Syy = fld<T>(f.w[SYY]), *Szz = fld<T>(f.w[SZZ]);
+    const T *Sxy = fld<T>(f.w[SXY]), *Syz = fld<T>(f.w[SYZ]), *Sxz = fld<T>(f.w[SXZ]);
+    float szz_z = dfwT<F>(Szz, iv, 1, hc);
+    float sxx_x = dfwT<F>(Sxx, iv, sx, hc);
+    float sxz_x = dbwT<F>(Sxz, iv, sx, hc);
+    float sxz_z = dbwT<F>(Sxz, iv, 1, hc);
+    float syz_y = dbwT<F>(Syz, iv, sy, hc);
+    float syz_z = dbwT<F>(Syz, iv, 1, hc);
+    float syy_y = dfwT<F>(Syy, iv, sy, hc);
+    float sxy_x = dbwT<F>(Sxy, iv, sx, hc);
+    float sxy_y = dbwT<F>(Sxy, iv, sy, hc);
     if (g.abs_type == 1) cpml_v3d(g, f, gz, gy, gx, sxx_x, syy_y, szz_z, sxy_y, sxy_x, syz_y, syz_z, sxz_x, sxz_z);
     v[0] += (sxx_x + sxy_y + sxz_z) * rip;
     v[1] += (syy_y + sxy_x + syz_z) * rjp;
     v[2] += (szz_z + sxz_x + syz_y) * rkp;
     if (g.abs_type == 2) taper_regs<3>(g, f.taper, gz, gy, gx, v);
-    f.w[VX][iv] = v[0];
-    f.w[VY][iv] = v[1];
-    f.w[VZ][iv] = v[2];
+    stv(wvx + iv, v[0]);
+    stv(wvy + iv, v[1]);
+    stv(wvz + iv, v[2]);
 }
 
-template <int F, int L>
+template <int F, int L, class T = float>
 __global__ void __launch_bounds__(256, 2) k_s3d_stream(Grid g, Fields f)
 {
     CELL3D
     const float *hc = g.hc;
     // per-cell streams first: stresses, memory variables, parameters
-    float s[6] = {__ldg(f.w[SXY] + iv), __ldg(f.w[SYZ] + iv), __ldg(f.w[SXZ] + iv),
-                  __ldg(f.w[SXX] + iv), __ldg(f.w[SYY] + iv), __ldg(f.w[SZZ] + iv)};
+    T *ws[6] = {fld<T>(f.w[SXY]), fld<T>(f.w[SYZ]), fld<T>(f.w[SXZ]),
+                fld<T>(f.w[SXX]), fld<T>(f.w[SYY]), fld<T>(f.w[SZZ])};
+    T *wr[6] = {fld<T>(f.r[RXY]), fld<T>(f.r[RYZ]), fld<T>(f.r[RXZ]),
+                fld<T>(f.r[RXX]), fld<T>(f.r[RYY]), fld<T>(f.r[RZZ])};
+    float s[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) s[q] = ldgv(ws[q] + iv);
     float r[6][L > 0 ? L : 1];
 #pragma unroll
     for (int l = 0; l < L; l++) {
         const i64 ir = l * g.nvol + iv;
-        r[0][l] = __ldg(f.r[RXY] + ir); r[1][l] = __ldg(f.r[RYZ] + ir); r[2][l] = __ldg(f.r[RXZ] + ir);
-        r[3][l] = __ldg(f.r[RXX] + ir); r[4][l] = __ldg(f.r[RYY] + ir); r[5][l] = __ldg(f.r[RZZ] + ir);
+#pragma unroll
+        for (int q = 0; q < 6; q++) r[q][l] = ldgv(wr[q] + ir);
     }
     const float lM = __ldg(f.p[PM] + ip), lmu = __ldg(f.p[PMU] + ip);
     const float lmuipkp = __ldg(f.p[PMUIPKP] + ip), lmuipjp = __ldg(f.p[PMUIPJP] + ip),
@@ -676,9 +722,10 @@ __global__ void __launch_bounds__(256, 2) k_s3d_stream(Grid g, Fields f)
         ltausipkp = __ldg(f.p[PTAUSIPKP] + ip); ltausipjp = __ldg(f.p[PTAUSIPJP] + ip);
         ltausjpkp = __ldg(f.p[PTAUSJPKP] + ip);
     }
-    float vzx = dfw<F>(f.w[VZ], iv, sx, hc), vzy = dfw<F>(f.w[VZ], iv, sy, hc), vzz = dbw<F>(f.w[VZ], iv, 1, hc);
-    float vyx = dfw<F>(f.w[VY], iv, sx, hc), vyy = dbw<F>(f.w[VY], iv, sy, hc), vyz = dfw<F>(f.w[VY], iv, 1, hc);
-    float vxx = dbw<F>(f.w[VX], iv, sx, hc), vxy = dfw<F>(f.w[VX], iv, sy, hc), vxz = dfw<F>(f.w[VX], iv, 1, hc);
+    const T *Vx = fld<T>(f.w[VX]), *Vy = fld<T>(f.w[VY]), *Vz = fld<T>(f.w[VZ]);
+    float vzx = dfwT<F>(Vz, iv, sx, hc), vzy = dfwT<F>(Vz, iv, sy, hc), vzz = dbwT<F>(Vz, iv, 1, hc);
+    float vyx = dfwT<F>(Vy, iv, sx, hc), vyy = dbwT<F>(Vy, iv, sy, hc), vyz = dfwT<F>(Vy, iv, 1, hc);
+    float vxx = dbwT<F>(Vx, iv, sx, hc), vxy = dfwT<F>(Vx, iv, sy, hc), vxz = dfwT<F>(Vx, iv, 1, hc);
     if (g.abs_type == 1) cpml_s3d(g, f, gz, gy, gx, vxx, vxy, vxz, vyx, vyy, vyz, vzx, vzy, vzz, false);
     float vxyyx = vxy + vyx, vyzzy = vyz + vzy, vxzzx = vxz + vzx;
     float vxxyyzz = vxx + vyy + vzz, vyyzz = vyy + vzz, vxxzz = vxx + vzz, vxxyy = vxx + vyy;
@@ -721,19 +768,19 @@ __global__ void __launch_bounds__(256, 2) k_s3d_stream(Grid g, Fields f)
 #pragma unroll
             for (int q = 0; q < 6; q++) a[q] += r[q][l];
             const i64 ir = l * g.nvol + iv;
-            f.r[RXY][ir] = r[0][l]; f.r[RYZ][ir] = r[1][l]; f.r[RXZ][ir] = r[2][l];
-            f.r[RXX][ir] = r[3][l]; f.r[RYY][ir] = r[4][l]; f.r[RZZ][ir] = r[5][l];
+#pragma unroll
+            for (int q = 0; q < 6; q++) stv(wr[q] + ir, r[q][l]);
         }
 #pragma unroll
         for (int q = 0; q < 6; q++) s[q] += ls[q] + g.dt2 * a[q];
     }
     if (g.abs_type == 2) taper_regs<6>(g, f.taper, gz, gy, gx, s);
-    f.w[SXY][iv] = s[0]; f.w[SYZ][iv] = s[1]; f.w[SXZ][iv] = s[2];
-    f.w[SXX][iv] = s[3]; f.w[SYY][iv] = s[4]; f.w[SZZ][iv] = s[5];
+#pragma unroll
+    for (int q = 0; q < 6; q++) stv(ws[q] + iv, s[q]);
 }
 
 // free surface 3D, one thread per (y, x) column (surface3D.cl:39-271)
-template <int F>
+template <int F, class T = float>
 __global__ void k_surf3d(Grid g, Fields f, int pdir)
 {
     int gy = blockIdx.x * blockDim.x + threadIdx.x + F;
@@ -743,18 +790,20 @@ __global__ void k_surf3d(Grid g, Fields f, int pdir)
     const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;
     i64 iv = gx * sx + (i64)gy * sy + gz;
     i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz - F);
-    float *sxx = f.w[SXX], *syy = f.w[SYY], *szz = f.w[SZZ], *syz = f.w[SYZ], *sxz = f.w[SXZ];
-    szz[iv] = 0.0f;
-    for (int l = 0; l < L; l++) f.r[RZZ][l * g.nvol + iv] = 0.0f;
+    T *sxx = fld<T>(f.w[SXX]), *syy = fld<T>(f.w[SYY]), *szz = fld<T>(f.w[SZZ]), *syz = fld<T>(f.w[SYZ]),
+      *sxz = fld<T>(f.w[SXZ]);
+    T *rxx = fld<T>(f.r[RXX]), *ryy = fld<T>(f.r[RYY]), *rzz = fld<T>(f.r[RZZ]);
+    stv(szz + iv, 0.0f);
+    for (int l = 0; l < L; l++) stv(rzz + l * g.nvol + iv, 0.0f);
 #pragma unroll
     for (int m = 1; m <= F; m++) {
-        szz[iv - m] = -szz[iv + m];
-        sxz[iv - m] = -sxz[iv + m - 1];
-        syz[iv - m] = -syz[iv + m - 1];
+        stv(szz + iv - m, -ldv(szz + iv + m));
+        stv(sxz + iv - m, -ldv(sxz + iv + m - 1));
+        stv(syz + iv - m, -ldv(syz + iv + m - 1));
     }
-    float vxx = dbw_rw<F>(f.w[VX], iv, sx, g.hc);
-    float vyy = dbw_rw<F>(f.w[VY], iv, sy, g.hc);
-    float vzz = dbw_rw<F>(f.w[VZ], iv, 1, g.hc);
+    float vxx = dbw_rwT<F>(fld<T>(f.w[VX]), iv, sx, g.hc);
+    float vyy = dbw_rwT<F>(fld<T>(f.w[VY]), iv, sy, g.hc);
+    float vzz = dbw_rwT<F>(fld<T>(f.w[VZ]), iv, 1, g.hc);
     if (g.abs_type == 1) {
         i64 nz = g.nz, ny = g.ny;
         if (gy - F < NAB) {
@@ -779,29 +828,29 @@ __global__ void k_surf3d(Grid g, Fields f, int pdir)
         float fm = f.p[PMU][ip] * 2.0f, gm = f.p[PM][ip];
         float h = -((gm - fm) * (gm - fm) * (vxx + vyy) / gm) - ((gm - fm) * vzz);
         // the reference adds h without the propagation direction (surface3D.cl:172-173)
-        sxx[iv] += h;
-        syy[iv] += h;
+        stv(sxx + iv, ldv(sxx + iv) + h);
+        stv(syy + iv, ldv(syy + iv) + h);
     } else {
         float taus = f.p[PTAUS][ip], taup = f.p[PTAUP][ip], mu = f.p[PMU][ip], M = f.p[PM][ip];
         float fm = mu * 2.0f * (1.0f + L * taus);
         float gm = M * (1.0f + L * taup);
         float h = -((gm - fm) * (gm - fm) * (vxx + vyy) / gm) - ((gm - fm) * vzz);
         float sumx = 0, sumy = 0;
-        for (int l = 0; l < L; l++) { sumx += f.r[RXX][l * g.nvol + iv]; sumy += f.r[RYY][l * g.nvol + iv]; }
-        sxx[iv] += pdir * (h - g.dt2 * sumx);
-        syy[iv] += pdir * (h - g.dt2 * sumy);
+        for (int l = 0; l < L; l++) { sumx += ldv(rxx + l * g.nvol + iv); sumy += ldv(ryy + l * g.nvol + iv); }
+        stv(sxx + iv, ldv(sxx + iv) + pdir * (h - g.dt2 * sumx));
+        stv(syy + iv, ldv(syy + iv) + pdir * (h - g.dt2 * sumy));
         float d = 2.0f * mu * taus / g.dt, e = M * taup / g.dt;
         sumx = 0; sumy = 0;
         for (int l = 0; l < L; l++) {
             float b = g.eta[l] / (1.0f + g.eta[l] * 0.5f);
             float hh = b * (((d - e) * ((fm / gm) - 1.0f) * (vxx + vyy)) - ((d - e) * vzz));
-            float rx = f.r[RXX][l * g.nvol + iv] + hh, ry = f.r[RYY][l * g.nvol + iv] + hh;
-            f.r[RXX][l * g.nvol + iv] = rx;
-            f.r[RYY][l * g.nvol + iv] = ry;
+            float rx = ldv(rxx + l * g.nvol + iv) + hh, ry = ldv(ryy + l * g.nvol + iv) + hh;
+            stv(rxx + l * g.nvol + iv, rx);
+            stv(ryy + l * g.nvol + iv, ry);
             sumx += rx; sumy += ry;
         }
-        sxx[iv] += g.dt2 * sumx;
-        syy[iv] += g.dt2 * sumy;
+        stv(sxx + iv, ldv(sxx + iv) + g.dt2 * sumx);
+        stv(syy + iv, ldv(syy + iv) + g.dt2 * sumy);
     }
 }
 
@@ -1424,8 +1473,9 @@ __global__ void k_surfadj3d_b(Grid g, Fields f, AdjFields a, const float *q)
 
 // ------------------------------------------------ point kernels (per shot)
 // src/automatic_kernels.c:394-629; several sources may share a cell
+template <class T = float>
 __global__ void k_sources(Fields f, PointSet s, const float *src, int nt_total, int t, int pdir, float dt,
-                          int freesurf, int F)
+                          int freesurf, int F, WScale ws)
 {
     int gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= s.n) return;
@@ -1436,12 +1486,14 @@ __global__ void k_sources(Fields f, PointSet s, const float *src, int nt_total, 
     for (int q = 0; q < s.ntarget[gid]; q++) {
         float dv = s.div[gid * 3 + q];
         float val = dv == 0.0f ? amp : amp / dv;
-        atomicAdd(f.w[s.field[gid * 3 + q]] + cell, val);
+        const int w = s.field[gid * 3 + q];
+        atomicAdd(fld<T>(f.w[w]) + cell, (T)(val * ws.w[w]));
     }
 }
 
 // src/automatic_kernels.c:22-219; out is [nsel][nrec][NT]
-__global__ void k_record(Fields f, PointSet r, float *out, int nt_total, int t, unsigned outmask, int nd)
+template <class T = float>
+__global__ void k_record(Fields f, PointSet r, float *out, int nt_total, int t, unsigned outmask, int nd, WScale ws)
 {
     int gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= r.n) return;
@@ -1452,11 +1504,13 @@ __global__ void k_record(Fields f, PointSet r, float *out, int nt_total, int t, 
         if (!(outmask & (1u << o))) continue;
         float v;
         if (o == SFD_OUT_P) {
-            if (nd == 3) v = (f.w[SXX][cell] + f.w[SZZ][cell] + f.w[SYY][cell]) / 3.0f;
-            else if (nd == 22) v = f.w[SXX][cell];
-            else v = (f.w[SXX][cell] + f.w[SZZ][cell]) / 2.0f;
+            const T *xx = fld<T>(f.w[SXX]), *zz = fld<T>(f.w[SZZ]);
+            if (nd == 3) v = (ldv(xx + cell) + ldv(zz + cell) + ldv(fld<T>(f.w[SYY]) + cell)) / 3.0f;
+            else if (nd == 22) v = ldv(xx + cell);
+            else v = (ldv(xx + cell) + ldv(zz + cell)) / 2.0f;
+            v /= ws.w[SXX];
         } else {
-            v = f.w[o][cell];
+            v = ldv(fld<T>(f.w[o]) + cell) / ws.w[o];
         }
         out[((i64)slot * r.n + gid) * nt_total + t] = v;
         slot++;
@@ -1502,6 +1556,11 @@ static inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b)
 
 void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
 {
+    if (g.fhalf && g.nd == 3) {   // FP16 storage: the streaming kernels only
+        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
+        DISPATCH_F(g.F, k_v3d_stream<FF, __half><<<gr, b, 0, st>>>(g, f));
+        return;
+    }
     // kernels 0 takes the streaming velocity kernel (0.52 ms at 256^3, against
     // 0.58 general and 0.63 TMA); only kernels 3 takes the TMA path here
     if (g.kernels == 3 && launch_update_v_tma(g, f, st)) return;
@@ -1527,6 +1586,16 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
 
 void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
 {
+    if (g.fhalf && g.nd == 3 && g.L <= 3) {   // FP16 storage: the streaming kernels only
+        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
+        switch (g.L) {
+        case 0: DISPATCH_F(g.F, k_s3d_stream<FF, 0, __half><<<gr, b, 0, st>>>(g, f)); break;
+        case 1: DISPATCH_F(g.F, k_s3d_stream<FF, 1, __half><<<gr, b, 0, st>>>(g, f)); break;
+        case 2: DISPATCH_F(g.F, k_s3d_stream<FF, 2, __half><<<gr, b, 0, st>>>(g, f)); break;
+        default: DISPATCH_F(g.F, k_s3d_stream<FF, 3, __half><<<gr, b, 0, st>>>(g, f)); break;
+        }
+        return;
+    }
     if ((g.kernels == 0 || g.kernels == 3) && launch_update_s_tma(g, f, st)) return;
     if (g.kernels == 2 && launch_update_s_fast(g, f, st)) return;
     if (g.nd == 21 || g.nd == 22) {
@@ -1562,7 +1631,8 @@ void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st)
     if (g.nd == 22) return;
     if (g.nd == 3) {
         dim3 b(32, 4), gr(cdiv(g.ny, 32), cdiv(g.nx, 4));
-        DISPATCH_F(g.F, k_surf3d<FF><<<gr, b, 0, st>>>(g, f, pdir));
+        if (g.fhalf) DISPATCH_F(g.F, k_surf3d<FF, __half><<<gr, b, 0, st>>>(g, f, pdir))
+        else DISPATCH_F(g.F, k_surf3d<FF><<<gr, b, 0, st>>>(g, f, pdir))
     } else {
         DISPATCH_F(g.F, k_surf2d<FF><<<cdiv(g.nx, 128), 128, 0, st>>>(g, f, pdir));
     }
@@ -1614,14 +1684,20 @@ void launch_sources(const Grid &g, const Fields &f, const PointSet &s, const flo
                     int pdir, cudaStream_t st)
 {
     if (s.n == 0) return;
-    k_sources<<<cdiv(s.n, 128), 128, 0, st>>>(f, s, src, nt_total, t, pdir, g.dt, g.freesurf, g.F);
+    if (g.fhalf)
+        k_sources<__half><<<cdiv(s.n, 128), 128, 0, st>>>(f, s, src, nt_total, t, pdir, g.dt, g.freesurf, g.F, g.ws);
+    else
+        k_sources<float><<<cdiv(s.n, 128), 128, 0, st>>>(f, s, src, nt_total, t, pdir, g.dt, g.freesurf, g.F, g.ws);
 }
 
 void launch_record(const Grid &g, const Fields &f, const PointSet &r, float *out, int nt_total, int t,
                    unsigned outmask, cudaStream_t st)
 {
     if (r.n == 0 || outmask == 0) return;
-    k_record<<<cdiv(r.n, 128), 128, 0, st>>>(f, r, out, nt_total, t, outmask, g.nd);
+    if (g.fhalf)
+        k_record<__half><<<cdiv(r.n, 128), 128, 0, st>>>(f, r, out, nt_total, t, outmask, g.nd, g.ws);
+    else
+        k_record<float><<<cdiv(r.n, 128), 128, 0, st>>>(f, r, out, nt_total, t, outmask, g.nd, g.ws);
 }
 
 void launch_residuals(const Grid &g, const AdjFields &a, const PointSet &r, const float *res, int nt_total, int t,

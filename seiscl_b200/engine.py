@@ -35,7 +35,8 @@ class sfd_config(C.Structure):
                 ("fl", C.c_float * 8), ("vppml", C.c_float), ("fpml", C.c_float), ("npower", C.c_float),
                 ("k_max_cpml", C.c_float), ("abpc", C.c_float), ("tmin", C.c_int), ("tmax", C.c_int),
                 ("param_type", C.c_int), ("restype", C.c_int), ("precision", C.c_int),
-                ("kernels", C.c_int), ("adjoint_reset_psi", C.c_int), ("reserved", C.c_int * 5)]
+                ("kernels", C.c_int), ("adjoint_reset_psi", C.c_int), ("field_precision", C.c_int),
+                ("reserved", C.c_int * 4)]
 
 
 class sfd_shot(C.Structure):
@@ -134,6 +135,7 @@ class Config:
     kernels: str = "fast"  # "fast" (3D: streaming velocity, TMA or streaming stress), "general", "register",
     #                        "tma", "stream"
     adjoint_reset_psi: bool = False  # True: the adjoint starts from zeroed CPML memory (not the reference's)
+    field_precision: str = "fp32"  # "fp16": wave fields / memory variables stored in FP16 (3D forward)
 
     def to_c(self) -> sfd_config:
         c = sfd_config()
@@ -166,6 +168,7 @@ class Config:
         c.precision = PREC[self.precision]
         c.kernels = {"fast": 0, "general": 1, "register": 2, "tma": 3, "stream": 4}[self.kernels]
         c.adjoint_reset_psi = 1 if self.adjoint_reset_psi else 0
+        c.field_precision = {"fp32": 0, "fp16": 1}[self.field_precision]
         return c
 
     @property

@@ -201,3 +201,41 @@ def test_acoustic_and_sh_forward_match_oracle(kw, cuda_device):
     for n in outs:
         assert np.abs(ref[n]).max() > 0, n
         assert rel_l2(got[n], ref[n]) < FWD_TOL, (n, rel_l2(got[n], ref[n]))
+
+
+FP16_CASES = [
+    dict(nd=3, freesurf=1, L=0, abs_type=1, src_type=100, nz=40, ny=36, nx=44, nt=150, nab=8),
+    dict(nd=3, freesurf=1, L=2, abs_type=1, src_type=2, nz=40, ny=36, nx=44, nt=150, nab=8),
+    dict(nd=3, freesurf=0, L=1, abs_type=2, src_type=0, nz=36, ny=30, nx=40, nt=150, nab=8, fdorder=4),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", FP16_CASES, ids=lambda k: "-".join("%s%s" % (a, b) for a, b in k.items()))
+def test_fp16_field_storage_against_fp32(kw, cuda_device):
+    """Wave fields and memory variables stored in FP16 (power-of-two scaled,
+    FP32 arithmetic) against the FP32 run: the reference's own criterion for
+    its FP16 modes, sum (d - r)^2 / sum r^2 < 1e-3 over all outputs
+    (test_consistency.py)."""
+    import dataclasses
+
+    from seiscl_b200.engine import Plan, SeisCLEngineError
+
+    cfg, model, acq = make_case(**kw)
+    outs = _outputs(3)
+    res = {}
+    for prec in ("fp32", "fp16"):
+        plan = Plan(dataclasses.replace(engine_config(cfg), field_precision=prec))
+        plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+        res[prec] = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
+        if prec == "fp16":
+            with pytest.raises(SeisCLEngineError):   # the fields really are FP16
+                plan.debug_array(0, 0, plan.nvol)
+            with pytest.raises(SeisCLEngineError):   # forward modelling only
+                plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs, save_boundaries=True)
+    # summed over all recorded outputs, as test_consistency.py does (a single
+    # component can be ~0 by symmetry, e.g. vy in the source's plane)
+    num = sum(float(((res["fp16"][n].astype(np.float64) - res["fp32"][n]) ** 2).sum()) for n in outs)
+    den = sum(float((res["fp32"][n].astype(np.float64) ** 2).sum()) for n in outs)
+    assert den > 0
+    assert num / den < 1e-3, num / den
