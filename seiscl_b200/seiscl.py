@@ -128,9 +128,10 @@ class SeisCL:
         Accepted for compatibility but without effect on a single CUDA
         device: ``with_docker``, ``with_mpi``, ``NP``, ``pref_device_type``,
         ``MPI_NPROC_SHOT``, ``nmax_dev``, ``no_use_GPUs`` (shots are spread
-        over ranks by ``seiscl_b200.shots`` instead). ``FP16`` selects the
-        storage of the saved boundaries: 0/1 FP32, 2/3 FP16; arithmetic is
-        FP32 in every mode."""
+        over ranks by ``seiscl_b200.shots`` instead). ``FP16`` 2 or 3 stores
+        the saved boundaries in FP16 and, for 3D forward runs, the wave fields
+        and memory variables too (power-of-two scaled, as the reference's
+        FP16=2 mode); arithmetic is FP32 in every mode."""
         try:
             engine.load_library()
         except Exception as exc:  # the engine is the only compute path
@@ -514,7 +515,8 @@ class SeisCL:
             K_MAX_CPML=float(self.K_MAX_CPML), nab=int(self.nab), abpc=float(self.abpc),
             tmin=self._steps(self.tmin), tmax=self._steps(self.tmax),
             param_type=int(self.param_type), restype=int(self.restype),
-            precision="fp16" if int(self.FP16) >= 2 else "fp32")
+            precision="fp16" if int(self.FP16) >= 2 else "fp32",
+            field_precision="fp16" if int(self.FP16) >= 2 and int(self.ND) == 3 and not self.gradout else "fp32")
 
     def _steps(self, seconds) -> int:
         """A time in seconds as a step count, FP32 quotient truncated
