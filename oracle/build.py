@@ -29,7 +29,7 @@ BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
 REF_SRC = os.environ.get("SEISCL_REF_SRC", "/root/reference/src")
 CFLAGS = ["-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-std=gnu17", "-w"]
-PORT_SOURCES = ["fdo_setup.c", "fdo_port.c", "fdo_driver.c"]
+PORT_SOURCES = ["fdo_setup.c", "fdo_port.c", "fdo_driver.c", "fdo_dft.c"]
 
 
 def _run(cmd):
@@ -92,7 +92,7 @@ def ref_defines(cfg: dict, nbnd: int, hc: list) -> list:
         "NLOCALP": 1,
         "LCOMM": 0,
         "COMM12": 0,
-        "BACK_PROP_TYPE": 1,
+        "BACK_PROP_TYPE": cfg.get("back_prop_type", 1),
         "RESTYPE": cfg.get("restype", 0),
         "HOUT": 0,
         "GRADSRCOUT": 0,
@@ -129,7 +129,7 @@ KERNELS = {
 
 def ref_key(cfg: dict) -> str:
     keys = ["nd", "nz", "ny", "nx", "fdorder", "maxrelerror", "nab", "freesurf", "abs_type", "L", "nt",
-            "dt", "dh", "restype"]
+            "dt", "dh", "restype", "back_prop_type"]
     blob = json.dumps({k: cfg.get(k) for k in keys}, sort_keys=True)
     return hashlib.sha1(blob.encode()).hexdigest()[:16]
 
@@ -165,6 +165,33 @@ def build_ref(cfg: dict, nbnd: int, hc: list) -> str:
         tmp = out + ".tmp%d" % os.getpid()
         _run(["gcc", *CFLAGS, "-shared", "-o", tmp, glue, *objs,
               *[os.path.join(HERE, s) for s in PORT_SOURCES], "-lm"])
+        os.replace(tmp, out)
+    return out
+
+
+def refcg_lib_path() -> str:
+    return os.path.join(REF_OUT, "libfdo_refcg.so")
+
+
+def build_refcg() -> str:
+    """Compile the reference's host file src/calc_grad.c (the DFT-gradient
+    assembly, OpenCL build) in place, with type-only stand-ins for the OpenCL
+    and HDF5 headers (oracle/refstub) and a glue file that fills the
+    reference's model/device structures (oracle/ref_calc_grad_glue.c)."""
+    out = refcg_lib_path()
+    if os.path.exists(out):
+        return out
+    if not ref_available():
+        raise FileNotFoundError("reference sources not found at %s" % REF_SRC)
+    os.makedirs(REF_OUT, exist_ok=True)
+    flags = [*CFLAGS, "-D__SEISCL__", "-D__NOMPI__", "-I" + os.path.join(HERE, "refstub"), "-I" + REF_SRC]
+    with tempfile.TemporaryDirectory() as td:
+        o1 = os.path.join(td, "calc_grad.o")
+        o2 = os.path.join(td, "glue.o")
+        _run(["gcc", *flags, "-c", "-o", o1, os.path.join(REF_SRC, "calc_grad.c")])
+        _run(["gcc", *flags, "-c", "-o", o2, os.path.join(HERE, "ref_calc_grad_glue.c")])
+        tmp = out + ".tmp%d" % os.getpid()
+        _run(["gcc", *CFLAGS, "-shared", "-o", tmp, o1, o2, "-lm"])
         os.replace(tmp, out)
     return out
 

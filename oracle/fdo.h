@@ -59,8 +59,10 @@ enum {
 };
 /* CPML / taper constants: per axis x,y,z: K, a, b, K_half, a_half, b_half */
 enum { C_K, C_A, C_B, C_KH, C_AH, C_BH, C_N };
-/* gradient outputs (per-parameter, in the reference's M/mu/rho basis) */
-enum { G_RHO, G_M, G_MU, G_N };
+/* gradient outputs (per-parameter, in the reference's M/mu/rho basis; the
+ * DFT gradient also fills taup and taus) */
+enum { G_RHO, G_M, G_MU, G_TAUP, G_TAUS, G_N };
+#define FDO_MAXFREQ 16
 
 typedef struct fdo_cfg {
     int nd;            /* 2 (P-SV) or 3 */
@@ -76,6 +78,9 @@ typedef struct fdo_cfg {
     float vppml, fpml, npower, k_max_cpml, abpc;
     int param_type;    /* 0: vp,vs,rho  1: M,mu,rho  2: Ip,Is,rho */
     int restype;       /* 0 or 1 (src/update_adjs2D.cl:441-470) */
+    int back_prop_type;/* 1: boundary-saving backpropagation, 2: DFT gradient */
+    int nfreqs;        /* DFT gradient: number of frequencies (<= FDO_MAXFREQ) */
+    float gradfreqs[FDO_MAXFREQ];  /* DFT gradient frequencies (Hz) */
 } fdo_cfg;
 
 /* One shot: sources and receivers, the reference's src_pos [nsrc][5] and
@@ -128,6 +133,12 @@ typedef struct fdo_state {
     int wave_ids[W_N];
     int nmem;
     int mem_ids[R_N];
+    /* DFT gradient (back_prop_type 2, src/assign_modeling_case.c:549-570) */
+    int dtnyq, ntnyq;
+    float df;
+    float gradfreqsn[FDO_MAXFREQ];
+    float *fw[2][W_N];     /* [forward, adjoint] DFT, complex [nfreqs][nvol] */
+    float *fr[2][R_N];     /* memory variables, complex [nfreqs][L*nvol] */
 } fdo_state;
 
 /* ---- setup (fdo_setup.c) ---- */
@@ -151,6 +162,11 @@ int fdo_forward(fdo_state *s, const fdo_kernels *k, const fdo_shot *shot,
 int fdo_adjoint(fdo_state *s, const fdo_kernels *k, const fdo_shot *shot,
                 const int outsel[O_N], int alltypes_mask, float *const res[O_N]);
 void fdo_zero_gradients(fdo_state *s);
+/* ---- DFT gradient (fdo_dft.c) ---- */
+void fdo_dft_factors(const fdo_state *s, int thist, float *re, float *im);
+void fdo_savefreqs(fdo_state *s, int slot, int thist);
+void fdo_zero_dft(fdo_state *s, int slot);
+void fdo_calc_grad(fdo_state *s);
 int  fdo_source_targets(int nd, int alltypes_mask, int type, int *fields, float *div);
 
 extern const fdo_kernels fdo_port_kernels;

@@ -9,6 +9,8 @@
  * varsout:  src/automatic_kernels.c:22-219
  * residuals src/automatic_kernels.c:631-836
  * gradient transform: src/calc_grad.c:975-1107
+ * DFT gradient (BACK_PROP_TYPE=2): the same loops with the transforms of
+ *   fdo_dft.c, src/time_stepping.c:766-781 (forward), :862-972 (adjoint)
  */
 #include "fdo.h"
 
@@ -154,39 +156,82 @@ void fdo_zero_gradients(fdo_state *s)
     for (int i = 0; i < G_N; i++) memset(s->grad[i], 0, sizeof(float) * s->npar);
 }
 
-int fdo_forward(fdo_state *s, const fdo_kernels *k, const fdo_shot *sh, const int outsel[O_N], int mask,
-                float *const seis[O_N], int save_boundaries)
+static void zero_psi(fdo_state *s)
 {
-    /* initialize_forward: zero wave fields, memory variables and CPML memory */
-    zero_fields(s, s->w, s->r);
     int nab = s->c.nab;
     i64 sx = 2 * (i64)nab * s->c.ny * s->c.nz, sy = (i64)s->c.nx * 2 * nab * s->c.nz,
         sz = (i64)s->c.nx * s->c.ny * 2 * nab;
     i64 psz[PS_N] = {sx, sx, sx, sy, sy, sy, sz, sz, sz, sx, sx, sx, sy, sy, sy, sz, sz, sz};
     for (int i = 0; i < PS_N; i++)
         if (s->psi[i]) memset(s->psi[i], 0, sizeof(float) * psz[i]);
+}
+
+int fdo_forward(fdo_state *s, const fdo_kernels *k, const fdo_shot *sh, const int outsel[O_N], int mask,
+                float *const seis[O_N], int save_boundaries)
+{
+    /* initialize_forward: zero wave fields, memory variables and CPML memory */
+    zero_fields(s, s->w, s->r);
+    zero_psi(s);
     for (int o = 0; o < O_N; o++)
         if (outsel[o]) memset(seis[o], 0, sizeof(float) * (i64)s->c.nt * sh->nrec);
-    if (save_boundaries) {
+    /* a gradient run keeps the boundary shells (BACK_PROP_TYPE 1) or the
+     * forward transforms (2) */
+    int dft = save_boundaries && s->c.back_prop_type == 2;
+    int bnd = save_boundaries && !dft;
+    if (bnd) {
         for (int q = 0; q < s->nwave; q++) {
             int w = s->wave_ids[q];
             if (!s->bnd[w]) s->bnd[w] = calloc((size_t)s->c.nt * s->nbnd + 1, sizeof(float));
         }
     }
+    if (dft) fdo_zero_dft(s, 0);
     for (int t = 0; t < s->c.tmax; t++) {
+        /* the state after t steps, before the sources of step t */
+        if (dft && t >= s->c.tmin && (t - s->c.tmin) % s->dtnyq == 0) fdo_savefreqs(s, 0, (t - s->c.tmin) / s->dtnyq);
         inject_sources(s, sh, mask, t, 1);
         k->update_v(s);
         k->update_s(s);
-        if (save_boundaries) k->savebnd(s, t);
+        if (bnd) k->savebnd(s, t);
         if (s->c.freesurf) k->surface(s, 1);
         record(s, sh, outsel, seis, t);
     }
     return 0;
 }
 
+/* DFT adjoint (src/time_stepping.c:621-680 and :862-972 with
+ * BACK_PROP_TYPE=2): the adjoint kernels' "r" arguments are bound to the
+ * forward buffers (src/clprogram.c:869-880), which start from zero together
+ * with the CPML memory; no boundary injection, no source removal; the
+ * adjoint fields are transformed at the forward's sampling times and the
+ * gradient is assembled from both transforms at the end. */
+static int adjoint_dft(fdo_state *s, const fdo_kernels *k, const fdo_shot *sh, const int outsel[O_N],
+                       float *const res[O_N])
+{
+    float *wr_keep[W_N], *rr_keep[R_N];
+    memcpy(wr_keep, s->wr, sizeof wr_keep);
+    memcpy(rr_keep, s->rr, sizeof rr_keep);
+    memcpy(s->wr, s->w, sizeof wr_keep);
+    memcpy(s->rr, s->r, sizeof rr_keep);
+    zero_fields(s, s->w, s->r);
+    zero_psi(s);
+    fdo_zero_dft(s, 1);
+    for (int t = s->c.tmax - 1; t > s->c.tmin; t--) {
+        if (s->c.freesurf) k->surface_adj(s);
+        inject_residuals(s, sh, outsel, res, t);
+        k->update_adjs(s);
+        k->update_adjv(s);
+        if ((t - s->c.tmin) % s->dtnyq == 0) fdo_savefreqs(s, 1, (t - s->c.tmin) / s->dtnyq);
+    }
+    fdo_calc_grad(s);
+    memcpy(s->wr, wr_keep, sizeof wr_keep);
+    memcpy(s->rr, rr_keep, sizeof rr_keep);
+    return 0;
+}
+
 int fdo_adjoint(fdo_state *s, const fdo_kernels *k, const fdo_shot *sh, const int outsel[O_N], int mask,
                 float *const res[O_N])
 {
+    if (s->c.back_prop_type == 2) return adjoint_dft(s, k, sh, outsel, res);
     /* initialize_adj: adjoint fields and memory variables start at zero; the
      * CPML memory keeps the forward run's final values (the adjoint kernels
      * bind the forward psi buffers by name, src/clprogram.c:806-811). */
@@ -288,6 +333,28 @@ void fdo_get_grad(void *hp, float *gvp, float *gvs, float *grho, float *rawM, fl
     if (rawrho) memcpy(rawrho, h->s.grad[G_RHO], n * sizeof(float));
 }
 void fdo_clear_grad(void *hp) { fdo_zero_gradients(&((fdo_handle *)hp)->s); }
+/* the accumulators as they are: rho, M, mu, taup, taus (G_* order) */
+void fdo_get_grad_raw(void *hp, float **out)
+{
+    fdo_handle *h = hp;
+    for (int i = 0; i < G_N; i++)
+        if (out[i]) memcpy(out[i], h->s.grad[i], h->s.npar * sizeof(float));
+}
+/* DFT of slot (0 forward, 1 adjoint): kind 0 wave field, 1 memory variable */
+float *fdo_dft_array(void *hp, int slot, int kind, int id)
+{
+    fdo_state *s = &((fdo_handle *)hp)->s;
+    return kind == 0 ? s->fw[slot][id] : s->fr[slot][id];
+}
+/* dtnyq, ntnyq and df of a DFT-gradient state; gradfreqsn into fn */
+void fdo_dft_info(void *hp, int *ni, float *df, float *fn)
+{
+    fdo_state *s = &((fdo_handle *)hp)->s;
+    ni[0] = s->dtnyq; ni[1] = s->ntnyq; *df = s->df;
+    for (int j = 0; j < s->c.nfreqs; j++) fn[j] = s->gradfreqsn[j];
+}
+/* assemble the gradient from the transforms now held (for the pin) */
+void fdo_run_calc_grad(void *hp) { fdo_calc_grad(&((fdo_handle *)hp)->s); }
 
 /* Access to internal arrays for field-level comparisons.  kind: 0 wave,
  * 1 adjoint wave, 2 memory, 3 adjoint memory, 4 psi, 5 param, 6 cpml x,

@@ -767,6 +767,9 @@ static void port_savebnd(fdo_state *s, int t)
 static void port_update_adjv2d(fdo_state *s)
 {
     const fdo_cfg *c = &s->c;
+    /* BACK_PROP_TYPE 2 compiles out the forward reconstruction, the
+     * boundary injection and the gradient (#if BACK_PROP_TYPE==1 blocks) */
+    const int bp1 = c->back_prop_type != 2;
     int F = c->fdoh, NZ = s->NZp, NX = s->NXp, nz = c->nz;
     const double *hc = s->hc;
     float *vx = s->w[W_VX], *vz = s->w[W_VZ];
@@ -789,12 +792,14 @@ static void port_update_adjv2d(fdo_state *s)
             float sxz_xr = dbw(sxzr, iv, NZ, hc, F);
             float lvx = ((sxx_x + sxz_z) * rip[ip]);
             float lvz = ((szz_z + sxz_x) * rkp[ip]);
-            vx[iv] -= lvx;
-            vz[iv] -= lvz;
-            int m = inject_ind2d(s, gz, gx);
-            if (m != -1) {
-                vx[iv] = s->bnd_cur[W_VX][m];
-                vz[iv] = s->bnd_cur[W_VZ][m];
+            if (bp1) {
+                vx[iv] -= lvx;
+                vz[iv] -= lvz;
+                int m = inject_ind2d(s, gz, gx);
+                if (m != -1) {
+                    vx[iv] = s->bnd_cur[W_VX][m];
+                    vz[iv] = s->bnd_cur[W_VZ][m];
+                }
             }
             if (c->abs_type == 1) cpml_v2d(s, gz, gx, &sxx_xr, &szz_zr, &sxz_xr, &sxz_zr);
             lvx = ((sxx_xr + sxz_zr) * rip[ip]);
@@ -805,13 +810,16 @@ static void port_update_adjv2d(fdo_state *s)
                 float *f[2] = {vxr, vzr};
                 taper2d(s, gz, gx, f, 2, iv);
             }
-            gradrho[ip] += -vx[iv] * lvx - vz[iv] * lvz;
+            if (bp1) gradrho[ip] += -vx[iv] * lvx - vz[iv] * lvz;
         }
 }
 
 static void port_update_adjs2d(fdo_state *s)
 {
     const fdo_cfg *c = &s->c;
+    /* BACK_PROP_TYPE 2 compiles out the forward reconstruction, the
+     * boundary injection and the gradient (#if BACK_PROP_TYPE==1 blocks) */
+    const int bp1 = c->back_prop_type != 2;
     int F = c->fdoh, NZ = s->NZp, NX = s->NXp, nz = c->nz, L = c->L;
     const double *hc = s->hc;
     const double DT = s->DT, DT2 = s->DT2;
@@ -851,8 +859,9 @@ static void port_update_adjs2d(fdo_state *s)
                 d = 2.0 * lmu * ltaus / DT;
                 e = lM * ltaup / DT;
             }
-            /* reconstruct the forward stresses */
-            if (L == 0) {
+            /* reconstruct the forward stresses (BACK_PROP_TYPE 1 only) */
+            if (!bp1) {
+            } else if (L == 0) {
                 sxz[iv] -= (fipkp * (vxz + vzx));
                 sxx[iv] -= (g * (vxx + vzz)) - (f * vzz);
                 szz[iv] -= (g * (vxx + vzz)) - (f * vxx);
@@ -880,7 +889,7 @@ static void port_update_adjs2d(fdo_state *s)
                 sxx[iv] -= lsxx + (DT2 * sumrxx);
                 szz[iv] -= lszz + (DT2 * sumrzz);
             }
-            int m = inject_ind2d(s, gz, gx);
+            int m = bp1 ? inject_ind2d(s, gz, gx) : -1;
             if (m != -1) {
                 sxx[iv] = s->bnd_cur[W_SXX][m];
                 szz[iv] = s->bnd_cur[W_SZZ][m];
@@ -925,7 +934,8 @@ static void port_update_adjs2d(fdo_state *s)
                 float *fl[3] = {sxzr, sxxr, szzr};
                 taper2d(s, gz, gx, fl, 3, iv);
             }
-            if (c->restype == 0) {
+            if (!bp1) {
+            } else if (c->restype == 0) {
                 float c1 = 1.0 / ((2.0 * lM - 2.0 * lmu) * (2.0 * lM - 2.0 * lmu));
                 float c3 = 1.0 / (lmu * lmu);
                 float c5 = 0.25 * c3;
@@ -985,6 +995,9 @@ static void port_surface_adj2d(fdo_state *s)
 static void port_update_adjv3d(fdo_state *s)
 {
     const fdo_cfg *c = &s->c;
+    /* BACK_PROP_TYPE 2 compiles out the forward reconstruction, the
+     * boundary injection and the gradient (#if BACK_PROP_TYPE==1 blocks) */
+    const int bp1 = c->back_prop_type != 2;
     int F = c->fdoh, NZ = s->NZp, NY = s->NYp, NX = s->NXp;
     i64 nz = c->nz, ny = c->ny;
     const double *hc = s->hc;
@@ -1023,10 +1036,12 @@ static void port_update_adjv3d(fdo_state *s)
                 float lvx = ((sxx_x + sxy_y + sxz_z) * rip[ip]);
                 float lvy = ((syy_y + sxy_x + syz_z) * rjp[ip]);
                 float lvz = ((szz_z + sxz_x + syz_y) * rkp[ip]);
-                vx[iv] -= lvx;
-                vy[iv] -= lvy;
-                vz[iv] -= lvz;
-                int m = inject_ind3d(s, gz, gy, gx);
+                if (bp1) {
+                    vx[iv] -= lvx;
+                    vy[iv] -= lvy;
+                    vz[iv] -= lvz;
+                }
+                int m = bp1 ? inject_ind3d(s, gz, gy, gx) : -1;
                 if (m != -1) {
                     vx[iv] = s->bnd_cur[W_VX][m];
                     vy[iv] = s->bnd_cur[W_VY][m];
@@ -1045,13 +1060,16 @@ static void port_update_adjv3d(fdo_state *s)
                     float *f[3] = {vxr, vyr, vzr};
                     taper3d(s, gz, gy, gx, f, 3, iv);
                 }
-                gradrho[ip] += -vx[iv] * lvx - vy[iv] * lvy - vz[iv] * lvz;
+                if (bp1) gradrho[ip] += -vx[iv] * lvx - vy[iv] * lvy - vz[iv] * lvz;
             }
 }
 
 static void port_update_adjs3d(fdo_state *s)
 {
     const fdo_cfg *c = &s->c;
+    /* BACK_PROP_TYPE 2 compiles out the forward reconstruction, the
+     * boundary injection and the gradient (#if BACK_PROP_TYPE==1 blocks) */
+    const int bp1 = c->back_prop_type != 2;
     int F = c->fdoh, NZ = s->NZp, NY = s->NYp, NX = s->NXp, L = c->L;
     i64 nz = c->nz, ny = c->ny;
     const double *hc = s->hc;
@@ -1106,7 +1124,8 @@ static void port_update_adjs3d(fdo_state *s)
                 }
                 float vxyyx = vxy + vyx, vyzzy = vyz + vzy, vxzzx = vxz + vzx;
                 float vxxyyzz = vxx + vyy + vzz, vyyzz = vyy + vzz, vxxzz = vxx + vzz, vxxyy = vxx + vyy;
-                if (L == 0) {
+                if (!bp1) {
+                } else if (L == 0) {
                     sxy[iv] -= (fipjp * vxyyx);
                     syz[iv] -= (fjpkp * vyzzy);
                     sxz[iv] -= (fipkp * vxzzx);
@@ -1148,7 +1167,7 @@ static void port_update_adjs3d(fdo_state *s)
                     syy[iv] -= lsyy + (DT2 * a5);
                     szz[iv] -= lszz + (DT2 * a6);
                 }
-                int m = inject_ind3d(s, gz, gy, gx);
+                int m = bp1 ? inject_ind3d(s, gz, gy, gx) : -1;
                 if (m != -1) {
                     sxx[iv] = s->bnd_cur[W_SXX][m];
                     syy[iv] = s->bnd_cur[W_SYY][m];
@@ -1211,7 +1230,8 @@ static void port_update_adjs3d(fdo_state *s)
                     float *fl[6] = {sxyr, syzr, sxzr, sxxr, syyr, szzr};
                     taper3d(s, gz, gy, gx, fl, 6, iv);
                 }
-                if (c->restype == 0) {
+                if (!bp1) {
+                } else if (c->restype == 0) {
                     float c1 = 1.0 / (3.0 * lM - 4.0 * lmu) / (3.0 * lM - 4.0 * lmu);
                     float c3 = 1.0 / lmu / lmu;
                     float c5 = 1.0 / 6.0 * c3;

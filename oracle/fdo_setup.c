@@ -235,6 +235,25 @@ int fdo_state_init(fdo_state *s, const fdo_cfg *c)
     for (int l = 0; l < c->L; l++) s->eta[l] = (2.0 * FDO_PI * c->fl[l]) * c->dt; /* :536-548 */
 
     s->nbnd = nbnd_count(&s->c);
+
+    if (c->back_prop_type == 2) {
+        /* DFT gradient frequencies, src/assign_modeling_case.c:549-570 */
+        if (c->nfreqs < 1 || c->nfreqs > FDO_MAXFREQ) return 4;
+        float fmaxout = 0;
+        for (int j = 0; j < c->nfreqs; j++)
+            if (c->gradfreqs[j] > fmaxout) fmaxout = c->gradfreqs[j];
+        if (!(fmaxout > 0)) return 4;
+        s->dtnyq = (int)ceil(0.0156 / fmaxout / c->dt);
+        s->ntnyq = (s->c.tmax - s->c.tmin) / s->dtnyq + 1;
+        s->df = 1.0 / s->ntnyq / c->dt / s->dtnyq;
+        for (int j = 0; j < c->nfreqs; j++) s->gradfreqsn[j] = floor(c->gradfreqs[j] / s->df);
+        for (int slot = 0; slot < 2; slot++) {
+            for (int i = 0; i < s->nwave; i++) s->fw[slot][s->wave_ids[i]] = zalloc(2 * c->nfreqs * s->nvol);
+            if (c->L > 0)
+                for (int i = 0; i < s->nmem; i++)
+                    s->fr[slot][s->mem_ids[i]] = zalloc(2 * c->nfreqs * s->nvol * c->L);
+        }
+    }
     return 0;
 }
 
@@ -246,6 +265,10 @@ void fdo_state_free(fdo_state *s)
     for (int i = 0; i < P_N; i++) free(s->p[i]);
     for (int i = 0; i < C_N; i++) { free(s->cx[i]); free(s->cy[i]); free(s->cz[i]); }
     for (int i = 0; i < G_N; i++) free(s->grad[i]);
+    for (int slot = 0; slot < 2; slot++) {
+        for (int i = 0; i < W_N; i++) free(s->fw[slot][i]);
+        for (int i = 0; i < R_N; i++) free(s->fr[slot][i]);
+    }
     free(s->taper);
     free(s->eta);
     memset(s, 0, sizeof *s);

@@ -38,12 +38,13 @@ class fdo_cfg(C.Structure):
                 ("dt", C.c_float), ("dh", C.c_float), ("f0", C.c_float), ("fl", C.c_float * 8),
                 ("vppml", C.c_float), ("fpml", C.c_float), ("npower", C.c_float),
                 ("k_max_cpml", C.c_float), ("abpc", C.c_float),
-                ("param_type", C.c_int), ("restype", C.c_int)]
+                ("param_type", C.c_int), ("restype", C.c_int), ("back_prop_type", C.c_int),
+                ("nfreqs", C.c_int), ("gradfreqs", C.c_float * 16)]
 
 
 DEFAULTS = dict(nd=2, ny=1, fdorder=8, maxrelerror=1, nab=16, freesurf=0, abs_type=1, L=0, tmin=0,
                 tmax=0, f0=15.0, fl=(15.0,), vppml=3500.0, fpml=15.0, npower=2.0, k_max_cpml=2.0,
-                abpc=6.0, param_type=0, restype=0)
+                abpc=6.0, param_type=0, restype=0, back_prop_type=1, gradfreqs=())
 
 
 def make_cfg(cfg: dict) -> fdo_cfg:
@@ -61,6 +62,13 @@ def make_cfg(cfg: dict) -> fdo_cfg:
     fl = list(np.atleast_1d(d["fl"]).astype(float))
     for i in range(8):
         c.fl[i] = fl[i] if i < len(fl) else 0.0
+    c.back_prop_type = int(d.get("back_prop_type", 1))
+    gf = [float(v) for v in np.atleast_1d(d.get("gradfreqs", ())).ravel()]
+    if len(gf) > 16:
+        raise ValueError("at most 16 DFT gradient frequencies")
+    c.nfreqs = len(gf)
+    for i, v in enumerate(gf):
+        c.gradfreqs[i] = v
     return c
 
 
@@ -77,6 +85,11 @@ def _lib(path):
     lib.fdo_run_adjoint.argtypes = [P, C.c_int, FP, FP, C.c_int, FP, C.POINTER(C.c_int), C.c_int,
                                     C.POINTER(FP)]
     lib.fdo_get_grad.argtypes = [P, FP, FP, FP, FP, FP, FP]
+    lib.fdo_get_grad_raw.argtypes = [P, C.POINTER(FP)]
+    lib.fdo_dft_array.restype = FP
+    lib.fdo_dft_array.argtypes = [P, C.c_int, C.c_int, C.c_int]
+    lib.fdo_dft_info.argtypes = [P, C.POINTER(C.c_int), FP, FP]
+    lib.fdo_run_calc_grad.argtypes = [P]
     lib.fdo_clear_grad.argtypes = [P]
     lib.fdo_array.restype = FP
     lib.fdo_array.argtypes = [P, C.c_int, C.c_int]
@@ -226,6 +239,43 @@ class Oracle:
     def clear_gradients(self):
         self.lib.fdo_clear_grad(self.h)
 
+    def raw_gradients(self) -> dict:
+        """The float accumulators as they are (no transf_grad): M, mu, rho,
+        taup, taus.  For the DFT gradient these are already in the
+        param_type basis (calc_grad.c applies the chain rule itself)."""
+        g = [np.zeros(self.npar, np.float32) for _ in range(5)]
+        ptrs = (C.POINTER(C.c_float) * 5)(*[_fptr(a) for a in g])
+        self.lib.fdo_get_grad_raw(self.h, ptrs)
+        sh = self.shape
+        return {"rho": g[0].reshape(sh), "M": g[1].reshape(sh), "mu": g[2].reshape(sh),
+                "taup": g[3].reshape(sh), "taus": g[4].reshape(sh)}
+
+    def dft_info(self) -> dict:
+        """DTNYQ, NTNYQ, df and gradfreqsn of a DFT-gradient state
+        (src/assign_modeling_case.c:549-570)."""
+        ni = (C.c_int * 2)()
+        df = C.c_float(0)
+        fn = np.zeros(16, np.float32)
+        self.lib.fdo_dft_info(self.h, ni, C.byref(df), _fptr(fn))
+        nf = len(np.atleast_1d(self.cfg.get("gradfreqs", ())))
+        return {"dtnyq": ni[0], "ntnyq": ni[1], "df": df.value, "gradfreqsn": fn[:nf].copy()}
+
+    def dft(self, slot: int, kind: str, name: str):
+        """View (not a copy) of the complex DFT of a wave field ("wave") or a
+        memory variable ("mem"): [nfreqs][(L)][nvol] complex64, slot 0
+        forward, 1 adjoint; None when absent."""
+        k, i = (0, WAVE_IDS[name]) if kind == "wave" else (1, MEM_IDS[name])
+        p = self.lib.fdo_dft_array(self.h, slot, k, i)
+        if not p:
+            return None
+        nf = len(np.atleast_1d(self.cfg.get("gradfreqs", ())))
+        n = nf * self.nvol * (self.cfg["L"] if kind == "mem" else 1)
+        return np.ctypeslib.as_array(p, shape=(2 * int(n),)).view(np.complex64)
+
+    def calc_grad(self):
+        """Assemble the DFT gradient from the transforms now held."""
+        self.lib.fdo_run_calc_grad(self.h)
+
     def array(self, kind: str, name: str) -> np.ndarray:
         """Copy of an internal array (for field-level comparisons)."""
         c = self.cfg
@@ -309,3 +359,48 @@ def holberg(fdorder: int, maxrelerror: int):
     if port_lib().fdo_holberg(fdorder, maxrelerror, hc):
         raise ValueError("bad FD order / error level")
     return list(hc)
+
+
+DFT_VARS = ["vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "syz", "sxz", "rxx", "ryy", "rzz", "rxy", "ryz", "rxz"]
+
+
+def ref_calc_grad(o: Oracle, fwd=None, adj=None) -> dict:
+    """The reference's own calc_grad (src/calc_grad.c compiled in place,
+    oracle/_ref) applied to copies of the transforms that `o` holds (or to
+    the given {name: complex array} dicts), starting from zero gradients.
+    Returns M, mu, rho, taup, taus as the reference's float host arrays."""
+    lib = C.CDLL(_build.build_refcg())
+    FP = C.POINTER(C.c_float)
+    lib.refcg_run.argtypes = [C.c_int] * 10 + [C.c_float, C.c_float, FP, FP] + [C.POINTER(FP)] * 4
+    c = o.cfg
+    keep = []
+
+    def buf(slot, given, name):
+        if given is not None:
+            a = given.get(name)
+        else:
+            a = o.dft(slot, "wave" if name in WAVE_IDS else "mem", name)
+        if a is None:
+            return None
+        a = np.array(a, np.complex64, copy=True)
+        keep.append(a)
+        return a.view(np.float32).ctypes.data_as(FP)
+
+    fw = (FP * 15)(*[buf(0, fwd, n) for n in DFT_VARS])
+    ad = (FP * 15)(*[buf(1, adj, n) for n in DFT_VARS])
+    L = int(c["L"])
+    pars = [o.array("param", k) for k in ("M", "mu", "rho", "taup", "taus")]
+    grads = [np.zeros(o.npar, np.float32) for _ in range(5)]
+    pp = (FP * 5)(*[_fptr(p) for p in pars])
+    gp = (FP * 5)(*[_fptr(g) for g in grads])
+    info = o.dft_info()
+    fl = np.zeros(8, np.float32)
+    fl[:L] = np.atleast_1d(c["fl"])[:L]
+    fn = np.ascontiguousarray(info["gradfreqsn"], np.float32)
+    rc = lib.refcg_run(c["nd"], c["nz"], c["ny"], c["nx"], c["fdorder"], L, int(c["param_type"]), len(fn),
+                       info["ntnyq"], info["dtnyq"], float(c["dt"]), float(c["f0"]), _fptr(fl), _fptr(fn), fw, ad, pp,
+                       gp)
+    if rc:
+        raise RuntimeError("reference calc_grad failed (%d)" % rc)
+    sh = o.shape
+    return {k: g.reshape(sh) for k, g in zip(("M", "mu", "rho", "taup", "taus"), grads)}

@@ -49,7 +49,11 @@ def _run(kw, ref=False):
     return cfg, model, acq, d, o.gradients(), o
 
 
-@pytest.mark.parametrize("name", sorted(INDEX))
+TIME_CASES = sorted(k for k, v in INDEX.items() if "extra" not in v)
+DFT_CASES = sorted(k for k, v in INDEX.items() if "extra" in v)
+
+
+@pytest.mark.parametrize("name", TIME_CASES)
 def test_port_reproduces_golden(name):
     entry = INDEX[name]
     cfg, model, acq, d, g, _ = _run(entry["kwargs"])
@@ -63,6 +67,35 @@ def test_port_reproduces_golden(name):
         else:
             v64 = v.astype(np.float64)
             assert np.array_equal(np.array([v64.sum(), (v64 * v64).sum(), np.abs(v64).max()]), gold["gradsum_" + k]), k
+
+
+@pytest.mark.parametrize("name", DFT_CASES)
+def test_port_reproduces_dft_golden(name):
+    """DFT gradient (BACK_PROP_TYPE=2): seismograms and transforms bit for bit
+    (the reference's adjoint kernels compiled with BACK_PROP_TYPE=2); the
+    gradient within 1e-6 of the reference's calc_grad (src/calc_grad.c, whose
+    float/double mix the restatement follows up to the order of a few
+    products)."""
+    from tests.golden.make_golden import run_dft
+
+    entry = INDEX[name]
+    cfg, model, acq, d, g, sums = run_dft(entry["kwargs"], entry["extra"], ref=False)
+    assert _input_hash(model, acq) == entry["input_sha256"]
+    gold = np.load(os.path.join(GOLD, name + ".npz"))
+    for k, v in d.items():
+        assert np.array_equal(v, gold["seis_" + k]), k
+    for k, v in sums.items():
+        assert np.array_equal(v, gold[k]), k
+    for k, v in g.items():
+        if cfg["nd"] == 2:
+            ref = gold["grad_" + k]
+            scale = np.abs(ref).max()
+            assert np.abs(v - ref).max() <= 1e-6 * scale, k
+        else:
+            v64 = v.astype(np.float64)
+            got = np.array([v64.sum(), (v64 * v64).sum(), np.abs(v64).max()])
+            ref = gold["gradsum_" + k]
+            assert np.allclose(got, ref, rtol=1e-5, atol=1e-6 * abs(ref[2]) * v.size), k
 
 
 def _ref_available():
@@ -152,3 +185,53 @@ def test_boundary_shell_maps_are_inverse(nd, freesurf):
                     count += 1
                     assert (x, y, z) in seen
     assert count == len(seen)
+
+
+DFT_LIVE = [
+    (dict(nd=2, freesurf=1, L=0, nt=120, seed=1), [10.0, 18.0, 25.0]),
+    (dict(nd=2, freesurf=0, L=2, nt=120, seed=2), [10.0, 18.0, 25.0]),
+    (dict(nd=3, freesurf=0, L=1, nz=30, ny=28, nx=32, nt=60, nab=6, seed=5, src_type=1), [20.0, 35.0]),
+    (dict(nd=3, freesurf=1, L=0, nz=30, ny=28, nx=32, nt=60, nab=6, seed=6, src_type=2), [20.0, 35.0]),
+]
+
+
+@pytest.mark.skipif(not _ref_available(), reason="reference tree not present")
+@pytest.mark.parametrize("param_type", [0, 1, 2])
+@pytest.mark.parametrize("case", DFT_LIVE, ids=lambda c: "nd%d-L%d" % (c[0]["nd"], c[0]["L"]))
+def test_dft_gradient_matches_reference_build(case, param_type):
+    """BACK_PROP_TYPE=2 against the reference: the adjoint kernels compiled
+    with BACK_PROP_TYPE=2 give the same transforms bit for bit; the oracle's
+    calc_grad agrees with the reference's compiled calc_grad."""
+    from oracle.oracle import ref_calc_grad
+    from tests.golden.make_golden import DFT_NAMES
+
+    kw, freqs = case
+    extra = dict(back_prop_type=2, gradfreqs=freqs, param_type=param_type)
+    got = []
+    for ref in (False, True):
+        from tests.golden.make_golden import model_inputs
+        from oracle.oracle import Oracle
+
+        cfg, model, acq = make_case(**kw)
+        cfg.update(extra)
+        o = Oracle(cfg, ref=ref)
+        a, b, rho = model_inputs(model, param_type)
+        assert o.set_model(a, b, rho, model["taup"], model["taus"]) == 0
+        outs = ["vx", "vy", "vz"] if cfg["nd"] == 3 else ["vx", "vz"]
+        d = o.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs, save_boundaries=True)
+        o.clear_gradients()
+        o.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], {k: (0.3 * v).astype(np.float32) for k, v in d.items()})
+        got.append((o, o.raw_gradients()))
+    (o0, g0), (o1, g1) = got
+    for slot in (0, 1):
+        for n in DFT_NAMES:
+            a = o0.dft(slot, "wave", n)
+            if a is not None:
+                assert np.array_equal(a, o1.dft(slot, "wave", n)), (slot, n)
+    for k in g0:
+        assert np.array_equal(g0[k], g1[k]), k
+    gr = ref_calc_grad(o0)
+    for k in gr:
+        scale = np.abs(gr[k]).max()
+        assert np.isfinite(g0[k]).all(), k
+        assert np.abs(g0[k] - gr[k]).max() <= 1e-6 * scale, k
