@@ -13,9 +13,13 @@
  *   - sfd_forward replaces the forward half of
  *     int time_stepping(model*, device**, struct filenames)
  *     (src/time_stepping.c:692, loop at :747-860);
- *   - sfd_adjoint replaces its gradient half (src/time_stepping.c:862-940)
- *     for BACK_PROP_TYPE=1 (boundary-saving reconstruction);
- *   - sfd_get_gradient replaces transf_grad (src/calc_grad.c:975-1107).
+ *   - sfd_adjoint replaces its gradient half (src/time_stepping.c:862-972)
+ *     for BACK_PROP_TYPE=1 (boundary-saving reconstruction) and
+ *     BACK_PROP_TYPE=2 (DFT gradient, with calc_grad, src/calc_grad.c:376-960);
+ *   - sfd_set_gradfreqs replaces the gradfreqs/gradfreqsn set-up
+ *     (src/read_hdf5.c:546-549, src/assign_modeling_case.c:549-570);
+ *   - sfd_get_gradient replaces transf_grad (src/calc_grad.c:975-1107) and
+ *     the gradient output of src/writehdf5.c:262-275.
  *
  * Layout conventions are the reference host's (src/read_hdf5.c:606-625):
  * model parameters are [nx][ny][nz] (3D) or [nx][nz] (2D) with z fastest;
@@ -90,7 +94,9 @@ typedef struct sfd_config {
                               only; arithmetic stays FP32).  No reference counterpart
                               in this form: the reference's FP16=2 mode also scales
                               by powers of two (src/assign_modeling_case.c:829-866). */
-    int reserved[4];
+    int back_prop_type;    /* BACK_PROP_TYPE: 0 or 1 boundary-saving backpropagation,
+                              2 DFT gradient at the frequencies of sfd_set_gradfreqs */
+    int reserved[3];
 } sfd_config;
 
 typedef struct sfd_shot {
@@ -128,17 +134,42 @@ int sfd_forward(sfd_plan *plan, const sfd_shot *shot, int srctype_mask, const in
 
 /* Adjoint of the shot last run by sfd_forward(save_boundaries=1):
  * residuals[k] are [nrec][NT] host arrays already scaled as adjoint sources
- * (see sfd_residual_scale); gradients accumulate in FP64 on the device. */
+ * (see sfd_residual_scale); gradients accumulate in FP64 on the device.
+ * With back_prop_type 2 the adjoint runs from zeroed fields without
+ * reconstructing the forward field (src/time_stepping.c:862-972), its
+ * transforms are taken at the forward's sampling times, and the shot's
+ * gradient is assembled from both (calc_grad, src/calc_grad.c:376-960). */
 int sfd_adjoint(sfd_plan *plan, const sfd_shot *shot, int srctype_mask, const int *outsel,
                 const float *const *residuals, void *stream);
 
 /* Zero the gradient accumulators (gradinit, automatic_kernels.c:840-930). */
 int sfd_zero_gradient(sfd_plan *plan);
 
-/* Gradients [nx][ny][nz] as floats: transformed (transform=1: gradvp,
- * gradvs, gradrho for param_type 0, calc_grad.c:975-1107) or raw
- * (transform=0: grad M, grad mu, grad rho of the stored parameters). */
+/* Gradients [nx][ny][nz] as floats.  back_prop_type 1: transformed
+ * (transform=1: gradvp, gradvs, gradrho for param_type 0, calc_grad.c:975-1107)
+ * or raw (transform=0: grad M, grad mu, grad rho of the stored parameters).
+ * back_prop_type 2: the accumulated DFT gradient of the param_type's three
+ * parameters, which calc_grad already expresses in that parametrisation (the
+ * reference applies no transf_grad there, time_stepping.c:976-1002);
+ * `transform` is ignored. */
 int sfd_get_gradient(sfd_plan *plan, int transform, float *g0, float *g1, float *g2);
+
+/* ---- DFT gradient (BACK_PROP_TYPE=2) ----
+ *
+ * Frequencies (Hz, 1..16 values) of the DFT gradient of a plan created with
+ * back_prop_type 2: DTNYQ = ceil(0.0156 / max(freqs) / dt), NTNYQ =
+ * (tmax - tmin) / DTNYQ + 1, df = 1 / (NTNYQ dt DTNYQ), and each frequency
+ * is taken at bin floor(f / df) (src/assign_modeling_case.c:549-570).  A
+ * bin of 0 Hz makes calc_grad divide by zero, as in the reference.  Device
+ * memory for the transforms (2 x nfreqs x 8 bytes per wave-field cell, and
+ * per memory-variable cell) is allocated by the next gradient forward run.
+ * info (may be NULL) receives DTNYQ, NTNYQ. */
+int sfd_set_gradfreqs(sfd_plan *plan, const float *freqs, int nfreqs, int *info);
+
+/* Gradients of the relaxation parameters taup and taus [nx][ny][nz], filled
+ * by the DFT gradient of viscoelastic plans (src/calc_grad.c:729-739); zero
+ * otherwise, as the reference leaves them. */
+int sfd_get_gradient_q(sfd_plan *plan, float *gtaup, float *gtaus);
 
 /* res_scale (residuals.c:452-568): scale residuals in place into adjoint
  * sources.  res[k] are [nrec][NT] host arrays for the selected outputs. */
@@ -210,8 +241,10 @@ int sfd_plan_uses_tma(const sfd_plan *plan);
 
 /* Copy a device array of the plan to the host (tests): kind 0 wave field,
  * 1 adjoint wave field, 2 memory variable, 3 transformed parameter,
- * 4 CPML constants of axis id (6 arrays of 2*nab), 5 psi array.  Returns the
- * number of floats written, or a negative error. */
+ * 4 CPML constants of axis id (6 arrays of 2*nab), 5 psi array, 6/7 forward/
+ * adjoint DFT of wave field id and 8/9 of memory variable id (interleaved
+ * complex, [nfreqs][(L)][padded cells]).  Returns the number of floats
+ * written, or a negative error. */
 int64_t sfd_debug_copy(sfd_plan *plan, int kind, int id, float *dst, int64_t cap);
 
 /* Kernel timing for benchmarks: runs the velocity update, the stress update

@@ -262,20 +262,24 @@ int alloc_adjoint(sfd_plan *p)
     const Grid &g = p->g;
     cudaError_t e;
     if (p->a.grad[0]) return SFD_OK;
+    // the DFT adjoint runs in the forward buffers (no separate adjoint fields)
+    const bool bp2 = p->cfg.back_prop_type == 2;
     for (int w = 0; w < NW; w++) {
         p->a.wr[w] = nullptr;
-        if (!is_wave_used(g, w)) continue;
+        if (bp2 || !is_wave_used(g, w)) continue;
         p->a.wr[w] = (float *)dalloc(p, sizeof(float) * g.nvol, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "adjoint field allocation failed");
     }
     for (int r = 0; r < NR; r++) {
         p->a.rr[r] = nullptr;
-        if (!is_mem_used(g, r)) continue;
+        if (bp2 || !is_mem_used(g, r)) continue;
         p->a.rr[r] = (float *)dalloc(p, sizeof(float) * g.nvol * g.L, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "adjoint memory-variable allocation failed");
     }
     int64_t npar = (int64_t)g.nz * g.ny * g.nx;
     for (int k = 0; k < NG; k++) {
+        p->a.grad[k] = nullptr;
+        if ((k == GTAUP || k == GTAUS) && !(bp2 && g.L > 0)) continue;
         p->a.grad[k] = (double *)dalloc(p, sizeof(double) * npar, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "gradient allocation failed");
         CKC(cudaMemset(p->a.grad[k], 0, sizeof(double) * npar));
@@ -283,6 +287,142 @@ int alloc_adjoint(sfd_plan *p)
     int64_t nq = (int64_t)g.nx * g.ny;
     p->d_surf_q = (float *)dalloc(p, sizeof(float) * nq, &e);
     if (e) return fail(p, SFD_ERR_MEMORY, "scratch allocation failed");
+    return SFD_OK;
+}
+
+// ---------------------------------------------------------- DFT gradient
+constexpr double PI_D = 3.141592653589793238462643383279502884197169;
+
+void free_dft(sfd_plan *p)
+{
+    for (int s = 0; s < 2; s++) {
+        for (int w = 0; w < NW; w++) {
+            if (p->d_fw[s][w]) cudaFree(p->d_fw[s][w]);
+            p->d_fw[s][w] = nullptr;
+        }
+        for (int r = 0; r < NR; r++) {
+            if (p->d_fr[s][r]) cudaFree(p->d_fr[s][r]);
+            p->d_fr[s][r] = nullptr;
+        }
+    }
+    p->dft_nf = 0;
+    p->have_dft = false;
+}
+
+// transforms of every wave field and memory variable, forward and adjoint
+int alloc_dft(sfd_plan *p)
+{
+    const Grid &g = p->g;
+    if (p->dft_nf == p->nfreqs) return SFD_OK;
+    free_dft(p);
+    const size_t nf = (size_t)p->nfreqs;
+    for (int s = 0; s < 2; s++) {
+        for (int w = 0; w < NW; w++) {
+            if (!is_wave_used(g, w)) continue;
+            if (cudaMalloc(&p->d_fw[s][w], sizeof(float2) * nf * g.nvol) != cudaSuccess) {
+                p->d_fw[s][w] = nullptr;
+                free_dft(p);
+                return fail(p, SFD_ERR_MEMORY, "DFT gradient buffers do not fit in device memory");
+            }
+        }
+        for (int r = 0; r < NR; r++) {
+            if (!is_mem_used(g, r)) continue;
+            if (cudaMalloc(&p->d_fr[s][r], sizeof(float2) * nf * g.nvol * g.L) != cudaSuccess) {
+                p->d_fr[s][r] = nullptr;
+                free_dft(p);
+                return fail(p, SFD_ERR_MEMORY, "DFT gradient buffers do not fit in device memory");
+            }
+        }
+    }
+    p->dft_nf = p->nfreqs;
+    return SFD_OK;
+}
+
+int zero_dft(sfd_plan *p, int slot, cudaStream_t st)
+{
+    const Grid &g = p->g;
+    for (int w = 0; w < NW; w++)
+        if (p->d_fw[slot][w]) CKC(cudaMemsetAsync(p->d_fw[slot][w], 0, sizeof(float2) * p->nfreqs * g.nvol, st));
+    for (int r = 0; r < NR; r++)
+        if (p->d_fr[slot][r])
+            CKC(cudaMemsetAsync(p->d_fr[slot][r], 0, sizeof(float2) * p->nfreqs * g.nvol * g.L, st));
+    return SFD_OK;
+}
+
+// Add sample `thist` of the current fields to the transforms of `slot`.
+// Factors DTNYQ*DT*exp(-i pi 2 k n / NTNYQ) in FP64, stored FP32
+// (src/automatic_kernels.c:1106-1110); cos/sin of pi x after an exact
+// reduction of x modulo 2.
+void dft_sample(sfd_plan *p, int slot, int thist, cudaStream_t st)
+{
+    const Grid &g = p->g;
+    DftSet d;
+    memset(&d, 0, sizeof d);
+    d.nf = p->nfreqs;
+    for (int k = 0; k < p->nfreqs; k++) {
+        const double ph = std::fmod(2.0 * p->gradfreqsn[k] * thist / p->ntnyq, 2.0);
+        d.re[k] = (float)(p->dtnyq * p->DT_lit * std::cos(PI_D * ph));
+        d.im[k] = (float)(-p->dtnyq * p->DT_lit * std::sin(PI_D * ph));
+    }
+    int n = 0;
+    for (int w = 0; w < NW; w++)
+        if (p->d_fw[slot][w]) { d.v[n] = p->f.w[w]; d.f[n] = p->d_fw[slot][w]; d.n[n] = g.nvol; n++; }
+    for (int r = 0; r < NR; r++)
+        if (p->d_fr[slot][r]) { d.v[n] = p->f.r[r]; d.f[n] = p->d_fr[slot][r]; d.n[n] = g.nvol * g.L; n++; }
+    d.nvar = n;
+    launch_savefreqs(d, st);
+}
+
+// The DFT adjoint and gradient assembly (time_stepping.c:862-972 with
+// BACK_PROP_TYPE=2): residuals are on the device already.
+int adjoint_dft(sfd_plan *p, const PointSet &R, unsigned omask, cudaStream_t st)
+{
+    const Grid &g = p->g;
+    const int NT = p->cfg.nt, tmin = p->cfg.tmin;
+    int rc;
+    // initsavefreqs + init_f (time_stepping.c:655-670): fields, memory
+    // variables, CPML memory and the adjoint transforms start at zero
+    if ((rc = zero_forward_state(p, st))) return rc;
+    if ((rc = zero_dft(p, 1, st))) return rc;
+    Grid ga = g;
+    ga.bp2 = 1;
+    AdjFields a = p->a;
+    for (int w = 0; w < NW; w++) { a.wr[w] = p->f.w[w]; a.bnd[w] = nullptr; }
+    for (int r = 0; r < NR; r++) a.rr[r] = p->f.r[r];
+    CKC(cudaEventRecord(p->ev0, st));
+    for (int t = p->cfg.tmax - 1; t > tmin; t--) {
+        if (g.freesurf) launch_surface_adj(ga, p->f, a, p->d_surf_q, st);
+        launch_residuals(ga, a, R, p->d_res, NT, t, omask, st);
+        launch_update_adj(ga, p->f, a, true, SFD_PREC_FP32, st);
+        launch_update_adj(ga, p->f, a, false, SFD_PREC_FP32, st);
+        if ((t - tmin) % p->dtnyq == 0) dft_sample(p, 1, (t - tmin) / p->dtnyq, st);
+    }
+    // calc_grad (src/calc_grad.c:376-420 for the constants)
+    GradDft d;
+    memset(&d, 0, sizeof d);
+    for (int s = 0; s < 2; s++) {
+        for (int w = 0; w < NW; w++) d.fw[s][w] = p->d_fw[s][w];
+        for (int r = 0; r < NR; r++) d.fr[s][r] = p->d_fr[s][r];
+    }
+    d.nf = p->nfreqs;
+    d.par_type = p->cfg.param_type;
+    for (int k = 0; k < p->nfreqs; k++) d.w[k] = (float)(2.0 * PI_D * p->df * p->gradfreqsn[k]);
+    const float w0 = (float)(2.0 * PI_D * p->cfg.f0);
+    float al = 0.0f;
+    for (int l = 0; l < g.L; l++) {
+        d.tausig[l] = (float)(1.0 / (2.0 * PI_D * p->cfg.fl[l]));
+        const double q = std::pow(w0 / (2.0 * PI_D * p->cfg.fl[l]), 2);
+        al = (float)(al + q / (1.0 + q));
+    }
+    d.al = al;
+    d.ntnyq = (float)p->ntnyq;
+    launch_calc_grad(g, p->f, p->a, d, st);
+    CKC(cudaEventRecord(p->ev1, st));
+    CKC(cudaGetLastError());
+    CKC(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1);
+    p->have_forward = false;
+    p->have_dft = false;
     return SFD_OK;
 }
 
@@ -312,6 +452,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     if (c.adjoint_reset_psi < 0 || c.adjoint_reset_psi > 1) return SFD_ERR_ARG;
     if (c.field_precision < 0 || c.field_precision > 1) return SFD_ERR_ARG;
     if (c.field_precision == 1 && (c.nd != 3 || c.L > 3)) return SFD_ERR_UNSUPPORTED;
+    if (c.back_prop_type < 0 || c.back_prop_type > 2) return SFD_ERR_ARG;
 
     sfd_plan *p = new sfd_plan();
     p->cfg = c;
@@ -362,6 +503,11 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     memset(&p->a, 0, sizeof p->a);
     p->last_ms = 0.0f;
     p->kshift = 0;
+    p->nfreqs = p->dtnyq = p->ntnyq = p->dft_nf = 0;
+    p->df = 0.0f;
+    memset(p->d_fw, 0, sizeof p->d_fw);
+    memset(p->d_fr, 0, sizeof p->d_fr);
+    p->have_dft = false;
     if (cudaGetDevice(&p->device) != cudaSuccess) { delete p; return SFD_ERR_CUDA; }
     if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) { delete p; return SFD_ERR_CUDA; }
     p->own_stream = true;
@@ -378,6 +524,7 @@ extern "C" void sfd_plan_destroy(sfd_plan *p)
     for (void *ptr : p->allocs) cudaFree(ptr);
     for (int w = 0; w < NW; w++)
         if (p->d_bnd[w]) cudaFree(p->d_bnd[w]);
+    free_dft(p);
     cudaEventDestroy(p->ev0);
     cudaEventDestroy(p->ev1);
     if (p->own_stream) cudaStreamDestroy(p->stream);
@@ -471,7 +618,16 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
         const int a = force_only ? e0 - p->kshift : e0, b = a + p->kshift;
         for (int w = 0; w < NW; w++) p->g.ws.w[w] = std::ldexp(1.0f, w <= VZ ? b : a);
     }
-    if (save_boundaries) {
+    // a gradient run keeps the boundary shells (BACK_PROP_TYPE 1) or the
+    // forward transforms (2)
+    const bool dft = save_boundaries && p->cfg.back_prop_type == 2;
+    if (dft) {
+        if (g.nd == 21 || g.nd == 22)
+            return fail(p, SFD_ERR_UNSUPPORTED, "the adjoint path covers P-SV and 3D elastic/viscoelastic media");
+        if (!p->nfreqs) return fail(p, SFD_ERR_STATE, "sfd_set_gradfreqs must be called before a DFT-gradient run");
+        if ((rc = alloc_dft(p))) return rc;
+        if ((rc = zero_dft(p, 0, st))) return rc;
+    } else if (save_boundaries) {
         if (g.nd == 21 || g.nd == 22)
             return fail(p, SFD_ERR_UNSUPPORTED, "the adjoint path covers P-SV and 3D elastic/viscoelastic media");
         if (g.nab <= 0 || g.nbnd <= 0) return fail(p, SFD_ERR_ARG, "boundary saving needs an absorbing layer");
@@ -489,13 +645,16 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
         }
     }
     p->have_forward = false;
-    const int NT = p->cfg.nt, tmax = p->cfg.tmax;
+    p->have_dft = false;
+    const int NT = p->cfg.nt, tmax = p->cfg.tmax, tmin = p->cfg.tmin;
     CKC(cudaEventRecord(p->ev0, st));
     for (int t = 0; t < tmax; t++) {
+        // the state after t steps, before the sources of step t (time_stepping.c:766-781)
+        if (dft && t >= tmin && (t - tmin) % p->dtnyq == 0) dft_sample(p, 0, (t - tmin) / p->dtnyq, st);
         launch_sources(g, p->f, S, p->d_src, NT, t, 1, st);
         launch_update_v(g, p->f, st);
         launch_update_s(g, p->f, st);
-        if (save_boundaries) launch_savebnd(g, p->f, bs, p->cfg.precision, (int64_t)t * g.nbnd, st);
+        if (save_boundaries && !dft) launch_savebnd(g, p->f, bs, p->cfg.precision, (int64_t)t * g.nbnd, st);
         if (g.freesurf) launch_surface(g, p->f, 1, st);
         launch_record(g, p->f, R, p->d_seis, NT, t, omask, st);
     }
@@ -514,6 +673,7 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
     if (tma_take_status())
         return fail(p, SFD_ERR_CUDA, "a TMA stage of the 3D stencil kernels did not arrive within its time bound");
     p->have_forward = save_boundaries != 0;
+    p->have_dft = dft;
     return SFD_OK;
 }
 
@@ -543,6 +703,10 @@ extern "C" int sfd_adjoint(sfd_plan *p, const sfd_shot *shot, int mask, const in
         CKC(cudaMemcpyAsync(p->d_res + (size_t)slot * shot->nrec * NT, residuals[o],
                             sizeof(float) * (size_t)shot->nrec * NT, cudaMemcpyHostToDevice, st));
         slot++;
+    }
+    if (p->cfg.back_prop_type == 2) {
+        if (!p->have_dft) return fail(p, SFD_ERR_STATE, "the forward transforms are missing (gradfreqs changed?)");
+        return adjoint_dft(p, R, omask, st);
     }
     // adjoint fields start at zero; the CPML memory carries over from the
     // forward run (the reference binds the forward psi buffers by name)
@@ -581,7 +745,54 @@ extern "C" int sfd_zero_gradient(sfd_plan *p)
     int rc;
     if ((rc = alloc_adjoint(p))) return rc;
     int64_t npar = (int64_t)p->g.nz * p->g.ny * p->g.nx;
-    for (int k = 0; k < NG; k++) CKC(cudaMemset(p->a.grad[k], 0, sizeof(double) * npar));
+    for (int k = 0; k < NG; k++)
+        if (p->a.grad[k]) CKC(cudaMemset(p->a.grad[k], 0, sizeof(double) * npar));
+    return SFD_OK;
+}
+
+extern "C" int sfd_set_gradfreqs(sfd_plan *p, const float *freqs, int nfreqs, int *info)
+{
+    if (!p || !freqs) return SFD_ERR_ARG;
+    if (p->cfg.back_prop_type != 2) return fail(p, SFD_ERR_STATE, "the plan was not created with back_prop_type 2");
+    if (nfreqs < 1 || nfreqs > MAXFREQ) return fail(p, SFD_ERR_ARG, "between 1 and 16 gradient frequencies");
+    // src/assign_modeling_case.c:549-570
+    float fmaxout = 0.0f;
+    for (int j = 0; j < nfreqs; j++) {
+        if (!std::isfinite(freqs[j]) || freqs[j] < 0.0f) return fail(p, SFD_ERR_ARG, "gradient frequencies must be >= 0");
+        if (freqs[j] > fmaxout) fmaxout = freqs[j];
+    }
+    if (!(fmaxout > 0.0f)) return fail(p, SFD_ERR_ARG, "the highest gradient frequency must be positive");
+    const float dt = p->cfg.dt;
+    p->dtnyq = (int)std::ceil(0.0156 / fmaxout / dt);
+    p->ntnyq = (p->cfg.tmax - p->cfg.tmin) / p->dtnyq + 1;
+    p->df = (float)(1.0 / p->ntnyq / dt / p->dtnyq);
+    for (int j = 0; j < nfreqs; j++) p->gradfreqsn[j] = std::floor(freqs[j] / p->df);
+    p->nfreqs = nfreqs;
+    p->have_dft = false;
+    if (info) {
+        info[0] = p->dtnyq;
+        info[1] = p->ntnyq;
+    }
+    return SFD_OK;
+}
+
+extern "C" int sfd_get_gradient_q(sfd_plan *p, float *gtaup, float *gtaus)
+{
+    if (!p) return SFD_ERR_ARG;
+    if (!p->a.grad[0]) return fail(p, SFD_ERR_STATE, "no gradient has been accumulated");
+    int64_t n = (int64_t)p->g.nz * p->g.ny * p->g.nx;
+    std::vector<double> h(n);
+    float *outs[2] = {gtaup, gtaus};
+    const int ids[2] = {GTAUP, GTAUS};
+    for (int q = 0; q < 2; q++) {
+        if (!outs[q]) continue;
+        if (!p->a.grad[ids[q]]) {
+            std::fill(outs[q], outs[q] + n, 0.0f);
+            continue;
+        }
+        CKC(cudaMemcpy(h.data(), p->a.grad[ids[q]], sizeof(double) * n, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < n; i++) outs[q][i] = (float)h[i];
+    }
     return SFD_OK;
 }
 
@@ -594,7 +805,8 @@ extern "C" int sfd_get_gradient(sfd_plan *p, int transform, float *g0, float *g1
     CKC(cudaMemcpy(gr.data(), p->a.grad[GRHO], sizeof(double) * n, cudaMemcpyDeviceToHost));
     CKC(cudaMemcpy(gM.data(), p->a.grad[GM], sizeof(double) * n, cudaMemcpyDeviceToHost));
     CKC(cudaMemcpy(gmu.data(), p->a.grad[GMU], sizeof(double) * n, cudaMemcpyDeviceToHost));
-    if (!transform) {
+    // the DFT gradient is already in the param_type's basis (no transf_grad)
+    if (!transform || p->cfg.back_prop_type == 2) {
         for (int64_t i = 0; i < n; i++) {
             if (g0) g0[i] = (float)gM[i];
             if (g1) g1[i] = (float)gmu[i];
@@ -692,6 +904,11 @@ extern "C" int64_t sfd_debug_copy(sfd_plan *p, int kind, int id, float *dst, int
         src = id == 0 ? p->f.cx[0] : (id == 1 ? p->f.cy[0] : p->f.cz[0]);
         n = (int64_t)NC * std::max(2 * g.nab, 1);
     } else if (kind == 5 && id >= 0 && id < NPSI) { src = p->f.psi[id]; n = p->psi_size[id]; }
+    else if ((kind == 6 || kind == 7) && id >= 0 && id < NW) { src = p->d_fw[kind - 6][id]; n = 2 * (int64_t)p->dft_nf * g.nvol; }
+    else if ((kind == 8 || kind == 9) && id >= 0 && id < NR) {
+        src = p->d_fr[kind - 8][id];
+        n = 2 * (int64_t)p->dft_nf * g.nvol * g.L;
+    }
     if (!src) return fail(p, SFD_ERR_ARG, "array not allocated");
     if (n > cap) return fail(p, SFD_ERR_ARG, "destination too small");
     cudaDeviceSynchronize();

@@ -28,7 +28,9 @@ enum {
 };
 // CPML constants per axis
 enum { CK, CA, CB, CKH, CAH, CBH, NC };
-enum { GRHO, GM, GMU, NG };
+// gradient accumulators; taup and taus are filled by the DFT gradient only
+enum { GRHO, GM, GMU, GTAUP, GTAUS, NG };
+constexpr int MAXFREQ = 16;   // DFT gradient frequencies per plan
 
 // Stored value = field x w[field]: 1 for FP32 storage; powers of two for
 // FP16 storage (set per shot from the source amplitude).
@@ -55,6 +57,8 @@ struct Grid {
     int nbnd;               // saved-boundary cells per field per step
     int restype;
     int kernels;            // 0: register-blocked 3D kernels where available, 1: general only
+    int bp2;                // adjoint kernels: 1 for the DFT gradient (no reconstruction,
+                            // boundary injection or on-the-fly gradient)
 };
 
 struct Fields {
@@ -115,4 +119,12 @@ struct sfd_plan {
     cudaEvent_t ev0, ev1;
     int kshift;             // FP16 storage: log2 ratio of velocity to stress scales
     float last_ms;
+    // DFT gradient (back_prop_type 2, src/assign_modeling_case.c:549-570)
+    int nfreqs, dtnyq, ntnyq;
+    float df;
+    float gradfreqsn[sfd::MAXFREQ];
+    float2 *d_fw[2][sfd::NW];   // [forward, adjoint] transforms [nfreqs][nvol]
+    float2 *d_fr[2][sfd::NR];   // memory variables [nfreqs][L][nvol]
+    int dft_nf;                 // frequencies the transform buffers were allocated for
+    bool have_dft;              // a forward run left its transforms on the device
 };

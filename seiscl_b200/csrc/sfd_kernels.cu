@@ -1070,34 +1070,37 @@ __global__ void __launch_bounds__(256) k_adjv2d(Grid g, Fields f, AdjFields a)
     if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
     i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
     const float *hc = g.hc;
-    float sxx_x = dfw<F>(f.w[SXX], iv, g.NZ, hc);
-    float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc);
-    float sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
-    float sxz_x = dbw<F>(f.w[SXZ], iv, g.NZ, hc);
+    float rip = __ldg(f.p[PRIP] + ip), rkp = __ldg(f.p[PRKP] + ip);
+    float vx = 0.0f, vz = 0.0f;
+    if (!g.bp2) {  // backpropagate the forward velocities (update_adjv2D.cl:205-240)
+        float sxx_x = dfw<F>(f.w[SXX], iv, g.NZ, hc);
+        float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc);
+        float sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
+        float sxz_x = dbw<F>(f.w[SXZ], iv, g.NZ, hc);
+        vx = f.w[VX][iv] - (sxx_x + sxz_z) * rip;
+        vz = f.w[VZ][iv] - (szz_z + sxz_x) * rkp;
+        int m = inject_ind2d(g, gz, gx);
+        if (m != -1) {
+            vx = to_f<T>(((const T *)a.bnd[VX])[m]);
+            vz = to_f<T>(((const T *)a.bnd[VZ])[m]);
+        }
+        f.w[VX][iv] = vx;
+        f.w[VZ][iv] = vz;
+    }
     float sxx_xr = dfw<F>(a.wr[SXX], iv, g.NZ, hc);
     float szz_zr = dfw<F>(a.wr[SZZ], iv, 1, hc);
     float sxz_zr = dbw<F>(a.wr[SXZ], iv, 1, hc);
     float sxz_xr = dbw<F>(a.wr[SXZ], iv, g.NZ, hc);
-    float rip = __ldg(f.p[PRIP] + ip), rkp = __ldg(f.p[PRKP] + ip);
-    float lvx = (sxx_x + sxz_z) * rip, lvz = (szz_z + sxz_x) * rkp;
-    float vx = f.w[VX][iv] - lvx, vz = f.w[VZ][iv] - lvz;
-    int m = inject_ind2d(g, gz, gx);
-    if (m != -1) {
-        vx = to_f<T>(((const T *)a.bnd[VX])[m]);
-        vz = to_f<T>(((const T *)a.bnd[VZ])[m]);
-    }
-    f.w[VX][iv] = vx;
-    f.w[VZ][iv] = vz;
     if (g.abs_type == 1) cpml_v2d(g, f, gz, gx, sxx_xr, szz_zr, sxz_xr, sxz_zr);
-    lvx = (sxx_xr + sxz_zr) * rip;
-    lvz = (szz_zr + sxz_xr) * rkp;
+    float lvx = (sxx_xr + sxz_zr) * rip;
+    float lvz = (szz_zr + sxz_xr) * rkp;
     a.wr[VX][iv] += lvx;
     a.wr[VZ][iv] += lvz;
     if (g.abs_type == 2) {
         float *fs[2] = {a.wr[VX], a.wr[VZ]};
         apply_taper<2>(g, f.taper, gz, 0, gx, fs, iv);
     }
-    a.grad[GRHO][ip] += (double)(-vx * lvx - vz * lvz);
+    if (!g.bp2) a.grad[GRHO][ip] += (double)(-vx * lvx - vz * lvz);
 }
 
 template <int F, typename T>
@@ -1108,8 +1111,11 @@ __global__ void __launch_bounds__(256) k_adjs2d(Grid g, Fields f, AdjFields a)
     if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
     i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
     const float *hc = g.hc;
-    float vxx = dbw<F>(f.w[VX], iv, g.NZ, hc), vxz = dfw<F>(f.w[VX], iv, 1, hc);
-    float vzz = dbw<F>(f.w[VZ], iv, 1, hc), vzx = dfw<F>(f.w[VZ], iv, g.NZ, hc);
+    float vxx = 0.0f, vxz = 0.0f, vzz = 0.0f, vzx = 0.0f;
+    if (!g.bp2) {
+        vxx = dbw<F>(f.w[VX], iv, g.NZ, hc); vxz = dfw<F>(f.w[VX], iv, 1, hc);
+        vzz = dbw<F>(f.w[VZ], iv, 1, hc); vzx = dfw<F>(f.w[VZ], iv, g.NZ, hc);
+    }
     float vxxr = dbw<F>(a.wr[VX], iv, g.NZ, hc), vxzr = dfw<F>(a.wr[VX], iv, 1, hc);
     float vzzr = dbw<F>(a.wr[VZ], iv, 1, hc), vzxr = dfw<F>(a.wr[VZ], iv, g.NZ, hc);
     const int L = g.L;
@@ -1128,13 +1134,16 @@ __global__ void __launch_bounds__(256) k_adjs2d(Grid g, Fields f, AdjFields a)
         d = 2.0f * lmu * ltaus / g.dt;
         e = lM * ltaup / g.dt;
     }
-    float sxx = f.w[SXX][iv], szz = f.w[SZZ][iv], sxz = f.w[SXZ][iv];
+    float sxx = 0.0f, szz = 0.0f, sxz = 0.0f;
     // reconstruct the forward stresses (update_adjs2D.cl:222-278)
-    if (L == 0) {
+    if (g.bp2) {
+    } else if (L == 0) {
+        sxx = f.w[SXX][iv]; szz = f.w[SZZ][iv]; sxz = f.w[SXZ][iv];
         sxz -= fipkp * (vxz + vzx);
         sxx -= gm * (vxx + vzz) - fm * vzz;
         szz -= gm * (vxx + vzz) - fm * vxx;
     } else {
+        sxx = f.w[SXX][iv]; szz = f.w[SZZ][iv]; sxz = f.w[SXZ][iv];
         float *rxx = f.r[RXX], *rzz = f.r[RZZ], *rxz = f.r[RXZ];
         float s1 = 0, s2 = 0, s3 = 0;
         for (int l = 0; l < L; l++) { i64 ir = l * g.nvol + iv; s1 += rxz[ir]; s2 += rxx[ir]; s3 += rzz[ir]; }
@@ -1156,13 +1165,15 @@ __global__ void __launch_bounds__(256) k_adjs2d(Grid g, Fields f, AdjFields a)
         sxx -= lsxx + g.dt2 * s2;
         szz -= lszz + g.dt2 * s3;
     }
-    int m = inject_ind2d(g, gz, gx);
-    if (m != -1) {
-        sxx = to_f<T>(((const T *)a.bnd[SXX])[m]);
-        szz = to_f<T>(((const T *)a.bnd[SZZ])[m]);
-        sxz = to_f<T>(((const T *)a.bnd[SXZ])[m]);
+    if (!g.bp2) {
+        int m = inject_ind2d(g, gz, gx);
+        if (m != -1) {
+            sxx = to_f<T>(((const T *)a.bnd[SXX])[m]);
+            szz = to_f<T>(((const T *)a.bnd[SZZ])[m]);
+            sxz = to_f<T>(((const T *)a.bnd[SXZ])[m]);
+        }
+        f.w[SXX][iv] = sxx; f.w[SZZ][iv] = szz; f.w[SXZ][iv] = sxz;
     }
-    f.w[SXX][iv] = sxx; f.w[SZZ][iv] = szz; f.w[SXZ][iv] = sxz;
     if (g.abs_type == 1) cpml_s2d(g, f, gz, gx, vxxr, vxzr, vzxr, vzzr);
     float lsxz, lsxx, lszz;
     if (L == 0) {
@@ -1200,7 +1211,8 @@ __global__ void __launch_bounds__(256) k_adjs2d(Grid g, Fields f, AdjFields a)
         float *fs[3] = {a.wr[SXZ], a.wr[SXX], a.wr[SZZ]};
         apply_taper<3>(g, f.taper, gz, 0, gx, fs, iv);
     }
-    if (g.restype == 0) {
+    if (g.bp2) {
+    } else if (g.restype == 0) {
         float c1 = 1.0f / ((2.0f * lM - 2.0f * lmu) * (2.0f * lM - 2.0f * lmu));
         float c3 = 1.0f / (lmu * lmu);
         float c5 = 0.25f * c3;
@@ -1260,39 +1272,41 @@ __global__ void __launch_bounds__(256) k_adjv3d(Grid g, Fields f, AdjFields a)
 {
     CELL3D
     const float *hc = g.hc;
-    float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc), sxx_x = dfw<F>(f.w[SXX], iv, sx, hc);
-    float sxz_x = dbw<F>(f.w[SXZ], iv, sx, hc), sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
-    float syz_y = dbw<F>(f.w[SYZ], iv, sy, hc), syz_z = dbw<F>(f.w[SYZ], iv, 1, hc);
-    float syy_y = dfw<F>(f.w[SYY], iv, sy, hc);
-    float sxy_x = dbw<F>(f.w[SXY], iv, sx, hc), sxy_y = dbw<F>(f.w[SXY], iv, sy, hc);
+    float rip = __ldg(f.p[PRIP] + ip), rjp = __ldg(f.p[PRJP] + ip), rkp = __ldg(f.p[PRKP] + ip);
+    float vx = 0.0f, vy = 0.0f, vz = 0.0f;
+    if (!g.bp2) {  // backpropagate the forward velocities (update_adjv3D.cl:297-340)
+        float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc), sxx_x = dfw<F>(f.w[SXX], iv, sx, hc);
+        float sxz_x = dbw<F>(f.w[SXZ], iv, sx, hc), sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
+        float syz_y = dbw<F>(f.w[SYZ], iv, sy, hc), syz_z = dbw<F>(f.w[SYZ], iv, 1, hc);
+        float syy_y = dfw<F>(f.w[SYY], iv, sy, hc);
+        float sxy_x = dbw<F>(f.w[SXY], iv, sx, hc), sxy_y = dbw<F>(f.w[SXY], iv, sy, hc);
+        vx = f.w[VX][iv] - (sxx_x + sxy_y + sxz_z) * rip;
+        vy = f.w[VY][iv] - (syy_y + sxy_x + syz_z) * rjp;
+        vz = f.w[VZ][iv] - (szz_z + sxz_x + syz_y) * rkp;
+        int m = inject_ind3d(g, gz, gy, gx);
+        if (m != -1) {
+            vx = to_f<T>(((const T *)a.bnd[VX])[m]);
+            vy = to_f<T>(((const T *)a.bnd[VY])[m]);
+            vz = to_f<T>(((const T *)a.bnd[VZ])[m]);
+        }
+        f.w[VX][iv] = vx; f.w[VY][iv] = vy; f.w[VZ][iv] = vz;
+    }
     float szz_zr = dfw<F>(a.wr[SZZ], iv, 1, hc), sxx_xr = dfw<F>(a.wr[SXX], iv, sx, hc);
     float sxz_xr = dbw<F>(a.wr[SXZ], iv, sx, hc), sxz_zr = dbw<F>(a.wr[SXZ], iv, 1, hc);
     float syz_yr = dbw<F>(a.wr[SYZ], iv, sy, hc), syz_zr = dbw<F>(a.wr[SYZ], iv, 1, hc);
     float syy_yr = dfw<F>(a.wr[SYY], iv, sy, hc);
     float sxy_xr = dbw<F>(a.wr[SXY], iv, sx, hc), sxy_yr = dbw<F>(a.wr[SXY], iv, sy, hc);
-    float rip = __ldg(f.p[PRIP] + ip), rjp = __ldg(f.p[PRJP] + ip), rkp = __ldg(f.p[PRKP] + ip);
-    float lvx = (sxx_x + sxy_y + sxz_z) * rip;
-    float lvy = (syy_y + sxy_x + syz_z) * rjp;
-    float lvz = (szz_z + sxz_x + syz_y) * rkp;
-    float vx = f.w[VX][iv] - lvx, vy = f.w[VY][iv] - lvy, vz = f.w[VZ][iv] - lvz;
-    int m = inject_ind3d(g, gz, gy, gx);
-    if (m != -1) {
-        vx = to_f<T>(((const T *)a.bnd[VX])[m]);
-        vy = to_f<T>(((const T *)a.bnd[VY])[m]);
-        vz = to_f<T>(((const T *)a.bnd[VZ])[m]);
-    }
-    f.w[VX][iv] = vx; f.w[VY][iv] = vy; f.w[VZ][iv] = vz;
     if (g.abs_type == 1)
         cpml_v3d(g, f, gz, gy, gx, sxx_xr, syy_yr, szz_zr, sxy_yr, sxy_xr, syz_yr, syz_zr, sxz_xr, sxz_zr);
-    lvx = (sxx_xr + sxy_yr + sxz_zr) * rip;
-    lvy = (syy_yr + sxy_xr + syz_zr) * rjp;
-    lvz = (szz_zr + sxz_xr + syz_yr) * rkp;
+    float lvx = (sxx_xr + sxy_yr + sxz_zr) * rip;
+    float lvy = (syy_yr + sxy_xr + syz_zr) * rjp;
+    float lvz = (szz_zr + sxz_xr + syz_yr) * rkp;
     a.wr[VX][iv] += lvx; a.wr[VY][iv] += lvy; a.wr[VZ][iv] += lvz;
     if (g.abs_type == 2) {
         float *fs[3] = {a.wr[VX], a.wr[VY], a.wr[VZ]};
         apply_taper<3>(g, f.taper, gz, gy, gx, fs, iv);
     }
-    a.grad[GRHO][ip] += (double)(-vx * lvx - vy * lvy - vz * lvz);
+    if (!g.bp2) a.grad[GRHO][ip] += (double)(-vx * lvx - vy * lvy - vz * lvz);
 }
 
 template <int F, typename T>
@@ -1300,9 +1314,12 @@ __global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
 {
     CELL3D
     const float *hc = g.hc;
-    float vzx = dfw<F>(f.w[VZ], iv, sx, hc), vzy = dfw<F>(f.w[VZ], iv, sy, hc), vzz = dbw<F>(f.w[VZ], iv, 1, hc);
-    float vyx = dfw<F>(f.w[VY], iv, sx, hc), vyy = dbw<F>(f.w[VY], iv, sy, hc), vyz = dfw<F>(f.w[VY], iv, 1, hc);
-    float vxx = dbw<F>(f.w[VX], iv, sx, hc), vxy = dfw<F>(f.w[VX], iv, sy, hc), vxz = dfw<F>(f.w[VX], iv, 1, hc);
+    float vzx = 0.0f, vzy = 0.0f, vzz = 0.0f, vyx = 0.0f, vyy = 0.0f, vyz = 0.0f, vxx = 0.0f, vxy = 0.0f, vxz = 0.0f;
+    if (!g.bp2) {
+        vzx = dfw<F>(f.w[VZ], iv, sx, hc); vzy = dfw<F>(f.w[VZ], iv, sy, hc); vzz = dbw<F>(f.w[VZ], iv, 1, hc);
+        vyx = dfw<F>(f.w[VY], iv, sx, hc); vyy = dbw<F>(f.w[VY], iv, sy, hc); vyz = dfw<F>(f.w[VY], iv, 1, hc);
+        vxx = dbw<F>(f.w[VX], iv, sx, hc); vxy = dfw<F>(f.w[VX], iv, sy, hc); vxz = dfw<F>(f.w[VX], iv, 1, hc);
+    }
     float vzxr = dfw<F>(a.wr[VZ], iv, sx, hc), vzyr = dfw<F>(a.wr[VZ], iv, sy, hc), vzzr = dbw<F>(a.wr[VZ], iv, 1, hc);
     float vyxr = dfw<F>(a.wr[VY], iv, sx, hc), vyyr = dbw<F>(a.wr[VY], iv, sy, hc), vyzr = dfw<F>(a.wr[VY], iv, 1, hc);
     float vxxr = dbw<F>(a.wr[VX], iv, sx, hc), vxyr = dfw<F>(a.wr[VX], iv, sy, hc), vxzr = dfw<F>(a.wr[VX], iv, 1, hc);
@@ -1327,9 +1344,14 @@ __global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
     }
     float vxyyx = vxy + vyx, vyzzy = vyz + vzy, vxzzx = vxz + vzx;
     float vxxyyzz = vxx + vyy + vzz, vyyzz = vyy + vzz, vxxzz = vxx + vzz, vxxyy = vxx + vyy;
-    float s[6] = {f.w[SXY][iv], f.w[SYZ][iv], f.w[SXZ][iv], f.w[SXX][iv], f.w[SYY][iv], f.w[SZZ][iv]};
+    float s[6] = {0, 0, 0, 0, 0, 0};
+    if (!g.bp2) {
+        s[0] = f.w[SXY][iv]; s[1] = f.w[SYZ][iv]; s[2] = f.w[SXZ][iv];
+        s[3] = f.w[SXX][iv]; s[4] = f.w[SYY][iv]; s[5] = f.w[SZZ][iv];
+    }
     float *const *r = f.r;
-    if (L == 0) {
+    if (g.bp2) {
+    } else if (L == 0) {
         s[0] -= fipjp * vxyyx; s[1] -= fjpkp * vyzzy; s[2] -= fipkp * vxzzx;
         s[3] -= gm * vxxyyzz - fm * vyyzz; s[4] -= gm * vxxyyzz - fm * vxxzz; s[5] -= gm * vxxyyzz - fm * vxxyy;
     } else {
@@ -1359,14 +1381,16 @@ __global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
         }
         for (int q = 0; q < 6; q++) s[q] -= ls[q] + g.dt2 * aa[q];
     }
-    int m = inject_ind3d(g, gz, gy, gx);
-    if (m != -1) {
-        s[3] = to_f<T>(((const T *)a.bnd[SXX])[m]); s[4] = to_f<T>(((const T *)a.bnd[SYY])[m]);
-        s[5] = to_f<T>(((const T *)a.bnd[SZZ])[m]); s[0] = to_f<T>(((const T *)a.bnd[SXY])[m]);
-        s[1] = to_f<T>(((const T *)a.bnd[SYZ])[m]); s[2] = to_f<T>(((const T *)a.bnd[SXZ])[m]);
+    if (!g.bp2) {
+        int m = inject_ind3d(g, gz, gy, gx);
+        if (m != -1) {
+            s[3] = to_f<T>(((const T *)a.bnd[SXX])[m]); s[4] = to_f<T>(((const T *)a.bnd[SYY])[m]);
+            s[5] = to_f<T>(((const T *)a.bnd[SZZ])[m]); s[0] = to_f<T>(((const T *)a.bnd[SXY])[m]);
+            s[1] = to_f<T>(((const T *)a.bnd[SYZ])[m]); s[2] = to_f<T>(((const T *)a.bnd[SXZ])[m]);
+        }
+        f.w[SXY][iv] = s[0]; f.w[SYZ][iv] = s[1]; f.w[SXZ][iv] = s[2];
+        f.w[SXX][iv] = s[3]; f.w[SYY][iv] = s[4]; f.w[SZZ][iv] = s[5];
     }
-    f.w[SXY][iv] = s[0]; f.w[SYZ][iv] = s[1]; f.w[SXZ][iv] = s[2];
-    f.w[SXX][iv] = s[3]; f.w[SYY][iv] = s[4]; f.w[SZZ][iv] = s[5];
     if (g.abs_type == 1) cpml_s3d(g, f, gz, gy, gx, vxxr, vxyr, vxzr, vyxr, vyyr, vyzr, vzxr, vzyr, vzzr, true);
     float vxyyxr = vxyr + vyxr, vyzzyr = vyzr + vzyr, vxzzxr = vxzr + vzxr;
     float vxxyyzzr = vxxr + vyyr + vzzr, vyyzzr = vyyr + vzzr, vxxzzr = vxxr + vzzr, vxxyyr = vxxr + vyyr;
@@ -1408,7 +1432,8 @@ __global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
     }
     float sxx = s[3], syy = s[4], szz = s[5], sxy = s[0], syz = s[1], sxz = s[2];
     float lsxy = ls[0], lsyz = ls[1], lsxz = ls[2], lsxx = ls[3], lsyy = ls[4], lszz = ls[5];
-    if (g.restype == 0) {
+    if (g.bp2) {
+    } else if (g.restype == 0) {
         float c1 = 1.0f / (3.0f * lM - 4.0f * lmu) / (3.0f * lM - 4.0f * lmu);
         float c3 = 1.0f / lmu / lmu;
         float c5 = 1.0f / 6.0f * c3;

@@ -33,4 +33,22 @@ void launch_record(const Grid &g, const Fields &f, const PointSet &r, float *out
 void launch_residuals(const Grid &g, const AdjFields &a, const PointSet &r, const float *res, int nt_total, int t,
                       unsigned outmask, cudaStream_t st);
 
+// DFT gradient (sfd_dft.cu)
+struct DftSet {             // variables transformed by one accumulation launch
+    const float *v[NW + NR];
+    float2 *f[NW + NR];
+    int64_t n[NW + NR];     // elements of each variable (nvol, or L*nvol)
+    int nvar, nf;
+    float re[MAXFREQ], im[MAXFREQ];
+};
+void launch_savefreqs(const DftSet &d, cudaStream_t st);
+struct GradDft {            // inputs of the per-cell assembly
+    const float2 *fw[2][NW], *fr[2][NR];
+    int nf, par_type;
+    float w[MAXFREQ];       // angular frequency of each bin (FP32, as the reference forms it)
+    float tausig[8];
+    float al, ntnyq;
+};
+void launch_calc_grad(const Grid &g, const Fields &f, const AdjFields &a, const GradDft &d, cudaStream_t st);
+
 }  // namespace sfd

@@ -36,7 +36,7 @@ class sfd_config(C.Structure):
                 ("k_max_cpml", C.c_float), ("abpc", C.c_float), ("tmin", C.c_int), ("tmax", C.c_int),
                 ("param_type", C.c_int), ("restype", C.c_int), ("precision", C.c_int),
                 ("kernels", C.c_int), ("adjoint_reset_psi", C.c_int), ("field_precision", C.c_int),
-                ("reserved", C.c_int * 4)]
+                ("back_prop_type", C.c_int), ("reserved", C.c_int * 3)]
 
 
 class sfd_shot(C.Structure):
@@ -57,6 +57,8 @@ EXPORTS = {
                               C.c_void_p]),
     "sfd_zero_gradient": (C.c_int, [C.c_void_p]),
     "sfd_get_gradient": (C.c_int, [C.c_void_p, C.c_int, FP, FP, FP]),
+    "sfd_get_gradient_q": (C.c_int, [C.c_void_p, FP, FP]),
+    "sfd_set_gradfreqs": (C.c_int, [C.c_void_p, FP, C.c_int, C.POINTER(C.c_int)]),
     "sfd_residual_scale": (C.c_int, [C.c_void_p, C.POINTER(sfd_shot), C.POINTER(C.c_int), C.POINTER(FP)]),
     "sfd_plan_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "sfd_plan_uses_tma": (C.c_int, [C.c_void_p]),
@@ -136,6 +138,8 @@ class Config:
     #                        "tma", "stream"
     adjoint_reset_psi: bool = False  # True: the adjoint starts from zeroed CPML memory (not the reference's)
     field_precision: str = "fp32"  # "fp16": wave fields / memory variables stored in FP16 (3D forward)
+    back_prop_type: int = 1  # 1: boundary-saving backpropagation, 2: DFT gradient at `gradfreqs`
+    gradfreqs: Sequence[float] = ()  # DFT gradient frequencies (Hz), back_prop_type 2
 
     def to_c(self) -> sfd_config:
         c = sfd_config()
@@ -169,6 +173,7 @@ class Config:
         c.kernels = {"fast": 0, "general": 1, "register": 2, "tma": 3, "stream": 4}[self.kernels]
         c.adjoint_reset_psi = 1 if self.adjoint_reset_psi else 0
         c.field_precision = {"fp32": 0, "fp16": 1}[self.field_precision]
+        c.back_prop_type = int(self.back_prop_type)
         return c
 
     @property
@@ -193,6 +198,18 @@ class Plan:
         info = (C.c_int64 * 8)()
         self.lib.sfd_plan_info(self.h, info)
         self.NZp, self.NYp, self.NXp, self.nvol, self.npar, self.nbnd, self.F, self.tmax = [int(v) for v in info]
+        self.dtnyq = self.ntnyq = None
+        if int(cfg.back_prop_type) == 2 and len(np.atleast_1d(cfg.gradfreqs)):
+            self.set_gradfreqs(cfg.gradfreqs)
+
+    def set_gradfreqs(self, freqs):
+        """DFT-gradient frequencies (Hz); returns (DTNYQ, NTNYQ)."""
+        f = _f32(np.atleast_1d(freqs)).ravel()
+        info = (C.c_int * 2)()
+        self._check(self.lib.sfd_set_gradfreqs(self.h, _ptr(f), int(f.size), info))
+        self.nfreqs = int(f.size)
+        self.dtnyq, self.ntnyq = int(info[0]), int(info[1])
+        return self.dtnyq, self.ntnyq
 
     def _check(self, rc):
         if rc:
@@ -275,14 +292,33 @@ class Plan:
         self._check(self.lib.sfd_zero_gradient(self.h))
 
     def gradient(self, transform=True):
+        """Accumulated gradient.  Boundary-saving plans: of the param_type's
+        parameters (transform=True) or of the stored M, mu, rho.  DFT plans:
+        always of the param_type's parameters, plus taup and taus when L > 0."""
         sh = self.cfg.model_shape
         g = [np.zeros(sh, np.float32) for _ in range(3)]
         self._check(self.lib.sfd_get_gradient(self.h, 1 if transform else 0, *[_ptr(a) for a in g]))
-        if transform:
+        dft = int(self.cfg.back_prop_type) == 2
+        if transform or dft:
             names = {0: ("vp", "vs", "rho"), 1: ("M", "mu", "rho"), 2: ("Ip", "Is", "rho")}[self.cfg.param_type]
         else:
             names = ("M", "mu", "rho")
-        return dict(zip(names, g))
+        out = dict(zip(names, g))
+        if dft and int(self.cfg.L) > 0:
+            q = [np.zeros(sh, np.float32) for _ in range(2)]
+            self._check(self.lib.sfd_get_gradient_q(self.h, *[_ptr(a) for a in q]))
+            out["taup"], out["taus"] = q
+        return out
+
+    def dft(self, slot: int, kind: str, name: str) -> np.ndarray:
+        """Device transform (copy) of a wave field ("wave") or memory
+        variable ("mem"), slot 0 forward / 1 adjoint, as complex64
+        [nfreqs][(L)][padded cells]."""
+        if kind == "wave":
+            k, i, n = 6 + slot, OUT_NAMES.index(name), self.nvol
+        else:
+            k, i, n = 8 + slot, ["rxx", "ryy", "rzz", "rxy", "ryz", "rxz"].index(name), self.nvol * int(self.cfg.L)
+        return self.debug_array(k, i, 2 * self.nfreqs * n).view(np.complex64)
 
     def debug_array(self, kind: int, idx: int, n: int) -> np.ndarray:
         out = np.zeros(n, np.float32)

@@ -502,8 +502,13 @@ class SeisCL:
     # ----------------------------------------------------------- execution
     def _engine_config(self) -> engine.Config:
         N = [int(v) for v in np.atleast_1d(self.N)]
-        if self.back_prop_type != 1 and self.gradout:
-            raise SeisCLError("Error: only back_prop_type=1 (boundary-saving backpropagation) is supported")
+        bpt = int(self.back_prop_type)
+        if bpt not in (1, 2):
+            raise SeisCLError("Error: back_prop_type must be 1 (backpropagation) or 2 (DFT)")
+        freqs = tuple(float(v) for v in np.atleast_1d(self.gradfreqs).ravel())
+        if bpt == 2 and self.gradout and not freqs:
+            # read_hdf5.c:546-549 requires /gradfreqs for the DFT gradient
+            raise SeisCLError("Error: back_prop_type=2 needs gradfreqs")
         for flag in ("Hout", "gradsrcout", "movout"):
             if getattr(self, flag):
                 raise SeisCLError("Error: %s is not provided by this engine" % flag)
@@ -516,7 +521,8 @@ class SeisCL:
             tmin=self._steps(self.tmin), tmax=self._steps(self.tmax),
             param_type=int(self.param_type), restype=int(self.restype),
             precision="fp16" if int(self.FP16) >= 2 else "fp32",
-            field_precision="fp16" if int(self.FP16) >= 2 and int(self.ND) == 3 and not self.gradout else "fp32")
+            field_precision="fp16" if int(self.FP16) >= 2 and int(self.ND) == 3 and not self.gradout else "fp32",
+            back_prop_type=bpt, gradfreqs=freqs if bpt == 2 else ())
 
     def _steps(self, seconds) -> int:
         """A time in seconds as a step count, FP32 quotient truncated
@@ -641,11 +647,24 @@ class SeisCL:
         rms = 0.0
         rmsnorm = 0.0
         res = {}
+        dft = int(self.back_prop_type) == 2
+        if dft:
+            # misfit at the gradient frequencies only (residuals.c:254-410):
+            # |FFT|^2 of the residual and of the data at bin int(f*nfft*dt + 1)
+            nfft = next_fast_size(tmax)
+            bins = [int(np.float32(f) * nfft * np.float32(self.dt) + 1)
+                    for f in np.atleast_1d(self.gradfreqs).ravel()]
         for k in names:
             o = out[k][:, :tmax].astype(np.float64)
             d = obs[k][:, :tmax].astype(np.float64)
-            rms += float(((d - o) ** 2).sum())
-            rmsnorm += float((d ** 2).sum())
+            if dft:
+                R = np.fft.rfft(d - o, n=nfft, axis=1)[:, bins]
+                D = np.fft.rfft(d, n=nfft, axis=1)[:, bins]
+                rms += float((np.abs(R) ** 2).sum())
+                rmsnorm += float((np.abs(D) ** 2).sum())
+            else:
+                rms += float(((d - o) ** 2).sum())
+                rmsnorm += float((d ** 2).sum())
             r = np.zeros_like(out[k])
             if rmsnorm_sc is not None:
                 r[:, :tmax] = sc[:, None] * ((1.0 - rmsnorm_sc)[:, None] * o - d)
@@ -741,12 +760,15 @@ class SeisCL:
             shape = tuple(int(v) for v in np.atleast_1d(self.N))
             names = {0: ("vp", "vs"), 1: ("M", "mu"), 2: ("Ip", "Is")}[self.param_type]
             gout = {}
-            for name in (names[0], names[1], "rho"):
-                if nd == 22 and name == names[1]:
+            qnames = ("taup", "taus") if int(self.L) > 0 else ()
+            for name in (names[0], names[1], "rho") + qnames:
+                if nd == 22 and name in (names[1], "taus"):
                     continue
                 if nd == 21 and name == names[0]:
                     continue
-                gout["grad" + name] = np.ascontiguousarray(np.transpose(g[name])).reshape(shape)
+                # the boundary-saving gradient leaves taup/taus at zero (writehdf5.c:262-275)
+                v = g[name] if name in g else np.zeros_like(g["rho"])
+                gout["grad" + name] = np.ascontiguousarray(np.transpose(v)).reshape(shape)
             self._files[self.file_gout] = gout
         ms = (time.perf_counter() - t0) * 1e3
         return "%d shot(s) (%d on rank %d of %d), %d trace(s), %d time steps: %.1f ms\n" % (

@@ -214,6 +214,51 @@ def test_residuals_match_loop_restatement(flags):
     assert np.isclose(rms, wrms, rtol=1e-5) and np.isclose(rmsnorm, wnorm, rtol=1e-5)
 
 
+def test_dft_misfit_matches_direct_transform():
+    """back_prop_type 2: the misfit is taken at the gradient frequencies only,
+    |DFT|^2 of the residual and of the data at bin int(f*nfft*dt + 1) of a
+    next_fast_size(tmax) transform (residuals.c:254-410); the adjoint sources
+    stay those of the time domain."""
+    from seiscl_b200.seiscl import next_fast_size
+
+    freqs = np.array([90.0, 180.0, 333.0])
+    s = _seis(NT=40, back_prop_type=2, gradfreqs=freqs)
+    s1 = _seis(NT=40)
+    rng = np.random.default_rng(4)
+    out = {k: rng.standard_normal((5, 40)).astype(np.float32) for k in ("vx", "vz")}
+    obs = {k: (0.8 * out[k] + 0.3 * rng.standard_normal((5, 40))).astype(np.float32) for k in out}
+    tmax = 37
+    res, rms, rmsnorm = s._residuals(out, obs, None, 40, tmax)
+    res1, _, _ = s1._residuals(out, obs, None, 40, tmax)
+    nfft = next_fast_size(tmax)
+    want = wnorm = 0.0
+    t = np.arange(tmax)
+    for f in freqs:
+        b = int(np.float32(f) * nfft * np.float32(s.dt) + 1)
+        e = np.exp(-2j * np.pi * b * t / nfft)
+        for k in out:
+            for g in range(5):
+                want += abs(np.sum((obs[k][g, :tmax].astype(np.float64) - out[k][g, :tmax]) * e)) ** 2
+                wnorm += abs(np.sum(obs[k][g, :tmax].astype(np.float64) * e)) ** 2
+    assert np.isclose(rms, want, rtol=1e-9) and np.isclose(rmsnorm, wnorm, rtol=1e-9)
+    for k in out:
+        assert np.array_equal(res[k], res1[k])
+
+
+def test_dft_job_needs_frequencies():
+    from seiscl_b200.seiscl import SeisCLError
+
+    s = _seis(back_prop_type=2, gradout=1)
+    with pytest.raises(SeisCLError):
+        s._engine_config()
+    s.gradfreqs = np.array([[5.0, 10.0]])
+    c = s._engine_config()
+    assert c.back_prop_type == 2 and c.gradfreqs == (5.0, 10.0)
+    s.back_prop_type = 3
+    with pytest.raises(SeisCLError):
+        s._engine_config()
+
+
 # ------------------------------------------------------------------ GPU jobs
 def _two_shot_job(**kw):
     s = _seis(**kw)
@@ -329,3 +374,54 @@ def test_inputres_job_equals_combined_job(cuda_device):
     g_in = s.read_grad()
     for a, b in zip(g_in, g_comb):
         assert rel_l2(a, b) < 1e-6
+
+
+@pytest.mark.gpu
+def test_dft_gradient_job_matches_oracle(cuda_device):
+    """A two-shot DFT-gradient job (back_prop_type 2) through the front end
+    against the oracle driven the same way; the misfit at the gradient
+    frequencies from the oracle's seismograms."""
+    from seiscl_b200.seiscl import next_fast_size
+
+    freqs = np.array([9.0, 17.0, 26.0])
+    s = _two_shot_job(rmsout=1, back_prop_type=2, gradfreqs=freqs)
+    true = _models(tuple(s.N), 17)
+    start = _models(tuple(s.N), 18)
+    o_true = _oracle_for(s, true)
+    obs = {}
+    for sid in (0, 1):
+        sp, src, rp, gi = _shot_rows(s, sid)
+        obs[sid] = o_true.forward(sp, src, rp, ["vx", "vz"])
+    data = {k: np.concatenate([obs[0][k], obs[1][k]], 0).T for k in ("vx", "vz")}
+    s.prepare_data(s.src_pos_all[3, :])
+    s.write_data(data)
+    s.cropgrad = False
+    s.set_forward(s.src_pos_all[3, :], start, withgrad=True)
+    s.execute()
+    gvp, gvs, grho = s.read_grad()
+    rms, rms_norm = s.read_rms()
+
+    from oracle.oracle import Oracle
+
+    cfg = _oracle_cfg(s)
+    cfg.update(back_prop_type=2, gradfreqs=list(freqs))
+    o = Oracle(cfg)
+    assert o.set_model(start["vp"].T, start["vs"].T, start["rho"].T) == 0
+    o.clear_gradients()
+    nfft = next_fast_size(s.NT)
+    bins = [int(np.float32(f) * nfft * np.float32(s.dt) + 1) for f in freqs]
+    r2 = n2 = 0.0
+    for sid in (0, 1):
+        sp, src, rp, gi = _shot_rows(s, sid)
+        d = o.forward(sp, src, rp, ["vx", "vz"], save_boundaries=True)
+        res = {k: d[k] - obs[sid][k] for k in d}
+        for k in d:
+            r2 += float((np.abs(np.fft.rfft(obs[sid][k].astype(np.float64) - d[k], n=nfft)[:, bins]) ** 2).sum())
+            n2 += float((np.abs(np.fft.rfft(obs[sid][k].astype(np.float64), n=nfft)[:, bins]) ** 2).sum())
+        o.adjoint(sp, src, rp, o.residual_scale(rp, res))
+    g = o.raw_gradients()
+    for name, got in (("M", gvp), ("mu", gvs), ("rho", grho)):
+        assert np.abs(g[name]).max() > 0
+        assert rel_l2(got.T, g[name]) < GRAD_TOL, name
+    assert np.isclose(rms_norm, np.sqrt(n2), rtol=1e-4)
+    assert np.isclose(rms, np.sqrt(r2) / np.sqrt(n2), rtol=1e-3)
