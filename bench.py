@@ -584,13 +584,19 @@ def main():
     v_gbs = ab["v"] / (kv / 1e3) / 1e9
     step_ms = loop_ms / args.steps / w["nt"]
     fused_gbs = ab["fused"] / (step_ms / 1e3) / 1e9
-    skern = ("stress update, streaming, FP16 storage (k_s3d_stream<4,%d,half>)" % w["L"]) if args.fields == "fp16" \
-        else ("stress update, TMA-pipelined (k_tma<1,%d,*>)" % w["L"]) if plan.uses_tma else \
-        ("stress update, general (k_s%dd)" % (3 if w["nd"] == 3 else 2))
+    fam = plan.kernel_family
+    kname = {"vector": "k_s3d_q4<%d>" % w["L"], "tma": "k_tma<1,%d,*>" % w["L"],
+             "stream": "k_s3d_stream<4,%d%s>" % (w["L"], ",half" if args.fields == "fp16" else ""),
+             "register": "k_s3d_fast", "general": "k_s3d", "2d": "k_s2d"}[fam]
+    skern = "stress update, %s%s (%s)" % ({"vector": "4-cell vectorised", "tma": "TMA-pipelined",
+                                           "stream": "streaming", "register": "register-blocked",
+                                           "general": "general", "2d": "general 2D"}[fam],
+                                          ", FP16 storage" if args.fields == "fp16" else "", kname)
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic_%s.json" % args.workload)
     if os.path.exists(tpath) and args.fields == "fp32":
-        traffic = json.load(open(tpath)).get("stress_kernel_bytes_per_launch")
+        # DRAM bytes per launch of the kernel that ran, from an ncu capture
+        traffic = json.load(open(tpath)).get("stress_kernel_bytes_per_launch", {}).get(kname)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

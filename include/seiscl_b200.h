@@ -77,13 +77,14 @@ typedef struct sfd_config {
     int param_type;    /* 0: vp,vs,rho  1: M,mu,rho  2: Ip,Is,rho */
     int restype;       /* 0: L2 (full gradient), 1: M only */
     int precision;     /* SFD_PREC_*: storage of the saved boundaries */
-    int kernels;       /* 0: fastest measured: in 3D the streaming velocity update and
-                             the TMA-pipelined stress update where eligible (else the
-                             streaming one); general kernels in 2D,
+    int kernels;       /* 0: fastest measured: in 3D the 4-cell vectorised kernels where
+                             they apply (8th order, nz a multiple of 4, L <= 3), else the
+                             streaming ones; general kernels in 2D,
                           1: general one-thread-per-cell kernels only,
                           2: register-blocked 3D kernels where available,
                           3: TMA-pipelined 3D velocity and stress updates,
-                          4: streaming one-thread-per-cell 3D kernels (per-cell loads first) */
+                          4: streaming one-thread-per-cell 3D kernels (per-cell loads first),
+                          5: 4-cell vectorised 3D kernels where they apply, else streaming */
     int adjoint_reset_psi; /* 0: the adjoint continues with the forward run's CPML memory
                               (reference behaviour, src/clprogram.c:806-811); 1: it starts
                               from zeroed CPML memory.  With sources whose wave field is
@@ -233,11 +234,15 @@ int sfd_host_cpml(const sfd_config *cfg, float *out);
 /* Introspection for tests: padded dims, counts, boundary cells. */
 int sfd_plan_info(const sfd_plan *plan, int64_t *out8);
 
-/* 1 when the plan's 3D stress update (and with kernels = 3 the velocity
- * update) runs on the TMA-pipelined kernels (kernels = 0 or 3, 8th order, nz a
- * multiple of 4), 0 otherwise; negative on error.  No counterpart in the
- * reference (kernel selection is internal to this engine). */
+/* 1 when the plan's 3D updates run on the TMA-pipelined kernels (kernels = 3,
+ * 8th order, nz a multiple of 4), 0 otherwise; negative on error.  No
+ * counterpart in the reference (kernel selection is internal to this engine). */
 int sfd_plan_uses_tma(const sfd_plan *plan);
+
+/* Kernel family of the plan's 3D stress update (after sfd_set_model): 0 not
+ * 3D, 1 general, 2 register-blocked, 3 TMA-pipelined, 4 streaming, 5 4-cell
+ * vectorised; negative on error.  No counterpart in the reference. */
+int sfd_plan_kernel_family(const sfd_plan *plan);
 
 /* Copy a device array of the plan to the host (tests): kind 0 wave field,
  * 1 adjoint wave field, 2 memory variable, 3 transformed parameter,

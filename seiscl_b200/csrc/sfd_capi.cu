@@ -190,14 +190,14 @@ int alloc_model(sfd_plan *p)
         bool used = g.abs_type == 1 && g.nab > 0 &&
                     (g.nd == 3 || (g.nd == 2 && used2) || (g.nd == 21 && used21) || (g.nd == 22 && used22));
         p->psi_size[i] = used ? sizes[i] : 0;
-        tot += p->psi_size[i];
+        tot += psi_span(p->psi_size[i]);
     }
     p->d_psi_all = tot ? (float *)dalloc(p, sizeof(float) * tot, &e) : nullptr;
     if (tot && e) return fail(p, SFD_ERR_MEMORY, "CPML allocation failed");
     int64_t off = 0;
     for (int i = 0; i < NPSI; i++) {
         p->f.psi[i] = p->psi_size[i] ? p->d_psi_all + off : nullptr;
-        off += p->psi_size[i];
+        off += psi_span(p->psi_size[i]);
     }
     int64_t npar = (int64_t)g.nz * g.ny * g.nx;
     for (int k = 0; k < NPAR; k++) {
@@ -252,7 +252,7 @@ int zero_forward_state(sfd_plan *p, cudaStream_t st)
     for (int r = 0; r < NR; r++)
         if (p->f.r[r]) CKC(cudaMemsetAsync(p->f.r[r], 0, wave_elem(g) * g.nvol * g.L, st));
     int64_t tot = 0;
-    for (int i = 0; i < NPSI; i++) tot += p->psi_size[i];
+    for (int i = 0; i < NPSI; i++) tot += psi_span(p->psi_size[i]);
     if (tot) CKC(cudaMemsetAsync(p->d_psi_all, 0, sizeof(float) * tot, st));
     return SFD_OK;
 }
@@ -448,7 +448,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     // N[0] must be even (read_hdf5.c:535-540)
     if (c.n[0] % 2) return SFD_ERR_ARG;
     if (c.precision < 0 || c.precision > 2) return SFD_ERR_ARG;
-    if (c.kernels < 0 || c.kernels > 4) return SFD_ERR_ARG;
+    if (c.kernels < 0 || c.kernels > 5) return SFD_ERR_ARG;
     if (c.adjoint_reset_psi < 0 || c.adjoint_reset_psi > 1) return SFD_ERR_ARG;
     if (c.field_precision < 0 || c.field_precision > 1) return SFD_ERR_ARG;
     if (c.field_precision == 1 && (c.nd != 3 || c.L > 3)) return SFD_ERR_UNSUPPORTED;
@@ -717,7 +717,7 @@ extern "C" int sfd_adjoint(sfd_plan *p, const sfd_shot *shot, int mask, const in
     if (p->cfg.adjoint_reset_psi) {
         // optional: start the adjoint with clean CPML memory instead
         int64_t tot = 0;
-        for (int i = 0; i < NPSI; i++) tot += p->psi_size[i];
+        for (int i = 0; i < NPSI; i++) tot += psi_span(p->psi_size[i]);
         if (tot) CKC(cudaMemsetAsync(p->d_psi_all, 0, sizeof(float) * tot, st));
     }
     AdjFields a = p->a;
@@ -887,6 +887,14 @@ extern "C" int sfd_plan_uses_tma(const sfd_plan *p)
     if (!p) return SFD_ERR_ARG;
     if (cudaSetDevice(p->device) != cudaSuccess) return SFD_ERR_CUDA;
     return tma_ready(p->g, p->f) ? 1 : 0;
+}
+
+extern "C" int sfd_plan_kernel_family(const sfd_plan *p)
+{
+    if (!p) return SFD_ERR_ARG;
+    if (!p->model_set) return 0;
+    if (cudaSetDevice(p->device) != cudaSuccess) return SFD_ERR_CUDA;
+    return stress_family(p->g, p->f);
 }
 
 extern "C" int64_t sfd_debug_copy(sfd_plan *p, int kind, int id, float *dst, int64_t cap)

@@ -28,6 +28,9 @@ enum {
 };
 // CPML constants per axis
 enum { CK, CA, CB, CKH, CAH, CBH, NC };
+// CPML memory arrays share one allocation; each starts on a 256-byte
+// boundary so the 4-cell kernels can move them with 128-bit accesses
+inline int64_t psi_span(int64_t n) { return (n + 63) & ~(int64_t)63; }
 // gradient accumulators; taup and taus are filled by the DFT gradient only
 enum { GRHO, GM, GMU, GTAUP, GTAUS, NG };
 constexpr int MAXFREQ = 16;   // DFT gradient frequencies per plan

@@ -693,6 +693,509 @@ __global__ void __launch_bounds__(256, 3) k_v3d_stream(Grid g, Fields f)
     stv(wvz + iv, v[2]);
 }
 
+// ------------------------------------------------- 4-cell vectorised 3D kernels
+// One thread updates four consecutive z cells with 128-bit loads and stores:
+// the per-cell streams cost one load per four cells, a z derivative one
+// 12-value window (three loads) for four cells, and an x or y derivative one
+// load per tap for four cells -- about a fifth of the load instructions of
+// the one-cell kernels, which are bound by load issue and latency, not by
+// DRAM bytes.  Requires 8th order (F = 4, so the interior starts on a 16-byte
+// boundary) and nz % 4 == 0 (so NZ = nz + 8 keeps every row aligned).  Same
+// operation order per cell as k_v3d.
+struct Q4 {
+    float v[4];
+};
+__device__ __forceinline__ Q4 ldq(const float *p)
+{
+    float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+    return Q4{{t.x, t.y, t.z, t.w}};
+}
+__device__ __forceinline__ Q4 ldq_rw(const float *p)
+{
+    float4 t = *reinterpret_cast<const float4 *>(p);
+    return Q4{{t.x, t.y, t.z, t.w}};
+}
+__device__ __forceinline__ void stq(float *p, const Q4 &q)
+{
+    *reinterpret_cast<float4 *>(p) = make_float4(q.v[0], q.v[1], q.v[2], q.v[3]);
+}
+// forward / backward differences of four cells along a stride (x or y)
+template <int F>
+__device__ __forceinline__ Q4 dfw_q(const float *__restrict__ v, i64 i, i64 st, const float *hc)
+{
+    Q4 a = ldq(v + i + st), b = ldq(v + i), r;
+#pragma unroll
+    for (int j = 0; j < 4; j++) r.v[j] = hc[0] * (a.v[j] - b.v[j]);
+#pragma unroll
+    for (int m = 2; m <= F; m++) {
+        a = ldq(v + i + m * st);
+        b = ldq(v + i - (m - 1) * st);
+#pragma unroll
+        for (int j = 0; j < 4; j++) r.v[j] = fmaf(hc[m - 1], a.v[j] - b.v[j], r.v[j]);
+    }
+    return r;
+}
+template <int F>
+__device__ __forceinline__ Q4 dbw_q(const float *__restrict__ v, i64 i, i64 st, const float *hc)
+{
+    Q4 a = ldq(v + i), b = ldq(v + i - st), r;
+#pragma unroll
+    for (int j = 0; j < 4; j++) r.v[j] = hc[0] * (a.v[j] - b.v[j]);
+#pragma unroll
+    for (int m = 2; m <= F; m++) {
+        a = ldq(v + i + (m - 1) * st);
+        b = ldq(v + i - m * st);
+#pragma unroll
+        for (int j = 0; j < 4; j++) r.v[j] = fmaf(hc[m - 1], a.v[j] - b.v[j], r.v[j]);
+    }
+    return r;
+}
+// the 12 values z0-4 .. z0+7 around four cells starting at z0 (a multiple of 4)
+struct W12 {
+    float w[12];
+};
+__device__ __forceinline__ W12 ldw(const float *__restrict__ v, i64 i)
+{
+    W12 r;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        float4 t = __ldg(reinterpret_cast<const float4 *>(v + i - 4 + 4 * k));
+        r.w[4 * k] = t.x; r.w[4 * k + 1] = t.y; r.w[4 * k + 2] = t.z; r.w[4 * k + 3] = t.w;
+    }
+    return r;
+}
+template <int F>
+__device__ __forceinline__ Q4 dfw_z(const W12 &w, const float *hc)
+{
+    Q4 r;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        float acc = hc[0] * (w.w[5 + j] - w.w[4 + j]);
+#pragma unroll
+        for (int m = 2; m <= F; m++) acc = fmaf(hc[m - 1], w.w[4 + j + m] - w.w[4 + j - (m - 1)], acc);
+        r.v[j] = acc;
+    }
+    return r;
+}
+template <int F>
+__device__ __forceinline__ Q4 dbw_z(const W12 &w, const float *hc)
+{
+    Q4 r;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        float acc = hc[0] * (w.w[4 + j] - w.w[3 + j]);
+#pragma unroll
+        for (int m = 2; m <= F; m++) acc = fmaf(hc[m - 1], w.w[4 + j + m - 1] - w.w[4 + j - m], acc);
+        r.v[j] = acc;
+    }
+    return r;
+}
+
+// CPML recursion on four consecutive z cells sharing one profile index
+// (y and x slabs: the psi arrays are z-fastest and 16-byte aligned there);
+// same order of operations per cell as cpml()
+__device__ __forceinline__ void cpml_q(float *psi, i64 q, const float *K, const float *a, const float *b, int ci,
+                                       Q4 &d)
+{
+    const float kk = __ldg(K + ci), aa = __ldg(a + ci), bb = __ldg(b + ci);
+    Q4 p = ldq_rw(psi + q);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        float ps = bb * p.v[j] + aa * d.v[j];
+        p.v[j] = ps;
+        d.v[j] = d.v[j] / kk + ps;
+    }
+    stq(psi + q, p);
+}
+
+// z-slab CPML on a quad that lies entirely inside the slab: the psi cells
+// are consecutive (z-type psi is [nx][ny][2 nab], k fastest), the profile
+// index differs per cell (ci0 + step * j)
+__device__ __forceinline__ void cpml_zq(float *psi, i64 q, const float *K, const float *a, const float *b, int ci0,
+                                        int step, Q4 &d)
+{
+    Q4 p = ldq_rw(psi + q);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int ci = ci0 + step * j;
+        float ps = __ldg(b + ci) * p.v[j] + __ldg(a + ci) * d.v[j];
+        p.v[j] = ps;
+        d.v[j] = d.v[j] / __ldg(K + ci) + ps;
+    }
+    stq(psi + q, p);
+}
+
+// The CPML corrections of cpml_v3d for a quad of z cells: z slabs per cell
+// (a quad may straddle a z-slab edge), y and x slabs per quad.
+__device__ __forceinline__ void cpml_v3d_q4(const Grid &g, const Fields &f, int gz0, int gy, int gx, Q4 &sxx_x,
+                                            Q4 &syy_y, Q4 &szz_z, Q4 &sxy_y, Q4 &sxy_x, Q4 &syz_y, Q4 &syz_z,
+                                            Q4 &sxz_x, Q4 &sxz_z)
+{
+    const int F = g.F, NAB = g.nab, NZ = g.NZ, NY = g.NY, NX = g.NX;
+    const i64 nz = g.nz, ny = g.ny;
+    if (NAB % 4 == 0 && gz0 > NZ - NAB - F - 1) {
+        i64 i = gx - F, jj = gy - F, k = gz0 - NZ + NAB + F + NAB;
+        int ind = 2 * NAB - 1 - (int)k;
+        i64 q = (i * ny + jj) * (2 * NAB) + k;
+        cpml_zq(f.psi[PSXZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, -1, sxz_z);
+        cpml_zq(f.psi[PSYZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, -1, syz_z);
+        cpml_zq(f.psi[PSZZ_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, -1, szz_z);
+    } else if (NAB % 4 == 0 && !g.freesurf && gz0 - F < NAB) {
+        i64 i = gx - F, jj = gy - F, k = gz0 - F;
+        i64 q = (i * ny + jj) * (2 * NAB) + k;
+        cpml_zq(f.psi[PSXZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, 1, sxz_z);
+        cpml_zq(f.psi[PSYZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, 1, syz_z);
+        cpml_zq(f.psi[PSZZ_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, 1, szz_z);
+    } else if (NAB % 4 != 0 && (gz0 + 3 > NZ - NAB - F - 1 || (!g.freesurf && gz0 - F < NAB))) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int gz = gz0 + j;
+            if (gz > NZ - NAB - F - 1) {
+                i64 i = gx - F, jj = gy - F, k = gz - NZ + NAB + F + NAB;
+                int ind = 2 * NAB - 1 - (int)k;
+                i64 q = (i * ny + jj) * (2 * NAB) + k;
+                cpml(f.psi[PSXZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, sxz_z.v[j]);
+                cpml(f.psi[PSYZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, syz_z.v[j]);
+                cpml(f.psi[PSZZ_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, szz_z.v[j]);
+            } else if (!g.freesurf && gz - F < NAB) {
+                i64 i = gx - F, jj = gy - F, k = gz - F;
+                i64 q = (i * ny + jj) * (2 * NAB) + k;
+                cpml(f.psi[PSXZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, sxz_z.v[j]);
+                cpml(f.psi[PSYZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, syz_z.v[j]);
+                cpml(f.psi[PSZZ_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, szz_z.v[j]);
+            }
+        }
+    }
+    const i64 k0 = gz0 - F;
+    if (gy - F < NAB) {
+        i64 i = gx - F, j = gy - F;
+        i64 q = (i * (2 * NAB) + j) * nz + k0;
+        cpml_q(f.psi[PSXY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], (int)j, sxy_y);
+        cpml_q(f.psi[PSYY_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, syy_y);
+        cpml_q(f.psi[PSYZ_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], (int)j, syz_y);
+    } else if (gy > NY - NAB - F - 1) {
+        i64 i = gx - F, j = gy - NY + NAB + F + NAB;
+        int ind = 2 * NAB - 1 - (int)j;
+        i64 q = (i * (2 * NAB) + j) * nz + k0;
+        cpml_q(f.psi[PSXY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], ind + 1, sxy_y);
+        cpml_q(f.psi[PSYY_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, syy_y);
+        cpml_q(f.psi[PSYZ_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], ind + 1, syz_y);
+    }
+    if (gx - F < NAB) {
+        i64 i = gx - F, j = gy - F;
+        i64 q = (i * ny + j) * nz + k0;
+        cpml_q(f.psi[PSXX_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, sxx_x);
+        cpml_q(f.psi[PSXY_X], q, f.cx[CK], f.cx[CA], f.cx[CB], (int)i, sxy_x);
+        cpml_q(f.psi[PSXZ_X], q, f.cx[CK], f.cx[CA], f.cx[CB], (int)i, sxz_x);
+    }
+    if (gx > NX - NAB - F - 1) {
+        i64 i = gx - NX + NAB + F + NAB, j = gy - F;
+        int ind = 2 * NAB - 1 - (int)i;
+        i64 q = (i * ny + j) * nz + k0;
+        cpml_q(f.psi[PSXX_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, sxx_x);
+        cpml_q(f.psi[PSXY_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, sxy_x);
+        cpml_q(f.psi[PSXZ_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, sxz_x);
+    }
+}
+
+#define CELL3D_Q4                                                                      \
+    constexpr int F = 4;                                                               \
+    const int gz0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4 + F;                   \
+    const int gy = blockIdx.y * blockDim.y + threadIdx.y + F;                          \
+    const int gx = blockIdx.z * blockDim.z + threadIdx.z + F;                          \
+    if (gz0 > g.NZ - F - 1 || gy > g.NY - F - 1 || gx > g.NX - F - 1) return;          \
+    const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;                                        \
+    const i64 iv = gx * sx + (i64)gy * sy + gz0;                                       \
+    const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
+
+__global__ void __launch_bounds__(128) k_v3d_q4(Grid g, Fields f)
+{
+    CELL3D_Q4
+    const float *hc = g.hc;
+    Q4 vx = ldq_rw(f.w[VX] + iv), vy = ldq_rw(f.w[VY] + iv), vz = ldq_rw(f.w[VZ] + iv);
+    const Q4 rip = ldq(f.p[PRIP] + ip), rjp = ldq(f.p[PRJP] + ip), rkp = ldq(f.p[PRKP] + ip);
+    const W12 wzz = ldw(f.w[SZZ], iv), wxz = ldw(f.w[SXZ], iv), wyz = ldw(f.w[SYZ], iv);
+    Q4 szz_z = dfw_z<F>(wzz, hc);
+    Q4 sxx_x = dfw_q<F>(f.w[SXX], iv, sx, hc);
+    Q4 sxz_x = dbw_q<F>(f.w[SXZ], iv, sx, hc);
+    Q4 sxz_z = dbw_z<F>(wxz, hc);
+    Q4 syz_y = dbw_q<F>(f.w[SYZ], iv, sy, hc);
+    Q4 syz_z = dbw_z<F>(wyz, hc);
+    Q4 syy_y = dfw_q<F>(f.w[SYY], iv, sy, hc);
+    Q4 sxy_x = dbw_q<F>(f.w[SXY], iv, sx, hc);
+    Q4 sxy_y = dbw_q<F>(f.w[SXY], iv, sy, hc);
+    if (g.abs_type == 1) cpml_v3d_q4(g, f, gz0, gy, gx, sxx_x, syy_y, szz_z, sxy_y, sxy_x, syz_y, syz_z, sxz_x, sxz_z);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        float v3[3] = {vx.v[j] + (sxx_x.v[j] + sxy_y.v[j] + sxz_z.v[j]) * rip.v[j],
+                       vy.v[j] + (syy_y.v[j] + sxy_x.v[j] + syz_z.v[j]) * rjp.v[j],
+                       vz.v[j] + (szz_z.v[j] + sxz_x.v[j] + syz_y.v[j]) * rkp.v[j]};
+        if (g.abs_type == 2) taper_regs<3>(g, f.taper, gz0 + j, gy, gx, v3);
+        vx.v[j] = v3[0]; vy.v[j] = v3[1]; vz.v[j] = v3[2];
+    }
+    stq(f.w[VX] + iv, vx);
+    stq(f.w[VY] + iv, vy);
+    stq(f.w[VZ] + iv, vz);
+}
+
+// CPML corrections of cpml_s3d (forward form) for a quad of z cells
+__device__ __forceinline__ void cpml_s3d_q4(const Grid &g, const Fields &f, int gz0, int gy, int gx, Q4 &vxx,
+                                            Q4 &vxy, Q4 &vxz, Q4 &vyx, Q4 &vyy, Q4 &vyz, Q4 &vzx, Q4 &vzy, Q4 &vzz)
+{
+    const int F = g.F, NAB = g.nab, NZ = g.NZ, NY = g.NY, NX = g.NX;
+    const i64 nz = g.nz, ny = g.ny;
+    // with NAB % 4 == 0 a quad lies in at most one z slab, entirely (the two
+    // plain ifs of cpml_s3d can only both hold when the slabs overlap, which
+    // needs nz < 2 NAB + 4 and takes the per-cell path)
+    const bool zq = NAB % 4 == 0 && g.nz >= 2 * NAB + 4;
+    if (zq && gz0 > NZ - NAB - F - 1) {
+        i64 i = gx - F, jj = gy - F, k = gz0 - NZ + NAB + F + NAB;
+        int ind = 2 * NAB - 1 - (int)k;
+        i64 q = (i * ny + jj) * (2 * NAB) + k;
+        cpml_zq(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, -1, vxz);
+        cpml_zq(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, -1, vyz);
+        cpml_zq(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, -1, vzz);
+    } else if (zq && !g.freesurf && gz0 - F < NAB) {
+        i64 i = gx - F, jj = gy - F, k = gz0 - F;
+        i64 q = (i * ny + jj) * (2 * NAB) + k;
+        cpml_zq(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, 1, vxz);
+        cpml_zq(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, 1, vyz);
+        cpml_zq(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, 1, vzz);
+    } else if (!zq && (gz0 + 3 > NZ - NAB - F - 1 || (!g.freesurf && gz0 - F < NAB))) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int gz = gz0 + j;
+            if (gz > NZ - NAB - F - 1) {
+                i64 i = gx - F, jj = gy - F, k = gz - NZ + NAB + F + NAB;
+                int ind = 2 * NAB - 1 - (int)k;
+                i64 q = (i * ny + jj) * (2 * NAB) + k;
+                cpml(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, vxz.v[j]);
+                cpml(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, vyz.v[j]);
+                cpml(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, vzz.v[j]);
+            }
+            if (!g.freesurf && gz - F < NAB) {
+                i64 i = gx - F, jj = gy - F, k = gz - F;
+                i64 q = (i * ny + jj) * (2 * NAB) + k;
+                cpml(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, vxz.v[j]);
+                cpml(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, vyz.v[j]);
+                cpml(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, vzz.v[j]);
+            }
+        }
+    }
+    const i64 k0 = gz0 - F;
+    if (gy - F < NAB) {
+        i64 i = gx - F, j = gy - F;
+        i64 q = (i * (2 * NAB) + j) * nz + k0;
+        cpml_q(f.psi[PVX_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, vxy);
+        cpml_q(f.psi[PVY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], (int)j, vyy);
+        cpml_q(f.psi[PVZ_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, vzy);
+    }
+    if (gy > NY - NAB - F - 1) {
+        i64 i = gx - F, j = gy - NY + NAB + F + NAB;
+        int ind = 2 * NAB - 1 - (int)j;
+        i64 q = (i * (2 * NAB) + j) * nz + k0;
+        cpml_q(f.psi[PVX_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, vxy);
+        cpml_q(f.psi[PVY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], ind + 1, vyy);
+        cpml_q(f.psi[PVZ_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, vzy);
+    }
+    if (gx - F < NAB) {
+        i64 i = gx - F, j = gy - F;
+        i64 q = (i * ny + j) * nz + k0;
+        cpml_q(f.psi[PVX_X], q, f.cx[CK], f.cx[CA], f.cx[CB], (int)i, vxx);
+        cpml_q(f.psi[PVY_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, vyx);
+        cpml_q(f.psi[PVZ_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, vzx);
+    }
+    if (gx > NX - NAB - F - 1) {
+        i64 i = gx - NX + NAB + F + NAB, j = gy - F;
+        int ind = 2 * NAB - 1 - (int)i;
+        i64 q = (i * ny + j) * nz + k0;
+        cpml_q(f.psi[PVX_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, vxx);
+        cpml_q(f.psi[PVY_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, vyx);
+        cpml_q(f.psi[PVZ_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, vzx);
+    }
+}
+
+// Stress and memory-variable update of four z cells (the arithmetic of
+// k_s3d_stream per cell).  The per-cell work runs in two phases -- normal
+// stresses (sxx, syy, szz with rxx, ryy, rzz) then shear stresses (sxy, syz,
+// sxz with rxy, ryz, rxz) -- each loading only its own memory variables and
+// parameters, so the live state fits in registers; the components are
+// independent, so the split changes no result.
+template <int L>
+__device__ __forceinline__ void s_normal_q4(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip,
+                                            const Q4 &vxx,
+                                            const Q4 &vyy, const Q4 &vzz)
+{
+    float *const ws[3] = {f.w[SXX], f.w[SYY], f.w[SZZ]};
+    float *const wr[3] = {f.r[RXX], f.r[RYY], f.r[RZZ]};
+    Q4 sq[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) sq[q] = ldq_rw(ws[q] + iv);
+    const Q4 qM = ldq(f.p[PM] + ip), qmu = ldq(f.p[PMU] + ip);
+    if constexpr (L == 0) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float vxxyyzz = vxx.v[j] + vyy.v[j] + vzz.v[j], vyyzz = vyy.v[j] + vzz.v[j];
+            float vxxzz = vxx.v[j] + vzz.v[j], vxxyy = vxx.v[j] + vyy.v[j];
+            float gm = qM.v[j], fm = 2.0f * qmu.v[j];
+            sq[0].v[j] += gm * vxxyyzz - fm * vyyzz;
+            sq[1].v[j] += gm * vxxyyzz - fm * vxxzz;
+            sq[2].v[j] += gm * vxxyyzz - fm * vxxyy;
+        }
+    } else {
+        const Q4 qtaup = ldq(f.p[PTAUP] + ip), qtaus = ldq(f.p[PTAUS] + ip);
+        Q4 rq[3][L];
+#pragma unroll
+        for (int l = 0; l < L; l++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) rq[q][l] = ldq_rw(wr[q] + l * g.nvol + iv);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float vxxyyzz = vxx.v[j] + vyy.v[j] + vzz.v[j], vyyzz = vyy.v[j] + vzz.v[j];
+            float vxxzz = vxx.v[j] + vzz.v[j], vxxyy = vxx.v[j] + vyy.v[j];
+            const float lM = qM.v[j], lmu = qmu.v[j], ltaup = qtaup.v[j], ltaus = qtaus.v[j];
+            float gm = lM * (1.0f + (float)L * ltaup);
+            float fm = 2.0f * lmu * (1.0f + (float)L * ltaus);
+            float d = 2.0f * lmu * ltaus / g.dt, e = lM * ltaup / g.dt;
+            float a[3] = {0, 0, 0};
+#pragma unroll
+            for (int l = 0; l < L; l++)
+#pragma unroll
+                for (int q = 0; q < 3; q++) a[q] += rq[q][l].v[j];
+            float ls[3] = {(gm * vxxyyzz - fm * vyyzz) + g.dt2 * a[0], (gm * vxxyyzz - fm * vxxzz) + g.dt2 * a[1],
+                           (gm * vxxyyzz - fm * vxxyy) + g.dt2 * a[2]};
+            a[0] = a[1] = a[2] = 0;
+#pragma unroll
+            for (int l = 0; l < L; l++) {
+                float el = g.eta[l];
+                float b = 1.0f / (1.0f + el * 0.5f), c = 1.0f - el * 0.5f;
+                rq[0][l].v[j] = b * (rq[0][l].v[j] * c - el * (e * vxxyyzz - d * vyyzz));
+                rq[1][l].v[j] = b * (rq[1][l].v[j] * c - el * (e * vxxyyzz - d * vxxzz));
+                rq[2][l].v[j] = b * (rq[2][l].v[j] * c - el * (e * vxxyyzz - d * vxxyy));
+#pragma unroll
+                for (int q = 0; q < 3; q++) a[q] += rq[q][l].v[j];
+            }
+#pragma unroll
+            for (int q = 0; q < 3; q++) sq[q].v[j] += ls[q] + g.dt2 * a[q];
+        }
+#pragma unroll
+        for (int l = 0; l < L; l++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) stq(wr[q] + l * g.nvol + iv, rq[q][l]);
+    }
+    if (g.abs_type == 2) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float v3[3] = {sq[0].v[j], sq[1].v[j], sq[2].v[j]};
+            taper_regs<3>(g, f.taper, gz0 + j, gy, gx, v3);
+#pragma unroll
+            for (int q = 0; q < 3; q++) sq[q].v[j] = v3[q];
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++) stq(ws[q] + iv, sq[q]);
+}
+
+template <int L>
+__device__ __forceinline__ void s_shear_q4(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip,
+                                           const Q4 &vxyyx,
+                                           const Q4 &vyzzy, const Q4 &vxzzx)
+{
+    float *const ws[3] = {f.w[SXY], f.w[SYZ], f.w[SXZ]};
+    float *const wr[3] = {f.r[RXY], f.r[RYZ], f.r[RXZ]};
+    Q4 sq[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) sq[q] = ldq_rw(ws[q] + iv);
+    const Q4 qmuipjp = ldq(f.p[PMUIPJP] + ip), qmujpkp = ldq(f.p[PMUJPKP] + ip), qmuipkp = ldq(f.p[PMUIPKP] + ip);
+    if constexpr (L == 0) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            sq[0].v[j] += qmuipjp.v[j] * vxyyx.v[j];
+            sq[1].v[j] += qmujpkp.v[j] * vyzzy.v[j];
+            sq[2].v[j] += qmuipkp.v[j] * vxzzx.v[j];
+        }
+    } else {
+        const Q4 qtausipjp = ldq(f.p[PTAUSIPJP] + ip), qtausjpkp = ldq(f.p[PTAUSJPKP] + ip),
+                 qtausipkp = ldq(f.p[PTAUSIPKP] + ip);
+        Q4 rq[3][L];
+#pragma unroll
+        for (int l = 0; l < L; l++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) rq[q][l] = ldq_rw(wr[q] + l * g.nvol + iv);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const float lmuipkp = qmuipkp.v[j], lmuipjp = qmuipjp.v[j], lmujpkp = qmujpkp.v[j];
+            const float ltausipkp = qtausipkp.v[j], ltausipjp = qtausipjp.v[j], ltausjpkp = qtausjpkp.v[j];
+            float fipjp = lmuipjp * (1.0f + (float)L * ltausipjp);
+            float fjpkp = lmujpkp * (1.0f + (float)L * ltausjpkp);
+            float fipkp = lmuipkp * (1.0f + (float)L * ltausipkp);
+            float dipjp = lmuipjp * ltausipjp / g.dt, djpkp = lmujpkp * ltausjpkp / g.dt,
+                  dipkp = lmuipkp * ltausipkp / g.dt;
+            float a[3] = {0, 0, 0};
+#pragma unroll
+            for (int l = 0; l < L; l++)
+#pragma unroll
+                for (int q = 0; q < 3; q++) a[q] += rq[q][l].v[j];
+            float ls[3] = {fipjp * vxyyx.v[j] + g.dt2 * a[0], fjpkp * vyzzy.v[j] + g.dt2 * a[1],
+                           fipkp * vxzzx.v[j] + g.dt2 * a[2]};
+            a[0] = a[1] = a[2] = 0;
+#pragma unroll
+            for (int l = 0; l < L; l++) {
+                float el = g.eta[l];
+                float b = 1.0f / (1.0f + el * 0.5f), c = 1.0f - el * 0.5f;
+                rq[0][l].v[j] = b * (rq[0][l].v[j] * c - el * (dipjp * vxyyx.v[j]));
+                rq[1][l].v[j] = b * (rq[1][l].v[j] * c - el * (djpkp * vyzzy.v[j]));
+                rq[2][l].v[j] = b * (rq[2][l].v[j] * c - el * (dipkp * vxzzx.v[j]));
+#pragma unroll
+                for (int q = 0; q < 3; q++) a[q] += rq[q][l].v[j];
+            }
+#pragma unroll
+            for (int q = 0; q < 3; q++) sq[q].v[j] += ls[q] + g.dt2 * a[q];
+        }
+#pragma unroll
+        for (int l = 0; l < L; l++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) stq(wr[q] + l * g.nvol + iv, rq[q][l]);
+    }
+    if (g.abs_type == 2) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float v3[3] = {sq[0].v[j], sq[1].v[j], sq[2].v[j]};
+            taper_regs<3>(g, f.taper, gz0 + j, gy, gx, v3);
+#pragma unroll
+            for (int q = 0; q < 3; q++) sq[q].v[j] = v3[q];
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++) stq(ws[q] + iv, sq[q]);
+}
+
+template <int L>
+__global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f)
+{
+    CELL3D_Q4
+    const float *hc = g.hc;
+    Q4 vzz = dbw_z<F>(ldw(f.w[VZ], iv), hc);
+    Q4 vyz = dfw_z<F>(ldw(f.w[VY], iv), hc);
+    Q4 vxz = dfw_z<F>(ldw(f.w[VX], iv), hc);
+    Q4 vzx = dfw_q<F>(f.w[VZ], iv, sx, hc), vzy = dfw_q<F>(f.w[VZ], iv, sy, hc);
+    Q4 vyx = dfw_q<F>(f.w[VY], iv, sx, hc), vyy = dbw_q<F>(f.w[VY], iv, sy, hc);
+    Q4 vxx = dbw_q<F>(f.w[VX], iv, sx, hc), vxy = dfw_q<F>(f.w[VX], iv, sy, hc);
+    if (g.abs_type == 1) cpml_s3d_q4(g, f, gz0, gy, gx, vxx, vxy, vxz, vyx, vyy, vyz, vzx, vzy, vzz);
+    Q4 vxyyx, vyzzy, vxzzx;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        vxyyx.v[j] = vxy.v[j] + vyx.v[j];
+        vyzzy.v[j] = vyz.v[j] + vzy.v[j];
+        vxzzx.v[j] = vxz.v[j] + vzx.v[j];
+    }
+    s_normal_q4<L>(g, f, gz0, gy, gx, iv, ip, vxx, vyy, vzz);
+    s_shear_q4<L>(g, f, gz0, gy, gx, iv, ip, vxyyx, vyzzy, vxzzx);
+}
+
+// true when the 4-cell kernels apply to this grid
+static inline bool q4_ok(const Grid &g) { return g.nd == 3 && g.F == 4 && g.nz % 4 == 0 && !g.fhalf; }
+
 template <int F, int L, class T = float>
 __global__ void __launch_bounds__(256, 2) k_s3d_stream(Grid g, Fields f)
 {
@@ -1586,8 +2089,9 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
         DISPATCH_F(g.F, k_v3d_stream<FF, __half><<<gr, b, 0, st>>>(g, f));
         return;
     }
-    // kernels 0 takes the streaming velocity kernel (0.52 ms at 256^3, against
-    // 0.58 general and 0.63 TMA); only kernels 3 takes the TMA path here
+    // kernels 0 takes the 4-cell vectorised kernel where it applies (0.43 ms
+    // at 256^3, against 0.57 streaming, 0.58 general and 0.63 TMA), else the
+    // streaming one; only kernels 3 takes the TMA path
     if (g.kernels == 3 && launch_update_v_tma(g, f, st)) return;
     if (g.kernels == 2 && launch_update_v_fast(g, f, st)) return;
     if (g.nd == 21 || g.nd == 22) {
@@ -1597,8 +2101,13 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
         return;
     }
     if (g.nd == 3) {
+        if ((g.kernels == 0 || g.kernels == 5) && q4_ok(g)) {
+            dim3 b(32, 2, 2), gr(cdiv(g.nz / 4, 32), cdiv(g.ny, 2), cdiv(g.nx, 2));
+            k_v3d_q4<<<gr, b, 0, st>>>(g, f);
+            return;
+        }
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
-        if (g.kernels == 0 || g.kernels == 4) {
+        if (g.kernels == 0 || g.kernels == 4 || g.kernels == 5) {
             DISPATCH_F(g.F, k_v3d_stream<FF><<<gr, b, 0, st>>>(g, f));
             return;
         }
@@ -1621,7 +2130,9 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
         }
         return;
     }
-    if ((g.kernels == 0 || g.kernels == 3) && launch_update_s_tma(g, f, st)) return;
+    // kernels 0: the 4-cell vectorised kernel where it applies (0.74 ms at
+    // 256^3, against 0.96 TMA and 0.98 streaming), else the streaming one
+    if (g.kernels == 3 && launch_update_s_tma(g, f, st)) return;
     if (g.kernels == 2 && launch_update_s_fast(g, f, st)) return;
     if (g.nd == 21 || g.nd == 22) {
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
@@ -1631,7 +2142,17 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
     }
     if (g.nd == 3) {
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
-        if ((g.kernels == 0 || g.kernels == 4) && g.L <= 3) {
+        if ((g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) {
+            dim3 b4(32, 2, 2), g4(cdiv(g.nz / 4, 32), cdiv(g.ny, 2), cdiv(g.nx, 2));
+            switch (g.L) {
+            case 0: k_s3d_q4<0><<<g4, b4, 0, st>>>(g, f); break;
+            case 1: k_s3d_q4<1><<<g4, b4, 0, st>>>(g, f); break;
+            case 2: k_s3d_q4<2><<<g4, b4, 0, st>>>(g, f); break;
+            default: k_s3d_q4<3><<<g4, b4, 0, st>>>(g, f); break;
+            }
+            return;
+        }
+        if ((g.kernels == 0 || g.kernels == 4 || g.kernels == 5) && g.L <= 3) {
             switch (g.L) {
             case 0: DISPATCH_F(g.F, k_s3d_stream<FF, 0><<<gr, b, 0, st>>>(g, f)); break;
             case 1: DISPATCH_F(g.F, k_s3d_stream<FF, 1><<<gr, b, 0, st>>>(g, f)); break;
@@ -1645,6 +2166,18 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
         DISPATCH_F(g.F, k_s2d<FF><<<gr, b, 0, st>>>(g, f));
     }
+}
+
+int stress_family(const Grid &g, const Fields &f)
+{
+    // the same selection as launch_update_s
+    if (g.nd != 3) return 0;
+    if (g.fhalf && g.L <= 3) return 4;
+    if (g.kernels == 3 && tma_ready(g, f)) return 3;
+    if (g.kernels == 2) return 2;
+    if ((g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) return 5;
+    if ((g.kernels == 0 || g.kernels == 4 || g.kernels == 5) && g.L <= 3) return 4;
+    return 1;
 }
 
 void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st)

@@ -21,6 +21,9 @@ bool launch_update_v_tma(const Grid &g, const Fields &f, cudaStream_t st);
 bool launch_update_s_tma(const Grid &g, const Fields &f, cudaStream_t st);
 bool tma_ready(const Grid &g, const Fields &f);  // the TMA kernels will run for this plan
 int tma_take_status();      // 1 if a TMA stage of the last launches never arrived (and clears it)
+// 3D stress-update family of a plan: 0 not 3D, 1 general, 2 register-blocked,
+// 3 TMA-pipelined, 4 streaming, 5 4-cell vectorised
+int stress_family(const Grid &g, const Fields &f);
 void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st);
 void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st);
 void launch_savebnd(const Grid &g, const Fields &f, const BndSlot &b, int prec, int64_t tofs, cudaStream_t st);

@@ -720,7 +720,7 @@ std::vector<CacheEntry> g_cache;
 
 bool eligible(const Grid &g)
 {
-    return g.nd == 3 && g.F == TF && (g.kernels == 0 || g.kernels == 3) && g.nz % 4 == 0 && g.NZ % 4 == 0 &&
+    return g.nd == 3 && g.F == TF && g.kernels == 3 && g.nz % 4 == 0 && g.NZ % 4 == 0 &&
            g.L >= 0 && g.L <= 3;
 }
 

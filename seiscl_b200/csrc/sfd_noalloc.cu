@@ -128,7 +128,7 @@ extern "C" int sfd_forward_noalloc(sfd_plan *p, const float *src_pos, const floa
     size_t off_w = need; need += align256(sizeof(float) * g.nvol * nwave);
     size_t off_r = need; need += align256(sizeof(float) * g.nvol * g.L * nmem);
     int64_t psi_total = 0;
-    for (int i = 0; i < NPSI; i++) psi_total += p->psi_size[i];
+    for (int i = 0; i < NPSI; i++) psi_total += psi_span(p->psi_size[i]);
     size_t off_psi = need; need += align256(sizeof(float) * psi_total);
     size_t off_map = need;
     need += align256(sizeof(int64_t) * (size_t)(nsrc + nrec)) + align256(sizeof(int) * 5 * (size_t)nsrc) +
@@ -162,7 +162,7 @@ extern "C" int sfd_forward_noalloc(sfd_plan *p, const float *src_pos, const floa
     int64_t poff = 0;
     for (int i = 0; i < NPSI; i++) {
         f.psi[i] = p->psi_size[i] ? (float *)(base + off_psi) + poff : nullptr;
-        poff += p->psi_size[i];
+        poff += psi_span(p->psi_size[i]);
     }
     unsigned char *m = base + off_map;
     int64_t *scell = (int64_t *)m;

@@ -62,6 +62,7 @@ EXPORTS = {
     "sfd_residual_scale": (C.c_int, [C.c_void_p, C.POINTER(sfd_shot), C.POINTER(C.c_int), C.POINTER(FP)]),
     "sfd_plan_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "sfd_plan_uses_tma": (C.c_int, [C.c_void_p]),
+    "sfd_plan_kernel_family": (C.c_int, [C.c_void_p]),
     "sfd_debug_copy": (C.c_int64, [C.c_void_p, C.c_int, C.c_int, FP, C.c_int64]),
     "sfd_last_loop_ms": (C.c_float, [C.c_void_p]),
     "sfd_bench_kernels": (C.c_int, [C.c_void_p, C.c_int, FP]),
@@ -134,8 +135,8 @@ class Config:
     param_type: int = 0
     restype: int = 0
     precision: str = "fp32"
-    kernels: str = "fast"  # "fast" (3D: streaming velocity, TMA or streaming stress), "general", "register",
-    #                        "tma", "stream"
+    kernels: str = "fast"  # "fast" (3D: 4-cell vectorised where eligible, else streaming), "general",
+    #                        "register", "tma", "stream", "vector"
     adjoint_reset_psi: bool = False  # True: the adjoint starts from zeroed CPML memory (not the reference's)
     field_precision: str = "fp32"  # "fp16": wave fields / memory variables stored in FP16 (3D forward)
     back_prop_type: int = 1  # 1: boundary-saving backpropagation, 2: DFT gradient at `gradfreqs`
@@ -170,7 +171,7 @@ class Config:
         c.param_type = int(self.param_type)
         c.restype = int(self.restype)
         c.precision = PREC[self.precision]
-        c.kernels = {"fast": 0, "general": 1, "register": 2, "tma": 3, "stream": 4}[self.kernels]
+        c.kernels = {"fast": 0, "general": 1, "register": 2, "tma": 3, "stream": 4, "vector": 5}[self.kernels]
         c.adjoint_reset_psi = 1 if self.adjoint_reset_psi else 0
         c.field_precision = {"fp32": 0, "fp16": 1}[self.field_precision]
         c.back_prop_type = int(self.back_prop_type)
@@ -340,6 +341,15 @@ class Plan:
         if rc < 0:
             self._check(rc)
         return rc == 1
+
+    @property
+    def kernel_family(self) -> str:
+        """Kernel family of the 3D stress update ("general", "register",
+        "tma", "stream", "vector"; "2d" for 2D plans)."""
+        rc = int(self.lib.sfd_plan_kernel_family(self.h))
+        if rc < 0:
+            self._check(rc)
+        return ["2d", "general", "register", "tma", "stream", "vector"][rc]
 
     @property
     def last_loop_ms(self) -> float:

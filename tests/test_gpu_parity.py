@@ -130,6 +130,11 @@ FAST_CASES = [
     dict(nd=3, freesurf=0, L=0, abs_type=1, src_type=2, nz=68, ny=35, nx=22, nt=60, nab=5),
     dict(nd=3, freesurf=0, L=1, abs_type=2, src_type=0, nz=40, ny=20, nx=44, nt=60, nab=6),
     dict(nd=3, freesurf=1, L=3, abs_type=1, src_type=100, nz=36, ny=18, nx=40, nt=60, nab=6),
+    # nab % 4 == 0: the vectorised kernels' whole-quad z-slab CPML path; the
+    # last case is below nz = 2 nab + 4, which takes the per-cell path
+    dict(nd=3, freesurf=0, L=2, abs_type=1, src_type=100, nz=40, ny=30, nx=34, nt=60, nab=8),
+    dict(nd=3, freesurf=1, L=1, abs_type=1, src_type=2, nz=44, ny=26, nx=30, nt=60, nab=4),
+    dict(nd=3, freesurf=1, L=0, abs_type=1, src_type=1, nz=16, ny=26, nx=22, nt=50, nab=8),
     # not eligible (odd nz tiles, other orders): register-blocked kernels only
     dict(nd=3, freesurf=1, L=2, abs_type=1, src_type=100, nz=38, ny=29, nx=31, nt=80, nab=6),
     dict(nd=3, freesurf=0, L=1, abs_type=2, src_type=2, nz=70, ny=35, nx=22, nt=60, nab=5),
@@ -141,9 +146,10 @@ FAST_CASES = [
 @pytest.mark.gpu
 @pytest.mark.parametrize("kw", FAST_CASES, ids=lambda k: "-".join("%s%s" % (a, b) for a, b in k.items()))
 def test_fast_3d_kernels_match_general(kw, cuda_device):
-    """The TMA-pipelined and register-blocked 3D kernels against the general
-    ones (ragged tiles, CPML and taper, free surface, L = 0..3, FDORDER
-    4/8/12) and the oracle.  Eligible cases must actually take the TMA path."""
+    """The vectorised, TMA-pipelined, streaming and register-blocked 3D
+    kernels against the general ones (ragged tiles, CPML and taper, free
+    surface, L = 0..3, FDORDER 4/8/12) and the oracle.  Eligible cases must
+    actually take the vectorised (default) and TMA paths."""
     import dataclasses
 
     from oracle.oracle import Oracle
@@ -152,21 +158,22 @@ def test_fast_3d_kernels_match_general(kw, cuda_device):
     cfg, model, acq = make_case(**kw)
     outs = _outputs(3)
     res = {}
-    for variant in ("fast", "tma", "stream", "register", "general"):
+    for variant in ("fast", "tma", "stream", "register", "vector", "general"):
         ec = dataclasses.replace(engine_config(cfg), kernels=variant)
         plan = Plan(ec)
         plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
-        if variant in ("fast", "tma"):
-            eligible = kw.get("fdorder", 8) == 8 and kw["nz"] % 4 == 0
-            assert plan.uses_tma == eligible
-        else:
-            assert not plan.uses_tma
+        eligible = kw.get("fdorder", 8) == 8 and kw["nz"] % 4 == 0
+        assert plan.uses_tma == (variant == "tma" and eligible)
+        want = {"fast": "vector" if eligible else "stream", "vector": "vector" if eligible else "stream",
+                "tma": "tma" if eligible else "general", "stream": "stream", "register": "register",
+                "general": "general"}[variant]
+        assert plan.kernel_family == want, (variant, plan.kernel_family)
         res[variant] = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
     ora = Oracle(cfg)
     ora.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
     ref = ora.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
     for n in outs:
-        for v in ("fast", "tma", "stream", "register"):
+        for v in ("fast", "tma", "stream", "register", "vector"):
             e_gen, e_ref = rel_l2(res[v][n], res["general"][n]), rel_l2(res[v][n], ref[n])
             assert e_gen < FAST_TOL and e_ref < FWD_TOL, (v, n, e_gen, e_ref)
 
