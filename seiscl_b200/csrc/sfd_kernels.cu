@@ -1193,6 +1193,432 @@ __global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f)
     s_shear_q4<L>(g, f, gz0, gy, gx, iv, ip, vxyyx, vyzzy, vxzzx);
 }
 
+// ------------------------------------------- 4-cell vectorised 3D adjoint
+// The adjoint kernels of k_adjv3d / k_adjs3d on quads of z cells, with the
+// same per-cell arithmetic: backpropagation of the forward field (not for
+// the DFT gradient, g.bp2), saved-boundary injection per cell, the adjoint
+// update with CPML, and the on-the-fly gradient accumulated in FP64.
+__device__ __forceinline__ void grad_add4(double *g, i64 ip, const float (&d)[4])
+{
+    double2 *p = reinterpret_cast<double2 *>(g + ip);
+    double2 a = p[0], b = p[1];
+    a.x += (double)d[0]; a.y += (double)d[1]; b.x += (double)d[2]; b.y += (double)d[3];
+    p[0] = a;
+    p[1] = b;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_adjv3d_q4(Grid g, Fields f, AdjFields a)
+{
+    CELL3D_Q4
+    const float *hc = g.hc;
+    const Q4 rip = ldq(f.p[PRIP] + ip), rjp = ldq(f.p[PRJP] + ip), rkp = ldq(f.p[PRKP] + ip);
+    Q4 vx = {{0, 0, 0, 0}}, vy = vx, vz = vx;
+    if (!g.bp2) {  // backpropagate the forward velocities (update_adjv3D.cl:297-340)
+        Q4 szz_z = dfw_z<F>(ldw(f.w[SZZ], iv), hc);
+        Q4 sxx_x = dfw_q<F>(f.w[SXX], iv, sx, hc);
+        Q4 sxz_x = dbw_q<F>(f.w[SXZ], iv, sx, hc);
+        Q4 sxz_z = dbw_z<F>(ldw(f.w[SXZ], iv), hc);
+        Q4 syz_y = dbw_q<F>(f.w[SYZ], iv, sy, hc);
+        Q4 syz_z = dbw_z<F>(ldw(f.w[SYZ], iv), hc);
+        Q4 syy_y = dfw_q<F>(f.w[SYY], iv, sy, hc);
+        Q4 sxy_x = dbw_q<F>(f.w[SXY], iv, sx, hc);
+        Q4 sxy_y = dbw_q<F>(f.w[SXY], iv, sy, hc);
+        vx = ldq_rw(f.w[VX] + iv); vy = ldq_rw(f.w[VY] + iv); vz = ldq_rw(f.w[VZ] + iv);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            vx.v[j] = vx.v[j] - (sxx_x.v[j] + sxy_y.v[j] + sxz_z.v[j]) * rip.v[j];
+            vy.v[j] = vy.v[j] - (syy_y.v[j] + sxy_x.v[j] + syz_z.v[j]) * rjp.v[j];
+            vz.v[j] = vz.v[j] - (szz_z.v[j] + sxz_x.v[j] + syz_y.v[j]) * rkp.v[j];
+            const int m = inject_ind3d(g, gz0 + j, gy, gx);
+            if (m != -1) {
+                vx.v[j] = to_f<T>(((const T *)a.bnd[VX])[m]);
+                vy.v[j] = to_f<T>(((const T *)a.bnd[VY])[m]);
+                vz.v[j] = to_f<T>(((const T *)a.bnd[VZ])[m]);
+            }
+        }
+        stq(f.w[VX] + iv, vx); stq(f.w[VY] + iv, vy); stq(f.w[VZ] + iv, vz);
+    }
+    Q4 szz_zr = dfw_z<F>(ldw(a.wr[SZZ], iv), hc);
+    Q4 sxx_xr = dfw_q<F>(a.wr[SXX], iv, sx, hc);
+    Q4 sxz_xr = dbw_q<F>(a.wr[SXZ], iv, sx, hc);
+    Q4 sxz_zr = dbw_z<F>(ldw(a.wr[SXZ], iv), hc);
+    Q4 syz_yr = dbw_q<F>(a.wr[SYZ], iv, sy, hc);
+    Q4 syz_zr = dbw_z<F>(ldw(a.wr[SYZ], iv), hc);
+    Q4 syy_yr = dfw_q<F>(a.wr[SYY], iv, sy, hc);
+    Q4 sxy_xr = dbw_q<F>(a.wr[SXY], iv, sx, hc);
+    Q4 sxy_yr = dbw_q<F>(a.wr[SXY], iv, sy, hc);
+    if (g.abs_type == 1)
+        cpml_v3d_q4(g, f, gz0, gy, gx, sxx_xr, syy_yr, szz_zr, sxy_yr, sxy_xr, syz_yr, syz_zr, sxz_xr, sxz_zr);
+    Q4 wx = ldq_rw(a.wr[VX] + iv), wy = ldq_rw(a.wr[VY] + iv), wz = ldq_rw(a.wr[VZ] + iv);
+    float gr[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const float lvx = (sxx_xr.v[j] + sxy_yr.v[j] + sxz_zr.v[j]) * rip.v[j];
+        const float lvy = (syy_yr.v[j] + sxy_xr.v[j] + syz_zr.v[j]) * rjp.v[j];
+        const float lvz = (szz_zr.v[j] + sxz_xr.v[j] + syz_yr.v[j]) * rkp.v[j];
+        float w3[3] = {wx.v[j] + lvx, wy.v[j] + lvy, wz.v[j] + lvz};
+        if (g.abs_type == 2) taper_regs<3>(g, f.taper, gz0 + j, gy, gx, w3);
+        wx.v[j] = w3[0]; wy.v[j] = w3[1]; wz.v[j] = w3[2];
+        gr[j] = -vx.v[j] * lvx - vy.v[j] * lvy - vz.v[j] * lvz;
+    }
+    stq(a.wr[VX] + iv, wx); stq(a.wr[VY] + iv, wy); stq(a.wr[VZ] + iv, wz);
+    if (!g.bp2) grad_add4(a.grad[GRHO], ip, gr);
+}
+
+// CPML of the adjoint stress update (cpml_s3d with adjoint_form): as
+// cpml_s3d_q4, except that a cell in both z slabs or both y slabs takes
+// only the first (else-if), as update_adjs3D.cl does
+__device__ __forceinline__ void cpml_s3d_adj_q4(const Grid &g, const Fields &f, int gz0, int gy, int gx, Q4 &vxx,
+                                                Q4 &vxy, Q4 &vxz, Q4 &vyx, Q4 &vyy, Q4 &vyz, Q4 &vzx, Q4 &vzy,
+                                                Q4 &vzz)
+{
+    const int F = g.F, NAB = g.nab, NZ = g.NZ, NY = g.NY, NX = g.NX;
+    const i64 nz = g.nz, ny = g.ny;
+    const bool zq = NAB % 4 == 0 && g.nz >= 2 * NAB + 4;
+    if (zq && gz0 > NZ - NAB - F - 1) {
+        i64 i = gx - F, jj = gy - F, k = gz0 - NZ + NAB + F + NAB;
+        int ind = 2 * NAB - 1 - (int)k;
+        i64 q = (i * ny + jj) * (2 * NAB) + k;
+        cpml_zq(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, -1, vxz);
+        cpml_zq(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, -1, vyz);
+        cpml_zq(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, -1, vzz);
+    } else if (zq && !g.freesurf && gz0 - F < NAB) {
+        i64 i = gx - F, jj = gy - F, k = gz0 - F;
+        i64 q = (i * ny + jj) * (2 * NAB) + k;
+        cpml_zq(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, 1, vxz);
+        cpml_zq(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, 1, vyz);
+        cpml_zq(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, 1, vzz);
+    } else if (!zq && (gz0 + 3 > NZ - NAB - F - 1 || (!g.freesurf && gz0 - F < NAB))) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int gz = gz0 + j;
+            const bool zb = gz > NZ - NAB - F - 1;
+            if (zb) {
+                i64 i = gx - F, jj = gy - F, k = gz - NZ + NAB + F + NAB;
+                int ind = 2 * NAB - 1 - (int)k;
+                i64 q = (i * ny + jj) * (2 * NAB) + k;
+                cpml(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, vxz.v[j]);
+                cpml(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, vyz.v[j]);
+                cpml(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, vzz.v[j]);
+            } else if (!g.freesurf && gz - F < NAB) {
+                i64 i = gx - F, jj = gy - F, k = gz - F;
+                i64 q = (i * ny + jj) * (2 * NAB) + k;
+                cpml(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, vxz.v[j]);
+                cpml(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, vyz.v[j]);
+                cpml(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, vzz.v[j]);
+            }
+        }
+    }
+    const i64 k0 = gz0 - F;
+    if (gy - F < NAB) {
+        i64 i = gx - F, j = gy - F;
+        i64 q = (i * (2 * NAB) + j) * nz + k0;
+        cpml_q(f.psi[PVX_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, vxy);
+        cpml_q(f.psi[PVY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], (int)j, vyy);
+        cpml_q(f.psi[PVZ_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, vzy);
+    } else if (gy > NY - NAB - F - 1) {
+        i64 i = gx - F, j = gy - NY + NAB + F + NAB;
+        int ind = 2 * NAB - 1 - (int)j;
+        i64 q = (i * (2 * NAB) + j) * nz + k0;
+        cpml_q(f.psi[PVX_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, vxy);
+        cpml_q(f.psi[PVY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], ind + 1, vyy);
+        cpml_q(f.psi[PVZ_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, vzy);
+    }
+    if (gx - F < NAB) {
+        i64 i = gx - F, j = gy - F;
+        i64 q = (i * ny + j) * nz + k0;
+        cpml_q(f.psi[PVX_X], q, f.cx[CK], f.cx[CA], f.cx[CB], (int)i, vxx);
+        cpml_q(f.psi[PVY_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, vyx);
+        cpml_q(f.psi[PVZ_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, vzx);
+    }
+    if (gx > NX - NAB - F - 1) {
+        i64 i = gx - NX + NAB + F + NAB, j = gy - F;
+        int ind = 2 * NAB - 1 - (int)i;
+        i64 q = (i * ny + j) * nz + k0;
+        cpml_q(f.psi[PVX_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, vxx);
+        cpml_q(f.psi[PVY_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, vyx);
+        cpml_q(f.psi[PVZ_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, vzx);
+    }
+}
+
+template <int L, typename T>
+__global__ void __launch_bounds__(128, 4) k_adjs3d_q4(Grid g, Fields f, AdjFields a)
+{
+    CELL3D_Q4
+    const float *hc = g.hc;
+    // adjoint velocity derivatives, with CPML
+    Q4 vzzr = dbw_z<F>(ldw(a.wr[VZ], iv), hc), vyzr = dfw_z<F>(ldw(a.wr[VY], iv), hc);
+    Q4 vxzr = dfw_z<F>(ldw(a.wr[VX], iv), hc);
+    Q4 vzxr = dfw_q<F>(a.wr[VZ], iv, sx, hc), vzyr = dfw_q<F>(a.wr[VZ], iv, sy, hc);
+    Q4 vyxr = dfw_q<F>(a.wr[VY], iv, sx, hc), vyyr = dbw_q<F>(a.wr[VY], iv, sy, hc);
+    Q4 vxxr = dbw_q<F>(a.wr[VX], iv, sx, hc), vxyr = dfw_q<F>(a.wr[VX], iv, sy, hc);
+    if (g.abs_type == 1) cpml_s3d_adj_q4(g, f, gz0, gy, gx, vxxr, vxyr, vxzr, vyxr, vyyr, vyzr, vzxr, vzyr, vzzr);
+    Q4 rsh[3];   // adjoint shear sums vxy+vyx, vyz+vzy, vxz+vzx
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        rsh[0].v[j] = vxyr.v[j] + vyxr.v[j];
+        rsh[1].v[j] = vyzr.v[j] + vzyr.v[j];
+        rsh[2].v[j] = vxzr.v[j] + vzxr.v[j];
+    }
+    const Q4 qM = ldq(f.p[PM] + ip), qmu = ldq(f.p[PMU] + ip);
+    float gM[4] = {0, 0, 0, 0}, gmu[4] = {0, 0, 0, 0};
+
+    // ---- normal stresses (sxx, syy, szz) with rxx, ryy, rzz: the forward
+    // reconstruction of the quad, then its adjoint update
+    {
+        const int wid[3] = {SXX, SYY, SZZ}, rid[3] = {RXX, RYY, RZZ};
+        Q4 qtaup = {{0, 0, 0, 0}}, qtaus = qtaup;
+        if (L > 0) { qtaup = ldq(f.p[PTAUP] + ip); qtaus = ldq(f.p[PTAUS] + ip); }
+        Q4 s3[3] = {{{0, 0, 0, 0}}, {{0, 0, 0, 0}}, {{0, 0, 0, 0}}};
+        if (!g.bp2) {
+            const Q4 vzz = dbw_z<F>(ldw(f.w[VZ], iv), hc);
+            const Q4 vyy = dbw_q<F>(f.w[VY], iv, sy, hc);
+            const Q4 vxx = dbw_q<F>(f.w[VX], iv, sx, hc);
+#pragma unroll
+            for (int c = 0; c < 3; c++) s3[c] = ldq_rw(f.w[wid[c]] + iv);
+            Q4 rf[3][L > 0 ? L : 1];
+            if constexpr (L > 0) {
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+#pragma unroll
+                    for (int l = 0; l < L; l++) rf[c][l] = ldq_rw(f.r[rid[c]] + l * g.nvol + iv);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float lM = qM.v[j], lmu = qmu.v[j];
+                float gm = lM, fm = 2.0f * lmu, d = 0, e = 0;
+                if (L > 0) {
+                    const float ltaup = qtaup.v[j], ltaus = qtaus.v[j];
+                    gm = lM * (1.0f + (float)L * ltaup);
+                    fm = 2.0f * lmu * (1.0f + (float)L * ltaus);
+                    d = 2.0f * lmu * ltaus / g.dt; e = lM * ltaup / g.dt;
+                }
+                const float vxxyyzz = vxx.v[j] + vyy.v[j] + vzz.v[j], vyyzz = vyy.v[j] + vzz.v[j];
+                const float vxxzz = vxx.v[j] + vzz.v[j], vxxyy = vxx.v[j] + vyy.v[j];
+                const float fw[3] = {gm * vxxyyzz - fm * vyyzz, gm * vxxyyzz - fm * vxxzz, gm * vxxyyzz - fm * vxxyy};
+                if (L == 0) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) s3[c].v[j] -= fw[c];
+                } else {
+                    const float dc[3] = {e * vxxyyzz - d * vyyzz, e * vxxyyzz - d * vxxzz, e * vxxyyzz - d * vxxyy};
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        float aa = 0;
+#pragma unroll
+                        for (int l = 0; l < L; l++) aa += rf[c][l].v[j];
+                        const float ls = fw[c] + g.dt2 * aa;
+                        aa = 0;
+                        // 3D reconstruction keeps the forward-time coefficients (update_adjs3D.cl:357-359)
+#pragma unroll
+                        for (int l = 0; l < L; l++) {
+                            const float el = g.eta[l];
+                            const float b = 1.0f / (1.0f + el * 0.5f), cc = 1.0f - el * 0.5f;
+                            aa += b * (rf[c][l].v[j] * cc - el * dc[c]);
+                        }
+                        s3[c].v[j] -= ls + g.dt2 * aa;
+                    }
+                }
+                const int m = inject_ind3d(g, gz0 + j, gy, gx);
+                if (m != -1) {
+                    s3[0].v[j] = to_f<T>(((const T *)a.bnd[SXX])[m]);
+                    s3[1].v[j] = to_f<T>(((const T *)a.bnd[SYY])[m]);
+                    s3[2].v[j] = to_f<T>(((const T *)a.bnd[SZZ])[m]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 3; c++) stq(f.w[wid[c]] + iv, s3[c]);
+        }
+        Q4 rr[3][L > 0 ? L : 1];
+        if constexpr (L > 0) {
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int l = 0; l < L; l++) rr[c][l] = ldq_rw(a.rr[rid[c]] + l * g.nvol + iv);
+        }
+        Q4 w3[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) w3[c] = ldq_rw(a.wr[wid[c]] + iv);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const float lM = qM.v[j], lmu = qmu.v[j];
+            float gm = lM, fm = 2.0f * lmu, d = 0, e = 0;
+            if (L > 0) {
+                const float ltaup = qtaup.v[j], ltaus = qtaus.v[j];
+                gm = lM * (1.0f + (float)L * ltaup);
+                fm = 2.0f * lmu * (1.0f + (float)L * ltaus);
+                d = 2.0f * lmu * ltaus / g.dt; e = lM * ltaup / g.dt;
+            }
+            const float vxxyyzzr = vxxr.v[j] + vyyr.v[j] + vzzr.v[j], vyyzzr = vyyr.v[j] + vzzr.v[j];
+            const float vxxzzr = vxxr.v[j] + vzzr.v[j], vxxyyr = vxxr.v[j] + vyyr.v[j];
+            float ls[3] = {gm * vxxyyzzr - fm * vyyzzr, gm * vxxyyzzr - fm * vxxzzr, gm * vxxyyzzr - fm * vxxyyr};
+            if (L == 0) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) w3[c].v[j] += ls[c];
+            } else {
+                const float dc[3] = {e * vxxyyzzr - d * vyyzzr, e * vxxyyzzr - d * vxxzzr, e * vxxyyzzr - d * vxxyyr};
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    float aa = 0;
+#pragma unroll
+                    for (int l = 0; l < L; l++) aa += rr[c][l].v[j];
+                    ls[c] += g.dt2 * aa;
+                    // stored into the forward memory variables; the sum keeps the
+                    // last adjoint value (update_adjs3D.cl:566-583); in the DFT
+                    // adjoint both are one buffer, so that value is the new one
+#pragma unroll
+                    for (int l = 0; l < L; l++) {
+                        const float el = g.eta[l];
+                        const float b = 1.0f / (1.0f + el * 0.5f), cc = 1.0f - el * 0.5f;
+                        const float n = b * (rr[c][l].v[j] * cc - el * dc[c]);
+                        aa = g.bp2 ? n : rr[c][l].v[j];
+                        rr[c][l].v[j] = n;
+                    }
+                    w3[c].v[j] += ls[c] + g.dt2 * aa;
+                }
+            }
+            if (!g.bp2 && g.restype == 0) {
+                const float c1 = 1.0f / (3.0f * lM - 4.0f * lmu) / (3.0f * lM - 4.0f * lmu);
+                const float c3 = 1.0f / lmu / lmu;
+                const float c5 = 1.0f / 6.0f * c3;
+                const float sxx = s3[0].v[j], syy = s3[1].v[j], szz = s3[2].v[j];
+                const float dM = c1 * (sxx + syy + szz) * (ls[0] + ls[1] + ls[2]);
+                gM[j] = -dM;
+                gmu[j] = 4.0f / 3.0f * dM - c5 * (ls[0] * (2.0f * sxx - syy - szz) + ls[1] * (2.0f * syy - sxx - szz) +
+                                                  ls[2] * (2.0f * szz - sxx - syy));
+            } else if (!g.bp2) {
+                gM[j] = -((s3[0].v[j] + s3[1].v[j] + s3[2].v[j]) * (ls[0] + ls[1] + ls[2]));
+            }
+        }
+        // the new adjoint memory values go to the forward arrays
+        if constexpr (L > 0) {
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int l = 0; l < L; l++) stq(f.r[rid[c]] + l * g.nvol + iv, rr[c][l]);
+        }
+        if (g.abs_type == 2) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                float t3[3] = {w3[0].v[j], w3[1].v[j], w3[2].v[j]};
+                taper_regs<3>(g, f.taper, gz0 + j, gy, gx, t3);
+#pragma unroll
+                for (int c = 0; c < 3; c++) w3[c].v[j] = t3[c];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) stq(a.wr[wid[c]] + iv, w3[c]);
+    }
+
+    // ---- shear stresses, one at a time: sxy (x,y), syz (y,z), sxz (x,z)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const int wid = c == 0 ? SXY : (c == 1 ? SYZ : SXZ);
+        const int rid = c == 0 ? RXY : (c == 1 ? RYZ : RXZ);
+        const int pmu = c == 0 ? PMUIPJP : (c == 1 ? PMUJPKP : PMUIPKP);
+        const int ptau = c == 0 ? PTAUSIPJP : (c == 1 ? PTAUSJPKP : PTAUSIPKP);
+        const Q4 qmuc = ldq(f.p[pmu] + ip);
+        Q4 qtauc = {{0, 0, 0, 0}};
+        if (L > 0) qtauc = ldq(f.p[ptau] + ip);
+        Q4 sc = {{0, 0, 0, 0}};
+        if (!g.bp2) {
+            Q4 d1, d2;   // forward derivative pair (vxy+vyx, vyz+vzy, vxz+vzx)
+            if (c == 0) { d1 = dfw_q<F>(f.w[VX], iv, sy, hc); d2 = dfw_q<F>(f.w[VY], iv, sx, hc); }
+            else if (c == 1) { d1 = dfw_z<F>(ldw(f.w[VY], iv), hc); d2 = dfw_q<F>(f.w[VZ], iv, sy, hc); }
+            else { d1 = dfw_z<F>(ldw(f.w[VX], iv), hc); d2 = dfw_q<F>(f.w[VZ], iv, sx, hc); }
+            sc = ldq_rw(f.w[wid] + iv);
+            Q4 rf[L > 0 ? L : 1];
+            if constexpr (L > 0) {
+#pragma unroll
+                for (int l = 0; l < L; l++) rf[l] = ldq_rw(f.r[rid] + l * g.nvol + iv);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float fsum = d1.v[j] + d2.v[j];
+                const float lmuc = qmuc.v[j];
+                if (L == 0) {
+                    sc.v[j] -= lmuc * fsum;
+                } else {
+                    const float lt = qtauc.v[j];
+                    const float fc = lmuc * (1.0f + (float)L * lt), dc = lmuc * lt / g.dt;
+                    float aa = 0;
+#pragma unroll
+                    for (int l = 0; l < L; l++) aa += rf[l].v[j];
+                    const float ls = fc * fsum + g.dt2 * aa;
+                    aa = 0;
+#pragma unroll
+                    for (int l = 0; l < L; l++) {
+                        const float el = g.eta[l];
+                        const float b = 1.0f / (1.0f + el * 0.5f), cc = 1.0f - el * 0.5f;
+                        aa += b * (rf[l].v[j] * cc - el * (dc * fsum));
+                    }
+                    sc.v[j] -= ls + g.dt2 * aa;
+                }
+                const int m = inject_ind3d(g, gz0 + j, gy, gx);
+                if (m != -1) sc.v[j] = to_f<T>(((const T *)a.bnd[wid])[m]);
+            }
+            stq(f.w[wid] + iv, sc);
+        }
+        const Q4 rsum = rsh[c];
+        Q4 rr[L > 0 ? L : 1];
+        if constexpr (L > 0) {
+#pragma unroll
+            for (int l = 0; l < L; l++) rr[l] = ldq_rw(a.rr[rid] + l * g.nvol + iv);
+        }
+        Q4 wc = ldq_rw(a.wr[wid] + iv);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const float lmuc = qmuc.v[j];
+            float fc = lmuc, dc = 0;
+            if (L > 0) {
+                const float lt = qtauc.v[j];
+                fc = lmuc * (1.0f + (float)L * lt);
+                dc = lmuc * lt / g.dt;
+            }
+            float ls = fc * rsum.v[j];
+            if (L == 0) {
+                wc.v[j] += ls;
+            } else {
+                float aa = 0;
+#pragma unroll
+                for (int l = 0; l < L; l++) aa += rr[l].v[j];
+                ls += g.dt2 * aa;
+#pragma unroll
+                for (int l = 0; l < L; l++) {
+                    const float el = g.eta[l];
+                    const float b = 1.0f / (1.0f + el * 0.5f), cc = 1.0f - el * 0.5f;
+                    const float n = b * (rr[l].v[j] * cc - el * (dc * rsum.v[j]));
+                    aa = g.bp2 ? n : rr[l].v[j];
+                    rr[l].v[j] = n;
+                }
+                wc.v[j] += ls + g.dt2 * aa;
+            }
+            if (!g.bp2 && g.restype == 0) {
+                const float lmu = qmu.v[j];
+                const float c3 = 1.0f / lmu / lmu;
+                gmu[j] += -c3 * (sc.v[j] * ls);
+            }
+        }
+        if constexpr (L > 0) {
+#pragma unroll
+            for (int l = 0; l < L; l++) stq(f.r[rid] + l * g.nvol + iv, rr[l]);
+        }
+        if (g.abs_type == 2) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                float t1[1] = {wc.v[j]};
+                taper_regs<1>(g, f.taper, gz0 + j, gy, gx, t1);
+                wc.v[j] = t1[0];
+            }
+        }
+        stq(a.wr[wid] + iv, wc);
+    }
+    if (!g.bp2) {
+        grad_add4(a.grad[GM], ip, gM);
+        if (g.restype == 0) grad_add4(a.grad[GMU], ip, gmu);
+    }
+}
+
 // true when the 4-cell kernels apply to this grid
 static inline bool q4_ok(const Grid &g) { return g.nd == 3 && g.F == 4 && g.nz % 4 == 0 && !g.fhalf; }
 
@@ -2211,6 +2637,21 @@ void launch_savebnd(const Grid &g, const Fields &f, const BndSlot &b, int prec, 
 template <typename T>
 static void launch_adj_t(const Grid &g, const Fields &f, const AdjFields &a, bool stress, cudaStream_t st)
 {
+    if (g.nd == 3 && (g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) {
+        if (stress) {
+            dim3 b(16, 8, 1), gr(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1));
+            switch (g.L) {
+            case 0: k_adjs3d_q4<0, T><<<gr, b, 0, st>>>(g, f, a); break;
+            case 1: k_adjs3d_q4<1, T><<<gr, b, 0, st>>>(g, f, a); break;
+            case 2: k_adjs3d_q4<2, T><<<gr, b, 0, st>>>(g, f, a); break;
+            default: k_adjs3d_q4<3, T><<<gr, b, 0, st>>>(g, f, a); break;
+            }
+        } else {
+            dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4));
+            k_adjv3d_q4<T><<<gr, b, 0, st>>>(g, f, a);
+        }
+        return;
+    }
     if (g.nd == 3) {
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
         if (stress) DISPATCH_F(g.F, k_adjs3d<FF, T><<<gr, b, 0, st>>>(g, f, a))

@@ -127,6 +127,9 @@ DFT_CASES = [
     (dict(nd=2, freesurf=0, L=1, abs_type=2, src_type=100, nt=160, seed=33), [15.0], 1),
     (dict(nd=3, freesurf=1, L=1, abs_type=1, src_type=100, nz=34, ny=30, nx=36, nt=90, nab=8, seed=34), [20.0, 35.0], 0),
     (dict(nd=3, freesurf=0, L=0, abs_type=1, src_type=2, nz=34, ny=30, nx=36, nt=90, nab=8, seed=35), [25.0], 2),
+    # nz % 4 == 0: the 4-cell vectorised adjoint kernels in their DFT form
+    (dict(nd=3, freesurf=0, L=2, abs_type=1, src_type=100, nz=36, ny=30, nx=32, nt=90, nab=8, seed=38), [20.0, 35.0], 1),
+    (dict(nd=3, freesurf=1, L=0, abs_type=1, src_type=2, nz=40, ny=28, nx=30, nt=90, nab=6, seed=39), [25.0], 0),
 ]
 
 
