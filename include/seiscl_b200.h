@@ -97,7 +97,12 @@ typedef struct sfd_config {
                               by powers of two (src/assign_modeling_case.c:829-866). */
     int back_prop_type;    /* BACK_PROP_TYPE: 0 or 1 boundary-saving backpropagation,
                               2 DFT gradient at the frequencies of sfd_set_gradfreqs */
-    int reserved[3];
+    int loop_graphs;       /* time loops as CUDA graphs: 0 for 2D grids (whose steps are a
+                              few microseconds of work, so launches dominate), 1 always,
+                              2 never.  A graph is captured on the first shot of a shape
+                              and replayed while nothing its launches depend on changes.
+                              No reference counterpart (launch mechanics). */
+    int reserved[2];
 } sfd_config;
 
 typedef struct sfd_shot {

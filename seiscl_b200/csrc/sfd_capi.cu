@@ -290,6 +290,64 @@ int alloc_adjoint(sfd_plan *p)
     return SFD_OK;
 }
 
+// ----------------------------------------------------------- loop graphs
+// The bytes a time loop's launches bake in: kernel arguments by value and
+// the buffers they point to.  Equal keys => the captured graph is valid.
+struct LoopKey {
+    std::string s;
+    template <class T>
+    void add(const T &v) { s.append(reinterpret_cast<const char *>(&v), sizeof v); }
+    void add_points(const PointSet &q)
+    {
+        add(q.n); add(q.cell); add(q.ntarget); add(q.field); add(q.div); add(q.kz);
+    }
+};
+
+bool graphs_on(const sfd_plan *p)
+{
+    const int m = p->cfg.loop_graphs;
+    if (m == 2) return false;
+    if (m == 1) return p->g.kernels != 3;   // the TMA path sets kernel attributes on first use
+    return p->g.nd != 3;
+}
+
+void drop_graph(sfd_plan::LoopGraph &lg)
+{
+    if (lg.exec) cudaGraphExecDestroy(lg.exec);
+    lg.exec = nullptr;
+    lg.key.clear();
+}
+
+// Run a time loop: its launches go to `st` directly, or -- when graphs are
+// on -- through a graph captured from them and cached under `key`.
+template <class Body>
+int run_loop(sfd_plan *p, sfd_plan::LoopGraph &lg, const std::string &key, cudaStream_t st, Body body)
+{
+    if (!graphs_on(p)) {
+        body(st);
+        return SFD_OK;
+    }
+    if (!lg.exec || lg.key != key) {
+        drop_graph(lg);
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            body(st);
+            if (cudaStreamEndCapture(st, &graph) == cudaSuccess && graph) {
+                if (cudaGraphInstantiate(&lg.exec, graph, 0) != cudaSuccess) lg.exec = nullptr;
+                cudaGraphDestroy(graph);
+            }
+        }
+        cudaGetLastError();
+        if (!lg.exec) {   // capture not possible here: run the launches directly
+            body(st);
+            return SFD_OK;
+        }
+        lg.key = key;
+    }
+    CKC(cudaGraphLaunch(lg.exec, st));
+    return SFD_OK;
+}
+
 // ---------------------------------------------------------- DFT gradient
 constexpr double PI_D = 3.141592653589793238462643383279502884197169;
 
@@ -389,14 +447,21 @@ int adjoint_dft(sfd_plan *p, const PointSet &R, unsigned omask, cudaStream_t st)
     AdjFields a = p->a;
     for (int w = 0; w < NW; w++) { a.wr[w] = p->f.w[w]; a.bnd[w] = nullptr; }
     for (int r = 0; r < NR; r++) a.rr[r] = p->f.r[r];
+    LoopKey key;
+    key.add(2); key.add(ga); key.add(p->f); key.add(a); key.add_points(R); key.add(omask); key.add(p->d_res);
+    key.add(p->d_surf_q); key.add(p->cfg.tmax); key.add(tmin); key.add(p->nfreqs); key.add(p->dtnyq);
+    key.add(p->ntnyq); key.add(p->gradfreqsn); key.add(p->d_fw); key.add(p->d_fr);
     CKC(cudaEventRecord(p->ev0, st));
-    for (int t = p->cfg.tmax - 1; t > tmin; t--) {
-        if (g.freesurf) launch_surface_adj(ga, p->f, a, p->d_surf_q, st);
-        launch_residuals(ga, a, R, p->d_res, NT, t, omask, st);
-        launch_update_adj(ga, p->f, a, true, SFD_PREC_FP32, st);
-        launch_update_adj(ga, p->f, a, false, SFD_PREC_FP32, st);
-        if ((t - tmin) % p->dtnyq == 0) dft_sample(p, 1, (t - tmin) / p->dtnyq, st);
-    }
+    int rc2 = run_loop(p, p->gadj, key.s, st, [&](cudaStream_t s) {
+        for (int t = p->cfg.tmax - 1; t > tmin; t--) {
+            if (g.freesurf) launch_surface_adj(ga, p->f, a, p->d_surf_q, s);
+            launch_residuals(ga, a, R, p->d_res, NT, t, omask, s);
+            launch_update_adj(ga, p->f, a, true, SFD_PREC_FP32, s);
+            launch_update_adj(ga, p->f, a, false, SFD_PREC_FP32, s);
+            if ((t - tmin) % p->dtnyq == 0) dft_sample(p, 1, (t - tmin) / p->dtnyq, s);
+        }
+    });
+    if (rc2) return rc2;
     // calc_grad (src/calc_grad.c:376-420 for the constants)
     GradDft d;
     memset(&d, 0, sizeof d);
@@ -453,6 +518,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     if (c.field_precision < 0 || c.field_precision > 1) return SFD_ERR_ARG;
     if (c.field_precision == 1 && (c.nd != 3 || c.L > 3)) return SFD_ERR_UNSUPPORTED;
     if (c.back_prop_type < 0 || c.back_prop_type > 2) return SFD_ERR_ARG;
+    if (c.loop_graphs < 0 || c.loop_graphs > 2) return SFD_ERR_ARG;
 
     sfd_plan *p = new sfd_plan();
     p->cfg = c;
@@ -525,6 +591,8 @@ extern "C" void sfd_plan_destroy(sfd_plan *p)
     for (int w = 0; w < NW; w++)
         if (p->d_bnd[w]) cudaFree(p->d_bnd[w]);
     free_dft(p);
+    drop_graph(p->gfwd);
+    drop_graph(p->gadj);
     cudaEventDestroy(p->ev0);
     cudaEventDestroy(p->ev1);
     if (p->own_stream) cudaStreamDestroy(p->stream);
@@ -647,17 +715,28 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
     p->have_forward = false;
     p->have_dft = false;
     const int NT = p->cfg.nt, tmax = p->cfg.tmax, tmin = p->cfg.tmin;
-    CKC(cudaEventRecord(p->ev0, st));
-    for (int t = 0; t < tmax; t++) {
-        // the state after t steps, before the sources of step t (time_stepping.c:766-781)
-        if (dft && t >= tmin && (t - tmin) % p->dtnyq == 0) dft_sample(p, 0, (t - tmin) / p->dtnyq, st);
-        launch_sources(g, p->f, S, p->d_src, NT, t, 1, st);
-        launch_update_v(g, p->f, st);
-        launch_update_s(g, p->f, st);
-        if (save_boundaries && !dft) launch_savebnd(g, p->f, bs, p->cfg.precision, (int64_t)t * g.nbnd, st);
-        if (g.freesurf) launch_surface(g, p->f, 1, st);
-        launch_record(g, p->f, R, p->d_seis, NT, t, omask, st);
+    LoopKey key;
+    key.add(1); key.add(p->g); key.add(p->f); key.add_points(S); key.add_points(R); key.add(p->d_src);
+    key.add(p->d_seis); key.add(omask); key.add(dft); key.add(save_boundaries != 0); key.add(bs);
+    key.add(p->cfg.precision); key.add(tmax); key.add(tmin);
+    if (dft) {
+        key.add(p->nfreqs); key.add(p->dtnyq); key.add(p->ntnyq); key.add(p->gradfreqsn); key.add(p->d_fw);
+        key.add(p->d_fr);
     }
+    CKC(cudaEventRecord(p->ev0, st));
+    int rcl = run_loop(p, p->gfwd, key.s, st, [&](cudaStream_t s) {
+        for (int t = 0; t < tmax; t++) {
+            // the state after t steps, before the sources of step t (time_stepping.c:766-781)
+            if (dft && t >= tmin && (t - tmin) % p->dtnyq == 0) dft_sample(p, 0, (t - tmin) / p->dtnyq, s);
+            launch_sources(g, p->f, S, p->d_src, NT, t, 1, s);
+            launch_update_v(g, p->f, s);
+            launch_update_s(g, p->f, s);
+            if (save_boundaries && !dft) launch_savebnd(g, p->f, bs, p->cfg.precision, (int64_t)t * g.nbnd, s);
+            if (g.freesurf) launch_surface(g, p->f, 1, s);
+            launch_record(g, p->f, R, p->d_seis, NT, t, omask, s);
+        }
+    });
+    if (rcl) return rcl;
     CKC(cudaEventRecord(p->ev1, st));
     CKC(cudaGetLastError());
     int slot = 0;
@@ -721,16 +800,23 @@ extern "C" int sfd_adjoint(sfd_plan *p, const sfd_shot *shot, int mask, const in
         if (tot) CKC(cudaMemsetAsync(p->d_psi_all, 0, sizeof(float) * tot, st));
     }
     AdjFields a = p->a;
+    LoopKey key;
+    key.add(3); key.add(g); key.add(p->f); key.add(a); key.add_points(S); key.add_points(R); key.add(p->d_src);
+    key.add(p->d_res); key.add(p->d_surf_q); key.add(omask); key.add(p->d_bnd); key.add(p->bnd_elem);
+    key.add(p->cfg.precision); key.add(p->cfg.tmax); key.add(p->cfg.tmin);
     CKC(cudaEventRecord(p->ev0, st));
-    for (int t = p->cfg.tmax - 1; t > p->cfg.tmin; t--) {
-        for (int w = 0; w < NW; w++)
-            a.bnd[w] = p->d_bnd[w] ? (const char *)p->d_bnd[w] + p->bnd_elem * (size_t)(t - 1) * g.nbnd : nullptr;
-        if (g.freesurf) launch_surface_adj(g, p->f, a, p->d_surf_q, st);
-        launch_residuals(g, a, R, p->d_res, NT, t, omask, st);
-        launch_update_adj(g, p->f, a, true, p->cfg.precision, st);
-        launch_update_adj(g, p->f, a, false, p->cfg.precision, st);
-        launch_sources(g, p->f, S, p->d_src, NT, t, -1, st);
-    }
+    int rcl = run_loop(p, p->gadj, key.s, st, [&](cudaStream_t s) {
+        for (int t = p->cfg.tmax - 1; t > p->cfg.tmin; t--) {
+            for (int w = 0; w < NW; w++)
+                a.bnd[w] = p->d_bnd[w] ? (const char *)p->d_bnd[w] + p->bnd_elem * (size_t)(t - 1) * g.nbnd : nullptr;
+            if (g.freesurf) launch_surface_adj(g, p->f, a, p->d_surf_q, s);
+            launch_residuals(g, a, R, p->d_res, NT, t, omask, s);
+            launch_update_adj(g, p->f, a, true, p->cfg.precision, s);
+            launch_update_adj(g, p->f, a, false, p->cfg.precision, s);
+            launch_sources(g, p->f, S, p->d_src, NT, t, -1, s);
+        }
+    });
+    if (rcl) return rcl;
     CKC(cudaEventRecord(p->ev1, st));
     CKC(cudaGetLastError());
     CKC(cudaStreamSynchronize(st));

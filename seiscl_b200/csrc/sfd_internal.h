@@ -130,4 +130,10 @@ struct sfd_plan {
     float2 *d_fr[2][sfd::NR];   // memory variables [nfreqs][L][nvol]
     int dft_nf;                 // frequencies the transform buffers were allocated for
     bool have_dft;              // a forward run left its transforms on the device
+    // time loops captured as CUDA graphs (small grids, where launches dominate);
+    // each is reused while its key -- every value its launches bake in -- is unchanged
+    struct LoopGraph {
+        cudaGraphExec_t exec = nullptr;
+        std::string key;
+    } gfwd, gadj;
 };

@@ -36,7 +36,7 @@ class sfd_config(C.Structure):
                 ("k_max_cpml", C.c_float), ("abpc", C.c_float), ("tmin", C.c_int), ("tmax", C.c_int),
                 ("param_type", C.c_int), ("restype", C.c_int), ("precision", C.c_int),
                 ("kernels", C.c_int), ("adjoint_reset_psi", C.c_int), ("field_precision", C.c_int),
-                ("back_prop_type", C.c_int), ("reserved", C.c_int * 3)]
+                ("back_prop_type", C.c_int), ("loop_graphs", C.c_int), ("reserved", C.c_int * 2)]
 
 
 class sfd_shot(C.Structure):
@@ -141,6 +141,7 @@ class Config:
     field_precision: str = "fp32"  # "fp16": wave fields / memory variables stored in FP16 (3D forward)
     back_prop_type: int = 1  # 1: boundary-saving backpropagation, 2: DFT gradient at `gradfreqs`
     gradfreqs: Sequence[float] = ()  # DFT gradient frequencies (Hz), back_prop_type 2
+    loop_graphs: str = "auto"  # time loops as CUDA graphs: "auto" (2D), "always", "never"
 
     def to_c(self) -> sfd_config:
         c = sfd_config()
@@ -175,6 +176,7 @@ class Config:
         c.adjoint_reset_psi = 1 if self.adjoint_reset_psi else 0
         c.field_precision = {"fp32": 0, "fp16": 1}[self.field_precision]
         c.back_prop_type = int(self.back_prop_type)
+        c.loop_graphs = {"auto": 0, "always": 1, "never": 2}[self.loop_graphs]
         return c
 
     @property
