@@ -160,6 +160,17 @@ int sfd_zero_gradient(sfd_plan *plan);
  * `transform` is ignored. */
 int sfd_get_gradient(sfd_plan *plan, int transform, float *g0, float *g1, float *g2);
 
+/* Movie (MOVOUT, time_stepping.c:272-350): every `movout` steps, the
+ * physical cells of each wave field selected in a run's outsel (the
+ * acoustic model's pressure included) are copied to dst[k] (k an SFD_OUT_*
+ * index), a host array of [NT/movout][nx][ny][nz] floats: snapshot
+ * (t+1)/movout - 1 after forward step t when (t+1) % movout == 0.  A
+ * boundary-saving gradient run films its adjoint instead -- the
+ * reconstructed forward field after adjoint step t when t % movout == 0,
+ * into the same slot formula (:927-929).  movout <= 0 turns it off.  The
+ * destinations must stay valid until the run that fills them returns. */
+int sfd_set_movie(sfd_plan *plan, int movout, float *const *dst);
+
 /* ---- DFT gradient (BACK_PROP_TYPE=2) ----
  *
  * Frequencies (Hz, 1..16 values) of the DFT gradient of a plan created with

@@ -290,6 +290,67 @@ int alloc_adjoint(sfd_plan *p)
     return SFD_OK;
 }
 
+// ----------------------------------------------------------------- movie
+// The movie films the call's selected wave fields (the reference films its
+// output variables, time_stepping.c:284-292): output index -> wave field.
+struct Movie {
+    int n = 0;
+    int out[SFD_NOUT];     // SFD_OUT_* index of each filmed variable
+    int wave[SFD_NOUT];    // its wave field
+    int nslot = 0;
+    int64_t ncell = 0;
+};
+
+int movie_setup(sfd_plan *p, unsigned omask, Movie &mv)
+{
+    const Grid &g = p->g;
+    mv.n = 0;
+    if (p->movout <= 0) return SFD_OK;
+    for (int o = 0; o < SFD_NOUT; o++) {
+        if (!(omask & (1u << o)) || !p->mov_dst[o]) continue;
+        int w = o;
+        if (o == SFD_OUT_P) {
+            if (g.nd != 22) continue;   // pressure is a wave field only in the acoustic model
+            w = SXX;
+        }
+        if (!p->f.w[w]) continue;
+        mv.out[mv.n] = o;
+        mv.wave[mv.n] = w;
+        mv.n++;
+    }
+    mv.nslot = p->cfg.nt / p->movout;
+    mv.ncell = (int64_t)g.nz * g.ny * g.nx;
+    if (!mv.n || !mv.nslot) { mv.n = 0; return SFD_OK; }
+    size_t need = (size_t)mv.n * mv.nslot * mv.ncell;
+    if (need > p->mov_cap) {
+        if (p->d_mov) cudaFree(p->d_mov);
+        p->d_mov = nullptr;
+        p->mov_cap = 0;
+        if (cudaMalloc(&p->d_mov, sizeof(float) * need) != cudaSuccess) {
+            p->d_mov = nullptr;
+            return fail(p, SFD_ERR_MEMORY, "movie buffer does not fit in device memory");
+        }
+        p->mov_cap = need;
+    }
+    CKC(cudaMemset(p->d_mov, 0, sizeof(float) * need));
+    return SFD_OK;
+}
+
+void movie_snap(const sfd_plan *p, const Movie &mv, int slot, cudaStream_t st)
+{
+    for (int q = 0; q < mv.n; q++)
+        launch_movie(p->g, p->f.w[mv.wave[q]], 1.0f / p->g.ws.w[mv.wave[q]],
+                     p->d_mov + ((size_t)q * mv.nslot + slot) * mv.ncell, st);
+}
+
+int movie_out(sfd_plan *p, const Movie &mv, cudaStream_t st)
+{
+    for (int q = 0; q < mv.n; q++)
+        CKC(cudaMemcpyAsync(p->mov_dst[mv.out[q]], p->d_mov + (size_t)q * mv.nslot * mv.ncell,
+                            sizeof(float) * (size_t)mv.nslot * mv.ncell, cudaMemcpyDeviceToHost, st));
+    return SFD_OK;
+}
+
 // ----------------------------------------------------------- loop graphs
 // The bytes a time loop's launches bake in: kernel arguments by value and
 // the buffers they point to.  Equal keys => the captured graph is valid.
@@ -572,6 +633,10 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     p->nfreqs = p->dtnyq = p->ntnyq = p->dft_nf = 0;
     p->df = 0.0f;
     memset(p->d_fw, 0, sizeof p->d_fw);
+    p->movout = 0;
+    memset(p->mov_dst, 0, sizeof p->mov_dst);
+    p->d_mov = nullptr;
+    p->mov_cap = 0;
     memset(p->d_fr, 0, sizeof p->d_fr);
     p->have_dft = false;
     if (cudaGetDevice(&p->device) != cudaSuccess) { delete p; return SFD_ERR_CUDA; }
@@ -591,6 +656,7 @@ extern "C" void sfd_plan_destroy(sfd_plan *p)
     for (int w = 0; w < NW; w++)
         if (p->d_bnd[w]) cudaFree(p->d_bnd[w]);
     free_dft(p);
+    if (p->d_mov) cudaFree(p->d_mov);
     drop_graph(p->gfwd);
     drop_graph(p->gadj);
     cudaEventDestroy(p->ev0);
@@ -715,7 +781,12 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
     p->have_forward = false;
     p->have_dft = false;
     const int NT = p->cfg.nt, tmax = p->cfg.tmax, tmin = p->cfg.tmin;
+    // the movie of a boundary-saving gradient run is filmed by its adjoint
+    // (time_stepping.c:819-822)
+    Movie mv;
+    if (!(save_boundaries && !dft) && (rc = movie_setup(p, omask, mv))) return rc;
     LoopKey key;
+    key.add(mv.n); key.add(p->movout); key.add(p->d_mov);
     key.add(1); key.add(p->g); key.add(p->f); key.add_points(S); key.add_points(R); key.add(p->d_src);
     key.add(p->d_seis); key.add(omask); key.add(dft); key.add(save_boundaries != 0); key.add(bs);
     key.add(p->cfg.precision); key.add(tmax); key.add(tmin);
@@ -734,9 +805,11 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
             if (save_boundaries && !dft) launch_savebnd(g, p->f, bs, p->cfg.precision, (int64_t)t * g.nbnd, s);
             if (g.freesurf) launch_surface(g, p->f, 1, s);
             launch_record(g, p->f, R, p->d_seis, NT, t, omask, s);
+            if (mv.n && (t + 1) % p->movout == 0) movie_snap(p, mv, (t + 1) / p->movout - 1, s);
         }
     });
     if (rcl) return rcl;
+    if (mv.n && (rc = movie_out(p, mv, st))) return rc;
     CKC(cudaEventRecord(p->ev1, st));
     CKC(cudaGetLastError());
     int slot = 0;
@@ -800,7 +873,12 @@ extern "C" int sfd_adjoint(sfd_plan *p, const sfd_shot *shot, int mask, const in
         if (tot) CKC(cudaMemsetAsync(p->d_psi_all, 0, sizeof(float) * tot, st));
     }
     AdjFields a = p->a;
+    // the movie of a boundary-saving gradient: the reconstructed forward
+    // field after each adjoint step with t % movout == 0 (time_stepping.c:927-929)
+    Movie mv;
+    if ((rc = movie_setup(p, omask, mv))) return rc;
     LoopKey key;
+    key.add(mv.n); key.add(p->movout); key.add(p->d_mov);
     key.add(3); key.add(g); key.add(p->f); key.add(a); key.add_points(S); key.add_points(R); key.add(p->d_src);
     key.add(p->d_res); key.add(p->d_surf_q); key.add(omask); key.add(p->d_bnd); key.add(p->bnd_elem);
     key.add(p->cfg.precision); key.add(p->cfg.tmax); key.add(p->cfg.tmin);
@@ -814,9 +892,11 @@ extern "C" int sfd_adjoint(sfd_plan *p, const sfd_shot *shot, int mask, const in
             launch_update_adj(g, p->f, a, true, p->cfg.precision, s);
             launch_update_adj(g, p->f, a, false, p->cfg.precision, s);
             launch_sources(g, p->f, S, p->d_src, NT, t, -1, s);
+            if (mv.n && t % p->movout == 0) movie_snap(p, mv, (t + 1) / p->movout - 1, s);
         }
     });
     if (rcl) return rcl;
+    if (mv.n && (rc = movie_out(p, mv, st))) return rc;
     CKC(cudaEventRecord(p->ev1, st));
     CKC(cudaGetLastError());
     CKC(cudaStreamSynchronize(st));
@@ -833,6 +913,15 @@ extern "C" int sfd_zero_gradient(sfd_plan *p)
     int64_t npar = (int64_t)p->g.nz * p->g.ny * p->g.nx;
     for (int k = 0; k < NG; k++)
         if (p->a.grad[k]) CKC(cudaMemset(p->a.grad[k], 0, sizeof(double) * npar));
+    return SFD_OK;
+}
+
+extern "C" int sfd_set_movie(sfd_plan *p, int movout, float *const *dst)
+{
+    if (!p) return SFD_ERR_ARG;
+    if (movout > 0 && !dst) return fail(p, SFD_ERR_ARG, "movie destinations missing");
+    p->movout = movout > 0 ? movout : 0;
+    for (int o = 0; o < SFD_NOUT; o++) p->mov_dst[o] = p->movout ? dst[o] : nullptr;
     return SFD_OK;
 }
 

@@ -130,6 +130,11 @@ struct sfd_plan {
     float2 *d_fr[2][sfd::NR];   // memory variables [nfreqs][L][nvol]
     int dft_nf;                 // frequencies the transform buffers were allocated for
     bool have_dft;              // a forward run left its transforms on the device
+    // movie (MOVOUT): snapshots of the selected wave fields every movout steps
+    int movout;
+    float *mov_dst[SFD_NOUT];   // host destinations, [NT/movout][nx][ny][nz] each
+    float *d_mov;               // device staging, [nsel][NT/movout][nx][ny][nz]
+    size_t mov_cap;             // floats allocated at d_mov
     // time loops captured as CUDA graphs (small grids, where launches dominate);
     // each is reused while its key -- every value its launches bake in -- is unchanged
     struct LoopGraph {

@@ -14,6 +14,8 @@
 //   adjoint   src/update_adj{v,s}{2D,3D}.cl, src/surface{2D,3D}_adj.cl
 //   boundary  src/savebnd{2D,3D}.cl, src/header_injectbnd.cl
 // Arithmetic is FP32 with FMA; gradients accumulate in FP64.
+#include <algorithm>
+
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -2595,6 +2597,28 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
         DISPATCH_F(g.F, k_s2d<FF><<<gr, b, 0, st>>>(g, f));
     }
+}
+
+// movie snapshot (time_stepping.c:272-350): padded field -> [nx][ny][nz]
+template <class T>
+__global__ void k_movie(Grid g, const T *fld, float inv_scale, float *dst)
+{
+    const i64 n = (i64)g.nz * g.ny * g.nx;
+    for (i64 idx = (i64)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (i64)gridDim.x * blockDim.x) {
+        const int k = (int)(idx % g.nz);
+        const i64 r = idx / g.nz;
+        const int j = (int)(r % g.ny), i = (int)(r / g.ny);
+        const i64 iv = ((i64)(i + g.F) * g.NY + (g.nd == 3 ? j + g.F : 0)) * g.NZ + (k + g.F);
+        dst[idx] = to_f<T>(fld[iv]) * inv_scale;
+    }
+}
+
+void launch_movie(const Grid &g, const float *fld, float inv_scale, float *dst, cudaStream_t st)
+{
+    const i64 n = (i64)g.nz * g.ny * g.nx;
+    unsigned blocks = (unsigned)std::min<i64>((n + 255) / 256, 148 * 16);
+    if (g.fhalf) k_movie<__half><<<blocks, 256, 0, st>>>(g, reinterpret_cast<const __half *>(fld), inv_scale, dst);
+    else k_movie<float><<<blocks, 256, 0, st>>>(g, fld, inv_scale, dst);
 }
 
 int stress_family(const Grid &g, const Fields &f)

@@ -36,6 +36,10 @@ void launch_record(const Grid &g, const Fields &f, const PointSet &r, float *out
 void launch_residuals(const Grid &g, const AdjFields &a, const PointSet &r, const float *res, int nt_total, int t,
                       unsigned outmask, cudaStream_t st);
 
+// movie snapshot: the physical cells of one wave field, divided by its
+// storage scale, into dst [nx][ny][nz]
+void launch_movie(const Grid &g, const float *fld, float inv_scale, float *dst, cudaStream_t st);
+
 // DFT gradient (sfd_dft.cu)
 struct DftSet {             // variables transformed by one accumulation launch
     const float *v[NW + NR];

@@ -59,6 +59,7 @@ EXPORTS = {
     "sfd_get_gradient": (C.c_int, [C.c_void_p, C.c_int, FP, FP, FP]),
     "sfd_get_gradient_q": (C.c_int, [C.c_void_p, FP, FP]),
     "sfd_set_gradfreqs": (C.c_int, [C.c_void_p, FP, C.c_int, C.POINTER(C.c_int)]),
+    "sfd_set_movie": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FP)]),
     "sfd_residual_scale": (C.c_int, [C.c_void_p, C.POINTER(sfd_shot), C.POINTER(C.c_int), C.POINTER(FP)]),
     "sfd_plan_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "sfd_plan_uses_tma": (C.c_int, [C.c_void_p]),
@@ -204,6 +205,20 @@ class Plan:
         self.dtnyq = self.ntnyq = None
         if int(cfg.back_prop_type) == 2 and len(np.atleast_1d(cfg.gradfreqs)):
             self.set_gradfreqs(cfg.gradfreqs)
+
+    def set_movie(self, movout: int, outputs=()):
+        """Film `outputs` (wave-field names) every `movout` steps in the next
+        runs (MOVOUT); returns {name: array [NT//movout][nx][(ny)][nz]} that
+        those runs fill.  movout <= 0 turns it off."""
+        self._movie = {}
+        ptrs = (FP * 10)()
+        if movout > 0:
+            nslot = int(self.cfg.NT) // int(movout)
+            for n in outputs:
+                self._movie[n] = np.zeros((nslot,) + tuple(self.cfg.model_shape), np.float32)
+                ptrs[OUT_NAMES.index(n)] = _ptr(self._movie[n])
+        self._check(self.lib.sfd_set_movie(self.h, int(movout), ptrs))
+        return self._movie
 
     def set_gradfreqs(self, freqs):
         """DFT-gradient frequencies (Hz); returns (DTNYQ, NTNYQ)."""

@@ -462,7 +462,19 @@ class SeisCL:
         return output
 
     def read_movie(self, workdir=None, filename=None):
-        raise SeisCLError('Could not read movie: snapshots are not produced by this engine')
+        """Movie of the last run (SeisCL.py:543-571): for each recorded
+        variable that is a wave field, the snapshots taken every ``movout``
+        steps, shaped as the reference returns them (N reversed, then
+        snapshot, then shot)."""
+        if filename is None:
+            filename = self.file_movout
+        mat = self._files.get(os.path.basename(filename))
+        if mat is None:
+            raise SeisCLError('Could not read data')
+        output = [np.transpose(mat["mov" + w]) for w in self.to_load_names if "mov" + w in mat]
+        if not output:
+            raise SeisCLError('Could not read data: variables not found')
+        return output
 
     def read_grad(self, workdir=None, param_names=None, filename=None):
         """Gradients of the last run, N-shaped, zeroed in the absorbing
@@ -509,7 +521,7 @@ class SeisCL:
         if bpt == 2 and self.gradout and not freqs:
             # read_hdf5.c:546-549 requires /gradfreqs for the DFT gradient
             raise SeisCLError("Error: back_prop_type=2 needs gradfreqs")
-        for flag in ("Hout", "gradsrcout", "movout"):
+        for flag in ("Hout", "gradsrcout"):
             if getattr(self, flag):
                 raise SeisCLError("Error: %s is not provided by this engine" % flag)
         return engine.Config(
@@ -705,9 +717,27 @@ class SeisCL:
         rms = rmsnorm = 0.0
         if self.gradout:
             plan.zero_gradient()
+        movout = int(self.movout)
+        movies = None
+        if movout > 0:
+            # [shot][snapshot][nx][(ny)][nz] per filmed variable (writehdf5.c:295-310)
+            films = [k for k in outs if k != "p" or nd == 22]
+            shape = (len(shots), NT // movout) + tuple(int(v) for v in np.atleast_1d(self.N)[::-1])
+            movies = {k: np.zeros(shape, np.float32) for k in films}
+        pending = None   # (shot index, arrays the last shot's runs filled)
+
+        def keep_movie():
+            if pending is not None:
+                for k, v in pending[1].items():
+                    movies[k][pending[0]] = v
         try:
-            for sid, si, gi in shots[smin:smax]:
+            for ishot, (sid, si, gi) in enumerate(shots):
+                if not smin <= ishot < smax:
+                    continue
+                keep_movie()
                 sp, src, rp = sp_all[si], src_all[si], rp_all[gi]
+                if movies is not None:
+                    pending = (ishot, plan.set_movie(movout, list(movies)))
                 if self.inputres and self.gradout:
                     res = {k: np.ascontiguousarray(np.transpose(resin[k + "res"]), dtype=np.float32)[
                         rp[:, 4].astype(int) - 1] for k in outs}
@@ -729,8 +759,12 @@ class SeisCL:
                         continue
                 res = plan.residual_scale(rp, res)
                 plan.adjoint(sp, src, rp, res)
+            keep_movie()
         except engine.SeisCLEngineError as exc:
             raise SeisCLError(str(exc)) from exc
+        finally:
+            if movies is not None:
+                plan.set_movie(0)
         if world > 1:
             # every rank filled only its own traces: one sum gives all of them
             # (Out_MPI.c:70-160); the gradient is summed after the chain rule,
@@ -738,7 +772,11 @@ class SeisCL:
             red = {"seis_" + k: v for k, v in seis.items()}
             red.update({"res_" + k: v for k, v in resid.items()})
             red["rms"] = np.array([rms, rmsnorm])
+            if movies is not None:
+                red.update({"mov_" + k: v for k, v in movies.items()})
             red = shots_mod.allreduce_sum(red)
+            if movies is not None:
+                movies = {k: red["mov_" + k] for k in movies}
             seis = {k: red["seis_" + k] for k in seis}
             resid = {k: red["res_" + k] for k in resid}
             rms, rmsnorm = (float(v) for v in red["rms"])
@@ -750,6 +788,8 @@ class SeisCL:
             dout["rec_pos"] = np.asarray(self.rec_pos).copy()
             if self.seisout or self.resout:
                 self._files[self.file_dout] = dout
+        if movies is not None:
+            self._files[self.file_movout] = {"mov" + k: v for k, v in movies.items()}
         if self.rmsout:
             self._files[self.file_rms] = {"rms": np.array([np.sqrt(rms)], np.float32),
                                           "rms_norm": np.array([np.sqrt(rmsnorm)], np.float32)}
