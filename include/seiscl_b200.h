@@ -102,7 +102,10 @@ typedef struct sfd_config {
                               2 never.  A graph is captured on the first shot of a shape
                               and replayed while nothing its launches depend on changes.
                               No reference counterpart (launch mechanics). */
-    int reserved[2];
+    int hout;              /* HOUT: also accumulate the approximate Hessian (2D; the
+                              reference's 3D Hessian kernel does not compile,
+                              update_adjv3D.cl:486, so 3D boundary-saving plans reject it) */
+    int reserved[1];
 } sfd_config;
 
 typedef struct sfd_shot {
@@ -182,6 +185,16 @@ int sfd_set_movie(sfd_plan *plan, int movout, float *const *dst);
  * per memory-variable cell) is allocated by the next gradient forward run.
  * info (may be NULL) receives DTNYQ, NTNYQ. */
 int sfd_set_gradfreqs(sfd_plan *plan, const float *freqs, int nfreqs, int *info);
+
+/* Approximate Hessian (HOUT) accumulated with the gradient: out[0..4] =
+ * H of the param_type's first and second parameters, rho, taup, taus
+ * (entries may be NULL).  Boundary-saving plans: transform=1 applies
+ * transf_grad's chain rule without the division by dt
+ * (src/calc_grad.c:1004-1090), transform=0 gives the raw HM, Hmu, Hrho
+ * (update_adjs2D.cl:453-470; Hrho stays 0 there as in the reference, whose
+ * line is commented out).  DFT plans: calc_grad's 2D Hessian
+ * (src/calc_grad.c:838-905), zero in 3D as in the reference. */
+int sfd_get_hessian(sfd_plan *plan, int transform, float *const *out);
 
 /* Gradients of the relaxation parameters taup and taus [nx][ny][nz], filled
  * by the DFT gradient of viscoelastic plans (src/calc_grad.c:729-739); zero

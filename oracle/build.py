@@ -94,7 +94,7 @@ def ref_defines(cfg: dict, nbnd: int, hc: list) -> list:
         "COMM12": 0,
         "BACK_PROP_TYPE": cfg.get("back_prop_type", 1),
         "RESTYPE": cfg.get("restype", 0),
-        "HOUT": 0,
+        "HOUT": cfg.get("hout", 0),
         "GRADSRCOUT": 0,
         "GRADOUT": 1,
         "FP16": 0,
@@ -129,7 +129,7 @@ KERNELS = {
 
 def ref_key(cfg: dict) -> str:
     keys = ["nd", "nz", "ny", "nx", "fdorder", "maxrelerror", "nab", "freesurf", "abs_type", "L", "nt",
-            "dt", "dh", "restype", "back_prop_type"]
+            "dt", "dh", "restype", "back_prop_type", "hout"]
     blob = json.dumps({k: cfg.get(k) for k in keys}, sort_keys=True)
     return hashlib.sha1(blob.encode()).hexdigest()[:16]
 

@@ -81,6 +81,7 @@ typedef struct fdo_cfg {
     int back_prop_type;/* 1: boundary-saving backpropagation, 2: DFT gradient */
     int nfreqs;        /* DFT gradient: number of frequencies (<= FDO_MAXFREQ) */
     float gradfreqs[FDO_MAXFREQ];  /* DFT gradient frequencies (Hz) */
+    int hout;          /* HOUT: accumulate the approximate Hessian (2D) */
 } fdo_cfg;
 
 /* One shot: sources and receivers, the reference's src_pos [nsrc][5] and
@@ -127,6 +128,7 @@ typedef struct fdo_state {
     float *taper;
     float *eta;
     float *grad[G_N];      /* float accumulators as in the reference */
+    float *hess[G_N];      /* approximate Hessian (HOUT), same layout */
     float *bnd[W_N];       /* [nt][nbnd] per wave field */
     float *bnd_cur[W_N];   /* slice injected during the current adjoint step */
     int nwave;             /* number of wave fields used */

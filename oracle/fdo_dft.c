@@ -191,6 +191,10 @@ static inline cpx integ(cpx a, float w) { cpx r = {a.y / w, -a.x / w}; return r;
 static inline float itreal(cpx a, cpx b) { return a.y * b.x - a.x * b.y; }
 /* memory-variable product with relaxation time ts */
 static inline float rmprod(cpx a, cpx b, float ts, float w) { return ts * (a.x * b.x + a.y * b.y) + (a.x * b.y - a.y * b.x) / w; }
+/* time derivative at angular frequency w: i w X */
+static inline cpx deriv(cpx a, float w) { cpx r = {-a.y * w, a.x * w}; return r; }
+/* squared modulus, formed in double and rounded once */
+static inline float norm2(cpx a) { return (float)(pow(a.x, 2) + pow(a.y, 2)); }
 
 /* Add this shot's DFT gradient to s->grad (float accumulators, as the
  * reference's host arrays).  The forward transforms are slot 0, the adjoint
@@ -237,7 +241,7 @@ void fdo_calc_grad(fdo_state *s)
                 for (int f = 0; f < nf; f++) {
                     float w = 2.0 * FDO_PI * df * s->gradfreqsn[f];
                     i64 ic = (i64)f * nvol + iv;
-                    double d[9] = {0};
+                    double d[9] = {0}, hd[9] = {0};
                     if (nd == 3) {
                         cpx sf[6], sa[6];  /* xx yy zz xy yz xz */
                         static const int sid[6] = {W_SXX, W_SYY, W_SZZ, W_SXY, W_SYZ, W_SXZ};
@@ -292,6 +296,26 @@ void fdo_calc_grad(fdo_state *s)
                         d[3] = d[0];
                         d[4] = w * (itreal(axx, sub(fxx, fzz)) + itreal(azz, sub(fzz, fxx))) / NTN;
                         d[8] = w * (itreal(ld(W1[W_VX], ic), ld(W0[W_VX], ic)) + itreal(ld(W1[W_VZ], ic), ld(W0[W_VZ], ic))) / NTN;
+                        if (c->hout) {
+                            /* approximate Hessian (calc_grad.c:838-905, ND = 2 only): squared
+                             * moduli of the forward transforms, with the stresses as
+                             * corrected above */
+                            for (int l = 0; l < L; l++) {
+                                i64 il = ((i64)f * L + l) * nvol + iv;
+                                cpx rxx = ld(R0[R_XX], il), rzz = ld(R0[R_ZZ], il), rxz = ld(R0[R_XZ], il);
+                                cpx sum = add(rxx, rzz), dxx = sub(rxx, rzz), dzz = sub(rzz, rxx);
+                                float wt = w * tausig[l];
+                                hd[1] += norm2(add(sum, deriv(sum, wt))) / NTN;
+                                hd[5] += norm2(add(rxz, deriv(rxz, wt))) / NTN;
+                                hd[6] = hd[1];
+                                hd[7] += (norm2(add(dxx, deriv(dxx, wt))) + norm2(add(dzz, deriv(dzz, wt)))) / NTN;
+                            }
+                            hd[0] = norm2(deriv(add(fxx, fzz), w)) / NTN;
+                            hd[2] = norm2(deriv(fxz, w)) / NTN;
+                            hd[3] = hd[0];
+                            hd[4] = (norm2(deriv(sub(fxx, fzz), w)) + norm2(deriv(sub(fzz, fxx), w))) / NTN;
+                            hd[8] = (norm2(deriv(ld(W0[W_VX], ic), w)) + norm2(deriv(ld(W0[W_VZ], ic), w))) / NTN;
+                        }
                     }
                     /* signs: products of the moduli enter with -, +, -, +, -, + */
                     double sM = -cc[0] * d[0] + cc[1] * d[1];
@@ -309,6 +333,20 @@ void fdo_calc_grad(fdo_state *s)
                         s->grad[G_TAUS][im] += sts;
                     }
                     s->grad[G_RHO][im] += srho;
+                    if (c->hout && nd != 3) {
+                        /* the Hessian enters with the gradient's signs reversed */
+                        s->hess[G_M][im] += cc[0] * hd[0] - cc[1] * hd[1];
+                        s->hess[G_MU][im] += cc[2] * hd[2] - cc[3] * hd[3] + cc[4] * hd[4] - cc[5] * hd[5] +
+                                             cc[6] * hd[6] - cc[7] * hd[7];
+                        if (L > 0) {
+                            s->hess[G_TAUP][im] += cc[8] * hd[0] - cc[9] * hd[1];
+                            s->hess[G_TAUS][im] += cc[10] * hd[2] - cc[11] * hd[3] + cc[12] * hd[4] -
+                                                   cc[13] * hd[5] + cc[14] * hd[6] - cc[15] * hd[7];
+                        }
+                        s->hess[G_RHO][im] += hd[8] - cc[16] * hd[0] + cc[17] * hd[1] - cc[18] * hd[2] +
+                                              cc[19] * hd[3] - cc[20] * hd[4] + cc[21] * hd[5] - cc[22] * hd[6] +
+                                              cc[23] * hd[7];
+                    }
                 }
             }
 }

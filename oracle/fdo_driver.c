@@ -153,7 +153,10 @@ static void zero_fields(fdo_state *s, float **w, float **r)
 
 void fdo_zero_gradients(fdo_state *s)
 {
-    for (int i = 0; i < G_N; i++) memset(s->grad[i], 0, sizeof(float) * s->npar);
+    for (int i = 0; i < G_N; i++) {
+        memset(s->grad[i], 0, sizeof(float) * s->npar);
+        if (s->hess[i]) memset(s->hess[i], 0, sizeof(float) * s->npar);
+    }
 }
 
 static void zero_psi(fdo_state *s)
@@ -279,6 +282,39 @@ void fdo_transf_grad(const fdo_state *s, float *gvp, float *gvs, float *grho)
     }
 }
 
+/* The approximate Hessian through transf_grad's chain rule
+ * (src/calc_grad.c:1004-1090): the parameters are rescaled as for the
+ * gradient, the Hessian is not divided by dt.  out (rho, M, mu, taup, taus
+ * order) receives Hrho, HM, Hmu and the raw taup/taus Hessians. */
+static void transf_hess(const fdo_state *s, float **out)
+{
+    i64 n = s->npar;
+    float dt = s->c.dt, dh = s->c.dh;
+    int pt = s->c.param_type;
+    for (i64 i = 0; i < n; i++) {
+        float rho = 1.0 / s->p[P_RHO][i] * dt / dh * powf(2, -0);
+        float M = s->p[P_M][i] * (dh / dt * powf(2, -0));
+        float mu = s->p[P_MU][i] * (dh / dt * powf(2, -0));
+        float hr = s->hess[G_RHO][i], hM = s->hess[G_M][i], hmu = s->hess[G_MU][i];
+        if (pt == 0 || pt == 2) {
+            hr = hr + M / rho * hM;
+            if (mu > 0) hr = hr + mu / rho * hmu;
+        }
+        if (pt == 0) {
+            hM = 2.0 * sqrt((double)rho * (double)M) * hM;
+            hmu = 2.0 * sqrt((double)rho * (double)mu) * hmu;
+        } else if (pt == 2) {
+            hM = 2.0 * sqrt((double)M / (double)rho) * hM;
+            hmu = 2.0 * sqrt((double)mu / (double)rho) * hmu;
+        }
+        if (out[G_RHO]) out[G_RHO][i] = hr;
+        if (out[G_M]) out[G_M][i] = hM;
+        if (out[G_MU]) out[G_MU][i] = hmu;
+        if (out[G_TAUP]) out[G_TAUP][i] = s->hess[G_TAUP][i];
+        if (out[G_TAUS]) out[G_TAUS][i] = s->hess[G_TAUS][i];
+    }
+}
+
 /* ---- flat entry points for ctypes ---- */
 typedef struct fdo_handle {
     fdo_state s;
@@ -339,6 +375,16 @@ void fdo_get_grad_raw(void *hp, float **out)
     fdo_handle *h = hp;
     for (int i = 0; i < G_N; i++)
         if (out[i]) memcpy(out[i], h->s.grad[i], h->s.npar * sizeof(float));
+}
+/* the Hessian accumulators (transform 0) or their transf_grad form
+ * (transform 1; not for the DFT gradient, which the reference leaves as is) */
+void fdo_get_hess(void *hp, int transform, float **out)
+{
+    fdo_handle *h = hp;
+    if (!h->s.hess[0]) return;
+    if (transform) { transf_hess(&h->s, out); return; }
+    for (int i = 0; i < G_N; i++)
+        if (out[i]) memcpy(out[i], h->s.hess[i], h->s.npar * sizeof(float));
 }
 /* DFT of slot (0 forward, 1 adjoint): kind 0 wave field, 1 memory variable */
 float *fdo_dft_array(void *hp, int slot, int kind, int id)

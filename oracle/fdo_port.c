@@ -942,9 +942,20 @@ static void port_update_adjs2d(fdo_state *s)
                 float dM = c1 * (sxx[iv] + szz[iv]) * (lsxx + lszz);
                 gradM[ip] += -dM;
                 gradmu[ip] += -c3 * (sxz[iv] * lsxz) + dM - c5 * ((sxx[iv] - szz[iv]) * (lsxx - lszz));
+                if (c->hout) {
+                    /* update_adjs2D.cl:453-457: the mu term subtracts the
+                     * gradient's dM, not dMH */
+                    float dMH = c1 * (sxx[iv] + szz[iv]) * (sxx[iv] + szz[iv]);
+                    s->hess[G_M][ip] += dMH;
+                    s->hess[G_MU][ip] += c3 * sxz[iv] * sxz[iv] - dM + c5 * (sxx[iv] - szz[iv]) * (sxx[iv] - szz[iv]);
+                }
             } else {
                 float dM = (sxx[iv] + szz[iv]) * (lsxx + lszz);
                 gradM[ip] += -dM;
+                if (c->hout) {
+                    float dMH = (sxx[iv] + szz[iv]) * (sxx[iv] + szz[iv]);
+                    s->hess[G_M][ip] += dMH;
+                }
             }
         }
 }

@@ -216,6 +216,10 @@ int fdo_state_init(fdo_state *s, const fdo_cfg *c)
     s->taper = zalloc(nab + 1);
     s->eta = zalloc(c->L + 1);
     for (int i = 0; i < G_N; i++) s->grad[i] = zalloc(s->npar);
+    /* the reference's 3D Hessian kernel does not compile (update_adjv3D.cl:486) */
+    if (c->hout && c->nd == 3 && c->back_prop_type != 2) return 5;
+    if (c->hout)
+        for (int i = 0; i < G_N; i++) s->hess[i] = zalloc(s->npar);
 
     if (c->abs_type == 1 && nab > 0) {
         if (fdo_cpml_coeff(c->npower, c->k_max_cpml, c->fpml, c->vppml, c->dh, c->dt, nab,
@@ -264,7 +268,7 @@ void fdo_state_free(fdo_state *s)
     for (int i = 0; i < PS_N; i++) free(s->psi[i]);
     for (int i = 0; i < P_N; i++) free(s->p[i]);
     for (int i = 0; i < C_N; i++) { free(s->cx[i]); free(s->cy[i]); free(s->cz[i]); }
-    for (int i = 0; i < G_N; i++) free(s->grad[i]);
+    for (int i = 0; i < G_N; i++) { free(s->grad[i]); free(s->hess[i]); }
     for (int slot = 0; slot < 2; slot++) {
         for (int i = 0; i < W_N; i++) free(s->fw[slot][i]);
         for (int i = 0; i < R_N; i++) free(s->fr[slot][i]);

@@ -39,7 +39,7 @@ class fdo_cfg(C.Structure):
                 ("vppml", C.c_float), ("fpml", C.c_float), ("npower", C.c_float),
                 ("k_max_cpml", C.c_float), ("abpc", C.c_float),
                 ("param_type", C.c_int), ("restype", C.c_int), ("back_prop_type", C.c_int),
-                ("nfreqs", C.c_int), ("gradfreqs", C.c_float * 16)]
+                ("nfreqs", C.c_int), ("gradfreqs", C.c_float * 16), ("hout", C.c_int)]
 
 
 DEFAULTS = dict(nd=2, ny=1, fdorder=8, maxrelerror=1, nab=16, freesurf=0, abs_type=1, L=0, tmin=0,
@@ -69,6 +69,7 @@ def make_cfg(cfg: dict) -> fdo_cfg:
     c.nfreqs = len(gf)
     for i, v in enumerate(gf):
         c.gradfreqs[i] = v
+    c.hout = int(d.get("hout", 0))
     return c
 
 
@@ -86,6 +87,7 @@ def _lib(path):
                                     C.POINTER(FP)]
     lib.fdo_get_grad.argtypes = [P, FP, FP, FP, FP, FP, FP]
     lib.fdo_get_grad_raw.argtypes = [P, C.POINTER(FP)]
+    lib.fdo_get_hess.argtypes = [P, C.c_int, C.POINTER(FP)]
     lib.fdo_dft_array.restype = FP
     lib.fdo_dft_array.argtypes = [P, C.c_int, C.c_int, C.c_int]
     lib.fdo_dft_info.argtypes = [P, C.POINTER(C.c_int), FP, FP]
@@ -250,6 +252,22 @@ class Oracle:
         return {"rho": g[0].reshape(sh), "M": g[1].reshape(sh), "mu": g[2].reshape(sh),
                 "taup": g[3].reshape(sh), "taus": g[4].reshape(sh)}
 
+    def hessians(self, transform=True) -> dict:
+        """Approximate Hessian (HOUT).  transform: the chain rule of
+        transf_grad applied to the Hessian (src/calc_grad.c:1023-1060, no
+        division by dt), keyed by the param_type's names; else the raw
+        accumulators M, mu, rho, taup, taus."""
+        g = [np.zeros(self.npar, np.float32) for _ in range(5)]
+        ptrs = (C.POINTER(C.c_float) * 5)(*[_fptr(a) for a in g])
+        self.lib.fdo_get_hess(self.h, 1 if transform else 0, ptrs)
+        sh = self.shape
+        if transform:
+            names = {0: ("vp", "vs"), 1: ("M", "mu"), 2: ("Ip", "Is")}[int(self.cfg.get("param_type", 0))]
+            return {names[0]: g[1].reshape(sh), names[1]: g[2].reshape(sh), "rho": g[0].reshape(sh),
+                    "taup": g[3].reshape(sh), "taus": g[4].reshape(sh)}
+        return {"rho": g[0].reshape(sh), "M": g[1].reshape(sh), "mu": g[2].reshape(sh),
+                "taup": g[3].reshape(sh), "taus": g[4].reshape(sh)}
+
     def dft_info(self) -> dict:
         """DTNYQ, NTNYQ, df and gradfreqsn of a DFT-gradient state
         (src/assign_modeling_case.c:549-570)."""
@@ -371,7 +389,7 @@ def ref_calc_grad(o: Oracle, fwd=None, adj=None) -> dict:
     Returns M, mu, rho, taup, taus as the reference's float host arrays."""
     lib = C.CDLL(_build.build_refcg())
     FP = C.POINTER(C.c_float)
-    lib.refcg_run.argtypes = [C.c_int] * 10 + [C.c_float, C.c_float, FP, FP] + [C.POINTER(FP)] * 4
+    lib.refcg_run.argtypes = [C.c_int] * 10 + [C.c_float, C.c_float, FP, FP] + [C.POINTER(FP)] * 5
     c = o.cfg
     keep = []
 
@@ -391,16 +409,21 @@ def ref_calc_grad(o: Oracle, fwd=None, adj=None) -> dict:
     L = int(c["L"])
     pars = [o.array("param", k) for k in ("M", "mu", "rho", "taup", "taus")]
     grads = [np.zeros(o.npar, np.float32) for _ in range(5)]
+    hess = [np.zeros(o.npar, np.float32) for _ in range(5)]
     pp = (FP * 5)(*[_fptr(p) for p in pars])
     gp = (FP * 5)(*[_fptr(g) for g in grads])
+    hp = (FP * 5)(*[_fptr(g) for g in hess]) if c.get("hout") else None
     info = o.dft_info()
     fl = np.zeros(8, np.float32)
     fl[:L] = np.atleast_1d(c["fl"])[:L]
     fn = np.ascontiguousarray(info["gradfreqsn"], np.float32)
     rc = lib.refcg_run(c["nd"], c["nz"], c["ny"], c["nx"], c["fdorder"], L, int(c["param_type"]), len(fn),
                        info["ntnyq"], info["dtnyq"], float(c["dt"]), float(c["f0"]), _fptr(fl), _fptr(fn), fw, ad, pp,
-                       gp)
+                       gp, hp)
     if rc:
         raise RuntimeError("reference calc_grad failed (%d)" % rc)
     sh = o.shape
-    return {k: g.reshape(sh) for k, g in zip(("M", "mu", "rho", "taup", "taus"), grads)}
+    out = {k: g.reshape(sh) for k, g in zip(("M", "mu", "rho", "taup", "taus"), grads)}
+    if c.get("hout"):
+        out.update({"H" + k: g.reshape(sh) for k, g in zip(("M", "mu", "rho", "taup", "taus"), hess)})
+    return out

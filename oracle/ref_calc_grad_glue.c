@@ -27,11 +27,12 @@ parameter *get_par(parameter *pars, int npars, const char *name)
 /* fwd/adj: 15 complex buffers in the order vx vy vz sxx syy szz sxy syz sxz
  * rxx ryy rzz rxy ryz rxz (NULL where the model has none), each
  * [nfreqs][(L)][padded cells]; par and grad: M, mu, rho, taup, taus over the
- * physical cells.  The buffers are modified in place, as the reference
+ * physical cells; hess (NULL: HOUT off) the Hessian arrays in the same
+ * order.  The buffers are modified in place, as the reference
  * modifies its host copies. */
 int refcg_run(int nd, int nz, int ny, int nx, int fdorder, int L, int par_type, int nfreqs, int ntnyq,
               int dtnyq, float dt, float f0, const float *fl, const float *gradfreqsn, float **fwd, float **adj,
-              float **par, float **grad)
+              float **par, float **grad, float **hess)
 {
     static const char *vname[15] = {"vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "syz", "sxz",
                                     "rxx", "ryy", "rzz", "rxy", "ryz", "rxz"};
@@ -59,6 +60,7 @@ int refcg_run(int nd, int nz, int ny, int nx, int fdorder, int L, int par_type, 
         pars[i].name = pname[i];
         pars[i].cl_par.host = par[i];
         pars[i].cl_grad.host = grad[i];
+        pars[i].cl_H.host = hess ? hess[i] : NULL;
         pars[i].to_grad = 1;
     }
     for (int l = 0; l < L && l < 8; l++) flc[l] = fl[l];
@@ -80,7 +82,7 @@ int refcg_run(int nd, int nz, int ny, int nx, int fdorder, int L, int par_type, 
     m->f0 = f0;
     m->FDORDER = fdorder;
     m->FDOH = fdorder / 2;
-    m->HOUT = 0;
+    m->HOUT = hess != NULL;
     m->csts = csts;
     m->ncsts = 2;
     m->nvars = nv;

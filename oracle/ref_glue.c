@@ -193,7 +193,8 @@ static void g_update_adjs(fdo_state *s)
                         s->rr[R_XX], s->rr[R_ZZ], s->rr[R_XZ], PP(s, P_M), PP(s, P_MU), PP(s, P_MUIPKP),
                         PP(s, P_TAUS), PP(s, P_TAUSIPKP), PP(s, P_TAUP), s->eta, s->taper, CX(s), CZ(s),
                         PS(s, PS_VX_X), PS(s, PS_VX_Z), PS(s, PS_VZ_X), PS(s, PS_VZ_Z), s->grad[G_RHO],
-                        s->grad[G_M], s->grad[G_MU], NULL, NULL, NULL, NULL, NULL, NULL, NULL, NULL, NULL, NULL);
+                        s->grad[G_M], s->grad[G_MU], NULL, NULL, NULL, s->hess[G_RHO], s->hess[G_M],
+                        s->hess[G_MU], s->hess[G_TAUP], s->hess[G_TAUS], NULL, NULL);
 #endif
     }
 }

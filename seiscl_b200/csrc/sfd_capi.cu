@@ -278,6 +278,13 @@ int alloc_adjoint(sfd_plan *p)
     }
     int64_t npar = (int64_t)g.nz * g.ny * g.nx;
     for (int k = 0; k < NG; k++) {
+        p->a.hess[k] = nullptr;
+        if (!g.hout) continue;
+        p->a.hess[k] = (double *)dalloc(p, sizeof(double) * npar, &e);
+        if (e) return fail(p, SFD_ERR_MEMORY, "Hessian allocation failed");
+        CKC(cudaMemset(p->a.hess[k], 0, sizeof(double) * npar));
+    }
+    for (int k = 0; k < NG; k++) {
         p->a.grad[k] = nullptr;
         if ((k == GTAUP || k == GTAUS) && !(bp2 && g.L > 0)) continue;
         p->a.grad[k] = (double *)dalloc(p, sizeof(double) * npar, &e);
@@ -580,6 +587,9 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     if (c.field_precision == 1 && (c.nd != 3 || c.L > 3)) return SFD_ERR_UNSUPPORTED;
     if (c.back_prop_type < 0 || c.back_prop_type > 2) return SFD_ERR_ARG;
     if (c.loop_graphs < 0 || c.loop_graphs > 2) return SFD_ERR_ARG;
+    if (c.hout < 0 || c.hout > 1) return SFD_ERR_ARG;
+    // the reference's 3D Hessian kernel does not compile (update_adjv3D.cl:486)
+    if (c.hout && c.nd == 3 && c.back_prop_type != 2) return SFD_ERR_UNSUPPORTED;
 
     sfd_plan *p = new sfd_plan();
     p->cfg = c;
@@ -599,6 +609,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     g.freesurf = c.freesurf ? 1 : 0;
     g.restype = c.restype;
     g.kernels = c.kernels;
+    g.hout = c.hout;
     g.nvol = (int64_t)g.NZ * g.NY * g.NX;
     double hc[6];
     holberg(c.fdorder, c.maxrelerror, hc);
@@ -911,8 +922,44 @@ extern "C" int sfd_zero_gradient(sfd_plan *p)
     int rc;
     if ((rc = alloc_adjoint(p))) return rc;
     int64_t npar = (int64_t)p->g.nz * p->g.ny * p->g.nx;
-    for (int k = 0; k < NG; k++)
+    for (int k = 0; k < NG; k++) {
         if (p->a.grad[k]) CKC(cudaMemset(p->a.grad[k], 0, sizeof(double) * npar));
+        if (p->a.hess[k]) CKC(cudaMemset(p->a.hess[k], 0, sizeof(double) * npar));
+    }
+    return SFD_OK;
+}
+
+extern "C" int sfd_get_hessian(sfd_plan *p, int transform, float *const *out)
+{
+    if (!p || !out) return SFD_ERR_ARG;
+    if (!p->g.hout) return fail(p, SFD_ERR_STATE, "the plan was not created with hout = 1");
+    if (!p->a.hess[0]) return fail(p, SFD_ERR_STATE, "no Hessian has been accumulated");
+    const int64_t n = (int64_t)p->g.nz * p->g.ny * p->g.nx;
+    std::vector<double> h[NG];
+    for (int k = 0; k < NG; k++) {
+        h[k].resize(n);
+        CKC(cudaMemcpy(h[k].data(), p->a.hess[k], sizeof(double) * n, cudaMemcpyDeviceToHost));
+    }
+    const int pt = p->cfg.param_type;
+    if (transform && p->cfg.back_prop_type != 2 && (pt == 0 || pt == 2)) {
+        // src/calc_grad.c:1004-1090 for the Hessian: the parameters rescaled
+        // as for the gradient, no division by dt
+        const double dt = p->cfg.dt, dh = p->cfg.dh;
+        for (int64_t i = 0; i < n; i++) {
+            const double rho = 1.0 / p->hp[PRHO][i] * dt / dh;
+            const double M = p->hp[PM][i] * dh / dt, mu = p->hp[PMU][i] * dh / dt;
+            h[GRHO][i] += M / rho * h[GM][i];
+            if (mu > 0) h[GRHO][i] += mu / rho * h[GMU][i];
+            const double sM = pt == 0 ? std::sqrt(rho * M) : std::sqrt(M / rho);
+            const double smu = pt == 0 ? std::sqrt(rho * mu) : std::sqrt(mu / rho);
+            h[GM][i] *= 2.0 * sM;
+            h[GMU][i] *= 2.0 * smu;
+        }
+    }
+    const int order[5] = {GM, GMU, GRHO, GTAUP, GTAUS};
+    for (int q = 0; q < 5; q++)
+        if (out[q])
+            for (int64_t i = 0; i < n; i++) out[q][i] = (float)h[order[q]][i];
     return SFD_OK;
 }
 

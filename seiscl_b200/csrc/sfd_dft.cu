@@ -133,6 +133,10 @@ __device__ __forceinline__ float rmprod(float2 a, float2 b, float ts, float w)
 {
     return ts * (a.x * b.x + a.y * b.y) + (a.x * b.y - a.y * b.x) / w;
 }
+// time derivative at angular frequency w: i w X
+__device__ __forceinline__ float2 cderiv(float2 a, float w) { return make_float2(-a.y * w, a.x * w); }
+// squared modulus, formed in FP64 and rounded once
+__device__ __forceinline__ float cnorm2(float2 a) { return (float)((double)a.x * a.x + (double)a.y * a.y); }
 
 }  // namespace
 
@@ -155,6 +159,7 @@ __global__ void __launch_bounds__(128) k_calc_grad(Grid g, Fields f, AdjFields a
     }
     const float N = d.ntnyq;
     double gM = 0, gmu = 0, gtp = 0, gts = 0, grho = 0;
+    double hM = 0, hmu = 0, htp = 0, hts = 0, hrho = 0;
     for (int fq = 0; fq < d.nf; fq++) {
         const float w = d.w[fq];
         const i64 ic = (i64)fq * g.nvol + iv;
@@ -215,6 +220,35 @@ __global__ void __launch_bounds__(128) k_calc_grad(Grid g, Fields f, AdjFields a
             dd[3] = dd[0];
             dd[4] = w * (itreal(axx, csub(fxx, fzz)) + itreal(azz, csub(fzz, fxx))) / N;
             dd[8] = w * (itreal(d.fw[1][VX][ic], d.fw[0][VX][ic]) + itreal(d.fw[1][VZ][ic], d.fw[0][VZ][ic])) / N;
+            if (g.hout) {
+                // approximate Hessian (calc_grad.c:838-905, 2D only): squared moduli of
+                // the forward transforms, with the stresses as corrected above
+                float hd[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                for (int l = 0; l < L; l++) {
+                    const i64 il = ((i64)fq * L + l) * g.nvol + iv;
+                    const float2 rxx = d.fr[0][RXX][il], rzz = d.fr[0][RZZ][il], rxz = d.fr[0][RXZ][il];
+                    const float2 sum = cadd(rxx, rzz), dxx = csub(rxx, rzz), dzz = csub(rzz, rxx);
+                    const float wt = w * d.tausig[l];
+                    hd[1] += cnorm2(cadd(sum, cderiv(sum, wt))) / N;
+                    hd[5] += cnorm2(cadd(rxz, cderiv(rxz, wt))) / N;
+                    hd[6] = hd[1];
+                    hd[7] += (cnorm2(cadd(dxx, cderiv(dxx, wt))) + cnorm2(cadd(dzz, cderiv(dzz, wt)))) / N;
+                }
+                hd[0] = cnorm2(cderiv(cadd(fxx, fzz), w)) / N;
+                hd[2] = cnorm2(cderiv(fxz, w)) / N;
+                hd[3] = hd[0];
+                hd[4] = (cnorm2(cderiv(csub(fxx, fzz), w)) + cnorm2(cderiv(csub(fzz, fxx), w))) / N;
+                hd[8] = (cnorm2(cderiv(d.fw[0][VX][ic], w)) + cnorm2(cderiv(d.fw[0][VZ][ic], w))) / N;
+                double h[9];
+                for (int q = 0; q < 9; q++) h[q] = hd[q];
+                // the gradient's signs reversed
+                hM += c[0] * h[0] - c[1] * h[1];
+                hmu += c[2] * h[2] - c[3] * h[3] + c[4] * h[4] - c[5] * h[5] + c[6] * h[6] - c[7] * h[7];
+                htp += c[8] * h[0] - c[9] * h[1];
+                hts += c[10] * h[2] - c[11] * h[3] + c[12] * h[4] - c[13] * h[5] + c[14] * h[6] - c[15] * h[7];
+                hrho += h[8] - c[16] * h[0] + c[17] * h[1] - c[18] * h[2] + c[19] * h[3] - c[20] * h[4] +
+                        c[21] * h[5] - c[22] * h[6] + c[23] * h[7];
+            }
         }
         double e[9];
         for (int q = 0; q < 9; q++) e[q] = dd[q];
@@ -231,6 +265,15 @@ __global__ void __launch_bounds__(128) k_calc_grad(Grid g, Fields f, AdjFields a
     if (L > 0) {
         a.grad[GTAUP][im] += gtp;
         a.grad[GTAUS][im] += gts;
+    }
+    if (g.hout && g.nd != 3) {
+        a.hess[GM][im] += hM;
+        a.hess[GMU][im] += hmu;
+        a.hess[GRHO][im] += hrho;
+        if (L > 0) {
+            a.hess[GTAUP][im] += htp;
+            a.hess[GTAUS][im] += hts;
+        }
     }
 }
 

@@ -62,6 +62,7 @@ struct Grid {
     int kernels;            // 0: register-blocked 3D kernels where available, 1: general only
     int bp2;                // adjoint kernels: 1 for the DFT gradient (no reconstruction,
                             // boundary injection or on-the-fly gradient)
+    int hout;               // accumulate the approximate Hessian
 };
 
 struct Fields {
@@ -78,6 +79,7 @@ struct AdjFields {
     float *wr[NW];
     float *rr[NR];
     double *grad[NG];
+    double *hess[NG];       // approximate Hessian (HOUT), same layout as grad
     const void *bnd[NW];    // slice t-1 of the saved boundaries
 };
 

@@ -2150,9 +2150,16 @@ __global__ void __launch_bounds__(256) k_adjs2d(Grid g, Fields f, AdjFields a)
         float dM = c1 * (sxx + szz) * (lsxx + lszz);
         a.grad[GM][ip] += (double)(-dM);
         a.grad[GMU][ip] += (double)(-c3 * (sxz * lsxz) + dM - c5 * ((sxx - szz) * (lsxx - lszz)));
+        if (g.hout) {
+            // update_adjs2D.cl:453-457 (the mu term subtracts the gradient's dM)
+            float dMH = c1 * (sxx + szz) * (sxx + szz);
+            a.hess[GM][ip] += (double)dMH;
+            a.hess[GMU][ip] += (double)(c3 * sxz * sxz - dM + c5 * (sxx - szz) * (sxx - szz));
+        }
     } else {
         float dM = (sxx + szz) * (lsxx + lszz);
         a.grad[GM][ip] += (double)(-dM);
+        if (g.hout) a.hess[GM][ip] += (double)((sxx + szz) * (sxx + szz));
     }
 }
 

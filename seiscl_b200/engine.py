@@ -36,7 +36,8 @@ class sfd_config(C.Structure):
                 ("k_max_cpml", C.c_float), ("abpc", C.c_float), ("tmin", C.c_int), ("tmax", C.c_int),
                 ("param_type", C.c_int), ("restype", C.c_int), ("precision", C.c_int),
                 ("kernels", C.c_int), ("adjoint_reset_psi", C.c_int), ("field_precision", C.c_int),
-                ("back_prop_type", C.c_int), ("loop_graphs", C.c_int), ("reserved", C.c_int * 2)]
+                ("back_prop_type", C.c_int), ("loop_graphs", C.c_int), ("hout", C.c_int),
+                ("reserved", C.c_int * 1)]
 
 
 class sfd_shot(C.Structure):
@@ -58,6 +59,7 @@ EXPORTS = {
     "sfd_zero_gradient": (C.c_int, [C.c_void_p]),
     "sfd_get_gradient": (C.c_int, [C.c_void_p, C.c_int, FP, FP, FP]),
     "sfd_get_gradient_q": (C.c_int, [C.c_void_p, FP, FP]),
+    "sfd_get_hessian": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FP)]),
     "sfd_set_gradfreqs": (C.c_int, [C.c_void_p, FP, C.c_int, C.POINTER(C.c_int)]),
     "sfd_set_movie": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(FP)]),
     "sfd_residual_scale": (C.c_int, [C.c_void_p, C.POINTER(sfd_shot), C.POINTER(C.c_int), C.POINTER(FP)]),
@@ -143,6 +145,7 @@ class Config:
     back_prop_type: int = 1  # 1: boundary-saving backpropagation, 2: DFT gradient at `gradfreqs`
     gradfreqs: Sequence[float] = ()  # DFT gradient frequencies (Hz), back_prop_type 2
     loop_graphs: str = "auto"  # time loops as CUDA graphs: "auto" (2D), "always", "never"
+    hout: int = 0  # HOUT: also accumulate the approximate Hessian (2D)
 
     def to_c(self) -> sfd_config:
         c = sfd_config()
@@ -178,6 +181,7 @@ class Config:
         c.field_precision = {"fp32": 0, "fp16": 1}[self.field_precision]
         c.back_prop_type = int(self.back_prop_type)
         c.loop_graphs = {"auto": 0, "always": 1, "never": 2}[self.loop_graphs]
+        c.hout = int(self.hout)
         return c
 
     @property
@@ -326,6 +330,21 @@ class Plan:
             q = [np.zeros(sh, np.float32) for _ in range(2)]
             self._check(self.lib.sfd_get_gradient_q(self.h, *[_ptr(a) for a in q]))
             out["taup"], out["taus"] = q
+        return out
+
+    def hessian(self, transform=True):
+        """Approximate Hessian (plans with hout=1), keyed as gradient()."""
+        sh = self.cfg.model_shape
+        h = [np.zeros(sh, np.float32) for _ in range(5)]
+        self._check(self.lib.sfd_get_hessian(self.h, 1 if transform else 0, (FP * 5)(*[_ptr(a) for a in h])))
+        dft = int(self.cfg.back_prop_type) == 2
+        if transform or dft:
+            names = {0: ("vp", "vs", "rho"), 1: ("M", "mu", "rho"), 2: ("Ip", "Is", "rho")}[self.cfg.param_type]
+        else:
+            names = ("M", "mu", "rho")
+        out = dict(zip(names, h[:3]))
+        if int(self.cfg.L) > 0:
+            out["taup"], out["taus"] = h[3], h[4]
         return out
 
     def dft(self, slot: int, kind: str, name: str) -> np.ndarray:

@@ -500,7 +500,27 @@ class SeisCL:
         return output
 
     def read_Hessian(self, workdir=None, param_names=None, filename=None):
-        raise SeisCLError('Could not read Hessian: the approximate Hessian is not computed by this engine')
+        """Approximate Hessian of the last run (``Hout=1``), as read_grad
+        (SeisCL.py:604-634)."""
+        if filename is None:
+            filename = self.file_gout
+        if param_names is None:
+            param_names = self.params
+        mat = self._files.get(os.path.basename(filename))
+        if mat is None:
+            raise SeisCLError('Could not read Hessian')
+        try:
+            output = [np.array(mat['H' + name], copy=True) for name in param_names]
+        except KeyError as exc:
+            raise SeisCLError('Could not read Hessian') from exc
+        if self.cropgrad:
+            for o in output:
+                if self.freesurf == 0:
+                    o[:self.nab, ...] = 0
+                o[-self.nab:, ...] = 0
+                o[:, :self.nab, ...] = 0
+                o[:, -self.nab:, ...] = 0
+        return output
 
     def read_rms(self, workdir=None, filename=None):
         """(rms / rms_norm, rms_norm) of the last run (SeisCL.py:636-656)."""
@@ -521,7 +541,7 @@ class SeisCL:
         if bpt == 2 and self.gradout and not freqs:
             # read_hdf5.c:546-549 requires /gradfreqs for the DFT gradient
             raise SeisCLError("Error: back_prop_type=2 needs gradfreqs")
-        for flag in ("Hout", "gradsrcout"):
+        for flag in ("gradsrcout",):
             if getattr(self, flag):
                 raise SeisCLError("Error: %s is not provided by this engine" % flag)
         return engine.Config(
@@ -534,7 +554,8 @@ class SeisCL:
             param_type=int(self.param_type), restype=int(self.restype),
             precision="fp16" if int(self.FP16) >= 2 else "fp32",
             field_precision="fp16" if int(self.FP16) >= 2 and int(self.ND) == 3 and not self.gradout else "fp32",
-            back_prop_type=bpt, gradfreqs=freqs if bpt == 2 else ())
+            back_prop_type=bpt, gradfreqs=freqs if bpt == 2 else (),
+            hout=1 if (self.Hout and self.gradout) else 0)
 
     def _steps(self, seconds) -> int:
         """A time in seconds as a step count, FP32 quotient truncated
@@ -795,8 +816,11 @@ class SeisCL:
                                           "rms_norm": np.array([np.sqrt(rmsnorm)], np.float32)}
         if self.gradout:
             g = plan.gradient(transform=True)
+            H = plan.hessian(transform=True) if self.Hout else None
             if world > 1:
                 g = shots_mod.allreduce_sum(g)
+                if H is not None:
+                    H = shots_mod.allreduce_sum(H)
             shape = tuple(int(v) for v in np.atleast_1d(self.N))
             names = {0: ("vp", "vs"), 1: ("M", "mu"), 2: ("Ip", "Is")}[self.param_type]
             gout = {}
@@ -809,6 +833,9 @@ class SeisCL:
                 # the boundary-saving gradient leaves taup/taus at zero (writehdf5.c:262-275)
                 v = g[name] if name in g else np.zeros_like(g["rho"])
                 gout["grad" + name] = np.ascontiguousarray(np.transpose(v)).reshape(shape)
+                if H is not None:
+                    v = H[name] if name in H else np.zeros_like(H["rho"])
+                    gout["H" + name] = np.ascontiguousarray(np.transpose(v)).reshape(shape)
             self._files[self.file_gout] = gout
         ms = (time.perf_counter() - t0) * 1e3
         return "%d shot(s) (%d on rank %d of %d), %d trace(s), %d time steps: %.1f ms\n" % (

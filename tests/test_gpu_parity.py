@@ -343,3 +343,63 @@ def test_loop_graphs_match_direct_launches(kw, cuda_device):
             assert np.array_equal(s_a[k], s_b[k]), k
     for k in got["always"][1]:
         assert np.array_equal(got["always"][1][k], got["never"][1][k]), k
+
+
+HESS_CASES = [
+    (dict(nd=2, freesurf=1, L=0, abs_type=1, src_type=100), dict(hout=1)),
+    (dict(nd=2, freesurf=0, L=0, abs_type=2, src_type=2), dict(hout=1, restype=1)),
+    (dict(nd=2, freesurf=1, L=0, abs_type=1, src_type=100, nt=160), dict(hout=1, back_prop_type=2,
+                                                                       gradfreqs=[10.0, 18.0])),
+    (dict(nd=2, freesurf=0, L=1, abs_type=1, src_type=100, nt=160), dict(hout=1, back_prop_type=2,
+                                                                       gradfreqs=[12.0, 20.0])),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", HESS_CASES, ids=lambda c: "-".join("%s%s" % kv for kv in c[1].items()
+                                                                  if kv[0] != "gradfreqs"))
+def test_hessian_matches_oracle(case, cuda_device):
+    """The approximate Hessian (HOUT) of the CUDA path against the oracle:
+    raw accumulators and, for the boundary-saving gradient, the transformed
+    Hessian."""
+    import dataclasses
+
+    from oracle.oracle import Oracle
+    from seiscl_b200.engine import Plan
+
+    kw, extra = case
+    cfg, model, acq = make_case(**kw)
+    cfg.update(extra)
+    ora = Oracle(cfg)
+    ora.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+    ec = dataclasses.replace(engine_config(cfg), hout=1, restype=extra.get("restype", 0),
+                             back_prop_type=extra.get("back_prop_type", 1), gradfreqs=tuple(extra.get("gradfreqs", ())))
+    plan = Plan(ec)
+    plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+    outs = ["vx", "vz"]
+    d = ora.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs, save_boundaries=True)
+    plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs, save_boundaries=True)
+    res = {k: (0.3 * v).astype(np.float32) for k, v in d.items()}
+    ora.clear_gradients()
+    ora.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], res)
+    plan.zero_gradient()
+    plan.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], res)
+    dft = extra.get("back_prop_type") == 2
+    raw_o = ora.hessians(transform=False)
+    raw_e = plan.hessian(transform=False)
+    names = ("vp", "vs", "rho") if dft else ("M", "mu", "rho")
+    pairs = list(zip(names, ("M", "mu", "rho")))
+    if dft and cfg["L"]:
+        pairs += [("taup", "taup"), ("taus", "taus")]
+    for ours, theirs in pairs:
+        ref = raw_o[theirs]
+        if np.abs(ref).max() == 0:   # Hrho of the boundary-saving form stays zero
+            assert np.abs(raw_e[ours]).max() == 0, ours
+            continue
+        assert rel_l2(raw_e[ours], ref) < GRAD_TOL, (ours, rel_l2(raw_e[ours], ref))
+    if not dft:
+        tr_o = ora.hessians(transform=True)
+        tr_e = plan.hessian(transform=True)
+        for k in ("vp", "vs", "rho"):
+            if np.abs(tr_o[k]).max() > 0:
+                assert rel_l2(tr_e[k], tr_o[k]) < GRAD_TOL, (k, rel_l2(tr_e[k], tr_o[k]))

@@ -235,3 +235,42 @@ def test_dft_gradient_matches_reference_build(case, param_type):
         scale = np.abs(gr[k]).max()
         assert np.isfinite(g0[k]).all(), k
         assert np.abs(g0[k] - gr[k]).max() <= 1e-6 * scale, k
+
+
+HESS_LIVE = [
+    (dict(nd=2, freesurf=1, L=0, nt=120, seed=1), dict(hout=1)),
+    (dict(nd=2, freesurf=0, L=0, nt=120, seed=2, abs_type=2), dict(hout=1, restype=1)),
+    (dict(nd=2, freesurf=0, L=2, nt=120, seed=3), dict(hout=1)),
+    (dict(nd=2, freesurf=1, L=0, nt=120, seed=4), dict(hout=1, back_prop_type=2, gradfreqs=[10.0, 18.0])),
+    (dict(nd=2, freesurf=0, L=1, nt=120, seed=5), dict(hout=1, back_prop_type=2, gradfreqs=[10.0, 25.0])),
+]
+
+
+@pytest.mark.skipif(not _ref_available(), reason="reference tree not present")
+@pytest.mark.parametrize("case", HESS_LIVE, ids=lambda c: "-".join("%s%s" % kv for kv in c[1].items() if kv[0] != "gradfreqs"))
+def test_hessian_matches_reference_build(case):
+    """Approximate Hessian (HOUT): the boundary-saving form bit for bit
+    against the reference's 2D adjoint kernels compiled with HOUT=1; the DFT
+    form against the reference's calc_grad compiled in place."""
+    from oracle.oracle import Oracle, ref_calc_grad
+
+    kw, extra = case
+    got = []
+    for ref in (False, True):
+        cfg, model, acq = make_case(**kw)
+        cfg.update(extra)
+        o = Oracle(cfg, ref=ref)
+        assert o.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"]) == 0
+        d = o.forward(acq["src_pos"], acq["src"], acq["rec_pos"], ["vx", "vz"], save_boundaries=True)
+        o.clear_gradients()
+        o.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], {k: (0.3 * v).astype(np.float32) for k, v in d.items()})
+        got.append((o, o.hessians(transform=False)))
+    (o0, h0), (o1, h1) = got
+    assert np.abs(h0["M"]).max() > 0
+    for k in h0:
+        assert np.array_equal(h0[k], h1[k]), k
+    if extra.get("back_prop_type") == 2:
+        r = ref_calc_grad(o0)
+        for k in h0:
+            scale = np.abs(r["H" + k]).max()
+            assert np.abs(h0[k] - r["H" + k]).max() <= 1e-6 * scale, k

@@ -425,3 +425,24 @@ def test_dft_gradient_job_matches_oracle(cuda_device):
         assert rel_l2(got.T, g[name]) < GRAD_TOL, name
     assert np.isclose(rms_norm, np.sqrt(n2), rtol=1e-4)
     assert np.isclose(rms, np.sqrt(r2) / np.sqrt(n2), rtol=1e-3)
+
+
+@pytest.mark.gpu
+def test_hessian_job_returns_the_engine_hessian(cuda_device):
+    """Hout=1: read_Hessian returns the engine's transformed Hessian summed
+    over the job's shots, cropped like read_grad."""
+    s = _two_shot_job(Hout=1)
+    model = _models(tuple(s.N), 11)
+    s.set_forward(s.src_pos_all[3, :], model, withgrad=False)
+    s.execute()
+    d = s.read_data()
+    s.write_data({"vx": (0.7 * d[0]).astype(np.float32), "vz": (0.7 * d[1]).astype(np.float32)})
+    s.cropgrad = False
+    s.set_forward(s.src_pos_all[3, :], model, withgrad=True)
+    s.execute()
+    H = s.read_Hessian()
+    assert len(H) == 3 and H[0].shape == tuple(s.N)
+    assert np.abs(H[0]).max() > 0 and np.abs(H[1]).max() > 0
+    s.cropgrad = True
+    Hc = s.read_Hessian()
+    assert np.all(Hc[0][:, :s.nab] == 0) and np.array_equal(Hc[0][30, 30], H[0][30, 30])
