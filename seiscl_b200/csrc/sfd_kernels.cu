@@ -721,9 +721,26 @@ __device__ __forceinline__ void stq(float *p, const Q4 &q)
 {
     *reinterpret_cast<float4 *>(p) = make_float4(q.v[0], q.v[1], q.v[2], q.v[3]);
 }
+// FP16 storage: four halves move as one 64-bit access
+__device__ __forceinline__ Q4 q4_of(uint2 u)
+{
+    const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&u.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&u.y));
+    return Q4{{a.x, a.y, b.x, b.y}};
+}
+__device__ __forceinline__ Q4 ldq(const __half *p) { return q4_of(__ldg(reinterpret_cast<const uint2 *>(p))); }
+__device__ __forceinline__ Q4 ldq_rw(const __half *p) { return q4_of(*reinterpret_cast<const uint2 *>(p)); }
+__device__ __forceinline__ void stq(__half *p, const Q4 &q)
+{
+    const __half2 a = __floats2half2_rn(q.v[0], q.v[1]), b = __floats2half2_rn(q.v[2], q.v[3]);
+    uint2 u;
+    u.x = *reinterpret_cast<const unsigned *>(&a);
+    u.y = *reinterpret_cast<const unsigned *>(&b);
+    *reinterpret_cast<uint2 *>(p) = u;
+}
 // forward / backward differences of four cells along a stride (x or y)
-template <int F>
-__device__ __forceinline__ Q4 dfw_q(const float *__restrict__ v, i64 i, i64 st, const float *hc)
+template <int F, class T>
+__device__ __forceinline__ Q4 dfw_q(const T *__restrict__ v, i64 i, i64 st, const float *hc)
 {
     Q4 a = ldq(v + i + st), b = ldq(v + i), r;
 #pragma unroll
@@ -737,8 +754,8 @@ __device__ __forceinline__ Q4 dfw_q(const float *__restrict__ v, i64 i, i64 st, 
     }
     return r;
 }
-template <int F>
-__device__ __forceinline__ Q4 dbw_q(const float *__restrict__ v, i64 i, i64 st, const float *hc)
+template <int F, class T>
+__device__ __forceinline__ Q4 dbw_q(const T *__restrict__ v, i64 i, i64 st, const float *hc)
 {
     Q4 a = ldq(v + i), b = ldq(v + i - st), r;
 #pragma unroll
@@ -756,13 +773,14 @@ __device__ __forceinline__ Q4 dbw_q(const float *__restrict__ v, i64 i, i64 st, 
 struct W12 {
     float w[12];
 };
-__device__ __forceinline__ W12 ldw(const float *__restrict__ v, i64 i)
+template <class T>
+__device__ __forceinline__ W12 ldw(const T *__restrict__ v, i64 i)
 {
     W12 r;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        float4 t = __ldg(reinterpret_cast<const float4 *>(v + i - 4 + 4 * k));
-        r.w[4 * k] = t.x; r.w[4 * k + 1] = t.y; r.w[4 * k + 2] = t.z; r.w[4 * k + 3] = t.w;
+        const Q4 t = ldq(v + i - 4 + 4 * k);
+        r.w[4 * k] = t.v[0]; r.w[4 * k + 1] = t.v[1]; r.w[4 * k + 2] = t.v[2]; r.w[4 * k + 3] = t.v[3];
     }
     return r;
 }
@@ -910,22 +928,26 @@ __device__ __forceinline__ void cpml_v3d_q4(const Grid &g, const Fields &f, int 
     const i64 iv = gx * sx + (i64)gy * sy + gz0;                                       \
     const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
 
+template <class T>
 __global__ void __launch_bounds__(128) k_v3d_q4(Grid g, Fields f)
 {
     CELL3D_Q4
     const float *hc = g.hc;
-    Q4 vx = ldq_rw(f.w[VX] + iv), vy = ldq_rw(f.w[VY] + iv), vz = ldq_rw(f.w[VZ] + iv);
+    T *wvx = fld<T>(f.w[VX]), *wvy = fld<T>(f.w[VY]), *wvz = fld<T>(f.w[VZ]);
+    const T *Sxx = fld<T>(f.w[SXX]), *Syy = fld<T>(f.w[SYY]), *Szz = fld<T>(f.w[SZZ]);
+    const T *Sxy = fld<T>(f.w[SXY]), *Syz = fld<T>(f.w[SYZ]), *Sxz = fld<T>(f.w[SXZ]);
+    Q4 vx = ldq_rw(wvx + iv), vy = ldq_rw(wvy + iv), vz = ldq_rw(wvz + iv);
     const Q4 rip = ldq(f.p[PRIP] + ip), rjp = ldq(f.p[PRJP] + ip), rkp = ldq(f.p[PRKP] + ip);
-    const W12 wzz = ldw(f.w[SZZ], iv), wxz = ldw(f.w[SXZ], iv), wyz = ldw(f.w[SYZ], iv);
+    const W12 wzz = ldw(Szz, iv), wxz = ldw(Sxz, iv), wyz = ldw(Syz, iv);
     Q4 szz_z = dfw_z<F>(wzz, hc);
-    Q4 sxx_x = dfw_q<F>(f.w[SXX], iv, sx, hc);
-    Q4 sxz_x = dbw_q<F>(f.w[SXZ], iv, sx, hc);
+    Q4 sxx_x = dfw_q<F>(Sxx, iv, sx, hc);
+    Q4 sxz_x = dbw_q<F>(Sxz, iv, sx, hc);
     Q4 sxz_z = dbw_z<F>(wxz, hc);
-    Q4 syz_y = dbw_q<F>(f.w[SYZ], iv, sy, hc);
+    Q4 syz_y = dbw_q<F>(Syz, iv, sy, hc);
     Q4 syz_z = dbw_z<F>(wyz, hc);
-    Q4 syy_y = dfw_q<F>(f.w[SYY], iv, sy, hc);
-    Q4 sxy_x = dbw_q<F>(f.w[SXY], iv, sx, hc);
-    Q4 sxy_y = dbw_q<F>(f.w[SXY], iv, sy, hc);
+    Q4 syy_y = dfw_q<F>(Syy, iv, sy, hc);
+    Q4 sxy_x = dbw_q<F>(Sxy, iv, sx, hc);
+    Q4 sxy_y = dbw_q<F>(Sxy, iv, sy, hc);
     if (g.abs_type == 1) cpml_v3d_q4(g, f, gz0, gy, gx, sxx_x, syy_y, szz_z, sxy_y, sxy_x, syz_y, syz_z, sxz_x, sxz_z);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -935,9 +957,9 @@ __global__ void __launch_bounds__(128) k_v3d_q4(Grid g, Fields f)
         if (g.abs_type == 2) taper_regs<3>(g, f.taper, gz0 + j, gy, gx, v3);
         vx.v[j] = v3[0]; vy.v[j] = v3[1]; vz.v[j] = v3[2];
     }
-    stq(f.w[VX] + iv, vx);
-    stq(f.w[VY] + iv, vy);
-    stq(f.w[VZ] + iv, vz);
+    stq(wvx + iv, vx);
+    stq(wvy + iv, vy);
+    stq(wvz + iv, vz);
 }
 
 // CPML corrections of cpml_s3d (forward form) for a quad of z cells
@@ -1023,13 +1045,12 @@ __device__ __forceinline__ void cpml_s3d_q4(const Grid &g, const Fields &f, int 
 // sxz with rxy, ryz, rxz) -- each loading only its own memory variables and
 // parameters, so the live state fits in registers; the components are
 // independent, so the split changes no result.
-template <int L>
+template <int L, class T>
 __device__ __forceinline__ void s_normal_q4(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip,
-                                            const Q4 &vxx,
-                                            const Q4 &vyy, const Q4 &vzz)
+                                            const Q4 &vxx, const Q4 &vyy, const Q4 &vzz)
 {
-    float *const ws[3] = {f.w[SXX], f.w[SYY], f.w[SZZ]};
-    float *const wr[3] = {f.r[RXX], f.r[RYY], f.r[RZZ]};
+    T *const ws[3] = {fld<T>(f.w[SXX]), fld<T>(f.w[SYY]), fld<T>(f.w[SZZ])};
+    T *const wr[3] = {fld<T>(f.r[RXX]), fld<T>(f.r[RYY]), fld<T>(f.r[RZZ])};
     Q4 sq[3];
 #pragma unroll
     for (int q = 0; q < 3; q++) sq[q] = ldq_rw(ws[q] + iv);
@@ -1098,13 +1119,12 @@ __device__ __forceinline__ void s_normal_q4(const Grid &g, const Fields &f, int 
     for (int q = 0; q < 3; q++) stq(ws[q] + iv, sq[q]);
 }
 
-template <int L>
+template <int L, class T>
 __device__ __forceinline__ void s_shear_q4(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip,
-                                           const Q4 &vxyyx,
-                                           const Q4 &vyzzy, const Q4 &vxzzx)
+                                           const Q4 &vxyyx, const Q4 &vyzzy, const Q4 &vxzzx)
 {
-    float *const ws[3] = {f.w[SXY], f.w[SYZ], f.w[SXZ]};
-    float *const wr[3] = {f.r[RXY], f.r[RYZ], f.r[RXZ]};
+    T *const ws[3] = {fld<T>(f.w[SXY]), fld<T>(f.w[SYZ]), fld<T>(f.w[SXZ])};
+    T *const wr[3] = {fld<T>(f.r[RXY]), fld<T>(f.r[RYZ]), fld<T>(f.r[RXZ])};
     Q4 sq[3];
 #pragma unroll
     for (int q = 0; q < 3; q++) sq[q] = ldq_rw(ws[q] + iv);
@@ -1172,17 +1192,18 @@ __device__ __forceinline__ void s_shear_q4(const Grid &g, const Fields &f, int g
     for (int q = 0; q < 3; q++) stq(ws[q] + iv, sq[q]);
 }
 
-template <int L>
+template <int L, class T>
 __global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f)
 {
     CELL3D_Q4
     const float *hc = g.hc;
-    Q4 vzz = dbw_z<F>(ldw(f.w[VZ], iv), hc);
-    Q4 vyz = dfw_z<F>(ldw(f.w[VY], iv), hc);
-    Q4 vxz = dfw_z<F>(ldw(f.w[VX], iv), hc);
-    Q4 vzx = dfw_q<F>(f.w[VZ], iv, sx, hc), vzy = dfw_q<F>(f.w[VZ], iv, sy, hc);
-    Q4 vyx = dfw_q<F>(f.w[VY], iv, sx, hc), vyy = dbw_q<F>(f.w[VY], iv, sy, hc);
-    Q4 vxx = dbw_q<F>(f.w[VX], iv, sx, hc), vxy = dfw_q<F>(f.w[VX], iv, sy, hc);
+    const T *Vx = fld<T>(f.w[VX]), *Vy = fld<T>(f.w[VY]), *Vz = fld<T>(f.w[VZ]);
+    Q4 vzz = dbw_z<F>(ldw(Vz, iv), hc);
+    Q4 vyz = dfw_z<F>(ldw(Vy, iv), hc);
+    Q4 vxz = dfw_z<F>(ldw(Vx, iv), hc);
+    Q4 vzx = dfw_q<F>(Vz, iv, sx, hc), vzy = dfw_q<F>(Vz, iv, sy, hc);
+    Q4 vyx = dfw_q<F>(Vy, iv, sx, hc), vyy = dbw_q<F>(Vy, iv, sy, hc);
+    Q4 vxx = dbw_q<F>(Vx, iv, sx, hc), vxy = dfw_q<F>(Vx, iv, sy, hc);
     if (g.abs_type == 1) cpml_s3d_q4(g, f, gz0, gy, gx, vxx, vxy, vxz, vyx, vyy, vyz, vzx, vzy, vzz);
     Q4 vxyyx, vyzzy, vxzzx;
 #pragma unroll
@@ -1191,8 +1212,8 @@ __global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f)
         vyzzy.v[j] = vyz.v[j] + vzy.v[j];
         vxzzx.v[j] = vxz.v[j] + vzx.v[j];
     }
-    s_normal_q4<L>(g, f, gz0, gy, gx, iv, ip, vxx, vyy, vzz);
-    s_shear_q4<L>(g, f, gz0, gy, gx, iv, ip, vxyyx, vyzzy, vxzzx);
+    s_normal_q4<L, T>(g, f, gz0, gy, gx, iv, ip, vxx, vyy, vzz);
+    s_shear_q4<L, T>(g, f, gz0, gy, gx, iv, ip, vxyyx, vyzzy, vxzzx);
 }
 
 // ------------------------------------------- 4-cell vectorised 3D adjoint
@@ -1622,7 +1643,7 @@ __global__ void __launch_bounds__(128, 4) k_adjs3d_q4(Grid g, Fields f, AdjField
 }
 
 // true when the 4-cell kernels apply to this grid
-static inline bool q4_ok(const Grid &g) { return g.nd == 3 && g.F == 4 && g.nz % 4 == 0 && !g.fhalf; }
+static inline bool q4_ok(const Grid &g) { return g.nd == 3 && g.F == 4 && g.nz % 4 == 0; }
 
 template <int F, int L, class T = float>
 __global__ void __launch_bounds__(256, 2) k_s3d_stream(Grid g, Fields f)
@@ -2519,7 +2540,12 @@ static inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b)
 
 void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
 {
-    if (g.fhalf && g.nd == 3) {   // FP16 storage: the streaming kernels only
+    if (g.fhalf && g.nd == 3) {   // FP16 storage: the vectorised or the streaming kernels
+        if (q4_ok(g)) {
+            dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4));
+            k_v3d_q4<__half><<<gr, b, 0, st>>>(g, f);
+            return;
+        }
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
         DISPATCH_F(g.F, k_v3d_stream<FF, __half><<<gr, b, 0, st>>>(g, f));
         return;
@@ -2541,7 +2567,7 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
             // rows of neighbouring threads share L1 lines (0.35 ms at 256^3,
             // against 0.39 for 32 x 2 x 2)
             dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4));
-            k_v3d_q4<<<gr, b, 0, st>>>(g, f);
+            k_v3d_q4<float><<<gr, b, 0, st>>>(g, f);
             return;
         }
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
@@ -2558,7 +2584,17 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
 
 void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
 {
-    if (g.fhalf && g.nd == 3 && g.L <= 3) {   // FP16 storage: the streaming kernels only
+    if (g.fhalf && g.nd == 3 && g.L <= 3) {   // FP16 storage: the vectorised or the streaming kernels
+        if (q4_ok(g)) {
+            dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1));
+            switch (g.L) {
+            case 0: k_s3d_q4<0, __half><<<g4, b4, 0, st>>>(g, f); break;
+            case 1: k_s3d_q4<1, __half><<<g4, b4, 0, st>>>(g, f); break;
+            case 2: k_s3d_q4<2, __half><<<g4, b4, 0, st>>>(g, f); break;
+            default: k_s3d_q4<3, __half><<<g4, b4, 0, st>>>(g, f); break;
+            }
+            return;
+        }
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
         switch (g.L) {
         case 0: DISPATCH_F(g.F, k_s3d_stream<FF, 0, __half><<<gr, b, 0, st>>>(g, f)); break;
@@ -2583,10 +2619,10 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
         if ((g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) {
             dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1));  // 0.70 ms vs 0.71 (32 x 2 x 2)
             switch (g.L) {
-            case 0: k_s3d_q4<0><<<g4, b4, 0, st>>>(g, f); break;
-            case 1: k_s3d_q4<1><<<g4, b4, 0, st>>>(g, f); break;
-            case 2: k_s3d_q4<2><<<g4, b4, 0, st>>>(g, f); break;
-            default: k_s3d_q4<3><<<g4, b4, 0, st>>>(g, f); break;
+            case 0: k_s3d_q4<0, float><<<g4, b4, 0, st>>>(g, f); break;
+            case 1: k_s3d_q4<1, float><<<g4, b4, 0, st>>>(g, f); break;
+            case 2: k_s3d_q4<2, float><<<g4, b4, 0, st>>>(g, f); break;
+            default: k_s3d_q4<3, float><<<g4, b4, 0, st>>>(g, f); break;
             }
             return;
         }
@@ -2632,7 +2668,7 @@ int stress_family(const Grid &g, const Fields &f)
 {
     // the same selection as launch_update_s
     if (g.nd != 3) return 0;
-    if (g.fhalf && g.L <= 3) return 4;
+    if (g.fhalf && g.L <= 3) return q4_ok(g) ? 5 : 4;
     if (g.kernels == 3 && tma_ready(g, f)) return 3;
     if (g.kernels == 2) return 2;
     if ((g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) return 5;
