@@ -79,8 +79,12 @@ typedef struct sfd_config {
     int precision;     /* SFD_PREC_*: storage of the saved boundaries */
     int kernels;       /* 0: fastest measured: in 3D the 4-cell vectorised kernels where
                              they apply (8th order, nz a multiple of 4, L <= 3), else the
-                             streaming ones; general kernels in 2D,
-                          1: general one-thread-per-cell kernels only,
+                             streaming ones; in 2D (P-SV, acoustic) modelling runs
+                             without saved boundaries, DFT or movie, two launches per
+                             step (the stress update carries the free surface, the
+                             receivers and the next step's sources),
+                          1: general one-thread-per-cell kernels only, one launch per
+                             reference kernel,
                           2: register-blocked 3D kernels where available,
                           3: TMA-pipelined 3D velocity and stress updates,
                           4: streaming one-thread-per-cell 3D kernels (per-cell loads first),

@@ -637,6 +637,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     p->bnd_elem = c.precision == SFD_PREC_FP32 ? 4 : 2;
     p->cap_src = p->cap_rec = 0;
     p->d_surf_q = nullptr;
+    p->d_ticket = nullptr;
     memset(&p->f, 0, sizeof p->f);
     memset(&p->a, 0, sizeof p->a);
     p->last_ms = 0.0f;
@@ -796,8 +797,19 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
     // (time_stepping.c:819-822)
     Movie mv;
     if (!(save_boundaries && !dft) && (rc = movie_setup(p, omask, mv))) return rc;
+    // 2D P-SV / acoustic modelling: two launches per step (update_v; update_s
+    // with the free surface, the receivers and the next step's sources)
+    const bool fuse2d = (g.nd == 2 || g.nd == 22) && g.kernels != 1 && !save_boundaries && !dft && !mv.n;
+    if (fuse2d) {
+        if (!p->d_ticket) {
+            cudaError_t e;
+            p->d_ticket = (int *)dalloc(p, sizeof(int), &e);
+            if (e) return fail(p, SFD_ERR_MEMORY, "step counter allocation failed");
+        }
+        CKC(cudaMemsetAsync(p->d_ticket, 0, sizeof(int), st));
+    }
     LoopKey key;
-    key.add(mv.n); key.add(p->movout); key.add(p->d_mov);
+    key.add(mv.n); key.add(p->movout); key.add(p->d_mov); key.add(fuse2d); key.add(p->d_ticket);
     key.add(1); key.add(p->g); key.add(p->f); key.add_points(S); key.add_points(R); key.add(p->d_src);
     key.add(p->d_seis); key.add(omask); key.add(dft); key.add(save_boundaries != 0); key.add(bs);
     key.add(p->cfg.precision); key.add(tmax); key.add(tmin);
@@ -807,6 +819,15 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
     }
     CKC(cudaEventRecord(p->ev0, st));
     int rcl = run_loop(p, p->gfwd, key.s, st, [&](cudaStream_t s) {
+        if (fuse2d) {
+            if (tmax > 0) launch_sources(g, p->f, S, p->d_src, NT, 0, 1, s);
+            for (int t = 0; t < tmax; t++) {
+                launch_update_v(g, p->f, s);
+                StepTail tl{p->d_ticket, R, p->d_seis, omask, t, S, p->d_src, t + 1 < tmax ? t + 1 : -1, NT};
+                launch_update_s_step(g, p->f, tl, s);
+            }
+            return;
+        }
         for (int t = 0; t < tmax; t++) {
             // the state after t steps, before the sources of step t (time_stepping.c:766-781)
             if (dft && t >= tmin && (t - tmin) % p->dtnyq == 0) dft_sample(p, 0, (t - tmin) / p->dtnyq, s);

@@ -92,6 +92,18 @@ struct PointSet {           // sources or receivers of one shot, device side
     const int *kz;          // z cell index (free-surface adjoint skip)
 };
 
+struct StepTail {           // fused 2D forward step: the work of its last block
+    int *ticket;            // blocks finished; 0 between launches
+    PointSet rec;           // receivers recorded at step t into out [nsel][nrec][nt_total]
+    float *out;
+    unsigned outmask;
+    int t;
+    PointSet src;           // sources injected for step tsrc (< 0: none)
+    const float *stf;       // [nsrc][nt_total]
+    int tsrc;
+    int nt_total;
+};
+
 }  // namespace sfd
 
 struct sfd_plan {
@@ -121,6 +133,7 @@ struct sfd_plan {
     int *d_src_nt, *d_src_field, *d_src_kz;
     float *d_src_div, *d_src, *d_seis, *d_res;
     float *d_surf_q;        // surface-adjoint scratch [nx][ny]
+    int *d_ticket;          // fused 2D steps: block counter of the stress launch
     cudaEvent_t ev0, ev1;
     int kshift;             // FP16 storage: log2 ratio of velocity to stress scales
     float last_ms;

@@ -311,12 +311,10 @@ __global__ void __launch_bounds__(256) k_v2d(Grid g, Fields f)
     }
 }
 
+// one cell of the P-SV stress update (update_s2D.cl:30-327)
 template <int F>
-__global__ void __launch_bounds__(256) k_s2d(Grid g, Fields f)
+__device__ __forceinline__ void s2d_cell(const Grid &g, const Fields &f, int gz, int gx)
 {
-    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
-    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
-    if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
     i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
     const float *hc = g.hc;
     float vxx = dbw<F>(f.w[VX], iv, g.NZ, hc);
@@ -371,12 +369,10 @@ __global__ void __launch_bounds__(256) k_s2d(Grid g, Fields f)
     }
 }
 
-// free surface, one thread per surface column (surface2D.cl:30-193)
+// free surface of one column (surface2D.cl:30-193)
 template <int F>
-__global__ void k_surf2d(Grid g, Fields f, int pdir)
+__device__ __forceinline__ void surf2d_column(const Grid &g, const Fields &f, int gx, int pdir)
 {
-    int gx = blockIdx.x * blockDim.x + threadIdx.x + F;
-    if (gx > g.NX - F - 1) return;
     int gz = F, NZ = g.NZ, L = g.L, NAB = g.nab;
     i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * NZ + gz;
     float *vx = f.w[VX], *vz = f.w[VZ], *sxx = f.w[SXX], *szz = f.w[SZZ], *sxz = f.w[SXZ];
@@ -423,6 +419,22 @@ __global__ void k_surf2d(Grid g, Fields f, int pdir)
         }
         sxx[iv] += pdir * (g.dt2 * sump);
     }
+}
+
+// free surface, one thread per surface column
+template <int F>
+__global__ void k_surf2d(Grid g, Fields f, int pdir)
+{
+    int gx = blockIdx.x * blockDim.x + threadIdx.x + F;
+    if (gx <= g.NX - F - 1) surf2d_column<F>(g, f, gx, pdir);
+}
+
+template <int F>
+__global__ void __launch_bounds__(256) k_s2d(Grid g, Fields f)
+{
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_cell<F>(g, f, gz, gx);
 }
 
 // ===================================================================== 3D
@@ -1852,12 +1864,10 @@ __global__ void __launch_bounds__(256) k_v2d_acc(Grid g, Fields f)
     f.w[VZ][iv] = vz;
 }
 
+// one cell of the acoustic pressure update (update_s2D_acc.cl:79-402)
 template <int F>
-__global__ void __launch_bounds__(256) k_s2d_acc(Grid g, Fields f)
+__device__ __forceinline__ void s2d_acc_cell(const Grid &g, const Fields &f, int gz, int gx)
 {
-    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
-    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
-    if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
     i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
     int NAB = g.nab, NZ = g.NZ, NX = g.NX, L = g.L;
     float vxx = dbw<F>(f.w[VX], iv, NZ, g.hc);
@@ -1908,6 +1918,14 @@ __global__ void __launch_bounds__(256) k_s2d_acc(Grid g, Fields f)
         if (gx > NX - NAB - F - 1) p *= tp[NX - F - gx - 1];
     }
     f.w[SXX][iv] = p;
+}
+
+template <int F>
+__global__ void __launch_bounds__(256) k_s2d_acc(Grid g, Fields f)
+{
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_acc_cell<F>(g, f, gz, gx);
 }
 
 // ================================================================== 2D SH
@@ -2457,12 +2475,11 @@ __global__ void k_surfadj3d_b(Grid g, Fields f, AdjFields a, const float *q)
 
 // ------------------------------------------------ point kernels (per shot)
 // src/automatic_kernels.c:394-629; several sources may share a cell
-template <class T = float>
-__global__ void k_sources(Fields f, PointSet s, const float *src, int nt_total, int t, int pdir, float dt,
-                          int freesurf, int F, WScale ws)
+template <class T>
+__device__ __forceinline__ void source_point(const Fields &f, const PointSet &s, const float *src, int nt_total,
+                                             int t, int pdir, float dt, int freesurf, int F, const WScale &ws,
+                                             int gid)
 {
-    int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= s.n) return;
     i64 cell = s.cell[gid];
     if (cell < 0) return;
     if (freesurf && pdir == -1 && s.kz[gid] < 2 * F) return;
@@ -2475,30 +2492,104 @@ __global__ void k_sources(Fields f, PointSet s, const float *src, int nt_total, 
     }
 }
 
-// src/automatic_kernels.c:22-219; out is [nsel][nrec][NT]
 template <class T = float>
-__global__ void k_record(Fields f, PointSet r, float *out, int nt_total, int t, unsigned outmask, int nd, WScale ws)
+__global__ void k_sources(Fields f, PointSet s, const float *src, int nt_total, int t, int pdir, float dt,
+                          int freesurf, int F, WScale ws)
 {
     int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= r.n) return;
+    if (gid < s.n) source_point<T>(f, s, src, nt_total, t, pdir, dt, freesurf, F, ws, gid);
+}
+
+// src/automatic_kernels.c:22-219; out is [nsel][nrec][NT].  L2: the loads
+// bypass L1 (values stored by other blocks of the running kernel).
+template <class T> __device__ __forceinline__ float ldv_l2(const T *p);
+template <> __device__ __forceinline__ float ldv_l2<float>(const float *p) { return __ldcg(p); }
+template <> __device__ __forceinline__ float ldv_l2<__half>(const __half *p) { return __half2float(__ldcg(p)); }
+
+template <class T, bool L2>
+__device__ __forceinline__ void record_point(const Fields &f, const PointSet &r, float *out, int nt_total, int t,
+                                             unsigned outmask, int nd, const WScale &ws, int gid)
+{
     i64 cell = r.cell[gid];
     if (cell < 0) return;
+    auto ld = [](const T *q) { return L2 ? ldv_l2<T>(q) : ldv(q); };
     int slot = 0;
     for (int o = 0; o < SFD_NOUT; o++) {
         if (!(outmask & (1u << o))) continue;
         float v;
         if (o == SFD_OUT_P) {
             const T *xx = fld<T>(f.w[SXX]), *zz = fld<T>(f.w[SZZ]);
-            if (nd == 3) v = (ldv(xx + cell) + ldv(zz + cell) + ldv(fld<T>(f.w[SYY]) + cell)) / 3.0f;
-            else if (nd == 22) v = ldv(xx + cell);
-            else v = (ldv(xx + cell) + ldv(zz + cell)) / 2.0f;
+            if (nd == 3) v = (ld(xx + cell) + ld(zz + cell) + ld(fld<T>(f.w[SYY]) + cell)) / 3.0f;
+            else if (nd == 22) v = ld(xx + cell);
+            else v = (ld(xx + cell) + ld(zz + cell)) / 2.0f;
             v /= ws.w[SXX];
         } else {
-            v = ldv(fld<T>(f.w[o]) + cell) / ws.w[o];
+            v = ld(fld<T>(f.w[o]) + cell) / ws.w[o];
         }
         out[((i64)slot * r.n + gid) * nt_total + t] = v;
         slot++;
     }
+}
+
+template <class T = float>
+__global__ void k_record(Fields f, PointSet r, float *out, int nt_total, int t, unsigned outmask, int nd, WScale ws)
+{
+    int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid < r.n) record_point<T, false>(f, r, out, nt_total, t, outmask, nd, ws, gid);
+}
+
+// ---------------------------------------------- fused 2D forward step tail
+// The stress kernel of a fused 2D step ends with the receivers of step t
+// and the sources of step t+1 (time_stepping.c:783-816 order: sources,
+// update_v, update_s, surface, record), run by the block that finishes
+// last: every block fences its stores and takes a ticket; the block with
+// the last ticket sees all stores of the launch, records, adds the next
+// step's sources and resets the ticket.  Nothing waits on another block.
+__device__ __forceinline__ void step_tail(const Grid &g, const Fields &f, const StepTail &tl)
+{
+    __shared__ int s_last;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nth = blockDim.x * blockDim.y * blockDim.z;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(tl.ticket, 1) == (int)(gridDim.x * gridDim.y * gridDim.z) - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int i = tid; i < tl.rec.n; i += nth)
+        record_point<float, true>(f, tl.rec, tl.out, tl.nt_total, tl.t, tl.outmask, g.nd, g.ws, i);
+    __syncthreads();
+    if (tl.tsrc >= 0)
+        for (int i = tid; i < tl.src.n; i += nth)
+            source_point<float>(f, tl.src, tl.stf, tl.nt_total, tl.tsrc, 1, g.dt, g.freesurf, g.F, g.ws, i);
+    if (tid == 0) *tl.ticket = 0;
+}
+
+// P-SV stress update, free surface (blocks of the top row: their 32 z
+// rows hold every stress the surface reads, rows F..2F) and step tail.
+// pdir (1) is a launch argument, as for the separate surface kernel, so
+// that both contract and round alike.
+template <int F>
+__global__ void __launch_bounds__(256) k_s2d_step(Grid g, Fields f, StepTail tl, int pdir)
+{
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_cell<F>(g, f, gz, gx);
+    if (g.freesurf && blockIdx.x == 0) {
+        __syncthreads();
+        if (threadIdx.x == 0 && gx <= g.NX - F - 1) surf2d_column<F>(g, f, gx, pdir);
+    }
+    step_tail(g, f, tl);
+}
+
+// acoustic pressure update and step tail (no free-surface kernel)
+template <int F>
+__global__ void __launch_bounds__(256) k_s2d_acc_step(Grid g, Fields f, StepTail tl)
+{
+    int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
+    int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
+    if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_acc_cell<F>(g, f, gz, gx);
+    step_tail(g, f, tl);
 }
 
 // src/automatic_kernels.c:631-836; res is [nsel][nrec][NT]
@@ -2674,6 +2765,15 @@ int stress_family(const Grid &g, const Fields &f)
     if ((g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) return 5;
     if ((g.kernels == 0 || g.kernels == 4 || g.kernels == 5) && g.L <= 3) return 4;
     return 1;
+}
+
+bool launch_update_s_step(const Grid &g, const Fields &f, const StepTail &tl, cudaStream_t st)
+{
+    if (g.nd != 2 && g.nd != 22) return false;
+    dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));   // 32 z rows >= 2F + 1: the surface stays in its block
+    if (g.nd == 2) DISPATCH_F(g.F, k_s2d_step<FF><<<gr, b, 0, st>>>(g, f, tl, 1))
+    else DISPATCH_F(g.F, k_s2d_acc_step<FF><<<gr, b, 0, st>>>(g, f, tl))
+    return true;
 }
 
 void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st)

@@ -26,6 +26,9 @@ int tma_take_status();      // 1 if a TMA stage of the last launches never arriv
 int stress_family(const Grid &g, const Fields &f);
 void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st);
 void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st);
+// 2D P-SV and acoustic forward: stress update, free surface, receivers of
+// step tl.t and sources of step tl.tsrc in one launch (false: not 2D)
+bool launch_update_s_step(const Grid &g, const Fields &f, const StepTail &tl, cudaStream_t st);
 void launch_savebnd(const Grid &g, const Fields &f, const BndSlot &b, int prec, int64_t tofs, cudaStream_t st);
 void launch_update_adj(const Grid &g, const Fields &f, const AdjFields &a, bool stress, int prec, cudaStream_t st);
 void launch_surface_adj(const Grid &g, const Fields &f, const AdjFields &a, float *q, cudaStream_t st);
