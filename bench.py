@@ -423,47 +423,47 @@ def run_gradient(args):
     }))
 
 
-def run_serving(args):
-    """Service mix: Poisson arrivals of forward (70 %) and gradient (30 %)
-    requests with random 2D and small 3D grids, orders 4/8, elastic or
-    viscoelastic, on a pool of workers sharing one GPU.  Reports requests
-    and shots per second and latency percentiles."""
-    import dataclasses
-
-    import torch
-
+def serving_requests(nreq, seed=501):
+    """The service mix (seeded): 70 % forward / 30 % gradient requests; 80 %
+    2D grids (nz 100-400, nx 200-1000), 20 % 3D (64-128^3); physics acoustic,
+    elastic or viscoelastic (L 1-3); FD order 4 or 8; NT 500-1500; 1-8 Ricker
+    shots at 5-20 Hz, 64 receivers; +-10 % random models.  Acoustic gradient
+    requests run as P-SV with vs = 0, the reference's route (the reference's
+    acoustic kernels have no adjoint)."""
     from seiscl_b200 import serving
     from seiscl_b200.engine import Config
     from seiscl_b200.qfit import band_frequencies, q_to_tau
 
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    rng = np.random.default_rng(501)
-    nreq = max(args.steps, 1)
-    reqs, arrivals = [], np.cumsum(rng.exponential(1.0 / args.rate, nreq))
+    rng = np.random.default_rng(seed)
+    reqs = []
     for i in range(nreq):
         three = rng.uniform() < 0.2
-        L = int(rng.integers(0, 3))
+        physics = ["acoustic", "elastic", "visco"][int(rng.integers(0, 3))]
+        L = int(rng.integers(1, 4)) if physics == "visco" else 0
         order = int(rng.choice([4, 8]))
         nt = int(rng.integers(500, 1500))
         f0 = float(rng.uniform(5, 20))
+        kind = "gradient" if rng.uniform() < 0.3 else "forward"
         if three:
             n = int(rng.integers(64, 129)) // 2 * 2
             N, shape = [n, n, n], (n, n, n)
         else:
             nz, nx = int(rng.integers(100, 400)) // 2 * 2, int(rng.integers(200, 1000))
             N, shape = [nz, nx], (nx, nz)
+        nd = 3 if three else (22 if physics == "acoustic" and kind == "forward" else 2)
         fl = band_frequencies(L, 0.5 * f0, 2.5 * f0) if L else [f0]
-        cfg = Config(N=N, ND=3 if three else 2, dh=10.0, dt=8e-4, NT=nt, L=L, f0=f0, FL=fl, FDORDER=order,
-                     freesurf=1, nab=16)
+        cfg = Config(N=N, ND=nd, dh=10.0, dt=8e-4, NT=nt, L=L, f0=f0, FL=fl, FDORDER=order,
+                     freesurf=0 if nd == 22 else 1, nab=16)
         vp = np.full(shape, 3000.0, np.float32) * (1 + 0.1 * rng.uniform(-1, 1, shape)).astype(np.float32)
-        m = {"vp": vp, "vs": (vp / 1.8).astype(np.float32), "rho": np.full(shape, 2000.0, np.float32)}
+        vs = np.zeros(shape, np.float32) if physics == "acoustic" else (vp / 1.8).astype(np.float32)
+        m = {"vp": vp, "vs": None if nd == 22 else vs, "rho": np.full(shape, 2000.0, np.float32)}
         if L:
             tau = q_to_tau(50.0, fl, 0.5 * f0, 2.5 * f0)
             m["taup"] = np.full(shape, tau, np.float32)
             m["taus"] = np.full(shape, tau, np.float32)
         nx_ = shape[0]
         shots = []
-        for k in range(int(rng.integers(1, 5))):
+        for k in range(int(rng.integers(1, 9))):
             x = float(rng.uniform(20, nx_ - 20)) * 10.0
             y = shape[1] // 2 * 10.0 if three else 0.0
             sp = np.array([[x, y, 50.0, k, 100]], np.float32)
@@ -473,11 +473,23 @@ def run_serving(args):
             rp[:, 2] = 50.0
             rp[:, 4] = np.arange(1, 65)
             shots.append((sp, ricker(f0, nt, cfg.dt)[None, :], rp))
-        kind = "gradient" if rng.uniform() < 0.3 else "forward"
         obs = [{"vx": np.zeros((64, nt), np.float32), "vz": np.zeros((64, nt), np.float32)} for _ in shots] \
             if kind == "gradient" else None
         reqs.append(serving.Request(cfg, m, shots, ("vx", "vz"), kind, obs, rid=i))
-    with serving.Server(workers=args.workers) as srv:
+    return reqs
+
+
+def _serve_stream(reqs, arrivals, workers, plain):
+    """Submit the requests at their arrival times; returns (results, wall s,
+    admission stats).  plain: one worker, time loops launched step by step
+    (no CUDA graphs), i.e. the shots one after another with plain launches."""
+    import dataclasses
+
+    from seiscl_b200 import serving
+
+    if plain:
+        reqs = [dataclasses.replace(q, config=dataclasses.replace(q.config, loop_graphs="never")) for q in reqs]
+    with serving.Server(workers=1 if plain else workers) as srv:
         futs = []
         t0 = time.perf_counter()
         for a, q in zip(arrivals, reqs):
@@ -487,18 +499,53 @@ def run_serving(args):
             futs.append(srv.submit(q))
         res = [f.result() for f in futs]
         wall = time.perf_counter() - t0
-    lat = [r.latency for r in res]
-    p = serving.percentiles(lat)
+        st = srv.stats()
+    return res, wall, st
+
+
+def run_serving(args):
+    """Service mix on one GPU: Poisson arrivals (rate --rate) of the
+    requests of ``serving_requests``, served by a pool of workers with
+    admission by device memory; then the same stream served plainly (one
+    request at a time, shots launched step by step).  Reports shots/s and
+    latency percentiles of both."""
+    import torch
+
+    from seiscl_b200 import serving
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    nreq = max(args.steps, 1)
+    reqs = serving_requests(nreq)
+    arrivals = np.cumsum(np.random.default_rng(502).exponential(1.0 / args.rate, nreq))
     nshots = sum(len(q.shots) for q in reqs)
+    # warm-up: load the library and the CUDA context outside the timed streams
+    _serve_stream(reqs[:1], [0.0], 1, False)
+    res, wall, st = _serve_stream(reqs, arrivals, args.workers, False)
+    p = serving.percentiles([r.latency for r in res])
+    plain = None
+    if not args.no_plain:
+        pres, pwall, _ = _serve_stream(reqs, arrivals, 1, True)
+        pp = serving.percentiles([r.latency for r in pres])
+        plain = {"shots_per_s": round(nshots / pwall, 3), "wall_s": round(pwall, 2),
+                 "latency_s": {k: round(v, 3) for k, v in pp.items()},
+                 "what": "same request stream, one request at a time, step-by-step launches (no CUDA graphs)"}
+    cells = 0.0
+    for q in reqs:
+        n = float(np.prod(q.config.N))
+        cells += n * q.config.NT * len(q.shots) * (2 if q.kind == "gradient" else 1)
     print(json.dumps({
         "metric": "shots/s", "value": round(nshots / wall, 3), "unit": "shots/s", "n_gpus": 1,
-        "steps": nreq, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "steps": nreq, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "serving", "requests": nreq, "arrival_rate_per_s": args.rate, "workers": args.workers,
+        "config": {"workload": "serving", "requests": nreq, "shots": nshots, "arrival_rate_per_s": args.rate,
+                   "workers": args.workers,
                    "mix": "70 % forward / 30 % gradient; 80 % 2D (100-400 x 200-1000), 20 % 3D (64-128^3); "
-                          "order 4/8; L 0-2; NT 500-1500; 1-4 shots"},
+                          "acoustic / elastic / visco L 1-3; order 4/8; NT 500-1500; 1-8 shots"},
         "requests_per_s": round(nreq / wall, 3), "latency_s": {k: round(v, 3) for k, v in p.items()},
-        "wall_s": round(wall, 2),
+        "wall_s": round(wall, 2), "gcell_updates_per_s": round(cells / wall / 1e9, 3),
+        "admission": {k: int(v) for k, v in st.items()},
+        "plain": plain,
+        "speedup_vs_plain": round(plain["wall_s"] / wall, 3) if plain else None,
     }))
 
 
@@ -514,6 +561,7 @@ def main():
                     help="storage of wave fields and memory variables (arithmetic is FP32 either way)")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: request arrival rate (1/s)")
     ap.add_argument("--workers", type=int, default=4, help="serving: worker threads")
+    ap.add_argument("--no-plain", action="store_true", help="serving: skip the plain one-at-a-time arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--ref-budget", type=float, default=15.0)

@@ -127,6 +127,18 @@ int sfd_plan_create(const sfd_config *cfg, sfd_plan **out);
 void sfd_plan_destroy(sfd_plan *plan);
 const char *sfd_last_error(const sfd_plan *plan);
 
+/* Device bytes a plan for `cfg` allocates to run shots with up to nsrc
+ * sources and nrec_sel = receivers x selected outputs: model, wave fields,
+ * memory variables, CPML memory, constants and shot buffers; gradient != 0
+ * adds what a gradient run holds (saved boundaries, adjoint fields and
+ * gradient sums for back_prop_type 1; the transforms at nfreqs frequencies
+ * for back_prop_type 2).  Computed from the configuration alone (no device
+ * call), for admission control by a caller that shares one device among
+ * many plans.  No counterpart in the reference. */
+int sfd_footprint(const sfd_config *cfg, int gradient, int nsrc, int64_t nrec_sel, int nfreqs, int64_t *bytes);
+/* Free and total memory of the current device (cudaMemGetInfo). */
+int sfd_device_memory(int64_t *free_bytes, int64_t *total_bytes);
+
 /* Upload the model.  params = {vp, vs, rho} (param_type 0), plus {taup, taus}
  * when L > 0, each a host array of nz*ny*nx floats in [nx][ny][nz] order.
  * vs may be NULL for zero shear.  Applies the reference transforms

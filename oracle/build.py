@@ -38,19 +38,21 @@ def _run(cmd):
         raise RuntimeError("oracle build failed: %s\n%s" % (" ".join(cmd), r.stderr[-4000:]))
 
 
-def port_lib_path() -> str:
-    return os.path.join(BUILD, "libfdo_port.so")
+def port_lib_path(fp64: bool = False) -> str:
+    return os.path.join(BUILD, "libfdo_port64.so" if fp64 else "libfdo_port.so")
 
 
-def build_port(force: bool = False) -> str:
-    out = port_lib_path()
+def build_port(force: bool = False, fp64: bool = False) -> str:
+    """The restatement as a shared library; fp64: its FP64 build (FDO_FP64)."""
+    out = port_lib_path(fp64)
     srcs = [os.path.join(HERE, s) for s in PORT_SOURCES + ["fdo.h"]]
     if not force and os.path.exists(out):
         if os.path.getmtime(out) >= max(os.path.getmtime(s) for s in srcs):
             return out
     os.makedirs(BUILD, exist_ok=True)
     tmp = out + ".tmp%d" % os.getpid()
-    _run(["gcc", *CFLAGS, "-shared", "-o", tmp, *[os.path.join(HERE, s) for s in PORT_SOURCES], "-lm"])
+    _run(["gcc", *CFLAGS, *(["-DFDO_FP64"] if fp64 else []), "-shared", "-o", tmp,
+          *[os.path.join(HERE, s) for s in PORT_SOURCES], "-lm"])
     os.replace(tmp, out)
     return out
 

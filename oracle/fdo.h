@@ -38,6 +38,17 @@
 
 #include <stdint.h>
 
+/* FDO_FP64: the FP64 build of the same restatement (every float of the
+ * interface, the state and the arithmetic becomes double), the double
+ * precision reference that FP32 and FP16-storage results are measured
+ * against.  Files include this header after their system headers. */
+#ifdef FDO_FP64
+#define float double
+#define sqrtf sqrt
+#define powf pow
+#define fabsf fabs
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif

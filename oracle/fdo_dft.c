@@ -33,11 +33,12 @@
  * test_oracle_pin.py checks this file against the reference's calc_grad
  * compiled in place.
  */
-#include "fdo.h"
 
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
+
+#include "fdo.h"   /* after the system headers: FDO_FP64 retypes float */
 
 #define FDO_PI 3.141592653589793238462643383279502884197169
 

@@ -12,12 +12,13 @@
  * DFT gradient (BACK_PROP_TYPE=2): the same loops with the transforms of
  *   fdo_dft.c, src/time_stepping.c:766-781 (forward), :862-972 (adjoint)
  */
-#include "fdo.h"
 
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+
+#include "fdo.h"   /* after the system headers: FDO_FP64 retypes float */
 
 typedef int64_t i64;
 

@@ -9,11 +9,12 @@
  * as the reference kernels do when HC1..HC6 are double literals
  * (src/header_FD.cl:87-265, src/clprogram.c:493-496).
  */
-#include "fdo.h"
 
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
+
+#include "fdo.h"   /* after the system headers: FDO_FP64 retypes float */
 
 typedef int64_t i64;
 

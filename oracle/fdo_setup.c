@@ -7,12 +7,13 @@
  * Every routine keeps the float/double mix of the reference host code so the
  * results are bit-identical to the reference compiled as C.
  */
-#include "fdo.h"
 
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+
+#include "fdo.h"   /* after the system headers: FDO_FP64 retypes float */
 
 #define FDO_PI (3.141592653589793238462643383279502884197169)
 

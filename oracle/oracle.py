@@ -5,7 +5,11 @@ tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use it.
 
 ``Oracle(cfg)`` runs the C restatement (fdo_port.c); ``Oracle(cfg, ref=True)``
 runs the reference's own kernel sources compiled in place (oracle/_ref), with
-the same restated time loop.  Inputs and outputs follow SeisCL's host
+the same restated time loop; ``Oracle(cfg, fp64=True)`` runs the FP64 build of
+the restatement (every float of it retyped double, fdo.h FDO_FP64): the
+double-precision result that FP32 and FP16-storage runs are measured against.
+Its inputs are the same FP32 values (configuration floats and arrays are
+rounded to FP32 first) and its outputs are float64.  Inputs and outputs follow SeisCL's host
 conventions: models are [nx][nz] (2D) or [nx][ny][nz] (3D) arrays with z
 fastest; src_pos is [nsrc][5], rec_pos [nrec][8], src [nsrc][NT]; seismograms
 are [nrec][NT] per recorded variable.
@@ -30,16 +34,22 @@ PSI_IDS = {n: i for i, n in enumerate(
      "psi_sxz_z", "psi_syz_z", "psi_szz_z"])}
 
 
-class fdo_cfg(C.Structure):
-    _fields_ = [("nd", C.c_int), ("nz", C.c_int), ("ny", C.c_int), ("nx", C.c_int),
-                ("fdorder", C.c_int), ("fdoh", C.c_int), ("maxrelerror", C.c_int),
-                ("nab", C.c_int), ("freesurf", C.c_int), ("abs_type", C.c_int), ("L", C.c_int),
-                ("nt", C.c_int), ("tmin", C.c_int), ("tmax", C.c_int),
-                ("dt", C.c_float), ("dh", C.c_float), ("f0", C.c_float), ("fl", C.c_float * 8),
-                ("vppml", C.c_float), ("fpml", C.c_float), ("npower", C.c_float),
-                ("k_max_cpml", C.c_float), ("abpc", C.c_float),
-                ("param_type", C.c_int), ("restype", C.c_int), ("back_prop_type", C.c_int),
-                ("nfreqs", C.c_int), ("gradfreqs", C.c_float * 16), ("hout", C.c_int)]
+def _cfg_class(real):
+    class _Cfg(C.Structure):
+        _fields_ = [("nd", C.c_int), ("nz", C.c_int), ("ny", C.c_int), ("nx", C.c_int),
+                    ("fdorder", C.c_int), ("fdoh", C.c_int), ("maxrelerror", C.c_int),
+                    ("nab", C.c_int), ("freesurf", C.c_int), ("abs_type", C.c_int), ("L", C.c_int),
+                    ("nt", C.c_int), ("tmin", C.c_int), ("tmax", C.c_int),
+                    ("dt", real), ("dh", real), ("f0", real), ("fl", real * 8),
+                    ("vppml", real), ("fpml", real), ("npower", real),
+                    ("k_max_cpml", real), ("abpc", real),
+                    ("param_type", C.c_int), ("restype", C.c_int), ("back_prop_type", C.c_int),
+                    ("nfreqs", C.c_int), ("gradfreqs", real * 16), ("hout", C.c_int)]
+    return _Cfg
+
+
+fdo_cfg = _cfg_class(C.c_float)
+fdo_cfg64 = _cfg_class(C.c_double)     # the FDO_FP64 build's layout
 
 
 DEFAULTS = dict(nd=2, ny=1, fdorder=8, maxrelerror=1, nab=16, freesurf=0, abs_type=1, L=0, tmin=0,
@@ -47,10 +57,10 @@ DEFAULTS = dict(nd=2, ny=1, fdorder=8, maxrelerror=1, nab=16, freesurf=0, abs_ty
                 abpc=6.0, param_type=0, restype=0, back_prop_type=1, gradfreqs=())
 
 
-def make_cfg(cfg: dict) -> fdo_cfg:
+def make_cfg(cfg: dict, fp64: bool = False):
     d = dict(DEFAULTS)
     d.update(cfg)
-    c = fdo_cfg()
+    c = fdo_cfg64() if fp64 else fdo_cfg()
     for k in ["nd", "nz", "ny", "nx", "fdorder", "maxrelerror", "nab", "freesurf", "abs_type", "L", "nt",
               "tmin", "tmax", "param_type", "restype"]:
         setattr(c, k, int(d[k]))
@@ -58,8 +68,8 @@ def make_cfg(cfg: dict) -> fdo_cfg:
     if c.nd != 3:
         c.ny = 1
     for k in ["dt", "dh", "f0", "vppml", "fpml", "npower", "k_max_cpml", "abpc"]:
-        setattr(c, k, float(d[k]))
-    fl = list(np.atleast_1d(d["fl"]).astype(float))
+        setattr(c, k, float(np.float32(d[k])))
+    fl = list(np.atleast_1d(d["fl"]).astype(np.float32).astype(float))
     for i in range(8):
         c.fl[i] = fl[i] if i < len(fl) else 0.0
     c.back_prop_type = int(d.get("back_prop_type", 1))
@@ -68,17 +78,18 @@ def make_cfg(cfg: dict) -> fdo_cfg:
         raise ValueError("at most 16 DFT gradient frequencies")
     c.nfreqs = len(gf)
     for i, v in enumerate(gf):
-        c.gradfreqs[i] = v
+        c.gradfreqs[i] = float(np.float32(v))
     c.hout = int(d.get("hout", 0))
     return c
 
 
-def _lib(path):
+def _lib(path, real=C.c_float):
     lib = C.CDLL(path)
     P = C.c_void_p
-    FP = C.POINTER(C.c_float)
+    FP = C.POINTER(real)
     lib.fdo_create.restype = P
-    lib.fdo_create.argtypes = [C.POINTER(fdo_cfg), C.c_int, C.POINTER(C.c_int)]
+    lib.fdo_create.argtypes = [C.POINTER(fdo_cfg64 if real is C.c_double else fdo_cfg), C.c_int,
+                               C.POINTER(C.c_int)]
     lib.fdo_destroy.argtypes = [P]
     lib.fdo_model.argtypes = [P, FP, FP, FP, FP, FP]
     lib.fdo_run_forward.argtypes = [P, C.c_int, FP, FP, C.c_int, FP, C.POINTER(C.c_int), C.c_int,
@@ -98,13 +109,14 @@ def _lib(path):
     lib.fdo_info.argtypes = [P, C.POINTER(C.c_int64)]
     lib.fdo_run_steps.argtypes = [P, C.c_int]
     lib.fdo_holberg.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
-    lib.fdo_source_targets.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]
+    lib.fdo_source_targets.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), FP]
     lib.fdo_inject_ind.argtypes = [P, C.c_int, C.c_int, C.c_int]
     lib.fdo_savebnd_cell.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
     return lib
 
 
 _PORT = None
+_PORT64 = None
 
 
 def port_lib():
@@ -114,10 +126,17 @@ def port_lib():
     return _PORT
 
 
+def port_lib64():
+    global _PORT64
+    if _PORT64 is None:
+        _PORT64 = _lib(_build.build_port(fp64=True), C.c_double)
+    return _PORT64
+
+
 def _fptr(a):
     if a is None:
         return None
-    return a.ctypes.data_as(C.POINTER(C.c_float))
+    return a.ctypes.data_as(C.POINTER(C.c_double if a.dtype == np.float64 else C.c_float))
 
 
 def source_type_mask(src_pos: np.ndarray) -> int:
@@ -134,13 +153,18 @@ def source_type_mask(src_pos: np.ndarray) -> int:
 
 
 class Oracle:
-    def __init__(self, cfg: dict, ref: bool = False):
+    def __init__(self, cfg: dict, ref: bool = False, fp64: bool = False):
+        if ref and fp64:
+            raise ValueError("the reference kernels are FP32 only")
         self.cfg = dict(DEFAULTS)
         self.cfg.update(cfg)
         if self.cfg["nd"] != 3:
             self.cfg["ny"] = 1
-        self._c = make_cfg(self.cfg)
-        self.lib = port_lib()
+        self.fp64 = fp64
+        self.dtype = np.float64 if fp64 else np.float32
+        self.real = C.c_double if fp64 else C.c_float
+        self._c = make_cfg(self.cfg, fp64)
+        self.lib = port_lib64() if fp64 else port_lib()
         if ref:
             h0 = self._make(self.lib, False)
             info = self._info(self.lib, h0)
@@ -184,7 +208,8 @@ class Oracle:
         return (c["nx"], c["ny"], c["nz"]) if c["nd"] == 3 else (c["nx"], c["nz"])
 
     def set_model(self, vp, vs, rho, taup=None, taus=None) -> int:
-        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float32).reshape(self.shape)
+        arrs = [None if a is None else
+                np.ascontiguousarray(np.asarray(a, np.float32), dtype=self.dtype).reshape(self.shape)
                 for a in (vp, vs, rho, taup, taus)]
         self._keep = arrs
         return self.lib.fdo_model(self.h, *[_fptr(a) for a in arrs])
@@ -195,16 +220,20 @@ class Oracle:
             sel[OUT_NAMES.index(n)] = 1
         return sel
 
+    def _in(self, a):
+        """An input array as the build takes it: FP32 values, in its type."""
+        return np.ascontiguousarray(np.asarray(a, np.float32), dtype=self.dtype)
+
     def forward(self, src_pos, src, rec_pos, outputs, mask=None, save_boundaries=False):
-        src_pos = np.ascontiguousarray(src_pos, np.float32).reshape(-1, 5)
-        rec_pos = np.ascontiguousarray(rec_pos, np.float32).reshape(-1, 8)
+        src_pos = self._in(src_pos).reshape(-1, 5)
+        rec_pos = self._in(rec_pos).reshape(-1, 8)
         nt = self.cfg["nt"]
-        src = np.ascontiguousarray(src, np.float32).reshape(src_pos.shape[0], nt)
+        src = self._in(src).reshape(src_pos.shape[0], nt)
         if mask is None:
             mask = source_type_mask(src_pos)
         nrec = rec_pos.shape[0]
-        outs = {n: np.zeros((nrec, nt), np.float32) for n in outputs}
-        ptrs = (C.POINTER(C.c_float) * 10)()
+        outs = {n: np.zeros((nrec, nt), self.dtype) for n in outputs}
+        ptrs = (C.POINTER(self.real) * 10)()
         for n, a in outs.items():
             ptrs[OUT_NAMES.index(n)] = _fptr(a)
         rc = self.lib.fdo_run_forward(self.h, src_pos.shape[0], _fptr(src_pos), _fptr(src), nrec,
@@ -215,14 +244,14 @@ class Oracle:
         return outs
 
     def adjoint(self, src_pos, src, rec_pos, residuals: dict, mask=None):
-        src_pos = np.ascontiguousarray(src_pos, np.float32).reshape(-1, 5)
-        rec_pos = np.ascontiguousarray(rec_pos, np.float32).reshape(-1, 8)
+        src_pos = self._in(src_pos).reshape(-1, 5)
+        rec_pos = self._in(rec_pos).reshape(-1, 8)
         nt = self.cfg["nt"]
-        src = np.ascontiguousarray(src, np.float32).reshape(src_pos.shape[0], nt)
+        src = self._in(src).reshape(src_pos.shape[0], nt)
         if mask is None:
             mask = source_type_mask(src_pos)
-        res = {n: np.ascontiguousarray(r, np.float32).reshape(rec_pos.shape[0], nt) for n, r in residuals.items()}
-        ptrs = (C.POINTER(C.c_float) * 10)()
+        res = {n: np.ascontiguousarray(r, self.dtype).reshape(rec_pos.shape[0], nt) for n, r in residuals.items()}
+        ptrs = (C.POINTER(self.real) * 10)()
         for n, a in res.items():
             ptrs[OUT_NAMES.index(n)] = _fptr(a)
         rc = self.lib.fdo_run_adjoint(self.h, src_pos.shape[0], _fptr(src_pos), _fptr(src), rec_pos.shape[0],
@@ -232,7 +261,7 @@ class Oracle:
 
     def gradients(self):
         n = self.npar
-        g = [np.zeros(n, np.float32) for _ in range(6)]
+        g = [np.zeros(n, self.dtype) for _ in range(6)]
         self.lib.fdo_get_grad(self.h, *[_fptr(a) for a in g])
         sh = self.shape
         return {"vp": g[0].reshape(sh), "vs": g[1].reshape(sh), "rho": g[2].reshape(sh),
@@ -245,8 +274,8 @@ class Oracle:
         """The float accumulators as they are (no transf_grad): M, mu, rho,
         taup, taus.  For the DFT gradient these are already in the
         param_type basis (calc_grad.c applies the chain rule itself)."""
-        g = [np.zeros(self.npar, np.float32) for _ in range(5)]
-        ptrs = (C.POINTER(C.c_float) * 5)(*[_fptr(a) for a in g])
+        g = [np.zeros(self.npar, self.dtype) for _ in range(5)]
+        ptrs = (C.POINTER(self.real) * 5)(*[_fptr(a) for a in g])
         self.lib.fdo_get_grad_raw(self.h, ptrs)
         sh = self.shape
         return {"rho": g[0].reshape(sh), "M": g[1].reshape(sh), "mu": g[2].reshape(sh),
@@ -257,8 +286,8 @@ class Oracle:
         transf_grad applied to the Hessian (src/calc_grad.c:1023-1060, no
         division by dt), keyed by the param_type's names; else the raw
         accumulators M, mu, rho, taup, taus."""
-        g = [np.zeros(self.npar, np.float32) for _ in range(5)]
-        ptrs = (C.POINTER(C.c_float) * 5)(*[_fptr(a) for a in g])
+        g = [np.zeros(self.npar, self.dtype) for _ in range(5)]
+        ptrs = (C.POINTER(self.real) * 5)(*[_fptr(a) for a in g])
         self.lib.fdo_get_hess(self.h, 1 if transform else 0, ptrs)
         sh = self.shape
         if transform:
@@ -272,8 +301,8 @@ class Oracle:
         """DTNYQ, NTNYQ, df and gradfreqsn of a DFT-gradient state
         (src/assign_modeling_case.c:549-570)."""
         ni = (C.c_int * 2)()
-        df = C.c_float(0)
-        fn = np.zeros(16, np.float32)
+        df = self.real(0)
+        fn = np.zeros(16, self.dtype)
         self.lib.fdo_dft_info(self.h, ni, C.byref(df), _fptr(fn))
         nf = len(np.atleast_1d(self.cfg.get("gradfreqs", ())))
         return {"dtnyq": ni[0], "ntnyq": ni[1], "df": df.value, "gradfreqsn": fn[:nf].copy()}
@@ -288,7 +317,7 @@ class Oracle:
             return None
         nf = len(np.atleast_1d(self.cfg.get("gradfreqs", ())))
         n = nf * self.nvol * (self.cfg["L"] if kind == "mem" else 1)
-        return np.ctypeslib.as_array(p, shape=(2 * int(n),)).view(np.complex64)
+        return np.ctypeslib.as_array(p, shape=(2 * int(n),)).view(np.complex128 if self.fp64 else np.complex64)
 
     def calc_grad(self):
         """Assemble the DFT gradient from the transforms now held."""

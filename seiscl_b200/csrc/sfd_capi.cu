@@ -162,6 +162,27 @@ int upload_shot(sfd_plan *p, const sfd_shot *shot, int mask, PointSet &S, PointS
 // bytes per stored wave-field / memory-variable value
 size_t wave_elem(const Grid &g) { return g.fhalf ? 2 : sizeof(float); }
 
+// CPML memory arrays of a grid (0: unused); returns the floats of their
+// 256-byte aligned spans
+int64_t psi_sizes(const Grid &g, int64_t size[NPSI])
+{
+    int64_t nab2 = 2 * (int64_t)g.nab;
+    int64_t sx = nab2 * g.ny * g.nz, sy = (int64_t)g.nx * nab2 * g.nz, sz = (int64_t)g.nx * g.ny * nab2;
+    int64_t sizes[NPSI] = {sx, sx, sx, sy, sy, sy, sz, sz, sz, sx, sx, sx, sy, sy, sy, sz, sz, sz};
+    int64_t tot = 0;
+    for (int i = 0; i < NPSI; i++) {
+        bool used2 = i == PVX_X || i == PVZ_X || i == PVX_Z || i == PVZ_Z || i == PSXX_X || i == PSXZ_X ||
+                     i == PSXZ_Z || i == PSZZ_Z;
+        bool used21 = i == PSXY_X || i == PSYZ_Z || i == PVY_X || i == PVY_Z;
+        bool used22 = i == PVX_X || i == PVZ_Z || i == PSXX_X || i == PSZZ_Z;  // + psi_p_x / psi_p_z
+        bool used = g.abs_type == 1 && g.nab > 0 &&
+                    (g.nd == 3 || (g.nd == 2 && used2) || (g.nd == 21 && used21) || (g.nd == 22 && used22));
+        size[i] = used ? sizes[i] : 0;
+        tot += psi_span(size[i]);
+    }
+    return tot;
+}
+
 int alloc_model(sfd_plan *p)
 {
     const Grid &g = p->g;
@@ -178,20 +199,7 @@ int alloc_model(sfd_plan *p)
         p->f.r[r] = (float *)dalloc(p, wave_elem(g) * g.nvol * g.L, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "memory-variable allocation failed");
     }
-    int64_t nab2 = 2 * (int64_t)g.nab;
-    int64_t sx = nab2 * g.ny * g.nz, sy = (int64_t)g.nx * nab2 * g.nz, sz = (int64_t)g.nx * g.ny * nab2;
-    int64_t sizes[NPSI] = {sx, sx, sx, sy, sy, sy, sz, sz, sz, sx, sx, sx, sy, sy, sy, sz, sz, sz};
-    int64_t tot = 0;
-    for (int i = 0; i < NPSI; i++) {
-        bool used2 = i == PVX_X || i == PVZ_X || i == PVX_Z || i == PVZ_Z || i == PSXX_X || i == PSXZ_X ||
-                     i == PSXZ_Z || i == PSZZ_Z;
-        bool used21 = i == PSXY_X || i == PSYZ_Z || i == PVY_X || i == PVY_Z;
-        bool used22 = i == PVX_X || i == PVZ_Z || i == PSXX_X || i == PSZZ_Z;  // + psi_p_x / psi_p_z
-        bool used = g.abs_type == 1 && g.nab > 0 &&
-                    (g.nd == 3 || (g.nd == 2 && used2) || (g.nd == 21 && used21) || (g.nd == 22 && used22));
-        p->psi_size[i] = used ? sizes[i] : 0;
-        tot += psi_span(p->psi_size[i]);
-    }
+    int64_t tot = psi_sizes(g, p->psi_size);
     p->d_psi_all = tot ? (float *)dalloc(p, sizeof(float) * tot, &e) : nullptr;
     if (tot && e) return fail(p, SFD_ERR_MEMORY, "CPML allocation failed");
     int64_t off = 0;
@@ -562,11 +570,9 @@ int adjoint_dft(sfd_plan *p, const PointSet &R, unsigned omask, cudaStream_t st)
 }  // namespace
 
 // ====================================================================== ABI
-extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
+namespace {
+int check_config(const sfd_config &c)
 {
-    if (!cfg || !out) return SFD_ERR_ARG;
-    *out = nullptr;
-    const sfd_config &c = *cfg;
     if (c.nd != 2 && c.nd != 3 && c.nd != 21 && c.nd != 22) return SFD_ERR_UNSUPPORTED;
     // the reference has no acoustic free surface (assign_modeling_case.c:957-970) and its
     // viscoelastic SH stress kernel does not compile (update_s2D_SH.cl:290)
@@ -590,10 +596,11 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     if (c.hout < 0 || c.hout > 1) return SFD_ERR_ARG;
     // the reference's 3D Hessian kernel does not compile (update_adjv3D.cl:486)
     if (c.hout && c.nd == 3 && c.back_prop_type != 2) return SFD_ERR_UNSUPPORTED;
+    return SFD_OK;
+}
 
-    sfd_plan *p = new sfd_plan();
-    p->cfg = c;
-    Grid &g = p->g;
+void init_grid(const sfd_config &c, Grid &g)
+{
     memset(&g, 0, sizeof g);
     g.nd = c.nd;
     g.F = c.fdorder / 2;
@@ -626,6 +633,20 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     g.fhalf = c.field_precision == 1;
     for (int w = 0; w < NW; w++) g.ws.w[w] = 1.0f;
     g.nbnd = nbnd_cells(g.nd, g.nz, g.ny, g.nx, g.F, g.nab, g.freesurf);
+}
+}  // namespace
+
+extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
+{
+    if (!cfg || !out) return SFD_ERR_ARG;
+    *out = nullptr;
+    const sfd_config &c = *cfg;
+    int rc = check_config(c);
+    if (rc) return rc;
+    sfd_plan *p = new sfd_plan();
+    p->cfg = c;
+    Grid &g = p->g;
+    init_grid(c, g);
     if (p->cfg.tmax <= 0 || p->cfg.tmax > c.nt) p->cfg.tmax = c.nt;
     if (p->cfg.tmin < 0) p->cfg.tmin = 0;
     p->DH_lit = literal9((double)c.dh);
@@ -657,6 +678,51 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     cudaEventCreate(&p->ev0);
     cudaEventCreate(&p->ev1);
     *out = p;
+    return SFD_OK;
+}
+
+extern "C" int sfd_footprint(const sfd_config *cfg, int gradient, int nsrc, int64_t nrec_sel, int nfreqs,
+                             int64_t *bytes)
+{
+    if (!cfg || !bytes || nsrc < 0 || nrec_sel < 0 || nfreqs < 0 || nfreqs > MAXFREQ) return SFD_ERR_ARG;
+    int rc = check_config(*cfg);
+    if (rc) return rc;
+    Grid g;
+    init_grid(*cfg, g);
+    const int64_t nt = cfg->nt, npar = (int64_t)g.nz * g.ny * g.nx;
+    int nwave = 0, nmem = 0;
+    for (int w = 0; w < NW; w++) nwave += is_wave_used(g, w);
+    for (int r = 0; r < NR; r++) nmem += is_mem_used(g, r);
+    // alloc_model: wave fields, memory variables, CPML memory, parameters, constants
+    int64_t psz[NPSI];
+    const int64_t nc = std::max(2 * g.nab, 1);
+    int64_t b = (int64_t)wave_elem(g) * g.nvol * (nwave + (int64_t)nmem * g.L) + 4 * psi_sizes(g, psz) +
+                4 * npar * NPAR + 4 * (3 * NC * nc + nc + 6 * nc);
+    // ensure_shot_buffers: source maps and signatures, receiver maps, seismograms and residuals
+    const int64_t cs = std::max<int64_t>(nsrc, 16), cr = std::max<int64_t>(nrec_sel, 16);
+    b += cs * (8 + 4 + 12 + 4 + 12 + 4 * nt) + cr * (8 + 8 * nt);
+    if (gradient) {
+        const bool bp2 = cfg->back_prop_type == 2;
+        int ng = 0;
+        for (int k = 0; k < NG; k++) ng += !((k == GTAUP || k == GTAUS) && !(bp2 && g.L > 0));
+        b += 8 * npar * (ng + (cfg->hout ? NG : 0)) + 4 * (int64_t)g.nx * g.ny;
+        if (bp2) {
+            b += 2 * 8 * (int64_t)nfreqs * g.nvol * (nwave + (int64_t)nmem * g.L);
+        } else {
+            b += 4 * g.nvol * (nwave + (int64_t)nmem * g.L);
+            b += (int64_t)(cfg->precision == SFD_PREC_FP32 ? 4 : 2) * nt * g.nbnd * nwave;
+        }
+    }
+    *bytes = b;
+    return SFD_OK;
+}
+
+extern "C" int sfd_device_memory(int64_t *free_bytes, int64_t *total_bytes)
+{
+    size_t f = 0, t = 0;
+    if (cudaMemGetInfo(&f, &t) != cudaSuccess) return SFD_ERR_CUDA;
+    if (free_bytes) *free_bytes = (int64_t)f;
+    if (total_bytes) *total_bytes = (int64_t)t;
     return SFD_OK;
 }
 

@@ -73,6 +73,9 @@ EXPORTS = {
     "sfd_host_point_cells": (C.c_int, [C.POINTER(sfd_config), FP, C.c_int, C.c_int, C.POINTER(C.c_int64)]),
     "sfd_host_source_targets": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "sfd_host_cpml": (C.c_int, [C.POINTER(sfd_config), FP]),
+    "sfd_footprint": (C.c_int, [C.POINTER(sfd_config), C.c_int, C.c_int, C.c_int64, C.c_int,
+                                C.POINTER(C.c_int64)]),
+    "sfd_device_memory": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
 }
 
 _LIB = None
@@ -437,3 +440,26 @@ def host_cpml(cfg: Config) -> np.ndarray:
     if rc:
         raise SeisCLEngineError(rc, "cpml failed")
     return out
+
+
+def footprint(cfg: Config, gradient: bool = False, nsrc: int = 1, nrec_sel: int = 0, nfreqs: int = 0) -> int:
+    """Device bytes a plan for ``cfg`` allocates for shots of up to ``nsrc``
+    sources and ``nrec_sel`` receiver traces (receivers x outputs), with a
+    gradient run's buffers when ``gradient`` (no device call)."""
+    lib = load_library()
+    out = C.c_int64(0)
+    rc = lib.sfd_footprint(C.byref(cfg.to_c()), 1 if gradient else 0, int(nsrc), int(nrec_sel), int(nfreqs),
+                           C.byref(out))
+    if rc:
+        raise SeisCLEngineError(rc, "footprint: unsupported configuration")
+    return int(out.value)
+
+
+def device_memory():
+    """(free, total) bytes of the current CUDA device."""
+    lib = load_library()
+    f, t = C.c_int64(0), C.c_int64(0)
+    rc = lib.sfd_device_memory(C.byref(f), C.byref(t))
+    if rc:
+        raise SeisCLEngineError(rc, "cudaMemGetInfo failed")
+    return int(f.value), int(t.value)

@@ -46,7 +46,7 @@ def _requests(n, seed=0):
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
-        nx, nz = int(rng.integers(30, 60)), int(rng.integers(30, 60))
+        nx, nz = int(rng.integers(30, 60)), int(rng.integers(15, 30)) * 2
         cfg = Config(N=[nz, nx], ND=2, NT=50, nab=8)
         m = {"vp": np.full((nx, nz), 3000.0 + 10 * i, np.float32), "vs": np.full((nx, nz), 1700.0, np.float32),
              "rho": np.full((nx, nz), 2000.0, np.float32)}
@@ -63,7 +63,7 @@ def test_server_results_equal_serial_runs(monkeypatch):
 
     monkeypatch.setattr(engine, "Plan", FakePlan)
     reqs = _requests(12)
-    with serving.Server(workers=3, plans_per_worker=2) as srv:
+    with serving.Server(workers=3, plans_per_worker=2, memory_budget=1 << 40) as srv:
         futs = [srv.submit(r) for r in reqs]
         res = [f.result(timeout=60) for f in futs]
     for r, q in zip(res, reqs):
@@ -84,7 +84,7 @@ def test_server_reports_errors_through_futures(monkeypatch):
     monkeypatch.setattr(engine, "Plan", FakePlan)
     bad = _requests(1)[0]
     bad.kind = "nonsense"
-    with serving.Server(workers=1) as srv:
+    with serving.Server(workers=1, memory_budget=1 << 40) as srv:
         f = srv.submit(bad)
         with pytest.raises(ValueError):
             f.result(timeout=60)
@@ -92,6 +92,123 @@ def test_server_reports_errors_through_futures(monkeypatch):
         assert ok.rid == 1
     with pytest.raises(RuntimeError):
         srv.submit(bad)
+
+
+class CountingPlan(FakePlan):
+    """FakePlan that records how many plans are alive and holds the GPU for
+    a while, so that requests overlap."""
+    alive = 0
+    peak = 0
+    lock = None
+
+    def __init__(self, cfg):
+        super().__init__(cfg)
+        with CountingPlan.lock:
+            CountingPlan.alive += 1
+            CountingPlan.peak = max(CountingPlan.peak, CountingPlan.alive)
+
+    def close(self):
+        with CountingPlan.lock:
+            CountingPlan.alive -= 1
+
+    def forward(self, *a, **k):
+        import time
+
+        time.sleep(0.01)
+        return super().forward(*a, **k)
+
+
+def _fake_footprint(req):
+    """Bytes proportional to the grid (any positive measure will do)."""
+    return int(np.prod(req.config.N)) * (3 if req.kind == "gradient" else 1)
+
+
+def test_admission_keeps_held_memory_within_budget(monkeypatch):
+    """Every admitted plan counts at its footprint; with a budget of about
+    two requests, never more than the budget is held, idle plans are evicted
+    to admit new configurations, and results are unchanged."""
+    import threading
+
+    from seiscl_b200 import engine, serving
+
+    CountingPlan.alive = CountingPlan.peak = 0
+    CountingPlan.lock = threading.Lock()
+    monkeypatch.setattr(engine, "Plan", CountingPlan)
+    reqs = _requests(16, seed=3)
+    sizes = [_fake_footprint(q) for q in reqs]
+    budget = 2 * max(sizes)
+    with serving.Server(workers=4, plans_per_worker=2, memory_budget=budget, footprint=_fake_footprint) as srv:
+        res = [f.result(timeout=60) for f in [srv.submit(q) for q in reqs]]
+        st = srv.stats()
+    assert st["peak_bytes"] <= budget and st["admitted"] == len(reqs) and st["rejected"] == 0
+    assert st["evicted"] > 0
+    assert CountingPlan.alive == 0           # every plan closed at the end
+    for r, q in zip(res, reqs):
+        ref = serving.serve(FakePlan(q.config), q)
+        for a, b in zip(r.seismograms, ref.seismograms):
+            for k in a:
+                assert np.array_equal(a[k], b[k])
+
+
+def test_admission_rejects_requests_larger_than_the_budget(monkeypatch):
+    from seiscl_b200 import engine, serving
+
+    monkeypatch.setattr(engine, "Plan", FakePlan)
+    reqs = _requests(4, seed=4)
+    big = max(reqs, key=_fake_footprint)
+    budget = _fake_footprint(big) - 1
+    with serving.Server(workers=2, memory_budget=budget, footprint=_fake_footprint) as srv:
+        futs = [srv.submit(q) for q in reqs]
+        for q, f in zip(reqs, futs):
+            if q is big:
+                with pytest.raises(MemoryError):
+                    f.result(timeout=60)
+            else:
+                assert f.result(timeout=60).rid == q.rid
+        assert srv.stats()["rejected"] == 1
+
+
+def test_footprint_grows_with_grid_and_gradient_buffers():
+    from seiscl_b200 import engine
+
+    c2 = engine.Config(N=[200, 300], ND=2, NT=1000, nab=16)
+    f2 = engine.footprint(c2, False, 1, 200)
+    g2 = engine.footprint(c2, True, 1, 200)
+    # wave fields, parameters and seismograms alone: 5 + 14 arrays of the grid
+    assert f2 >= 4 * (5 * 208 * 308 + 14 * 200 * 300) + 4 * 2 * 200 * 1000
+    assert g2 > f2
+    c3 = engine.Config(N=[64, 64, 64], ND=3, NT=500, L=2, FL=[5.0, 40.0], nab=10)
+    f3 = engine.footprint(c3, False, 1, 100)
+    assert f3 > engine.footprint(engine.Config(N=[64, 64, 64], ND=3, NT=500, nab=10), False, 1, 100)
+    import dataclasses
+    h3 = engine.footprint(dataclasses.replace(c3, precision="fp16"), True, 1, 100)
+    assert engine.footprint(c3, True, 1, 100) > h3 > f3
+
+
+@pytest.mark.gpu
+def test_footprint_matches_device_allocation(cuda_device):
+    """The footprint estimate against cudaMemGetInfo around a plan's runs."""
+    from seiscl_b200 import engine
+    from seiscl_b200.engine import Plan
+
+    for kw in (dict(nd=2, nz=200, nx=300, nt=400, nab=16), dict(nd=3, nz=64, ny=60, nx=68, nt=200, nab=10, L=2)):
+        cfg, model, acq = make_case(**kw)
+        ec = engine_config(cfg)
+        nrec = len(acq["rec_pos"])
+        for grad in (False, True):
+            free0, _ = engine.device_memory()
+            plan = Plan(ec)
+            plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+            d = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], ["vx", "vz"], save_boundaries=grad)
+            if grad:
+                plan.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], d)
+            free1, _ = engine.device_memory()
+            plan.close()
+            used = free0 - free1
+            est = engine.footprint(ec, grad, 1, nrec * 2)
+            # allocation granularity (2 MiB pages per cudaMalloc) and CUDA graphs
+            # add to what the arrays need
+            assert est <= used + (8 << 20) and used <= 1.5 * est + (64 << 20), (kw, grad, est, used)
 
 
 @pytest.mark.gpu
