@@ -481,15 +481,16 @@ def serving_requests(nreq, seed=501):
 
 def _serve_stream(reqs, arrivals, workers, plain):
     """Submit the requests at their arrival times; returns (results, wall s,
-    admission stats).  plain: one worker, time loops launched step by step
-    (no CUDA graphs), i.e. the shots one after another with plain launches."""
+    admission stats).  plain: one worker, no batching, time loops launched
+    step by step (no CUDA graphs), i.e. the shots one after another with
+    plain launches."""
     import dataclasses
 
     from seiscl_b200 import serving
 
     if plain:
         reqs = [dataclasses.replace(q, config=dataclasses.replace(q.config, loop_graphs="never")) for q in reqs]
-    with serving.Server(workers=1 if plain else workers) as srv:
+    with serving.Server(workers=1 if plain else workers, max_batch=1 if plain else 8) as srv:
         futs = []
         t0 = time.perf_counter()
         for a, q in zip(arrivals, reqs):
@@ -528,7 +529,7 @@ def run_serving(args):
         pp = serving.percentiles([r.latency for r in pres])
         plain = {"shots_per_s": round(nshots / pwall, 3), "wall_s": round(pwall, 2),
                  "latency_s": {k: round(v, 3) for k, v in pp.items()},
-                 "what": "same request stream, one request at a time, step-by-step launches (no CUDA graphs)"}
+                 "what": "same request stream, one request and one shot at a time, step-by-step launches (no CUDA graphs)"}
     cells = 0.0
     for q in reqs:
         n = float(np.prod(q.config.N))

@@ -101,15 +101,22 @@ typedef struct sfd_config {
                               by powers of two (src/assign_modeling_case.c:829-866). */
     int back_prop_type;    /* BACK_PROP_TYPE: 0 or 1 boundary-saving backpropagation,
                               2 DFT gradient at the frequencies of sfd_set_gradfreqs */
-    int loop_graphs;       /* time loops as CUDA graphs: 0 for 2D grids (whose steps are a
-                              few microseconds of work, so launches dominate), 1 always,
+    int loop_graphs;       /* time loops as CUDA graphs: 0 for 2D grids and 3D grids of up
+                              to 2^22 padded cells (~160^3), whose steps are microseconds
+                              of work so that launches dominate, 1 always,
                               2 never.  A graph is captured on the first shot of a shape
                               and replayed while nothing its launches depend on changes.
                               No reference counterpart (launch mechanics). */
     int hout;              /* HOUT: also accumulate the approximate Hessian (2D; the
                               reference's 3D Hessian kernel does not compile,
                               update_adjv3D.cl:486, so 3D boundary-saving plans reject it) */
-    int reserved[1];
+    int batch;             /* shots one launch advances together (2D P-SV and acoustic;
+                              0 or 1: one).  The plan holds `batch` copies of every
+                              per-shot array; sfd_forward_batch / sfd_adjoint_batch run
+                              up to that many shots of the same model at once, each
+                              launch covering all of them.  No reference counterpart
+                              (the reference runs the shots of a group one by one,
+                              time_stepping.c:705-722). */
 } sfd_config;
 
 typedef struct sfd_shot {
@@ -136,6 +143,8 @@ const char *sfd_last_error(const sfd_plan *plan);
  * call), for admission control by a caller that shares one device among
  * many plans.  No counterpart in the reference. */
 int sfd_footprint(const sfd_config *cfg, int gradient, int nsrc, int64_t nrec_sel, int nfreqs, int64_t *bytes);
+/* Device bytes the plan holds now (every allocation it made and keeps). */
+int64_t sfd_plan_device_bytes(const sfd_plan *plan);
 /* Free and total memory of the current device (cudaMemGetInfo). */
 int sfd_device_memory(int64_t *free_bytes, int64_t *total_bytes);
 
@@ -220,6 +229,19 @@ int sfd_get_gradient_q(sfd_plan *plan, float *gtaup, float *gtaus);
 /* res_scale (residuals.c:452-568): scale residuals in place into adjoint
  * sources.  res[k] are [nrec][NT] host arrays for the selected outputs. */
 int sfd_residual_scale(sfd_plan *plan, const sfd_shot *shot, const int *outsel, float *const *res);
+
+/* Batched shots (cfg.batch > 1, 2D P-SV and acoustic): nshot <= batch shots
+ * of the plan's model advance together, each launch of the time loop
+ * covering all of them.  Shot s works on copy s of every per-shot array, so
+ * each shot's result is the one sfd_forward gives it alone.  seis[o] (and
+ * residuals[o]) hold the traces of all shots in shot order, [sum nrec][NT];
+ * the adjoint must follow a forward of the same shots.  The gradient
+ * accumulates per shot copy and sfd_get_gradient returns the sum over
+ * copies (in copy order).  sfd_forward / sfd_adjoint are the one-shot case. */
+int sfd_forward_batch(sfd_plan *plan, int nshot, const sfd_shot *shots, int mask, const int *outsel,
+                      float *const *seis, int save_boundaries, void *stream);
+int sfd_adjoint_batch(sfd_plan *plan, int nshot, const sfd_shot *shots, int mask, const int *outsel,
+                      const float *const *residuals, void *stream);
 
 /* ---- forward modelling without allocation ----
  *

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -32,12 +33,50 @@ int fail(sfd_plan *p, int code, const std::string &msg)
                         std::string(#call) + ": " + cudaGetErrorString(e_));                           \
     } while (0)
 
-void *dalloc(sfd_plan *p, size_t bytes, cudaError_t *err)
+// Device memory comes from the device's stream-ordered pool, ordered on the
+// plan's stream: unlike cudaMalloc / cudaFree, allocating and freeing does
+// not synchronize the device, so plans created and destroyed while others
+// run (a serving process) leave the running ones alone.  The pool keeps
+// freed memory for reuse (release threshold: unlimited).
+void pool_setup(int dev)
+{
+    static std::atomic<uint64_t> done{0};
+    if (dev < 0 || dev >= 64 || (done.load() >> dev) & 1) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    done.fetch_or(uint64_t(1) << dev);
+}
+
+// allocation owned by the caller (freed with dfree); tracked in dev_bytes
+void *dalloc_raw(sfd_plan *p, size_t bytes, cudaError_t *err)
 {
     void *ptr = nullptr;
-    *err = cudaMalloc(&ptr, bytes ? bytes : 16);
-    if (*err != cudaSuccess) return nullptr;
-    p->allocs.push_back(ptr);
+    pool_setup(p->device);
+    *err = cudaMallocAsync(&ptr, bytes ? bytes : 16, p->stream);
+    if (*err == cudaSuccess) *err = cudaStreamSynchronize(p->stream);   // usable from any stream
+    if (*err != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    p->dev_bytes += bytes;
+    return ptr;
+}
+
+void dfree(sfd_plan *p, void *ptr, size_t bytes)
+{
+    if (!ptr) return;
+    cudaFreeAsync(ptr, p->stream);
+    p->dev_bytes -= bytes;
+}
+
+// allocation owned by the plan (freed with it)
+void *dalloc(sfd_plan *p, size_t bytes, cudaError_t *err)
+{
+    void *ptr = dalloc_raw(p, bytes, err);
+    if (ptr) p->allocs.push_back({ptr, bytes});
     return ptr;
 }
 
@@ -111,34 +150,44 @@ oom:
 }
 
 // host-side mapping of a shot's sources and receivers, uploaded to the device
-int upload_shot(sfd_plan *p, const sfd_shot *shot, int mask, PointSet &S, PointSet &R, cudaStream_t st)
+int upload_shots(sfd_plan *p, int nshot, const sfd_shot *shots, int mask, PointSet &S, PointSet &R,
+                 cudaStream_t st)
 {
     const Grid &g = p->g;
-    int nsrc = shot->nsrc, nrec = shot->nrec, F = g.F;
+    const int F = g.F, NT = p->cfg.nt;
+    int nsrc = 0, nrec = 0;
+    for (int b = 0; b < nshot; b++) { nsrc += shots[b].nsrc; nrec += shots[b].nrec; }
     std::vector<int64_t> scell(nsrc), rcell(nrec);
     std::vector<int> snt(nsrc), sfield(3 * nsrc), skz(nsrc);
-    std::vector<float> sdiv(3 * nsrc);
-    for (int s = 0; s < nsrc; s++) {
-        int i, j, k;
-        point_cell(shot->src_pos + 5 * s, p->DH_lit, F, i, j, k);
-        if (g.nd != 3) j = 0;  // 2D kernels index [(i)*NZ+k] (automatic_kernels.c:536-543)
-        // sources outside [F, NX-F-1] along x are dropped (automatic_kernels.c:506-511)
-        if (i < F || i > g.NX - F - 1) { scell[s] = -1; snt[s] = 0; continue; }
-        if (j < 0 || j >= g.NY || k < 0 || k >= g.NZ)
-            return fail(p, SFD_ERR_ARG, "source position outside the padded grid");
-        scell[s] = ((int64_t)i * g.NY + j) * g.NZ + k;
-        skz[s] = k;
-        int type = (int)shot->src_pos[5 * s + 4];
-        snt[s] = source_targets(g.nd, mask, type, &sfield[3 * s], &sdiv[3 * s]);
-    }
-    for (int r = 0; r < nrec; r++) {
-        int i, j, k;
-        point_cell(shot->rec_pos + 8 * r, p->DH_lit, F, i, j, k);
-        if (g.nd != 3) j = 0;
-        if (i < F || i > g.NX - F - 1) { rcell[r] = -1; continue; }
-        if (j < 0 || j >= g.NY || k < 0 || k >= g.NZ)
-            return fail(p, SFD_ERR_ARG, "receiver position outside the padded grid");
-        rcell[r] = ((int64_t)i * g.NY + j) * g.NZ + k;
+    std::vector<float> sdiv(3 * nsrc), ssig((size_t)nsrc * NT);
+    int s = 0, r = 0;
+    for (int b = 0; b < nshot; b++) {
+        const sfd_shot *shot = &shots[b];
+        // shot b's points address copy b of the wave fields
+        const int64_t base = (int64_t)b * g.nvol;
+        for (int q = 0; q < shot->nsrc; q++, s++) {
+            int i, j, k;
+            point_cell(shot->src_pos + 5 * q, p->DH_lit, F, i, j, k);
+            if (g.nd != 3) j = 0;  // 2D kernels index [(i)*NZ+k] (automatic_kernels.c:536-543)
+            std::memcpy(&ssig[(size_t)s * NT], shot->src + (size_t)q * NT, sizeof(float) * NT);
+            // sources outside [F, NX-F-1] along x are dropped (automatic_kernels.c:506-511)
+            if (i < F || i > g.NX - F - 1) { scell[s] = -1; snt[s] = 0; continue; }
+            if (j < 0 || j >= g.NY || k < 0 || k >= g.NZ)
+                return fail(p, SFD_ERR_ARG, "source position outside the padded grid");
+            scell[s] = base + ((int64_t)i * g.NY + j) * g.NZ + k;
+            skz[s] = k;
+            int type = (int)shot->src_pos[5 * q + 4];
+            snt[s] = source_targets(g.nd, mask, type, &sfield[3 * s], &sdiv[3 * s]);
+        }
+        for (int q = 0; q < shot->nrec; q++, r++) {
+            int i, j, k;
+            point_cell(shot->rec_pos + 8 * q, p->DH_lit, F, i, j, k);
+            if (g.nd != 3) j = 0;
+            if (i < F || i > g.NX - F - 1) { rcell[r] = -1; continue; }
+            if (j < 0 || j >= g.NY || k < 0 || k >= g.NZ)
+                return fail(p, SFD_ERR_ARG, "receiver position outside the padded grid");
+            rcell[r] = base + ((int64_t)i * g.NY + j) * g.NZ + k;
+        }
     }
     {
         if (nsrc) {
@@ -147,8 +196,7 @@ int upload_shot(sfd_plan *p, const sfd_shot *shot, int mask, PointSet &S, PointS
             CKC(cudaMemcpyAsync(p->d_src_kz, skz.data(), sizeof(int) * nsrc, cudaMemcpyHostToDevice, st));
             CKC(cudaMemcpyAsync(p->d_src_field, sfield.data(), sizeof(int) * 3 * nsrc, cudaMemcpyHostToDevice, st));
             CKC(cudaMemcpyAsync(p->d_src_div, sdiv.data(), sizeof(float) * 3 * nsrc, cudaMemcpyHostToDevice, st));
-            CKC(cudaMemcpyAsync(p->d_src, shot->src, sizeof(float) * (size_t)nsrc * p->cfg.nt,
-                                cudaMemcpyHostToDevice, st));
+            CKC(cudaMemcpyAsync(p->d_src, ssig.data(), sizeof(float) * ssig.size(), cudaMemcpyHostToDevice, st));
         }
         if (nrec) CKC(cudaMemcpyAsync(p->d_rec_cell, rcell.data(), sizeof(int64_t) * nrec, cudaMemcpyHostToDevice, st));
         // pageable sources: wait so the host vectors may go out of scope
@@ -157,6 +205,11 @@ int upload_shot(sfd_plan *p, const sfd_shot *shot, int mask, PointSet &S, PointS
     S = PointSet{nsrc, p->d_src_cell, p->d_src_nt, p->d_src_field, p->d_src_div, p->d_src_kz};
     R = PointSet{nrec, p->d_rec_cell, nullptr, nullptr, nullptr, nullptr};
     return SFD_OK;
+}
+
+int upload_shot(sfd_plan *p, const sfd_shot *shot, int mask, PointSet &S, PointSet &R, cudaStream_t st)
+{
+    return upload_shots(p, 1, shot, mask, S, R, st);
 }
 
 // bytes per stored wave-field / memory-variable value
@@ -190,17 +243,17 @@ int alloc_model(sfd_plan *p)
     for (int w = 0; w < NW; w++) {
         p->f.w[w] = nullptr;
         if (!is_wave_used(g, w)) continue;
-        p->f.w[w] = (float *)dalloc(p, wave_elem(g) * g.nvol, &e);
+        p->f.w[w] = (float *)dalloc(p, wave_elem(g) * g.nvol * p->batch, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "wave field allocation failed");
     }
     for (int r = 0; r < NR; r++) {
         p->f.r[r] = nullptr;
         if (!is_mem_used(g, r)) continue;
-        p->f.r[r] = (float *)dalloc(p, wave_elem(g) * g.nvol * g.L, &e);
+        p->f.r[r] = (float *)dalloc(p, wave_elem(g) * g.nvol * g.L * p->batch, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "memory-variable allocation failed");
     }
     int64_t tot = psi_sizes(g, p->psi_size);
-    p->d_psi_all = tot ? (float *)dalloc(p, sizeof(float) * tot, &e) : nullptr;
+    p->d_psi_all = tot ? (float *)dalloc(p, sizeof(float) * tot * p->batch, &e) : nullptr;
     if (tot && e) return fail(p, SFD_ERR_MEMORY, "CPML allocation failed");
     int64_t off = 0;
     for (int i = 0; i < NPSI; i++) {
@@ -255,13 +308,14 @@ int upload_constants(sfd_plan *p)
 int zero_forward_state(sfd_plan *p, cudaStream_t st)
 {
     const Grid &g = p->g;
+    const size_t nb = (size_t)g.nb;   // the shots of this run
     for (int w = 0; w < NW; w++)
-        if (p->f.w[w]) CKC(cudaMemsetAsync(p->f.w[w], 0, wave_elem(g) * g.nvol, st));
+        if (p->f.w[w]) CKC(cudaMemsetAsync(p->f.w[w], 0, wave_elem(g) * g.nvol * nb, st));
     for (int r = 0; r < NR; r++)
-        if (p->f.r[r]) CKC(cudaMemsetAsync(p->f.r[r], 0, wave_elem(g) * g.nvol * g.L, st));
+        if (p->f.r[r]) CKC(cudaMemsetAsync(p->f.r[r], 0, wave_elem(g) * g.nvol * g.L * nb, st));
     int64_t tot = 0;
     for (int i = 0; i < NPSI; i++) tot += psi_span(p->psi_size[i]);
-    if (tot) CKC(cudaMemsetAsync(p->d_psi_all, 0, sizeof(float) * tot, st));
+    if (tot) CKC(cudaMemsetAsync(p->d_psi_all, 0, sizeof(float) * tot * nb, st));
     return SFD_OK;
 }
 
@@ -275,32 +329,32 @@ int alloc_adjoint(sfd_plan *p)
     for (int w = 0; w < NW; w++) {
         p->a.wr[w] = nullptr;
         if (bp2 || !is_wave_used(g, w)) continue;
-        p->a.wr[w] = (float *)dalloc(p, sizeof(float) * g.nvol, &e);
+        p->a.wr[w] = (float *)dalloc(p, sizeof(float) * g.nvol * p->batch, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "adjoint field allocation failed");
     }
     for (int r = 0; r < NR; r++) {
         p->a.rr[r] = nullptr;
         if (bp2 || !is_mem_used(g, r)) continue;
-        p->a.rr[r] = (float *)dalloc(p, sizeof(float) * g.nvol * g.L, &e);
+        p->a.rr[r] = (float *)dalloc(p, sizeof(float) * g.nvol * g.L * p->batch, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "adjoint memory-variable allocation failed");
     }
     int64_t npar = (int64_t)g.nz * g.ny * g.nx;
     for (int k = 0; k < NG; k++) {
         p->a.hess[k] = nullptr;
         if (!g.hout) continue;
-        p->a.hess[k] = (double *)dalloc(p, sizeof(double) * npar, &e);
+        p->a.hess[k] = (double *)dalloc(p, sizeof(double) * npar * p->batch, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "Hessian allocation failed");
-        CKC(cudaMemset(p->a.hess[k], 0, sizeof(double) * npar));
+        CKC(cudaMemsetAsync(p->a.hess[k], 0, sizeof(double) * npar * p->batch, p->stream));
     }
     for (int k = 0; k < NG; k++) {
         p->a.grad[k] = nullptr;
         if ((k == GTAUP || k == GTAUS) && !(bp2 && g.L > 0)) continue;
-        p->a.grad[k] = (double *)dalloc(p, sizeof(double) * npar, &e);
+        p->a.grad[k] = (double *)dalloc(p, sizeof(double) * npar * p->batch, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "gradient allocation failed");
-        CKC(cudaMemset(p->a.grad[k], 0, sizeof(double) * npar));
+        CKC(cudaMemsetAsync(p->a.grad[k], 0, sizeof(double) * npar * p->batch, p->stream));
     }
     int64_t nq = (int64_t)g.nx * g.ny;
-    p->d_surf_q = (float *)dalloc(p, sizeof(float) * nq, &e);
+    p->d_surf_q = (float *)dalloc(p, sizeof(float) * nq * p->batch, &e);
     if (e) return fail(p, SFD_ERR_MEMORY, "scratch allocation failed");
     return SFD_OK;
 }
@@ -338,16 +392,16 @@ int movie_setup(sfd_plan *p, unsigned omask, Movie &mv)
     if (!mv.n || !mv.nslot) { mv.n = 0; return SFD_OK; }
     size_t need = (size_t)mv.n * mv.nslot * mv.ncell;
     if (need > p->mov_cap) {
-        if (p->d_mov) cudaFree(p->d_mov);
+        dfree(p, p->d_mov, sizeof(float) * p->mov_cap);
         p->d_mov = nullptr;
         p->mov_cap = 0;
-        if (cudaMalloc(&p->d_mov, sizeof(float) * need) != cudaSuccess) {
-            p->d_mov = nullptr;
-            return fail(p, SFD_ERR_MEMORY, "movie buffer does not fit in device memory");
-        }
+        cudaError_t e;
+        p->d_mov = (float *)dalloc_raw(p, sizeof(float) * need, &e);
+        if (!p->d_mov) return fail(p, SFD_ERR_MEMORY, "movie buffer does not fit in device memory");
         p->mov_cap = need;
     }
-    CKC(cudaMemset(p->d_mov, 0, sizeof(float) * need));
+    CKC(cudaMemsetAsync(p->d_mov, 0, sizeof(float) * need, p->stream));
+    CKC(cudaStreamSynchronize(p->stream));
     return SFD_OK;
 }
 
@@ -384,7 +438,7 @@ bool graphs_on(const sfd_plan *p)
     const int m = p->cfg.loop_graphs;
     if (m == 2) return false;
     if (m == 1) return p->g.kernels != 3;   // the TMA path sets kernel attributes on first use
-    return p->g.nd != 3;
+    return p->g.nd != 3 || (p->g.nvol <= ((int64_t)1 << 22) && p->g.kernels != 3 && p->g.kernels != 2);
 }
 
 void drop_graph(sfd_plan::LoopGraph &lg)
@@ -405,6 +459,13 @@ int run_loop(sfd_plan *p, sfd_plan::LoopGraph &lg, const std::string &key, cudaS
     }
     if (!lg.exec || lg.key != key) {
         drop_graph(lg);
+        // auto mode captures a loop the second time it runs unchanged: a plan
+        // that runs one shot of a shape would only pay for the capture
+        if (p->cfg.loop_graphs == 0 && lg.seen != key) {
+            lg.seen = key;
+            body(st);
+            return SFD_OK;
+        }
         cudaGraph_t graph = nullptr;
         if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
             body(st);
@@ -429,13 +490,14 @@ constexpr double PI_D = 3.141592653589793238462643383279502884197169;
 
 void free_dft(sfd_plan *p)
 {
+    const size_t nf = (size_t)p->dft_nf;
     for (int s = 0; s < 2; s++) {
         for (int w = 0; w < NW; w++) {
-            if (p->d_fw[s][w]) cudaFree(p->d_fw[s][w]);
+            dfree(p, p->d_fw[s][w], sizeof(float2) * nf * p->g.nvol);
             p->d_fw[s][w] = nullptr;
         }
         for (int r = 0; r < NR; r++) {
-            if (p->d_fr[s][r]) cudaFree(p->d_fr[s][r]);
+            dfree(p, p->d_fr[s][r], sizeof(float2) * nf * p->g.nvol * p->g.L);
             p->d_fr[s][r] = nullptr;
         }
     }
@@ -450,25 +512,26 @@ int alloc_dft(sfd_plan *p)
     if (p->dft_nf == p->nfreqs) return SFD_OK;
     free_dft(p);
     const size_t nf = (size_t)p->nfreqs;
+    p->dft_nf = p->nfreqs;   // the size free_dft releases
+    cudaError_t e;
     for (int s = 0; s < 2; s++) {
         for (int w = 0; w < NW; w++) {
             if (!is_wave_used(g, w)) continue;
-            if (cudaMalloc(&p->d_fw[s][w], sizeof(float2) * nf * g.nvol) != cudaSuccess) {
-                p->d_fw[s][w] = nullptr;
+            p->d_fw[s][w] = (float2 *)dalloc_raw(p, sizeof(float2) * nf * g.nvol, &e);
+            if (!p->d_fw[s][w]) {
                 free_dft(p);
                 return fail(p, SFD_ERR_MEMORY, "DFT gradient buffers do not fit in device memory");
             }
         }
         for (int r = 0; r < NR; r++) {
             if (!is_mem_used(g, r)) continue;
-            if (cudaMalloc(&p->d_fr[s][r], sizeof(float2) * nf * g.nvol * g.L) != cudaSuccess) {
-                p->d_fr[s][r] = nullptr;
+            p->d_fr[s][r] = (float2 *)dalloc_raw(p, sizeof(float2) * nf * g.nvol * g.L, &e);
+            if (!p->d_fr[s][r]) {
                 free_dft(p);
                 return fail(p, SFD_ERR_MEMORY, "DFT gradient buffers do not fit in device memory");
             }
         }
     }
-    p->dft_nf = p->nfreqs;
     return SFD_OK;
 }
 
@@ -596,6 +659,9 @@ int check_config(const sfd_config &c)
     if (c.hout < 0 || c.hout > 1) return SFD_ERR_ARG;
     // the reference's 3D Hessian kernel does not compile (update_adjv3D.cl:486)
     if (c.hout && c.nd == 3 && c.back_prop_type != 2) return SFD_ERR_UNSUPPORTED;
+    if (c.batch < 0 || c.batch > 64) return SFD_ERR_ARG;
+    // batched shots: the 2D P-SV and acoustic kernels, boundary-saving gradients
+    if (c.batch > 1 && ((c.nd != 2 && c.nd != 22) || c.back_prop_type == 2)) return SFD_ERR_UNSUPPORTED;
     return SFD_OK;
 }
 
@@ -631,8 +697,16 @@ void init_grid(const sfd_config &c, Grid &g)
     }
     g.inv_dt = 1.0f / c.dt;
     g.fhalf = c.field_precision == 1;
-    for (int w = 0; w < NW; w++) g.ws.w[w] = 1.0f;
+    for (int w = 0; w < NW; w++) g.ws.w[w] = g.bsc[w] = g.bsci[w] = 1.0f;
     g.nbnd = nbnd_cells(g.nd, g.nz, g.ny, g.nx, g.F, g.nab, g.freesurf);
+    g.nb = 1;
+    g.sb_w = g.nvol;
+    g.sb_r = g.nvol * g.L;
+    int64_t psz[NPSI];
+    g.sb_psi = psi_sizes(g, psz);
+    g.sb_g = (int64_t)g.nz * g.ny * g.nx;
+    g.sb_q = (int64_t)g.nx * g.ny;
+    g.sb_bnd = (int64_t)(c.precision == SFD_PREC_FP32 ? 4 : 2) * c.nt * g.nbnd;
 }
 }  // namespace
 
@@ -659,10 +733,13 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     p->cap_src = p->cap_rec = 0;
     p->d_surf_q = nullptr;
     p->d_ticket = nullptr;
+    p->dev_bytes = 0;
+    p->batch = std::max(1, c.batch);
+    p->fwd_nb = 0;
     memset(&p->f, 0, sizeof p->f);
     memset(&p->a, 0, sizeof p->a);
     p->last_ms = 0.0f;
-    p->kshift = 0;
+    p->kshift = p->bshift = 0;
     p->nfreqs = p->dtnyq = p->ntnyq = p->dft_nf = 0;
     p->df = 0.0f;
     memset(p->d_fw, 0, sizeof p->d_fw);
@@ -696,25 +773,32 @@ extern "C" int sfd_footprint(const sfd_config *cfg, int gradient, int nsrc, int6
     // alloc_model: wave fields, memory variables, CPML memory, parameters, constants
     int64_t psz[NPSI];
     const int64_t nc = std::max(2 * g.nab, 1);
-    int64_t b = (int64_t)wave_elem(g) * g.nvol * (nwave + (int64_t)nmem * g.L) + 4 * psi_sizes(g, psz) +
+    const int64_t B = std::max(1, cfg->batch);   // copies of the per-shot arrays
+    int64_t b = B * ((int64_t)wave_elem(g) * g.nvol * (nwave + (int64_t)nmem * g.L) + 4 * psi_sizes(g, psz)) +
                 4 * npar * NPAR + 4 * (3 * NC * nc + nc + 6 * nc);
     // ensure_shot_buffers: source maps and signatures, receiver maps, seismograms and residuals
     const int64_t cs = std::max<int64_t>(nsrc, 16), cr = std::max<int64_t>(nrec_sel, 16);
     b += cs * (8 + 4 + 12 + 4 + 12 + 4 * nt) + cr * (8 + 8 * nt);
+    if (!gradient && (g.nd == 2 || g.nd == 22)) b += sizeof(int);   // fused-step block counter
     if (gradient) {
         const bool bp2 = cfg->back_prop_type == 2;
         int ng = 0;
         for (int k = 0; k < NG; k++) ng += !((k == GTAUP || k == GTAUS) && !(bp2 && g.L > 0));
-        b += 8 * npar * (ng + (cfg->hout ? NG : 0)) + 4 * (int64_t)g.nx * g.ny;
+        b += B * (8 * npar * (ng + (cfg->hout ? NG : 0)) + 4 * (int64_t)g.nx * g.ny);
         if (bp2) {
             b += 2 * 8 * (int64_t)nfreqs * g.nvol * (nwave + (int64_t)nmem * g.L);
         } else {
-            b += 4 * g.nvol * (nwave + (int64_t)nmem * g.L);
-            b += (int64_t)(cfg->precision == SFD_PREC_FP32 ? 4 : 2) * nt * g.nbnd * nwave;
+            b += B * 4 * g.nvol * (nwave + (int64_t)nmem * g.L);
+            b += B * (int64_t)(cfg->precision == SFD_PREC_FP32 ? 4 : 2) * nt * g.nbnd * nwave;
         }
     }
     *bytes = b;
     return SFD_OK;
+}
+
+extern "C" int64_t sfd_plan_device_bytes(const sfd_plan *p)
+{
+    return p ? p->dev_bytes : SFD_ERR_ARG;
 }
 
 extern "C" int sfd_device_memory(int64_t *free_bytes, int64_t *total_bytes)
@@ -730,13 +814,13 @@ extern "C" void sfd_plan_destroy(sfd_plan *p)
 {
     if (!p) return;
     cudaStreamSynchronize(p->stream);
-    for (void *ptr : p->allocs) cudaFree(ptr);
-    for (int w = 0; w < NW; w++)
-        if (p->d_bnd[w]) cudaFree(p->d_bnd[w]);
-    free_dft(p);
-    if (p->d_mov) cudaFree(p->d_mov);
     drop_graph(p->gfwd);
     drop_graph(p->gadj);
+    for (auto &a : p->allocs) dfree(p, a.first, a.second);
+    for (int w = 0; w < NW; w++) dfree(p, p->d_bnd[w], p->bnd_elem * (size_t)p->cfg.nt * p->g.nbnd * p->batch);
+    free_dft(p);
+    dfree(p, p->d_mov, sizeof(float) * p->mov_cap);
+    cudaStreamSynchronize(p->stream);
     cudaEventDestroy(p->ev0);
     cudaEventDestroy(p->ev1);
     if (p->own_stream) cudaStreamDestroy(p->stream);
@@ -755,18 +839,21 @@ extern "C" int sfd_set_model(sfd_plan *p, const float *const *params)
         if ((rc = upload_constants(p))) return rc;
     }
     int64_t npar = (int64_t)p->g.nz * p->g.ny * p->g.nx;
-    if (p->g.fhalf) {
-        // FP16 storage keeps velocities as v * 2^b and stresses as s * 2^a with
-        // b - a = kshift ~ log2 of the impedance, so both stay near the same
-        // magnitude; the moduli carry 2^-kshift and the buoyancies 2^kshift
-        // (exact power-of-two scalings of the FP32 parameters).
+    // FP16 stores keep velocities as v * 2^b and stresses as s * 2^a with
+    // b - a ~ log2 of the impedance, so both stay near the same magnitude
+    {
         double acc = 0.0;
         int64_t n = 0, step = std::max<int64_t>(1, npar / 4096);
         for (int64_t i = 0; i < npar; i += step) {
             const double z = std::sqrt((double)p->hp[PM][i] / (double)p->hp[PRIP][i]);
             if (z > 0 && std::isfinite(z)) { acc += std::log2(z); n++; }
         }
-        p->kshift = n ? (int)std::lround(acc / n) : 0;
+        p->bshift = n ? (int)std::lround(acc / n) : 0;
+    }
+    if (p->g.fhalf) {
+        // FP16 wave fields: the moduli carry 2^-kshift and the buoyancies
+        // 2^kshift (exact power-of-two scalings of the FP32 parameters).
+        p->kshift = p->bshift;
         const int up[3] = {PRIP, PRJP, PRKP}, down[5] = {PM, PMU, PMUIPKP, PMUIPJP, PMUJPKP};
         std::vector<float> tmp(npar);
         for (int k = 0; k < NPAR; k++) {
@@ -796,39 +883,92 @@ extern "C" int sfd_source_type_mask(const float *src_pos, int nsrc_all)
     return m;
 }
 
+namespace {
+// the shots of one batched call: sources, receivers and their totals
+struct ShotBatch {
+    int n, nsrc, nrec;
+    const sfd_shot *shots;
+};
+int check_batch(sfd_plan *p, int nshot, const sfd_shot *shots, ShotBatch &sb)
+{
+    if (nshot < 1 || !shots) return fail(p, SFD_ERR_ARG, "a batch needs at least one shot");
+    if (nshot > p->batch) return fail(p, SFD_ERR_ARG, "more shots than the plan's batch");
+    sb.n = nshot;
+    sb.shots = shots;
+    sb.nsrc = sb.nrec = 0;
+    for (int b = 0; b < nshot; b++) {
+        if (shots[b].nsrc < 0 || shots[b].nrec < 0) return fail(p, SFD_ERR_ARG, "negative source or receiver count");
+        sb.nsrc += shots[b].nsrc;
+        sb.nrec += shots[b].nrec;
+    }
+    return SFD_OK;
+}
+}  // namespace
+
 extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const int *outsel, float *const *seis,
                            int save_boundaries, void *stream)
 {
     if (!p || !shot) return SFD_ERR_ARG;
+    return sfd_forward_batch(p, 1, shot, mask, outsel, seis, save_boundaries, stream);
+}
+
+extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, int mask, const int *outsel,
+                                 float *const *seis, int save_boundaries, void *stream)
+{
+    if (!p) return SFD_ERR_ARG;
     if (!p->model_set) return fail(p, SFD_ERR_STATE, "sfd_set_model must be called first");
     int rc;
+    ShotBatch sb;
+    if ((rc = check_batch(p, nshot, shots, sb))) return rc;
     if ((rc = check_outsel(p, outsel))) return rc;
+    if (nshot > 1 && save_boundaries && p->cfg.back_prop_type == 2)
+        return fail(p, SFD_ERR_UNSUPPORTED, "batched shots cover the boundary-saving gradient");
+    if (nshot > 1 && p->movout > 0) return fail(p, SFD_ERR_UNSUPPORTED, "a movie films one shot per run");
     cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+    p->g.nb = nshot;
     const Grid &g = p->g;
     int nsel;
     unsigned omask = outmask_of(outsel, g.nd, &nsel);
-    if ((rc = ensure_shot_buffers(p, shot->nsrc, shot->nrec, nsel))) return rc;
+    if ((rc = ensure_shot_buffers(p, sb.nsrc, sb.nrec, nsel))) return rc;
     PointSet S, R;
-    if ((rc = upload_shot(p, shot, mask, S, R, st))) return rc;
+    if ((rc = upload_shots(p, nshot, shots, mask, S, R, st))) return rc;
     if ((rc = zero_forward_state(p, st))) return rc;
-    if (nsel) CKC(cudaMemsetAsync(p->d_seis, 0, sizeof(float) * (size_t)nsel * shot->nrec * p->cfg.nt, st));
+    if (nsel) CKC(cudaMemsetAsync(p->d_seis, 0, sizeof(float) * (size_t)nsel * sb.nrec * p->cfg.nt, st));
     BndSlot bs;
     memset(&bs, 0, sizeof bs);
+    // FP16 stores: the source injects about 2^4 per step into the field it
+    // feeds (velocities for force sources, stresses otherwise)
+    auto store_exponents = [&](int shift, int &a, int &b) {
+        float smax = 0.0f;
+        bool force_only = sb.nsrc > 0;
+        for (int q = 0; q < nshot; q++)
+            for (int i = 0; i < shots[q].nsrc; i++) {
+                const int ty = (int)shots[q].src_pos[5 * i + 4];
+                if (ty != 0 && ty != 1 && ty != 2) force_only = false;
+                for (int t = 0; t < p->cfg.nt; t++)
+                    smax = std::max(smax, std::fabs(shots[q].src[(int64_t)i * p->cfg.nt + t]));
+            }
+        const double inj = (double)smax * p->cfg.dt;
+        const int e0 = inj > 0 ? (int)std::lround(4.0 - std::log2(inj)) : 0;
+        a = force_only ? e0 - shift : e0;
+        b = a + shift;
+    };
     if (g.fhalf) {
         if (save_boundaries)
             return fail(p, SFD_ERR_UNSUPPORTED, "FP16 wave-field storage covers forward modelling only");
-        // the source injects about 2^4 per step into the field it feeds
-        float smax = 0.0f;
-        bool force_only = shot->nsrc > 0;
-        for (int i = 0; i < shot->nsrc; i++) {
-            const int ty = (int)shot->src_pos[5 * i + 4];
-            if (ty != 0 && ty != 1 && ty != 2) force_only = false;
-            for (int t = 0; t < p->cfg.nt; t++) smax = std::max(smax, std::fabs(shot->src[(int64_t)i * p->cfg.nt + t]));
-        }
-        const double inj = (double)smax * p->cfg.dt;
-        const int e0 = inj > 0 ? (int)std::lround(4.0 - std::log2(inj)) : 0;
-        const int a = force_only ? e0 - p->kshift : e0, b = a + p->kshift;
+        int a, b;
+        store_exponents(p->kshift, a, b);
         for (int w = 0; w < NW; w++) p->g.ws.w[w] = std::ldexp(1.0f, w <= VZ ? b : a);
+    }
+    for (int w = 0; w < NW; w++) p->g.bsc[w] = p->g.bsci[w] = 1.0f;
+    if (save_boundaries && p->cfg.precision == SFD_PREC_FP16) {
+        // without a scale, velocities (~stress / impedance) fall below FP16's range
+        int a, b;
+        store_exponents(p->bshift, a, b);
+        for (int w = 0; w < NW; w++) {
+            p->g.bsc[w] = std::ldexp(1.0f, w <= VZ ? b : a);
+            p->g.bsci[w] = std::ldexp(1.0f, w <= VZ ? -b : -a);
+        }
     }
     // a gradient run keeps the boundary shells (BACK_PROP_TYPE 1) or the
     // forward transforms (2)
@@ -846,11 +986,9 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
         for (int w = 0; w < NW; w++) {
             if (!p->f.w[w]) continue;
             if (!p->d_bnd[w]) {
-                cudaError_t e = cudaMalloc(&p->d_bnd[w], p->bnd_elem * (size_t)p->cfg.nt * g.nbnd);
-                if (e != cudaSuccess) {
-                    p->d_bnd[w] = nullptr;
-                    return fail(p, SFD_ERR_MEMORY, "saved-boundary store does not fit in device memory");
-                }
+                cudaError_t e;
+                p->d_bnd[w] = dalloc_raw(p, p->bnd_elem * (size_t)p->cfg.nt * g.nbnd * p->batch, &e);
+                if (!p->d_bnd[w]) return fail(p, SFD_ERR_MEMORY, "saved-boundary store does not fit in device memory");
             }
             bs.p[w] = p->d_bnd[w];
             bs.fields[bs.nfield++] = w;
@@ -914,8 +1052,8 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
     for (int o = 0; o < SFD_NOUT; o++) {
         if (!(omask & (1u << o))) continue;
         if (seis && seis[o])
-            CKC(cudaMemcpyAsync(seis[o], p->d_seis + (size_t)slot * shot->nrec * NT,
-                                sizeof(float) * (size_t)shot->nrec * NT, cudaMemcpyDeviceToHost, st));
+            CKC(cudaMemcpyAsync(seis[o], p->d_seis + (size_t)slot * sb.nrec * NT,
+                                sizeof(float) * (size_t)sb.nrec * NT, cudaMemcpyDeviceToHost, st));
         slot++;
     }
     CKC(cudaStreamSynchronize(st));
@@ -923,6 +1061,7 @@ extern "C" int sfd_forward(sfd_plan *p, const sfd_shot *shot, int mask, const in
     if (tma_take_status())
         return fail(p, SFD_ERR_CUDA, "a TMA stage of the 3D stencil kernels did not arrive within its time bound");
     p->have_forward = save_boundaries != 0;
+    p->fwd_nb = nshot;
     p->have_dft = dft;
     return SFD_OK;
 }
@@ -931,27 +1070,38 @@ extern "C" int sfd_adjoint(sfd_plan *p, const sfd_shot *shot, int mask, const in
                            const float *const *residuals, void *stream)
 {
     if (!p || !shot) return SFD_ERR_ARG;
+    return sfd_adjoint_batch(p, 1, shot, mask, outsel, residuals, stream);
+}
+
+extern "C" int sfd_adjoint_batch(sfd_plan *p, int nshot, const sfd_shot *shots, int mask, const int *outsel,
+                                 const float *const *residuals, void *stream)
+{
+    if (!p) return SFD_ERR_ARG;
+    int rc;
+    ShotBatch sb;
+    if ((rc = check_batch(p, nshot, shots, sb))) return rc;
     if (p->g.nd == 21 || p->g.nd == 22)
         return fail(p, SFD_ERR_UNSUPPORTED, "the adjoint path covers P-SV and 3D elastic/viscoelastic media");
     if (p->g.fhalf) return fail(p, SFD_ERR_UNSUPPORTED, "FP16 wave-field storage covers forward modelling only");
     if (!p->have_forward) return fail(p, SFD_ERR_STATE, "sfd_adjoint needs a preceding sfd_forward with saved boundaries");
-    int rc;
+    if (nshot != p->fwd_nb) return fail(p, SFD_ERR_STATE, "the adjoint must follow a forward run of the same shots");
     if ((rc = check_outsel(p, outsel))) return rc;
     if ((rc = alloc_adjoint(p))) return rc;
     cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;
+    p->g.nb = nshot;
     const Grid &g = p->g;
     int nsel;
     unsigned omask = outmask_of(outsel, g.nd, &nsel);
-    if ((rc = ensure_shot_buffers(p, shot->nsrc, shot->nrec, nsel))) return rc;
+    if ((rc = ensure_shot_buffers(p, sb.nsrc, sb.nrec, nsel))) return rc;
     PointSet S, R;
-    if ((rc = upload_shot(p, shot, mask, S, R, st))) return rc;
+    if ((rc = upload_shots(p, nshot, shots, mask, S, R, st))) return rc;
     const int NT = p->cfg.nt;
     int slot = 0;
     for (int o = 0; o < SFD_NOUT; o++) {
         if (!(omask & (1u << o))) continue;
         if (!residuals || !residuals[o]) return fail(p, SFD_ERR_ARG, "missing residual array");
-        CKC(cudaMemcpyAsync(p->d_res + (size_t)slot * shot->nrec * NT, residuals[o],
-                            sizeof(float) * (size_t)shot->nrec * NT, cudaMemcpyHostToDevice, st));
+        CKC(cudaMemcpyAsync(p->d_res + (size_t)slot * sb.nrec * NT, residuals[o],
+                            sizeof(float) * (size_t)sb.nrec * NT, cudaMemcpyHostToDevice, st));
         slot++;
     }
     if (p->cfg.back_prop_type == 2) {
@@ -961,14 +1111,14 @@ extern "C" int sfd_adjoint(sfd_plan *p, const sfd_shot *shot, int mask, const in
     // adjoint fields start at zero; the CPML memory carries over from the
     // forward run (the reference binds the forward psi buffers by name)
     for (int w = 0; w < NW; w++)
-        if (p->a.wr[w]) CKC(cudaMemsetAsync(p->a.wr[w], 0, sizeof(float) * g.nvol, st));
+        if (p->a.wr[w]) CKC(cudaMemsetAsync(p->a.wr[w], 0, sizeof(float) * g.nvol * nshot, st));
     for (int r = 0; r < NR; r++)
-        if (p->a.rr[r]) CKC(cudaMemsetAsync(p->a.rr[r], 0, sizeof(float) * g.nvol * g.L, st));
+        if (p->a.rr[r]) CKC(cudaMemsetAsync(p->a.rr[r], 0, sizeof(float) * g.nvol * g.L * nshot, st));
     if (p->cfg.adjoint_reset_psi) {
         // optional: start the adjoint with clean CPML memory instead
         int64_t tot = 0;
         for (int i = 0; i < NPSI; i++) tot += psi_span(p->psi_size[i]);
-        if (tot) CKC(cudaMemsetAsync(p->d_psi_all, 0, sizeof(float) * tot, st));
+        if (tot) CKC(cudaMemsetAsync(p->d_psi_all, 0, sizeof(float) * tot * nshot, st));
     }
     AdjFields a = p->a;
     // the movie of a boundary-saving gradient: the reconstructed forward
@@ -1003,15 +1153,35 @@ extern "C" int sfd_adjoint(sfd_plan *p, const sfd_shot *shot, int mask, const in
     return SFD_OK;
 }
 
+namespace {
+// the sum over the plan's shot copies of a device array of n doubles, in
+// copy order
+int fetch_sum(sfd_plan *p, const double *d, double *h, int64_t n)
+{
+    if (p->batch == 1) {
+        CKC(cudaMemcpy(h, d, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        return SFD_OK;
+    }
+    std::vector<double> all((size_t)n * p->batch);
+    CKC(cudaMemcpy(all.data(), d, sizeof(double) * all.size(), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < n; i++) {
+        double acc = all[i];
+        for (int b = 1; b < p->batch; b++) acc += all[(size_t)b * n + i];
+        h[i] = acc;
+    }
+    return SFD_OK;
+}
+}  // namespace
+
 extern "C" int sfd_zero_gradient(sfd_plan *p)
 {
     if (!p) return SFD_ERR_ARG;
     int rc;
     if ((rc = alloc_adjoint(p))) return rc;
-    int64_t npar = (int64_t)p->g.nz * p->g.ny * p->g.nx;
+    int64_t npar = (int64_t)p->g.nz * p->g.ny * p->g.nx * p->batch;
     for (int k = 0; k < NG; k++) {
-        if (p->a.grad[k]) CKC(cudaMemset(p->a.grad[k], 0, sizeof(double) * npar));
-        if (p->a.hess[k]) CKC(cudaMemset(p->a.hess[k], 0, sizeof(double) * npar));
+        if (p->a.grad[k]) CKC(cudaMemsetAsync(p->a.grad[k], 0, sizeof(double) * npar, p->stream));
+        if (p->a.hess[k]) CKC(cudaMemsetAsync(p->a.hess[k], 0, sizeof(double) * npar, p->stream));
     }
     return SFD_OK;
 }
@@ -1025,7 +1195,7 @@ extern "C" int sfd_get_hessian(sfd_plan *p, int transform, float *const *out)
     std::vector<double> h[NG];
     for (int k = 0; k < NG; k++) {
         h[k].resize(n);
-        CKC(cudaMemcpy(h[k].data(), p->a.hess[k], sizeof(double) * n, cudaMemcpyDeviceToHost));
+        if (int rc_ = fetch_sum(p, p->a.hess[k], h[k].data(), n)) return rc_;
     }
     const int pt = p->cfg.param_type;
     if (transform && p->cfg.back_prop_type != 2 && (pt == 0 || pt == 2)) {
@@ -1099,7 +1269,7 @@ extern "C" int sfd_get_gradient_q(sfd_plan *p, float *gtaup, float *gtaus)
             std::fill(outs[q], outs[q] + n, 0.0f);
             continue;
         }
-        CKC(cudaMemcpy(h.data(), p->a.grad[ids[q]], sizeof(double) * n, cudaMemcpyDeviceToHost));
+        if (int rc_ = fetch_sum(p, p->a.grad[ids[q]], h.data(), n)) return rc_;
         for (int64_t i = 0; i < n; i++) outs[q][i] = (float)h[i];
     }
     return SFD_OK;
@@ -1111,9 +1281,9 @@ extern "C" int sfd_get_gradient(sfd_plan *p, int transform, float *g0, float *g1
     if (!p->a.grad[0]) return fail(p, SFD_ERR_STATE, "no gradient has been accumulated");
     int64_t n = (int64_t)p->g.nz * p->g.ny * p->g.nx;
     std::vector<double> gr(n), gM(n), gmu(n);
-    CKC(cudaMemcpy(gr.data(), p->a.grad[GRHO], sizeof(double) * n, cudaMemcpyDeviceToHost));
-    CKC(cudaMemcpy(gM.data(), p->a.grad[GM], sizeof(double) * n, cudaMemcpyDeviceToHost));
-    CKC(cudaMemcpy(gmu.data(), p->a.grad[GMU], sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (int rc_ = fetch_sum(p, p->a.grad[GRHO], gr.data(), n)) return rc_;
+    if (int rc_ = fetch_sum(p, p->a.grad[GM], gM.data(), n)) return rc_;
+    if (int rc_ = fetch_sum(p, p->a.grad[GMU], gmu.data(), n)) return rc_;
     // the DFT gradient is already in the param_type's basis (no transf_grad)
     if (!transform || p->cfg.back_prop_type == 2) {
         for (int64_t i = 0; i < n; i++) {
@@ -1241,6 +1411,7 @@ extern "C" int sfd_bench_kernels(sfd_plan *p, int nrep, float *out_ms)
     if (!p || !out_ms || nrep <= 0) return SFD_ERR_ARG;
     if (!p->model_set) return fail(p, SFD_ERR_STATE, "no model");
     cudaStream_t st = p->stream;
+    p->g.nb = 1;
     const Grid &g = p->g;
     for (int k = 0; k < 3; k++) out_ms[k] = 0.0f;
     for (int which = 0; which < 3; which++) {

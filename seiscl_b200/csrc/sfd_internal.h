@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "seiscl_b200.h"
@@ -57,12 +58,22 @@ struct Grid {
     float inv_dt;           // 1/dt rounded to FP32
     int fhalf;              // 1: wave fields and memory variables stored in FP16 (3D forward)
     WScale ws;              // storage scale per wave field (all 1 for FP32)
+    float bsc[NW], bsci[NW];  // saved-boundary store scale per wave field and its inverse
+                              // (powers of two for FP16 stores, 1 otherwise)
     int nbnd;               // saved-boundary cells per field per step
     int restype;
     int kernels;            // 0: register-blocked 3D kernels where available, 1: general only
     int bp2;                // adjoint kernels: 1 for the DFT gradient (no reconstruction,
                             // boundary injection or on-the-fly gradient)
     int hout;               // accumulate the approximate Hessian
+    // batched shots (2D): the launch covers nb shots, blockIdx.z = shot; shot
+    // b works on copy b of each per-shot array, these strides apart
+    int nb;
+    int64_t sb_w, sb_r;     // wave fields (nvol), memory variables (L nvol)
+    int64_t sb_psi;         // the CPML block (floats)
+    int64_t sb_g;           // gradient / Hessian sums (physical cells)
+    int64_t sb_q;           // surface-adjoint scratch (nx ny)
+    int64_t sb_bnd;         // saved-boundary store of one field (bytes)
 };
 
 struct Fields {
@@ -119,7 +130,8 @@ struct sfd_plan {
     std::vector<float> hp[sfd::NPAR];
     bool model_set;
     // device memory
-    std::vector<void *> allocs;
+    std::vector<std::pair<void *, size_t>> allocs;   // owned by the plan
+    int64_t dev_bytes;      // device bytes the plan holds
     sfd::Fields f;
     sfd::AdjFields a;
     float *d_psi_all;
@@ -134,8 +146,11 @@ struct sfd_plan {
     float *d_src_div, *d_src, *d_seis, *d_res;
     float *d_surf_q;        // surface-adjoint scratch [nx][ny]
     int *d_ticket;          // fused 2D steps: block counter of the stress launch
+    int batch;              // copies of the per-shot arrays (shots per launch)
+    int fwd_nb;             // shots of the forward run whose boundaries are saved
     cudaEvent_t ev0, ev1;
     int kshift;             // FP16 storage: log2 ratio of velocity to stress scales
+    int bshift;             // the same ratio for FP16 saved boundaries (set whatever the storage)
     float last_ms;
     // DFT gradient (back_prop_type 2, src/assign_modeling_case.c:549-570)
     int nfreqs, dtnyq, ntnyq;
@@ -155,5 +170,6 @@ struct sfd_plan {
     struct LoopGraph {
         cudaGraphExec_t exec = nullptr;
         std::string key;
+        std::string seen;   // key of the last loop run without a graph
     } gfwd, gadj;
 };

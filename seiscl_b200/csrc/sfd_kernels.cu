@@ -120,6 +120,47 @@ template <> __device__ __forceinline__ float from_f<float>(float v) { return v; 
 template <> __device__ __forceinline__ __half from_f<__half>(float v) { return __float2half_rn(v); }
 template <> __device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
 
+// batched shots: shot b of a launch (blockIdx.z) works on copy b of every
+// per-shot array
+__device__ __forceinline__ void shot_fields(const Grid &g, Fields &f, int b)
+{
+#pragma unroll
+    for (int w = 0; w < NW; w++)
+        if (f.w[w]) f.w[w] += b * g.sb_w;
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+        if (f.r[r]) f.r[r] += b * g.sb_r;
+#pragma unroll
+    for (int i = 0; i < NPSI; i++)
+        if (f.psi[i]) f.psi[i] += b * g.sb_psi;
+}
+__device__ __forceinline__ void shot_adj(const Grid &g, AdjFields &a, int b)
+{
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+        if (a.wr[w]) a.wr[w] += b * g.sb_w;
+        if (a.bnd[w]) a.bnd[w] = (const char *)a.bnd[w] + b * g.sb_bnd;
+    }
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+        if (a.rr[r]) a.rr[r] += b * g.sb_r;
+#pragma unroll
+    for (int k = 0; k < NG; k++) {
+        if (a.grad[k]) a.grad[k] += b * g.sb_g;
+        if (a.hess[k]) a.hess[k] += b * g.sb_g;
+    }
+}
+#define SHOT_F  if (g.nb > 1) shot_fields(g, f, blockIdx.z);
+#define SHOT_FA if (g.nb > 1) { shot_fields(g, f, blockIdx.z); shot_adj(g, a, blockIdx.z); }
+
+// a saved boundary value (slice t-1) back in field units: FP16 stores carry
+// a power-of-two scale (exact; 1 for FP32 and BF16 stores)
+template <class T>
+__device__ __forceinline__ float bnd_at(const Grid &g, const AdjFields &a, int w, i64 m)
+{
+    return to_f<T>(((const T *)a.bnd[w])[m]) * g.bsci[w];
+}
+
 // ------------------------------------------------------- boundary shells
 struct BndDims {
     int NXbnd, NYbnd, NZbnd, lbnd, lbnds;
@@ -293,6 +334,7 @@ __device__ __forceinline__ void cpml_s2d(const Grid &g, const Fields &f, int gz,
 template <int F>
 __global__ void __launch_bounds__(256) k_v2d(Grid g, Fields f)
 {
+    SHOT_F
     int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
     if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
@@ -425,6 +467,7 @@ __device__ __forceinline__ void surf2d_column(const Grid &g, const Fields &f, in
 template <int F>
 __global__ void k_surf2d(Grid g, Fields f, int pdir)
 {
+    SHOT_F
     int gx = blockIdx.x * blockDim.x + threadIdx.x + F;
     if (gx <= g.NX - F - 1) surf2d_column<F>(g, f, gx, pdir);
 }
@@ -432,6 +475,7 @@ __global__ void k_surf2d(Grid g, Fields f, int pdir)
 template <int F>
 __global__ void __launch_bounds__(256) k_s2d(Grid g, Fields f)
 {
+    SHOT_F
     int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
     if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_cell<F>(g, f, gz, gx);
@@ -1267,9 +1311,9 @@ __global__ void __launch_bounds__(128) k_adjv3d_q4(Grid g, Fields f, AdjFields a
             vz.v[j] = vz.v[j] - (szz_z.v[j] + sxz_x.v[j] + syz_y.v[j]) * rkp.v[j];
             const int m = inject_ind3d(g, gz0 + j, gy, gx);
             if (m != -1) {
-                vx.v[j] = to_f<T>(((const T *)a.bnd[VX])[m]);
-                vy.v[j] = to_f<T>(((const T *)a.bnd[VY])[m]);
-                vz.v[j] = to_f<T>(((const T *)a.bnd[VZ])[m]);
+                vx.v[j] = bnd_at<T>(g, a, VX, m);
+                vy.v[j] = bnd_at<T>(g, a, VY, m);
+                vz.v[j] = bnd_at<T>(g, a, VZ, m);
             }
         }
         stq(f.w[VX] + iv, vx); stq(f.w[VY] + iv, vy); stq(f.w[VZ] + iv, vz);
@@ -1456,9 +1500,9 @@ __global__ void __launch_bounds__(128, 4) k_adjs3d_q4(Grid g, Fields f, AdjField
                 }
                 const int m = inject_ind3d(g, gz0 + j, gy, gx);
                 if (m != -1) {
-                    s3[0].v[j] = to_f<T>(((const T *)a.bnd[SXX])[m]);
-                    s3[1].v[j] = to_f<T>(((const T *)a.bnd[SYY])[m]);
-                    s3[2].v[j] = to_f<T>(((const T *)a.bnd[SZZ])[m]);
+                    s3[0].v[j] = bnd_at<T>(g, a, SXX, m);
+                    s3[1].v[j] = bnd_at<T>(g, a, SYY, m);
+                    s3[2].v[j] = bnd_at<T>(g, a, SZZ, m);
                 }
             }
 #pragma unroll
@@ -1590,7 +1634,7 @@ __global__ void __launch_bounds__(128, 4) k_adjs3d_q4(Grid g, Fields f, AdjField
                     sc.v[j] -= ls + g.dt2 * aa;
                 }
                 const int m = inject_ind3d(g, gz0 + j, gy, gx);
-                if (m != -1) sc.v[j] = to_f<T>(((const T *)a.bnd[wid])[m]);
+                if (m != -1) sc.v[j] = bnd_at<T>(g, a, wid, m);
             }
             stq(f.w[wid] + iv, sc);
         }
@@ -1826,6 +1870,7 @@ __global__ void k_surf3d(Grid g, Fields f, int pdir)
 template <int F>
 __global__ void __launch_bounds__(256) k_v2d_acc(Grid g, Fields f)
 {
+    SHOT_F
     int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
     if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
@@ -1923,6 +1968,7 @@ __device__ __forceinline__ void s2d_acc_cell(const Grid &g, const Fields &f, int
 template <int F>
 __global__ void __launch_bounds__(256) k_s2d_acc(Grid g, Fields f)
 {
+    SHOT_F
     int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
     if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_acc_cell<F>(g, f, gz, gx);
@@ -2020,14 +2066,16 @@ __global__ void k_surf_sh(Grid g, Fields f)
 template <typename T>
 __global__ void k_savebnd(Grid g, Fields f, BndSlot b, i64 tofs)
 {
+    SHOT_F
     int gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= g.nbnd) return;
+    const i64 sh = (i64)blockIdx.z * (g.sb_bnd / (i64)sizeof(T));
     int i, j, k;
     if (!shell_cell(g, gid, i, j, k)) return;
     i64 iv = ((i64)i * g.NY + j) * g.NZ + k;
     for (int q = 0; q < b.nfield; q++) {
         int w = b.fields[q];
-        ((T *)b.p[w])[tofs + gid] = from_f<T>(f.w[w][iv]);
+        ((T *)b.p[w])[sh + tofs + gid] = from_f<T>(f.w[w][iv] * g.bsc[w]);
     }
 }
 
@@ -2035,6 +2083,7 @@ __global__ void k_savebnd(Grid g, Fields f, BndSlot b, i64 tofs)
 template <int F, typename T>
 __global__ void __launch_bounds__(256) k_adjv2d(Grid g, Fields f, AdjFields a)
 {
+    SHOT_FA
     int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
     if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
@@ -2051,8 +2100,8 @@ __global__ void __launch_bounds__(256) k_adjv2d(Grid g, Fields f, AdjFields a)
         vz = f.w[VZ][iv] - (szz_z + sxz_x) * rkp;
         int m = inject_ind2d(g, gz, gx);
         if (m != -1) {
-            vx = to_f<T>(((const T *)a.bnd[VX])[m]);
-            vz = to_f<T>(((const T *)a.bnd[VZ])[m]);
+            vx = bnd_at<T>(g, a, VX, m);
+            vz = bnd_at<T>(g, a, VZ, m);
         }
         f.w[VX][iv] = vx;
         f.w[VZ][iv] = vz;
@@ -2076,6 +2125,7 @@ __global__ void __launch_bounds__(256) k_adjv2d(Grid g, Fields f, AdjFields a)
 template <int F, typename T>
 __global__ void __launch_bounds__(256) k_adjs2d(Grid g, Fields f, AdjFields a)
 {
+    SHOT_FA
     int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
     if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
@@ -2138,9 +2188,9 @@ __global__ void __launch_bounds__(256) k_adjs2d(Grid g, Fields f, AdjFields a)
     if (!g.bp2) {
         int m = inject_ind2d(g, gz, gx);
         if (m != -1) {
-            sxx = to_f<T>(((const T *)a.bnd[SXX])[m]);
-            szz = to_f<T>(((const T *)a.bnd[SZZ])[m]);
-            sxz = to_f<T>(((const T *)a.bnd[SXZ])[m]);
+            sxx = bnd_at<T>(g, a, SXX, m);
+            szz = bnd_at<T>(g, a, SZZ, m);
+            sxz = bnd_at<T>(g, a, SXZ, m);
         }
         f.w[SXX][iv] = sxx; f.w[SZZ][iv] = szz; f.w[SXZ][iv] = sxz;
     }
@@ -2209,6 +2259,8 @@ __global__ void __launch_bounds__(256) k_adjs2d(Grid g, Fields f, AdjFields a)
 template <int F>
 __global__ void k_surfadj2d_a(Grid g, Fields f, AdjFields a, float *q)
 {
+    SHOT_FA
+    q += blockIdx.z * g.sb_q;
     int gx = blockIdx.x * blockDim.x + threadIdx.x + F;
     if (gx > g.NX - F - 1) return;
     int gz = F;
@@ -2231,6 +2283,8 @@ __global__ void k_surfadj2d_a(Grid g, Fields f, AdjFields a, float *q)
 template <int F>
 __global__ void k_surfadj2d_b(Grid g, Fields f, AdjFields a, const float *q)
 {
+    SHOT_FA
+    q += blockIdx.z * g.sb_q;
     int gx = blockIdx.x * blockDim.x + threadIdx.x + F;
     if (gx > g.NX - F - 1) return;
     int gz = F, x = gx - F, nx = g.nx;
@@ -2262,9 +2316,9 @@ __global__ void __launch_bounds__(256) k_adjv3d(Grid g, Fields f, AdjFields a)
         vz = f.w[VZ][iv] - (szz_z + sxz_x + syz_y) * rkp;
         int m = inject_ind3d(g, gz, gy, gx);
         if (m != -1) {
-            vx = to_f<T>(((const T *)a.bnd[VX])[m]);
-            vy = to_f<T>(((const T *)a.bnd[VY])[m]);
-            vz = to_f<T>(((const T *)a.bnd[VZ])[m]);
+            vx = bnd_at<T>(g, a, VX, m);
+            vy = bnd_at<T>(g, a, VY, m);
+            vz = bnd_at<T>(g, a, VZ, m);
         }
         f.w[VX][iv] = vx; f.w[VY][iv] = vy; f.w[VZ][iv] = vz;
     }
@@ -2361,9 +2415,9 @@ __global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
     if (!g.bp2) {
         int m = inject_ind3d(g, gz, gy, gx);
         if (m != -1) {
-            s[3] = to_f<T>(((const T *)a.bnd[SXX])[m]); s[4] = to_f<T>(((const T *)a.bnd[SYY])[m]);
-            s[5] = to_f<T>(((const T *)a.bnd[SZZ])[m]); s[0] = to_f<T>(((const T *)a.bnd[SXY])[m]);
-            s[1] = to_f<T>(((const T *)a.bnd[SYZ])[m]); s[2] = to_f<T>(((const T *)a.bnd[SXZ])[m]);
+            s[3] = bnd_at<T>(g, a, SXX, m); s[4] = bnd_at<T>(g, a, SYY, m);
+            s[5] = bnd_at<T>(g, a, SZZ, m); s[0] = bnd_at<T>(g, a, SXY, m);
+            s[1] = bnd_at<T>(g, a, SYZ, m); s[2] = bnd_at<T>(g, a, SXZ, m);
         }
         f.w[SXY][iv] = s[0]; f.w[SYZ][iv] = s[1]; f.w[SXZ][iv] = s[2];
         f.w[SXX][iv] = s[3]; f.w[SYY][iv] = s[4]; f.w[SZZ][iv] = s[5];
@@ -2574,10 +2628,12 @@ __global__ void __launch_bounds__(256) k_s2d_step(Grid g, Fields f, StepTail tl,
 {
     int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
-    if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_cell<F>(g, f, gz, gx);
+    Fields fs = f;   // this block's shot; the tail's points carry their shot in their cells
+    if (g.nb > 1) shot_fields(g, fs, blockIdx.z);
+    if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_cell<F>(g, fs, gz, gx);
     if (g.freesurf && blockIdx.x == 0) {
         __syncthreads();
-        if (threadIdx.x == 0 && gx <= g.NX - F - 1) surf2d_column<F>(g, f, gx, pdir);
+        if (threadIdx.x == 0 && gx <= g.NX - F - 1) surf2d_column<F>(g, fs, gx, pdir);
     }
     step_tail(g, f, tl);
 }
@@ -2588,7 +2644,9 @@ __global__ void __launch_bounds__(256) k_s2d_acc_step(Grid g, Fields f, StepTail
 {
     int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
-    if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_acc_cell<F>(g, f, gz, gx);
+    Fields fs = f;
+    if (g.nb > 1) shot_fields(g, fs, blockIdx.z);
+    if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_acc_cell<F>(g, fs, gz, gx);
     step_tail(g, f, tl);
 }
 
@@ -2647,7 +2705,7 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
     if (g.kernels == 3 && launch_update_v_tma(g, f, st)) return;
     if (g.kernels == 2 && launch_update_v_fast(g, f, st)) return;
     if (g.nd == 21 || g.nd == 22) {
-        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
+        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
         if (g.nd == 21) DISPATCH_F(g.F, k_v2d_sh<FF><<<gr, b, 0, st>>>(g, f))
         else DISPATCH_F(g.F, k_v2d_acc<FF><<<gr, b, 0, st>>>(g, f))
         return;
@@ -2668,7 +2726,7 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
         }
         DISPATCH_F(g.F, k_v3d<FF><<<gr, b, 0, st>>>(g, f));
     } else {
-        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
+        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
         DISPATCH_F(g.F, k_v2d<FF><<<gr, b, 0, st>>>(g, f));
     }
 }
@@ -2700,7 +2758,7 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
     if (g.kernels == 3 && launch_update_s_tma(g, f, st)) return;
     if (g.kernels == 2 && launch_update_s_fast(g, f, st)) return;
     if (g.nd == 21 || g.nd == 22) {
-        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
+        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
         if (g.nd == 21) DISPATCH_F(g.F, k_s2d_sh<FF><<<gr, b, 0, st>>>(g, f))
         else DISPATCH_F(g.F, k_s2d_acc<FF><<<gr, b, 0, st>>>(g, f))
         return;
@@ -2728,7 +2786,7 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
         }
         DISPATCH_F(g.F, k_s3d<FF><<<gr, b, 0, st>>>(g, f));
     } else {
-        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
+        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
         DISPATCH_F(g.F, k_s2d<FF><<<gr, b, 0, st>>>(g, f));
     }
 }
@@ -2770,7 +2828,7 @@ int stress_family(const Grid &g, const Fields &f)
 bool launch_update_s_step(const Grid &g, const Fields &f, const StepTail &tl, cudaStream_t st)
 {
     if (g.nd != 2 && g.nd != 22) return false;
-    dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));   // 32 z rows >= 2F + 1: the surface stays in its block
+    dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);   // 32 z rows >= 2F + 1: the surface stays in its block
     if (g.nd == 2) DISPATCH_F(g.F, k_s2d_step<FF><<<gr, b, 0, st>>>(g, f, tl, 1))
     else DISPATCH_F(g.F, k_s2d_acc_step<FF><<<gr, b, 0, st>>>(g, f, tl))
     return true;
@@ -2788,14 +2846,14 @@ void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st)
         if (g.fhalf) DISPATCH_F(g.F, k_surf3d<FF, __half><<<gr, b, 0, st>>>(g, f, pdir))
         else DISPATCH_F(g.F, k_surf3d<FF><<<gr, b, 0, st>>>(g, f, pdir))
     } else {
-        DISPATCH_F(g.F, k_surf2d<FF><<<cdiv(g.nx, 128), 128, 0, st>>>(g, f, pdir));
+        DISPATCH_F(g.F, k_surf2d<FF><<<dim3(cdiv(g.nx, 128), 1, g.nb), 128, 0, st>>>(g, f, pdir));
     }
 }
 
 void launch_savebnd(const Grid &g, const Fields &f, const BndSlot &b, int prec, int64_t tofs, cudaStream_t st)
 {
-    unsigned gr = cdiv(g.nbnd, 256);
-    if (gr == 0) return;
+    dim3 gr(cdiv(g.nbnd, 256), 1, g.nb);
+    if (gr.x == 0) return;
     if (prec == SFD_PREC_FP16) k_savebnd<__half><<<gr, 256, 0, st>>>(g, f, b, tofs);
     else if (prec == SFD_PREC_BF16) k_savebnd<__nv_bfloat16><<<gr, 256, 0, st>>>(g, f, b, tofs);
     else k_savebnd<float><<<gr, 256, 0, st>>>(g, f, b, tofs);
@@ -2824,7 +2882,7 @@ static void launch_adj_t(const Grid &g, const Fields &f, const AdjFields &a, boo
         if (stress) DISPATCH_F(g.F, k_adjs3d<FF, T><<<gr, b, 0, st>>>(g, f, a))
         else DISPATCH_F(g.F, k_adjv3d<FF, T><<<gr, b, 0, st>>>(g, f, a))
     } else {
-        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8));
+        dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
         if (stress) DISPATCH_F(g.F, k_adjs2d<FF, T><<<gr, b, 0, st>>>(g, f, a))
         else DISPATCH_F(g.F, k_adjv2d<FF, T><<<gr, b, 0, st>>>(g, f, a))
     }
@@ -2844,8 +2902,8 @@ void launch_surface_adj(const Grid &g, const Fields &f, const AdjFields &a, floa
         DISPATCH_F(g.F, k_surfadj3d_a<FF><<<gr, b, 0, st>>>(g, f, a, q));
         DISPATCH_F(g.F, k_surfadj3d_b<FF><<<gr, b, 0, st>>>(g, f, a, q));
     } else {
-        DISPATCH_F(g.F, k_surfadj2d_a<FF><<<cdiv(g.nx, 128), 128, 0, st>>>(g, f, a, q));
-        DISPATCH_F(g.F, k_surfadj2d_b<FF><<<cdiv(g.nx, 128), 128, 0, st>>>(g, f, a, q));
+        DISPATCH_F(g.F, k_surfadj2d_a<FF><<<dim3(cdiv(g.nx, 128), 1, g.nb), 128, 0, st>>>(g, f, a, q));
+        DISPATCH_F(g.F, k_surfadj2d_b<FF><<<dim3(cdiv(g.nx, 128), 1, g.nb), 128, 0, st>>>(g, f, a, q));
     }
 }
 

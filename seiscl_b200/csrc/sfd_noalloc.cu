@@ -102,6 +102,7 @@ extern "C" int sfd_forward_noalloc(sfd_plan *p, const float *src_pos, const floa
         p->err = "invalid shot arrays";
         return SFD_ERR_ARG;
     }
+    p->g.nb = 1;   // one shot, whatever the plan's batch
     const Grid &g = p->g;
     unsigned omask = 0;
     int nsel = 0;

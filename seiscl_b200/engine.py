@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 from dataclasses import dataclass, field
-from typing import Dict, Optional, Sequence
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -37,7 +37,7 @@ class sfd_config(C.Structure):
                 ("param_type", C.c_int), ("restype", C.c_int), ("precision", C.c_int),
                 ("kernels", C.c_int), ("adjoint_reset_psi", C.c_int), ("field_precision", C.c_int),
                 ("back_prop_type", C.c_int), ("loop_graphs", C.c_int), ("hout", C.c_int),
-                ("reserved", C.c_int * 1)]
+                ("batch", C.c_int)]
 
 
 class sfd_shot(C.Structure):
@@ -56,6 +56,10 @@ EXPORTS = {
                               C.c_int, C.c_void_p]),
     "sfd_adjoint": (C.c_int, [C.c_void_p, C.POINTER(sfd_shot), C.c_int, C.POINTER(C.c_int), C.POINTER(FP),
                               C.c_void_p]),
+    "sfd_forward_batch": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(sfd_shot), C.c_int, C.POINTER(C.c_int),
+                                    C.POINTER(FP), C.c_int, C.c_void_p]),
+    "sfd_adjoint_batch": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(sfd_shot), C.c_int, C.POINTER(C.c_int),
+                                    C.POINTER(FP), C.c_void_p]),
     "sfd_zero_gradient": (C.c_int, [C.c_void_p]),
     "sfd_get_gradient": (C.c_int, [C.c_void_p, C.c_int, FP, FP, FP]),
     "sfd_get_gradient_q": (C.c_int, [C.c_void_p, FP, FP]),
@@ -76,6 +80,7 @@ EXPORTS = {
     "sfd_footprint": (C.c_int, [C.POINTER(sfd_config), C.c_int, C.c_int, C.c_int64, C.c_int,
                                 C.POINTER(C.c_int64)]),
     "sfd_device_memory": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "sfd_plan_device_bytes": (C.c_int64, [C.c_void_p]),
 }
 
 _LIB = None
@@ -147,8 +152,9 @@ class Config:
     field_precision: str = "fp32"  # "fp16": wave fields / memory variables stored in FP16 (3D forward)
     back_prop_type: int = 1  # 1: boundary-saving backpropagation, 2: DFT gradient at `gradfreqs`
     gradfreqs: Sequence[float] = ()  # DFT gradient frequencies (Hz), back_prop_type 2
-    loop_graphs: str = "auto"  # time loops as CUDA graphs: "auto" (2D), "always", "never"
+    loop_graphs: str = "auto"  # time loops as CUDA graphs: "auto" (2D, 3D up to 2^22 cells), "always", "never"
     hout: int = 0  # HOUT: also accumulate the approximate Hessian (2D)
+    batch: int = 1  # shots advanced together by forward_batch / adjoint_batch (2D P-SV and acoustic)
 
     def to_c(self) -> sfd_config:
         c = sfd_config()
@@ -181,6 +187,7 @@ class Config:
         c.precision = PREC[self.precision]
         c.kernels = {"fast": 0, "general": 1, "register": 2, "tma": 3, "stream": 4, "vector": 5}[self.kernels]
         c.adjoint_reset_psi = 1 if self.adjoint_reset_psi else 0
+        c.batch = int(self.batch)
         c.field_precision = {"fp32": 0, "fp16": 1}[self.field_precision]
         c.back_prop_type = int(self.back_prop_type)
         c.loop_graphs = {"auto": 0, "always": 1, "never": 2}[self.loop_graphs]
@@ -298,6 +305,48 @@ class Plan:
             ptrs[i] = _ptr(res[n])
         self._check(self.lib.sfd_adjoint(self.h, C.byref(shot), int(mask), sel, ptrs, None))
 
+    def forward_batch(self, shots, outputs, mask=None, save_boundaries=False) -> List[Dict[str, np.ndarray]]:
+        """Up to ``cfg.batch`` shots [(src_pos, src, rec_pos), ...] advanced
+        together (one launch per kernel and step for all of them); returns
+        their seismograms, one dict per shot."""
+        nt = self.cfg.NT
+        made = [self._shot(sp, src, rp, nt) for sp, src, rp in shots]
+        arr = (sfd_shot * len(made))(*[m[0] for m in made])
+        if mask is None:
+            mask = source_type_mask(np.concatenate([m[1][0] for m in made]))
+        nrec = [m[0].nrec for m in made]
+        sel = (C.c_int * 10)()
+        ptrs = (FP * 10)()
+        flat = {}
+        for n in outputs:
+            i = OUT_NAMES.index(n)
+            sel[i] = 1
+            flat[n] = np.zeros((sum(nrec), nt), np.float32)
+            ptrs[i] = _ptr(flat[n])
+        self._check(self.lib.sfd_forward_batch(self.h, len(made), arr, int(mask), sel, ptrs,
+                                               1 if save_boundaries else 0, None))
+        cuts = np.cumsum([0] + nrec)
+        return [{n: flat[n][cuts[b]:cuts[b + 1]] for n in outputs} for b in range(len(made))]
+
+    def adjoint_batch(self, shots, residuals: Sequence[Dict[str, np.ndarray]], mask=None):
+        """The adjoint of the batch a ``forward_batch(..., save_boundaries=True)``
+        ran; ``residuals`` one dict per shot."""
+        nt = self.cfg.NT
+        made = [self._shot(sp, src, rp, nt) for sp, src, rp in shots]
+        arr = (sfd_shot * len(made))(*[m[0] for m in made])
+        if mask is None:
+            mask = source_type_mask(np.concatenate([m[1][0] for m in made]))
+        sel = (C.c_int * 10)()
+        ptrs = (FP * 10)()
+        flat = {}
+        for n in residuals[0]:
+            i = OUT_NAMES.index(n)
+            sel[i] = 1
+            flat[n] = np.ascontiguousarray(np.concatenate(
+                [_f32(r[n], (m[0].nrec, nt)) for r, m in zip(residuals, made)]), np.float32)
+            ptrs[i] = _ptr(flat[n])
+        self._check(self.lib.sfd_adjoint_batch(self.h, len(made), arr, int(mask), sel, ptrs, None))
+
     def residual_scale(self, rec_pos, residuals: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
         nt = self.cfg.NT
         rp = _f32(rec_pos).reshape(-1, 8)
@@ -380,6 +429,11 @@ class Plan:
         if rc < 0:
             self._check(rc)
         return rc == 1
+
+    @property
+    def device_bytes(self) -> int:
+        """Device memory the plan holds now."""
+        return int(self.lib.sfd_plan_device_bytes(self.h))
 
     @property
     def kernel_family(self) -> str:

@@ -114,6 +114,7 @@ def test_gradient_against_fp64(kw, cuda_device):
     res = {k: (0.3 * v).astype(np.float32) for k, v in d.items()}
     o.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], res)
     gref = o.gradients()
+    got = {}
     for prec in ("fp32", "fp16", "bf16"):
         plan = Plan(dataclasses.replace(engine_config(cfg), precision=prec))
         plan.set_model(model["vp"], model["vs"], model["rho"])
@@ -124,7 +125,9 @@ def test_gradient_against_fp64(kw, cuda_device):
         plan.close()
         errs = {k: rel_l2(g[k], gref[k]) for k in ("vp", "vs", "rho")}
         print("FP64ERR gradient %s boundaries %s %s" % (kw, prec, {k: round(v, 9) for k, v in errs.items()}))
-        assert max(errs.values()) < 1e-3, (prec, errs)
+        got[prec] = errs
+    for prec in ("fp32", "fp16", "bf16"):
+        assert max(got[prec].values()) < 1e-3, (prec, got)
 
 
 @pytest.mark.gpu
