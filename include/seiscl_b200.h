@@ -110,8 +110,9 @@ typedef struct sfd_config {
     int hout;              /* HOUT: also accumulate the approximate Hessian (2D; the
                               reference's 3D Hessian kernel does not compile,
                               update_adjv3D.cl:486, so 3D boundary-saving plans reject it) */
-    int batch;             /* shots one launch advances together (2D P-SV and acoustic;
-                              0 or 1: one).  The plan holds `batch` copies of every
+    int batch;             /* shots one launch advances together (0 or 1: one; P-SV,
+                              acoustic and 3D with FP32 fields, kernels 0, 1, 4 or 5,
+                              boundary-saving gradients).  The plan holds `batch` copies of every
                               per-shot array; sfd_forward_batch / sfd_adjoint_batch run
                               up to that many shots of the same model at once, each
                               launch covering all of them.  No reference counterpart
@@ -230,7 +231,7 @@ int sfd_get_gradient_q(sfd_plan *plan, float *gtaup, float *gtaus);
  * sources.  res[k] are [nrec][NT] host arrays for the selected outputs. */
 int sfd_residual_scale(sfd_plan *plan, const sfd_shot *shot, const int *outsel, float *const *res);
 
-/* Batched shots (cfg.batch > 1, 2D P-SV and acoustic): nshot <= batch shots
+/* Batched shots (cfg.batch > 1): nshot <= batch shots
  * of the plan's model advance together, each launch of the time loop
  * covering all of them.  Shot s works on copy s of every per-shot array, so
  * each shot's result is the one sfd_forward gives it alone.  seis[o] (and

@@ -660,8 +660,11 @@ int check_config(const sfd_config &c)
     // the reference's 3D Hessian kernel does not compile (update_adjv3D.cl:486)
     if (c.hout && c.nd == 3 && c.back_prop_type != 2) return SFD_ERR_UNSUPPORTED;
     if (c.batch < 0 || c.batch > 64) return SFD_ERR_ARG;
-    // batched shots: the 2D P-SV and acoustic kernels, boundary-saving gradients
-    if (c.batch > 1 && ((c.nd != 2 && c.nd != 22) || c.back_prop_type == 2)) return SFD_ERR_UNSUPPORTED;
+    // batched shots: P-SV, acoustic and 3D one-cell / 4-cell kernels in FP32,
+    // boundary-saving gradients
+    if (c.batch > 1 && (c.nd == 21 || c.back_prop_type == 2 || c.field_precision != 0 || c.kernels == 2 ||
+                        c.kernels == 3))
+        return SFD_ERR_UNSUPPORTED;
     return SFD_OK;
 }
 

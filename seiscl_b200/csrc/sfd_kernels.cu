@@ -590,11 +590,14 @@ __device__ __forceinline__ void cpml_s3d(const Grid &g, const Fields &f, int gz,
     }
 }
 
+// grid z: the x blocks of each shot of the launch, shot after shot
 #define CELL3D                                                                         \
+    const int nxb_ = gridDim.z / g.nb, shot = blockIdx.z / nxb_;                       \
     int gz = blockIdx.x * blockDim.x + threadIdx.x + F;                                \
     int gy = blockIdx.y * blockDim.y + threadIdx.y + F;                                \
-    int gx = blockIdx.z * blockDim.z + threadIdx.z + F;                                \
+    int gx = (blockIdx.z - shot * nxb_) * blockDim.z + threadIdx.z + F;                \
     if (gz > g.NZ - F - 1 || gy > g.NY - F - 1 || gx > g.NX - F - 1) return;           \
+    if (g.nb > 1) shot_fields(g, f, shot);                                             \
     const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;                                        \
     i64 iv = gx * sx + (i64)gy * sy + gz;                                              \
     i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz - F);
@@ -976,10 +979,12 @@ __device__ __forceinline__ void cpml_v3d_q4(const Grid &g, const Fields &f, int 
 
 #define CELL3D_Q4                                                                      \
     constexpr int F = 4;                                                               \
+    const int nxb_ = gridDim.z / g.nb, shot = blockIdx.z / nxb_;                       \
     const int gz0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4 + F;                   \
     const int gy = blockIdx.y * blockDim.y + threadIdx.y + F;                          \
-    const int gx = blockIdx.z * blockDim.z + threadIdx.z + F;                          \
+    const int gx = (blockIdx.z - shot * nxb_) * blockDim.z + threadIdx.z + F;          \
     if (gz0 > g.NZ - F - 1 || gy > g.NY - F - 1 || gx > g.NX - F - 1) return;          \
+    if (g.nb > 1) shot_fields(g, f, shot);                                             \
     const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;                                        \
     const i64 iv = gx * sx + (i64)gy * sy + gz0;                                       \
     const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
@@ -1290,6 +1295,7 @@ template <typename T>
 __global__ void __launch_bounds__(128) k_adjv3d_q4(Grid g, Fields f, AdjFields a)
 {
     CELL3D_Q4
+    if (g.nb > 1) shot_adj(g, a, shot);
     const float *hc = g.hc;
     const Q4 rip = ldq(f.p[PRIP] + ip), rjp = ldq(f.p[PRJP] + ip), rkp = ldq(f.p[PRKP] + ip);
     Q4 vx = {{0, 0, 0, 0}}, vy = vx, vz = vx;
@@ -1425,6 +1431,7 @@ template <int L, typename T>
 __global__ void __launch_bounds__(128, 4) k_adjs3d_q4(Grid g, Fields f, AdjFields a)
 {
     CELL3D_Q4
+    if (g.nb > 1) shot_adj(g, a, shot);
     const float *hc = g.hc;
     // adjoint velocity derivatives, with CPML
     Q4 vzzr = dbw_z<F>(ldw(a.wr[VZ], iv), hc), vyzr = dfw_z<F>(ldw(a.wr[VY], iv), hc);
@@ -1791,6 +1798,7 @@ __global__ void __launch_bounds__(256, 2) k_s3d_stream(Grid g, Fields f)
 template <int F, class T = float>
 __global__ void k_surf3d(Grid g, Fields f, int pdir)
 {
+    SHOT_F
     int gy = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
     if (gy > g.NY - F - 1 || gx > g.NX - F - 1) return;
@@ -2302,6 +2310,7 @@ template <int F, typename T>
 __global__ void __launch_bounds__(256) k_adjv3d(Grid g, Fields f, AdjFields a)
 {
     CELL3D
+    if (g.nb > 1) shot_adj(g, a, shot);
     const float *hc = g.hc;
     float rip = __ldg(f.p[PRIP] + ip), rjp = __ldg(f.p[PRJP] + ip), rkp = __ldg(f.p[PRKP] + ip);
     float vx = 0.0f, vy = 0.0f, vz = 0.0f;
@@ -2344,6 +2353,7 @@ template <int F, typename T>
 __global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
 {
     CELL3D
+    if (g.nb > 1) shot_adj(g, a, shot);
     const float *hc = g.hc;
     float vzx = 0.0f, vzy = 0.0f, vzz = 0.0f, vyx = 0.0f, vyy = 0.0f, vyz = 0.0f, vxx = 0.0f, vxy = 0.0f, vxz = 0.0f;
     if (!g.bp2) {
@@ -2484,6 +2494,8 @@ __global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
 template <int F>
 __global__ void k_surfadj3d_a(Grid g, Fields f, AdjFields a, float *q)
 {
+    SHOT_FA
+    q += blockIdx.z * g.sb_q;
     int gy = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
     if (gy > g.NY - F - 1 || gx > g.NX - F - 1) return;
@@ -2509,6 +2521,8 @@ __global__ void k_surfadj3d_a(Grid g, Fields f, AdjFields a, float *q)
 template <int F>
 __global__ void k_surfadj3d_b(Grid g, Fields f, AdjFields a, const float *q)
 {
+    SHOT_FA
+    q += blockIdx.z * g.sb_q;
     int gy = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
     if (gy > g.NY - F - 1 || gx > g.NX - F - 1) return;
@@ -2691,11 +2705,11 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
 {
     if (g.fhalf && g.nd == 3) {   // FP16 storage: the vectorised or the streaming kernels
         if (q4_ok(g)) {
-            dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4));
+            dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4) * g.nb);
             k_v3d_q4<__half><<<gr, b, 0, st>>>(g, f);
             return;
         }
-        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
+        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
         DISPATCH_F(g.F, k_v3d_stream<FF, __half><<<gr, b, 0, st>>>(g, f));
         return;
     }
@@ -2715,11 +2729,11 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
             // 8 quads (32 z cells) x 4 y x 4 x per CTA: the y and x stencil
             // rows of neighbouring threads share L1 lines (0.35 ms at 256^3,
             // against 0.39 for 32 x 2 x 2)
-            dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4));
+            dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4) * g.nb);
             k_v3d_q4<float><<<gr, b, 0, st>>>(g, f);
             return;
         }
-        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
+        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
         if (g.kernels == 0 || g.kernels == 4 || g.kernels == 5) {
             DISPATCH_F(g.F, k_v3d_stream<FF><<<gr, b, 0, st>>>(g, f));
             return;
@@ -2735,7 +2749,7 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
 {
     if (g.fhalf && g.nd == 3 && g.L <= 3) {   // FP16 storage: the vectorised or the streaming kernels
         if (q4_ok(g)) {
-            dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1));
+            dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);
             switch (g.L) {
             case 0: k_s3d_q4<0, __half><<<g4, b4, 0, st>>>(g, f); break;
             case 1: k_s3d_q4<1, __half><<<g4, b4, 0, st>>>(g, f); break;
@@ -2744,7 +2758,7 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
             }
             return;
         }
-        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
+        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
         switch (g.L) {
         case 0: DISPATCH_F(g.F, k_s3d_stream<FF, 0, __half><<<gr, b, 0, st>>>(g, f)); break;
         case 1: DISPATCH_F(g.F, k_s3d_stream<FF, 1, __half><<<gr, b, 0, st>>>(g, f)); break;
@@ -2764,9 +2778,9 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
         return;
     }
     if (g.nd == 3) {
-        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
+        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
         if ((g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) {
-            dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1));  // 0.70 ms vs 0.71 (32 x 2 x 2)
+            dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);  // 0.70 ms vs 0.71 (32 x 2 x 2)
             switch (g.L) {
             case 0: k_s3d_q4<0, float><<<g4, b4, 0, st>>>(g, f); break;
             case 1: k_s3d_q4<1, float><<<g4, b4, 0, st>>>(g, f); break;
@@ -2842,7 +2856,7 @@ void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st)
     }
     if (g.nd == 22) return;
     if (g.nd == 3) {
-        dim3 b(32, 4), gr(cdiv(g.ny, 32), cdiv(g.nx, 4));
+        dim3 b(32, 4), gr(cdiv(g.ny, 32), cdiv(g.nx, 4), g.nb);
         if (g.fhalf) DISPATCH_F(g.F, k_surf3d<FF, __half><<<gr, b, 0, st>>>(g, f, pdir))
         else DISPATCH_F(g.F, k_surf3d<FF><<<gr, b, 0, st>>>(g, f, pdir))
     } else {
@@ -2864,7 +2878,7 @@ static void launch_adj_t(const Grid &g, const Fields &f, const AdjFields &a, boo
 {
     if (g.nd == 3 && (g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) {
         if (stress) {
-            dim3 b(16, 8, 1), gr(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1));
+            dim3 b(16, 8, 1), gr(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);
             switch (g.L) {
             case 0: k_adjs3d_q4<0, T><<<gr, b, 0, st>>>(g, f, a); break;
             case 1: k_adjs3d_q4<1, T><<<gr, b, 0, st>>>(g, f, a); break;
@@ -2872,13 +2886,13 @@ static void launch_adj_t(const Grid &g, const Fields &f, const AdjFields &a, boo
             default: k_adjs3d_q4<3, T><<<gr, b, 0, st>>>(g, f, a); break;
             }
         } else {
-            dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4));
+            dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4) * g.nb);
             k_adjv3d_q4<T><<<gr, b, 0, st>>>(g, f, a);
         }
         return;
     }
     if (g.nd == 3) {
-        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2));
+        dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
         if (stress) DISPATCH_F(g.F, k_adjs3d<FF, T><<<gr, b, 0, st>>>(g, f, a))
         else DISPATCH_F(g.F, k_adjv3d<FF, T><<<gr, b, 0, st>>>(g, f, a))
     } else {
@@ -2898,7 +2912,7 @@ void launch_update_adj(const Grid &g, const Fields &f, const AdjFields &a, bool 
 void launch_surface_adj(const Grid &g, const Fields &f, const AdjFields &a, float *q, cudaStream_t st)
 {
     if (g.nd == 3) {
-        dim3 b(32, 4), gr(cdiv(g.ny, 32), cdiv(g.nx, 4));
+        dim3 b(32, 4), gr(cdiv(g.ny, 32), cdiv(g.nx, 4), g.nb);
         DISPATCH_F(g.F, k_surfadj3d_a<FF><<<gr, b, 0, st>>>(g, f, a, q));
         DISPATCH_F(g.F, k_surfadj3d_b<FF><<<gr, b, 0, st>>>(g, f, a, q));
     } else {

@@ -76,16 +76,22 @@ def _key(cfg: engine.Config):
     return tuple((f.name, repr(getattr(cfg, f.name))) for f in dataclasses.fields(cfg))
 
 
-def plan_config(req: Request, max_batch: int = 8) -> engine.Config:
-    """The configuration of the plans serving ``req``: several shots of a 2D
-    P-SV or acoustic request advance together in one plan (``batch``, up to
-    ``max_batch``; acoustic gradients have no adjoint and are not batched).
-    A function of the request alone."""
+def plan_config(req: Request, max_batch: int = 8, batch_bytes: int = 8 << 30) -> engine.Config:
+    """The configuration of the plans serving ``req``: several shots of a
+    request advance together in one plan (``batch``: up to ``max_batch``
+    shots, as many as fit in ``batch_bytes`` of device memory; P-SV,
+    acoustic forward and 3D requests with FP32 fields).  A function of the
+    request alone."""
     c = req.config
     n = len(req.shots)
-    if n > 1 and max_batch > 1 and c.back_prop_type != 2 and (c.ND == 2 or (c.ND == 22 and req.kind == "forward")):
-        return dataclasses.replace(c, batch=min(n, max_batch))
-    return c
+    ok = (c.ND in (2, 3) or (c.ND == 22 and req.kind == "forward")) and c.back_prop_type != 2 and \
+        c.field_precision == "fp32" and c.kernels in ("fast", "general", "stream", "vector")
+    if n < 2 or max_batch < 2 or not ok:
+        return c
+    b = min(n, max_batch)
+    while b > 1 and request_footprint(req, dataclasses.replace(c, batch=b)) > batch_bytes:
+        b -= 1
+    return dataclasses.replace(c, batch=b) if b > 1 else c
 
 
 def request_footprint(req: Request, cfg: Optional[engine.Config] = None, max_batch: int = 8) -> int:

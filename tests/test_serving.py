@@ -182,8 +182,8 @@ def _multi_shot_request(nd, nshots, seed):
     from seiscl_b200 import serving
 
     q = _requests(1, seed=seed)[0]
-    if nd == 3:
-        q.config = dataclasses.replace(q.config, ND=3, N=[20, 20, 20])
+    if nd == 3:   # FP16 wave fields: not batched
+        q.config = dataclasses.replace(q.config, ND=3, N=[20, 20, 20], field_precision="fp16")
     sp, src, rp = q.shots[0]
     q.shots = [(sp, src, rp + np.float32(j)) for j in range(nshots)]
     q.kind = "gradient"
