@@ -55,7 +55,8 @@ GRADIENT_WORKLOADS = {
 
 
 def build_gradient_workload(name, nshots):
-    """Seeded true and starting models and the first ``nshots`` shots."""
+    """Seeded true and starting models and ``nshots`` shots (the workload's
+    shot positions, repeated when more are asked for)."""
     from scipy.ndimage import gaussian_filter
 
     w = dict(GRADIENT_WORKLOADS[name])
@@ -74,7 +75,7 @@ def build_gradient_workload(name, nshots):
         gx = np.linspace(w["nab"], nx - w["nab"] - 1, 500).astype(int)
         shots = []
         for i in range(nshots):
-            sp = np.array([[xs[i] * dh, 0, 5 * dh, i, w["src_type"]]], np.float32)
+            sp = np.array([[xs[i % w["nshots"]] * dh, 0, 5 * dh, i, w["src_type"]]], np.float32)
             rp = np.zeros((len(gx), 8), np.float32)
             rp[:, 0] = gx * dh
             rp[:, 2] = 5 * dh
@@ -100,7 +101,8 @@ def build_gradient_workload(name, nshots):
         gxx, gyy = np.meshgrid(g, g, indexing="ij")
         shots = []
         for i in range(nshots):
-            cx, cy = (2 * (i % 4) + 1) / 8.0 * nx, (2 * (i // 4) + 1) / 8.0 * ny
+            k = i % w["nshots"]   # the 4 x 4 shot grid, repeated
+            cx, cy = (2 * (k % 4) + 1) / 8.0 * nx, (2 * (k // 4) + 1) / 8.0 * ny
             sp = np.array([[cx * dh, cy * dh, 5 * dh, i, w["src_type"]]], np.float32)
             rp = np.zeros((gxx.size, 8), np.float32)
             rp[:, 0] = gxx.ravel() * dh
@@ -356,8 +358,9 @@ def run_reference_arm(args, w, model, acq):
 
 
 def run_gradient(args):
-    """Gradient workloads: per step one shot of forward (saving boundaries),
-    L2 residual against observed data, res_scale and adjoint.  Metric counts
+    """Gradient workloads: per step a batch of shots (``--batch``; default 8
+    in 2D, 1 in 3D) advanced together: forward (saving boundaries), L2
+    residual against observed data, res_scale and adjoint.  Metric counts
     both sweeps: cells * NT * 2 per shot."""
     import dataclasses
 
@@ -370,25 +373,29 @@ def run_gradient(args):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     if world > 1:
         raise SystemExit("gradient workloads run on one GPU per process without torchrun")
-    nuse = args.warmup + args.steps
+    B = args.batch if args.batch > 0 else (8 if GRADIENT_WORKLOADS[args.workload]["nd"] != 3 else 1)
+    nuse = (args.warmup + args.steps) * B
     w, true, start, shots = build_gradient_workload(args.workload, nuse)
     if args.nt > 0:
         w["nt"] = args.nt
         shots = [(sp, src[:, :args.nt].copy(), rp) for sp, src, rp in shots]
     outs = w["outputs"]
-    cfg = dataclasses.replace(engine_config(w), precision=w["precision"])
+    cfg = dataclasses.replace(engine_config(w), precision=w["precision"], batch=B)
     plan = Plan(cfg)
     plan.set_model(true["vp"], true["vs"], true["rho"])
-    obs = [plan.forward(sp, src, rp, outs) for sp, src, rp in shots]   # observed data, untimed
+    obs = []   # observed data, untimed
+    for i in range(0, nuse, B):
+        obs += plan.forward_batch(shots[i:i + B], outs)
     plan.set_model(start["vp"], start["vs"], start["rho"])
     plan.zero_gradient()
 
     def one(i):
-        sp, src, rp = shots[i]
-        d = plan.forward(sp, src, rp, outs, save_boundaries=True)
+        group = shots[i * B:(i + 1) * B]
+        ds = plan.forward_batch(group, outs, save_boundaries=True)
         ms = plan.last_loop_ms
-        res = {k: d[k] - obs[i][k] for k in outs}
-        plan.adjoint(sp, src, rp, plan.residual_scale(rp, res))
+        adj = [plan.residual_scale(rp, {k: d[k] - obs[i * B + j][k] for k in outs})
+               for j, ((sp, src, rp), d) in enumerate(zip(group, ds))]
+        plan.adjoint_batch(group, adj)
         return ms + plan.last_loop_ms
 
     for i in range(args.warmup):
@@ -399,23 +406,25 @@ def run_gradient(args):
     loop_ms = 0.0
     with clk:
         t0 = time.perf_counter()
-        for i in range(args.warmup, nuse):
+        for i in range(args.warmup, args.warmup + args.steps):
             loop_ms += one(i)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
     g = plan.gradient(transform=True)
     cells = w["nz"] * w["ny"] * w["nx"]
-    updates = cells * w["nt"] * 2 * args.steps
-    rec = shots[0][2].shape[0]
+    updates = cells * w["nt"] * 2 * args.steps * B
+    rec = shots[0][2].shape[0] * B
     print(json.dumps({
         "metric": "Gcell-updates/s", "value": round(updates / (loop_ms / 1e3) / 1e9, 3), "unit": "Gcell-updates/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(loop_ms / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "grid": [w["nz"], w["ny"], w["nx"]], "nt": w["nt"],
                    "fdorder": w["fdorder"], "boundaries": w["precision"], "outputs": outs,
-                   "step": "one shot: forward + residual + res_scale + adjoint (2 sweeps counted)"},
+                   "batch": B,
+                   "step": "%d shot(s) advanced together: forward + residual + res_scale + adjoint "
+                           "(2 sweeps counted)" % B},
         "e2e": {"value": round(updates / wall / 1e9, 3), "unit": "Gcell-updates/s",
-                "h2d_bytes_per_step": int(sum(a.nbytes for a in shots[0]) + len(outs) * rec * w["nt"] * 4),
+                "h2d_bytes_per_step": int(B * sum(a.nbytes for a in shots[0]) + len(outs) * rec * w["nt"] * 4),
                 "d2h_bytes_per_step": int(len(outs) * rec * w["nt"] * 4)},
         "gradient_finite": bool(all(np.isfinite(v).all() for k, v in g.items() if k in ("vp", "rho"))),
         "gpu_launches": None,
@@ -563,6 +572,7 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="serving: request arrival rate (1/s)")
     ap.add_argument("--workers", type=int, default=4, help="serving: worker threads")
     ap.add_argument("--no-plain", action="store_true", help="serving: skip the plain one-at-a-time arm")
+    ap.add_argument("--batch", type=int, default=0, help="gradient workloads: shots per step (0: 8 in 2D, 1 in 3D)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--ref-budget", type=float, default=15.0)
