@@ -274,6 +274,8 @@ int alloc_model(sfd_plan *p)
         p->f.cz[k] = cst + (2 * NC + k) * nc;
     }
     p->f.taper = cst + 3 * NC * nc;
+    p->d_ticket = (int *)dalloc(p, sizeof(int), &e);   // block counter of the fused steps
+    if (e) return fail(p, SFD_ERR_MEMORY, "step counter allocation failed");
     for (int ax = 0; ax < 3; ax++)
         for (int h = 0; h < 2; h++) p->f.kinv[ax][h] = cst + 3 * NC * nc + nc + (2 * ax + h) * nc;
     return SFD_OK;
@@ -782,7 +784,7 @@ extern "C" int sfd_footprint(const sfd_config *cfg, int gradient, int nsrc, int6
     // ensure_shot_buffers: source maps and signatures, receiver maps, seismograms and residuals
     const int64_t cs = std::max<int64_t>(nsrc, 16), cr = std::max<int64_t>(nrec_sel, 16);
     b += cs * (8 + 4 + 12 + 4 + 12 + 4 * nt) + cr * (8 + 8 * nt);
-    if (!gradient && (g.nd == 2 || g.nd == 22)) b += sizeof(int);   // fused-step block counter
+    b += sizeof(int);   // fused-step block counter
     if (gradient) {
         const bool bp2 = cfg->back_prop_type == 2;
         int ng = 0;
@@ -1004,17 +1006,15 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     // (time_stepping.c:819-822)
     Movie mv;
     if (!(save_boundaries && !dft) && (rc = movie_setup(p, omask, mv))) return rc;
-    // 2D P-SV / acoustic modelling: two launches per step (update_v; update_s
-    // with the free surface, the receivers and the next step's sources)
+    // modelling runs of 2D P-SV / acoustic grids: two launches per step
+    // (update_v; update_s with the free surface, the receivers and the next
+    // step's sources, the last two done by the block that finishes last).
+    // Not in 3D: there the last-block handshake costs each of the ~10^4
+    // blocks of a launch a fence and an atomic round trip, and a surface
+    // done by the top blocks of the stress kernel holds them on the SMs;
+    // both made a 256^3 step slower (1.31 and 1.19 ms against 1.13).
     const bool fuse2d = (g.nd == 2 || g.nd == 22) && g.kernels != 1 && !save_boundaries && !dft && !mv.n;
-    if (fuse2d) {
-        if (!p->d_ticket) {
-            cudaError_t e;
-            p->d_ticket = (int *)dalloc(p, sizeof(int), &e);
-            if (e) return fail(p, SFD_ERR_MEMORY, "step counter allocation failed");
-        }
-        CKC(cudaMemsetAsync(p->d_ticket, 0, sizeof(int), st));
-    }
+    if (fuse2d) CKC(cudaMemsetAsync(p->d_ticket, 0, sizeof(int), st));
     LoopKey key;
     key.add(mv.n); key.add(p->movout); key.add(p->d_mov); key.add(fuse2d); key.add(p->d_ticket);
     key.add(1); key.add(p->g); key.add(p->f); key.add_points(S); key.add_points(R); key.add(p->d_src);
