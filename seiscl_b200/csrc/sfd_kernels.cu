@@ -591,18 +591,25 @@ __device__ __forceinline__ void cpml_s3d(const Grid &g, const Fields &f, int gz,
 }
 
 // grid z: the x blocks of each shot of the launch, shot after shot
+#define SHOT3D                                                                         \
+    int shot = 0, xb_ = blockIdx.z;                                                    \
+    if (MB) {                                                                          \
+        const int nxb_ = gridDim.z / g.nb;                                             \
+        shot = blockIdx.z / nxb_;                                                      \
+        xb_ = blockIdx.z - shot * nxb_;                                                \
+    }
 #define CELL3D                                                                         \
-    const int nxb_ = gridDim.z / g.nb, shot = blockIdx.z / nxb_;                       \
+    SHOT3D                                                                             \
     int gz = blockIdx.x * blockDim.x + threadIdx.x + F;                                \
     int gy = blockIdx.y * blockDim.y + threadIdx.y + F;                                \
-    int gx = (blockIdx.z - shot * nxb_) * blockDim.z + threadIdx.z + F;                \
+    int gx = xb_ * blockDim.z + threadIdx.z + F;                                       \
     if (gz > g.NZ - F - 1 || gy > g.NY - F - 1 || gx > g.NX - F - 1) return;           \
-    if (g.nb > 1) shot_fields(g, f, shot);                                             \
+    if (MB) shot_fields(g, f, shot);                                                   \
     const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;                                        \
     i64 iv = gx * sx + (i64)gy * sy + gz;                                              \
     i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz - F);
 
-template <int F>
+template <int F, bool MB = false>
 __global__ void __launch_bounds__(256) k_v3d(Grid g, Fields f)
 {
     CELL3D
@@ -626,7 +633,7 @@ __global__ void __launch_bounds__(256) k_v3d(Grid g, Fields f)
     }
 }
 
-template <int F>
+template <int F, bool MB = false>
 __global__ void __launch_bounds__(256) k_s3d(Grid g, Fields f)
 {
     CELL3D
@@ -725,7 +732,7 @@ __device__ __forceinline__ void taper_regs(const Grid &g, const float *taper, in
     if (gx > g.NX - NAB - F - 1) mul(__ldg(taper + g.NX - F - gx - 1));
 }
 
-template <int F, class T = float>
+template <int F, class T = float, bool MB = false>
 __global__ void __launch_bounds__(256, 3) k_v3d_stream(Grid g, Fields f)
 {
     CELL3D
@@ -977,19 +984,25 @@ __device__ __forceinline__ void cpml_v3d_q4(const Grid &g, const Fields &f, int 
     }
 }
 
+// MB (a template parameter of the kernel): the launch covers several shots
 #define CELL3D_Q4                                                                      \
     constexpr int F = 4;                                                               \
-    const int nxb_ = gridDim.z / g.nb, shot = blockIdx.z / nxb_;                       \
+    int shot = 0, xb_ = blockIdx.z;                                                    \
+    if (MB) {                                                                          \
+        const int nxb_ = gridDim.z / g.nb;                                             \
+        shot = blockIdx.z / nxb_;                                                      \
+        xb_ = blockIdx.z - shot * nxb_;                                                \
+    }                                                                                  \
     const int gz0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4 + F;                   \
     const int gy = blockIdx.y * blockDim.y + threadIdx.y + F;                          \
-    const int gx = (blockIdx.z - shot * nxb_) * blockDim.z + threadIdx.z + F;          \
+    const int gx = xb_ * blockDim.z + threadIdx.z + F;                                 \
     if (gz0 > g.NZ - F - 1 || gy > g.NY - F - 1 || gx > g.NX - F - 1) return;          \
-    if (g.nb > 1) shot_fields(g, f, shot);                                             \
+    if (MB) shot_fields(g, f, shot);                                                   \
     const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;                                        \
     const i64 iv = gx * sx + (i64)gy * sy + gz0;                                       \
     const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
 
-template <class T>
+template <class T, bool MB = false>
 __global__ void __launch_bounds__(128) k_v3d_q4(Grid g, Fields f)
 {
     CELL3D_Q4
@@ -1253,7 +1266,7 @@ __device__ __forceinline__ void s_shear_q4(const Grid &g, const Fields &f, int g
     for (int q = 0; q < 3; q++) stq(ws[q] + iv, sq[q]);
 }
 
-template <int L, class T>
+template <int L, class T, bool MB = false>
 __global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f)
 {
     CELL3D_Q4
@@ -1291,11 +1304,11 @@ __device__ __forceinline__ void grad_add4(double *g, i64 ip, const float (&d)[4]
     p[1] = b;
 }
 
-template <typename T>
+template <typename T, bool MB = false>
 __global__ void __launch_bounds__(128) k_adjv3d_q4(Grid g, Fields f, AdjFields a)
 {
     CELL3D_Q4
-    if (g.nb > 1) shot_adj(g, a, shot);
+    if (MB) shot_adj(g, a, shot);
     const float *hc = g.hc;
     const Q4 rip = ldq(f.p[PRIP] + ip), rjp = ldq(f.p[PRJP] + ip), rkp = ldq(f.p[PRKP] + ip);
     Q4 vx = {{0, 0, 0, 0}}, vy = vx, vz = vx;
@@ -1427,11 +1440,11 @@ __device__ __forceinline__ void cpml_s3d_adj_q4(const Grid &g, const Fields &f, 
     }
 }
 
-template <int L, typename T>
+template <int L, typename T, bool MB = false>
 __global__ void __launch_bounds__(128, 4) k_adjs3d_q4(Grid g, Fields f, AdjFields a)
 {
     CELL3D_Q4
-    if (g.nb > 1) shot_adj(g, a, shot);
+    if (MB) shot_adj(g, a, shot);
     const float *hc = g.hc;
     // adjoint velocity derivatives, with CPML
     Q4 vzzr = dbw_z<F>(ldw(a.wr[VZ], iv), hc), vyzr = dfw_z<F>(ldw(a.wr[VY], iv), hc);
@@ -1708,7 +1721,7 @@ __global__ void __launch_bounds__(128, 4) k_adjs3d_q4(Grid g, Fields f, AdjField
 // true when the 4-cell kernels apply to this grid
 static inline bool q4_ok(const Grid &g) { return g.nd == 3 && g.F == 4 && g.nz % 4 == 0; }
 
-template <int F, int L, class T = float>
+template <int F, int L, class T = float, bool MB = false>
 __global__ void __launch_bounds__(256, 2) k_s3d_stream(Grid g, Fields f)
 {
     CELL3D
@@ -2306,11 +2319,11 @@ __global__ void k_surfadj2d_b(Grid g, Fields f, AdjFields a, const float *q)
 }
 
 // ------------------------------------------------------- adjoint kernels 3D
-template <int F, typename T>
+template <int F, typename T, bool MB = false>
 __global__ void __launch_bounds__(256) k_adjv3d(Grid g, Fields f, AdjFields a)
 {
     CELL3D
-    if (g.nb > 1) shot_adj(g, a, shot);
+    if (MB) shot_adj(g, a, shot);
     const float *hc = g.hc;
     float rip = __ldg(f.p[PRIP] + ip), rjp = __ldg(f.p[PRJP] + ip), rkp = __ldg(f.p[PRKP] + ip);
     float vx = 0.0f, vy = 0.0f, vz = 0.0f;
@@ -2349,11 +2362,11 @@ __global__ void __launch_bounds__(256) k_adjv3d(Grid g, Fields f, AdjFields a)
     if (!g.bp2) a.grad[GRHO][ip] += (double)(-vx * lvx - vy * lvy - vz * lvz);
 }
 
-template <int F, typename T>
+template <int F, typename T, bool MB = false>
 __global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
 {
     CELL3D
-    if (g.nb > 1) shot_adj(g, a, shot);
+    if (MB) shot_adj(g, a, shot);
     const float *hc = g.hc;
     float vzx = 0.0f, vzy = 0.0f, vzz = 0.0f, vyx = 0.0f, vyy = 0.0f, vyz = 0.0f, vxx = 0.0f, vxy = 0.0f, vxz = 0.0f;
     if (!g.bp2) {
@@ -2690,6 +2703,11 @@ __global__ void k_residuals(AdjFields a, PointSet r, const float *res, int nt_to
 // ------------------------------------------------------------- launchers
 static inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
 
+// batched launches (several shots) use the MB = true instantiations
+#define MB_DISPATCH(g, ...)                                                     \
+    if ((g).nb > 1) { constexpr bool MBV = true; __VA_ARGS__; }                  \
+    else { constexpr bool MBV = false; __VA_ARGS__; }
+
 #define DISPATCH_F(F, ...)                                                      \
     switch (F) {                                                               \
     case 1: { constexpr int FF = 1; __VA_ARGS__; } break;                      \
@@ -2730,15 +2748,15 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
             // rows of neighbouring threads share L1 lines (0.35 ms at 256^3,
             // against 0.39 for 32 x 2 x 2)
             dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4) * g.nb);
-            k_v3d_q4<float><<<gr, b, 0, st>>>(g, f);
+            MB_DISPATCH(g, k_v3d_q4<float, MBV><<<gr, b, 0, st>>>(g, f))
             return;
         }
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
         if (g.kernels == 0 || g.kernels == 4 || g.kernels == 5) {
-            DISPATCH_F(g.F, k_v3d_stream<FF><<<gr, b, 0, st>>>(g, f));
+            DISPATCH_F(g.F, MB_DISPATCH(g, k_v3d_stream<FF, float, MBV><<<gr, b, 0, st>>>(g, f)));
             return;
         }
-        DISPATCH_F(g.F, k_v3d<FF><<<gr, b, 0, st>>>(g, f));
+        DISPATCH_F(g.F, MB_DISPATCH(g, k_v3d<FF, MBV><<<gr, b, 0, st>>>(g, f)));
     } else {
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
         DISPATCH_F(g.F, k_v2d<FF><<<gr, b, 0, st>>>(g, f));
@@ -2782,23 +2800,23 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
         if ((g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) {
             dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);  // 0.70 ms vs 0.71 (32 x 2 x 2)
             switch (g.L) {
-            case 0: k_s3d_q4<0, float><<<g4, b4, 0, st>>>(g, f); break;
-            case 1: k_s3d_q4<1, float><<<g4, b4, 0, st>>>(g, f); break;
-            case 2: k_s3d_q4<2, float><<<g4, b4, 0, st>>>(g, f); break;
-            default: k_s3d_q4<3, float><<<g4, b4, 0, st>>>(g, f); break;
+            case 0: MB_DISPATCH(g, k_s3d_q4<0, float, MBV><<<g4, b4, 0, st>>>(g, f)) break;
+            case 1: MB_DISPATCH(g, k_s3d_q4<1, float, MBV><<<g4, b4, 0, st>>>(g, f)) break;
+            case 2: MB_DISPATCH(g, k_s3d_q4<2, float, MBV><<<g4, b4, 0, st>>>(g, f)) break;
+            default: MB_DISPATCH(g, k_s3d_q4<3, float, MBV><<<g4, b4, 0, st>>>(g, f)) break;
             }
             return;
         }
         if ((g.kernels == 0 || g.kernels == 4 || g.kernels == 5) && g.L <= 3) {
             switch (g.L) {
-            case 0: DISPATCH_F(g.F, k_s3d_stream<FF, 0><<<gr, b, 0, st>>>(g, f)); break;
-            case 1: DISPATCH_F(g.F, k_s3d_stream<FF, 1><<<gr, b, 0, st>>>(g, f)); break;
-            case 2: DISPATCH_F(g.F, k_s3d_stream<FF, 2><<<gr, b, 0, st>>>(g, f)); break;
-            default: DISPATCH_F(g.F, k_s3d_stream<FF, 3><<<gr, b, 0, st>>>(g, f)); break;
+            case 0: DISPATCH_F(g.F, MB_DISPATCH(g, k_s3d_stream<FF, 0, float, MBV><<<gr, b, 0, st>>>(g, f))); break;
+            case 1: DISPATCH_F(g.F, MB_DISPATCH(g, k_s3d_stream<FF, 1, float, MBV><<<gr, b, 0, st>>>(g, f))); break;
+            case 2: DISPATCH_F(g.F, MB_DISPATCH(g, k_s3d_stream<FF, 2, float, MBV><<<gr, b, 0, st>>>(g, f))); break;
+            default: DISPATCH_F(g.F, MB_DISPATCH(g, k_s3d_stream<FF, 3, float, MBV><<<gr, b, 0, st>>>(g, f))); break;
             }
             return;
         }
-        DISPATCH_F(g.F, k_s3d<FF><<<gr, b, 0, st>>>(g, f));
+        DISPATCH_F(g.F, MB_DISPATCH(g, k_s3d<FF, MBV><<<gr, b, 0, st>>>(g, f)));
     } else {
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
         DISPATCH_F(g.F, k_s2d<FF><<<gr, b, 0, st>>>(g, f));
@@ -2880,21 +2898,21 @@ static void launch_adj_t(const Grid &g, const Fields &f, const AdjFields &a, boo
         if (stress) {
             dim3 b(16, 8, 1), gr(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);
             switch (g.L) {
-            case 0: k_adjs3d_q4<0, T><<<gr, b, 0, st>>>(g, f, a); break;
-            case 1: k_adjs3d_q4<1, T><<<gr, b, 0, st>>>(g, f, a); break;
-            case 2: k_adjs3d_q4<2, T><<<gr, b, 0, st>>>(g, f, a); break;
-            default: k_adjs3d_q4<3, T><<<gr, b, 0, st>>>(g, f, a); break;
+            case 0: MB_DISPATCH(g, k_adjs3d_q4<0, T, MBV><<<gr, b, 0, st>>>(g, f, a)) break;
+            case 1: MB_DISPATCH(g, k_adjs3d_q4<1, T, MBV><<<gr, b, 0, st>>>(g, f, a)) break;
+            case 2: MB_DISPATCH(g, k_adjs3d_q4<2, T, MBV><<<gr, b, 0, st>>>(g, f, a)) break;
+            default: MB_DISPATCH(g, k_adjs3d_q4<3, T, MBV><<<gr, b, 0, st>>>(g, f, a)) break;
             }
         } else {
             dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4) * g.nb);
-            k_adjv3d_q4<T><<<gr, b, 0, st>>>(g, f, a);
+            MB_DISPATCH(g, k_adjv3d_q4<T, MBV><<<gr, b, 0, st>>>(g, f, a))
         }
         return;
     }
     if (g.nd == 3) {
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
-        if (stress) DISPATCH_F(g.F, k_adjs3d<FF, T><<<gr, b, 0, st>>>(g, f, a))
-        else DISPATCH_F(g.F, k_adjv3d<FF, T><<<gr, b, 0, st>>>(g, f, a))
+        if (stress) DISPATCH_F(g.F, MB_DISPATCH(g, k_adjs3d<FF, T, MBV><<<gr, b, 0, st>>>(g, f, a)))
+        else DISPATCH_F(g.F, MB_DISPATCH(g, k_adjv3d<FF, T, MBV><<<gr, b, 0, st>>>(g, f, a)))
     } else {
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
         if (stress) DISPATCH_F(g.F, k_adjs2d<FF, T><<<gr, b, 0, st>>>(g, f, a))
