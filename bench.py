@@ -374,13 +374,16 @@ def run_gradient(args):
     if world > 1:
         raise SystemExit("gradient workloads run on one GPU per process without torchrun")
     B = args.batch if args.batch > 0 else (8 if GRADIENT_WORKLOADS[args.workload]["nd"] != 3 else 1)
+    if args.checkpoint:
+        B = 1   # checkpointed gradients run one shot per launch
     nuse = (args.warmup + args.steps) * B
     w, true, start, shots = build_gradient_workload(args.workload, nuse)
     if args.nt > 0:
         w["nt"] = args.nt
         shots = [(sp, src[:, :args.nt].copy(), rp) for sp, src, rp in shots]
     outs = w["outputs"]
-    cfg = dataclasses.replace(engine_config(w), precision=w["precision"], batch=B)
+    cfg = dataclasses.replace(engine_config(w), precision=w["precision"], batch=B,
+                              checkpoint=args.checkpoint)
     plan = Plan(cfg)
     plan.set_model(true["vp"], true["vs"], true["rho"])
     obs = []   # observed data, untimed
@@ -421,6 +424,8 @@ def run_gradient(args):
         "config": {"workload": args.workload, "grid": [w["nz"], w["ny"], w["nx"]], "nt": w["nt"],
                    "fdorder": w["fdorder"], "boundaries": w["precision"], "outputs": outs,
                    "batch": B,
+                   "recompute": ("snapshots every %d steps" % args.checkpoint) if args.checkpoint
+                   else "saved boundaries, backpropagation",
                    "step": "%d shot(s) advanced together: forward + residual + res_scale + adjoint "
                            "(2 sweeps counted)" % B},
         "e2e": {"value": round(updates / wall / 1e9, 3), "unit": "Gcell-updates/s",
@@ -573,6 +578,8 @@ def main():
     ap.add_argument("--workers", type=int, default=4, help="serving: worker threads")
     ap.add_argument("--no-plain", action="store_true", help="serving: skip the plain one-at-a-time arm")
     ap.add_argument("--batch", type=int, default=0, help="gradient workloads: shots per step (0: 8 in 2D, 1 in 3D)")
+    ap.add_argument("--checkpoint", type=int, default=0,
+                    help="gradient workloads: snapshot every K steps and recompute (0: saved boundaries)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--ref-budget", type=float, default=15.0)

@@ -118,6 +118,18 @@ typedef struct sfd_config {
                               launch covering all of them.  No reference counterpart
                               (the reference runs the shots of a group one by one,
                               time_stepping.c:705-722). */
+    int checkpoint;        /* gradient recompute strategy: 0 saves the boundary shells and
+                              backpropagates the forward field (BACK_PROP_TYPE 1, the
+                              reference's); K > 0 keeps a snapshot of the whole forward
+                              state every K steps and, during the adjoint, recomputes each
+                              K-step segment forward from its snapshot, storing the wave
+                              fields of every step of the segment: the adjoint reads the
+                              forward field instead of reconstructing it (no boundary
+                              store; memory: (nt/K) snapshots + K wave-field states, in
+                              `precision`, CPML memory in FP32).  P-SV and 3D, batch 1,
+                              FP32 wave fields.  The reference's INPUTRES checkpoint
+                              (time_stepping.c:92-270) saves the final state and the
+                              boundaries instead. */
 } sfd_config;
 
 typedef struct sfd_shot {

@@ -487,6 +487,177 @@ int run_loop(sfd_plan *p, sfd_plan::LoopGraph &lg, const std::string &key, cudaS
     return SFD_OK;
 }
 
+// --------------------------------------------------- checkpointed gradients
+// A snapshot holds the wave fields and memory variables in the store type of
+// `precision` (FP16 with the power-of-two scales of the saved boundaries)
+// and the CPML memory in FP32, in that order; the segment store holds the
+// wave fields of each step of a K-step segment.
+struct CkptSizes {
+    int nwave, nmem, K, nseg;
+    int64_t psi;            // CPML floats
+    size_t elem, snap, seg;
+};
+CkptSizes ckpt_sizes(const Grid &g, const sfd_config &c)
+{
+    CkptSizes z;
+    z.nwave = z.nmem = 0;
+    for (int w = 0; w < NW; w++) z.nwave += is_wave_used(g, w);
+    for (int r = 0; r < NR; r++) z.nmem += is_mem_used(g, r);
+    int64_t psz[NPSI];
+    z.psi = psi_sizes(g, psz);
+    const int tmax = (c.tmax > 0 && c.tmax <= c.nt) ? c.tmax : c.nt;
+    z.K = std::max(1, std::min(c.checkpoint, tmax));
+    z.nseg = (tmax + z.K - 1) / z.K;
+    z.elem = c.precision == SFD_PREC_FP32 ? 4 : 2;
+    z.snap = z.elem * g.nvol * (z.nwave + (size_t)z.nmem * g.L) + sizeof(float) * z.psi;
+    z.seg = z.elem * g.nvol * z.nwave * (size_t)z.K;
+    return z;
+}
+
+int alloc_ckpt(sfd_plan *p)
+{
+    const CkptSizes z = ckpt_sizes(p->g, p->cfg);
+    if (p->d_snap) return SFD_OK;
+    cudaError_t e;
+    p->d_snap = (char *)dalloc(p, z.snap * z.nseg, &e);
+    if (!p->d_snap) return fail(p, SFD_ERR_MEMORY, "checkpoint snapshots do not fit in device memory");
+    p->d_seg = (char *)dalloc(p, z.seg, &e);
+    if (!p->d_seg) return fail(p, SFD_ERR_MEMORY, "checkpoint segment store does not fit in device memory");
+    p->d_psi_adj = (float *)dalloc(p, sizeof(float) * std::max<int64_t>(z.psi, 1), &e);
+    if (!p->d_psi_adj) return fail(p, SFD_ERR_MEMORY, "adjoint CPML allocation failed");
+    p->snap_bytes = z.snap;
+    p->seg_bytes = z.seg;
+    p->nseg = z.nseg;
+    return SFD_OK;
+}
+
+// wave fields (and memory variables) <-> snapshot j
+void ckpt_snapshot(sfd_plan *p, int j, bool load, cudaStream_t st)
+{
+    const Grid &g = p->g;
+    const CkptSizes z = ckpt_sizes(g, p->cfg);
+    char *base = p->d_snap + (size_t)j * p->snap_bytes;
+    PackSet ps;
+    memset(&ps, 0, sizeof ps);
+    size_t off = 0;
+    for (int w = 0; w < NW; w++) {
+        if (!p->f.w[w]) continue;
+        ps.src[ps.narr] = load ? (const void *)(base + off) : (const void *)p->f.w[w];
+        ps.dst[ps.narr] = load ? (void *)p->f.w[w] : (void *)(base + off);
+        ps.n[ps.narr] = g.nvol;
+        ps.scale[ps.narr] = load ? g.bsci[w] : g.bsc[w];
+        ps.narr++;
+        off += z.elem * g.nvol;
+    }
+    for (int r = 0; r < NR; r++) {   // memory variables: the scale of the stresses
+        if (!p->f.r[r]) continue;
+        ps.src[ps.narr] = load ? (const void *)(base + off) : (const void *)p->f.r[r];
+        ps.dst[ps.narr] = load ? (void *)p->f.r[r] : (void *)(base + off);
+        ps.n[ps.narr] = g.nvol * g.L;
+        ps.scale[ps.narr] = load ? g.bsci[SXX] : g.bsc[SXX];
+        ps.narr++;
+        off += z.elem * g.nvol * g.L;
+    }
+    launch_pack(ps, p->cfg.precision, load, st);
+    if (z.psi) {
+        float *sp = (float *)(base + off);
+        if (load) cudaMemcpyAsync(p->d_psi_all, sp, sizeof(float) * z.psi, cudaMemcpyDeviceToDevice, st);
+        else cudaMemcpyAsync(sp, p->d_psi_all, sizeof(float) * z.psi, cudaMemcpyDeviceToDevice, st);
+    }
+}
+
+// the wave fields now -> slot k of the segment store; the stored fields of
+// slot k as the adjoint kernels read them
+void ckpt_store(sfd_plan *p, int k, cudaStream_t st)
+{
+    const Grid &g = p->g;
+    const CkptSizes z = ckpt_sizes(g, p->cfg);
+    PackSet ps;
+    memset(&ps, 0, sizeof ps);
+    char *base = p->d_seg + (size_t)k * z.elem * g.nvol * z.nwave;
+    for (int w = 0; w < NW; w++) {
+        if (!p->f.w[w]) continue;
+        ps.src[ps.narr] = p->f.w[w];
+        ps.dst[ps.narr] = base + z.elem * g.nvol * ps.narr;
+        ps.n[ps.narr] = g.nvol;
+        ps.scale[ps.narr] = g.bsc[w];
+        ps.narr++;
+    }
+    launch_pack(ps, p->cfg.precision, false, st);
+}
+void ckpt_slot(const sfd_plan *p, int k, AdjFields &a)
+{
+    const Grid &g = p->g;
+    const CkptSizes z = ckpt_sizes(g, p->cfg);
+    const char *base = p->d_seg + (size_t)k * z.elem * g.nvol * z.nwave;
+    int q = 0;
+    for (int w = 0; w < NW; w++) {
+        a.fwd[w] = nullptr;
+        if (!p->f.w[w]) continue;
+        a.fwd[w] = base + z.elem * g.nvol * q++;
+    }
+}
+
+// The checkpointed adjoint: per K-step segment, from the last one, the
+// forward run recomputed from the segment's snapshot (storing the wave
+// fields of each step after its sources, before update_v: the fields that
+// backpropagation would have reconstructed), then the adjoint steps of the
+// segment, the same launches as the boundary-saving adjoint minus the
+// reconstruction, injection and source removal.
+int adjoint_ckpt(sfd_plan *p, const PointSet &S, const PointSet &R, unsigned omask, cudaStream_t st)
+{
+    const Grid &g = p->g;
+    const CkptSizes z = ckpt_sizes(g, p->cfg);
+    const int NT = p->cfg.nt, tmax = p->cfg.tmax, tmin = p->cfg.tmin;
+    // the adjoint's CPML memory: the forward run's (the reference binds the
+    // same buffers, src/clprogram.c:806-811) or zero
+    if (z.psi) {
+        if (p->cfg.adjoint_reset_psi) CKC(cudaMemsetAsync(p->d_psi_adj, 0, sizeof(float) * z.psi, st));
+        else CKC(cudaMemcpyAsync(p->d_psi_adj, p->d_psi_all, sizeof(float) * z.psi, cudaMemcpyDeviceToDevice, st));
+    }
+    Fields fa = p->f;
+    for (int i = 0; i < NPSI; i++)
+        fa.psi[i] = p->f.psi[i] ? p->d_psi_adj + (p->f.psi[i] - p->d_psi_all) : nullptr;
+    Grid ga = g;
+    ga.ckpt = 1;
+    AdjFields a = p->a;
+    for (int w = 0; w < NW; w++) a.bnd[w] = nullptr;
+    LoopKey key;
+    key.add(4); key.add(ga); key.add(p->f); key.add(fa); key.add(a); key.add_points(S); key.add_points(R);
+    key.add(p->d_src); key.add(p->d_res); key.add(p->d_surf_q); key.add(omask); key.add(p->d_snap); key.add(p->d_seg);
+    key.add(p->cfg.precision); key.add(tmax); key.add(tmin); key.add(z.K);
+    CKC(cudaEventRecord(p->ev0, st));
+    int rcl = run_loop(p, p->gadj, key.s, st, [&](cudaStream_t s) {
+        for (int j = z.nseg - 1; j >= 0; j--) {
+            const int t0 = j * z.K, thi = std::min(t0 + z.K, tmax) - 1, tlo = std::max(t0, tmin + 1);
+            if (thi < tlo) continue;
+            ckpt_snapshot(p, j, true, s);
+            for (int t = t0; t <= thi; t++) {
+                launch_sources(g, p->f, S, p->d_src, NT, t, 1, s);
+                ckpt_store(p, t - t0, s);
+                if (t == thi) break;
+                launch_update_v(g, p->f, s);
+                launch_update_s(g, p->f, s);
+                if (g.freesurf) launch_surface(g, p->f, 1, s);
+            }
+            for (int t = thi; t >= tlo; t--) {
+                ckpt_slot(p, t - t0, a);
+                if (g.freesurf) launch_surface_adj(ga, fa, a, p->d_surf_q, s);
+                launch_residuals(ga, a, R, p->d_res, NT, t, omask, s);
+                launch_update_adj(ga, fa, a, true, p->cfg.precision, s);
+                launch_update_adj(ga, fa, a, false, p->cfg.precision, s);
+            }
+        }
+    });
+    if (rcl) return rcl;
+    CKC(cudaEventRecord(p->ev1, st));
+    CKC(cudaGetLastError());
+    CKC(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1);
+    p->have_forward = false;
+    return SFD_OK;
+}
+
 // ---------------------------------------------------------- DFT gradient
 constexpr double PI_D = 3.141592653589793238462643383279502884197169;
 
@@ -662,6 +833,11 @@ int check_config(const sfd_config &c)
     // the reference's 3D Hessian kernel does not compile (update_adjv3D.cl:486)
     if (c.hout && c.nd == 3 && c.back_prop_type != 2) return SFD_ERR_UNSUPPORTED;
     if (c.batch < 0 || c.batch > 64) return SFD_ERR_ARG;
+    if (c.checkpoint < 0) return SFD_ERR_ARG;
+    // checkpointed gradients: boundary-saving semantics on P-SV and 3D grids, one shot per launch
+    if (c.checkpoint > 0 && (c.back_prop_type == 2 || (c.nd != 2 && c.nd != 3) || c.batch > 1 ||
+                             c.field_precision != 0))
+        return SFD_ERR_UNSUPPORTED;
     // batched shots: P-SV, acoustic and 3D one-cell / 4-cell kernels in FP32,
     // boundary-saving gradients
     if (c.batch > 1 && (c.nd == 21 || c.back_prop_type == 2 || c.field_precision != 0 || c.kernels == 2 ||
@@ -741,6 +917,10 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     p->dev_bytes = 0;
     p->batch = std::max(1, c.batch);
     p->fwd_nb = 0;
+    p->d_snap = p->d_seg = nullptr;
+    p->d_psi_adj = nullptr;
+    p->snap_bytes = p->seg_bytes = 0;
+    p->nseg = 0;
     memset(&p->f, 0, sizeof p->f);
     memset(&p->a, 0, sizeof p->a);
     p->last_ms = 0.0f;
@@ -794,7 +974,12 @@ extern "C" int sfd_footprint(const sfd_config *cfg, int gradient, int nsrc, int6
             b += 2 * 8 * (int64_t)nfreqs * g.nvol * (nwave + (int64_t)nmem * g.L);
         } else {
             b += B * 4 * g.nvol * (nwave + (int64_t)nmem * g.L);
-            b += B * (int64_t)(cfg->precision == SFD_PREC_FP32 ? 4 : 2) * nt * g.nbnd * nwave;
+            if (cfg->checkpoint > 0) {   // snapshots, segment store, adjoint CPML memory
+                const CkptSizes z = ckpt_sizes(g, *cfg);
+                b += (int64_t)(z.snap * z.nseg + z.seg) + 4 * std::max<int64_t>(z.psi, 1);
+            } else {
+                b += B * (int64_t)(cfg->precision == SFD_PREC_FP32 ? 4 : 2) * nt * g.nbnd * nwave;
+            }
         }
     }
     *bytes = b;
@@ -978,12 +1163,16 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     // a gradient run keeps the boundary shells (BACK_PROP_TYPE 1) or the
     // forward transforms (2)
     const bool dft = save_boundaries && p->cfg.back_prop_type == 2;
+    const bool ckpt = save_boundaries && !dft && p->cfg.checkpoint > 0;
     if (dft) {
         if (g.nd == 21 || g.nd == 22)
             return fail(p, SFD_ERR_UNSUPPORTED, "the adjoint path covers P-SV and 3D elastic/viscoelastic media");
         if (!p->nfreqs) return fail(p, SFD_ERR_STATE, "sfd_set_gradfreqs must be called before a DFT-gradient run");
         if ((rc = alloc_dft(p))) return rc;
         if ((rc = zero_dft(p, 0, st))) return rc;
+    } else if (save_boundaries && p->cfg.checkpoint > 0) {
+        if (p->movout > 0) return fail(p, SFD_ERR_UNSUPPORTED, "a checkpointed gradient films no movie");
+        if ((rc = alloc_ckpt(p))) return rc;
     } else if (save_boundaries) {
         if (g.nd == 21 || g.nd == 22)
             return fail(p, SFD_ERR_UNSUPPORTED, "the adjoint path covers P-SV and 3D elastic/viscoelastic media");
@@ -1019,7 +1208,7 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     key.add(mv.n); key.add(p->movout); key.add(p->d_mov); key.add(fuse2d); key.add(p->d_ticket);
     key.add(1); key.add(p->g); key.add(p->f); key.add_points(S); key.add_points(R); key.add(p->d_src);
     key.add(p->d_seis); key.add(omask); key.add(dft); key.add(save_boundaries != 0); key.add(bs);
-    key.add(p->cfg.precision); key.add(tmax); key.add(tmin);
+    key.add(p->cfg.precision); key.add(tmax); key.add(tmin); key.add(ckpt); key.add(p->d_snap);
     if (dft) {
         key.add(p->nfreqs); key.add(p->dtnyq); key.add(p->ntnyq); key.add(p->gradfreqsn); key.add(p->d_fw);
         key.add(p->d_fr);
@@ -1038,10 +1227,11 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
         for (int t = 0; t < tmax; t++) {
             // the state after t steps, before the sources of step t (time_stepping.c:766-781)
             if (dft && t >= tmin && (t - tmin) % p->dtnyq == 0) dft_sample(p, 0, (t - tmin) / p->dtnyq, s);
+            if (ckpt && t % p->cfg.checkpoint == 0) ckpt_snapshot(p, t / p->cfg.checkpoint, false, s);
             launch_sources(g, p->f, S, p->d_src, NT, t, 1, s);
             launch_update_v(g, p->f, s);
             launch_update_s(g, p->f, s);
-            if (save_boundaries && !dft) launch_savebnd(g, p->f, bs, p->cfg.precision, (int64_t)t * g.nbnd, s);
+            if (save_boundaries && !dft && !ckpt) launch_savebnd(g, p->f, bs, p->cfg.precision, (int64_t)t * g.nbnd, s);
             if (g.freesurf) launch_surface(g, p->f, 1, s);
             launch_record(g, p->f, R, p->d_seis, NT, t, omask, s);
             if (mv.n && (t + 1) % p->movout == 0) movie_snap(p, mv, (t + 1) / p->movout - 1, s);
@@ -1117,6 +1307,7 @@ extern "C" int sfd_adjoint_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
         if (p->a.wr[w]) CKC(cudaMemsetAsync(p->a.wr[w], 0, sizeof(float) * g.nvol * nshot, st));
     for (int r = 0; r < NR; r++)
         if (p->a.rr[r]) CKC(cudaMemsetAsync(p->a.rr[r], 0, sizeof(float) * g.nvol * g.L * nshot, st));
+    if (p->cfg.checkpoint > 0) return adjoint_ckpt(p, S, R, omask, st);
     if (p->cfg.adjoint_reset_psi) {
         // optional: start the adjoint with clean CPML memory instead
         int64_t tot = 0;

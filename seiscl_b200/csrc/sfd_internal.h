@@ -66,6 +66,8 @@ struct Grid {
     int bp2;                // adjoint kernels: 1 for the DFT gradient (no reconstruction,
                             // boundary injection or on-the-fly gradient)
     int hout;               // accumulate the approximate Hessian
+    int ckpt;               // adjoint kernels: the forward field comes from a.fwd (checkpointed
+                            // gradient), not from backpropagation and boundary injection
     // batched shots (2D): the launch covers nb shots, blockIdx.z = shot; shot
     // b works on copy b of each per-shot array, these strides apart
     int nb;
@@ -92,6 +94,7 @@ struct AdjFields {
     double *grad[NG];
     double *hess[NG];       // approximate Hessian (HOUT), same layout as grad
     const void *bnd[NW];    // slice t-1 of the saved boundaries
+    const void *fwd[NW];    // checkpointed gradients: the forward wave fields of the step
 };
 
 struct PointSet {           // sources or receivers of one shot, device side
@@ -146,6 +149,12 @@ struct sfd_plan {
     float *d_src_div, *d_src, *d_seis, *d_res;
     float *d_surf_q;        // surface-adjoint scratch [nx][ny]
     int *d_ticket;          // fused 2D steps: block counter of the stress launch
+    // checkpointed gradients (cfg.checkpoint = K > 0)
+    char *d_snap;           // [nseg] snapshots: wave fields, memory variables (store type), CPML (FP32)
+    char *d_seg;            // [K][wave fields] of the segment being backpropagated (store type)
+    float *d_psi_adj;       // the adjoint's CPML memory
+    size_t snap_bytes, seg_bytes;
+    int nseg;
     int batch;              // copies of the per-shot arrays (shots per launch)
     int fwd_nb;             // shots of the forward run whose boundaries are saved
     cudaEvent_t ev0, ev1;

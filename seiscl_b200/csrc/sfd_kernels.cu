@@ -161,6 +161,15 @@ __device__ __forceinline__ float bnd_at(const Grid &g, const AdjFields &a, int w
     return to_f<T>(((const T *)a.bnd[w])[m]) * g.bsci[w];
 }
 
+// checkpointed gradients (g.ckpt): the forward wave field of the adjoint
+// step, stored when the forward run was recomputed from a snapshot (same
+// storage type and scales as the saved boundaries)
+template <class T>
+__device__ __forceinline__ float fwd_at(const Grid &g, const AdjFields &a, int w, i64 iv)
+{
+    return to_f<T>(((const T *)a.fwd[w])[iv]) * g.bsci[w];
+}
+
 // ------------------------------------------------------- boundary shells
 struct BndDims {
     int NXbnd, NYbnd, NZbnd, lbnd, lbnds;
@@ -1312,7 +1321,14 @@ __global__ void __launch_bounds__(128) k_adjv3d_q4(Grid g, Fields f, AdjFields a
     const float *hc = g.hc;
     const Q4 rip = ldq(f.p[PRIP] + ip), rjp = ldq(f.p[PRJP] + ip), rkp = ldq(f.p[PRKP] + ip);
     Q4 vx = {{0, 0, 0, 0}}, vy = vx, vz = vx;
-    if (!g.bp2) {  // backpropagate the forward velocities (update_adjv3D.cl:297-340)
+    if (g.ckpt) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            vx.v[j] = fwd_at<T>(g, a, VX, iv + j);
+            vy.v[j] = fwd_at<T>(g, a, VY, iv + j);
+            vz.v[j] = fwd_at<T>(g, a, VZ, iv + j);
+        }
+    } else if (!g.bp2) {  // backpropagate the forward velocities (update_adjv3D.cl:297-340)
         Q4 szz_z = dfw_z<F>(ldw(f.w[SZZ], iv), hc);
         Q4 sxx_x = dfw_q<F>(f.w[SXX], iv, sx, hc);
         Q4 sxz_x = dbw_q<F>(f.w[SXZ], iv, sx, hc);
@@ -1470,7 +1486,12 @@ __global__ void __launch_bounds__(128, 4) k_adjs3d_q4(Grid g, Fields f, AdjField
         Q4 qtaup = {{0, 0, 0, 0}}, qtaus = qtaup;
         if (L > 0) { qtaup = ldq(f.p[PTAUP] + ip); qtaus = ldq(f.p[PTAUS] + ip); }
         Q4 s3[3] = {{{0, 0, 0, 0}}, {{0, 0, 0, 0}}, {{0, 0, 0, 0}}};
-        if (!g.bp2) {
+        if (g.ckpt) {
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) s3[c].v[j] = fwd_at<T>(g, a, wid[c], iv + j);
+        } else if (!g.bp2) {
             const Q4 vzz = dbw_z<F>(ldw(f.w[VZ], iv), hc);
             const Q4 vyy = dbw_q<F>(f.w[VY], iv, sy, hc);
             const Q4 vxx = dbw_q<F>(f.w[VX], iv, sx, hc);
@@ -1620,7 +1641,10 @@ __global__ void __launch_bounds__(128, 4) k_adjs3d_q4(Grid g, Fields f, AdjField
         Q4 qtauc = {{0, 0, 0, 0}};
         if (L > 0) qtauc = ldq(f.p[ptau] + ip);
         Q4 sc = {{0, 0, 0, 0}};
-        if (!g.bp2) {
+        if (g.ckpt) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) sc.v[j] = fwd_at<T>(g, a, wid, iv + j);
+        } else if (!g.bp2) {
             Q4 d1, d2;   // forward derivative pair (vxy+vyx, vyz+vzy, vxz+vzx)
             if (c == 0) { d1 = dfw_q<F>(f.w[VX], iv, sy, hc); d2 = dfw_q<F>(f.w[VY], iv, sx, hc); }
             else if (c == 1) { d1 = dfw_z<F>(ldw(f.w[VY], iv), hc); d2 = dfw_q<F>(f.w[VZ], iv, sy, hc); }
@@ -2112,7 +2136,10 @@ __global__ void __launch_bounds__(256) k_adjv2d(Grid g, Fields f, AdjFields a)
     const float *hc = g.hc;
     float rip = __ldg(f.p[PRIP] + ip), rkp = __ldg(f.p[PRKP] + ip);
     float vx = 0.0f, vz = 0.0f;
-    if (!g.bp2) {  // backpropagate the forward velocities (update_adjv2D.cl:205-240)
+    if (g.ckpt) {
+        vx = fwd_at<T>(g, a, VX, iv);
+        vz = fwd_at<T>(g, a, VZ, iv);
+    } else if (!g.bp2) {  // backpropagate the forward velocities (update_adjv2D.cl:205-240)
         float sxx_x = dfw<F>(f.w[SXX], iv, g.NZ, hc);
         float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc);
         float sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
@@ -2153,7 +2180,7 @@ __global__ void __launch_bounds__(256) k_adjs2d(Grid g, Fields f, AdjFields a)
     i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
     const float *hc = g.hc;
     float vxx = 0.0f, vxz = 0.0f, vzz = 0.0f, vzx = 0.0f;
-    if (!g.bp2) {
+    if (!g.bp2 && !g.ckpt) {
         vxx = dbw<F>(f.w[VX], iv, g.NZ, hc); vxz = dfw<F>(f.w[VX], iv, 1, hc);
         vzz = dbw<F>(f.w[VZ], iv, 1, hc); vzx = dfw<F>(f.w[VZ], iv, g.NZ, hc);
     }
@@ -2178,6 +2205,8 @@ __global__ void __launch_bounds__(256) k_adjs2d(Grid g, Fields f, AdjFields a)
     float sxx = 0.0f, szz = 0.0f, sxz = 0.0f;
     // reconstruct the forward stresses (update_adjs2D.cl:222-278)
     if (g.bp2) {
+    } else if (g.ckpt) {
+        sxx = fwd_at<T>(g, a, SXX, iv); szz = fwd_at<T>(g, a, SZZ, iv); sxz = fwd_at<T>(g, a, SXZ, iv);
     } else if (L == 0) {
         sxx = f.w[SXX][iv]; szz = f.w[SZZ][iv]; sxz = f.w[SXZ][iv];
         sxz -= fipkp * (vxz + vzx);
@@ -2206,7 +2235,7 @@ __global__ void __launch_bounds__(256) k_adjs2d(Grid g, Fields f, AdjFields a)
         sxx -= lsxx + g.dt2 * s2;
         szz -= lszz + g.dt2 * s3;
     }
-    if (!g.bp2) {
+    if (!g.bp2 && !g.ckpt) {
         int m = inject_ind2d(g, gz, gx);
         if (m != -1) {
             sxx = bnd_at<T>(g, a, SXX, m);
@@ -2327,7 +2356,9 @@ __global__ void __launch_bounds__(256) k_adjv3d(Grid g, Fields f, AdjFields a)
     const float *hc = g.hc;
     float rip = __ldg(f.p[PRIP] + ip), rjp = __ldg(f.p[PRJP] + ip), rkp = __ldg(f.p[PRKP] + ip);
     float vx = 0.0f, vy = 0.0f, vz = 0.0f;
-    if (!g.bp2) {  // backpropagate the forward velocities (update_adjv3D.cl:297-340)
+    if (g.ckpt) {
+        vx = fwd_at<T>(g, a, VX, iv); vy = fwd_at<T>(g, a, VY, iv); vz = fwd_at<T>(g, a, VZ, iv);
+    } else if (!g.bp2) {  // backpropagate the forward velocities (update_adjv3D.cl:297-340)
         float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc), sxx_x = dfw<F>(f.w[SXX], iv, sx, hc);
         float sxz_x = dbw<F>(f.w[SXZ], iv, sx, hc), sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
         float syz_y = dbw<F>(f.w[SYZ], iv, sy, hc), syz_z = dbw<F>(f.w[SYZ], iv, 1, hc);
@@ -2369,7 +2400,7 @@ __global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
     if (MB) shot_adj(g, a, shot);
     const float *hc = g.hc;
     float vzx = 0.0f, vzy = 0.0f, vzz = 0.0f, vyx = 0.0f, vyy = 0.0f, vyz = 0.0f, vxx = 0.0f, vxy = 0.0f, vxz = 0.0f;
-    if (!g.bp2) {
+    if (!g.bp2 && !g.ckpt) {
         vzx = dfw<F>(f.w[VZ], iv, sx, hc); vzy = dfw<F>(f.w[VZ], iv, sy, hc); vzz = dbw<F>(f.w[VZ], iv, 1, hc);
         vyx = dfw<F>(f.w[VY], iv, sx, hc); vyy = dbw<F>(f.w[VY], iv, sy, hc); vyz = dfw<F>(f.w[VY], iv, 1, hc);
         vxx = dbw<F>(f.w[VX], iv, sx, hc); vxy = dfw<F>(f.w[VX], iv, sy, hc); vxz = dfw<F>(f.w[VX], iv, 1, hc);
@@ -2399,12 +2430,15 @@ __global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
     float vxyyx = vxy + vyx, vyzzy = vyz + vzy, vxzzx = vxz + vzx;
     float vxxyyzz = vxx + vyy + vzz, vyyzz = vyy + vzz, vxxzz = vxx + vzz, vxxyy = vxx + vyy;
     float s[6] = {0, 0, 0, 0, 0, 0};
-    if (!g.bp2) {
+    if (g.ckpt) {
+        s[0] = fwd_at<T>(g, a, SXY, iv); s[1] = fwd_at<T>(g, a, SYZ, iv); s[2] = fwd_at<T>(g, a, SXZ, iv);
+        s[3] = fwd_at<T>(g, a, SXX, iv); s[4] = fwd_at<T>(g, a, SYY, iv); s[5] = fwd_at<T>(g, a, SZZ, iv);
+    } else if (!g.bp2) {
         s[0] = f.w[SXY][iv]; s[1] = f.w[SYZ][iv]; s[2] = f.w[SXZ][iv];
         s[3] = f.w[SXX][iv]; s[4] = f.w[SYY][iv]; s[5] = f.w[SZZ][iv];
     }
     float *const *r = f.r;
-    if (g.bp2) {
+    if (g.bp2 || g.ckpt) {
     } else if (L == 0) {
         s[0] -= fipjp * vxyyx; s[1] -= fjpkp * vyzzy; s[2] -= fipkp * vxzzx;
         s[3] -= gm * vxxyyzz - fm * vyyzz; s[4] -= gm * vxxyyzz - fm * vxxzz; s[5] -= gm * vxxyyzz - fm * vxxyy;
@@ -2435,7 +2469,7 @@ __global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
         }
         for (int q = 0; q < 6; q++) s[q] -= ls[q] + g.dt2 * aa[q];
     }
-    if (!g.bp2) {
+    if (!g.bp2 && !g.ckpt) {
         int m = inject_ind3d(g, gz, gy, gx);
         if (m != -1) {
             s[3] = bnd_at<T>(g, a, SXX, m); s[4] = bnd_at<T>(g, a, SYY, m);
@@ -2879,6 +2913,39 @@ void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st)
         else DISPATCH_F(g.F, k_surf3d<FF><<<gr, b, 0, st>>>(g, f, pdir))
     } else {
         DISPATCH_F(g.F, k_surf2d<FF><<<dim3(cdiv(g.nx, 128), 1, g.nb), 128, 0, st>>>(g, f, pdir));
+    }
+}
+
+// FP32 arrays to T stores (pack) or back (unpack), value times scale; one
+// grid row per array, a grid-stride loop over its elements
+template <class T, bool UNPACK>
+__global__ void k_pack(PackSet ps)
+{
+    const int q = blockIdx.y;
+    const i64 n = ps.n[q];
+    const float sc = ps.scale[q];
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+        if (UNPACK) ((float *)ps.dst[q])[i] = to_f<T>(((const T *)ps.src[q])[i]) * sc;
+        else ((T *)ps.dst[q])[i] = from_f<T>(((const float *)ps.src[q])[i] * sc);
+    }
+}
+
+void launch_pack(const PackSet &ps, int prec, bool unpack, cudaStream_t st)
+{
+    if (ps.narr <= 0) return;
+    i64 nmax = 0;
+    for (int q = 0; q < ps.narr; q++) nmax = ps.n[q] > nmax ? ps.n[q] : nmax;
+    dim3 gr((unsigned)std::min<i64>((nmax + 255) / 256, 148 * 8), (unsigned)ps.narr);
+    if (gr.x == 0) return;
+    if (prec == SFD_PREC_FP16) {
+        if (unpack) k_pack<__half, true><<<gr, 256, 0, st>>>(ps);
+        else k_pack<__half, false><<<gr, 256, 0, st>>>(ps);
+    } else if (prec == SFD_PREC_BF16) {
+        if (unpack) k_pack<__nv_bfloat16, true><<<gr, 256, 0, st>>>(ps);
+        else k_pack<__nv_bfloat16, false><<<gr, 256, 0, st>>>(ps);
+    } else {
+        if (unpack) k_pack<float, true><<<gr, 256, 0, st>>>(ps);
+        else k_pack<float, false><<<gr, 256, 0, st>>>(ps);
     }
 }
 

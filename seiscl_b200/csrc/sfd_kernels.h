@@ -43,6 +43,18 @@ void launch_residuals(const Grid &g, const AdjFields &a, const PointSet &r, cons
 // storage scale, into dst [nx][ny][nz]
 void launch_movie(const Grid &g, const float *fld, float inv_scale, float *dst, cudaStream_t st);
 
+// checkpointed gradients: copies of wave fields / memory variables between
+// their FP32 arrays and stores of the saved-boundary precision (FP16 stores
+// scaled by powers of two)
+struct PackSet {
+    const void *src[NW + NR];
+    void *dst[NW + NR];
+    int64_t n[NW + NR];
+    float scale[NW + NR];   // applied to each value on the way
+    int narr;
+};
+void launch_pack(const PackSet &ps, int prec, bool unpack, cudaStream_t st);
+
 // DFT gradient (sfd_dft.cu)
 struct DftSet {             // variables transformed by one accumulation launch
     const float *v[NW + NR];

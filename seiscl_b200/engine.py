@@ -37,7 +37,7 @@ class sfd_config(C.Structure):
                 ("param_type", C.c_int), ("restype", C.c_int), ("precision", C.c_int),
                 ("kernels", C.c_int), ("adjoint_reset_psi", C.c_int), ("field_precision", C.c_int),
                 ("back_prop_type", C.c_int), ("loop_graphs", C.c_int), ("hout", C.c_int),
-                ("batch", C.c_int)]
+                ("batch", C.c_int), ("checkpoint", C.c_int)]
 
 
 class sfd_shot(C.Structure):
@@ -154,7 +154,8 @@ class Config:
     gradfreqs: Sequence[float] = ()  # DFT gradient frequencies (Hz), back_prop_type 2
     loop_graphs: str = "auto"  # time loops as CUDA graphs: "auto" (2D, 3D up to 2^22 cells), "always", "never"
     hout: int = 0  # HOUT: also accumulate the approximate Hessian (2D)
-    batch: int = 1  # shots advanced together by forward_batch / adjoint_batch (2D P-SV and acoustic)
+    batch: int = 1  # shots advanced together by forward_batch / adjoint_batch
+    checkpoint: int = 0  # gradients: 0 boundary saving + backpropagation; K > 0 snapshots every K steps + recompute
 
     def to_c(self) -> sfd_config:
         c = sfd_config()
@@ -188,6 +189,7 @@ class Config:
         c.kernels = {"fast": 0, "general": 1, "register": 2, "tma": 3, "stream": 4, "vector": 5}[self.kernels]
         c.adjoint_reset_psi = 1 if self.adjoint_reset_psi else 0
         c.batch = int(self.batch)
+        c.checkpoint = int(self.checkpoint)
         c.field_precision = {"fp32": 0, "fp16": 1}[self.field_precision]
         c.back_prop_type = int(self.back_prop_type)
         c.loop_graphs = {"auto": 0, "always": 1, "never": 2}[self.loop_graphs]
