@@ -76,7 +76,7 @@ def _key(cfg: engine.Config):
     return tuple((f.name, repr(getattr(cfg, f.name))) for f in dataclasses.fields(cfg))
 
 
-def plan_config(req: Request, max_batch: int = 8, batch_bytes: int = 8 << 30) -> engine.Config:
+def plan_config(req: Request, max_batch: int = 8, batch_bytes: int = 24 << 30) -> engine.Config:
     """The configuration of the plans serving ``req``: several shots of a
     request advance together in one plan (``batch``: up to ``max_batch``
     shots, as many as fit in ``batch_bytes`` of device memory; P-SV,
