@@ -528,28 +528,59 @@ def run_serving(args):
 
     from seiscl_b200 import serving
 
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    dist = None
+    if world > 1:   # one service per GPU, each taking every world-th request of the stream
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     nreq = max(args.steps, 1)
-    reqs = serving_requests(nreq)
-    arrivals = np.cumsum(np.random.default_rng(502).exponential(1.0 / args.rate, nreq))
-    nshots = sum(len(q.shots) for q in reqs)
+    reqs_all = serving_requests(nreq)
+    arrivals_all = np.cumsum(np.random.default_rng(502).exponential(1.0 / args.rate, nreq))
+    reqs, arrivals = reqs_all[rank::world], arrivals_all[rank::world]
+    nshots = sum(len(q.shots) for q in reqs_all)
     # warm-up: load the library and the CUDA context outside the timed streams
     _serve_stream(reqs[:1], [0.0], 1, False)
+    if dist:
+        dist.barrier()
     res, wall, st = _serve_stream(reqs, arrivals, args.workers, False)
-    p = serving.percentiles([r.latency for r in res])
-    plain = None
+    pwall = None
     if not args.no_plain:
+        if dist:
+            dist.barrier()
         pres, pwall, _ = _serve_stream(reqs, arrivals, 1, True)
-        pp = serving.percentiles([r.latency for r in pres])
+    lat = np.array([r.latency for r in res], np.float64)
+    plat = np.array([r.latency for r in pres], np.float64) if pwall is not None else np.zeros(0)
+    if dist:   # walls: the slowest rank; latencies: all requests
+        tt = torch.tensor([wall, pwall or 0.0], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        wall, pwall = float(tt[0]), (float(tt[1]) if pwall is not None else None)
+        gl, gp = [None] * world, [None] * world
+        dist.all_gather_object(gl, lat.tolist())
+        dist.all_gather_object(gp, plat.tolist())
+        lat = np.concatenate([np.asarray(x, np.float64) for x in gl])
+        plat = np.concatenate([np.asarray(x, np.float64) for x in gp])
+        dist.destroy_process_group()
+        if rank != 0:
+            return
+    p = serving.percentiles(lat)
+    plain = None
+    if pwall is not None:
+        pp = serving.percentiles(plat)
         plain = {"shots_per_s": round(nshots / pwall, 3), "wall_s": round(pwall, 2),
                  "latency_s": {k: round(v, 3) for k, v in pp.items()},
                  "what": "same request stream, one request and one shot at a time, step-by-step launches (no CUDA graphs)"}
+    reqs = reqs_all
     cells = 0.0
     for q in reqs:
         n = float(np.prod(q.config.N))
         cells += n * q.config.NT * len(q.shots) * (2 if q.kind == "gradient" else 1)
     print(json.dumps({
-        "metric": "shots/s", "value": round(nshots / wall, 3), "unit": "shots/s", "n_gpus": 1,
+        "metric": "shots/s", "value": round(nshots / wall, 3), "unit": "shots/s", "n_gpus": world,
         "steps": nreq, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": "serving", "requests": nreq, "shots": nshots, "arrival_rate_per_s": args.rate,

@@ -392,3 +392,48 @@ class Server:
 def percentiles(latencies: Sequence[float], qs=(50, 99)) -> Dict[str, float]:
     a = np.sort(np.asarray(latencies, np.float64))
     return {"p%d" % q: float(np.percentile(a, q)) if len(a) else float("nan") for q in qs}
+
+
+class Router:
+    """Requests over several GPUs of one process: one ``Server`` per device
+    (its workers bound to that device), each request sent to the server
+    with the fewest requests in flight (ties: the first).  The serving
+    router across GPUs; ``bench.py --workload serving`` under torchrun runs
+    one server per rank instead, each taking its share of the stream.
+
+    ``Router(devices=[0, 1, 2, 3], workers=4, ...)``; other keywords go to
+    every ``Server``."""
+
+    def __init__(self, devices: Sequence[Optional[int]], **server_kw):
+        if not devices:
+            raise ValueError("a router needs at least one device")
+        self.devices = list(devices)
+        self.servers = [Server(device=d, **server_kw) for d in self.devices]
+        self._inflight = [0] * len(self.servers)
+        self._lock = threading.Lock()
+
+    def submit(self, req: Request) -> Future:
+        with self._lock:
+            i = min(range(len(self.servers)), key=lambda k: (self._inflight[k], k))
+            self._inflight[i] += 1
+        fut = self.servers[i].submit(req)
+
+        def done(_f, i=i):
+            with self._lock:
+                self._inflight[i] -= 1
+
+        fut.add_done_callback(done)
+        return fut
+
+    def stats(self) -> List[Dict[str, int]]:
+        return [s.stats() for s in self.servers]
+
+    def close(self):
+        for s in self.servers:
+            s.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -220,6 +220,30 @@ def test_batches_and_slots_keep_shot_order_and_sum_gradients(monkeypatch, nd):
     assert np.allclose(got.gradient["vp"], one.gradient["vp"], rtol=1e-6) and got.misfit == one.misfit
 
 
+def test_router_spreads_requests_over_servers(monkeypatch):
+    """One server per device; each request goes to the least busy one and
+    comes back unchanged."""
+    import threading
+
+    from seiscl_b200 import engine, serving
+
+    CountingPlan.alive = CountingPlan.peak = 0
+    CountingPlan.lock = threading.Lock()
+    monkeypatch.setattr(engine, "Plan", CountingPlan)
+    reqs = _requests(12, seed=8)
+    with serving.Router([None, None, None], workers=1, memory_budget=1 << 40,
+                        footprint=_fake_footprint) as router:
+        res = [f.result(timeout=60) for f in [router.submit(q) for q in reqs]]
+        admitted = [st["admitted"] for st in router.stats()]
+    assert sum(admitted) == len(reqs) and min(admitted) >= 1
+    for r, q in zip(res, reqs):
+        ref = serving.serve(FakePlan(q.config), q)
+        assert r.rid == q.rid
+        for a, b in zip(r.seismograms, ref.seismograms):
+            for k in a:
+                assert np.array_equal(a[k], b[k])
+
+
 def test_footprint_grows_with_grid_and_gradient_buffers():
     from seiscl_b200 import engine
 
