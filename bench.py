@@ -691,9 +691,10 @@ def main():
                                           ", FP16 storage" if args.fields == "fp16" else "", kname)
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic_%s.json" % args.workload)
-    if os.path.exists(tpath) and args.fields == "fp32":
+    if os.path.exists(tpath):
         # DRAM bytes per launch of the kernel that ran, from an ncu capture
-        traffic = json.load(open(tpath)).get("stress_kernel_bytes_per_launch", {}).get(kname)
+        key = kname if args.fields == "fp32" else kname + ",fp16"
+        traffic = json.load(open(tpath)).get("stress_kernel_bytes_per_launch", {}).get(key)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
