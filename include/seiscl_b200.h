@@ -158,6 +158,10 @@ const char *sfd_last_error(const sfd_plan *plan);
 int sfd_footprint(const sfd_config *cfg, int gradient, int nsrc, int64_t nrec_sel, int nfreqs, int64_t *bytes);
 /* Device bytes the plan holds now (every allocation it made and keeps). */
 int64_t sfd_plan_device_bytes(const sfd_plan *plan);
+/* Plans allocate from the current device's stream-ordered memory pool,
+ * which keeps freed memory for the next plan; this returns what no plan
+ * holds to the device (synchronises the device). */
+int sfd_release_memory(void);
 /* Free and total memory of the current device (cudaMemGetInfo). */
 int sfd_device_memory(int64_t *free_bytes, int64_t *total_bytes);
 

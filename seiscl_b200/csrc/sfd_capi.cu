@@ -991,6 +991,16 @@ extern "C" int64_t sfd_plan_device_bytes(const sfd_plan *p)
     return p ? p->dev_bytes : SFD_ERR_ARG;
 }
 
+extern "C" int sfd_release_memory(void)
+{
+    int dev;
+    cudaMemPool_t pool;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess)
+        return SFD_ERR_CUDA;
+    if (cudaDeviceSynchronize() != cudaSuccess || cudaMemPoolTrimTo(pool, 0) != cudaSuccess) return SFD_ERR_CUDA;
+    return SFD_OK;
+}
+
 extern "C" int sfd_device_memory(int64_t *free_bytes, int64_t *total_bytes)
 {
     size_t f = 0, t = 0;

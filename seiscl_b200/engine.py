@@ -81,6 +81,7 @@ EXPORTS = {
                                 C.POINTER(C.c_int64)]),
     "sfd_device_memory": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "sfd_plan_device_bytes": (C.c_int64, [C.c_void_p]),
+    "sfd_release_memory": (C.c_int, []),
 }
 
 _LIB = None
@@ -519,3 +520,11 @@ def device_memory():
     if rc:
         raise SeisCLEngineError(rc, "cudaMemGetInfo failed")
     return int(f.value), int(t.value)
+
+
+def release_memory():
+    """Return the device memory no plan holds (plans allocate from the
+    device's pool, which keeps freed memory for the next plan)."""
+    rc = load_library().sfd_release_memory()
+    if rc:
+        raise SeisCLEngineError(rc, "cudaMemPoolTrimTo failed")

@@ -269,6 +269,22 @@ class Server:
             for _, plan, _ in self._idle.values():
                 plan.close()
             self._idle.clear()
+        if self._budget is not None and self._footprint is request_footprint:
+            # give the device memory of the closed plans back, on the
+            # service's device (a thread, so the caller's device is untouched)
+            def release():
+                try:
+                    if self._device is not None:
+                        import torch
+
+                        torch.cuda.set_device(self._device)
+                    engine.release_memory()
+                except Exception:
+                    pass
+
+            t = threading.Thread(target=release)
+            t.start()
+            t.join()
 
     def stats(self) -> Dict[str, int]:
         """Admission counters, the budget and the peak of bytes held."""
