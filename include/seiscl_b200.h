@@ -101,9 +101,10 @@ typedef struct sfd_config {
                               by powers of two (src/assign_modeling_case.c:829-866). */
     int back_prop_type;    /* BACK_PROP_TYPE: 0 or 1 boundary-saving backpropagation,
                               2 DFT gradient at the frequencies of sfd_set_gradfreqs */
-    int loop_graphs;       /* time loops as CUDA graphs: 0 for 2D grids and 3D grids of up
-                              to 2^22 padded cells (~160^3), whose steps are microseconds
-                              of work so that launches dominate, 1 always,
+    int loop_graphs;       /* time loops as CUDA graphs: 0 (auto) for every loop but those
+                              of the register-blocked and TMA 3D kernels, captured the
+                              second time a loop runs unchanged (launches dominate small
+                              grids; 1 % at 256^3), 1 always from the first run,
                               2 never.  A graph is captured on the first shot of a shape
                               and replayed while nothing its launches depend on changes.
                               No reference counterpart (launch mechanics). */

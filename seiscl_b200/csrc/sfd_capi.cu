@@ -440,7 +440,7 @@ bool graphs_on(const sfd_plan *p)
     const int m = p->cfg.loop_graphs;
     if (m == 2) return false;
     if (m == 1) return p->g.kernels != 3;   // the TMA path sets kernel attributes on first use
-    return p->g.nd != 3 || (p->g.nvol <= ((int64_t)1 << 22) && p->g.kernels != 3 && p->g.kernels != 2);
+    return p->g.nd != 3 || (p->g.kernels != 3 && p->g.kernels != 2);
 }
 
 void drop_graph(sfd_plan::LoopGraph &lg)

@@ -153,7 +153,7 @@ class Config:
     field_precision: str = "fp32"  # "fp16": wave fields / memory variables stored in FP16 (3D forward)
     back_prop_type: int = 1  # 1: boundary-saving backpropagation, 2: DFT gradient at `gradfreqs`
     gradfreqs: Sequence[float] = ()  # DFT gradient frequencies (Hz), back_prop_type 2
-    loop_graphs: str = "auto"  # time loops as CUDA graphs: "auto" (2D, 3D up to 2^22 cells), "always", "never"
+    loop_graphs: str = "auto"  # time loops as CUDA graphs: "auto" (from the 2nd run of a loop), "always", "never"
     hout: int = 0  # HOUT: also accumulate the approximate Hessian (2D)
     batch: int = 1  # shots advanced together by forward_batch / adjoint_batch
     checkpoint: int = 0  # gradients: 0 boundary saving + backpropagation; K > 0 snapshots every K steps + recompute
