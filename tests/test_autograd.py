@@ -53,3 +53,33 @@ def test_gradient_matches_central_differences(src_type, cuda_device):
         fd = (L(1) - L(-1)) / (2 * eps)
         an = float((g * delta).sum())
         assert abs(an / fd - 1) < tol[name], (name, an / fd)
+
+
+@pytest.mark.gpu
+def test_checkpointed_plan_behind_autograd(cuda_device):
+    """The snapshot-checkpoint recompute strategy behind torch.autograd: the
+    same gradient as boundary-saving reconstruction inside the region the
+    boundary shells enclose, and the same central-difference check."""
+    import torch
+
+    from seiscl_b200.autograd import seismograms
+    from seiscl_b200.engine import Plan
+
+    cfg, model, acq = make_case(nd=2, freesurf=0, L=0, abs_type=1, src_type=100, nt=400, nz=80, nx=90, nab=12)
+    shots = [(acq["src_pos"], acq["src"], acq["rec_pos"])]
+    outs = ["vx", "vz"]
+    m = {k: torch.tensor(model[k].T.copy(), dtype=torch.float64) for k in ("vp", "vs", "rho")}
+    grads = {}
+    for K in (0, 25):
+        plan = Plan(dataclasses.replace(engine_config(cfg), adjoint_reset_psi=True, checkpoint=K))
+        d0 = seismograms(plan, m["vp"], m["vs"], m["rho"], shots, outs).detach().double()
+        w = d0 / float((d0 * d0).sum())
+        mr = {k: v.clone().requires_grad_(True) for k, v in m.items()}
+        (seismograms(plan, mr["vp"], mr["vs"], mr["rho"], shots, outs).double() * w).sum().backward()
+        grads[K] = {k: v.grad.double().numpy() for k, v in mr.items()}
+        plan.close()
+    e = cfg["nab"] + 6
+    for name in ("vp", "vs", "rho"):
+        a, b = grads[25][name][e:-e, e:-e], grads[0][name][e:-e, e:-e]
+        assert np.abs(b).max() > 0, name
+        assert np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()) < 2e-4, name
