@@ -1011,8 +1011,8 @@ __device__ __forceinline__ void cpml_v3d_q4(const Grid &g, const Fields &f, int 
     const i64 iv = gx * sx + (i64)gy * sy + gz0;                                       \
     const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
 
-template <class T, bool MB = false>
-__global__ void __launch_bounds__(128) k_v3d_q4(Grid g, Fields f)
+template <class T, bool MB>
+__device__ __forceinline__ void v3d_q4(const Grid &g, Fields f)
 {
     CELL3D_Q4
     const float *hc = g.hc;
@@ -1043,6 +1043,22 @@ __global__ void __launch_bounds__(128) k_v3d_q4(Grid g, Fields f)
     stq(wvx + iv, vx);
     stq(wvy + iv, vy);
     stq(wvz + iv, vz);
+}
+
+template <class T, bool MB = false>
+__global__ void __launch_bounds__(128) k_v3d_q4(Grid g, Fields f)
+{
+    v3d_q4<T, MB>(g, f);
+}
+
+// The single-shot FP32 launch asks for 4 resident CTAs per SM (at most 128
+// registers, from 136, with a 36-byte spill): 0.333 ms against 0.345 at
+// 256^3 L=2 on a B200.  5 CTAs (102 registers) is slower again, and a
+// component-at-a-time update with 80 registers slower still (0.37 ms): the
+// kernel is bound by the stencil loads each thread keeps in flight.
+__global__ void __launch_bounds__(128, 4) k_v3d_q4_b4(Grid g, Fields f)
+{
+    v3d_q4<float, false>(g, f);
 }
 
 // CPML corrections of cpml_s3d (forward form) for a quad of z cells
@@ -2782,7 +2798,8 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
             // rows of neighbouring threads share L1 lines (0.35 ms at 256^3,
             // against 0.39 for 32 x 2 x 2)
             dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4) * g.nb);
-            MB_DISPATCH(g, k_v3d_q4<float, MBV><<<gr, b, 0, st>>>(g, f))
+            if (g.nb > 1) k_v3d_q4<float, true><<<gr, b, 0, st>>>(g, f);
+            else k_v3d_q4_b4<<<gr, b, 0, st>>>(g, f);
             return;
         }
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
