@@ -165,6 +165,12 @@ int64_t sfd_plan_device_bytes(const sfd_plan *plan);
 int sfd_release_memory(void);
 /* Free and total memory of the current device (cudaMemGetInfo). */
 int sfd_device_memory(int64_t *free_bytes, int64_t *total_bytes);
+/* Host-only self-check of the cache that keeps the 3D TMA kernels' tensor
+ * maps between launches: `nthreads` threads make `iters` lookups each over
+ * more keys than it holds and verify every value they copy out.  Returns the
+ * number of bad copies (0 = sound).  Needs no device.  No counterpart in the
+ * reference (which has no host state shared between threads). */
+int64_t sfd_selftest_cache(int nthreads, int iters);
 
 /* Upload the model.  params = {vp, vs, rho} (param_type 0), plus {taup, taus}
  * when L > 0, each a host array of nz*ny*nx floats in [nx][ny][nz] order.
@@ -283,7 +289,12 @@ int sfd_adjoint_batch(sfd_plan *plan, int nshot, const sfd_shot *shots, int mask
  *   nsel selected outputs in SFD_OUT_* order.
  * - The first call on a device looks up the array's device address
  *   (cudaGetSymbolAddress) with that device current; make that first call
- *   before any stream capture.
+ *   before any stream capture.  Under CUDA's lazy module loading (the
+ *   default since CUDA 12.2) that first call is also when the driver loads
+ *   this part of the library onto the device and commits the array's
+ *   SFD_NOALLOC_SCRATCH_BYTES: a caller that reserves the rest of the
+ *   device afterwards should make its first call at start-up, before it
+ *   takes that reservation.  Later calls commit nothing.
  * - Every call on a device shares the one array.  Each call clears what must
  *   start at zero, but calls that overlap on the GPU (different streams or
  *   threads at once) race on it: issue them one after another.

@@ -31,6 +31,7 @@
 #include <mutex>
 #include <vector>
 
+#include "sfd_cache.h"
 #include "sfd_internal.h"
 #include "sfd_kernels.h"
 
@@ -711,12 +712,12 @@ MapKey key_of(const Grid &g, const Fields &f)
 }
 
 struct CacheEntry {
-    MapKey key;
     TmaMaps v, s;
     bool ok_v, ok_s;
 };
-std::mutex g_cache_mu;
-std::vector<CacheEntry> g_cache;
+// encoded maps, 16 most recent grid/field sets; launches copy their maps
+// out under the cache's lock (plans run on several threads at once)
+KeyedCache<MapKey, CacheEntry, 16> g_cache;
 
 bool eligible(const Grid &g)
 {
@@ -764,20 +765,20 @@ bool build_maps(const Grid &g, const Fields &f, CacheEntry &e)
 
 // Maps of this grid and field set, encoded once and reused; entries are keyed
 // by every pointer and size, so a reused allocation address with other sizes
-// gets its own entry.
-const CacheEntry *maps_for(const Grid &g, const Fields &f)
+// gets its own entry.  `which` 0 copies the velocity kernel's maps into *out,
+// 1 the stress kernel's; returns whether they were encoded.
+bool maps_for(const Grid &g, const Fields &f, int which, TmaMaps *out)
 {
-    const MapKey key = key_of(g, f);
-    std::lock_guard<std::mutex> lk(g_cache_mu);
-    for (auto &e : g_cache)
-        if (e.key == key) return &e;
-    if (g_cache.size() >= 16) g_cache.erase(g_cache.begin());
-    CacheEntry e;
-    std::memset(&e, 0, sizeof(e));
-    e.key = key;
-    build_maps(g, f, e);
-    g_cache.push_back(e);
-    return &g_cache.back();
+    return g_cache.with(
+        key_of(g, f),
+        [&](CacheEntry &e) {
+            std::memset(&e, 0, sizeof(e));
+            build_maps(g, f, e);
+        },
+        [&](const CacheEntry &e) {
+            if (out) *out = which == 0 ? e.v : e.s;
+            return which == 0 ? e.ok_v : e.ok_s;
+        });
 }
 
 int sm_count()
@@ -882,21 +883,21 @@ static bool launch_tma(const Grid &g, const TmaMaps &m, const Fields &f, cudaStr
 bool launch_update_v_tma(const Grid &g, const Fields &f, cudaStream_t st)
 {
     if (!eligible(g)) return false;
-    const CacheEntry *e = maps_for(g, f);
-    if (!e->ok_v) return false;
-    return launch_tma<0, 0>(g, e->v, f, st);
+    TmaMaps m;
+    if (!maps_for(g, f, 0, &m)) return false;
+    return launch_tma<0, 0>(g, m, f, st);
 }
 
 bool launch_update_s_tma(const Grid &g, const Fields &f, cudaStream_t st)
 {
     if (!eligible(g)) return false;
-    const CacheEntry *e = maps_for(g, f);
-    if (!e->ok_s) return false;
+    TmaMaps m;
+    if (!maps_for(g, f, 1, &m)) return false;
     switch (g.L) {
-    case 0: return launch_tma<1, 0>(g, e->s, f, st);
-    case 1: return launch_tma<1, 1>(g, e->s, f, st);
-    case 2: return launch_tma<1, 2>(g, e->s, f, st);
-    case 3: return launch_tma<1, 3>(g, e->s, f, st);
+    case 0: return launch_tma<1, 0>(g, m, f, st);
+    case 1: return launch_tma<1, 1>(g, m, f, st);
+    case 2: return launch_tma<1, 2>(g, m, f, st);
+    case 3: return launch_tma<1, 3>(g, m, f, st);
     default: return false;
     }
 }
@@ -904,8 +905,7 @@ bool launch_update_s_tma(const Grid &g, const Fields &f, cudaStream_t st)
 bool tma_ready(const Grid &g, const Fields &f)
 {
     if (!eligible(g) || !encode_fn()) return false;
-    const CacheEntry *e = maps_for(g, f);
-    return e->ok_v && e->ok_s;
+    return maps_for(g, f, 0, nullptr) && maps_for(g, f, 1, nullptr);
 }
 
 int tma_take_status()

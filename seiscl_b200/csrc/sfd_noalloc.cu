@@ -102,8 +102,10 @@ extern "C" int sfd_forward_noalloc(sfd_plan *p, const float *src_pos, const floa
         p->err = "invalid shot arrays";
         return SFD_ERR_ARG;
     }
-    p->g.nb = 1;   // one shot, whatever the plan's batch
-    const Grid &g = p->g;
+    // one shot, whatever the plan's batch; a local copy leaves the plan's
+    // state as it was
+    Grid g = p->g;
+    g.nb = 1;
     unsigned omask = 0;
     int nsel = 0;
     for (int o = 0; o < SFD_NOUT; o++) {
@@ -208,5 +210,11 @@ extern "C" int sfd_forward_noalloc(sfd_plan *p, const float *src_pos, const floa
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) { p->err = cudaGetErrorString(e); return SFD_ERR_CUDA; }
+    // a TMA stage that gave up on its bounded wait leaves wrong seismograms
+    // and raises the device status word; report it as sfd_forward does
+    if (tma_take_status()) {
+        p->err = "a TMA pipeline stage timed out (results invalid)";
+        return SFD_ERR_CUDA;
+    }
     return SFD_OK;
 }

@@ -58,3 +58,19 @@ def test_invalid_configs_rejected():
         h = C.c_void_p()
         rc = lib.sfd_plan_create(C.byref(c), C.byref(h))
         assert rc in (-1, -7), bad
+
+
+def test_tma_map_cache_is_thread_safe():
+    """The tensor-map cache is read by launches on several threads (the
+    service runs plans on worker threads): lookups that evict and rebuild
+    entries concurrently must never hand out a torn or stale value."""
+    import ctypes as C
+
+    from seiscl_b200.engine import load_library
+
+    lib = load_library()
+    fn = lib.sfd_selftest_cache
+    fn.restype = C.c_int64
+    fn.argtypes = [C.c_int, C.c_int]
+    assert fn(8, 20000) == 0
+    assert fn(0, 1) < 0
