@@ -21,9 +21,11 @@ Accuracy: this is an adjoint-state gradient of the continuous equations
 evaluated on the grid, not the exact adjoint of the discrete scheme.  Checked
 against central finite differences along the gradient direction (interior,
 no free surface) it agrees to a few percent for vp and vs and to tens of
-percent for rho; near a free surface it is less accurate.  For force sources
-create the plan with ``adjoint_reset_psi=True``: the reference's adjoint
-carries the forward CPML memory over, which then dominates the adjoint field.
+percent for rho; near a free surface it is less accurate.  Force sources
+(types 0, 1, 2) need a plan created with ``adjoint_reset_psi=True``, and
+``seismograms`` refuses them otherwise: the reference's adjoint carries the
+forward CPML memory over, which then dominates the adjoint field and makes
+the gradient wrong by orders of magnitude.
 """
 from __future__ import annotations
 
@@ -88,5 +90,14 @@ def seismograms(plan: Plan, vp: torch.Tensor, vs: torch.Tensor, rho: torch.Tenso
     ``shots``: sequence of (src_pos [nsrc][5], src [nsrc][NT], rec_pos
     [nrec][8]) host arrays; ``outputs``: seismogram names ("vx", "vz", "p",
     ...).  Returns [nshot][len(outputs)][nrec][NT] on vp's device; every shot
-    must have the same receiver count."""
-    return _Seismograms.apply(vp, vs, rho, plan, list(shots), tuple(outputs))
+    must have the same receiver count.  Raises ValueError for force sources
+    on a plan without ``adjoint_reset_psi`` (see the module docstring)."""
+    shots = list(shots)
+    if not plan.cfg.adjoint_reset_psi:
+        for sp, _, _ in shots:
+            types = np.asarray(sp, np.float32).reshape(-1, 5)[:, 4].astype(int)
+            if np.isin(types, (0, 1, 2)).any():
+                raise ValueError("force sources need a plan created with adjoint_reset_psi=True: with the "
+                                 "forward run's CPML memory carried into the adjoint (the reference's "
+                                 "behaviour) their gradient is dominated by it")
+    return _Seismograms.apply(vp, vs, rho, plan, shots, tuple(outputs))

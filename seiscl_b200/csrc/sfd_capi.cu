@@ -274,8 +274,10 @@ int alloc_model(sfd_plan *p)
         p->f.cz[k] = cst + (2 * NC + k) * nc;
     }
     p->f.taper = cst + 3 * NC * nc;
-    p->d_ticket = (int *)dalloc(p, sizeof(int), &e);   // block counter of the fused steps
+    // block counter of the fused steps, instability flag
+    p->d_ticket = (int *)dalloc(p, 2 * sizeof(int), &e);
     if (e) return fail(p, SFD_ERR_MEMORY, "step counter allocation failed");
+    p->d_unstable = p->d_ticket + 1;
     for (int ax = 0; ax < 3; ax++)
         for (int h = 0; h < 2; h++) p->f.kinv[ax][h] = cst + 3 * NC * nc + nc + (2 * ax + h) * nc;
     return SFD_OK;
@@ -420,6 +422,37 @@ int movie_out(sfd_plan *p, const Movie &mv, cudaStream_t st)
         CKC(cudaMemcpyAsync(p->mov_dst[mv.out[q]], p->d_mov + (size_t)q * mv.nslot * mv.ncell,
                             sizeof(float) * (size_t)mv.nslot * mv.ncell, cudaMemcpyDeviceToHost, st));
     return SFD_OK;
+}
+
+// ------------------------------------------------- instability detection
+// Every FINITE_CHECK_EVERY steps (and after the last) a loop scans one
+// velocity field of its shots for non-finite values; the first step at which
+// one is seen is kept in p->d_unstable and turned into SFD_ERR_UNSTABLE when
+// the loop has finished (the reference aborts on a NaN misfit,
+// src/residuals.c:444-448).
+const float *check_field(float *const *w)
+{
+    for (int q : {VX, VY, VZ})
+        if (w[q]) return w[q];
+    return nullptr;
+}
+
+int arm_unstable(sfd_plan *p, cudaStream_t st)
+{
+    CKC(cudaMemsetAsync(p->d_unstable, 0x7f, sizeof(int), st));
+    return SFD_OK;
+}
+
+// call after the loop's stream has been synchronised
+int take_unstable(sfd_plan *p, cudaStream_t st, const char *what)
+{
+    int v = 0;
+    CKC(cudaMemcpyAsync(&v, p->d_unstable, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CKC(cudaStreamSynchronize(st));
+    if (v == 0x7f7f7f7f) return SFD_OK;
+    char buf[200];
+    snprintf(buf, sizeof buf, "Simulation has become unstable: non-finite %s wave field at step %d", what, v);
+    return fail(p, SFD_ERR_UNSTABLE, buf);
 }
 
 // ----------------------------------------------------------- loop graphs
@@ -626,6 +659,10 @@ int adjoint_ckpt(sfd_plan *p, const PointSet &S, const PointSet &R, unsigned oma
     key.add(4); key.add(ga); key.add(p->f); key.add(fa); key.add(a); key.add_points(S); key.add_points(R);
     key.add(p->d_src); key.add(p->d_res); key.add(p->d_surf_q); key.add(omask); key.add(p->d_snap); key.add(p->d_seg);
     key.add(p->cfg.precision); key.add(tmax); key.add(tmin); key.add(z.K);
+    const float *chk = check_field(a.wr);
+    const int64_t nchk = g.nvol * g.nb;
+    int rc;
+    if ((rc = arm_unstable(p, st))) return rc;
     CKC(cudaEventRecord(p->ev0, st));
     int rcl = run_loop(p, p->gadj, key.s, st, [&](cudaStream_t s) {
         for (int j = z.nseg - 1; j >= 0; j--) {
@@ -646,6 +683,8 @@ int adjoint_ckpt(sfd_plan *p, const PointSet &S, const PointSet &R, unsigned oma
                 launch_residuals(ga, a, R, p->d_res, NT, t, omask, s);
                 launch_update_adj(ga, fa, a, true, p->cfg.precision, s);
                 launch_update_adj(ga, fa, a, false, p->cfg.precision, s);
+                if (t % FINITE_CHECK_EVERY == 0 || t == tmin + 1)
+                    launch_finite_check(g, chk, nchk, t, p->d_unstable, s);
             }
         }
     });
@@ -655,7 +694,7 @@ int adjoint_ckpt(sfd_plan *p, const PointSet &S, const PointSet &R, unsigned oma
     CKC(cudaStreamSynchronize(st));
     cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1);
     p->have_forward = false;
-    return SFD_OK;
+    return take_unstable(p, st, "adjoint");
 }
 
 // ---------------------------------------------------------- DFT gradient
@@ -763,6 +802,9 @@ int adjoint_dft(sfd_plan *p, const PointSet &R, unsigned omask, cudaStream_t st)
     key.add(2); key.add(ga); key.add(p->f); key.add(a); key.add_points(R); key.add(omask); key.add(p->d_res);
     key.add(p->d_surf_q); key.add(p->cfg.tmax); key.add(tmin); key.add(p->nfreqs); key.add(p->dtnyq);
     key.add(p->ntnyq); key.add(p->gradfreqsn); key.add(p->d_fw); key.add(p->d_fr);
+    const float *chk = check_field(a.wr);
+    const int64_t nchk = g.nvol * g.nb;
+    if ((rc = arm_unstable(p, st))) return rc;
     CKC(cudaEventRecord(p->ev0, st));
     int rc2 = run_loop(p, p->gadj, key.s, st, [&](cudaStream_t s) {
         for (int t = p->cfg.tmax - 1; t > tmin; t--) {
@@ -771,6 +813,8 @@ int adjoint_dft(sfd_plan *p, const PointSet &R, unsigned omask, cudaStream_t st)
             launch_update_adj(ga, p->f, a, true, SFD_PREC_FP32, s);
             launch_update_adj(ga, p->f, a, false, SFD_PREC_FP32, s);
             if ((t - tmin) % p->dtnyq == 0) dft_sample(p, 1, (t - tmin) / p->dtnyq, s);
+            if (t % FINITE_CHECK_EVERY == 0 || t == tmin + 1)
+                launch_finite_check(g, chk, nchk, t, p->d_unstable, s);
         }
     });
     if (rc2) return rc2;
@@ -800,7 +844,7 @@ int adjoint_dft(sfd_plan *p, const PointSet &R, unsigned omask, cudaStream_t st)
     cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1);
     p->have_forward = false;
     p->have_dft = false;
-    return SFD_OK;
+    return take_unstable(p, st, "adjoint");
 }
 
 }  // namespace
@@ -914,6 +958,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     p->cap_src = p->cap_rec = 0;
     p->d_surf_q = nullptr;
     p->d_ticket = nullptr;
+    p->d_unstable = nullptr;
     p->dev_bytes = 0;
     p->batch = std::max(1, c.batch);
     p->fwd_nb = 0;
@@ -964,7 +1009,7 @@ extern "C" int sfd_footprint(const sfd_config *cfg, int gradient, int nsrc, int6
     // ensure_shot_buffers: source maps and signatures, receiver maps, seismograms and residuals
     const int64_t cs = std::max<int64_t>(nsrc, 16), cr = std::max<int64_t>(nrec_sel, 16);
     b += cs * (8 + 4 + 12 + 4 + 12 + 4 * nt) + cr * (8 + 8 * nt);
-    b += sizeof(int);   // fused-step block counter
+    b += 2 * sizeof(int);   // fused-step block counter, instability flag
     if (gradient) {
         const bool bp2 = cfg->back_prop_type == 2;
         int ng = 0;
@@ -1223,6 +1268,12 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
         key.add(p->nfreqs); key.add(p->dtnyq); key.add(p->ntnyq); key.add(p->gradfreqsn); key.add(p->d_fw);
         key.add(p->d_fr);
     }
+    const float *chk = check_field(p->f.w);
+    const int64_t nchk = g.nvol * g.nb;
+    auto check = [&](int t, cudaStream_t s) {
+        if ((t + 1) % FINITE_CHECK_EVERY == 0 || t == tmax - 1) launch_finite_check(g, chk, nchk, t, p->d_unstable, s);
+    };
+    if ((rc = arm_unstable(p, st))) return rc;
     CKC(cudaEventRecord(p->ev0, st));
     int rcl = run_loop(p, p->gfwd, key.s, st, [&](cudaStream_t s) {
         if (fuse2d) {
@@ -1231,6 +1282,7 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
                 launch_update_v(g, p->f, s);
                 StepTail tl{p->d_ticket, R, p->d_seis, omask, t, S, p->d_src, t + 1 < tmax ? t + 1 : -1, NT};
                 launch_update_s_step(g, p->f, tl, s);
+                check(t, s);
             }
             return;
         }
@@ -1245,6 +1297,7 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
             if (g.freesurf) launch_surface(g, p->f, 1, s);
             launch_record(g, p->f, R, p->d_seis, NT, t, omask, s);
             if (mv.n && (t + 1) % p->movout == 0) movie_snap(p, mv, (t + 1) / p->movout - 1, s);
+            check(t, s);
         }
     });
     if (rcl) return rcl;
@@ -1263,6 +1316,7 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1);
     if (tma_take_status())
         return fail(p, SFD_ERR_CUDA, "a TMA stage of the 3D stencil kernels did not arrive within its time bound");
+    if ((rc = take_unstable(p, st, "forward"))) return rc;
     p->have_forward = save_boundaries != 0;
     p->fwd_nb = nshot;
     p->have_dft = dft;
@@ -1334,6 +1388,9 @@ extern "C" int sfd_adjoint_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     key.add(3); key.add(g); key.add(p->f); key.add(a); key.add_points(S); key.add_points(R); key.add(p->d_src);
     key.add(p->d_res); key.add(p->d_surf_q); key.add(omask); key.add(p->d_bnd); key.add(p->bnd_elem);
     key.add(p->cfg.precision); key.add(p->cfg.tmax); key.add(p->cfg.tmin);
+    const float *chk = check_field(a.wr);
+    const int64_t nchk = g.nvol * g.nb;
+    if ((rc = arm_unstable(p, st))) return rc;
     CKC(cudaEventRecord(p->ev0, st));
     int rcl = run_loop(p, p->gadj, key.s, st, [&](cudaStream_t s) {
         for (int t = p->cfg.tmax - 1; t > p->cfg.tmin; t--) {
@@ -1345,6 +1402,8 @@ extern "C" int sfd_adjoint_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
             launch_update_adj(g, p->f, a, false, p->cfg.precision, s);
             launch_sources(g, p->f, S, p->d_src, NT, t, -1, s);
             if (mv.n && t % p->movout == 0) movie_snap(p, mv, (t + 1) / p->movout - 1, s);
+            if (t % FINITE_CHECK_EVERY == 0 || t == p->cfg.tmin + 1)
+                launch_finite_check(g, chk, nchk, t, p->d_unstable, s);
         }
     });
     if (rcl) return rcl;
@@ -1354,7 +1413,7 @@ extern "C" int sfd_adjoint_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     CKC(cudaStreamSynchronize(st));
     cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1);
     p->have_forward = false;
-    return SFD_OK;
+    return take_unstable(p, st, "adjoint");
 }
 
 namespace {

@@ -149,6 +149,7 @@ struct sfd_plan {
     float *d_src_div, *d_src, *d_seis, *d_res;
     float *d_surf_q;        // surface-adjoint scratch [nx][ny]
     int *d_ticket;          // fused 2D steps: block counter of the stress launch
+    int *d_unstable;        // first checked step with a non-finite wave field (INT_MAX: none)
     // checkpointed gradients (cfg.checkpoint = K > 0)
     char *d_snap;           // [nseg] snapshots: wave fields, memory variables (store type), CPML (FP32)
     char *d_seg;            // [K][wave fields] of the segment being backpropagated (store type)

@@ -2888,6 +2888,38 @@ __global__ void k_movie(Grid g, const T *fld, float inv_scale, float *dst)
     }
 }
 
+// One wave field scanned for non-finite values (the reference tests the
+// misfit for NaN once per run, src/residuals.c:444-448; here the field is
+// tested every FINITE_CHECK_EVERY steps so a run reports the step near which
+// it diverged).
+template <class T>
+__global__ void __launch_bounds__(256) k_finite(const T *__restrict__ v, i64 n, int t, int *first)
+{
+    bool bad = false;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+        bad |= !isfinite(to_f<T>(v[i]));
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicMin(first, t);
+}
+__global__ void __launch_bounds__(256) k_finite4(const float4 *__restrict__ v, i64 n4, int t, int *first)
+{
+    bool bad = false;
+    for (i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x; i < n4; i += (i64)gridDim.x * blockDim.x) {
+        const float4 q = __ldg(v + i);
+        bad |= !(isfinite(q.x) && isfinite(q.y) && isfinite(q.z) && isfinite(q.w));
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicMin(first, t);
+}
+
+void launch_finite_check(const Grid &g, const float *fld, int64_t n, int t, int *first, cudaStream_t st)
+{
+    if (!fld || n <= 0) return;
+    const unsigned blocks = (unsigned)std::min<i64>((n + 1023) / 1024, 148 * 8);
+    if (g.fhalf) k_finite<__half><<<blocks, 256, 0, st>>>(reinterpret_cast<const __half *>(fld), n, t, first);
+    else if (n % 4 == 0 && ((uintptr_t)fld & 15) == 0)
+        k_finite4<<<blocks, 256, 0, st>>>(reinterpret_cast<const float4 *>(fld), n / 4, t, first);
+    else k_finite<float><<<blocks, 256, 0, st>>>(fld, n, t, first);
+}
+
 void launch_movie(const Grid &g, const float *fld, float inv_scale, float *dst, cudaStream_t st)
 {
     const i64 n = (i64)g.nz * g.ny * g.nx;

@@ -39,6 +39,11 @@ void launch_record(const Grid &g, const Fields &f, const PointSet &r, float *out
 void launch_residuals(const Grid &g, const AdjFields &a, const PointSet &r, const float *res, int nt_total, int t,
                       unsigned outmask, cudaStream_t st);
 
+// instability detection: if any of the n values of a wave field (FP32, or
+// FP16 when g.fhalf) is not finite, *first = min(*first, t)
+void launch_finite_check(const Grid &g, const float *fld, int64_t n, int t, int *first, cudaStream_t st);
+constexpr int FINITE_CHECK_EVERY = 64;   // time steps between checks
+
 // movie snapshot: the physical cells of one wave field, divided by its
 // storage scale, into dst [nx][ny][nz]
 void launch_movie(const Grid &g, const float *fld, float inv_scale, float *dst, cudaStream_t st);

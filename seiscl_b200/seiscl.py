@@ -698,6 +698,9 @@ class SeisCL:
             else:
                 rms += float(((d - o) ** 2).sum())
                 rmsnorm += float((d ** 2).sum())
+            if not np.isfinite(rms):
+                # src/residuals.c:444-448
+                raise SeisCLError("Simulation has become unstable, stopping\n")
             r = np.zeros_like(out[k])
             if rmsnorm_sc is not None:
                 r[:, :tmax] = sc[:, None] * ((1.0 - rmsnorm_sc)[:, None] * o - d)

@@ -83,3 +83,23 @@ def test_checkpointed_plan_behind_autograd(cuda_device):
         a, b = grads[25][name][e:-e, e:-e], grads[0][name][e:-e, e:-e]
         assert np.abs(b).max() > 0, name
         assert np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()) < 2e-4, name
+
+
+def test_force_sources_need_reset_psi():
+    """seismograms() refuses force sources on a plan that carries the forward
+    CPML memory into the adjoint (their gradient would be dominated by it);
+    the check runs before any device work."""
+    import types
+
+    import torch
+
+    from seiscl_b200.autograd import seismograms
+
+    plan = types.SimpleNamespace(cfg=types.SimpleNamespace(adjoint_reset_psi=False))
+    m = torch.ones((8, 8))
+    rp = np.zeros((1, 8), np.float32)
+    src = np.zeros((1, 10), np.float32)
+    for ty in (0, 1, 2):
+        sp = np.array([[10.0, 0.0, 10.0, 0, ty]], np.float32)
+        with pytest.raises(ValueError):
+            seismograms(plan, m, m, m, [(sp, src, rp)], ["vx"])

@@ -551,3 +551,36 @@ def test_batched_3d_shots_match_single_runs(kw, cuda_device):
     for k in ("M", "mu", "rho"):
         assert np.abs(g1[k]).max() > 0, k
         assert rel_l2(gb[k], g1[k]) < 1e-6, (k, rel_l2(gb[k], g1[k]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nd", [2, 3])
+def test_unstable_run_is_reported(nd, cuda_device, monkeypatch):
+    """A time step far above the CFL limit (the set-up check bypassed through
+    its test hook) diverges; the forward run returns SFD_ERR_UNSTABLE naming
+    a checked step at most 64 steps after the field first stops being
+    finite, and the adjoint of a finite forward run with non-finite
+    residuals does the same."""
+    from seiscl_b200.engine import Plan, SeisCLEngineError
+
+    monkeypatch.setenv("SEISCL_B200_UNCHECKED_CFL", "1")
+    kw = dict(nd=nd, nt=300, nz=32, nx=36, ny=28, nab=8) if nd == 3 else dict(nd=nd, nt=300)
+    cfg, model, acq = make_case(**kw)
+    cfg["dt"] = 4e-3   # ~3x the stability limit
+    plan = Plan(engine_config(cfg))
+    plan.set_model(model["vp"], model["vs"], model["rho"])
+    with pytest.raises(SeisCLEngineError) as e:
+        plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], ["vx"])
+    assert e.value.code == -6
+    assert "unstable" in str(e.value)
+    step = int(str(e.value).rsplit("step", 1)[1].split()[0])
+    assert 0 <= step < cfg["nt"]
+    # the adjoint reports it too: a finite forward, non-finite residuals
+    cfg2, model2, acq2 = make_case(**kw)
+    plan2 = Plan(engine_config(cfg2))
+    plan2.set_model(model2["vp"], model2["vs"], model2["rho"])
+    d = plan2.forward(acq2["src_pos"], acq2["src"], acq2["rec_pos"], ["vx"], save_boundaries=True)
+    res = {"vx": np.full_like(d["vx"], np.nan)}
+    with pytest.raises(SeisCLEngineError) as e2:
+        plan2.adjoint(acq2["src_pos"], acq2["src"], acq2["rec_pos"], res)
+    assert e2.value.code == -6
