@@ -297,6 +297,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def clock_log_path(args, rank):
+    """Where the nvidia-smi clock samples of the timed region go: the path
+    given by --clock-log (one file per rank), else the system's temporary
+    directory."""
+    import tempfile
+
+    if args.clock_log:
+        root, ext = os.path.splitext(args.clock_log)
+        return "%s_r%d%s" % (root, rank, ext or ".csv")
+    return os.path.join(tempfile.gettempdir(), "seiscl_b200_clocks_%d_r%d.csv" % (os.getpid(), rank))
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -404,8 +416,7 @@ def run_gradient(args):
     for i in range(args.warmup):
         one(i)
     torch.cuda.synchronize()
-    clk = ClockSampler(os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
-                                    else "/tmp", "clocks_bench_r%d.csv" % rank))
+    clk = ClockSampler(clock_log_path(args, rank))
     loop_ms = 0.0
     with clk:
         t0 = time.perf_counter()
@@ -616,6 +627,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=15.0)
     ap.add_argument("--kernel-reps", type=int, default=20)
     ap.add_argument("--nt", type=int, default=0, help="override NT (profiling runs only)")
+    ap.add_argument("--clock-log", default="", help="file for the clock samples of the timed region "
+                    "(default: the system temporary directory)")
     args = ap.parse_args()
     if args.workload in GRADIENT_WORKLOADS:
         return run_gradient(args)
@@ -654,8 +667,7 @@ def main():
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    clk = ClockSampler(os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
-                                    else "/tmp", "clocks_bench_r%d.csv" % rank))
+    clk = ClockSampler(clock_log_path(args, rank))
     loop_ms = 0.0
     with clk:
         torch.cuda.synchronize()
@@ -673,8 +685,10 @@ def main():
     total_updates = cells * w["nt"] * args.steps * world
     value = total_updates / (loop_ms / 1e3) / 1e9
     e2e = total_updates / wall / 1e9
-    # kernel-level roofline (dominant kernel = stress update)
-    kv, ks, ksurf = plan.bench_kernels(args.kernel_reps)
+    # kernel-level roofline: the fused step kernel where the plan runs it
+    # (velocity + stress + free surface in one launch per step), else the
+    # dominant stress update
+    kv, ks, ksurf, kfused = plan.bench_kernels(args.kernel_reps)
     ab = algorithmic_bytes(w, 2 if args.fields == "fp16" else 4)
     peak, peak_kind = measured_peaks()
     s_gbs = ab["s"] / (ks / 1e3) / 1e9
@@ -682,6 +696,7 @@ def main():
     step_ms = loop_ms / args.steps / w["nt"]
     fused_gbs = ab["fused"] / (step_ms / 1e3) / 1e9
     fam = plan.kernel_family
+    fused = bool(plan.fused_step and kfused > 0)
     kname = {"vector": "k_s3d_q4<%d>" % w["L"], "tma": "k_tma<1,%d,*>" % w["L"],
              "stream": "k_s3d_stream<4,%d%s>" % (w["L"], ",half" if args.fields == "fp16" else ""),
              "register": "k_s3d_fast", "general": "k_s3d", "2d": "k_s2d"}[fam]
@@ -689,6 +704,13 @@ def main():
                                            "stream": "streaming", "register": "register-blocked",
                                            "general": "general", "2d": "general 2D"}[fam],
                                           ", FP16 storage" if args.fields == "fp16" else "", kname)
+    if fused:
+        kname = "k_fused3d_q4<%d>" % w["L"]
+        skern = "fused 3D step: velocity, stress, memory variables, free surface (%s)" % kname
+        k_bytes, k_ms = ab["fused"], kfused
+    else:
+        k_bytes, k_ms = ab["s"], ks
+    k_gbs = k_bytes / (k_ms / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic_%s.json" % args.workload)
     if os.path.exists(tpath):
@@ -703,10 +725,13 @@ def main():
             cpu = {"error": str(e)[:200]}
     h2d = sp.nbytes + src.nbytes + rp.nbytes
     d2h = len(outs) * rp.shape[0] * w["nt"] * 4
-    if w["nd"] == 3:
-        launches_per_shot = w["nt"] * (4 + (1 if w["freesurf"] else 0))
+    checks = (w["nt"] + 63) // 64   # finite checks of the instability detection
+    if w["nd"] == 3 and fused:      # sources, fused step, receivers
+        launches_per_shot = 3 * w["nt"] + checks
+    elif w["nd"] == 3:
+        launches_per_shot = w["nt"] * (4 + (1 if w["freesurf"] else 0)) + checks
     else:   # 2D modelling: update_v and the fused stress/surface/receiver/source launch
-        launches_per_shot = 2 * w["nt"] + 1
+        launches_per_shot = 2 * w["nt"] + 1 + checks
     field_gb = cells * 4 * (9 + 6 * w["L"]) / 1e9 if w["nd"] == 3 else cells * 4 * (5 + 3 * w["L"]) / 1e9
     l2 = ("inputs larger than L2 (%.2f GB of fields)" % field_gb if field_gb > 0.126 else
           "working set L2-resident by design (%.1f MB of fields, reread every time step); no flush" % (field_gb * 1e3))
@@ -728,13 +753,17 @@ def main():
                    "l2": l2},
         "e2e": {"value": round(e2e, 3), "unit": "Gcell-updates/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
-        "roofline": {"bound": "hbm", "kernel": skern, "achieved": round(s_gbs, 1),
-                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(s_gbs / peak, 4),
-                     "traffic": traffic, "bytes_per_cell": round(ab["s"] / cells, 2),
-                     "velocity_kernel_gbs": round(v_gbs, 1), "kernel_ms": [round(kv, 4), round(ks, 4),
-                                                                           round(ksurf, 4)],
+        "roofline": {"bound": "hbm", "kernel": skern, "achieved": round(k_gbs, 1),
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(k_gbs / peak, 4),
+                     "traffic": traffic, "bytes_per_cell": round(k_bytes / cells, 2),
+                     "kernel_ms": round(k_ms, 4),
+                     "separate_kernels": {"velocity_ms": round(kv, 4), "stress_ms": round(ks, 4),
+                                          "surface_ms": round(ksurf, 4), "velocity_gbs": round(v_gbs, 1),
+                                          "stress_gbs": round(s_gbs, 1)},
                      "fused_min_bytes_per_cell": round(ab["fused"] / cells, 2),
-                     "step_effective_gbs_fused_basis": round(fused_gbs, 1)},
+                     "step_ms": round(step_ms, 4),
+                     "step_effective_gbs_fused_basis": round(fused_gbs, 1),
+                     "step_frac_fused_basis": round(fused_gbs / peak, 4)},
         "cpu_baseline": cpu,
         "gpu_launches": launches_per_shot * args.steps,
         "clocks": clk.summary(local),

@@ -348,11 +348,20 @@ int sfd_plan_kernel_family(const sfd_plan *plan);
  * written, or a negative error. */
 int64_t sfd_debug_copy(sfd_plan *plan, int kind, int id, float *dst, int64_t cap);
 
-/* Kernel timing for benchmarks: runs the velocity update, the stress update
- * and (with a free surface) the surface kernel `nrep` times each on the
- * plan's stream, bracketed by CUDA events, and writes the mean milliseconds
- * per launch to out_ms[0..2].  The wave fields are modified. */
+/* Kernel timing for benchmarks: runs the velocity update, the stress update,
+ * (with a free surface) the surface kernel and (where the plan has it) the
+ * fused 3D step `nrep` times each on the plan's stream, bracketed by CUDA
+ * events, and writes the mean milliseconds per launch to out_ms[0..3] (0 for
+ * a kernel not run).  The wave fields are modified. */
 int sfd_bench_kernels(sfd_plan *plan, int nrep, float *out_ms);
+
+/* 1 when the plan's 3D modelling runs (sfd_forward without saved boundaries,
+ * DFT or movie, one shot) advance each time step in one fused launch --
+ * velocity, stress, memory variables and free surface (3D, 8th order, nz a
+ * multiple of 4, FP32 fields, L <= 3, kernels 0, batch 1) -- else 0.  No
+ * counterpart in the reference, which launches update_v and update_s
+ * separately (src/time_stepping.c:426-479). */
+int sfd_plan_fused_step(const sfd_plan *plan);
 
 /* Milliseconds spent in the device time loop of the last sfd_forward /
  * sfd_adjoint (CUDA events on the plan's stream). */

@@ -278,6 +278,13 @@ int alloc_model(sfd_plan *p)
     p->d_ticket = (int *)dalloc(p, 2 * sizeof(int), &e);
     if (e) return fail(p, SFD_ERR_MEMORY, "step counter allocation failed");
     p->d_unstable = p->d_ticket + 1;
+    // fused 3D step: ticket counter and per-unit flags (single-shot plans)
+    const FusedShape fsh = fused_shape(g);
+    p->d_fsync = nullptr;
+    if (p->batch == 1 && fsh.units) {
+        p->d_fsync = (int *)dalloc(p, sizeof(int) * (size_t)(1 + fsh.units), &e);
+        if (e) return fail(p, SFD_ERR_MEMORY, "fused-step flag allocation failed");
+    }
     for (int ax = 0; ax < 3; ax++)
         for (int h = 0; h < 2; h++) p->f.kinv[ax][h] = cst + 3 * NC * nc + nc + (2 * ax + h) * nc;
     return SFD_OK;
@@ -959,6 +966,7 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     p->d_surf_q = nullptr;
     p->d_ticket = nullptr;
     p->d_unstable = nullptr;
+    p->d_fsync = nullptr;
     p->dev_bytes = 0;
     p->batch = std::max(1, c.batch);
     p->fwd_nb = 0;
@@ -1010,6 +1018,12 @@ extern "C" int sfd_footprint(const sfd_config *cfg, int gradient, int nsrc, int6
     const int64_t cs = std::max<int64_t>(nsrc, 16), cr = std::max<int64_t>(nrec_sel, 16);
     b += cs * (8 + 4 + 12 + 4 + 12 + 4 * nt) + cr * (8 + 8 * nt);
     b += 2 * sizeof(int);   // fused-step block counter, instability flag
+    {
+        Grid gk = g;
+        gk.kernels = cfg->kernels;
+        const FusedShape fsh = fused_shape(gk);
+        if (B == 1 && fsh.units) b += 4 * (1 + fsh.units);   // fused 3D step tickets and flags
+    }
     if (gradient) {
         const bool bp2 = cfg->back_prop_type == 2;
         int ng = 0;
@@ -1259,8 +1273,12 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     // both made a 256^3 step slower (1.31 and 1.19 ms against 1.13).
     const bool fuse2d = (g.nd == 2 || g.nd == 22) && g.kernels != 1 && !save_boundaries && !dft && !mv.n;
     if (fuse2d) CKC(cudaMemsetAsync(p->d_ticket, 0, sizeof(int), st));
+    // 3D modelling runs: one launch per step for the velocity, stress and
+    // free-surface updates (sfd_kernels.cu, fused 3D forward step)
+    const FusedShape fsh = fused_shape(g);
+    const bool fuse3d = g.nd == 3 && nshot == 1 && p->d_fsync && fsh.units && !save_boundaries && !dft && !mv.n;
     LoopKey key;
-    key.add(mv.n); key.add(p->movout); key.add(p->d_mov); key.add(fuse2d); key.add(p->d_ticket);
+    key.add(mv.n); key.add(p->movout); key.add(p->d_mov); key.add(fuse2d); key.add(p->d_ticket); key.add(fuse3d);
     key.add(1); key.add(p->g); key.add(p->f); key.add_points(S); key.add_points(R); key.add(p->d_src);
     key.add(p->d_seis); key.add(omask); key.add(dft); key.add(save_boundaries != 0); key.add(bs);
     key.add(p->cfg.precision); key.add(tmax); key.add(tmin); key.add(ckpt); key.add(p->d_snap);
@@ -1282,6 +1300,16 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
                 launch_update_v(g, p->f, s);
                 StepTail tl{p->d_ticket, R, p->d_seis, omask, t, S, p->d_src, t + 1 < tmax ? t + 1 : -1, NT};
                 launch_update_s_step(g, p->f, tl, s);
+                check(t, s);
+            }
+            return;
+        }
+        if (fuse3d) {
+            cudaMemsetAsync(p->d_fsync, 0, sizeof(int) * (size_t)(1 + fsh.units), s);
+            for (int t = 0; t < tmax; t++) {
+                launch_sources(g, p->f, S, p->d_src, NT, t, 1, s);
+                launch_fused_step(g, p->f, p->d_fsync, t, s);
+                launch_record(g, p->f, R, p->d_seis, NT, t, omask, s);
                 check(t, s);
             }
             return;
@@ -1316,6 +1344,8 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     cudaEventElapsedTime(&p->last_ms, p->ev0, p->ev1);
     if (tma_take_status())
         return fail(p, SFD_ERR_CUDA, "a TMA stage of the 3D stencil kernels did not arrive within its time bound");
+    if (fuse3d && fused_take_status())
+        return fail(p, SFD_ERR_CUDA, "a fused 3D step did not see its neighbours' velocities within its time bound");
     if ((rc = take_unstable(p, st, "forward"))) return rc;
     p->have_forward = save_boundaries != 0;
     p->fwd_nb = nshot;
@@ -1676,14 +1706,18 @@ extern "C" int sfd_bench_kernels(sfd_plan *p, int nrep, float *out_ms)
     cudaStream_t st = p->stream;
     p->g.nb = 1;
     const Grid &g = p->g;
-    for (int k = 0; k < 3; k++) out_ms[k] = 0.0f;
-    for (int which = 0; which < 3; which++) {
-        if (which == 2 && !g.freesurf) break;
+    for (int k = 0; k < 4; k++) out_ms[k] = 0.0f;
+    const bool fused = p->d_fsync && fused_shape(g).units;
+    for (int which = 0; which < 4; which++) {
+        if (which == 2 && !g.freesurf) continue;
+        if (which == 3 && !fused) break;
+        if (which == 3) CKC(cudaMemsetAsync(p->d_fsync, 0, sizeof(int) * (size_t)(1 + fused_shape(g).units), st));
         CKC(cudaEventRecord(p->ev0, st));
         for (int r = 0; r < nrep; r++) {
             if (which == 0) launch_update_v(g, p->f, st);
             else if (which == 1) launch_update_s(g, p->f, st);
-            else launch_surface(g, p->f, 1, st);
+            else if (which == 2) launch_surface(g, p->f, 1, st);
+            else launch_fused_step(g, p->f, p->d_fsync, r, st);
         }
         CKC(cudaEventRecord(p->ev1, st));
         CKC(cudaEventSynchronize(p->ev1));
@@ -1692,7 +1726,15 @@ extern "C" int sfd_bench_kernels(sfd_plan *p, int nrep, float *out_ms)
         cudaEventElapsedTime(&ms, p->ev0, p->ev1);
         out_ms[which] = ms / nrep;
     }
+    if (fused && fused_take_status())
+        return fail(p, SFD_ERR_CUDA, "a fused 3D step did not see its neighbours' velocities within its time bound");
     return SFD_OK;
+}
+
+extern "C" int sfd_plan_fused_step(const sfd_plan *p)
+{
+    if (!p) return SFD_ERR_ARG;
+    return p->d_fsync && fused_shape(p->g).units ? 1 : 0;
 }
 
 // ------------------------------------------------------------ host-only

@@ -106,6 +106,13 @@ struct PointSet {           // sources or receivers of one shot, device side
     const int *kz;          // z cell index (free-surface adjoint skip)
 };
 
+struct FusedSync {          // fused 3D step: work-unit tickets and flags
+    unsigned *ticket;       // CTAs of the run so far (zeroed before step 0; wraps)
+    int *flags;             // per unit: last step (+1) whose velocities are done
+    unsigned base;          // tickets taken by the run's earlier steps (mod 2^32)
+    int ntz, nty;           // tiles along z and y
+};
+
 struct StepTail {           // fused 2D forward step: the work of its last block
     int *ticket;            // blocks finished; 0 between launches
     PointSet rec;           // receivers recorded at step t into out [nsel][nrec][nt_total]
@@ -150,6 +157,7 @@ struct sfd_plan {
     float *d_surf_q;        // surface-adjoint scratch [nx][ny]
     int *d_ticket;          // fused 2D steps: block counter of the stress launch
     int *d_unstable;        // first checked step with a non-finite wave field (INT_MAX: none)
+    int *d_fsync;           // fused 3D step: ticket counter + one flag per work unit
     // checkpointed gradients (cfg.checkpoint = K > 0)
     char *d_snap;           // [nseg] snapshots: wave fields, memory variables (store type), CPML (FP32)
     char *d_seg;            // [K][wave fields] of the segment being backpropagated (store type)

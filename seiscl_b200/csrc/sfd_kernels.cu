@@ -813,32 +813,53 @@ __device__ __forceinline__ void stq(__half *p, const Q4 &q)
     u.y = *reinterpret_cast<const unsigned *>(&b);
     *reinterpret_cast<uint2 *>(p) = u;
 }
+// Load policy of the stencil reads (template parameter LP): 0 the read-only
+// path (__ldg; arrays no thread writes during the launch), 1 a plain global
+// load (arrays that other CTAs write later in the same launch, read before
+// they do), 2 L2 only (__ldcg: values other CTAs wrote earlier in the same
+// launch, which a stale L1 line must not hide).
+template <int LP>
+__device__ __forceinline__ Q4 ldq_p(const float *p)
+{
+    float4 t;
+    if constexpr (LP == 0) t = __ldg(reinterpret_cast<const float4 *>(p));
+    else if constexpr (LP == 1) t = *reinterpret_cast<const float4 *>(p);
+    else t = __ldcg(reinterpret_cast<const float4 *>(p));
+    return Q4{{t.x, t.y, t.z, t.w}};
+}
+template <int LP>
+__device__ __forceinline__ Q4 ldq_p(const __half *p)
+{
+    static_assert(LP == 0, "FP16 fields are read through the read-only path only");
+    return ldq(p);
+}
+
 // forward / backward differences of four cells along a stride (x or y)
-template <int F, class T>
+template <int F, class T, int LP = 0>
 __device__ __forceinline__ Q4 dfw_q(const T *__restrict__ v, i64 i, i64 st, const float *hc)
 {
-    Q4 a = ldq(v + i + st), b = ldq(v + i), r;
+    Q4 a = ldq_p<LP>(v + i + st), b = ldq_p<LP>(v + i), r;
 #pragma unroll
     for (int j = 0; j < 4; j++) r.v[j] = hc[0] * (a.v[j] - b.v[j]);
 #pragma unroll
     for (int m = 2; m <= F; m++) {
-        a = ldq(v + i + m * st);
-        b = ldq(v + i - (m - 1) * st);
+        a = ldq_p<LP>(v + i + m * st);
+        b = ldq_p<LP>(v + i - (m - 1) * st);
 #pragma unroll
         for (int j = 0; j < 4; j++) r.v[j] = fmaf(hc[m - 1], a.v[j] - b.v[j], r.v[j]);
     }
     return r;
 }
-template <int F, class T>
+template <int F, class T, int LP = 0>
 __device__ __forceinline__ Q4 dbw_q(const T *__restrict__ v, i64 i, i64 st, const float *hc)
 {
-    Q4 a = ldq(v + i), b = ldq(v + i - st), r;
+    Q4 a = ldq_p<LP>(v + i), b = ldq_p<LP>(v + i - st), r;
 #pragma unroll
     for (int j = 0; j < 4; j++) r.v[j] = hc[0] * (a.v[j] - b.v[j]);
 #pragma unroll
     for (int m = 2; m <= F; m++) {
-        a = ldq(v + i + (m - 1) * st);
-        b = ldq(v + i - m * st);
+        a = ldq_p<LP>(v + i + (m - 1) * st);
+        b = ldq_p<LP>(v + i - m * st);
 #pragma unroll
         for (int j = 0; j < 4; j++) r.v[j] = fmaf(hc[m - 1], a.v[j] - b.v[j], r.v[j]);
     }
@@ -848,13 +869,13 @@ __device__ __forceinline__ Q4 dbw_q(const T *__restrict__ v, i64 i, i64 st, cons
 struct W12 {
     float w[12];
 };
-template <class T>
+template <class T, int LP = 0>
 __device__ __forceinline__ W12 ldw(const T *__restrict__ v, i64 i)
 {
     W12 r;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        const Q4 t = ldq(v + i - 4 + 4 * k);
+        const Q4 t = ldq_p<LP>(v + i - 4 + 4 * k);
         r.w[4 * k] = t.v[0]; r.w[4 * k + 1] = t.v[1]; r.w[4 * k + 2] = t.v[2]; r.w[4 * k + 3] = t.v[3];
     }
     return r;
@@ -1011,26 +1032,29 @@ __device__ __forceinline__ void cpml_v3d_q4(const Grid &g, const Fields &f, int 
     const i64 iv = gx * sx + (i64)gy * sy + gz0;                                       \
     const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
 
-template <class T, bool MB>
-__device__ __forceinline__ void v3d_q4(const Grid &g, Fields f)
+// velocity update of the quad (gz0..gz0+3, gy, gx); LP: load policy of the
+// stress reads
+template <class T, int LP = 0>
+__device__ __forceinline__ void v3d_q4_at(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip)
 {
-    CELL3D_Q4
+    constexpr int F = 4;
+    const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;
     const float *hc = g.hc;
     T *wvx = fld<T>(f.w[VX]), *wvy = fld<T>(f.w[VY]), *wvz = fld<T>(f.w[VZ]);
     const T *Sxx = fld<T>(f.w[SXX]), *Syy = fld<T>(f.w[SYY]), *Szz = fld<T>(f.w[SZZ]);
     const T *Sxy = fld<T>(f.w[SXY]), *Syz = fld<T>(f.w[SYZ]), *Sxz = fld<T>(f.w[SXZ]);
     Q4 vx = ldq_rw(wvx + iv), vy = ldq_rw(wvy + iv), vz = ldq_rw(wvz + iv);
     const Q4 rip = ldq(f.p[PRIP] + ip), rjp = ldq(f.p[PRJP] + ip), rkp = ldq(f.p[PRKP] + ip);
-    const W12 wzz = ldw(Szz, iv), wxz = ldw(Sxz, iv), wyz = ldw(Syz, iv);
+    const W12 wzz = ldw<T, LP>(Szz, iv), wxz = ldw<T, LP>(Sxz, iv), wyz = ldw<T, LP>(Syz, iv);
     Q4 szz_z = dfw_z<F>(wzz, hc);
-    Q4 sxx_x = dfw_q<F>(Sxx, iv, sx, hc);
-    Q4 sxz_x = dbw_q<F>(Sxz, iv, sx, hc);
+    Q4 sxx_x = dfw_q<F, T, LP>(Sxx, iv, sx, hc);
+    Q4 sxz_x = dbw_q<F, T, LP>(Sxz, iv, sx, hc);
     Q4 sxz_z = dbw_z<F>(wxz, hc);
-    Q4 syz_y = dbw_q<F>(Syz, iv, sy, hc);
+    Q4 syz_y = dbw_q<F, T, LP>(Syz, iv, sy, hc);
     Q4 syz_z = dbw_z<F>(wyz, hc);
-    Q4 syy_y = dfw_q<F>(Syy, iv, sy, hc);
-    Q4 sxy_x = dbw_q<F>(Sxy, iv, sx, hc);
-    Q4 sxy_y = dbw_q<F>(Sxy, iv, sy, hc);
+    Q4 syy_y = dfw_q<F, T, LP>(Syy, iv, sy, hc);
+    Q4 sxy_x = dbw_q<F, T, LP>(Sxy, iv, sx, hc);
+    Q4 sxy_y = dbw_q<F, T, LP>(Sxy, iv, sy, hc);
     if (g.abs_type == 1) cpml_v3d_q4(g, f, gz0, gy, gx, sxx_x, syy_y, szz_z, sxy_y, sxy_x, syz_y, syz_z, sxz_x, sxz_z);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
@@ -1043,6 +1067,13 @@ __device__ __forceinline__ void v3d_q4(const Grid &g, Fields f)
     stq(wvx + iv, vx);
     stq(wvy + iv, vy);
     stq(wvz + iv, vz);
+}
+
+template <class T, bool MB>
+__device__ __forceinline__ void v3d_q4(const Grid &g, Fields f)
+{
+    CELL3D_Q4
+    v3d_q4_at<T, 0>(g, f, gz0, gy, gx, iv, ip);
 }
 
 template <class T, bool MB = false>
@@ -1144,9 +1175,17 @@ __device__ __forceinline__ void cpml_s3d_q4(const Grid &g, const Fields &f, int 
 // sxz with rxy, ryz, rxz) -- each loading only its own memory variables and
 // parameters, so the live state fits in registers; the components are
 // independent, so the split changes no result.
+//
+// surf: the free surface of the same step follows the update in registers
+// (the fused step kernel; k_surf3d's arithmetic at z = F, forward direction):
+// the quad at gz0 = F zeroes szz and rzz there, corrects sxx, syy, rxx, ryy
+// with the velocity derivatives of the update (CPML-corrected as k_surf3d
+// forms them) and writes the images szz(F-m) = -szz(F+m) for m = 1..3 and
+// sxz(F-m) = -sxz(F+m-1), syz(F-m) = -syz(F+m-1) for m = 1..4; the quad at
+// gz0 = F+4 writes szz(F-4) = -szz(F+4).
 template <int L, class T>
 __device__ __forceinline__ void s_normal_q4(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip,
-                                            const Q4 &vxx, const Q4 &vyy, const Q4 &vzz)
+                                            const Q4 &vxx, const Q4 &vyy, const Q4 &vzz, bool surf = false)
 {
     T *const ws[3] = {fld<T>(f.w[SXX]), fld<T>(f.w[SYY]), fld<T>(f.w[SZZ])};
     T *const wr[3] = {fld<T>(f.r[RXX]), fld<T>(f.r[RYY]), fld<T>(f.r[RZZ])};
@@ -1154,6 +1193,8 @@ __device__ __forceinline__ void s_normal_q4(const Grid &g, const Fields &f, int 
 #pragma unroll
     for (int q = 0; q < 3; q++) sq[q] = ldq_rw(ws[q] + iv);
     const Q4 qM = ldq(f.p[PM] + ip), qmu = ldq(f.p[PMU] + ip);
+    Q4 rq[3][L > 0 ? L : 1];
+    Q4 qtaup, qtaus;
     if constexpr (L == 0) {
 #pragma unroll
         for (int j = 0; j < 4; j++) {
@@ -1165,8 +1206,8 @@ __device__ __forceinline__ void s_normal_q4(const Grid &g, const Fields &f, int 
             sq[2].v[j] += gm * vxxyyzz - fm * vxxyy;
         }
     } else {
-        const Q4 qtaup = ldq(f.p[PTAUP] + ip), qtaus = ldq(f.p[PTAUS] + ip);
-        Q4 rq[3][L];
+        qtaup = ldq(f.p[PTAUP] + ip);
+        qtaus = ldq(f.p[PTAUS] + ip);
 #pragma unroll
         for (int l = 0; l < L; l++)
 #pragma unroll
@@ -1200,10 +1241,6 @@ __device__ __forceinline__ void s_normal_q4(const Grid &g, const Fields &f, int 
 #pragma unroll
             for (int q = 0; q < 3; q++) sq[q].v[j] += ls[q] + g.dt2 * a[q];
         }
-#pragma unroll
-        for (int l = 0; l < L; l++)
-#pragma unroll
-            for (int q = 0; q < 3; q++) stq(wr[q] + l * g.nvol + iv, rq[q][l]);
     }
     if (g.abs_type == 2) {
 #pragma unroll
@@ -1214,13 +1251,59 @@ __device__ __forceinline__ void s_normal_q4(const Grid &g, const Fields &f, int 
             for (int q = 0; q < 3; q++) sq[q].v[j] = v3[q];
         }
     }
+    if (surf && gz0 == g.F + 4) stv(ws[2] + iv - 8, -sq[2].v[0]);
+    if (surf && gz0 == g.F) {
+        const float vx0 = vxx.v[0], vy0 = vyy.v[0], vz0 = vzz.v[0];
+        sq[2].v[0] = 0.0f;
+        if constexpr (L == 0) {
+            float fm = qmu.v[0] * 2.0f, gm = qM.v[0];
+            float h = -((gm - fm) * (gm - fm) * (vx0 + vy0) / gm) - ((gm - fm) * vz0);
+            sq[0].v[0] += h;
+            sq[1].v[0] += h;
+        } else {
+            const float taus = qtaus.v[0], taup = qtaup.v[0], mu = qmu.v[0], M = qM.v[0];
+            float fm = mu * 2.0f * (1.0f + L * taus);
+            float gm = M * (1.0f + L * taup);
+            float h = -((gm - fm) * (gm - fm) * (vx0 + vy0) / gm) - ((gm - fm) * vz0);
+            float sumx = 0, sumy = 0;
+#pragma unroll
+            for (int l = 0; l < L; l++) {
+                rq[2][l].v[0] = 0.0f;
+                sumx += rq[0][l].v[0];
+                sumy += rq[1][l].v[0];
+            }
+            sq[0].v[0] = sq[0].v[0] + (h - g.dt2 * sumx);
+            sq[1].v[0] = sq[1].v[0] + (h - g.dt2 * sumy);
+            float d = 2.0f * mu * taus / g.dt, e = M * taup / g.dt;
+            sumx = 0; sumy = 0;
+#pragma unroll
+            for (int l = 0; l < L; l++) {
+                float b = g.eta[l] / (1.0f + g.eta[l] * 0.5f);
+                float hh = b * (((d - e) * ((fm / gm) - 1.0f) * (vx0 + vy0)) - ((d - e) * vz0));
+                rq[0][l].v[0] += hh;
+                rq[1][l].v[0] += hh;
+                sumx += rq[0][l].v[0];
+                sumy += rq[1][l].v[0];
+            }
+            sq[0].v[0] += g.dt2 * sumx;
+            sq[1].v[0] += g.dt2 * sumy;
+        }
+#pragma unroll
+        for (int m = 1; m <= 3; m++) stv(ws[2] + iv - m, -sq[2].v[m]);
+    }
+    if constexpr (L > 0) {
+#pragma unroll
+        for (int l = 0; l < L; l++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) stq(wr[q] + l * g.nvol + iv, rq[q][l]);
+    }
 #pragma unroll
     for (int q = 0; q < 3; q++) stq(ws[q] + iv, sq[q]);
 }
 
 template <int L, class T>
 __device__ __forceinline__ void s_shear_q4(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip,
-                                           const Q4 &vxyyx, const Q4 &vyzzy, const Q4 &vxzzx)
+                                           const Q4 &vxyyx, const Q4 &vyzzy, const Q4 &vxzzx, bool surf = false)
 {
     T *const ws[3] = {fld<T>(f.w[SXY]), fld<T>(f.w[SYZ]), fld<T>(f.w[SXZ])};
     T *const wr[3] = {fld<T>(f.r[RXY]), fld<T>(f.r[RYZ]), fld<T>(f.r[RXZ])};
@@ -1287,22 +1370,33 @@ __device__ __forceinline__ void s_shear_q4(const Grid &g, const Fields &f, int g
             for (int q = 0; q < 3; q++) sq[q].v[j] = v3[q];
         }
     }
+    if (surf && gz0 == g.F) {
+#pragma unroll
+        for (int m = 1; m <= 4; m++) {
+            stv(ws[2] + iv - m, -sq[2].v[m - 1]);   // sxz
+            stv(ws[1] + iv - m, -sq[1].v[m - 1]);   // syz
+        }
+    }
 #pragma unroll
     for (int q = 0; q < 3; q++) stq(ws[q] + iv, sq[q]);
 }
 
-template <int L, class T, bool MB = false>
-__global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f)
+// stress update of the quad (gz0..gz0+3, gy, gx); LP: load policy of the
+// velocity reads; surf: free surface folded in (see s_normal_q4)
+template <int L, class T, int LP = 0>
+__device__ __forceinline__ void s3d_q4_at(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip,
+                                          bool surf = false)
 {
-    CELL3D_Q4
+    constexpr int F = 4;
+    const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;
     const float *hc = g.hc;
     const T *Vx = fld<T>(f.w[VX]), *Vy = fld<T>(f.w[VY]), *Vz = fld<T>(f.w[VZ]);
-    Q4 vzz = dbw_z<F>(ldw(Vz, iv), hc);
-    Q4 vyz = dfw_z<F>(ldw(Vy, iv), hc);
-    Q4 vxz = dfw_z<F>(ldw(Vx, iv), hc);
-    Q4 vzx = dfw_q<F>(Vz, iv, sx, hc), vzy = dfw_q<F>(Vz, iv, sy, hc);
-    Q4 vyx = dfw_q<F>(Vy, iv, sx, hc), vyy = dbw_q<F>(Vy, iv, sy, hc);
-    Q4 vxx = dbw_q<F>(Vx, iv, sx, hc), vxy = dfw_q<F>(Vx, iv, sy, hc);
+    Q4 vzz = dbw_z<F>(ldw<T, LP>(Vz, iv), hc);
+    Q4 vyz = dfw_z<F>(ldw<T, LP>(Vy, iv), hc);
+    Q4 vxz = dfw_z<F>(ldw<T, LP>(Vx, iv), hc);
+    Q4 vzx = dfw_q<F, T, LP>(Vz, iv, sx, hc), vzy = dfw_q<F, T, LP>(Vz, iv, sy, hc);
+    Q4 vyx = dfw_q<F, T, LP>(Vy, iv, sx, hc), vyy = dbw_q<F, T, LP>(Vy, iv, sy, hc);
+    Q4 vxx = dbw_q<F, T, LP>(Vx, iv, sx, hc), vxy = dfw_q<F, T, LP>(Vx, iv, sy, hc);
     if (g.abs_type == 1) cpml_s3d_q4(g, f, gz0, gy, gx, vxx, vxy, vxz, vyx, vyy, vyz, vzx, vzy, vzz);
     Q4 vxyyx, vyzzy, vxzzx;
 #pragma unroll
@@ -1311,8 +1405,183 @@ __global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f)
         vyzzy.v[j] = vyz.v[j] + vzy.v[j];
         vxzzx.v[j] = vxz.v[j] + vzx.v[j];
     }
-    s_normal_q4<L, T>(g, f, gz0, gy, gx, iv, ip, vxx, vyy, vzz);
-    s_shear_q4<L, T>(g, f, gz0, gy, gx, iv, ip, vxyyx, vyzzy, vxzzx);
+    s_normal_q4<L, T>(g, f, gz0, gy, gx, iv, ip, vxx, vyy, vzz, surf);
+    s_shear_q4<L, T>(g, f, gz0, gy, gx, iv, ip, vxyyx, vyzzy, vxzzx, surf);
+}
+
+template <int L, class T, bool MB = false>
+__global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f)
+{
+    CELL3D_Q4
+    s3d_q4_at<L, T, 0>(g, f, gz0, gy, gx, iv, ip);
+}
+
+// ------------------------------------------------- fused 3D forward step
+// One launch advances the whole grid one time step: velocity update, stress
+// and memory-variable update and (with a free surface) the free surface, so
+// the stresses read by the velocity stencils are read again by the stress
+// update of the same CTA, and the velocities it wrote are read back, while
+// both are still in L2.  Per cell the arithmetic is that of k_v3d_q4,
+// k_s3d_q4 and k_surf3d, in that order.
+//
+// Work unit: a block of FZ z cells x FY y rows (a "tile") times a chunk of
+// FX x planes.  A CTA takes a ticket (atomicAdd) and works on unit number
+// ticket - base, units ordered chunk-major (x slowest), so the units a CTA
+// waits for were always taken by CTAs that started earlier.  Phase 1 updates
+// the velocities of planes [x0 + 4, x1 + 4) of the tile (chunk 0 from x = F,
+// the last chunk up to the grid's end) and publishes the unit's flag; phase
+// 2 waits for the flags of the units whose velocities its stencils read --
+// the same chunk's four y/z neighbours and, for the first 4 planes, the
+// previous chunk's tile and its neighbours -- then updates the stresses of
+// planes [x0, x1).  Everything is updated in place; the waits also order
+// every stress overwrite after all velocity reads of the old value: a
+// stress cell of unit (c, t) is read by the velocity stencils of units
+// (c, t), (c, t's y/z neighbours) and (c - 1, t and its neighbours) only,
+// the units (c, t) waits for.  A unit waits at most ntz tickets ahead, so
+// progress needs only ntz + 2 co-resident CTAs (ntz <= 64 is required).
+// Reads of velocities in phase 2 go through L2 (__ldcg): other CTAs wrote
+// them during the launch.  Waits are bounded (FUSED_WAIT_NS of
+// %globaltimer); a wait that runs out sets g_fused_status, which makes every
+// later CTA and launch skip its work and the host report an error.
+constexpr int FZ = 32, FY = 8, FX = 8;
+constexpr unsigned long long FUSED_WAIT_NS = 2000000000ull;
+__device__ int g_fused_status;   // 0 ok, 1 a wait ran out
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// wait until *flag >= want; false when the bound ran out or another CTA's did
+__device__ bool fused_wait(const int *flag, int want)
+{
+    if (ld_acquire_gpu(flag) >= want) return true;
+    const unsigned long long t0 = global_ns();
+    unsigned ns = 32;
+    for (;;) {
+        __nanosleep(ns);
+        if (ns < 512) ns *= 2;
+        if (ld_acquire_gpu(flag) >= want) return true;
+        if (*(volatile int *)&g_fused_status) return false;
+        if (global_ns() - t0 > FUSED_WAIT_NS) return false;
+    }
+}
+
+template <int L>
+__global__ void __launch_bounds__(128, 4) k_fused3d_q4(Grid g, Fields f, FusedSync fs, int epoch)
+{
+    constexpr int F = 4;
+    __shared__ int s_unit, s_go;
+    const int tid = threadIdx.x + 8 * (threadIdx.y + 4 * threadIdx.z);
+    if (tid == 0) {
+        s_unit = (int)(atomicAdd(fs.ticket, 1u) - fs.base);
+        s_go = *(volatile int *)&g_fused_status == 0;
+    }
+    __syncthreads();
+    if (!s_go) return;
+    const int ntile = fs.ntz * fs.nty, unit = s_unit;
+    const int c = unit / ntile, tile = unit - c * ntile, ty = tile / fs.ntz, tz = tile - ty * fs.ntz;
+    const int gz0 = F + tz * FZ + 4 * threadIdx.x;
+    const bool zok = gz0 <= g.NZ - F - 1;
+    const int xs0 = F + c * FX, xs1 = min(xs0 + FX, g.NX - F);
+    const int xv0 = c == 0 ? F : xs0 + 4, xv1 = min(xs1 + 4, g.NX - F);
+    const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;
+    // phase 1: velocities (stress reads: plain loads, written later in the launch)
+    if (zok) {
+        for (int gx = xv0 + (int)threadIdx.z; gx < xv1; gx += 4)
+            for (int yy = threadIdx.y; yy < FY; yy += 4) {
+                const int gy = F + ty * FY + yy;
+                if (gy > g.NY - F - 1) continue;
+                const i64 iv = gx * sx + (i64)gy * sy + gz0;
+                const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
+                v3d_q4_at<float, 1>(g, f, gz0, gy, gx, iv, ip);
+            }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        st_release_gpu(fs.flags + unit, epoch);
+        bool ok = true;
+        for (int cc = c; cc >= max(c - 1, 0) && ok; cc--) {
+            const int base = cc * ntile;
+            if (cc != c) ok = ok && fused_wait(fs.flags + base + tile, epoch);
+            if (tz > 0) ok = ok && fused_wait(fs.flags + base + tile - 1, epoch);
+            if (tz < fs.ntz - 1) ok = ok && fused_wait(fs.flags + base + tile + 1, epoch);
+            if (ty > 0) ok = ok && fused_wait(fs.flags + base + tile - fs.ntz, epoch);
+            if (ty < fs.nty - 1) ok = ok && fused_wait(fs.flags + base + tile + fs.ntz, epoch);
+        }
+        if (!ok) atomicExch(&g_fused_status, 1);
+        s_go = ok;
+        __threadfence();
+    }
+    __syncthreads();
+    if (!s_go || !zok) return;
+    // phase 2: stresses, memory variables, free surface (velocity reads via L2)
+    const bool surf = g.freesurf != 0;
+    for (int gx = xs0 + (int)threadIdx.z; gx < xs1; gx += 4)
+        for (int yy = threadIdx.y; yy < FY; yy += 4) {
+            const int gy = F + ty * FY + yy;
+            if (gy > g.NY - F - 1) continue;
+            const i64 iv = gx * sx + (i64)gy * sy + gz0;
+            const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
+            s3d_q4_at<L, float, 2>(g, f, gz0, gy, gx, iv, ip, surf);
+        }
+}
+
+FusedShape fused_shape(const Grid &g)
+{
+    FusedShape s{0, 0, 0, 0};
+    if (g.nd != 3 || g.F != 4 || g.nz % 4 || g.fhalf || g.L < 0 || g.L > 3 || g.kernels != 0) return s;
+    const int ntz = (g.nz + FZ - 1) / FZ, nty = (g.ny + FY - 1) / FY, nch = (g.nx + FX - 1) / FX;
+    if (ntz > 64) return s;
+    s.ntz = ntz;
+    s.nty = nty;
+    s.nchunk = nch;
+    s.units = (int64_t)ntz * nty * nch;
+    return s;
+}
+
+bool launch_fused_step(const Grid &g, const Fields &f, int *sync, int t, cudaStream_t st)
+{
+    const FusedShape sh = fused_shape(g);
+    if (!sh.units || g.nb != 1 || !sync) return false;
+    static int resident = -1;   // CTAs of the kernel one SM holds (any L; checked once)
+    if (resident < 0) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused3d_q4<3>, 128, 0) != cudaSuccess) n = 0;
+        resident = n;
+    }
+    if (resident < 1) return false;
+    FusedSync fs{reinterpret_cast<unsigned *>(sync), sync + 1, (unsigned)((uint64_t)t * (uint64_t)sh.units),
+                 sh.ntz, sh.nty};
+    const dim3 b(8, 4, 4);
+    const unsigned gr = (unsigned)sh.units;
+    switch (g.L) {
+    case 0: k_fused3d_q4<0><<<gr, b, 0, st>>>(g, f, fs, t + 1); break;
+    case 1: k_fused3d_q4<1><<<gr, b, 0, st>>>(g, f, fs, t + 1); break;
+    case 2: k_fused3d_q4<2><<<gr, b, 0, st>>>(g, f, fs, t + 1); break;
+    default: k_fused3d_q4<3><<<gr, b, 0, st>>>(g, f, fs, t + 1); break;
+    }
+    return true;
+}
+
+int fused_take_status()
+{
+    int v = 0, zero = 0;
+    if (cudaMemcpyFromSymbol(&v, g_fused_status, sizeof(int)) != cudaSuccess) return -1;
+    if (v) cudaMemcpyToSymbol(g_fused_status, &zero, sizeof(int));
+    return v;
 }
 
 // ------------------------------------------- 4-cell vectorised 3D adjoint

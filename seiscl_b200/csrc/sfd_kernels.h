@@ -25,6 +25,19 @@ int tma_take_status();      // 1 if a TMA stage of the last launches never arriv
 // 3 TMA-pipelined, 4 streaming, 5 4-cell vectorised
 int stress_family(const Grid &g, const Fields &f);
 void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st);
+// Fused 3D forward step (velocity, stress, free surface in one launch; see
+// sfd_kernels.cu).  Work units = ntz x nty x nchunk; units = 0 when the plan's
+// grid does not take it (3D, 8th order, nz % 4 == 0, FP32 fields, L <= 3,
+// kernels 0, at most 64 z tiles).
+struct FusedShape {
+    int ntz, nty, nchunk;
+    int64_t units;
+};
+FusedShape fused_shape(const Grid &g);
+// sync: 1 + units ints (a ticket counter, one flag per unit), zeroed before
+// step 0 of a run; t: the step's index in the run.  False: not launched.
+bool launch_fused_step(const Grid &g, const Fields &f, int *sync, int t, cudaStream_t st);
+int fused_take_status();    // 1 if a fused step's wait ran out (and clears it)
 void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st);
 // 2D P-SV and acoustic forward: stress update, free surface, receivers of
 // step tl.t and sources of step tl.tsrc in one launch (false: not 2D)

@@ -70,6 +70,7 @@ EXPORTS = {
     "sfd_plan_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "sfd_plan_uses_tma": (C.c_int, [C.c_void_p]),
     "sfd_plan_kernel_family": (C.c_int, [C.c_void_p]),
+    "sfd_plan_fused_step": (C.c_int, [C.c_void_p]),
     "sfd_debug_copy": (C.c_int64, [C.c_void_p, C.c_int, C.c_int, FP, C.c_int64]),
     "sfd_last_loop_ms": (C.c_float, [C.c_void_p]),
     "sfd_bench_kernels": (C.c_int, [C.c_void_p, C.c_int, FP]),
@@ -420,10 +421,20 @@ class Plan:
         return out[:got]
 
     def bench_kernels(self, nrep: int = 20):
-        """Mean ms per launch of (velocity, stress, surface) kernels."""
-        out = (C.c_float * 3)()
+        """Mean ms per launch of the (velocity, stress, surface, fused step)
+        kernels; 0 for one the plan does not have."""
+        out = (C.c_float * 4)()
         self._check(self.lib.sfd_bench_kernels(self.h, int(nrep), out))
         return list(out)
+
+    @property
+    def fused_step(self) -> bool:
+        """True when 3D modelling runs advance each step in one fused launch
+        (velocity, stress, memory variables, free surface)."""
+        rc = int(self.lib.sfd_plan_fused_step(self.h))
+        if rc < 0:
+            self._check(rc)
+        return rc == 1
 
     @property
     def uses_tma(self) -> bool:
