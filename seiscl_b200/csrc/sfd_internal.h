@@ -111,6 +111,7 @@ struct FusedSync {          // fused 3D step: work-unit tickets and flags
     int *flags;             // per unit: last step (+1) whose velocities are done
     unsigned base;          // tickets taken by the run's earlier steps (mod 2^32)
     int ntz, nty;           // tiles along z and y
+    int units;              // work units of one step
 };
 
 struct StepTail {           // fused 2D forward step: the work of its last block

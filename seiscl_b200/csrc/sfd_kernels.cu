@@ -1491,6 +1491,10 @@ __global__ void __launch_bounds__(128, 4) k_fused3d_q4(Grid g, Fields f, FusedSy
     __syncthreads();
     if (!s_go) return;
     const int ntile = fs.ntz * fs.nty, unit = s_unit;
+    if (unit < 0 || unit >= fs.units) {   // the counter was not reset: never index past the flags
+        if (tid == 0) atomicExch(&g_fused_status, 1);
+        return;
+    }
     const int c = unit / ntile, tile = unit - c * ntile, ty = tile / fs.ntz, tz = tile - ty * fs.ntz;
     const int gz0 = F + tz * FZ + 4 * threadIdx.x;
     const bool zok = gz0 <= g.NZ - F - 1;
@@ -1544,7 +1548,7 @@ FusedShape fused_shape(const Grid &g)
     FusedShape s{0, 0, 0, 0};
     if (g.nd != 3 || g.F != 4 || g.nz % 4 || g.fhalf || g.L < 0 || g.L > 3 || g.kernels != 0) return s;
     const int ntz = (g.nz + FZ - 1) / FZ, nty = (g.ny + FY - 1) / FY, nch = (g.nx + FX - 1) / FX;
-    if (ntz > 64) return s;
+    if (ntz > 64 || (int64_t)ntz * nty * nch > (1 << 30)) return s;
     s.ntz = ntz;
     s.nty = nty;
     s.nchunk = nch;
@@ -1564,7 +1568,7 @@ bool launch_fused_step(const Grid &g, const Fields &f, int *sync, int t, cudaStr
     }
     if (resident < 1) return false;
     FusedSync fs{reinterpret_cast<unsigned *>(sync), sync + 1, (unsigned)((uint64_t)t * (uint64_t)sh.units),
-                 sh.ntz, sh.nty};
+                 sh.ntz, sh.nty, (int)sh.units};
     const dim3 b(8, 4, 4);
     const unsigned gr = (unsigned)sh.units;
     switch (g.L) {
