@@ -591,7 +591,7 @@ FUSED_CASES = [
     dict(nd=3, freesurf=1, L=2, abs_type=1, src_type=2, nz=36, ny=34, nx=38, nt=120, nab=8),
     dict(nd=3, freesurf=1, L=0, abs_type=1, src_type=100, nz=64, ny=16, nx=24, nt=100, nab=8),
     dict(nd=3, freesurf=0, L=1, abs_type=2, src_type=1, nz=40, ny=21, nx=17, nt=100, nab=6),
-    dict(nd=3, freesurf=1, L=3, abs_type=1, src_type=0, nz=100, ny=12, nx=9, nt=80, nab=4),
+    dict(nd=3, freesurf=1, L=3, abs_type=1, src_type=0, nz=100, ny=12, nx=19, nt=80, nab=4),
     dict(nd=3, freesurf=0, L=2, abs_type=1, src_type=100, nz=32, ny=40, nx=44, nt=80, nab=10),
 ]
 
