@@ -126,9 +126,13 @@ def ricker(f0, nt, dt):
         np.float32)
 
 
-def build_workload(name):
-    """Seeded synthetic model and acquisition of a workload (host layout)."""
+def build_workload(name, grid=0):
+    """Seeded synthetic model and acquisition of a workload (host layout);
+    grid > 0 replaces a 3D workload's grid with grid^3 cells (profiling runs;
+    the receiver array then covers what fits)."""
     w = dict(WORKLOADS[name])
+    if grid > 0 and w["nd"] == 3:
+        w["nz"] = w["ny"] = w["nx"] = int(grid)
     nd, nz, ny, nx = w["nd"], w["nz"], w["ny"], w["nx"]
     dh = w["dh"]
     if nd == 3:
@@ -165,8 +169,9 @@ def build_workload(name):
     nt, dt = w["nt"], w["dt"]
     if nd == 3:
         src_pos = np.array([[nx // 2 * dh, ny // 2 * dh, 5 * dh, 0, w["src_type"]]], np.float32)
-        gx, gy = np.meshgrid(np.arange(64) * 4 + 2, np.arange(64) * 4 + 2, indexing="ij")
-        rec = np.zeros((64 * 64, 8), np.float32)
+        nr = min(64, (min(nx, ny) - 3) // 4 + 1)
+        gx, gy = np.meshgrid(np.arange(nr) * 4 + 2, np.arange(nr) * 4 + 2, indexing="ij")
+        rec = np.zeros((nr * nr, 8), np.float32)
         rec[:, 0] = gx.ravel() * dh
         rec[:, 1] = gy.ravel() * dh
         rec[:, 2] = 5 * dh
@@ -627,6 +632,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=15.0)
     ap.add_argument("--kernel-reps", type=int, default=20)
     ap.add_argument("--nt", type=int, default=0, help="override NT (profiling runs only)")
+    ap.add_argument("--grid", type=int, default=0, help="3D workloads: override the grid with n^3 (profiling "
+                    "runs only)")
     ap.add_argument("--clock-log", default="", help="file for the clock samples of the timed region "
                     "(default: the system temporary directory)")
     args = ap.parse_args()
@@ -635,7 +642,7 @@ def main():
     if args.workload == "serving":
         return run_serving(args)
 
-    w, model, acq = build_workload(args.workload)
+    w, model, acq = build_workload(args.workload, grid=args.grid)
     if args.nt > 0:
         w["nt"] = args.nt
         acq["src"] = acq["src"][:, :args.nt].copy()

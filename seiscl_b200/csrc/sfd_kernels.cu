@@ -1501,7 +1501,10 @@ __global__ void __launch_bounds__(128, 4) k_fused3d_q4(Grid g, Fields f, FusedSy
     const int xs0 = F + c * FX, xs1 = min(xs0 + FX, g.NX - F);
     const int xv0 = c == 0 ? F : xs0 + 4, xv1 = min(xs1 + 4, g.NX - F);
     const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;
-    // phase 1: velocities (stress reads: plain loads, written later in the launch)
+    // phase 1: velocities.  The stress reads take the read-only path: no
+    // stress cell this phase reads is overwritten before the phase ends (the
+    // writer waits for this unit's flag), and no reader in this launch
+    // needs a value written in it.
     if (zok) {
         for (int gx = xv0 + (int)threadIdx.z; gx < xv1; gx += 4)
             for (int yy = threadIdx.y; yy < FY; yy += 4) {
@@ -1509,7 +1512,7 @@ __global__ void __launch_bounds__(128, 4) k_fused3d_q4(Grid g, Fields f, FusedSy
                 if (gy > g.NY - F - 1) continue;
                 const i64 iv = gx * sx + (i64)gy * sy + gz0;
                 const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
-                v3d_q4_at<float, 1>(g, f, gz0, gy, gx, iv, ip);
+                v3d_q4_at<float, 0>(g, f, gz0, gy, gx, iv, ip);
             }
     }
     __syncthreads();
