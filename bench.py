@@ -735,8 +735,9 @@ def main():
     checks = (w["nt"] + 63) // 64   # finite checks of the instability detection
     if w["nd"] == 3 and fused:      # sources, fused step, receivers
         launches_per_shot = 3 * w["nt"] + checks
-    elif w["nd"] == 3:
-        launches_per_shot = w["nt"] * (4 + (1 if w["freesurf"] else 0)) + checks
+    elif w["nd"] == 3:   # sources, velocity, stress (FP32 4-cell: with the free surface), [surface], receivers
+        sep_surface = w["freesurf"] and (fam != "vector" or args.fields == "fp16")
+        launches_per_shot = w["nt"] * (4 + (1 if sep_surface else 0)) + checks
     else:   # 2D modelling: update_v and the fused stress/surface/receiver/source launch
         launches_per_shot = 2 * w["nt"] + 1 + checks
     field_gb = cells * 4 * (9 + 6 * w["L"]) / 1e9 if w["nd"] == 3 else cells * 4 * (5 + 3 * w["L"]) / 1e9

@@ -88,7 +88,11 @@ typedef struct sfd_config {
                           2: register-blocked 3D kernels where available,
                           3: TMA-pipelined 3D velocity and stress updates,
                           4: streaming one-thread-per-cell 3D kernels (per-cell loads first),
-                          5: 4-cell vectorised 3D kernels where they apply, else streaming */
+                          5: 4-cell vectorised 3D kernels where they apply, else streaming,
+                          6: as 0, and 3D modelling runs of one shot advance each step in
+                             one fused launch (velocity, stress, memory variables, free
+                             surface; sfd_plan_fused_step).  With 0 the single-shot 3D
+                             modelling stress kernel applies the free surface itself. */
     int adjoint_reset_psi; /* 0: the adjoint continues with the forward run's CPML memory
                               (reference behaviour, src/clprogram.c:806-811); 1: it starts
                               from zeroed CPML memory.  With sources whose wave field is
@@ -357,8 +361,8 @@ int sfd_bench_kernels(sfd_plan *plan, int nrep, float *out_ms);
 
 /* 1 when the plan's 3D modelling runs (sfd_forward without saved boundaries,
  * DFT or movie, one shot) advance each time step in one fused launch --
- * velocity, stress, memory variables and free surface (3D, 8th order, nz a
- * multiple of 4, FP32 fields, L <= 3, kernels 0, batch 1) -- else 0.  No
+ * velocity, stress, memory variables and free surface (kernels 6; 3D, 8th
+ * order, nz a multiple of 4, FP32 fields, L <= 3, batch 1) -- else 0.  No
  * counterpart in the reference, which launches update_v and update_s
  * separately (src/time_stepping.c:426-479). */
 int sfd_plan_fused_step(const sfd_plan *plan);

@@ -6,6 +6,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -874,7 +875,7 @@ int check_config(const sfd_config &c)
     // N[0] must be even (read_hdf5.c:535-540)
     if (c.n[0] % 2) return SFD_ERR_ARG;
     if (c.precision < 0 || c.precision > 2) return SFD_ERR_ARG;
-    if (c.kernels < 0 || c.kernels > 5) return SFD_ERR_ARG;
+    if (c.kernels < 0 || c.kernels > 6) return SFD_ERR_ARG;
     if (c.adjoint_reset_psi < 0 || c.adjoint_reset_psi > 1) return SFD_ERR_ARG;
     if (c.field_precision < 0 || c.field_precision > 1) return SFD_ERR_ARG;
     if (c.field_precision == 1 && (c.nd != 3 || c.L > 3)) return SFD_ERR_UNSUPPORTED;
@@ -913,7 +914,8 @@ void init_grid(const sfd_config &c, Grid &g)
     g.L = c.L;
     g.freesurf = c.freesurf ? 1 : 0;
     g.restype = c.restype;
-    g.kernels = c.kernels;
+    g.kernels = c.kernels == 6 ? 0 : c.kernels;   // 6: the kernels of 0, plus the fused modelling step
+    g.fused = c.kernels == 6;
     g.hout = c.hout;
     g.nvol = (int64_t)g.NZ * g.NY * g.NX;
     double hc[6];
@@ -1019,9 +1021,7 @@ extern "C" int sfd_footprint(const sfd_config *cfg, int gradient, int nsrc, int6
     b += cs * (8 + 4 + 12 + 4 + 12 + 4 * nt) + cr * (8 + 8 * nt);
     b += 2 * sizeof(int);   // fused-step block counter, instability flag
     {
-        Grid gk = g;
-        gk.kernels = cfg->kernels;
-        const FusedShape fsh = fused_shape(gk);
+        const FusedShape fsh = fused_shape(g);
         if (B == 1 && fsh.units) b += 4 * (1 + fsh.units);   // fused 3D step tickets and flags
     }
     if (gradient) {
@@ -1277,6 +1277,7 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     // free-surface updates (sfd_kernels.cu, fused 3D forward step)
     const FusedShape fsh = fused_shape(g);
     const bool fuse3d = g.nd == 3 && nshot == 1 && p->d_fsync && fsh.units && !save_boundaries && !dft && !mv.n;
+    const bool bnd_shells = save_boundaries && !dft && !ckpt;
     LoopKey key;
     key.add(mv.n); key.add(p->movout); key.add(p->d_mov); key.add(fuse2d); key.add(p->d_ticket); key.add(fuse3d);
     key.add(1); key.add(p->g); key.add(p->f); key.add_points(S); key.add_points(R); key.add(p->d_src);
@@ -1320,9 +1321,11 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
             if (ckpt && t % p->cfg.checkpoint == 0) ckpt_snapshot(p, t / p->cfg.checkpoint, false, s);
             launch_sources(g, p->f, S, p->d_src, NT, t, 1, s);
             launch_update_v(g, p->f, s);
-            launch_update_s(g, p->f, s);
-            if (save_boundaries && !dft && !ckpt) launch_savebnd(g, p->f, bs, p->cfg.precision, (int64_t)t * g.nbnd, s);
-            if (g.freesurf) launch_surface(g, p->f, 1, s);
+            // the stress kernel may apply the free surface itself, unless the
+            // saved boundaries must see the stresses before it
+            const bool folded = launch_update_s(g, p->f, s, !bnd_shells);
+            if (bnd_shells) launch_savebnd(g, p->f, bs, p->cfg.precision, (int64_t)t * g.nbnd, s);
+            if (g.freesurf && !folded) launch_surface(g, p->f, 1, s);
             launch_record(g, p->f, R, p->d_seis, NT, t, omask, s);
             if (mv.n && (t + 1) % p->movout == 0) movie_snap(p, mv, (t + 1) / p->movout - 1, s);
             check(t, s);

@@ -63,6 +63,7 @@ struct Grid {
     int nbnd;               // saved-boundary cells per field per step
     int restype;
     int kernels;            // 0: register-blocked 3D kernels where available, 1: general only
+    int fused;              // 1: 3D modelling runs take the fused step kernel (sfd_config.kernels 6)
     int bp2;                // adjoint kernels: 1 for the DFT gradient (no reconstruction,
                             // boundary injection or on-the-fly gradient)
     int hout;               // accumulate the approximate Hessian

@@ -15,6 +15,7 @@
 //   boundary  src/savebnd{2D,3D}.cl, src/header_injectbnd.cl
 // Arithmetic is FP32 with FMA; gradients accumulate in FP64.
 #include <algorithm>
+#include <type_traits>
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -1409,11 +1410,13 @@ __device__ __forceinline__ void s3d_q4_at(const Grid &g, const Fields &f, int gz
     s_shear_q4<L, T>(g, f, gz0, gy, gx, iv, ip, vxyyx, vyzzy, vxzzx, surf);
 }
 
+// surf: the free surface of the step applied in the same launch (single-shot
+// modelling runs; see s_normal_q4)
 template <int L, class T, bool MB = false>
-__global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f)
+__global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f, bool surf)
 {
     CELL3D_Q4
-    s3d_q4_at<L, T, 0>(g, f, gz0, gy, gx, iv, ip);
+    s3d_q4_at<L, T, 0>(g, f, gz0, gy, gx, iv, ip, surf);
 }
 
 // ------------------------------------------------- fused 3D forward step
@@ -1549,7 +1552,7 @@ __global__ void __launch_bounds__(128, 4) k_fused3d_q4(Grid g, Fields f, FusedSy
 FusedShape fused_shape(const Grid &g)
 {
     FusedShape s{0, 0, 0, 0};
-    if (g.nd != 3 || g.F != 4 || g.nz % 4 || g.fhalf || g.L < 0 || g.L > 3 || g.kernels != 0) return s;
+    if (!g.fused || g.nd != 3 || g.F != 4 || g.nz % 4 || g.fhalf || g.L < 0 || g.L > 3 || g.kernels != 0) return s;
     const int ntz = (g.nz + FZ - 1) / FZ, nty = (g.ny + FY - 1) / FY, nch = (g.nx + FX - 1) / FX;
     if (ntz > 64 || (int64_t)ntz * nty * nch > (1 << 30)) return s;
     s.ntz = ntz;
@@ -3090,18 +3093,18 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
     }
 }
 
-void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
+bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_surface)
 {
     if (g.fhalf && g.nd == 3 && g.L <= 3) {   // FP16 storage: the vectorised or the streaming kernels
         if (q4_ok(g)) {
             dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);
             switch (g.L) {
-            case 0: k_s3d_q4<0, __half><<<g4, b4, 0, st>>>(g, f); break;
-            case 1: k_s3d_q4<1, __half><<<g4, b4, 0, st>>>(g, f); break;
-            case 2: k_s3d_q4<2, __half><<<g4, b4, 0, st>>>(g, f); break;
-            default: k_s3d_q4<3, __half><<<g4, b4, 0, st>>>(g, f); break;
+            case 0: k_s3d_q4<0, __half><<<g4, b4, 0, st>>>(g, f, false); break;
+            case 1: k_s3d_q4<1, __half><<<g4, b4, 0, st>>>(g, f, false); break;
+            case 2: k_s3d_q4<2, __half><<<g4, b4, 0, st>>>(g, f, false); break;
+            default: k_s3d_q4<3, __half><<<g4, b4, 0, st>>>(g, f, false); break;
             }
-            return;
+            return false;
         }
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
         switch (g.L) {
@@ -3110,29 +3113,31 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
         case 2: DISPATCH_F(g.F, k_s3d_stream<FF, 2, __half><<<gr, b, 0, st>>>(g, f)); break;
         default: DISPATCH_F(g.F, k_s3d_stream<FF, 3, __half><<<gr, b, 0, st>>>(g, f)); break;
         }
-        return;
+        return false;
     }
     // kernels 0: the 4-cell vectorised kernel where it applies (0.74 ms at
     // 256^3, against 0.96 TMA and 0.98 streaming), else the streaming one
-    if (g.kernels == 3 && launch_update_s_tma(g, f, st)) return;
-    if (g.kernels == 2 && launch_update_s_fast(g, f, st)) return;
+    if (g.kernels == 3 && launch_update_s_tma(g, f, st)) return false;
+    if (g.kernels == 2 && launch_update_s_fast(g, f, st)) return false;
+    // single-shot FP32 4-cell kernels apply the free surface in the same launch
+    const bool surf = fold_surface && g.freesurf && g.nb == 1;
     if (g.nd == 21 || g.nd == 22) {
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
         if (g.nd == 21) DISPATCH_F(g.F, k_s2d_sh<FF><<<gr, b, 0, st>>>(g, f))
         else DISPATCH_F(g.F, k_s2d_acc<FF><<<gr, b, 0, st>>>(g, f))
-        return;
+        return false;
     }
     if (g.nd == 3) {
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
         if ((g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) {
             dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);  // 0.70 ms vs 0.71 (32 x 2 x 2)
             switch (g.L) {
-            case 0: MB_DISPATCH(g, k_s3d_q4<0, float, MBV><<<g4, b4, 0, st>>>(g, f)) break;
-            case 1: MB_DISPATCH(g, k_s3d_q4<1, float, MBV><<<g4, b4, 0, st>>>(g, f)) break;
-            case 2: MB_DISPATCH(g, k_s3d_q4<2, float, MBV><<<g4, b4, 0, st>>>(g, f)) break;
-            default: MB_DISPATCH(g, k_s3d_q4<3, float, MBV><<<g4, b4, 0, st>>>(g, f)) break;
+            case 0: MB_DISPATCH(g, k_s3d_q4<0, float, MBV><<<g4, b4, 0, st>>>(g, f, surf)) break;
+            case 1: MB_DISPATCH(g, k_s3d_q4<1, float, MBV><<<g4, b4, 0, st>>>(g, f, surf)) break;
+            case 2: MB_DISPATCH(g, k_s3d_q4<2, float, MBV><<<g4, b4, 0, st>>>(g, f, surf)) break;
+            default: MB_DISPATCH(g, k_s3d_q4<3, float, MBV><<<g4, b4, 0, st>>>(g, f, surf)) break;
             }
-            return;
+            return surf;
         }
         if ((g.kernels == 0 || g.kernels == 4 || g.kernels == 5) && g.L <= 3) {
             switch (g.L) {
@@ -3141,7 +3146,7 @@ void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st)
             case 2: DISPATCH_F(g.F, MB_DISPATCH(g, k_s3d_stream<FF, 2, float, MBV><<<gr, b, 0, st>>>(g, f))); break;
             default: DISPATCH_F(g.F, MB_DISPATCH(g, k_s3d_stream<FF, 3, float, MBV><<<gr, b, 0, st>>>(g, f))); break;
             }
-            return;
+            return false;
         }
         DISPATCH_F(g.F, MB_DISPATCH(g, k_s3d<FF, MBV><<<gr, b, 0, st>>>(g, f)));
     } else {

@@ -24,11 +24,13 @@ int tma_take_status();      // 1 if a TMA stage of the last launches never arriv
 // 3D stress-update family of a plan: 0 not 3D, 1 general, 2 register-blocked,
 // 3 TMA-pipelined, 4 streaming, 5 4-cell vectorised
 int stress_family(const Grid &g, const Fields &f);
-void launch_update_s(const Grid &g, const Fields &f, cudaStream_t st);
+// fold_surface: single-shot FP32 4-cell kernels may apply the free surface in
+// the same launch (true returned: the caller skips launch_surface)
+bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_surface = false);
 // Fused 3D forward step (velocity, stress, free surface in one launch; see
 // sfd_kernels.cu).  Work units = ntz x nty x nchunk; units = 0 when the plan's
-// grid does not take it (3D, 8th order, nz % 4 == 0, FP32 fields, L <= 3,
-// kernels 0, at most 64 z tiles).
+// grid does not take it (sfd_config.kernels 6; 3D, 8th order, nz % 4 == 0,
+// FP32 fields, L <= 3, at most 64 z tiles).
 struct FusedShape {
     int ntz, nty, nchunk;
     int64_t units;

@@ -149,7 +149,8 @@ class Config:
     restype: int = 0
     precision: str = "fp32"
     kernels: str = "fast"  # "fast" (3D: 4-cell vectorised where eligible, else streaming), "general",
-    #                        "register", "tma", "stream", "vector"
+    #                        "register", "tma", "stream", "vector", "fused" ("fast" plus the fused
+    #                        one-launch modelling step)
     adjoint_reset_psi: bool = False  # True: the adjoint starts from zeroed CPML memory (not the reference's)
     field_precision: str = "fp32"  # "fp16": wave fields / memory variables stored in FP16 (3D forward)
     back_prop_type: int = 1  # 1: boundary-saving backpropagation, 2: DFT gradient at `gradfreqs`
@@ -188,7 +189,8 @@ class Config:
         c.param_type = int(self.param_type)
         c.restype = int(self.restype)
         c.precision = PREC[self.precision]
-        c.kernels = {"fast": 0, "general": 1, "register": 2, "tma": 3, "stream": 4, "vector": 5}[self.kernels]
+        c.kernels = {"fast": 0, "general": 1, "register": 2, "tma": 3, "stream": 4, "vector": 5,
+                     "fused": 6}[self.kernels]
         c.adjoint_reset_psi = 1 if self.adjoint_reset_psi else 0
         c.batch = int(self.batch)
         c.checkpoint = int(self.checkpoint)

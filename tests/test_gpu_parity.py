@@ -615,10 +615,10 @@ def test_fused_3d_step_matches_separate_kernels(kw, cuda_device):
     cfg, model, acq = make_case(**kw)
     outs = _outputs(3)
     res, fields = {}, {}
-    for variant in ("fast", "vector"):
+    for variant in ("fused", "vector"):
         plan = Plan(dataclasses.replace(engine_config(cfg), kernels=variant))
         plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
-        assert plan.fused_step == (variant == "fast")
+        assert plan.fused_step == (variant == "fused")
         res[variant] = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
         nv = plan.nvol
         fields[variant] = [plan.debug_array(0, i, nv) for i in range(9)]
@@ -626,11 +626,11 @@ def test_fused_3d_step_matches_separate_kernels(kw, cuda_device):
             fields[variant] += [plan.debug_array(2, i, nv * cfg["L"]) for i in range(6)]
     for n in outs:
         assert np.abs(res["vector"][n]).max() > 0
-        assert rel_l2(res["fast"][n], res["vector"][n]) < 1e-6, n
-    errs = [rel_l2(a, b) for a, b in zip(fields["fast"], fields["vector"])]
+        assert rel_l2(res["fused"][n], res["vector"][n]) < 1e-6, n
+    errs = [rel_l2(a, b) for a, b in zip(fields["fused"], fields["vector"])]
     assert max(errs) < 1e-5, errs
     ora = Oracle(cfg)
     ora.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
     ref = ora.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
     for n in outs:
-        assert rel_l2(res["fast"][n], ref[n]) < FWD_TOL, n
+        assert rel_l2(res["fused"][n], ref[n]) < FWD_TOL, n
