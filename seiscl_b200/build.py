@@ -16,8 +16,8 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libseiscl_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "-I" + os.path.join(ROOT, "include"),
-         "--expt-relaxed-constexpr"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2,-Werror=return-type",
+         "-I" + os.path.join(ROOT, "include"), "--expt-relaxed-constexpr"]
 
 
 def sources():

@@ -3153,6 +3153,7 @@ bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
         DISPATCH_F(g.F, k_s2d<FF><<<gr, b, 0, st>>>(g, f));
     }
+    return false;
 }
 
 // movie snapshot (time_stepping.c:272-350): padded field -> [nx][ny][nz]
