@@ -7,12 +7,17 @@ the same attribute names (the reference calls them ``csts``), the same
 same array orientations (models ``N``-shaped, seismograms ``NT x ntraces``,
 ``src_pos_all`` 5 x nsrc, ``rec_pos_all`` 8 x ntraces).
 
-What differs is the transport. The reference writes HDF5 files into
-``workdir`` and runs the ``SeisCL_MPI`` executable, which reads them back
-(SeisCL.py:459-505, src/read_hdf5.c, src/writehdf5.c). Here the files become
-in-memory records keyed by the same file names, and ``execute`` drives the
-time loop of src/time_stepping.c:693-900 directly through the C ABI of
-``libseiscl_b200.so`` on the current CUDA device:
+The reference writes HDF5 files into ``workdir`` and runs the
+``SeisCL_MPI`` executable, which reads them back (SeisCL.py:459-505,
+src/read_hdf5.c, src/writehdf5.c).  Here ``execute`` drives the time loop of
+src/time_stepping.c:693-900 in-process through the C ABI of
+``libseiscl_b200.so`` on the current CUDA device, and the job files are
+records keyed by the same file names: kept in memory by default, or -- with
+``files=True`` -- written to and read from HDF5 files in ``workdir`` with the
+reference's names, datasets and transposes (``seiscl_b200.h5lite``), so a
+workflow that exchanges files, or the command line
+``python -m seiscl_b200.cli <base> [din]`` (SeisCL_MPI's arguments), works on
+the same files:
 
 * per shot (sources grouped by ascending ``srcid``, read_hdf5.c:357-393):
   forward modelling with the selected seismogram outputs;
@@ -37,7 +42,31 @@ from typing import Dict, List, Optional
 import numpy as np
 
 from . import engine
+from . import h5lite
 from . import shots as shots_mod
+
+# The keys SeisCL writes to and reads from the constants file (SeisCL.py:23-30)
+CSTS = ['N', 'ND', 'dh', 'dt', 'NT', 'freesurf', 'FDORDER', 'MAXRELERROR',
+        'L', 'f0', 'FL', 'src_pos', 'rec_pos', 'src', 'abs_type', 'VPPML',
+        'NPOWER', 'FPML', 'K_MAX_CPML', 'nab', 'abpc', 'pref_device_type',
+        'no_use_GPUs', 'MPI_NPROC_SHOT', 'nmax_dev', 'back_prop_type',
+        'param_type', 'gradfreqs', 'tmax', 'tmin', 'scalerms',
+        'scalermsnorm', 'scaleshot',
+        'fmin', 'fmax', 'gradout', 'Hout', 'gradsrcout', 'seisout', 'resout',
+        'rmsout', 'movout', 'restype', 'inputres', 'FP16']
+
+
+def _to_file(name: str, value):
+    """An in-memory record value as its HDF5 dataset: SeisCL.py writes
+    np.transpose(array) (N-shaped models become [nx][(ny)][nz] z-fastest, NT x
+    ntraces seismograms [ntraces][NT]); movies are kept in file order."""
+    a = np.asarray(value)
+    return a if name.startswith("mov") else np.transpose(a)
+
+
+def _from_file(name: str, value):
+    a = np.asarray(value)
+    return a if name.startswith("mov") else np.transpose(a)
 
 # Seismogram variables of each modelling case (assign_modeling_case.c:1242-1322);
 # "p" is a transformed variable of the elastic cases and a field in acoustics.
@@ -122,6 +151,7 @@ class SeisCL:
                  seisout: int = 2, resout: int = 0, rmsout: int = 0,
                  movout: int = 0,
                  file: str = "SeisCL", workdir: str = "./seiscl",
+                 files: bool = False,
                  ):
         """Keyword meanings and defaults are those of SeisCL.py:38-300.
 
@@ -131,7 +161,11 @@ class SeisCL:
         over ranks by ``seiscl_b200.shots`` instead). ``FP16`` 2 or 3 stores
         the saved boundaries in FP16 and, for 3D forward runs, the wave fields
         and memory variables too (power-of-two scaled, as the reference's
-        FP16=2 mode); arithmetic is FP32 in every mode."""
+        FP16=2 mode); arithmetic is FP32 in every mode.
+
+        ``files`` (no counterpart in the reference, which always uses files):
+        True writes and reads the job files as HDF5 in ``workdir``; False
+        keeps them in memory."""
         try:
             engine.load_library()
         except Exception as exc:  # the engine is the only compute path
@@ -198,7 +232,9 @@ class SeisCL:
         self.workdir = workdir
         self.wavelet_generator = self.ricker_wavelet
         self.__to_load_names = None
-        # In-memory stand-ins of the HDF5 files, keyed by file name.
+        # The job files, keyed by file name (also written to / read from
+        # workdir as HDF5 when use_files)
+        self.use_files = bool(files)
         self._files: Dict[str, Dict[str, np.ndarray]] = {}
         self._model: Optional[Dict[str, np.ndarray]] = None
         self._plan = None
@@ -263,6 +299,36 @@ class SeisCL:
     def csts(self):
         return self.__dict__
 
+    # ------------------------------------------------------------ job files
+    def _path(self, filename, workdir=None):
+        if os.path.isabs(filename):
+            return filename
+        return os.path.join(self.workdir if workdir is None else workdir, filename)
+
+    def _put(self, filename, record, workdir=None):
+        """Store a job file: in memory, and as HDF5 in workdir when use_files."""
+        self._files[os.path.basename(filename)] = record
+        if self.use_files:
+            path = self._path(filename, workdir)
+            os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+            try:
+                h5lite.write(path, {k: _to_file(k, v) for k, v in record.items()
+                                    if v is not None and np.asarray(v).dtype.kind in "biuf"})
+            except (OSError, h5lite.H5Error) as exc:
+                raise SeisCLError("could not write %s: %s\n" % (path, exc)) from exc
+
+    def _get(self, filename, workdir=None):
+        """A job file's record, or None when there is none."""
+        if self.use_files:
+            path = self._path(filename, workdir)
+            if not os.path.exists(path):
+                return None
+            try:
+                return {k: _from_file(k, v) for k, v in h5lite.read(path).items()}
+            except (OSError, h5lite.H5Error) as exc:
+                raise SeisCLError("could not read %s: %s\n" % (path, exc)) from exc
+        return self._files.get(os.path.basename(filename))
+
     @property
     def to_load_names(self):
         """Seismogram names for ``seisout`` (SeisCL.py:377-409); the acoustic
@@ -302,7 +368,7 @@ class SeisCL:
             rec = {}
             for n, word in enumerate(self.to_load_names):
                 rec[word + "res"] = np.asarray(residuals[n], dtype=np.float32)
-            self._files[self.file_res] = rec
+            self._put(self.file_res, rec, workdir)
             self.inputres = 1
         else:
             self.inputres = 0
@@ -315,17 +381,23 @@ class SeisCL:
         return "%s: in-process CUDA engine, file %s" % (self.progname, self.file)
 
     def write_csts(self, workdir=None, filename=None):
+        """The constants of ``CSTS`` (SeisCL.py:703-721)."""
         if filename is None:
             filename = self.file_csts
-        self._files[filename] = {k: v for k, v in self.__dict__.items() if not k.startswith("_")}
+        self._put(filename, {k: self.__dict__[k] for k in CSTS if self.__dict__.get(k) is not None}, workdir)
 
     def read_csts(self, workdir=None, filename=None):
+        """Replace the constants with those of the constants file
+        (SeisCL.py:682-701)."""
         if filename is None:
             filename = self.file_csts
-        if filename not in self._files:
+        rec = self._get(filename, workdir)
+        if rec is None:
             raise SeisCLError('could not read parameter file \n')
-        for k, v in self._files[filename].items():
-            self.__dict__[k] = v
+        for k, v in rec.items():
+            if k in CSTS:
+                v = np.asarray(v)
+                self.__dict__[k] = v.item() if v.ndim == 0 else v
 
     def write_model(self, params, workdir=None):
         """Store the model (SeisCL.py:747-763): every name of ``params`` is
@@ -334,7 +406,7 @@ class SeisCL:
             if param not in params:
                 raise SeisCLError('Parameter with %s not defined\n' % param)
         self._model = {k: np.asarray(v, dtype=np.float32).copy() for k, v in params.items()}
-        self._files[self.file_model] = self._model
+        self._put(self.file_model, self._model, workdir)
 
     def write_data(self, data, workdir=None, filename=None):
         """Store observed data (SeisCL.py:658-680); arrays are NT x ntraces."""
@@ -347,8 +419,7 @@ class SeisCL:
             data['rec_pos'] = self.rec_pos
         if 'src' not in data:
             data['src'] = self.src
-        self._files[os.path.basename(filename)] = {k: (None if v is None else np.array(v, copy=True))
-                                                   for k, v in data.items()}
+        self._put(filename, {k: (None if v is None else np.array(v, copy=True)) for k, v in data.items()}, workdir)
 
     def prepare_data(self, srcids):
         """Select sources and receivers of ``srcids`` (SeisCL.py:765-808)."""
@@ -453,7 +524,7 @@ class SeisCL:
         if filename is None:
             filename = self.file_dout
         suf = "res" if residuals else "out"
-        mat = self._files.get(os.path.basename(filename))
+        mat = self._get(filename, workdir)
         if mat is None:
             raise SeisCLError('Could not read data')
         output = [mat[w + suf] for w in self.to_load_names if w + suf in mat]
@@ -468,7 +539,7 @@ class SeisCL:
         snapshot, then shot)."""
         if filename is None:
             filename = self.file_movout
-        mat = self._files.get(os.path.basename(filename))
+        mat = self._get(filename, workdir)
         if mat is None:
             raise SeisCLError('Could not read data')
         output = [np.transpose(mat["mov" + w]) for w in self.to_load_names if "mov" + w in mat]
@@ -483,7 +554,7 @@ class SeisCL:
             filename = self.file_gout
         if param_names is None:
             param_names = self.params
-        mat = self._files.get(os.path.basename(filename))
+        mat = self._get(filename, workdir)
         if mat is None:
             raise SeisCLError('Could not read grad')
         try:
@@ -506,7 +577,7 @@ class SeisCL:
             filename = self.file_gout
         if param_names is None:
             param_names = self.params
-        mat = self._files.get(os.path.basename(filename))
+        mat = self._get(filename, workdir)
         if mat is None:
             raise SeisCLError('Could not read Hessian')
         try:
@@ -526,7 +597,7 @@ class SeisCL:
         """(rms / rms_norm, rms_norm) of the last run (SeisCL.py:636-656)."""
         if filename is None:
             filename = self.file_rms
-        mat = self._files.get(os.path.basename(filename))
+        mat = self._get(filename, workdir)
         if mat is None:
             raise SeisCLError('Forward modeling failed, could not read rms\n')
         return mat['rms'][0] / mat['rms_norm'][0], mat['rms_norm'][0]
@@ -714,6 +785,11 @@ class SeisCL:
         current CUDA device and store its outputs (SeisCL.py:487-505,
         src/time_stepping.c:693-900). Returns a short log."""
         t0 = time.perf_counter()
+        if self.use_files:
+            model = self._get(self.file_model, workdir)
+            if model is None:
+                raise SeisCLError("Error: Could not open the input file model")
+            self._model = model
         plan = self._get_plan()
         nd = int(self.ND)
         NT = int(self.NT)
@@ -722,8 +798,8 @@ class SeisCL:
         except engine.SeisCLEngineError as exc:
             raise SeisCLError(str(exc)) from exc
         tmax = plan.tmax
-        din = self._files.get(os.path.basename(self.file_din))
-        resin = self._files.get(self.file_res) if self.inputres else None
+        din = self._get(self.file_din, workdir)
+        resin = self._get(self.file_res, workdir) if self.inputres else None
         if self.inputres and self.resout:
             raise SeisCLError("Error: Cannot input and output residuals simultaneously")
         outs = self._outputs(din, resin)
@@ -811,12 +887,13 @@ class SeisCL:
             dout["src_pos"] = np.asarray(self.src_pos).copy()
             dout["rec_pos"] = np.asarray(self.rec_pos).copy()
             if self.seisout or self.resout:
-                self._files[self.file_dout] = dout
+                self._put(self.file_dout, dout, workdir)
         if movies is not None:
-            self._files[self.file_movout] = {"mov" + k: v for k, v in movies.items()}
+            self._put(self.file_movout, {"mov" + k: v for k, v in movies.items()}, workdir)
         if self.rmsout:
-            self._files[self.file_rms] = {"rms": np.array([np.sqrt(rms)], np.float32),
-                                          "rms_norm": np.array([np.sqrt(rmsnorm)], np.float32)}
+            # 1 x 1 datasets (writehdf5.c:249-257)
+            self._put(self.file_rms, {"rms": np.array([[np.sqrt(rms)]], np.float32),
+                                      "rms_norm": np.array([[np.sqrt(rmsnorm)]], np.float32)}, workdir)
         if self.gradout:
             g = plan.gradient(transform=True)
             H = plan.hessian(transform=True) if self.Hout else None
@@ -839,7 +916,7 @@ class SeisCL:
                 if H is not None:
                     v = H[name] if name in H else np.zeros_like(H["rho"])
                     gout["H" + name] = np.ascontiguousarray(np.transpose(v)).reshape(shape)
-            self._files[self.file_gout] = gout
+            self._put(self.file_gout, gout, workdir)
         ms = (time.perf_counter() - t0) * 1e3
         return "%d shot(s) (%d on rank %d of %d), %d trace(s), %d time steps: %.1f ms\n" % (
             len(shots), smax - smin, rank, world, ntr, NT, ms)
