@@ -352,6 +352,16 @@ int sfd_plan_kernel_family(const sfd_plan *plan);
  * written, or a negative error. */
 int64_t sfd_debug_copy(sfd_plan *plan, int kind, int id, float *dst, int64_t cap);
 
+/* Tests of single kernels (adjoint dot products): copy n host floats into a
+ * device array (kinds 0-2 of sfd_debug_copy; n must be the array's size;
+ * kind 1 allocates the adjoint fields), and run one kernel on the plan's
+ * arrays -- which 0 velocity update, 1 stress update, 2 free surface
+ * (forward), 3 free-surface adjoint on the adjoint fields (the reference's
+ * surface_adj, src/surface2D_adj.cl:35-148, src/surface3D_adj.cl:29-116) --
+ * returning after it finished.  No counterpart in the reference. */
+int64_t sfd_debug_load(sfd_plan *plan, int kind, int id, const float *src, int64_t n);
+int sfd_debug_launch(sfd_plan *plan, int which);
+
 /* Kernel timing for benchmarks: runs the velocity update, the stress update,
  * (with a free surface) the surface kernel and (where the plan has it) the
  * fused 3D step `nrep` times each on the plan's stream, bracketed by CUDA

@@ -1700,6 +1700,55 @@ extern "C" int64_t sfd_debug_copy(sfd_plan *p, int kind, int id, float *dst, int
     return n;
 }
 
+extern "C" int64_t sfd_debug_load(sfd_plan *p, int kind, int id, const float *src, int64_t n)
+{
+    if (!p || !src || n < 0) return SFD_ERR_ARG;
+    if (!p->model_set) return fail(p, SFD_ERR_STATE, "sfd_set_model must be called first");
+    const Grid &g = p->g;
+    if (g.fhalf) return fail(p, SFD_ERR_UNSUPPORTED, "wave fields are stored in FP16");
+    int rc;
+    if (kind == 1 && (rc = alloc_adjoint(p))) return rc;
+    void *dst = nullptr;
+    int64_t cap = 0;
+    if (kind == 0 && id >= 0 && id < NW) { dst = p->f.w[id]; cap = g.nvol; }
+    else if (kind == 1 && id >= 0 && id < NW) { dst = p->a.wr[id]; cap = g.nvol; }
+    else if (kind == 2 && id >= 0 && id < NR) { dst = p->f.r[id]; cap = g.nvol * g.L; }
+    if (!dst) return fail(p, SFD_ERR_ARG, "array not allocated");
+    if (n != cap) return fail(p, SFD_ERR_ARG, "size differs from the array's");
+    cudaDeviceSynchronize();
+    if (cudaMemcpy(dst, src, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(p, SFD_ERR_CUDA, "copy failed");
+    return n;
+}
+
+extern "C" int sfd_debug_launch(sfd_plan *p, int which)
+{
+    if (!p) return SFD_ERR_ARG;
+    if (!p->model_set) return fail(p, SFD_ERR_STATE, "sfd_set_model must be called first");
+    cudaStream_t st = p->stream;
+    p->g.nb = 1;
+    const Grid &g = p->g;
+    int rc;
+    switch (which) {
+    case 0: launch_update_v(g, p->f, st); break;
+    case 1: launch_update_s(g, p->f, st); break;
+    case 2:
+        if (!g.freesurf) return fail(p, SFD_ERR_STATE, "the plan has no free surface");
+        launch_surface(g, p->f, 1, st);
+        break;
+    case 3:
+        if (!g.freesurf) return fail(p, SFD_ERR_STATE, "the plan has no free surface");
+        if (g.nd == 21 || g.nd == 22) return fail(p, SFD_ERR_UNSUPPORTED, "no surface adjoint for this physics");
+        if ((rc = alloc_adjoint(p))) return rc;
+        launch_surface_adj(g, p->f, p->a, p->d_surf_q, st);
+        break;
+    default: return fail(p, SFD_ERR_ARG, "unknown kernel");
+    }
+    CKC(cudaGetLastError());
+    CKC(cudaStreamSynchronize(st));
+    return SFD_OK;
+}
+
 extern "C" float sfd_last_loop_ms(const sfd_plan *p) { return p ? p->last_ms : 0.0f; }
 
 extern "C" int sfd_bench_kernels(sfd_plan *p, int nrep, float *out_ms)

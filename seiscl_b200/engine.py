@@ -72,6 +72,8 @@ EXPORTS = {
     "sfd_plan_kernel_family": (C.c_int, [C.c_void_p]),
     "sfd_plan_fused_step": (C.c_int, [C.c_void_p]),
     "sfd_debug_copy": (C.c_int64, [C.c_void_p, C.c_int, C.c_int, FP, C.c_int64]),
+    "sfd_debug_load": (C.c_int64, [C.c_void_p, C.c_int, C.c_int, FP, C.c_int64]),
+    "sfd_debug_launch": (C.c_int, [C.c_void_p, C.c_int]),
     "sfd_last_loop_ms": (C.c_float, [C.c_void_p]),
     "sfd_bench_kernels": (C.c_int, [C.c_void_p, C.c_int, FP]),
     "sfd_host_transform": (C.c_int, [C.POINTER(sfd_config), C.POINTER(FP), C.POINTER(FP)]),
@@ -414,6 +416,19 @@ class Plan:
         else:
             k, i, n = 8 + slot, ["rxx", "ryy", "rzz", "rxy", "ryz", "rxz"].index(name), self.nvol * int(self.cfg.L)
         return self.debug_array(k, i, 2 * self.nfreqs * n).view(np.complex64)
+
+    def debug_load(self, kind: int, idx: int, values) -> None:
+        """Overwrite a device array (0 wave field, 1 adjoint wave field, 2
+        memory variables) with ``values`` (tests)."""
+        a = _f32(values).ravel()
+        got = self.lib.sfd_debug_load(self.h, kind, idx, _ptr(a), a.size)
+        if got < 0:
+            self._check(int(got))
+
+    def debug_launch(self, which: int) -> None:
+        """Run one kernel on the plan's arrays: 0 velocity update, 1 stress
+        update, 2 free surface, 3 free-surface adjoint (tests)."""
+        self._check(self.lib.sfd_debug_launch(self.h, int(which)))
 
     def debug_array(self, kind: int, idx: int, n: int) -> np.ndarray:
         out = np.zeros(n, np.float32)

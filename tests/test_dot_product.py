@@ -1,0 +1,144 @@
+"""Adjoint dot-product tests of the CUDA kernels.
+
+SeisCL builds its adjoint by symmetrisation (SeisCL/tests/dot_prod_surface.py
+and dot_prod_surface_3D.py): with L = diag(1/b, -C^-1) -- b the buoyancies of
+the velocity updates, C the stiffness of the stress update -- one time step
+F = L US UV (velocity update, then stress update) is self-adjoint, and with a
+free surface S the adjoint of L S US UV is L US UV (L^-1 S* L), where the
+surface-adjoint kernel applies L^-1 S* L itself
+(src/surface2D_adj.cl:35-148, src/surface3D_adj.cl:29-116).  These tests
+apply the engine's own kernels (through sfd_debug_load / sfd_debug_launch)
+to random fields u and w, apply L on the host in FP64, and check
+
+    <w, L S US UV u> = <u, L US UV S_adj w>
+
+(dot_prod_surface.py:286-409, "Dot product for LFT" and "F_s' = LSF"), in 2D
+and 3D, 4th and 8th order (the 3D 8th-order case runs the 4-cell vectorised
+kernels), without and with the free surface.  The fields are drawn in
+units that balance the terms of the products (velocities times sqrt(b),
+stresses times sqrt(M)), so the velocity-stress coupling, not the diagonal,
+carries the sums.  A wrong adjoint (the surface adjoint left out) must
+break the identity by orders of magnitude more than the tolerance.
+"""
+import numpy as np
+import pytest
+
+from tests._cases import engine_config, make_case
+
+TOL = 2e-5
+IDS = {"vx": 0, "vy": 1, "vz": 2, "sxx": 3, "syy": 4, "szz": 5, "sxy": 6, "syz": 7, "sxz": 8}
+PIDX = {"M": 0, "mu": 1, "rip": 5, "rjp": 6, "rkp": 7, "muipkp": 8, "muipjp": 9, "mujpkp": 10}
+
+
+def _setup(nd, fdorder, freesurf):
+    from seiscl_b200.engine import Plan
+
+    kw = dict(nd=nd, nz=32, ny=28, nx=24, nt=4) if nd == 3 else dict(nd=nd, nz=40, nx=44, nt=4)
+    cfg, model, acq = make_case(nab=0, freesurf=freesurf, fdorder=fdorder, L=0, **kw)
+    plan = Plan(engine_config(cfg))
+    shape = model["vp"].shape
+    plan.set_model(np.full(shape, 3000.0, np.float32), np.full(shape, 1700.0, np.float32),
+                   np.full(shape, 2000.0, np.float32))
+    names = ["vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "syz", "sxz"] if nd == 3 else ["vx", "vz", "sxx", "szz",
+                                                                                          "sxz"]
+    F = fdorder // 2
+    dims = (plan.NXp, plan.NYp, plan.NZp) if nd == 3 else (plan.NXp, plan.NZp)
+    npar = int(np.prod(shape))
+    par = {k: plan.debug_array(3, i, npar).astype(np.float64).reshape(shape) for k, i in PIDX.items()}
+    return plan, names, F, dims, par
+
+
+def _interior(F, dims):
+    return tuple(slice(F, d - F) for d in dims)
+
+
+SHEAR_MU = {"sxy": "muipjp", "syz": "mujpkp", "sxz": "muipkp"}
+
+
+def _random(rng, names, F, dims, par):
+    """Random interior values; a shear stress stays zero where its averaged
+    modulus is zero (the reference's averages leave the last cells at zero,
+    src/assign_modeling_case.c:134-170): the update keeps it zero there, so
+    the identity holds on the remaining cells."""
+    out = {}
+    sl = _interior(F, dims)
+    for n in names:
+        a = np.zeros(dims)
+        scale = np.sqrt(par["rip"].mean()) if n[0] == "v" else np.sqrt(par["M"].mean())
+        a[sl] = rng.uniform(0.0, 1.0, a[sl].shape) * scale
+        if n in SHEAR_MU:
+            a[sl] *= par[SHEAR_MU[n]] != 0
+        out[n] = a
+    return out
+
+
+def _div(a, b):
+    return np.divide(a, b, out=np.zeros_like(a), where=b != 0)
+
+
+def _apply_L(f, names, F, dims, par, nd):
+    """L = diag(1/b, -C^-1) on the interior (the stresses negated everywhere,
+    as dot_prod_surface.py's apply_L)."""
+    sl = _interior(F, dims)
+    g = {k: v.copy() for k, v in f.items()}
+    b = {"vx": par["rip"], "vy": par["rjp"], "vz": par["rkp"]}
+    for n in names:
+        if n[0] == "v":
+            g[n][sl] = f[n][sl] / b[n]
+    M, mu = par["M"], par["mu"]
+    if nd == 2:
+        a = 1.0 / (4.0 * M * mu - 4.0 * mu ** 2)
+        g["sxx"][sl] = a * (M * f["sxx"][sl] - (M - 2 * mu) * f["szz"][sl])
+        g["szz"][sl] = a * (M * f["szz"][sl] - (M - 2 * mu) * f["sxx"][sl])
+        g["sxz"][sl] = _div(f["sxz"][sl], par["muipkp"])
+    else:
+        # C^-1 of the normal block: (I - (M - 2 mu) / (3 M - 4 mu) J) / (2 mu)
+        tr = f["sxx"][sl] + f["syy"][sl] + f["szz"][sl]
+        k = (M - 2 * mu) / (3 * M - 4 * mu)
+        for n in ("sxx", "syy", "szz"):
+            g[n][sl] = (f[n][sl] - k * tr) / (2 * mu)
+        for n, m in SHEAR_MU.items():
+            g[n][sl] = _div(f[n][sl], par[m])
+    for n in names:
+        if n[0] == "s":
+            g[n] = -g[n]
+    return g
+
+
+def _run(plan, names, dims, f, kernels, adjoint_fields=False):
+    kind = 1 if adjoint_fields else 0
+    for n in names:
+        plan.debug_load(kind, IDS[n], f[n].astype(np.float32))
+    for k in kernels:
+        plan.debug_launch(k)
+    return {n: plan.debug_array(kind, IDS[n], plan.nvol).astype(np.float64).reshape(dims) for n in names}
+
+
+def _dot(a, b):
+    return sum(float(np.sum(a[k] * b[k])) for k in a)
+
+
+CASES = [(2, 4, 0), (2, 8, 0), (3, 8, 0), (3, 4, 0), (2, 8, 1), (2, 4, 1), (3, 8, 1)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nd,fdorder,freesurf", CASES)
+def test_adjoint_dot_product(nd, fdorder, freesurf, cuda_device):
+    plan, names, F, dims, par = _setup(nd, fdorder, freesurf)
+    rng = np.random.default_rng(100 * nd + 10 * fdorder + freesurf)
+    u = _random(rng, names, F, dims, par)
+    w = _random(rng, names, F, dims, par)
+    fwd = [0, 1, 2] if freesurf else [0, 1]
+    Fu = _apply_L(_run(plan, names, dims, u, fwd), names, F, dims, par, nd)
+    p1 = _dot(w, Fu)
+    w1 = _run(plan, names, dims, w, [3], adjoint_fields=True) if freesurf else w
+    Fw = _apply_L(_run(plan, names, dims, w1, [0, 1]), names, F, dims, par, nd)
+    p2 = _dot(u, Fw)
+    err = abs(p1 - p2) / max(abs(p1), abs(p2))
+    assert err < TOL, (p1, p2, err)
+    if freesurf:
+        # without the surface adjoint the identity must fail clearly
+        Fw0 = _apply_L(_run(plan, names, dims, w, [0, 1]), names, F, dims, par, nd)
+        bad = abs(p1 - _dot(u, Fw0)) / max(abs(p1), abs(p2))
+        assert bad > 100 * TOL, bad
+    plan.close()
