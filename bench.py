@@ -160,10 +160,11 @@ def build_workload(name, grid=0):
     taup = taus = None
     fl = [w["f0"]]
     if w["L"] > 0:
-        from seiscl_b200.qfit import band_frequencies, q_to_tau
+        # FL and tau of SeisCL's constant-Q least-squares fit (Q_tau.py's QTAU
+        # over the band, tau_optimize, Q2tau(q))
+        from seiscl_b200.qfit import constant_q_band
 
-        fl = band_frequencies(w["L"], *w["fband"])
-        tau = q_to_tau(w["q"], fl, *w["fband"])
+        fl, tau = constant_q_band(w["L"], w["q"], *w["fband"])
         taup = np.full(vp.shape, tau, np.float32)
         taus = np.full(vp.shape, tau, np.float32)
     nt, dt = w["nt"], w["dt"]
@@ -216,9 +217,9 @@ def reference_build_configs():
 def build_workload_light(name):
     w = dict(WORKLOADS[name])
     if w["L"] > 0:
-        from seiscl_b200.qfit import band_frequencies
+        from seiscl_b200.qfit import constant_q_band
 
-        w["fl"] = band_frequencies(w["L"], *w["fband"])
+        w["fl"] = constant_q_band(w["L"], w["q"], *w["fband"])[0]
     else:
         w["fl"] = [w["f0"]]
     return w, None, None
@@ -323,19 +324,27 @@ def measured_peaks():
 
 
 def cpu_baseline(w, model, acq, budget_s=20.0, prefer_ref=True):
-    """The CPU oracle on the host cores over a bounded number of time steps
-    of the same grid (OpenMP over all threads)."""
+    """The reference's kernels on the host cores over a bounded number of
+    time steps of the same grid (OpenMP over all threads), from the fastest
+    build of them this CPU can run: -O3 -march=native (when the building
+    machine's instruction set is available here), else -O3 -march=x86-64-v3,
+    else the -O2 pinning build; the C restatement when none was built."""
     from oracle import build as ob
-    from oracle.oracle import Oracle
-
-    from oracle.oracle import DEFAULTS
+    from oracle.oracle import DEFAULTS, Oracle
 
     cfg = oracle_config(w)
     full = dict(DEFAULTS)
     full.update(cfg)
-    ref = bool(prefer_ref and os.path.exists(ob.ref_lib_path(full)))
-    kind = "reference" if ref else "port"
-    o = Oracle(cfg, ref=ref)
+    speed, flags = None, None
+    if prefer_ref:
+        for sp, fl in (("native", "-O3 -march=native -fopenmp"), ("v3", "-O3 -march=x86-64-v3 -fopenmp"),
+                       ("pin", "-O2 -ffp-contract=off -fopenmp")):
+            path = ob.ref_lib_path(full, sp)
+            if os.path.exists(path) and (sp != "native" or ob.native_usable(path)):
+                speed, flags = sp, fl
+                break
+    kind = "reference" if speed else "port"
+    o = Oracle(cfg, ref=bool(speed), speed=speed or "pin")
     rc = o.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
     if rc:
         raise RuntimeError("oracle rejected the model (%d)" % rc)
@@ -348,9 +357,10 @@ def cpu_baseline(w, model, acq, budget_s=20.0, prefer_ref=True):
     el = time.perf_counter() - t0
     cells = w["nz"] * w["ny"] * w["nx"]
     o.close()
+    what = ("the reference's kernel sources built with %s" % flags) if speed else "the C restatement (-O2)"
     return dict(value=cells * nsteps / el / 1e9, unit="Gcell-updates/s", cores=os.cpu_count(), kind=kind,
-                sample="%d time steps of the %dx%dx%d grid (velocity, stress and free-surface kernels)"
-                       % (nsteps, w["nz"], w["ny"], w["nx"])), nsteps, el
+                sample="%d time steps of the %dx%dx%d grid (velocity, stress and free-surface kernels), %s"
+                       % (nsteps, w["nz"], w["ny"], w["nx"], what)), nsteps, el
 
 
 def run_reference_arm(args, w, model, acq):

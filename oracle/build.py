@@ -6,14 +6,20 @@ TEST INFRASTRUCTURE ONLY: the checker of the CUDA path, never the product.
   fdo_driver.c) into ``oracle/_build/libfdo_port.so``.  It needs only gcc and
   runs anywhere, including the GPU box.
 * ``build_ref(cfg)`` compiles the reference's own kernel sources *in place*
-  from the reference tree (``SEISCL_REF_SRC`` or /root/reference/src) with the
-  same -D constants the reference passes at run time (src/clprogram.c:449-571),
-  links them with ref_glue.c and the restated time loop, and writes
-  ``oracle/_ref/libfdo_ref_<key>.so``.  Nothing from the reference tree is
-  copied.  Each grid needs its own build because the reference fixes sizes at
-  compile time.
+  from the reference tree (``SEISCL_REF_SRC``, else ``reference/src`` beside
+  the repository) with the same -D constants the reference passes at run time
+  (src/clprogram.c:449-571), links them with ref_glue.c and the restated time
+  loop, and writes ``oracle/_ref/libfdo_ref_<key>.so``.  Nothing from the
+  reference tree is copied.  Each grid needs its own build because the
+  reference fixes sizes at compile time.
 
-Both builds use -O2 -ffp-contract=off so the two agree bit for bit.
+The port and the pinning build of the reference use -O2 -ffp-contract=off so
+the two agree bit for bit.  For timing the reference on the host cores
+(the benchmark's CPU baseline and reference arm) ``build_ref(cfg, speed=...)``
+makes two more builds of the same sources with ``-O3 -fopenmp`` and
+``-march=x86-64-v3`` (AVX2 + FMA, any current x86-64 server) or
+``-march=native`` (this build machine's instruction set, recorded beside the
+library so a run on another CPU can tell whether it may load it).
 """
 from __future__ import annotations
 
@@ -27,8 +33,11 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
-REF_SRC = os.environ.get("SEISCL_REF_SRC", "/root/reference/src")
+REF_SRC = os.environ.get("SEISCL_REF_SRC",
+                         os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference", "src"))
 CFLAGS = ["-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-std=gnu17", "-w"]
+SPEED_FLAGS = {"v3": ["-O3", "-march=x86-64-v3", "-fPIC", "-fopenmp", "-std=gnu17", "-w"],
+               "native": ["-O3", "-march=native", "-fPIC", "-fopenmp", "-std=gnu17", "-w"]}
 PORT_SOURCES = ["fdo_setup.c", "fdo_port.c", "fdo_driver.c", "fdo_dft.c"]
 
 
@@ -136,13 +145,38 @@ def ref_key(cfg: dict) -> str:
     return hashlib.sha1(blob.encode()).hexdigest()[:16]
 
 
-def ref_lib_path(cfg: dict) -> str:
-    return os.path.join(REF_OUT, "libfdo_ref_%s.so" % ref_key(cfg))
+def ref_lib_path(cfg: dict, speed: str = "pin") -> str:
+    suffix = "" if speed == "pin" else "_" + speed
+    return os.path.join(REF_OUT, "libfdo_ref_%s%s.so" % (ref_key(cfg), suffix))
 
 
-def build_ref(cfg: dict, nbnd: int, hc: list) -> str:
-    """Compile the reference kernels for this grid (needs the reference tree)."""
-    out = ref_lib_path(cfg)
+def cpu_flags() -> set:
+    """Instruction-set flags of this machine's CPU (/proc/cpuinfo)."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("flags"):
+                return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def native_usable(path: str) -> bool:
+    """Whether a -march=native build may run here: every instruction-set flag
+    of the machine that built it is present on this CPU."""
+    try:
+        built = set(json.load(open(path + ".cpu.json"))["flags"])
+    except (OSError, ValueError, KeyError):
+        return False
+    return built <= cpu_flags()
+
+
+def build_ref(cfg: dict, nbnd: int, hc: list, speed: str = "pin") -> str:
+    """Compile the reference kernels for this grid (needs the reference tree).
+    speed "pin": the bit-exact pinning build; "v3" / "native": -O3 timing
+    builds (see the module docstring)."""
+    out = ref_lib_path(cfg, speed)
+    flags = CFLAGS if speed == "pin" else SPEED_FLAGS[speed]
     if os.path.exists(out):
         return out
     if not ref_available():
@@ -154,7 +188,7 @@ def build_ref(cfg: dict, nbnd: int, hc: list) -> str:
         objs = []
         for fname, entry, local_off, inject in KERNELS[nd]:
             obj = os.path.join(td, entry + ".o")
-            cmd = ["gcc", *CFLAGS, "-c", "-o", obj, os.path.join(HERE, "ref_tu.c"), "-I" + HERE,
+            cmd = ["gcc", *flags, "-c", "-o", obj, os.path.join(HERE, "ref_tu.c"), "-I" + HERE,
                    "-I" + REF_SRC, *defs, "-DLOCAL_OFF=%d" % local_off,
                    "-DREF_KERNEL_FILE=%s" % fname, "-D%s=ref_%s" % (entry, entry)]
             if inject:
@@ -163,10 +197,13 @@ def build_ref(cfg: dict, nbnd: int, hc: list) -> str:
             objs.append(obj)
         glue = os.path.join(td, "glue.o")
         gdefs = [d for d in defs if d.split("=")[0] in ("-DND", "-DNX", "-DNY", "-DNZ", "-DFDOH")]
-        _run(["gcc", *CFLAGS, "-c", "-o", glue, os.path.join(HERE, "ref_glue.c"), "-I" + HERE, *gdefs])
+        _run(["gcc", *flags, "-c", "-o", glue, os.path.join(HERE, "ref_glue.c"), "-I" + HERE, *gdefs])
         tmp = out + ".tmp%d" % os.getpid()
-        _run(["gcc", *CFLAGS, "-shared", "-o", tmp, glue, *objs,
+        _run(["gcc", *flags, "-shared", "-o", tmp, glue, *objs,
               *[os.path.join(HERE, s) for s in PORT_SOURCES], "-lm"])
+        if speed == "native":
+            with open(out + ".cpu.json", "w") as fh:
+                json.dump({"flags": sorted(cpu_flags())}, fh)
         os.replace(tmp, out)
     return out
 

@@ -153,7 +153,7 @@ def source_type_mask(src_pos: np.ndarray) -> int:
 
 
 class Oracle:
-    def __init__(self, cfg: dict, ref: bool = False, fp64: bool = False):
+    def __init__(self, cfg: dict, ref: bool = False, fp64: bool = False, speed: str = "pin"):
         if ref and fp64:
             raise ValueError("the reference kernels are FP32 only")
         self.cfg = dict(DEFAULTS)
@@ -171,7 +171,7 @@ class Oracle:
             self.lib.fdo_destroy(h0)
             hc = (C.c_double * 7)()
             self.lib.fdo_holberg(self._c.fdorder, self._c.maxrelerror, hc)
-            path = _build.build_ref(self.cfg, int(info[5]), list(hc))
+            path = _build.build_ref(self.cfg, int(info[5]), list(hc), speed)
             self.lib = _lib(path)
         self.h = self._make(self.lib, ref)
         self.info = self._info(self.lib, self.h)
