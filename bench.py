@@ -642,6 +642,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=15.0)
     ap.add_argument("--kernel-reps", type=int, default=20)
     ap.add_argument("--nt", type=int, default=0, help="override NT (profiling runs only)")
+    ap.add_argument("--kernels", default="fast", choices=["fast", "fused", "vector", "stream", "tma", "general"],
+                    help="3D kernel family (default: the fastest measured)")
     ap.add_argument("--grid", type=int, default=0, help="3D workloads: override the grid with n^3 (profiling "
                     "runs only)")
     ap.add_argument("--clock-log", default="", help="file for the clock samples of the timed region "
@@ -676,7 +678,7 @@ def main():
 
     import dataclasses
 
-    plan = Plan(dataclasses.replace(engine_config(w), field_precision=args.fields))
+    plan = Plan(dataclasses.replace(engine_config(w), field_precision=args.fields, kernels=args.kernels))
     plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
     sp, src, rp, outs = acq["src_pos"], acq["src"], acq["rec_pos"], acq["outputs"]
     for _ in range(args.warmup):

@@ -1422,31 +1422,31 @@ __global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f, bool surf)
 // ------------------------------------------------- fused 3D forward step
 // One launch advances the whole grid one time step: velocity update, stress
 // and memory-variable update and (with a free surface) the free surface, so
-// the stresses read by the velocity stencils are read again by the stress
-// update of the same CTA, and the velocities it wrote are read back, while
-// both are still in L2.  Per cell the arithmetic is that of k_v3d_q4,
+// the stresses the velocity stencils read are read again by the stress
+// updates of nearby work units, and the velocities written are read back,
+// while both are still in L2.  Per cell the arithmetic is that of k_v3d_q4,
 // k_s3d_q4 and k_surf3d, in that order.
 //
-// Work unit: a block of FZ z cells x FY y rows (a "tile") times a chunk of
-// FX x planes.  A CTA takes a ticket (atomicAdd) and works on unit number
-// ticket - base, units ordered chunk-major (x slowest), so the units a CTA
-// waits for were always taken by CTAs that started earlier.  Phase 1 updates
-// the velocities of planes [x0 + 4, x1 + 4) of the tile (chunk 0 from x = F,
-// the last chunk up to the grid's end) and publishes the unit's flag; phase
-// 2 waits for the flags of the units whose velocities its stencils read --
-// the same chunk's four y/z neighbours and, for the first 4 planes, the
-// previous chunk's tile and its neighbours -- then updates the stresses of
-// planes [x0, x1).  Everything is updated in place; the waits also order
-// every stress overwrite after all velocity reads of the old value: a
-// stress cell of unit (c, t) is read by the velocity stencils of units
-// (c, t), (c, t's y/z neighbours) and (c - 1, t and its neighbours) only,
-// the units (c, t) waits for.  A unit waits at most ntz tickets ahead, so
-// progress needs only ntz + 2 co-resident CTAs (ntz <= 64 is required).
-// Reads of velocities in phase 2 go through L2 (__ldcg): other CTAs wrote
-// them during the launch.  Waits are bounded (FUSED_WAIT_NS of
-// %globaltimer); a wait that runs out sets g_fused_status, which makes every
-// later CTA and launch skip its work and the host report an error.
-constexpr int FZ = 32, FY = 8, FX = 8;
+// Work unit: a tile of FZ z cells x FY y rows in one x plane.  A CTA takes a
+// ticket (atomicAdd) and works on unit number ticket - base; units are
+// numbered plane by plane (x slowest).  Unit (c, t) first updates the
+// velocities of plane F + c + 4 of tile t (unit 0 also planes F .. F + 3) and
+// publishes its flag, then waits for the flags of the units whose velocities
+// its stress stencils read -- planes F + c - 4 .. F + c + 4 of its own tile
+// (units c - 8 .. c - 1) and plane F + c of the four y/z neighbour tiles
+// (units c - 4) -- and updates the stresses of plane F + c.  Every wait is
+// on a unit with a lower number, taken by a CTA that started earlier, so the
+// waits always end however few CTAs are resident.  Everything is updated
+// in place; the same waits order every stress overwrite after all velocity
+// reads of the old value: the stresses of plane F + c in tile t are read by
+// the velocity updates of planes F + c - 4 .. F + c + 4 in tile t (units
+// c - 8 .. c) and of plane F + c in its neighbours (units c - 4), exactly
+// the units (c, t) waits for.  Velocity reads of the stress phase go
+// through L2 (__ldcg): other CTAs wrote them during the launch.  Waits are
+// bounded (FUSED_WAIT_NS of %globaltimer); one that runs out sets
+// g_fused_status, which makes every later CTA and launch skip its work and
+// the host report an error.
+constexpr int FZ = 32, FY = 16;
 constexpr unsigned long long FUSED_WAIT_NS = 2000000000ull;
 __device__ int g_fused_status;   // 0 ok, 1 a wait ran out
 
@@ -1486,7 +1486,7 @@ __global__ void __launch_bounds__(128, 4) k_fused3d_q4(Grid g, Fields f, FusedSy
 {
     constexpr int F = 4;
     __shared__ int s_unit, s_go;
-    const int tid = threadIdx.x + 8 * (threadIdx.y + 4 * threadIdx.z);
+    const int tid = threadIdx.x + 8 * threadIdx.y;
     if (tid == 0) {
         s_unit = (int)(atomicAdd(fs.ticket, 1u) - fs.base);
         s_go = *(volatile int *)&g_fused_status == 0;
@@ -1499,62 +1499,65 @@ __global__ void __launch_bounds__(128, 4) k_fused3d_q4(Grid g, Fields f, FusedSy
         return;
     }
     const int c = unit / ntile, tile = unit - c * ntile, ty = tile / fs.ntz, tz = tile - ty * fs.ntz;
-    const int gz0 = F + tz * FZ + 4 * threadIdx.x;
-    const bool zok = gz0 <= g.NZ - F - 1;
-    const int xs0 = F + c * FX, xs1 = min(xs0 + FX, g.NX - F);
-    const int xv0 = c == 0 ? F : xs0 + 4, xv1 = min(xs1 + 4, g.NX - F);
+    const int gz0 = F + tz * FZ + 4 * threadIdx.x, gy = F + ty * FY + threadIdx.y;
+    const bool ok_cell = gz0 <= g.NZ - F - 1 && gy <= g.NY - F - 1;
+    const int nxp = g.NX - 2 * F;   // x planes
     const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;
-    // phase 1: velocities.  The stress reads take the read-only path: no
-    // stress cell this phase reads is overwritten before the phase ends (the
-    // writer waits for this unit's flag), and no reader in this launch
-    // needs a value written in it.
-    if (zok) {
-        for (int gx = xv0 + (int)threadIdx.z; gx < xv1; gx += 4)
-            for (int yy = threadIdx.y; yy < FY; yy += 4) {
-                const int gy = F + ty * FY + yy;
-                if (gy > g.NY - F - 1) continue;
-                const i64 iv = gx * sx + (i64)gy * sy + gz0;
-                const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
-                v3d_q4_at<float, 0>(g, f, gz0, gy, gx, iv, ip);
-            }
+    // phase 1: velocities of plane F + c + 4 (unit 0: planes F .. F + 4).
+    // The stress reads take the read-only path: no stress cell read here is
+    // overwritten before this unit's flag is up, and nothing in this launch
+    // reads a stress value written in it.
+    if (ok_cell) {
+        const int x0 = c == 0 ? F : F + c + 4, x1 = min(F + c + 5, g.NX - F);
+        for (int gx = x0; gx < x1; gx++) {
+            const i64 iv = gx * sx + (i64)gy * sy + gz0;
+            const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
+            v3d_q4_at<float, 0>(g, f, gz0, gy, gx, iv, ip);
+        }
     }
     __syncthreads();
     if (tid == 0) {
         __threadfence();
         st_release_gpu(fs.flags + unit, epoch);
-        bool ok = true;
-        for (int cc = c; cc >= max(c - 1, 0) && ok; cc--) {
-            const int base = cc * ntile;
-            if (cc != c) ok = ok && fused_wait(fs.flags + base + tile, epoch);
-            if (tz > 0) ok = ok && fused_wait(fs.flags + base + tile - 1, epoch);
-            if (tz < fs.ntz - 1) ok = ok && fused_wait(fs.flags + base + tile + 1, epoch);
-            if (ty > 0) ok = ok && fused_wait(fs.flags + base + tile - fs.ntz, epoch);
-            if (ty < fs.nty - 1) ok = ok && fused_wait(fs.flags + base + tile + fs.ntz, epoch);
+    }
+    // the units this one reads velocities of: threads 0..7 the own tile's
+    // planes (units c - 8 .. c - 1; unit 0 holds planes F .. F + 4), threads
+    // 8..11 the neighbours' plane F + c (unit c - 4)
+    bool ok = true;
+    if (tid < 12) {
+        int wu = -1;
+        if (tid < 8) {
+            const int uc = c - 8 + tid;
+            if (uc >= 0 && uc <= nxp - 5) wu = uc * ntile + tile;
+        } else {
+            const int nt = tid == 8 ? (tz > 0 ? tile - 1 : -1)
+                         : tid == 9 ? (tz < fs.ntz - 1 ? tile + 1 : -1)
+                         : tid == 10 ? (ty > 0 ? tile - fs.ntz : -1)
+                                     : (ty < fs.nty - 1 ? tile + fs.ntz : -1);
+            if (nt >= 0) wu = max(c - 4, 0) * ntile + nt;
         }
-        if (!ok) atomicExch(&g_fused_status, 1);
-        s_go = ok;
+        if (wu >= 0) ok = fused_wait(fs.flags + wu, epoch);
         __threadfence();
     }
-    __syncthreads();
-    if (!s_go || !zok) return;
-    // phase 2: stresses, memory variables, free surface (velocity reads via L2)
-    const bool surf = g.freesurf != 0;
-    for (int gx = xs0 + (int)threadIdx.z; gx < xs1; gx += 4)
-        for (int yy = threadIdx.y; yy < FY; yy += 4) {
-            const int gy = F + ty * FY + yy;
-            if (gy > g.NY - F - 1) continue;
-            const i64 iv = gx * sx + (i64)gy * sy + gz0;
-            const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
-            s3d_q4_at<L, float, 2>(g, f, gz0, gy, gx, iv, ip, surf);
-        }
+    if (!__syncthreads_and(ok)) {
+        if (tid == 0) atomicExch(&g_fused_status, 1);
+        return;
+    }
+    if (!ok_cell) return;
+    // phase 2: stresses, memory variables, free surface of plane F + c
+    // (velocity reads through L2)
+    const int gx = F + c;
+    const i64 iv = gx * sx + (i64)gy * sy + gz0;
+    const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
+    s3d_q4_at<L, float, 2>(g, f, gz0, gy, gx, iv, ip, g.freesurf != 0);
 }
 
 FusedShape fused_shape(const Grid &g)
 {
     FusedShape s{0, 0, 0, 0};
     if (!g.fused || g.nd != 3 || g.F != 4 || g.nz % 4 || g.fhalf || g.L < 0 || g.L > 3 || g.kernels != 0) return s;
-    const int ntz = (g.nz + FZ - 1) / FZ, nty = (g.ny + FY - 1) / FY, nch = (g.nx + FX - 1) / FX;
-    if (ntz > 64 || (int64_t)ntz * nty * nch > (1 << 30)) return s;
+    const int ntz = (g.nz + FZ - 1) / FZ, nty = (g.ny + FY - 1) / FY, nch = g.nx;
+    if (g.nx < 5 || (int64_t)ntz * nty * nch > (1 << 30)) return s;
     s.ntz = ntz;
     s.nty = nty;
     s.nchunk = nch;
@@ -1566,16 +1569,9 @@ bool launch_fused_step(const Grid &g, const Fields &f, int *sync, int t, cudaStr
 {
     const FusedShape sh = fused_shape(g);
     if (!sh.units || g.nb != 1 || !sync) return false;
-    static int resident = -1;   // CTAs of the kernel one SM holds (any L; checked once)
-    if (resident < 0) {
-        int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused3d_q4<3>, 128, 0) != cudaSuccess) n = 0;
-        resident = n;
-    }
-    if (resident < 1) return false;
     FusedSync fs{reinterpret_cast<unsigned *>(sync), sync + 1, (unsigned)((uint64_t)t * (uint64_t)sh.units),
                  sh.ntz, sh.nty, (int)sh.units};
-    const dim3 b(8, 4, 4);
+    const dim3 b(8, FY, 1);
     const unsigned gr = (unsigned)sh.units;
     switch (g.L) {
     case 0: k_fused3d_q4<0><<<gr, b, 0, st>>>(g, f, fs, t + 1); break;

@@ -30,7 +30,8 @@ bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_
 // Fused 3D forward step (velocity, stress, free surface in one launch; see
 // sfd_kernels.cu).  Work units = ntz x nty x nchunk; units = 0 when the plan's
 // grid does not take it (sfd_config.kernels 6; 3D, 8th order, nz % 4 == 0,
-// FP32 fields, L <= 3, at most 64 z tiles).
+// FP32 fields, L <= 3, nx >= 5).  nchunk = x planes (one unit per tile and
+// plane).
 struct FusedShape {
     int ntz, nty, nchunk;
     int64_t units;
