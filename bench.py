@@ -642,7 +642,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=15.0)
     ap.add_argument("--kernel-reps", type=int, default=20)
     ap.add_argument("--nt", type=int, default=0, help="override NT (profiling runs only)")
-    ap.add_argument("--kernels", default="fast", choices=["fast", "fused", "vector", "stream", "tma", "general"],
+    ap.add_argument("--kernels", default="fast", choices=["fast", "fused", "async", "vector", "stream", "tma", "general"],
                     help="3D kernel family (default: the fastest measured)")
     ap.add_argument("--grid", type=int, default=0, help="3D workloads: override the grid with n^3 (profiling "
                     "runs only)")

@@ -875,7 +875,7 @@ int check_config(const sfd_config &c)
     // N[0] must be even (read_hdf5.c:535-540)
     if (c.n[0] % 2) return SFD_ERR_ARG;
     if (c.precision < 0 || c.precision > 2) return SFD_ERR_ARG;
-    if (c.kernels < 0 || c.kernels > 6) return SFD_ERR_ARG;
+    if (c.kernels < 0 || c.kernels > 7) return SFD_ERR_ARG;
     if (c.adjoint_reset_psi < 0 || c.adjoint_reset_psi > 1) return SFD_ERR_ARG;
     if (c.field_precision < 0 || c.field_precision > 1) return SFD_ERR_ARG;
     if (c.field_precision == 1 && (c.nd != 3 || c.L > 3)) return SFD_ERR_UNSUPPORTED;
@@ -914,8 +914,11 @@ void init_grid(const sfd_config &c, Grid &g)
     g.L = c.L;
     g.freesurf = c.freesurf ? 1 : 0;
     g.restype = c.restype;
-    g.kernels = c.kernels == 6 ? 0 : c.kernels;   // 6: the kernels of 0, plus the fused modelling step
+    // 6: the kernels of 0, plus the fused modelling step; 7: the kernels of 0
+    // with the cp.async-staged velocity update
+    g.kernels = (c.kernels == 6 || c.kernels == 7) ? 0 : c.kernels;
     g.fused = c.kernels == 6;
+    g.vasync = c.kernels == 7;
     g.hout = c.hout;
     g.nvol = (int64_t)g.NZ * g.NY * g.NX;
     double hc[6];

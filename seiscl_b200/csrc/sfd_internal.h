@@ -64,6 +64,7 @@ struct Grid {
     int restype;
     int kernels;            // 0: register-blocked 3D kernels where available, 1: general only
     int fused;              // 1: 3D modelling runs take the fused step kernel (sfd_config.kernels 6)
+    int vasync;             // 1: 3D single-shot velocity updates take the cp.async-staged kernel (kernels 7)
     int bp2;                // adjoint kernels: 1 for the DFT gradient (no reconstruction,
                             // boundary injection or on-the-fly gradient)
     int hout;               // accumulate the approximate Hessian

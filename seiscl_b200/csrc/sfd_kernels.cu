@@ -1093,6 +1093,226 @@ __global__ void __launch_bounds__(128, 4) k_v3d_q4_b4(Grid g, Fields f)
     v3d_q4<float, false>(g, f);
 }
 
+// ------------------------------------- velocity update staged by cp.async
+// k_v3d_q4's arithmetic with its stress operands staged in shared memory by
+// asynchronous copies (cp.async, 16 bytes each), so the bytes in flight do
+// not hold registers.  A CTA owns a tile of AZ z cells x AY y rows and
+// marches over AX x planes; one thread updates one quad (4 z cells) per
+// plane.  Shared memory holds
+//   ring   sxx, sxy, sxz (the x derivatives) over the tile's own columns, for
+//          planes x-4 .. x+5 (10 slots; plane x+5 arrives while x is computed);
+//   halo   syy, szz, syz, sxy, sxz over the tile plus a 4-cell y/z halo for
+//          plane x (y and z derivatives), double-buffered.
+// The copies of plane x+2 are issued after plane x is computed and committed
+// as one group; cp.async.wait_group 1 then leaves only the newest group in
+// flight.  The waits are on the thread's own copies: they always end.
+constexpr int AZ = 32, AY = 16, AX = 16;
+constexpr int AHZ = AZ + 8, AHY = AY + 8;
+constexpr int ARING = 10;
+struct VAsyncSmem {
+    float ring[3][ARING][AY][AZ];
+    float halo[2][5][AHY][AHZ];
+};
+constexpr size_t VASYNC_SMEM = sizeof(VAsyncSmem);
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+__device__ __forceinline__ Q4 lds4(const float *p)
+{
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    return Q4{{t.x, t.y, t.z, t.w}};
+}
+// forward / backward differences of a quad over shared-memory rows `st`
+// floats apart (the operation order of dfw_q / dbw_q)
+__device__ __forceinline__ Q4 dfw_s(const float *p, int st, const float *hc)
+{
+    Q4 a = lds4(p + st), b = lds4(p), r;
+#pragma unroll
+    for (int j = 0; j < 4; j++) r.v[j] = hc[0] * (a.v[j] - b.v[j]);
+#pragma unroll
+    for (int m = 2; m <= 4; m++) {
+        a = lds4(p + m * st);
+        b = lds4(p - (m - 1) * st);
+#pragma unroll
+        for (int j = 0; j < 4; j++) r.v[j] = fmaf(hc[m - 1], a.v[j] - b.v[j], r.v[j]);
+    }
+    return r;
+}
+__device__ __forceinline__ Q4 dbw_s(const float *p, int st, const float *hc)
+{
+    Q4 a = lds4(p), b = lds4(p - st), r;
+#pragma unroll
+    for (int j = 0; j < 4; j++) r.v[j] = hc[0] * (a.v[j] - b.v[j]);
+#pragma unroll
+    for (int m = 2; m <= 4; m++) {
+        a = lds4(p + (m - 1) * st);
+        b = lds4(p - m * st);
+#pragma unroll
+        for (int j = 0; j < 4; j++) r.v[j] = fmaf(hc[m - 1], a.v[j] - b.v[j], r.v[j]);
+    }
+    return r;
+}
+// the 12 values z0-4 .. z0+7 of a quad from a halo row (p at z0 - 4)
+__device__ __forceinline__ W12 ldw_s(const float *p)
+{
+    W12 r;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const Q4 t = lds4(p + 4 * k);
+        r.w[4 * k] = t.v[0]; r.w[4 * k + 1] = t.v[1]; r.w[4 * k + 2] = t.v[2]; r.w[4 * k + 3] = t.v[3];
+    }
+    return r;
+}
+
+// issue the copies of plane x: ring slot of plane x+5 (when inside the grid)
+// and the haloed tiles of plane x into halo buffer hb
+__device__ __forceinline__ void vasync_issue(const Grid &g, const Fields &f, VAsyncSmem &sm, int z0, int y0,
+                                             int xr, int xh, int hb, int tid)
+{
+    const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;
+    if (xr >= 0 && xr < g.NX) {
+        const float *rf[3] = {f.w[SXX], f.w[SXY], f.w[SXZ]};
+        const int slot = xr % ARING;
+        for (int i = tid; i < 3 * AY * (AZ / 4); i += 128) {
+            const int q = i / (AY * (AZ / 4)), r = (i / (AZ / 4)) % AY, c = i % (AZ / 4);
+            const int gy = y0 + r, gz = z0 + 4 * c;
+            if (gy < g.NY && gz + 3 < g.NZ)
+                cp_async16(&sm.ring[q][slot][r][4 * c], rf[q] + xr * sx + (i64)gy * sy + gz);
+        }
+    }
+    if (xh >= 0) {
+        const float *hf[5] = {f.w[SYY], f.w[SZZ], f.w[SYZ], f.w[SXY], f.w[SXZ]};
+        for (int i = tid; i < 5 * AHY * (AHZ / 4); i += 128) {
+            const int q = i / (AHY * (AHZ / 4)), r = (i / (AHZ / 4)) % AHY, c = i % (AHZ / 4);
+            const int gy = y0 - 4 + r, gz = z0 - 4 + 4 * c;
+            if (gy >= 0 && gy < g.NY && gz >= 0 && gz + 3 < g.NZ)
+                cp_async16(&sm.halo[hb][q][r][4 * c], hf[q] + xh * sx + (i64)gy * sy + gz);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128, 2) k_v3d_async(Grid g, Fields f)
+{
+    constexpr int F = 4;
+    extern __shared__ __align__(16) unsigned char vasync_raw[];
+    VAsyncSmem &sm = *reinterpret_cast<VAsyncSmem *>(vasync_raw);
+    const int tid = threadIdx.x + 8 * threadIdx.y;
+    const int z0 = F + blockIdx.x * AZ, y0 = F + blockIdx.y * AY;
+    const int xb = F + blockIdx.z * AX, xe = min(xb + AX, g.NX - F);
+    const int qz = threadIdx.x, yy = threadIdx.y;
+    const int gz0 = z0 + 4 * qz, gy = y0 + yy;
+    const bool ok = gz0 <= g.NZ - F - 1 && gy <= g.NY - F - 1;
+    const float *hc = g.hc;
+    const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;
+    // prologue: ring planes xb-4 .. xb+4 and the halo of plane xb (group 0),
+    // ring plane xb+5 and the halo of plane xb+1 (group 1)
+    for (int xr = xb - 4; xr < xb + 4; xr++) vasync_issue(g, f, sm, z0, y0, xr, -1, 0, tid);
+    vasync_issue(g, f, sm, z0, y0, xb + 4, xb, 0, tid);
+    cp_async_commit();
+    vasync_issue(g, f, sm, z0, y0, xb + 5, xb + 1 < xe ? xb + 1 : -1, 1, tid);
+    cp_async_commit();
+    for (int gx = xb; gx < xe; gx++) {
+        const int hb = (gx - xb) & 1;
+        Q4 vx, vy, vz, rip, rjp, rkp;
+        const i64 iv = gx * sx + (i64)gy * sy + gz0;
+        const i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz0 - F);
+        if (ok) {
+            vx = ldq_rw(f.w[VX] + iv); vy = ldq_rw(f.w[VY] + iv); vz = ldq_rw(f.w[VZ] + iv);
+            rip = ldq(f.p[PRIP] + ip); rjp = ldq(f.p[PRJP] + ip); rkp = ldq(f.p[PRKP] + ip);
+        }
+        cp_async_wait<1>();
+        __syncthreads();
+        if (ok) {
+            const float *H0 = &sm.halo[hb][0][0][0];
+            const int HP = AHY * AHZ;                 // floats per haloed tile
+            const int hrow = (yy + 4) * AHZ + 4 * qz;  // the quad's row, at z0 - 4 of its window
+            const W12 wzz = ldw_s(H0 + 1 * HP + hrow), wxz = ldw_s(H0 + 4 * HP + hrow),
+                      wyz = ldw_s(H0 + 2 * HP + hrow);
+            const int RP = AY * AZ;                    // floats per ring slot
+            const int rc = yy * AZ + 4 * qz;
+            auto ring_at = [&](int q, int x) { return &sm.ring[q][x % ARING][0][0] + rc; };
+            Q4 szz_z = dfw_z<F>(wzz, hc);
+            Q4 sxx_x, sxz_x, sxy_x;
+            {
+                // x differences across ring slots (plane offsets wrap modulo ARING)
+                const float *c0 = ring_at(0, gx);
+                (void)RP;
+                Q4 a = lds4(ring_at(0, gx + 1)), b = lds4(c0), r;
+#pragma unroll
+                for (int j = 0; j < 4; j++) r.v[j] = hc[0] * (a.v[j] - b.v[j]);
+#pragma unroll
+                for (int m = 2; m <= F; m++) {
+                    a = lds4(ring_at(0, gx + m));
+                    b = lds4(ring_at(0, gx - (m - 1)));
+#pragma unroll
+                    for (int j = 0; j < 4; j++) r.v[j] = fmaf(hc[m - 1], a.v[j] - b.v[j], r.v[j]);
+                }
+                sxx_x = r;
+                for (int q = 1; q <= 2; q++) {
+                    a = lds4(ring_at(q, gx));
+                    b = lds4(ring_at(q, gx - 1));
+#pragma unroll
+                    for (int j = 0; j < 4; j++) r.v[j] = hc[0] * (a.v[j] - b.v[j]);
+#pragma unroll
+                    for (int m = 2; m <= F; m++) {
+                        a = lds4(ring_at(q, gx + m - 1));
+                        b = lds4(ring_at(q, gx - m));
+#pragma unroll
+                        for (int j = 0; j < 4; j++) r.v[j] = fmaf(hc[m - 1], a.v[j] - b.v[j], r.v[j]);
+                    }
+                    if (q == 1) sxy_x = r;
+                    else sxz_x = r;
+                }
+            }
+            Q4 sxz_z = dbw_z<F>(wxz, hc);
+            Q4 syz_y = dbw_s(H0 + 2 * HP + hrow + 4, AHZ, hc);
+            Q4 syz_z = dbw_z<F>(wyz, hc);
+            Q4 syy_y = dfw_s(H0 + 0 * HP + hrow + 4, AHZ, hc);
+            Q4 sxy_y = dbw_s(H0 + 3 * HP + hrow + 4, AHZ, hc);
+            if (g.abs_type == 1)
+                cpml_v3d_q4(g, f, gz0, gy, gx, sxx_x, syy_y, szz_z, sxy_y, sxy_x, syz_y, syz_z, sxz_x, sxz_z);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                float v3[3] = {vx.v[j] + (sxx_x.v[j] + sxy_y.v[j] + sxz_z.v[j]) * rip.v[j],
+                               vy.v[j] + (syy_y.v[j] + sxy_x.v[j] + syz_z.v[j]) * rjp.v[j],
+                               vz.v[j] + (szz_z.v[j] + sxz_x.v[j] + syz_y.v[j]) * rkp.v[j]};
+                if (g.abs_type == 2) taper_regs<3>(g, f.taper, gz0 + j, gy, gx, v3);
+                vx.v[j] = v3[0]; vy.v[j] = v3[1]; vz.v[j] = v3[2];
+            }
+            stq(f.w[VX] + iv, vx);
+            stq(f.w[VY] + iv, vy);
+            stq(f.w[VZ] + iv, vz);
+        }
+        __syncthreads();   // plane gx-4's ring slot and halo buffer hb are free
+        vasync_issue(g, f, sm, z0, y0, gx + 6, gx + 2 < xe ? gx + 2 : -1, hb, tid);
+        cp_async_commit();
+    }
+    cp_async_wait<0>();
+}
+
+bool launch_update_v_async(const Grid &g, const Fields &f, cudaStream_t st)
+{
+    if (g.nd != 3 || g.F != 4 || g.nz % 4 || g.fhalf || g.nb != 1) return false;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_v3d_async, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)VASYNC_SMEM) !=
+            cudaSuccess)
+            return false;
+        attr = true;
+    }
+    const dim3 b(8, AY), gr((g.nz + AZ - 1) / AZ, (g.ny + AY - 1) / AY, (g.nx + AX - 1) / AX);
+    k_v3d_async<<<gr, b, VASYNC_SMEM, st>>>(g, f);
+    return true;
+}
+
 // CPML corrections of cpml_s3d (forward form) for a quad of z cells
 __device__ __forceinline__ void cpml_s3d_q4(const Grid &g, const Fields &f, int gz0, int gy, int gx, Q4 &vxx,
                                             Q4 &vxy, Q4 &vxz, Q4 &vyx, Q4 &vyy, Q4 &vyz, Q4 &vzx, Q4 &vzy, Q4 &vzz)
@@ -3061,6 +3281,7 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
     // streaming one; only kernels 3 takes the TMA path
     if (g.kernels == 3 && launch_update_v_tma(g, f, st)) return;
     if (g.kernels == 2 && launch_update_v_fast(g, f, st)) return;
+    if (g.vasync && launch_update_v_async(g, f, st)) return;
     if (g.nd == 21 || g.nd == 22) {
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
         if (g.nd == 21) DISPATCH_F(g.F, k_v2d_sh<FF><<<gr, b, 0, st>>>(g, f))

@@ -15,6 +15,7 @@ struct BndSlot {            // saved-boundary stores, by value
 
 void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st);
 bool launch_update_v_fast(const Grid &g, const Fields &f, cudaStream_t st);
+bool launch_update_v_async(const Grid &g, const Fields &f, cudaStream_t st);
 bool launch_update_s_fast(const Grid &g, const Fields &f, cudaStream_t st);
 int fast3d_xchunk(const Grid &g);
 bool launch_update_v_tma(const Grid &g, const Fields &f, cudaStream_t st);

@@ -192,7 +192,7 @@ class Config:
         c.restype = int(self.restype)
         c.precision = PREC[self.precision]
         c.kernels = {"fast": 0, "general": 1, "register": 2, "tma": 3, "stream": 4, "vector": 5,
-                     "fused": 6}[self.kernels]
+                     "fused": 6, "async": 7}[self.kernels]
         c.adjoint_reset_psi = 1 if self.adjoint_reset_psi else 0
         c.batch = int(self.batch)
         c.checkpoint = int(self.checkpoint)
