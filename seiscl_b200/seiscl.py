@@ -866,20 +866,22 @@ class SeisCL:
             if movies is not None:
                 plan.set_movie(0)
         if world > 1:
-            # every rank filled only its own traces: one sum gives all of them
-            # (Out_MPI.c:70-160); the gradient is summed after the chain rule,
-            # which is linear in the accumulated kernels
-            red = {"seis_" + k: v for k, v in seis.items()}
-            red.update({"res_" + k: v for k, v in resid.items()})
-            red["rms"] = np.array([rms, rmsnorm])
+            # every rank filled only the traces of its own shots, a contiguous
+            # block of rows (shots and traces ascend by srcid): gather the
+            # blocks (Out_MPI.c:70-160); the misfit is summed, and the
+            # gradient below too, after the chain rule, which is linear in the
+            # accumulated kernels
+            rows = [gi for _, _, gi in shots[smin:smax]]
+            lo = int(min((r.min() for r in rows if len(r)), default=0))
+            hi = int(max((r.max() + 1 for r in rows if len(r)), default=lo))
+            tr = {"seis_" + k: v for k, v in seis.items()}
+            tr.update({"res_" + k: v for k, v in resid.items()})
+            tr = shots_mod.gather_rows(tr, lo, hi)
+            seis = {k: tr["seis_" + k] for k in seis}
+            resid = {k: tr["res_" + k] for k in resid}
             if movies is not None:
-                red.update({"mov_" + k: v for k, v in movies.items()})
-            red = shots_mod.allreduce_sum(red)
-            if movies is not None:
-                movies = {k: red["mov_" + k] for k in movies}
-            seis = {k: red["seis_" + k] for k in seis}
-            resid = {k: red["res_" + k] for k in resid}
-            rms, rmsnorm = (float(v) for v in red["rms"])
+                movies = shots_mod.gather_rows(movies, smin, smax)
+            rms, rmsnorm = (float(v) for v in shots_mod.allreduce_sum({"rms": np.array([rms, rmsnorm])})["rms"])
         if not (self.inputres and self.gradout):
             dout = {k + "out": np.ascontiguousarray(seis[k].T) for k in outs}
             if self.resout and not self.inputres:
