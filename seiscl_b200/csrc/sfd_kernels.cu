@@ -909,26 +909,29 @@ __device__ __forceinline__ Q4 dbw_z(const W12 &w, const float *hc)
 }
 
 // CPML recursion on four consecutive z cells sharing one profile index
-// (y and x slabs: the psi arrays are z-fastest and 16-byte aligned there);
-// same order of operations per cell as cpml()
-__device__ __forceinline__ void cpml_q(float *psi, i64 q, const float *K, const float *a, const float *b, int ci,
+// (y and x slabs: the psi arrays are z-fastest and 16-byte aligned there).
+// cpml()'s recursion, with the division by K replaced by a multiplication by
+// 1/K (Fields::kinv, rounded to FP32 on the host): within one rounding of
+// the quotient per cell, and a third cheaper in the CPML slabs, where the
+// FP32 divisions took as long as the slabs' own psi traffic.
+__device__ __forceinline__ void cpml_q(float *psi, i64 q, const float *Ki, const float *a, const float *b, int ci,
                                        Q4 &d)
 {
-    const float kk = __ldg(K + ci), aa = __ldg(a + ci), bb = __ldg(b + ci);
+    const float ki = __ldg(Ki + ci), aa = __ldg(a + ci), bb = __ldg(b + ci);
     Q4 p = ldq_rw(psi + q);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
         float ps = bb * p.v[j] + aa * d.v[j];
         p.v[j] = ps;
-        d.v[j] = d.v[j] / kk + ps;
+        d.v[j] = d.v[j] * ki + ps;
     }
     stq(psi + q, p);
 }
 
 // z-slab CPML on a quad that lies entirely inside the slab: the psi cells
 // are consecutive (z-type psi is [nx][ny][2 nab], k fastest), the profile
-// index differs per cell (ci0 + step * j)
-__device__ __forceinline__ void cpml_zq(float *psi, i64 q, const float *K, const float *a, const float *b, int ci0,
+// index differs per cell (ci0 + step * j); multiplies by 1/K as cpml_q
+__device__ __forceinline__ void cpml_zq(float *psi, i64 q, const float *Ki, const float *a, const float *b, int ci0,
                                         int step, Q4 &d)
 {
     Q4 p = ldq_rw(psi + q);
@@ -937,9 +940,19 @@ __device__ __forceinline__ void cpml_zq(float *psi, i64 q, const float *K, const
         const int ci = ci0 + step * j;
         float ps = __ldg(b + ci) * p.v[j] + __ldg(a + ci) * d.v[j];
         p.v[j] = ps;
-        d.v[j] = d.v[j] / __ldg(K + ci) + ps;
+        d.v[j] = d.v[j] * __ldg(Ki + ci) + ps;
     }
     stq(psi + q, p);
+}
+
+// Grids whose absorbing slabs cannot overlap (every axis at least 2 nab
+// cells, the z axis 2 nab + 4) with nab % 4 == 0: a cell lies in at most one
+// slab per axis and a z quad lies wholly inside or outside a z slab, so each
+// axis takes one path, its side picked by selects.  The general forms below
+// follow the reference's branch structure, which small grids need.
+__device__ __forceinline__ bool cpml_slabs_apart(const Grid &g)
+{
+    return g.nab % 4 == 0 && g.nz >= 2 * g.nab + 4 && g.ny >= 2 * g.nab && g.nx >= 2 * g.nab;
 }
 
 // The CPML corrections of cpml_v3d for a quad of z cells: z slabs per cell
@@ -950,19 +963,52 @@ __device__ __forceinline__ void cpml_v3d_q4(const Grid &g, const Fields &f, int 
 {
     const int F = g.F, NAB = g.nab, NZ = g.NZ, NY = g.NY, NX = g.NX;
     const i64 nz = g.nz, ny = g.ny;
+    if (cpml_slabs_apart(g)) {
+        // side-merged form: far-side profile indices are 2 nab - k (integer
+        // grid) and 2 nab - 1 - k (half grid) of the slab-local index k
+        const i64 k0 = gz0 - F;
+        const bool zhi = gz0 > NZ - NAB - F - 1, zlo = !g.freesurf && gz0 - F < NAB;
+        if (zhi || zlo) {
+            const int k = zhi ? gz0 - NZ + 2 * NAB + F : gz0 - F;
+            const int st = zhi ? -1 : 1, cf = zhi ? 2 * NAB - k : k, ch = zhi ? 2 * NAB - 1 - k : k;
+            const i64 q = ((i64)(gx - F) * ny + (gy - F)) * (2 * NAB) + k;
+            cpml_zq(f.psi[PSXZ_Z], q, f.kinv[2][0], f.cz[CA], f.cz[CB], cf, st, sxz_z);
+            cpml_zq(f.psi[PSYZ_Z], q, f.kinv[2][0], f.cz[CA], f.cz[CB], cf, st, syz_z);
+            cpml_zq(f.psi[PSZZ_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], ch, st, szz_z);
+        }
+        const bool ylo = gy - F < NAB, yhi = gy > NY - NAB - F - 1;
+        if (ylo || yhi) {
+            const int j = ylo ? gy - F : gy - NY + 2 * NAB + F;
+            const int cf = ylo ? j : 2 * NAB - j, ch = ylo ? j : 2 * NAB - 1 - j;
+            const i64 q = ((i64)(gx - F) * (2 * NAB) + j) * nz + k0;
+            cpml_q(f.psi[PSXY_Y], q, f.kinv[1][0], f.cy[CA], f.cy[CB], cf, sxy_y);
+            cpml_q(f.psi[PSYY_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], ch, syy_y);
+            cpml_q(f.psi[PSYZ_Y], q, f.kinv[1][0], f.cy[CA], f.cy[CB], cf, syz_y);
+        }
+        const bool xlo = gx - F < NAB, xhi = gx > NX - NAB - F - 1;
+        if (xlo || xhi) {
+            const int i = xlo ? gx - F : gx - NX + 2 * NAB + F;
+            const int cf = xlo ? i : 2 * NAB - i, ch = xlo ? i : 2 * NAB - 1 - i;
+            const i64 q = ((i64)i * ny + (gy - F)) * nz + k0;
+            cpml_q(f.psi[PSXX_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], ch, sxx_x);
+            cpml_q(f.psi[PSXY_X], q, f.kinv[0][0], f.cx[CA], f.cx[CB], cf, sxy_x);
+            cpml_q(f.psi[PSXZ_X], q, f.kinv[0][0], f.cx[CA], f.cx[CB], cf, sxz_x);
+        }
+        return;
+    }
     if (NAB % 4 == 0 && gz0 > NZ - NAB - F - 1) {
         i64 i = gx - F, jj = gy - F, k = gz0 - NZ + NAB + F + NAB;
         int ind = 2 * NAB - 1 - (int)k;
         i64 q = (i * ny + jj) * (2 * NAB) + k;
-        cpml_zq(f.psi[PSXZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, -1, sxz_z);
-        cpml_zq(f.psi[PSYZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, -1, syz_z);
-        cpml_zq(f.psi[PSZZ_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, -1, szz_z);
+        cpml_zq(f.psi[PSXZ_Z], q, f.kinv[2][0], f.cz[CA], f.cz[CB], ind + 1, -1, sxz_z);
+        cpml_zq(f.psi[PSYZ_Z], q, f.kinv[2][0], f.cz[CA], f.cz[CB], ind + 1, -1, syz_z);
+        cpml_zq(f.psi[PSZZ_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], ind, -1, szz_z);
     } else if (NAB % 4 == 0 && !g.freesurf && gz0 - F < NAB) {
         i64 i = gx - F, jj = gy - F, k = gz0 - F;
         i64 q = (i * ny + jj) * (2 * NAB) + k;
-        cpml_zq(f.psi[PSXZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, 1, sxz_z);
-        cpml_zq(f.psi[PSYZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, 1, syz_z);
-        cpml_zq(f.psi[PSZZ_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, 1, szz_z);
+        cpml_zq(f.psi[PSXZ_Z], q, f.kinv[2][0], f.cz[CA], f.cz[CB], (int)k, 1, sxz_z);
+        cpml_zq(f.psi[PSYZ_Z], q, f.kinv[2][0], f.cz[CA], f.cz[CB], (int)k, 1, syz_z);
+        cpml_zq(f.psi[PSZZ_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], (int)k, 1, szz_z);
     } else if (NAB % 4 != 0 && (gz0 + 3 > NZ - NAB - F - 1 || (!g.freesurf && gz0 - F < NAB))) {
 #pragma unroll
         for (int j = 0; j < 4; j++) {
@@ -987,31 +1033,31 @@ __device__ __forceinline__ void cpml_v3d_q4(const Grid &g, const Fields &f, int 
     if (gy - F < NAB) {
         i64 i = gx - F, j = gy - F;
         i64 q = (i * (2 * NAB) + j) * nz + k0;
-        cpml_q(f.psi[PSXY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], (int)j, sxy_y);
-        cpml_q(f.psi[PSYY_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, syy_y);
-        cpml_q(f.psi[PSYZ_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], (int)j, syz_y);
+        cpml_q(f.psi[PSXY_Y], q, f.kinv[1][0], f.cy[CA], f.cy[CB], (int)j, sxy_y);
+        cpml_q(f.psi[PSYY_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], (int)j, syy_y);
+        cpml_q(f.psi[PSYZ_Y], q, f.kinv[1][0], f.cy[CA], f.cy[CB], (int)j, syz_y);
     } else if (gy > NY - NAB - F - 1) {
         i64 i = gx - F, j = gy - NY + NAB + F + NAB;
         int ind = 2 * NAB - 1 - (int)j;
         i64 q = (i * (2 * NAB) + j) * nz + k0;
-        cpml_q(f.psi[PSXY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], ind + 1, sxy_y);
-        cpml_q(f.psi[PSYY_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, syy_y);
-        cpml_q(f.psi[PSYZ_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], ind + 1, syz_y);
+        cpml_q(f.psi[PSXY_Y], q, f.kinv[1][0], f.cy[CA], f.cy[CB], ind + 1, sxy_y);
+        cpml_q(f.psi[PSYY_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], ind, syy_y);
+        cpml_q(f.psi[PSYZ_Y], q, f.kinv[1][0], f.cy[CA], f.cy[CB], ind + 1, syz_y);
     }
     if (gx - F < NAB) {
         i64 i = gx - F, j = gy - F;
         i64 q = (i * ny + j) * nz + k0;
-        cpml_q(f.psi[PSXX_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, sxx_x);
-        cpml_q(f.psi[PSXY_X], q, f.cx[CK], f.cx[CA], f.cx[CB], (int)i, sxy_x);
-        cpml_q(f.psi[PSXZ_X], q, f.cx[CK], f.cx[CA], f.cx[CB], (int)i, sxz_x);
+        cpml_q(f.psi[PSXX_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], (int)i, sxx_x);
+        cpml_q(f.psi[PSXY_X], q, f.kinv[0][0], f.cx[CA], f.cx[CB], (int)i, sxy_x);
+        cpml_q(f.psi[PSXZ_X], q, f.kinv[0][0], f.cx[CA], f.cx[CB], (int)i, sxz_x);
     }
     if (gx > NX - NAB - F - 1) {
         i64 i = gx - NX + NAB + F + NAB, j = gy - F;
         int ind = 2 * NAB - 1 - (int)i;
         i64 q = (i * ny + j) * nz + k0;
-        cpml_q(f.psi[PSXX_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, sxx_x);
-        cpml_q(f.psi[PSXY_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, sxy_x);
-        cpml_q(f.psi[PSXZ_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, sxz_x);
+        cpml_q(f.psi[PSXX_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], ind, sxx_x);
+        cpml_q(f.psi[PSXY_X], q, f.kinv[0][0], f.cx[CA], f.cx[CB], ind + 1, sxy_x);
+        cpml_q(f.psi[PSXZ_X], q, f.kinv[0][0], f.cx[CA], f.cx[CB], ind + 1, sxz_x);
     }
 }
 
@@ -1319,6 +1365,37 @@ __device__ __forceinline__ void cpml_s3d_q4(const Grid &g, const Fields &f, int 
 {
     const int F = g.F, NAB = g.nab, NZ = g.NZ, NY = g.NY, NX = g.NX;
     const i64 nz = g.nz, ny = g.ny;
+    if (cpml_slabs_apart(g)) {   // side-merged form, as in cpml_v3d_q4
+        const i64 k0 = gz0 - F;
+        const bool zhi = gz0 > NZ - NAB - F - 1, zlo = !g.freesurf && gz0 - F < NAB;
+        if (zhi || zlo) {
+            const int k = zhi ? gz0 - NZ + 2 * NAB + F : gz0 - F;
+            const int st = zhi ? -1 : 1, cf = zhi ? 2 * NAB - k : k, ch = zhi ? 2 * NAB - 1 - k : k;
+            const i64 q = ((i64)(gx - F) * ny + (gy - F)) * (2 * NAB) + k;
+            cpml_zq(f.psi[PVX_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], ch, st, vxz);
+            cpml_zq(f.psi[PVY_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], ch, st, vyz);
+            cpml_zq(f.psi[PVZ_Z], q, f.kinv[2][0], f.cz[CA], f.cz[CB], cf, st, vzz);
+        }
+        const bool ylo = gy - F < NAB, yhi = gy > NY - NAB - F - 1;
+        if (ylo || yhi) {
+            const int j = ylo ? gy - F : gy - NY + 2 * NAB + F;
+            const int cf = ylo ? j : 2 * NAB - j, ch = ylo ? j : 2 * NAB - 1 - j;
+            const i64 q = ((i64)(gx - F) * (2 * NAB) + j) * nz + k0;
+            cpml_q(f.psi[PVX_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], ch, vxy);
+            cpml_q(f.psi[PVY_Y], q, f.kinv[1][0], f.cy[CA], f.cy[CB], cf, vyy);
+            cpml_q(f.psi[PVZ_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], ch, vzy);
+        }
+        const bool xlo = gx - F < NAB, xhi = gx > NX - NAB - F - 1;
+        if (xlo || xhi) {
+            const int i = xlo ? gx - F : gx - NX + 2 * NAB + F;
+            const int cf = xlo ? i : 2 * NAB - i, ch = xlo ? i : 2 * NAB - 1 - i;
+            const i64 q = ((i64)i * ny + (gy - F)) * nz + k0;
+            cpml_q(f.psi[PVX_X], q, f.kinv[0][0], f.cx[CA], f.cx[CB], cf, vxx);
+            cpml_q(f.psi[PVY_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], ch, vyx);
+            cpml_q(f.psi[PVZ_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], ch, vzx);
+        }
+        return;
+    }
     // with NAB % 4 == 0 a quad lies in at most one z slab, entirely (the two
     // plain ifs of cpml_s3d can only both hold when the slabs overlap, which
     // needs nz < 2 NAB + 4 and takes the per-cell path)
@@ -1327,15 +1404,15 @@ __device__ __forceinline__ void cpml_s3d_q4(const Grid &g, const Fields &f, int 
         i64 i = gx - F, jj = gy - F, k = gz0 - NZ + NAB + F + NAB;
         int ind = 2 * NAB - 1 - (int)k;
         i64 q = (i * ny + jj) * (2 * NAB) + k;
-        cpml_zq(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, -1, vxz);
-        cpml_zq(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, -1, vyz);
-        cpml_zq(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, -1, vzz);
+        cpml_zq(f.psi[PVX_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], ind, -1, vxz);
+        cpml_zq(f.psi[PVY_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], ind, -1, vyz);
+        cpml_zq(f.psi[PVZ_Z], q, f.kinv[2][0], f.cz[CA], f.cz[CB], ind + 1, -1, vzz);
     } else if (zq && !g.freesurf && gz0 - F < NAB) {
         i64 i = gx - F, jj = gy - F, k = gz0 - F;
         i64 q = (i * ny + jj) * (2 * NAB) + k;
-        cpml_zq(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, 1, vxz);
-        cpml_zq(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, 1, vyz);
-        cpml_zq(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, 1, vzz);
+        cpml_zq(f.psi[PVX_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], (int)k, 1, vxz);
+        cpml_zq(f.psi[PVY_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], (int)k, 1, vyz);
+        cpml_zq(f.psi[PVZ_Z], q, f.kinv[2][0], f.cz[CA], f.cz[CB], (int)k, 1, vzz);
     } else if (!zq && (gz0 + 3 > NZ - NAB - F - 1 || (!g.freesurf && gz0 - F < NAB))) {
 #pragma unroll
         for (int j = 0; j < 4; j++) {
@@ -1361,32 +1438,32 @@ __device__ __forceinline__ void cpml_s3d_q4(const Grid &g, const Fields &f, int 
     if (gy - F < NAB) {
         i64 i = gx - F, j = gy - F;
         i64 q = (i * (2 * NAB) + j) * nz + k0;
-        cpml_q(f.psi[PVX_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, vxy);
-        cpml_q(f.psi[PVY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], (int)j, vyy);
-        cpml_q(f.psi[PVZ_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, vzy);
+        cpml_q(f.psi[PVX_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], (int)j, vxy);
+        cpml_q(f.psi[PVY_Y], q, f.kinv[1][0], f.cy[CA], f.cy[CB], (int)j, vyy);
+        cpml_q(f.psi[PVZ_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], (int)j, vzy);
     }
     if (gy > NY - NAB - F - 1) {
         i64 i = gx - F, j = gy - NY + NAB + F + NAB;
         int ind = 2 * NAB - 1 - (int)j;
         i64 q = (i * (2 * NAB) + j) * nz + k0;
-        cpml_q(f.psi[PVX_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, vxy);
-        cpml_q(f.psi[PVY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], ind + 1, vyy);
-        cpml_q(f.psi[PVZ_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, vzy);
+        cpml_q(f.psi[PVX_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], ind, vxy);
+        cpml_q(f.psi[PVY_Y], q, f.kinv[1][0], f.cy[CA], f.cy[CB], ind + 1, vyy);
+        cpml_q(f.psi[PVZ_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], ind, vzy);
     }
     if (gx - F < NAB) {
         i64 i = gx - F, j = gy - F;
         i64 q = (i * ny + j) * nz + k0;
-        cpml_q(f.psi[PVX_X], q, f.cx[CK], f.cx[CA], f.cx[CB], (int)i, vxx);
-        cpml_q(f.psi[PVY_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, vyx);
-        cpml_q(f.psi[PVZ_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, vzx);
+        cpml_q(f.psi[PVX_X], q, f.kinv[0][0], f.cx[CA], f.cx[CB], (int)i, vxx);
+        cpml_q(f.psi[PVY_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], (int)i, vyx);
+        cpml_q(f.psi[PVZ_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], (int)i, vzx);
     }
     if (gx > NX - NAB - F - 1) {
         i64 i = gx - NX + NAB + F + NAB, j = gy - F;
         int ind = 2 * NAB - 1 - (int)i;
         i64 q = (i * ny + j) * nz + k0;
-        cpml_q(f.psi[PVX_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, vxx);
-        cpml_q(f.psi[PVY_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, vyx);
-        cpml_q(f.psi[PVZ_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, vzx);
+        cpml_q(f.psi[PVX_X], q, f.kinv[0][0], f.cx[CA], f.cx[CB], ind + 1, vxx);
+        cpml_q(f.psi[PVY_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], ind, vyx);
+        cpml_q(f.psi[PVZ_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], ind, vzx);
     }
 }
 
@@ -1905,15 +1982,15 @@ __device__ __forceinline__ void cpml_s3d_adj_q4(const Grid &g, const Fields &f, 
         i64 i = gx - F, jj = gy - F, k = gz0 - NZ + NAB + F + NAB;
         int ind = 2 * NAB - 1 - (int)k;
         i64 q = (i * ny + jj) * (2 * NAB) + k;
-        cpml_zq(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, -1, vxz);
-        cpml_zq(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], ind, -1, vyz);
-        cpml_zq(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], ind + 1, -1, vzz);
+        cpml_zq(f.psi[PVX_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], ind, -1, vxz);
+        cpml_zq(f.psi[PVY_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], ind, -1, vyz);
+        cpml_zq(f.psi[PVZ_Z], q, f.kinv[2][0], f.cz[CA], f.cz[CB], ind + 1, -1, vzz);
     } else if (zq && !g.freesurf && gz0 - F < NAB) {
         i64 i = gx - F, jj = gy - F, k = gz0 - F;
         i64 q = (i * ny + jj) * (2 * NAB) + k;
-        cpml_zq(f.psi[PVX_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, 1, vxz);
-        cpml_zq(f.psi[PVY_Z], q, f.cz[CKH], f.cz[CAH], f.cz[CBH], (int)k, 1, vyz);
-        cpml_zq(f.psi[PVZ_Z], q, f.cz[CK], f.cz[CA], f.cz[CB], (int)k, 1, vzz);
+        cpml_zq(f.psi[PVX_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], (int)k, 1, vxz);
+        cpml_zq(f.psi[PVY_Z], q, f.kinv[2][1], f.cz[CAH], f.cz[CBH], (int)k, 1, vyz);
+        cpml_zq(f.psi[PVZ_Z], q, f.kinv[2][0], f.cz[CA], f.cz[CB], (int)k, 1, vzz);
     } else if (!zq && (gz0 + 3 > NZ - NAB - F - 1 || (!g.freesurf && gz0 - F < NAB))) {
 #pragma unroll
         for (int j = 0; j < 4; j++) {
@@ -1939,31 +2016,31 @@ __device__ __forceinline__ void cpml_s3d_adj_q4(const Grid &g, const Fields &f, 
     if (gy - F < NAB) {
         i64 i = gx - F, j = gy - F;
         i64 q = (i * (2 * NAB) + j) * nz + k0;
-        cpml_q(f.psi[PVX_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, vxy);
-        cpml_q(f.psi[PVY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], (int)j, vyy);
-        cpml_q(f.psi[PVZ_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], (int)j, vzy);
+        cpml_q(f.psi[PVX_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], (int)j, vxy);
+        cpml_q(f.psi[PVY_Y], q, f.kinv[1][0], f.cy[CA], f.cy[CB], (int)j, vyy);
+        cpml_q(f.psi[PVZ_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], (int)j, vzy);
     } else if (gy > NY - NAB - F - 1) {
         i64 i = gx - F, j = gy - NY + NAB + F + NAB;
         int ind = 2 * NAB - 1 - (int)j;
         i64 q = (i * (2 * NAB) + j) * nz + k0;
-        cpml_q(f.psi[PVX_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, vxy);
-        cpml_q(f.psi[PVY_Y], q, f.cy[CK], f.cy[CA], f.cy[CB], ind + 1, vyy);
-        cpml_q(f.psi[PVZ_Y], q, f.cy[CKH], f.cy[CAH], f.cy[CBH], ind, vzy);
+        cpml_q(f.psi[PVX_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], ind, vxy);
+        cpml_q(f.psi[PVY_Y], q, f.kinv[1][0], f.cy[CA], f.cy[CB], ind + 1, vyy);
+        cpml_q(f.psi[PVZ_Y], q, f.kinv[1][1], f.cy[CAH], f.cy[CBH], ind, vzy);
     }
     if (gx - F < NAB) {
         i64 i = gx - F, j = gy - F;
         i64 q = (i * ny + j) * nz + k0;
-        cpml_q(f.psi[PVX_X], q, f.cx[CK], f.cx[CA], f.cx[CB], (int)i, vxx);
-        cpml_q(f.psi[PVY_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, vyx);
-        cpml_q(f.psi[PVZ_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], (int)i, vzx);
+        cpml_q(f.psi[PVX_X], q, f.kinv[0][0], f.cx[CA], f.cx[CB], (int)i, vxx);
+        cpml_q(f.psi[PVY_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], (int)i, vyx);
+        cpml_q(f.psi[PVZ_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], (int)i, vzx);
     }
     if (gx > NX - NAB - F - 1) {
         i64 i = gx - NX + NAB + F + NAB, j = gy - F;
         int ind = 2 * NAB - 1 - (int)i;
         i64 q = (i * ny + j) * nz + k0;
-        cpml_q(f.psi[PVX_X], q, f.cx[CK], f.cx[CA], f.cx[CB], ind + 1, vxx);
-        cpml_q(f.psi[PVY_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, vyx);
-        cpml_q(f.psi[PVZ_X], q, f.cx[CKH], f.cx[CAH], f.cx[CBH], ind, vzx);
+        cpml_q(f.psi[PVX_X], q, f.kinv[0][0], f.cx[CA], f.cx[CB], ind + 1, vxx);
+        cpml_q(f.psi[PVY_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], ind, vyx);
+        cpml_q(f.psi[PVZ_X], q, f.kinv[0][1], f.cx[CAH], f.cx[CBH], ind, vzx);
     }
 }
 
@@ -2372,20 +2449,20 @@ __global__ void k_surf3d(Grid g, Fields f, int pdir)
         i64 nz = g.nz, ny = g.ny;
         if (gy - F < NAB) {
             i64 i = gx - F, j = gy - F;
-            vyy = vyy / f.cy[CK][j] + f.psi[PVY_Y][(i * (2 * NAB) + j) * nz];
+            vyy = vyy * f.kinv[1][0][j] + f.psi[PVY_Y][(i * (2 * NAB) + j) * nz];
         } else if (gy > g.NY - NAB - F - 1) {
             i64 i = gx - F, j = gy - g.NY + NAB + F + NAB;
             int ind = 2 * NAB - 1 - (int)j;
-            vyy = vyy / f.cy[CK][ind + 1] + f.psi[PVY_Y][(i * (2 * NAB) + j) * nz];
+            vyy = vyy * f.kinv[1][0][ind + 1] + f.psi[PVY_Y][(i * (2 * NAB) + j) * nz];
         }
         if (gx - F < NAB) {
             i64 i = gx - F, j = gy - F;
-            vxx = vxx / f.cx[CK][i] + f.psi[PVX_X][(i * ny + j) * nz];
+            vxx = vxx * f.kinv[0][0][i] + f.psi[PVX_X][(i * ny + j) * nz];
         }
         if (gx > g.NX - NAB - F - 1) {
             i64 i = gx - g.NX + NAB + F + NAB, j = gy - F;
             int ind = 2 * NAB - 1 - (int)i;
-            vxx = vxx / f.cx[CK][ind + 1] + f.psi[PVX_X][(i * ny + j) * nz];
+            vxx = vxx * f.kinv[0][0][ind + 1] + f.psi[PVX_X][(i * ny + j) * nz];
         }
     }
     if (L == 0) {
@@ -3290,10 +3367,11 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
     }
     if (g.nd == 3) {
         if ((g.kernels == 0 || g.kernels == 5) && q4_ok(g)) {
-            // 8 quads (32 z cells) x 4 y x 4 x per CTA: the y and x stencil
-            // rows of neighbouring threads share L1 lines (0.35 ms at 256^3,
-            // against 0.39 for 32 x 2 x 2)
-            dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4) * g.nb);
+            // 16 quads (64 z cells) x 4 y x 2 x per CTA: the y and x stencil
+            // rows of neighbouring threads share L1 lines.  Interior-only
+            // timing at 256^3 on a B200: 0.268 ms, against 0.275 for 8 x 4 x
+            // 4, 0.284 for 8 x 2 x 8 and 0.34 for 4 x 8 x 4 quads x y x x
+            dim3 b(16, 4, 2), gr(cdiv(g.nz / 4, 16), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
             if (g.nb > 1) k_v3d_q4<float, true><<<gr, b, 0, st>>>(g, f);
             else k_v3d_q4_b4<<<gr, b, 0, st>>>(g, f);
             return;

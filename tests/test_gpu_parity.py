@@ -208,6 +208,10 @@ def test_vectorised_adjoint_matches_general(kw, cuda_device):
     assert plans["fast"].kernel_family == "vector"
     d = plans["general"].forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs, save_boundaries=True)
     plans["fast"].forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs, save_boundaries=True)
+    n = plans["fast"].nvol
+    # the forward fields at the last step: the scale of the reconstruction,
+    # which backpropagates them to ~0 at t = 0
+    scale = [float(np.linalg.norm(plans["general"].debug_array(0, i, n).astype(np.float64))) for i in range(9)]
     res = {k: (0.3 * v).astype(np.float32) for k, v in d.items()}
     g = {}
     for variant, plan in plans.items():
@@ -218,12 +222,21 @@ def test_vectorised_adjoint_matches_general(kw, cuda_device):
         ref = g["general"][k]
         assert np.abs(ref).max() > 0, k
         assert rel_l2(g["fast"][k], ref) < 2e-5, (k, rel_l2(g["fast"][k], ref))
-    n = plans["fast"].nvol
-    for kind, names in ((1, range(9)), (0, range(9))):
-        for i in names:
-            a = plans["fast"].debug_array(kind, i, n)
-            b = plans["general"].debug_array(kind, i, n)
-            assert rel_l2(a, b) < 2e-5, (kind, i)
+    for i in range(9):
+        a = plans["fast"].debug_array(1, i, n)
+        b = plans["general"].debug_array(1, i, n)
+        assert rel_l2(a, b) < 2e-5, ("adjoint", i)
+    for i in range(9):
+        # reconstructed forward fields, relative to their size before the
+        # backpropagation: the CPML multiplies by 1/K in the 4-cell kernels
+        # and divides by K in the one-cell ones, so the two runs differ by
+        # roundings, and the residual the reconstruction leaves at t = 0 is
+        # itself of rounding size
+        a = plans["fast"].debug_array(0, i, n).astype(np.float64)
+        b = plans["general"].debug_array(0, i, n).astype(np.float64)
+        assert scale[i] > 0
+        e = float(np.linalg.norm(a - b)) / max(float(np.linalg.norm(b)), scale[i])
+        assert e < 2e-5, ("reconstructed", i, e)
     if cfg["L"]:
         # the reference's viscoelastic backpropagation is unstable
         # (update_adjs2D.cl:232): rounding differences grow, so the
