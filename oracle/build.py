@@ -5,6 +5,10 @@ TEST INFRASTRUCTURE ONLY: the checker of the CUDA path, never the product.
 * ``build_port()`` compiles the C restatement (fdo_setup.c, fdo_port.c,
   fdo_driver.c) into ``oracle/_build/libfdo_port.so``.  It needs only gcc and
   runs anywhere, including the GPU box.
+* ``build_ref_gpu(cfg, hc)`` compiles the reference's 3D forward CUDA
+  kernels in place with nvcc for sm_100a (oracle/ref_gpu_tu.cu) into
+  ``oracle/_ref/libfdo_refgpu_<key>.so``: the reference's own GPU code, for
+  parity and timing beside this package's kernels (tests only).
 * ``build_ref(cfg)`` compiles the reference's own kernel sources *in place*
   from the reference tree (``SEISCL_REF_SRC``, else ``reference/src`` beside
   the repository) with the same -D constants the reference passes at run time
@@ -204,6 +208,50 @@ def build_ref(cfg: dict, nbnd: int, hc: list, speed: str = "pin") -> str:
         if speed == "native":
             with open(out + ".cpu.json", "w") as fh:
                 json.dump({"flags": sorted(cpu_flags())}, fh)
+        os.replace(tmp, out)
+    return out
+
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+# the reference's 3D forward kernels, compiled for the GPU: file, entry point
+GPU_KERNELS = [("update_v3D.cl", "update_v"), ("update_s3D.cl", "update_s"), ("surface3D.cl", "freesurface")]
+GPU_BLOCK = (32, 4, 4)   # src/Init_OpenCL.c:493-500 for 3D: 32 x FDORDER/2 x FDORDER/2 at order 8
+
+
+def ref_gpu_lib_path(cfg: dict) -> str:
+    return os.path.join(REF_OUT, "libfdo_refgpu_%s.so" % ref_key(cfg))
+
+
+def build_ref_gpu(cfg: dict, hc: list) -> str:
+    """Compile the reference's 3D forward CUDA kernels (update_v3D.cl,
+    update_s3D.cl, surface3D.cl) in place for sm_100a, as its CUDA build
+    compiles them with NVRTC (src/clprogram.c:449-571: the grid and physics
+    constants as -D options, LOCAL_OFF 0, cuda_fp16.h pre-included), one
+    translation unit per file (oracle/ref_gpu_tu.cu), into
+    oracle/_ref/libfdo_refgpu_<key>.so with a launcher per kernel.  Each
+    grid needs its own build; the update kernels need nz a multiple of 32
+    and ny, nx multiples of 4 (the launch covers the grid exactly)."""
+    out = ref_gpu_lib_path(cfg)
+    if os.path.exists(out):
+        return out
+    if cfg["nd"] != 3 or cfg["fdorder"] != 8:
+        raise ValueError("the GPU build covers the 3D 8th-order kernels")
+    if not ref_available():
+        raise FileNotFoundError("reference kernel sources not found at %s" % REF_SRC)
+    os.makedirs(REF_OUT, exist_ok=True)
+    defs = ref_defines(cfg, 0, hc)
+    arch = ["-gencode", "arch=compute_100a,code=sm_100a"]
+    with tempfile.TemporaryDirectory() as td:
+        objs = []
+        for fname, entry in GPU_KERNELS:
+            obj = os.path.join(td, entry + ".o")
+            _run([NVCC, *arch, "-O3", "-std=c++17", "-w", "-Xcompiler", "-fPIC", "-c", "-o", obj,
+                  os.path.join(HERE, "ref_gpu_tu.cu"), "-I" + HERE, "-I" + REF_SRC, *defs, "-DLOCAL_OFF=0",
+                  "-DREF_KERNEL_FILE=%s" % fname, "-D%s=ref_gpu_%s" % (entry, entry),
+                  "-DREF_ENTRY=ref_gpu_%s" % entry, "-DREF_LAUNCH=ref_gpu_launch_%s" % entry])
+            objs.append(obj)
+        tmp = out + ".tmp%d" % os.getpid()
+        _run([NVCC, *arch, "-shared", "-o", tmp, *objs, "-lcudart"])
         os.replace(tmp, out)
     return out
 

@@ -325,6 +325,17 @@ class Oracle:
 
     def array(self, kind: str, name: str) -> np.ndarray:
         """Copy of an internal array (for field-level comparisons)."""
+        a = self._view(kind, name)
+        return None if a is None else a.copy()
+
+    def set_array(self, kind: str, name: str, values) -> None:
+        """Overwrite an internal array (a state to step from)."""
+        a = self._view(kind, name)
+        if a is None:
+            raise KeyError("%s %s is not allocated" % (kind, name))
+        a[:] = np.asarray(values, a.dtype).ravel()
+
+    def _view(self, kind: str, name: str):
         c = self.cfg
         nab = c["nab"]
         if kind in ("wave", "adj"):
@@ -353,7 +364,7 @@ class Oracle:
         p = self.lib.fdo_array(self.h, k, i)
         if not p:
             return None
-        return np.ctypeslib.as_array(p, shape=(int(n),)).copy()
+        return np.ctypeslib.as_array(p, shape=(int(n),))
 
     def residual_scale(self, rec_pos, residuals: dict) -> dict:
         """Adjoint-source scaling of src/residuals.c:452-568 (res_scale,
