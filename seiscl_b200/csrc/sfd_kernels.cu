@@ -1681,7 +1681,7 @@ __device__ __forceinline__ void s_shear_q4(const Grid &g, const Fields &f, int g
 
 // stress update of the quad (gz0..gz0+3, gy, gx); LP: load policy of the
 // velocity reads; surf: free surface folded in (see s_normal_q4); PF: first
-// ask L2 for the quad's per-cell streams (FP32 fields)
+// ask L2 for the quad's per-cell streams
 template <int L, class T, int LP = 0, bool PF = false>
 __device__ __forceinline__ void s3d_q4_at(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip,
                                           bool surf = false)
@@ -1690,13 +1690,13 @@ __device__ __forceinline__ void s3d_q4_at(const Grid &g, const Fields &f, int gz
     const i64 sx = (i64)g.NY * g.NZ, sy = g.NZ;
     const float *hc = g.hc;
     if constexpr (PF) {
-        static_assert(std::is_same<T, float>::value, "stream prefetch of FP32 fields");
 #pragma unroll
-        for (int q = SXX; q <= SXZ; q++) asm volatile("prefetch.global.L2 [%0];" ::"l"(f.w[q] + iv));
+        for (int q = SXX; q <= SXZ; q++) asm volatile("prefetch.global.L2 [%0];" ::"l"(fld<T>(f.w[q]) + iv));
 #pragma unroll
         for (int l = 0; l < L; l++)
 #pragma unroll
-            for (int q = 0; q < NR; q++) asm volatile("prefetch.global.L2 [%0];" ::"l"(f.r[q] + l * g.nvol + iv));
+            for (int q = 0; q < NR; q++)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(fld<T>(f.r[q]) + l * g.nvol + iv));
         constexpr int np = L > 0 ? 10 : 5;
         constexpr int pid[10] = {PM, PMU, PMUIPJP, PMUJPKP, PMUIPKP, PTAUP, PTAUS, PTAUSIPJP, PTAUSJPKP, PTAUSIPKP};
 #pragma unroll
@@ -1730,19 +1730,20 @@ __global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f, bool surf)
     s3d_q4_at<L, T, 0>(g, f, gz0, gy, gx, iv, ip, surf);
 }
 
-// Single-shot FP32 launches: each thread first asks L2 for its own per-cell
-// streams (prefetch.global.L2 of its stresses, memory variables and
-// parameters), so they are on their way while the velocity stencils load,
-// and the launch takes 3 CTAs per SM (168 registers) so that more stencil
-// loads stay in flight.  256^3, L=2, CPML 20 on a B200: 0.651 ms against
-// 0.695 for k_s3d_q4 (0.571 against 0.601 without absorbing boundary); the
-// prefetch at 4 CTAs per SM gave 0.674, 3 CTAs without it 0.713.
-template <int L>
+// Single-shot launches of the default selection: each thread first asks L2
+// for its own per-cell streams (prefetch.global.L2 of its stresses, memory
+// variables and parameters), so they are on their way while the velocity
+// stencils load, and the launch takes 3 CTAs per SM (168 registers) so that
+// more stencil loads stay in flight.  256^3, L=2, CPML 20, FP32 on a B200:
+// 0.651 ms against 0.695 for k_s3d_q4 (0.571 against 0.601 without
+// absorbing boundary); the prefetch at 4 CTAs per SM gave 0.674, 3 CTAs
+// without it 0.713.
+template <int L, class T>
 __global__ void __launch_bounds__(128, 3) k_s3d_q4_pf(Grid g, Fields f, bool surf)
 {
     constexpr bool MB = false;
     CELL3D_Q4
-    s3d_q4_at<L, float, 0, true>(g, f, gz0, gy, gx, iv, ip, surf);
+    s3d_q4_at<L, T, 0, true>(g, f, gz0, gy, gx, iv, ip, surf);
 }
 
 // ------------------------------------------------- fused 3D forward step
@@ -3422,6 +3423,15 @@ bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_
     if (g.fhalf && g.nd == 3 && g.L <= 3) {   // FP16 storage: the vectorised or the streaming kernels
         if (q4_ok(g)) {
             dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);
+            if (g.kernels == 0 && g.nb == 1) {   // with the stream prefetch, as the FP32 default
+                switch (g.L) {
+                case 0: k_s3d_q4_pf<0, __half><<<g4, b4, 0, st>>>(g, f, false); break;
+                case 1: k_s3d_q4_pf<1, __half><<<g4, b4, 0, st>>>(g, f, false); break;
+                case 2: k_s3d_q4_pf<2, __half><<<g4, b4, 0, st>>>(g, f, false); break;
+                default: k_s3d_q4_pf<3, __half><<<g4, b4, 0, st>>>(g, f, false); break;
+                }
+                return false;
+            }
             switch (g.L) {
             case 0: k_s3d_q4<0, __half><<<g4, b4, 0, st>>>(g, f, false); break;
             case 1: k_s3d_q4<1, __half><<<g4, b4, 0, st>>>(g, f, false); break;
@@ -3455,12 +3465,12 @@ bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
         if ((g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) {
             dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);  // 0.70 ms vs 0.71 (32 x 2 x 2)
-            if (g.nb == 1) {
+            if (g.nb == 1 && g.kernels == 0) {   // kernels 5 keeps k_s3d_q4 (no prefetch)
                 switch (g.L) {
-                case 0: k_s3d_q4_pf<0><<<g4, b4, 0, st>>>(g, f, surf); break;
-                case 1: k_s3d_q4_pf<1><<<g4, b4, 0, st>>>(g, f, surf); break;
-                case 2: k_s3d_q4_pf<2><<<g4, b4, 0, st>>>(g, f, surf); break;
-                default: k_s3d_q4_pf<3><<<g4, b4, 0, st>>>(g, f, surf); break;
+                case 0: k_s3d_q4_pf<0, float><<<g4, b4, 0, st>>>(g, f, surf); break;
+                case 1: k_s3d_q4_pf<1, float><<<g4, b4, 0, st>>>(g, f, surf); break;
+                case 2: k_s3d_q4_pf<2, float><<<g4, b4, 0, st>>>(g, f, surf); break;
+                default: k_s3d_q4_pf<3, float><<<g4, b4, 0, st>>>(g, f, surf); break;
                 }
                 return surf;
             }
