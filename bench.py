@@ -410,7 +410,8 @@ def run_gradient(args):
         shots = [(sp, src[:, :args.nt].copy(), rp) for sp, src, rp in shots]
     outs = w["outputs"]
     cfg = dataclasses.replace(engine_config(w), precision=w["precision"], batch=B,
-                              checkpoint=args.checkpoint)
+                              checkpoint=args.checkpoint,
+                              kernels=args.kernels if args.kernels in ("fast", "vector") else "fast")
     plan = Plan(cfg)
     plan.set_model(true["vp"], true["vs"], true["rho"])
     obs = []   # observed data, untimed

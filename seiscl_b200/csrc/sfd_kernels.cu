@@ -1931,11 +1931,28 @@ __device__ __forceinline__ void grad_add4(double *g, i64 ip, const float (&d)[4]
     p[1] = b;
 }
 
-template <typename T, bool MB = false>
-__global__ void __launch_bounds__(128) k_adjv3d_q4(Grid g, Fields f, AdjFields a)
+// L2 prefetch of one quad's cell in a per-cell stream
+__device__ __forceinline__ void pf_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// PF (single-shot launches of the default selection): the thread first asks
+// L2 for its quad's per-cell streams -- the forward and adjoint velocities,
+// the buoyancies and the density gradient sum -- and the launch takes 3 CTAs
+// per SM, as k_s3d_q4_pf does for the forward stress update.
+template <typename T, bool MB = false, bool PF = false>
+__global__ void __launch_bounds__(128, PF ? 3 : 1) k_adjv3d_q4(Grid g, Fields f, AdjFields a)
 {
     CELL3D_Q4
     if (MB) shot_adj(g, a, shot);
+    if constexpr (PF) {
+        const bool recon = !g.ckpt && !g.bp2;
+#pragma unroll
+        for (int q = VX; q <= VZ; q++) {
+            pf_l2(a.wr[q] + iv);
+            if (recon) pf_l2(f.w[q] + iv);
+        }
+        pf_l2(f.p[PRIP] + ip); pf_l2(f.p[PRJP] + ip); pf_l2(f.p[PRKP] + ip);
+        if (!g.bp2) pf_l2(a.grad[GRHO] + ip);
+    }
     const float *hc = g.hc;
     const Q4 rip = ldq(f.p[PRIP] + ip), rjp = ldq(f.p[PRJP] + ip), rkp = ldq(f.p[PRKP] + ip);
     Q4 vx = {{0, 0, 0, 0}}, vy = vx, vz = vx;
@@ -2074,11 +2091,43 @@ __device__ __forceinline__ void cpml_s3d_adj_q4(const Grid &g, const Fields &f, 
     }
 }
 
-template <int L, typename T, bool MB = false>
-__global__ void __launch_bounds__(128, 4) k_adjs3d_q4(Grid g, Fields f, AdjFields a)
+// PF: prefetch of the quad's per-cell streams (forward and adjoint stresses
+// and memory variables, parameters, the M and mu gradient sums) and 3 CTAs
+// per SM, as k_adjv3d_q4.  The saved-boundary index of each cell of the quad
+// is found once and kept for the four phases.
+template <int L, typename T, bool MB = false, bool PF = false>
+__global__ void __launch_bounds__(128, PF ? 3 : 4) k_adjs3d_q4(Grid g, Fields f, AdjFields a)
 {
     CELL3D_Q4
     if (MB) shot_adj(g, a, shot);
+    const bool recon = !g.ckpt && !g.bp2;
+    if constexpr (PF) {
+#pragma unroll
+        for (int q = SXX; q <= SXZ; q++) {
+            pf_l2(a.wr[q] + iv);
+            if (recon) pf_l2(f.w[q] + iv);
+        }
+#pragma unroll
+        for (int l = 0; l < L; l++)
+#pragma unroll
+            for (int q = 0; q < NR; q++) {
+                pf_l2(a.rr[q] + l * g.nvol + iv);
+                if (recon) pf_l2(f.r[q] + l * g.nvol + iv);
+            }
+        constexpr int np = L > 0 ? 10 : 5;
+        constexpr int pid[10] = {PM, PMU, PMUIPJP, PMUJPKP, PMUIPKP, PTAUP, PTAUS, PTAUSIPJP, PTAUSJPKP, PTAUSIPKP};
+#pragma unroll
+        for (int k = 0; k < np; k++) pf_l2(f.p[pid[k]] + ip);
+        if (!g.bp2) {
+            pf_l2(a.grad[GM] + ip);
+            if (g.restype == 0) pf_l2(a.grad[GMU] + ip);
+        }
+    }
+    int mq[4] = {-1, -1, -1, -1};
+    if (recon) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) mq[j] = inject_ind3d(g, gz0 + j, gy, gx);
+    }
     const float *hc = g.hc;
     // adjoint velocity derivatives, with CPML
     Q4 vzzr = dbw_z<F>(ldw(a.wr[VZ], iv), hc), vyzr = dfw_z<F>(ldw(a.wr[VY], iv), hc);
@@ -2157,7 +2206,7 @@ __global__ void __launch_bounds__(128, 4) k_adjs3d_q4(Grid g, Fields f, AdjField
                         s3[c].v[j] -= ls + g.dt2 * aa;
                     }
                 }
-                const int m = inject_ind3d(g, gz0 + j, gy, gx);
+                const int m = mq[j];
                 if (m != -1) {
                     s3[0].v[j] = bnd_at<T>(g, a, SXX, m);
                     s3[1].v[j] = bnd_at<T>(g, a, SYY, m);
@@ -2295,7 +2344,7 @@ __global__ void __launch_bounds__(128, 4) k_adjs3d_q4(Grid g, Fields f, AdjField
                     }
                     sc.v[j] -= ls + g.dt2 * aa;
                 }
-                const int m = inject_ind3d(g, gz0 + j, gy, gx);
+                const int m = mq[j];
                 if (m != -1) sc.v[j] = bnd_at<T>(g, a, wid, m);
             }
             stq(f.w[wid] + iv, sc);
@@ -3636,8 +3685,18 @@ template <typename T>
 static void launch_adj_t(const Grid &g, const Fields &f, const AdjFields &a, bool stress, cudaStream_t st)
 {
     if (g.nd == 3 && (g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) {
+        const bool pf = g.kernels == 0 && g.nb == 1;   // kernels 5 keeps the kernels without the prefetch
         if (stress) {
             dim3 b(16, 8, 1), gr(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);
+            if (pf) {
+                switch (g.L) {
+                case 0: k_adjs3d_q4<0, T, false, true><<<gr, b, 0, st>>>(g, f, a); break;
+                case 1: k_adjs3d_q4<1, T, false, true><<<gr, b, 0, st>>>(g, f, a); break;
+                case 2: k_adjs3d_q4<2, T, false, true><<<gr, b, 0, st>>>(g, f, a); break;
+                default: k_adjs3d_q4<3, T, false, true><<<gr, b, 0, st>>>(g, f, a); break;
+                }
+                return;
+            }
             switch (g.L) {
             case 0: MB_DISPATCH(g, k_adjs3d_q4<0, T, MBV><<<gr, b, 0, st>>>(g, f, a)) break;
             case 1: MB_DISPATCH(g, k_adjs3d_q4<1, T, MBV><<<gr, b, 0, st>>>(g, f, a)) break;
@@ -3646,6 +3705,10 @@ static void launch_adj_t(const Grid &g, const Fields &f, const AdjFields &a, boo
             }
         } else {
             dim3 b(8, 4, 4), gr(cdiv(g.nz / 4, 8), cdiv(g.ny, 4), cdiv(g.nx, 4) * g.nb);
+            if (pf) {
+                k_adjv3d_q4<T, false, true><<<gr, b, 0, st>>>(g, f, a);
+                return;
+            }
             MB_DISPATCH(g, k_adjv3d_q4<T, MBV><<<gr, b, 0, st>>>(g, f, a))
         }
         return;
