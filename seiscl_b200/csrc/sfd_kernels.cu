@@ -2785,10 +2785,17 @@ __global__ void k_savebnd(Grid g, Fields f, BndSlot b, i64 tofs)
     int i, j, k;
     if (!shell_cell(g, gid, i, j, k)) return;
     i64 iv = ((i64)i * g.NY + j) * g.NZ + k;
-    for (int q = 0; q < b.nfield; q++) {
-        int w = b.fields[q];
-        ((T *)b.p[w])[sh + tofs + gid] = from_f<T>(f.w[w][iv] * g.bsc[w]);
-    }
+    // every field index is a compile-time constant (a saved field has its
+    // store in b.p[w]): indexing the parameter structs with a run-time field
+    // id made each thread copy them to local memory (a 688-byte stack frame);
+    // all loads go out before the stores
+    float v[NW];
+#pragma unroll
+    for (int w = 0; w < NW; w++)
+        if (b.p[w]) v[w] = f.w[w][iv];
+#pragma unroll
+    for (int w = 0; w < NW; w++)
+        if (b.p[w]) ((T *)b.p[w])[sh + tofs + gid] = from_f<T>(v[w] * g.bsc[w]);
 }
 
 // ------------------------------------------------------- adjoint kernels 2D
