@@ -717,7 +717,7 @@ def main():
     fused_gbs = ab["fused"] / (step_ms / 1e3) / 1e9
     fam = plan.kernel_family
     fused = bool(plan.fused_step and kfused > 0)
-    vec_name = ("k_s3d_q4_pf<%d>" if args.kernels == "fast" else "k_s3d_q4<%d>") % w["L"]
+    vec_name = ("k_s3d_q4_pf<%d>" if args.kernels == "fast" and w["L"] > 0 else "k_s3d_q4<%d>") % w["L"]
     kname = {"vector": vec_name, "tma": "k_tma<1,%d,*>" % w["L"],
              "stream": "k_s3d_stream<4,%d%s>" % (w["L"], ",half" if args.fields == "fp16" else ""),
              "register": "k_s3d_fast", "general": "k_s3d", "2d": "k_s2d"}[fam]

@@ -3411,6 +3411,21 @@ __global__ void k_residuals(AdjFields a, PointSet r, const float *res, int nt_to
 // ------------------------------------------------------------- launchers
 static inline unsigned cdiv(long a, long b) { return (unsigned)((a + b - 1) / b); }
 
+// CTA shape (quads x y rows x x planes) of a 4-cell launch: the preferred
+// shape, or half as many quads along z and twice the rows when that leaves
+// fewer threads without a quad (nz = 200: 50 quads per column fill 56 slots
+// of 8 instead of 64 of 16)
+static dim3 q4_block(const Grid &g, unsigned bx, unsigned by, unsigned bz)
+{
+    const unsigned nq = (unsigned)(g.nz / 4);
+    if (bx >= 16 && cdiv(nq, bx / 2) * (bx / 2) < cdiv(nq, bx) * bx) return dim3(bx / 2, by * 2, bz);
+    return dim3(bx, by, bz);
+}
+static dim3 q4_grid(const Grid &g, dim3 b)
+{
+    return dim3(cdiv(g.nz / 4, b.x), cdiv(g.ny, b.y), cdiv(g.nx, b.z) * g.nb);
+}
+
 // batched launches (several shots) use the MB = true instantiations
 #define MB_DISPATCH(g, ...)                                                     \
     if ((g).nb > 1) { constexpr bool MBV = true; __VA_ARGS__; }                  \
@@ -3457,7 +3472,7 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
             // rows of neighbouring threads share L1 lines.  Interior-only
             // timing at 256^3 on a B200: 0.268 ms, against 0.275 for 8 x 4 x
             // 4, 0.284 for 8 x 2 x 8 and 0.34 for 4 x 8 x 4 quads x y x x
-            dim3 b(16, 4, 2), gr(cdiv(g.nz / 4, 16), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
+            const dim3 b = q4_block(g, 16, 4, 2), gr = q4_grid(g, b);
             if (g.nb > 1) k_v3d_q4<float, true><<<gr, b, 0, st>>>(g, f);
             else k_v3d_q4_b4<<<gr, b, 0, st>>>(g, f);
             return;
@@ -3478,8 +3493,8 @@ bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_
 {
     if (g.fhalf && g.nd == 3 && g.L <= 3) {   // FP16 storage: the vectorised or the streaming kernels
         if (q4_ok(g)) {
-            dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);
-            if (g.kernels == 0 && g.nb == 1) {   // with the stream prefetch, as the FP32 default
+            const dim3 b4 = q4_block(g, 16, 8, 1), g4 = q4_grid(g, b4);
+            if (g.kernels == 0 && g.nb == 1 && g.L > 0) {   // with the stream prefetch, as the FP32 default
                 switch (g.L) {
                 case 0: k_s3d_q4_pf<0, __half><<<g4, b4, 0, st>>>(g, f, false); break;
                 case 1: k_s3d_q4_pf<1, __half><<<g4, b4, 0, st>>>(g, f, false); break;
@@ -3520,8 +3535,11 @@ bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_
     if (g.nd == 3) {
         dim3 b(32, 4, 2), gr(cdiv(g.nz, 32), cdiv(g.ny, 4), cdiv(g.nx, 2) * g.nb);
         if ((g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) {
-            dim3 b4(16, 8, 1), g4(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);  // 0.70 ms vs 0.71 (32 x 2 x 2)
-            if (g.nb == 1 && g.kernels == 0) {   // kernels 5 keeps k_s3d_q4 (no prefetch)
+            const dim3 b4 = q4_block(g, 16, 8, 1), g4 = q4_grid(g, b4);  // 0.70 ms vs 0.71 (32 x 2 x 2)
+            // the stream prefetch pays where memory variables add per-cell
+            // streams: 256^3, L=2: 0.654 ms against 0.706; elastic (L=0):
+            // 0.376 against 0.366 without it.  kernels 5 keeps k_s3d_q4.
+            if (g.nb == 1 && g.kernels == 0 && g.L > 0) {
                 switch (g.L) {
                 case 0: k_s3d_q4_pf<0, float><<<g4, b4, 0, st>>>(g, f, surf); break;
                 case 1: k_s3d_q4_pf<1, float><<<g4, b4, 0, st>>>(g, f, surf); break;
@@ -3694,7 +3712,7 @@ static void launch_adj_t(const Grid &g, const Fields &f, const AdjFields &a, boo
     if (g.nd == 3 && (g.kernels == 0 || g.kernels == 5) && q4_ok(g) && g.L <= 3) {
         const bool pf = g.kernels == 0 && g.nb == 1;   // kernels 5 keeps the kernels without the prefetch
         if (stress) {
-            dim3 b(16, 8, 1), gr(cdiv(g.nz / 4, 16), cdiv(g.ny, 8), cdiv(g.nx, 1) * g.nb);
+            const dim3 b = q4_block(g, 16, 8, 1), gr = q4_grid(g, b);
             if (pf) {
                 switch (g.L) {
                 case 0: k_adjs3d_q4<0, T, false, true><<<gr, b, 0, st>>>(g, f, a); break;
