@@ -470,7 +470,8 @@ def serving_requests(nreq, seed=501):
     elastic or viscoelastic (L 1-3); FD order 4 or 8; NT 500-1500; 1-8 Ricker
     shots at 5-20 Hz, 64 receivers; +-10 % random models.  Acoustic gradient
     requests run as P-SV with vs = 0, the reference's route (the reference's
-    acoustic kernels have no adjoint)."""
+    acoustic kernels have no adjoint); acoustic requests have no free
+    surface, elastic and viscoelastic ones do."""
     from seiscl_b200 import serving
     from seiscl_b200.engine import Config
     from seiscl_b200.qfit import band_frequencies, q_to_tau
@@ -493,8 +494,10 @@ def serving_requests(nreq, seed=501):
             N, shape = [nz, nx], (nx, nz)
         nd = 3 if three else (22 if physics == "acoustic" and kind == "forward" else 2)
         fl = band_frequencies(L, 0.5 * f0, 2.5 * f0) if L else [f0]
+        # acoustic media have no free surface: the reference's free-surface
+        # adjoint divides by mu, which is zero there
         cfg = Config(N=N, ND=nd, dh=10.0, dt=8e-4, NT=nt, L=L, f0=f0, FL=fl, FDORDER=order,
-                     freesurf=0 if nd == 22 else 1, nab=16)
+                     freesurf=0 if physics == "acoustic" else 1, nab=16)
         vp = np.full(shape, 3000.0, np.float32) * (1 + 0.1 * rng.uniform(-1, 1, shape)).astype(np.float32)
         vs = np.zeros(shape, np.float32) if physics == "acoustic" else (vp / 1.8).astype(np.float32)
         m = {"vp": vp, "vs": None if nd == 22 else vs, "rho": np.full(shape, 2000.0, np.float32)}

@@ -1112,6 +1112,15 @@ extern "C" int sfd_set_model(sfd_plan *p, const float *const *params)
         }
         p->bshift = n ? (int)std::lround(acc / n) : 0;
     }
+    {
+        // the free-surface adjoint forms C^-1 at the top row with the factor
+        // 1 / (4 M mu - 4 mu^2) in 2D and 1 / (6 M mu - 8 mu^2) in 3D
+        // (surface2D_adj.cl, surface3D_adj.cl): undefined where mu = 0
+        p->surf_mu_zero = false;
+        const int64_t ncol = (int64_t)p->g.ny * p->g.nx;
+        for (int64_t c = 0; c < ncol && !p->surf_mu_zero; c++)
+            if (!(p->hp[PMU][c * p->g.nz] > 0.0f)) p->surf_mu_zero = true;
+    }
     if (p->g.fhalf) {
         // FP16 wave fields: the moduli carry 2^-kshift and the buoyancies
         // 2^kshift (exact power-of-two scalings of the FP32 parameters).
@@ -1378,6 +1387,9 @@ extern "C" int sfd_adjoint_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     if (p->g.fhalf) return fail(p, SFD_ERR_UNSUPPORTED, "FP16 wave-field storage covers forward modelling only");
     if (!p->have_forward) return fail(p, SFD_ERR_STATE, "sfd_adjoint needs a preceding sfd_forward with saved boundaries");
     if (nshot != p->fwd_nb) return fail(p, SFD_ERR_STATE, "the adjoint must follow a forward run of the same shots");
+    if (p->g.freesurf && p->surf_mu_zero)
+        return fail(p, SFD_ERR_UNSUPPORTED, "the free-surface adjoint divides by mu, which is zero at the surface "
+                                            "(acoustic media: use a plan without a free surface)");
     if ((rc = check_outsel(p, outsel))) return rc;
     if ((rc = alloc_adjoint(p))) return rc;
     cudaStream_t st = stream ? (cudaStream_t)stream : p->stream;

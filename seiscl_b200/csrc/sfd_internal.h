@@ -172,6 +172,7 @@ struct sfd_plan {
     cudaEvent_t ev0, ev1;
     int kshift;             // FP16 storage: log2 ratio of velocity to stress scales
     int bshift;             // the same ratio for FP16 saved boundaries (set whatever the storage)
+    bool surf_mu_zero;      // mu is zero somewhere on the top row (the free-surface adjoint is undefined)
     float last_ms;
     // DFT gradient (back_prop_type 2, src/assign_modeling_case.c:549-570)
     int nfreqs, dtnyq, ntnyq;

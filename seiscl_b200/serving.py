@@ -76,6 +76,9 @@ def _key(cfg: engine.Config):
     return tuple((f.name, repr(getattr(cfg, f.name))) for f in dataclasses.fields(cfg))
 
 
+CHECKPOINT_STEPS = 50   # snapshot interval of viscoelastic gradient requests
+
+
 def plan_config(req: Request, max_batch: int = 8, batch_bytes: int = 24 << 30) -> engine.Config:
     """The configuration of the plans serving ``req``: several shots of a
     request advance together in one plan (``batch``: up to ``max_batch``
@@ -84,8 +87,13 @@ def plan_config(req: Request, max_batch: int = 8, batch_bytes: int = 24 << 30) -
     request alone."""
     c = req.config
     n = len(req.shots)
+    if req.kind == "gradient" and c.L > 0 and c.ND in (2, 3) and c.back_prop_type != 2 and not c.checkpoint:
+        # with memory variables the backpropagation from saved boundaries
+        # (the reference's BACK_PROP_TYPE 1) is unstable over long runs: the
+        # forward field is recomputed from snapshots instead, one shot per launch
+        return dataclasses.replace(c, checkpoint=CHECKPOINT_STEPS)
     ok = (c.ND in (2, 3) or (c.ND == 22 and req.kind == "forward")) and c.back_prop_type != 2 and \
-        c.field_precision == "fp32" and c.kernels in ("fast", "general", "stream", "vector")
+        c.field_precision == "fp32" and c.kernels in ("fast", "general", "stream", "vector") and not c.checkpoint
     if n < 2 or max_batch < 2 or not ok:
         return c
     b = min(n, max_batch)
@@ -192,6 +200,11 @@ def serve(plans, req: Request) -> Result:
         else:   # the chain rule is linear in the accumulated kernels: sum in slot order
             grad = {name: np.sum([g[name].astype(np.float64) for g in grads], axis=0).astype(np.float32)
                     for name in grads[0]}
+        vs = m.get("vs")
+        if vs is not None and not np.any(vs):
+            # acoustic media run as P-SV with vs = 0: the vs gradient carries
+            # 1 / mu^2 and is undefined; vp and rho are the acoustic gradient
+            grad.pop("vs", None)
     return Result(req.rid, seis, grad, float(sum(misfits)), 0.0, 0.0, 0.0)
 
 

@@ -339,3 +339,64 @@ def test_concurrent_requests_are_deterministic(cuda_device):
         if ref.gradient is not None:
             for k in ref.gradient:
                 assert np.array_equal(r.gradient[k], ref.gradient[k]), (i, k)
+
+
+def _grad_request(cfg, model, acq, nshots=3):
+    from seiscl_b200.serving import Request
+
+    shots = [(acq["src_pos"], acq["src"], acq["rec_pos"])] * nshots
+    nrec, nt = acq["rec_pos"].shape[0], cfg.NT
+    obs = [{"vx": np.zeros((nrec, nt), np.float32), "vz": np.zeros((nrec, nt), np.float32)} for _ in shots]
+    return Request(cfg, model, shots, ("vx", "vz"), "gradient", obs)
+
+
+def test_viscoelastic_gradient_requests_recompute_from_snapshots():
+    """Gradient requests with memory variables run the snapshot-checkpoint
+    recompute, one shot per launch (the reference's backpropagation of
+    memory variables is unstable over long runs); elastic ones batch."""
+    from seiscl_b200.serving import CHECKPOINT_STEPS, plan_config
+
+    cfg, model, acq = make_case(nd=2, L=2, nt=60, seed=8)
+    c = plan_config(_grad_request(engine_config(cfg), model, acq))
+    assert c.checkpoint == CHECKPOINT_STEPS and c.batch in (0, 1)
+    cfg, model, acq = make_case(nd=2, L=0, nt=60, seed=8)
+    c = plan_config(_grad_request(engine_config(cfg), model, acq))
+    assert not c.checkpoint and c.batch == 3
+
+
+@pytest.mark.gpu
+def test_viscoelastic_gradient_request_stays_finite(cuda_device):
+    """A 2D viscoelastic gradient request of 1200 steps through the service:
+    finite gradients (the boundary-saving backpropagation of the memory
+    variables can overflow on runs this long)."""
+    from seiscl_b200.serving import serve_alone
+
+    cfg, model, acq = make_case(nd=2, L=2, nt=1200, nz=60, nx=80, nab=10, seed=9)
+    r = serve_alone(_grad_request(engine_config(cfg), model, acq, nshots=2))
+    assert set(r.gradient) >= {"vp", "vs", "rho"}
+    for k, v in r.gradient.items():
+        assert np.isfinite(v).all(), k
+        assert np.abs(v).max() > 0, k
+
+
+@pytest.mark.gpu
+def test_acoustic_gradients(cuda_device):
+    """Acoustic media (P-SV with vs = 0): with a free surface the adjoint is
+    refused with a message (the free-surface adjoint divides by mu); without
+    one the service returns finite vp and rho gradients and no vs gradient."""
+    from seiscl_b200.engine import Plan, SeisCLEngineError
+    from seiscl_b200.serving import serve_alone
+
+    cfg, model, acq = make_case(nd=2, L=0, nt=150, seed=10)
+    model = dict(model, vs=np.zeros_like(model["vs"]))
+    plan = Plan(engine_config(cfg))
+    plan.set_model(model["vp"], model["vs"], model["rho"])
+    d = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], ["vx", "vz"], save_boundaries=True)
+    with pytest.raises(SeisCLEngineError, match="free-surface adjoint"):
+        plan.adjoint(acq["src_pos"], acq["src"], acq["rec_pos"], d)
+    plan.close()
+    cfg0 = dataclasses.replace(engine_config(cfg), freesurf=0)
+    r = serve_alone(_grad_request(cfg0, model, acq, nshots=2))
+    assert "vs" not in r.gradient
+    for k in ("vp", "rho"):
+        assert np.isfinite(r.gradient[k]).all() and np.abs(r.gradient[k]).max() > 0, k
