@@ -200,7 +200,9 @@ int sfd_forward(sfd_plan *plan, const sfd_shot *shot, int srctype_mask, const in
  * With back_prop_type 2 the adjoint runs from zeroed fields without
  * reconstructing the forward field (src/time_stepping.c:862-972), its
  * transforms are taken at the forward's sampling times, and the shot's
- * gradient is assembled from both (calc_grad, src/calc_grad.c:376-960). */
+ * gradient is assembled from both (calc_grad, src/calc_grad.c:376-960).
+ * Returns SFD_ERR_UNSUPPORTED for a plan with a free surface whose model has
+ * mu = 0 on the top row (the free-surface adjoint divides by mu there). */
 int sfd_adjoint(sfd_plan *plan, const sfd_shot *shot, int srctype_mask, const int *outsel,
                 const float *const *residuals, void *stream);
 
