@@ -54,12 +54,15 @@ GRADIENT_WORKLOADS = {
 }
 
 
-def build_gradient_workload(name, nshots):
+def build_gradient_workload(name, nshots, grid=0):
     """Seeded true and starting models and ``nshots`` shots (the workload's
-    shot positions, repeated when more are asked for)."""
+    shot positions, repeated when more are asked for); grid > 0 replaces a 3D
+    workload's grid with grid^3 cells (profiling runs)."""
     from scipy.ndimage import gaussian_filter
 
     w = dict(GRADIENT_WORKLOADS[name])
+    if grid > 0 and w["nd"] == 3:
+        w["nz"] = w["ny"] = w["nx"] = int(grid)
     w["fl"] = [w["f0"]]
     nd, nz, ny, nx, dh = w["nd"], w["nz"], w["ny"], w["nx"], w["dh"]
     z = np.arange(nz, dtype=np.float64)
@@ -97,7 +100,8 @@ def build_gradient_workload(name, nshots):
             vp *= 1.0 + 0.08 * (1 if k % 2 == 0 else -1) * np.exp(
                 -((xx - c[0]) ** 2 + (yy - c[1]) ** 2 + (zz - c[2]) ** 2) / (2 * 15.0 ** 2))
         vs = vp / 1.8
-        g = np.arange(100) * 4 + (nx - 400) // 2 + 2
+        nr = 100 if min(nx, ny) >= 400 else min(100, (min(nx, ny) - 3) // 4 + 1)   # smaller grids: what fits
+        g = np.arange(nr) * 4 + (min(nx, ny) - 4 * nr) // 2 + 2
         gxx, gyy = np.meshgrid(g, g, indexing="ij")
         shots = []
         for i in range(nshots):
@@ -404,7 +408,7 @@ def run_gradient(args):
     if args.checkpoint:
         B = 1   # checkpointed gradients run one shot per launch
     nuse = (args.warmup + args.steps) * B
-    w, true, start, shots = build_gradient_workload(args.workload, nuse)
+    w, true, start, shots = build_gradient_workload(args.workload, nuse, grid=args.grid)
     if args.nt > 0:
         w["nt"] = args.nt
         shots = [(sp, src[:, :args.nt].copy(), rp) for sp, src, rp in shots]
