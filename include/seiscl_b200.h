@@ -99,8 +99,8 @@ typedef struct sfd_config {
                               large (forces), the carried-over memory dominates the adjoint
                               field inside the absorbing layers; 1 removes that. */
     int field_precision;   /* 0: wave fields and memory variables in FP32; 1: in FP16,
-                              scaled by powers of two per shot (3D forward modelling
-                              only; arithmetic stays FP32).  No reference counterpart
+                              scaled by powers of two per shot (forward modelling of 3D
+                              and 2D P-SV grids, L <= 3; arithmetic stays FP32).  No reference counterpart
                               in this form: the reference's FP16=2 mode also scales
                               by powers of two (src/assign_modeling_case.c:829-866). */
     int back_prop_type;    /* BACK_PROP_TYPE: 0 or 1 boundary-saving backpropagation,

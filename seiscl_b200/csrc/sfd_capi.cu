@@ -878,7 +878,8 @@ int check_config(const sfd_config &c)
     if (c.kernels < 0 || c.kernels > 7) return SFD_ERR_ARG;
     if (c.adjoint_reset_psi < 0 || c.adjoint_reset_psi > 1) return SFD_ERR_ARG;
     if (c.field_precision < 0 || c.field_precision > 1) return SFD_ERR_ARG;
-    if (c.field_precision == 1 && (c.nd != 3 || c.L > 3)) return SFD_ERR_UNSUPPORTED;
+    // 16-bit fields: 3D (L <= 3, the 4-cell and streaming kernels) and 2D P-SV
+    if (c.field_precision == 1 && ((c.nd != 3 && c.nd != 2) || c.L > 3)) return SFD_ERR_UNSUPPORTED;
     if (c.back_prop_type < 0 || c.back_prop_type > 2) return SFD_ERR_ARG;
     if (c.loop_graphs < 0 || c.loop_graphs > 2) return SFD_ERR_ARG;
     if (c.hout < 0 || c.hout > 1) return SFD_ERR_ARG;

@@ -265,19 +265,22 @@ __device__ __forceinline__ bool shell_cell(const Grid &g, int gid, int &i, int &
 }
 
 // ------------------------------------------------------------------ taper
-template <int NF>
+template <int NF, class T = float>
 __device__ __forceinline__ void apply_taper(const Grid &g, const float *taper, int gz, int gy, int gx,
-                                            float *const *fs, i64 iv)
+                                            T *const *fs, i64 iv)
 {
     int F = g.F, NAB = g.nab;
-    if (!g.freesurf && gz - F < NAB) { float t = __ldg(taper + gz - F); for (int q = 0; q < NF; q++) fs[q][iv] *= t; }
-    if (gz > g.NZ - NAB - F - 1) { float t = __ldg(taper + g.NZ - F - gz - 1); for (int q = 0; q < NF; q++) fs[q][iv] *= t; }
+    auto mul = [&](float t) {
+        for (int q = 0; q < NF; q++) stv(fs[q] + iv, ldv(fs[q] + iv) * t);
+    };
+    if (!g.freesurf && gz - F < NAB) mul(__ldg(taper + gz - F));
+    if (gz > g.NZ - NAB - F - 1) mul(__ldg(taper + g.NZ - F - gz - 1));
     if (g.nd == 3) {
-        if (gy - F < NAB) { float t = __ldg(taper + gy - F); for (int q = 0; q < NF; q++) fs[q][iv] *= t; }
-        if (gy > g.NY - NAB - F - 1) { float t = __ldg(taper + g.NY - F - gy - 1); for (int q = 0; q < NF; q++) fs[q][iv] *= t; }
+        if (gy - F < NAB) mul(__ldg(taper + gy - F));
+        if (gy > g.NY - NAB - F - 1) mul(__ldg(taper + g.NY - F - gy - 1));
     }
-    if (gx - F < NAB) { float t = __ldg(taper + gx - F); for (int q = 0; q < NF; q++) fs[q][iv] *= t; }
-    if (gx > g.NX - NAB - F - 1) { float t = __ldg(taper + g.NX - F - gx - 1); for (int q = 0; q < NF; q++) fs[q][iv] *= t; }
+    if (gx - F < NAB) mul(__ldg(taper + gx - F));
+    if (gx > g.NX - NAB - F - 1) mul(__ldg(taper + g.NX - F - gx - 1));
 }
 
 // ===================================================================== 2D
@@ -341,7 +344,9 @@ __device__ __forceinline__ void cpml_s2d(const Grid &g, const Fields &f, int gz,
     }
 }
 
-template <int F>
+// T: storage of the wave fields and memory variables (float, or __half
+// holding them times power-of-two scales; the arithmetic is FP32)
+template <int F, class T = float>
 __global__ void __launch_bounds__(256) k_v2d(Grid g, Fields f)
 {
     SHOT_F
@@ -350,38 +355,40 @@ __global__ void __launch_bounds__(256) k_v2d(Grid g, Fields f)
     if (gz > g.NZ - F - 1 || gx > g.NX - F - 1) return;
     i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
     const float *hc = g.hc;
-    float sxx_x = dfw<F>(f.w[SXX], iv, g.NZ, hc);
-    float szz_z = dfw<F>(f.w[SZZ], iv, 1, hc);
-    float sxz_z = dbw<F>(f.w[SXZ], iv, 1, hc);
-    float sxz_x = dbw<F>(f.w[SXZ], iv, g.NZ, hc);
+    T *vx = fld<T>(f.w[VX]), *vz = fld<T>(f.w[VZ]);
+    float sxx_x = dfwT<F>(fld<T>(f.w[SXX]), iv, g.NZ, hc);
+    float szz_z = dfwT<F>(fld<T>(f.w[SZZ]), iv, 1, hc);
+    float sxz_z = dbwT<F>(fld<T>(f.w[SXZ]), iv, 1, hc);
+    float sxz_x = dbwT<F>(fld<T>(f.w[SXZ]), iv, g.NZ, hc);
     if (g.abs_type == 1) cpml_v2d(g, f, gz, gx, sxx_x, szz_z, sxz_x, sxz_z);
-    f.w[VX][iv] += (sxx_x + sxz_z) * __ldg(f.p[PRIP] + ip);
-    f.w[VZ][iv] += (szz_z + sxz_x) * __ldg(f.p[PRKP] + ip);
+    stv(vx + iv, ldv(vx + iv) + (sxx_x + sxz_z) * __ldg(f.p[PRIP] + ip));
+    stv(vz + iv, ldv(vz + iv) + (szz_z + sxz_x) * __ldg(f.p[PRKP] + ip));
     if (g.abs_type == 2) {
-        float *fs[2] = {f.w[VX], f.w[VZ]};
+        T *fs[2] = {vx, vz};
         apply_taper<2>(g, f.taper, gz, 0, gx, fs, iv);
     }
 }
 
 // one cell of the P-SV stress update (update_s2D.cl:30-327)
-template <int F>
+template <int F, class T = float>
 __device__ __forceinline__ void s2d_cell(const Grid &g, const Fields &f, int gz, int gx)
 {
     i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * g.NZ + gz;
     const float *hc = g.hc;
-    float vxx = dbw<F>(f.w[VX], iv, g.NZ, hc);
-    float vxz = dfw<F>(f.w[VX], iv, 1, hc);
-    float vzz = dbw<F>(f.w[VZ], iv, 1, hc);
-    float vzx = dfw<F>(f.w[VZ], iv, g.NZ, hc);
+    T *wsxx = fld<T>(f.w[SXX]), *wszz = fld<T>(f.w[SZZ]), *wsxz = fld<T>(f.w[SXZ]);
+    float vxx = dbwT<F>(fld<T>(f.w[VX]), iv, g.NZ, hc);
+    float vxz = dfwT<F>(fld<T>(f.w[VX]), iv, 1, hc);
+    float vzz = dbwT<F>(fld<T>(f.w[VZ]), iv, 1, hc);
+    float vzx = dfwT<F>(fld<T>(f.w[VZ]), iv, g.NZ, hc);
     if (g.abs_type == 1) cpml_s2d(g, f, gz, gx, vxx, vxz, vzx, vzz);
     const int L = g.L;
     if (L == 0) {
         float fipkp = __ldg(f.p[PMUIPKP] + ip);
         float fm = 2.0f * __ldg(f.p[PMU] + ip);
         float gm = __ldg(f.p[PM] + ip);
-        f.w[SXZ][iv] += fipkp * (vxz + vzx);
-        f.w[SXX][iv] += gm * (vxx + vzz) - fm * vzz;
-        f.w[SZZ][iv] += gm * (vxx + vzz) - fm * vxx;
+        stv(wsxz + iv, ldv(wsxz + iv) + fipkp * (vxz + vzx));
+        stv(wsxx + iv, ldv(wsxx + iv) + (gm * (vxx + vzz) - fm * vzz));
+        stv(wszz + iv, ldv(wszz + iv) + (gm * (vxx + vzz) - fm * vxx));
     } else {
         float lM = __ldg(f.p[PM] + ip), lmu = __ldg(f.p[PMU] + ip), lmuipkp = __ldg(f.p[PMUIPKP] + ip);
         float ltaup = __ldg(f.p[PTAUP] + ip), ltaus = __ldg(f.p[PTAUS] + ip), ltausipkp = __ldg(f.p[PTAUSIPKP] + ip);
@@ -391,11 +398,11 @@ __device__ __forceinline__ void s2d_cell(const Grid &g, const Fields &f, int gz,
         float dipkp = lmuipkp * ltausipkp / g.dt;
         float d = 2.0f * lmu * ltaus / g.dt;
         float e = lM * ltaup / g.dt;
-        float *rxx = f.r[RXX], *rzz = f.r[RZZ], *rxz = f.r[RXZ];
+        T *rxx = fld<T>(f.r[RXX]), *rzz = fld<T>(f.r[RZZ]), *rxz = fld<T>(f.r[RXZ]);
         float sxz_ = 0, sxx_ = 0, szz_ = 0;
         for (int l = 0; l < L; l++) {
             i64 ir = l * g.nvol + iv;
-            sxz_ += rxz[ir]; sxx_ += rxx[ir]; szz_ += rzz[ir];
+            sxz_ += ldv(rxz + ir); sxx_ += ldv(rxx + ir); szz_ += ldv(rzz + ir);
         }
         float lsxz = fipkp * (vxz + vzx) + g.dt2 * sxz_;
         float lsxx = (gm * (vxx + vzz) - fm * vzz) + g.dt2 * sxx_;
@@ -405,38 +412,42 @@ __device__ __forceinline__ void s2d_cell(const Grid &g, const Fields &f, int gz,
             float el = g.eta[l];
             float b = 1.0f / (1.0f + el * 0.5f), c = 1.0f - el * 0.5f;
             i64 ir = l * g.nvol + iv;
-            float a1 = b * (rxz[ir] * c - el * (dipkp * (vxz + vzx)));
-            float a2 = b * (rxx[ir] * c - el * (e * (vxx + vzz) - d * vzz));
-            float a3 = b * (rzz[ir] * c - el * (e * (vxx + vzz) - d * vxx));
-            rxz[ir] = a1; rxx[ir] = a2; rzz[ir] = a3;
+            float a1 = b * (ldv(rxz + ir) * c - el * (dipkp * (vxz + vzx)));
+            float a2 = b * (ldv(rxx + ir) * c - el * (e * (vxx + vzz) - d * vzz));
+            float a3 = b * (ldv(rzz + ir) * c - el * (e * (vxx + vzz) - d * vxx));
+            stv(rxz + ir, a1); stv(rxx + ir, a2); stv(rzz + ir, a3);
+            // the stored values (rounded to T) are what the next step reads;
+            // the sums use the FP32 ones, as the FP32 build does
             sxz_ += a1; sxx_ += a2; szz_ += a3;
         }
-        f.w[SXZ][iv] += lsxz + g.dt2 * sxz_;
-        f.w[SXX][iv] += lsxx + g.dt2 * sxx_;
-        f.w[SZZ][iv] += lszz + g.dt2 * szz_;
+        stv(wsxz + iv, ldv(wsxz + iv) + (lsxz + g.dt2 * sxz_));
+        stv(wsxx + iv, ldv(wsxx + iv) + (lsxx + g.dt2 * sxx_));
+        stv(wszz + iv, ldv(wszz + iv) + (lszz + g.dt2 * szz_));
     }
     if (g.abs_type == 2) {
-        float *fs[3] = {f.w[SXX], f.w[SZZ], f.w[SXZ]};
+        T *fs[3] = {wsxx, wszz, wsxz};
         apply_taper<3>(g, f.taper, gz, 0, gx, fs, iv);
     }
 }
 
 // free surface of one column (surface2D.cl:30-193)
-template <int F>
+template <int F, class T = float>
 __device__ __forceinline__ void surf2d_column(const Grid &g, const Fields &f, int gx, int pdir)
 {
     int gz = F, NZ = g.NZ, L = g.L, NAB = g.nab;
     i64 ip = (i64)(gx - F) * g.nz + (gz - F), iv = (i64)gx * NZ + gz;
-    float *vx = f.w[VX], *vz = f.w[VZ], *sxx = f.w[SXX], *szz = f.w[SZZ], *sxz = f.w[SXZ];
-    szz[iv] = 0.0f;
-    for (int l = 0; l < L; l++) f.r[RZZ][l * g.nvol + iv] = 0.0f;
+    T *vx = fld<T>(f.w[VX]), *vz = fld<T>(f.w[VZ]), *sxx = fld<T>(f.w[SXX]), *szz = fld<T>(f.w[SZZ]),
+      *sxz = fld<T>(f.w[SXZ]);
+    T *rxx = fld<T>(f.r[RXX]), *rzz = fld<T>(f.r[RZZ]);
+    stv(szz + iv, 0.0f);
+    for (int l = 0; l < L; l++) stv(rzz + l * g.nvol + iv, 0.0f);
 #pragma unroll
     for (int m = 1; m <= F; m++) {
-        szz[iv - m] = -szz[iv + m];
-        sxz[iv - m] = -sxz[iv + m - 1];
+        stv(szz + iv - m, -ldv(szz + iv + m));
+        stv(sxz + iv - m, -ldv(sxz + iv + m - 1));
     }
-    float vxx = dbw_rw<F>(vx, iv, NZ, g.hc);
-    float vzz = dbw_rw<F>(vz, iv, 1, g.hc);
+    float vxx = dbw_rwT<F>(vx, iv, NZ, g.hc);
+    float vzz = dbw_rwT<F>(vz, iv, 1, g.hc);
     if (g.abs_type == 1) {
         if (gx - F < NAB) {
             int i = gx - F;
@@ -450,45 +461,45 @@ __device__ __forceinline__ void surf2d_column(const Grid &g, const Fields &f, in
     if (L == 0) {
         float fm = f.p[PMU][ip] * 2.0f, gm = f.p[PM][ip];
         float h = -((gm - fm) * (gm - fm) * vxx / gm) - ((gm - fm) * vzz);
-        sxx[iv] += pdir * h;
+        stv(sxx + iv, ldv(sxx + iv) + pdir * h);
     } else {
         float taus = f.p[PTAUS][ip], taup = f.p[PTAUP][ip], mu = f.p[PMU][ip], M = f.p[PM][ip];
         float fm = mu * 2.0f * (1.0f + L * taus);
         float gm = M * (1.0f + L * taup);
         float h = -((gm - fm) * (gm - fm) * vxx / gm) - ((gm - fm) * vzz);
         float sump = 0;
-        for (int l = 0; l < L; l++) sump += f.r[RXX][l * g.nvol + iv];
+        for (int l = 0; l < L; l++) sump += ldv(rxx + l * g.nvol + iv);
         h += -g.dt2 * sump;
-        sxx[iv] += pdir * h;
+        stv(sxx + iv, ldv(sxx + iv) + pdir * h);
         float d = 2.0f * mu * taus / g.dt, e = M * taup / g.dt;
         sump = 0;
         for (int l = 0; l < L; l++) {
             float b = g.eta[l] / (1.0f + g.eta[l] * 0.5f);
             float hh = b * (((d - e) * ((fm / gm) - 1.0f) * vxx) - ((d - e) * vzz));
-            float r = f.r[RXX][l * g.nvol + iv] + pdir * hh;
-            f.r[RXX][l * g.nvol + iv] = r;
+            float r = ldv(rxx + l * g.nvol + iv) + pdir * hh;
+            stv(rxx + l * g.nvol + iv, r);
             sump += r;
         }
-        sxx[iv] += pdir * (g.dt2 * sump);
+        stv(sxx + iv, ldv(sxx + iv) + pdir * (g.dt2 * sump));
     }
 }
 
 // free surface, one thread per surface column
-template <int F>
+template <int F, class T = float>
 __global__ void k_surf2d(Grid g, Fields f, int pdir)
 {
     SHOT_F
     int gx = blockIdx.x * blockDim.x + threadIdx.x + F;
-    if (gx <= g.NX - F - 1) surf2d_column<F>(g, f, gx, pdir);
+    if (gx <= g.NX - F - 1) surf2d_column<F, T>(g, f, gx, pdir);
 }
 
-template <int F>
+template <int F, class T = float>
 __global__ void __launch_bounds__(256) k_s2d(Grid g, Fields f)
 {
     SHOT_F
     int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
-    if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_cell<F>(g, f, gz, gx);
+    if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_cell<F, T>(g, f, gz, gx);
 }
 
 // ===================================================================== 3D
@@ -3334,6 +3345,7 @@ __global__ void k_record(Fields f, PointSet r, float *out, int nt_total, int t, 
 // last: every block fences its stores and takes a ticket; the block with
 // the last ticket sees all stores of the launch, records, adds the next
 // step's sources and resets the ticket.  Nothing waits on another block.
+template <class T = float>
 __device__ __forceinline__ void step_tail(const Grid &g, const Fields &f, const StepTail &tl)
 {
     __shared__ int s_last;
@@ -3346,11 +3358,11 @@ __device__ __forceinline__ void step_tail(const Grid &g, const Fields &f, const 
     if (!s_last) return;
     __threadfence();
     for (int i = tid; i < tl.rec.n; i += nth)
-        record_point<float, true>(f, tl.rec, tl.out, tl.nt_total, tl.t, tl.outmask, g.nd, g.ws, i);
+        record_point<T, true>(f, tl.rec, tl.out, tl.nt_total, tl.t, tl.outmask, g.nd, g.ws, i);
     __syncthreads();
     if (tl.tsrc >= 0)
         for (int i = tid; i < tl.src.n; i += nth)
-            source_point<float>(f, tl.src, tl.stf, tl.nt_total, tl.tsrc, 1, g.dt, g.freesurf, g.F, g.ws, i);
+            source_point<T>(f, tl.src, tl.stf, tl.nt_total, tl.tsrc, 1, g.dt, g.freesurf, g.F, g.ws, i);
     if (tid == 0) *tl.ticket = 0;
 }
 
@@ -3358,19 +3370,19 @@ __device__ __forceinline__ void step_tail(const Grid &g, const Fields &f, const 
 // rows hold every stress the surface reads, rows F..2F) and step tail.
 // pdir (1) is a launch argument, as for the separate surface kernel, so
 // that both contract and round alike.
-template <int F>
+template <int F, class T = float>
 __global__ void __launch_bounds__(256) k_s2d_step(Grid g, Fields f, StepTail tl, int pdir)
 {
     int gz = blockIdx.x * blockDim.x + threadIdx.x + F;
     int gx = blockIdx.y * blockDim.y + threadIdx.y + F;
     Fields fs = f;   // this block's shot; the tail's points carry their shot in their cells
     if (g.nb > 1) shot_fields(g, fs, blockIdx.z);
-    if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_cell<F>(g, fs, gz, gx);
+    if (gz <= g.NZ - F - 1 && gx <= g.NX - F - 1) s2d_cell<F, T>(g, fs, gz, gx);
     if (g.freesurf && blockIdx.x == 0) {
         __syncthreads();
-        if (threadIdx.x == 0 && gx <= g.NX - F - 1) surf2d_column<F>(g, fs, gx, pdir);
+        if (threadIdx.x == 0 && gx <= g.NX - F - 1) surf2d_column<F, T>(g, fs, gx, pdir);
     }
-    step_tail(g, f, tl);
+    step_tail<T>(g, f, tl);
 }
 
 // acoustic pressure update and step tail (no free-surface kernel)
@@ -3485,7 +3497,8 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
         DISPATCH_F(g.F, MB_DISPATCH(g, k_v3d<FF, MBV><<<gr, b, 0, st>>>(g, f)));
     } else {
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
-        DISPATCH_F(g.F, k_v2d<FF><<<gr, b, 0, st>>>(g, f));
+        if (g.fhalf) DISPATCH_F(g.F, k_v2d<FF, __half><<<gr, b, 0, st>>>(g, f))
+        else DISPATCH_F(g.F, k_v2d<FF><<<gr, b, 0, st>>>(g, f));
     }
 }
 
@@ -3568,7 +3581,8 @@ bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_
         DISPATCH_F(g.F, MB_DISPATCH(g, k_s3d<FF, MBV><<<gr, b, 0, st>>>(g, f)));
     } else {
         dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);
-        DISPATCH_F(g.F, k_s2d<FF><<<gr, b, 0, st>>>(g, f));
+        if (g.fhalf) DISPATCH_F(g.F, k_s2d<FF, __half><<<gr, b, 0, st>>>(g, f))
+        else DISPATCH_F(g.F, k_s2d<FF><<<gr, b, 0, st>>>(g, f));
     }
     return false;
 }
@@ -3643,7 +3657,8 @@ bool launch_update_s_step(const Grid &g, const Fields &f, const StepTail &tl, cu
 {
     if (g.nd != 2 && g.nd != 22) return false;
     dim3 b(32, 8), gr(cdiv(g.nz, 32), cdiv(g.nx, 8), g.nb);   // 32 z rows >= 2F + 1: the surface stays in its block
-    if (g.nd == 2) DISPATCH_F(g.F, k_s2d_step<FF><<<gr, b, 0, st>>>(g, f, tl, 1))
+    if (g.nd == 2 && g.fhalf) DISPATCH_F(g.F, k_s2d_step<FF, __half><<<gr, b, 0, st>>>(g, f, tl, 1))
+    else if (g.nd == 2) DISPATCH_F(g.F, k_s2d_step<FF><<<gr, b, 0, st>>>(g, f, tl, 1))
     else DISPATCH_F(g.F, k_s2d_acc_step<FF><<<gr, b, 0, st>>>(g, f, tl))
     return true;
 }
@@ -3660,7 +3675,8 @@ void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st)
         if (g.fhalf) DISPATCH_F(g.F, k_surf3d<FF, __half><<<gr, b, 0, st>>>(g, f, pdir))
         else DISPATCH_F(g.F, k_surf3d<FF><<<gr, b, 0, st>>>(g, f, pdir))
     } else {
-        DISPATCH_F(g.F, k_surf2d<FF><<<dim3(cdiv(g.nx, 128), 1, g.nb), 128, 0, st>>>(g, f, pdir));
+        if (g.fhalf) DISPATCH_F(g.F, k_surf2d<FF, __half><<<dim3(cdiv(g.nx, 128), 1, g.nb), 128, 0, st>>>(g, f, pdir))
+        else DISPATCH_F(g.F, k_surf2d<FF><<<dim3(cdiv(g.nx, 128), 1, g.nb), 128, 0, st>>>(g, f, pdir));
     }
 }
 

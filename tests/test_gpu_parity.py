@@ -325,6 +325,48 @@ def test_fp16_field_storage_against_fp32(kw, cuda_device):
     assert num / den < 1e-3, num / den
 
 
+FP16_2D_CASES = [
+    dict(nd=2, freesurf=1, L=0, abs_type=1, src_type=100, nt=300, seed=81),
+    dict(nd=2, freesurf=1, L=2, abs_type=1, src_type=2, nt=300, seed=82, fdorder=4),
+    dict(nd=2, freesurf=0, L=1, abs_type=2, src_type=0, nt=300, seed=83, nz=70, nx=60),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", FP16_2D_CASES, ids=["psv_fs", "psv_visco_o4", "psv_taper"])
+def test_fp16_2d_field_storage_against_fp32(kw, cuda_device):
+    """2D P-SV wave fields and memory variables stored in FP16 (power-of-two
+    scaled, FP32 arithmetic) against the FP32 run, with the reference's
+    criterion for its FP16 modes (sum (d - r)^2 / sum r^2 < 1e-3 over all
+    outputs, test_consistency.py); the two-launch steps and the one-launch-
+    per-kernel path agree in FP16 too; boundary saving is refused."""
+    import dataclasses
+
+    from seiscl_b200.engine import Plan, SeisCLEngineError
+
+    cfg, model, acq = make_case(**kw)
+    outs = ["vx", "vz", "p"]
+    res = {}
+    for prec, kern in (("fp32", "fast"), ("fp16", "fast"), ("fp16", "general")):
+        plan = Plan(dataclasses.replace(engine_config(cfg), field_precision=prec, kernels=kern))
+        plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+        res[(prec, kern)] = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
+        if prec == "fp16" and kern == "fast":
+            with pytest.raises(SeisCLEngineError):   # the fields really are FP16
+                plan.debug_array(0, 0, plan.nvol)
+            with pytest.raises(SeisCLEngineError):   # forward modelling only
+                plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs, save_boundaries=True)
+        plan.close()
+    ref, half = res[("fp32", "fast")], res[("fp16", "fast")]
+    num = sum(float(((half[n].astype(np.float64) - ref[n]) ** 2).sum()) for n in outs)
+    den = sum(float((ref[n].astype(np.float64) ** 2).sum()) for n in outs)
+    assert den > 0
+    print("FP16-2D %s energy ratio %.3g" % (kw, num / den))
+    assert num / den < 1e-3, num / den
+    for n in outs:
+        assert rel_l2(res[("fp16", "general")][n], half[n]) < 1e-6, n
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("kw", [dict(nd=2, freesurf=1, L=1, abs_type=1, src_type=100, nt=120),
                                 dict(nd=3, freesurf=1, L=2, abs_type=1, src_type=2, nz=36, ny=30, nx=34, nt=60,

@@ -80,7 +80,7 @@ def test_forward_against_fp64(kw, cuda_device):
     cfg, model, acq = make_case(**kw)
     outs = ["vx", "vy", "vz", "p"] if cfg["nd"] == 3 else ["vx", "vz", "p"]
     ref = _fp64(cfg, model).forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
-    precs = ("fp32", "fp16") if cfg["nd"] == 3 else ("fp32",)
+    precs = ("fp32", "fp16")
     for prec in precs:
         plan = Plan(dataclasses.replace(engine_config(cfg), field_precision=prec))
         plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
