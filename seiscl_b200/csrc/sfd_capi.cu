@@ -1205,7 +1205,9 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     PointSet S, R;
     if ((rc = upload_shots(p, nshot, shots, mask, S, R, st))) return rc;
     if ((rc = zero_forward_state(p, st))) return rc;
-    if (nsel) CKC(cudaMemsetAsync(p->d_seis, 0, sizeof(float) * (size_t)nsel * sb.nrec * p->cfg.nt, st));
+    // a batch without receivers has no seismogram buffer (none is allocated
+    // for zero traces): no copy of zero bytes goes to a null pointer
+    if (nsel && sb.nrec) CKC(cudaMemsetAsync(p->d_seis, 0, sizeof(float) * (size_t)nsel * sb.nrec * p->cfg.nt, st));
     BndSlot bs;
     memset(&bs, 0, sizeof bs);
     // FP16 stores: the source injects about 2^4 per step into the field it
@@ -1351,7 +1353,7 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     int slot = 0;
     for (int o = 0; o < SFD_NOUT; o++) {
         if (!(omask & (1u << o))) continue;
-        if (seis && seis[o])
+        if (seis && seis[o] && sb.nrec)
             CKC(cudaMemcpyAsync(seis[o], p->d_seis + (size_t)slot * sb.nrec * NT,
                                 sizeof(float) * (size_t)sb.nrec * NT, cudaMemcpyDeviceToHost, st));
         slot++;
@@ -1406,8 +1408,9 @@ extern "C" int sfd_adjoint_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     for (int o = 0; o < SFD_NOUT; o++) {
         if (!(omask & (1u << o))) continue;
         if (!residuals || !residuals[o]) return fail(p, SFD_ERR_ARG, "missing residual array");
-        CKC(cudaMemcpyAsync(p->d_res + (size_t)slot * sb.nrec * NT, residuals[o],
-                            sizeof(float) * (size_t)sb.nrec * NT, cudaMemcpyHostToDevice, st));
+        if (sb.nrec)
+            CKC(cudaMemcpyAsync(p->d_res + (size_t)slot * sb.nrec * NT, residuals[o],
+                                sizeof(float) * (size_t)sb.nrec * NT, cudaMemcpyHostToDevice, st));
         slot++;
     }
     if (p->cfg.back_prop_type == 2) {

@@ -186,7 +186,8 @@ extern "C" int sfd_forward_noalloc(sfd_plan *p, const float *src_pos, const floa
     // previous call's contents
     cudaError_t e = cudaMemsetAsync(base, 0, off_map, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int), st);
-    if (e == cudaSuccess && nsel) e = cudaMemsetAsync(seis, 0, sizeof(float) * (size_t)nsel * nrec * p->cfg.nt, st);
+    if (e == cudaSuccess && nsel && nrec)
+        e = cudaMemsetAsync(seis, 0, sizeof(float) * (size_t)nsel * nrec * p->cfg.nt, st);
     if (e != cudaSuccess) { p->err = cudaGetErrorString(e); return SFD_ERR_CUDA; }
     if (nsrc + nrec > 0)
         k_noalloc_map<<<(nsrc + nrec + 127) / 128, 128, 0, st>>>(g, p->DH_lit, src_pos, nsrc, rec_pos, nrec, tt, scell,
