@@ -407,6 +407,8 @@ def run_gradient(args):
     B = args.batch if args.batch > 0 else (8 if GRADIENT_WORKLOADS[args.workload]["nd"] != 3 else 1)
     if args.checkpoint:
         B = 1   # checkpointed gradients run one shot per launch
+    elif args.fields == "fp16":
+        raise SystemExit("FP16 wave fields in a gradient need --checkpoint K")
     nuse = (args.warmup + args.steps) * B
     w, true, start, shots = build_gradient_workload(args.workload, nuse, grid=args.grid)
     if args.nt > 0:
@@ -414,7 +416,7 @@ def run_gradient(args):
         shots = [(sp, src[:, :args.nt].copy(), rp) for sp, src, rp in shots]
     outs = w["outputs"]
     cfg = dataclasses.replace(engine_config(w), precision=w["precision"], batch=B,
-                              checkpoint=args.checkpoint,
+                              checkpoint=args.checkpoint, field_precision=args.fields,
                               kernels=args.kernels if args.kernels in ("fast", "vector") else "fast")
     plan = Plan(cfg)
     plan.set_model(true["vp"], true["vs"], true["rho"])
@@ -453,7 +455,8 @@ def run_gradient(args):
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(loop_ms / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "grid": [w["nz"], w["ny"], w["nx"]], "nt": w["nt"],
-                   "fdorder": w["fdorder"], "boundaries": w["precision"], "outputs": outs,
+                   "fdorder": w["fdorder"], "boundaries": w["precision"], "field_storage": args.fields,
+                   "outputs": outs,
                    "batch": B,
                    "recompute": ("snapshots every %d steps" % args.checkpoint) if args.checkpoint
                    else "saved boundaries, backpropagation",

@@ -100,7 +100,9 @@ typedef struct sfd_config {
                               field inside the absorbing layers; 1 removes that. */
     int field_precision;   /* 0: wave fields and memory variables in FP32; 1: in FP16,
                               scaled by powers of two per shot (forward modelling of 3D
-                              and 2D P-SV grids, L <= 3; arithmetic stays FP32).  No reference counterpart
+                              and 2D P-SV grids, L <= 3, and the forward and recomputed
+                              runs of a checkpointed gradient, whose adjoint fields stay
+                              FP32; arithmetic stays FP32).  No reference counterpart
                               in this form: the reference's FP16=2 mode also scales
                               by powers of two (src/assign_modeling_case.c:829-866). */
     int back_prop_type;    /* BACK_PROP_TYPE: 0 or 1 boundary-saving backpropagation,
@@ -131,8 +133,9 @@ typedef struct sfd_config {
                               fields of every step of the segment: the adjoint reads the
                               forward field instead of reconstructing it (no boundary
                               store; memory: (nt/K) snapshots + K wave-field states, in
-                              `precision`, CPML memory in FP32).  P-SV and 3D, batch 1,
-                              FP32 wave fields.  The reference's INPUTRES checkpoint
+                              `precision`, CPML memory in FP32; with FP16 wave-field
+                              storage the snapshots hold the FP16 fields as they are).
+                              P-SV and 3D, batch 1.  The reference's INPUTRES checkpoint
                               (time_stepping.c:92-270) saves the final state and the
                               boundaries instead. */
 } sfd_config;

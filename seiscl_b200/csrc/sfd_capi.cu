@@ -536,8 +536,17 @@ int run_loop(sfd_plan *p, sfd_plan::LoopGraph &lg, const std::string &key, cudaS
 struct CkptSizes {
     int nwave, nmem, K, nseg;
     int64_t psi;            // CPML floats
-    size_t elem, snap, seg;
+    size_t elem, selem, snap, seg;   // bytes per stored value: segment store, snapshot fields
 };
+// FP16 wave-field storage: log2 of the factor a parameter carries (the
+// moduli 2^-kshift, the buoyancies 2^kshift, the rest 1)
+int param_exponent(int k, int kshift)
+{
+    if (k == PRIP || k == PRJP || k == PRKP) return kshift;
+    if (k == PM || k == PMU || k == PMUIPKP || k == PMUIPJP || k == PMUJPKP) return -kshift;
+    return 0;
+}
+
 CkptSizes ckpt_sizes(const Grid &g, const sfd_config &c)
 {
     CkptSizes z;
@@ -550,7 +559,9 @@ CkptSizes ckpt_sizes(const Grid &g, const sfd_config &c)
     z.K = std::max(1, std::min(c.checkpoint, tmax));
     z.nseg = (tmax + z.K - 1) / z.K;
     z.elem = c.precision == SFD_PREC_FP32 ? 4 : 2;
-    z.snap = z.elem * g.nvol * (z.nwave + (size_t)z.nmem * g.L) + sizeof(float) * z.psi;
+    // FP16 wave-field storage: the snapshots copy the FP16 fields unchanged
+    z.selem = g.fhalf ? 2 : z.elem;
+    z.snap = z.selem * g.nvol * (z.nwave + (size_t)z.nmem * g.L) + sizeof(float) * z.psi;
     z.seg = z.elem * g.nvol * z.nwave * (size_t)z.K;
     return z;
 }
@@ -572,6 +583,33 @@ int alloc_ckpt(sfd_plan *p)
     return SFD_OK;
 }
 
+// FP16 wave-field storage: the unscaled parameters of the adjoint, uploaded
+// once per model
+int prepare_adjoint_params(sfd_plan *p)
+{
+    for (int k = 0; k < NPAR; k++) p->padj[k] = p->f.p[k];
+    if (!p->g.fhalf) return SFD_OK;
+    const Grid &g = p->g;
+    const int64_t npar = (int64_t)g.nz * g.ny * g.nx;
+    int nscaled = 0;
+    for (int k = 0; k < NPAR; k++) nscaled += p->f.p[k] && param_exponent(k, 1) != 0;
+    cudaError_t e;
+    if (!p->d_padj) {
+        p->d_padj = (float *)dalloc(p, sizeof(float) * npar * nscaled, &e);
+        if (!p->d_padj) return fail(p, SFD_ERR_MEMORY, "unscaled adjoint parameters do not fit in device memory");
+    }
+    int q = 0;
+    for (int k = 0; k < NPAR; k++) {
+        if (!p->f.p[k] || param_exponent(k, 1) == 0) continue;
+        float *dst = p->d_padj + npar * q++;
+        if (!p->padj_valid)
+            CKC(cudaMemcpy(dst, p->hp[k].data(), sizeof(float) * npar, cudaMemcpyHostToDevice));
+        p->padj[k] = dst;
+    }
+    p->padj_valid = true;
+    return SFD_OK;
+}
+
 // wave fields (and memory variables) <-> snapshot j
 void ckpt_snapshot(sfd_plan *p, int j, bool load, cudaStream_t st)
 {
@@ -581,8 +619,15 @@ void ckpt_snapshot(sfd_plan *p, int j, bool load, cudaStream_t st)
     PackSet ps;
     memset(&ps, 0, sizeof ps);
     size_t off = 0;
+    // FP16 wave-field storage: the fields are copied as they are (exact)
+    auto copy = [&](void *field, size_t bytes) {
+        if (load) cudaMemcpyAsync(field, base + off, bytes, cudaMemcpyDeviceToDevice, st);
+        else cudaMemcpyAsync(base + off, field, bytes, cudaMemcpyDeviceToDevice, st);
+        off += bytes;
+    };
     for (int w = 0; w < NW; w++) {
         if (!p->f.w[w]) continue;
+        if (g.fhalf) { copy(p->f.w[w], z.selem * g.nvol); continue; }
         ps.src[ps.narr] = load ? (const void *)(base + off) : (const void *)p->f.w[w];
         ps.dst[ps.narr] = load ? (void *)p->f.w[w] : (void *)(base + off);
         ps.n[ps.narr] = g.nvol;
@@ -592,6 +637,7 @@ void ckpt_snapshot(sfd_plan *p, int j, bool load, cudaStream_t st)
     }
     for (int r = 0; r < NR; r++) {   // memory variables: the scale of the stresses
         if (!p->f.r[r]) continue;
+        if (g.fhalf) { copy(p->f.r[r], z.selem * g.nvol * g.L); continue; }
         ps.src[ps.narr] = load ? (const void *)(base + off) : (const void *)p->f.r[r];
         ps.dst[ps.narr] = load ? (void *)p->f.r[r] : (void *)(base + off);
         ps.n[ps.narr] = g.nvol * g.L;
@@ -621,10 +667,11 @@ void ckpt_store(sfd_plan *p, int k, cudaStream_t st)
         ps.src[ps.narr] = p->f.w[w];
         ps.dst[ps.narr] = base + z.elem * g.nvol * ps.narr;
         ps.n[ps.narr] = g.nvol;
-        ps.scale[ps.narr] = g.bsc[w];
+        // FP16 wave fields carry 2^a or 2^b: taken off before the store's own scale
+        ps.scale[ps.narr] = g.fhalf ? g.bsc[w] / g.ws.w[w] : g.bsc[w];
         ps.narr++;
     }
-    launch_pack(ps, p->cfg.precision, false, st);
+    launch_pack(ps, p->cfg.precision, false, st, g.fhalf);
 }
 void ckpt_slot(const sfd_plan *p, int k, AdjFields &a)
 {
@@ -653,14 +700,35 @@ int adjoint_ckpt(sfd_plan *p, const PointSet &S, const PointSet &R, unsigned oma
     // the adjoint's CPML memory: the forward run's (the reference binds the
     // same buffers, src/clprogram.c:806-811) or zero
     if (z.psi) {
-        if (p->cfg.adjoint_reset_psi) CKC(cudaMemsetAsync(p->d_psi_adj, 0, sizeof(float) * z.psi, st));
-        else CKC(cudaMemcpyAsync(p->d_psi_adj, p->d_psi_all, sizeof(float) * z.psi, cudaMemcpyDeviceToDevice, st));
+        if (p->cfg.adjoint_reset_psi) {
+            CKC(cudaMemsetAsync(p->d_psi_adj, 0, sizeof(float) * z.psi, st));
+        } else if (g.fhalf) {
+            // the forward CPML memory is in the units of the FP16 fields:
+            // psi of velocity derivatives carries 2^b, of stress derivatives 2^a
+            PackSet ps;
+            memset(&ps, 0, sizeof ps);
+            for (int i = 0; i < NPSI; i++) {
+                if (!p->f.psi[i] || !p->psi_size[i]) continue;
+                ps.src[ps.narr] = p->f.psi[i];
+                ps.dst[ps.narr] = p->d_psi_adj + (p->f.psi[i] - p->d_psi_all);
+                ps.n[ps.narr] = p->psi_size[i];
+                ps.scale[ps.narr] = 1.0f / g.ws.w[i < PSXX_X ? VX : SXX];
+                if (++ps.narr == PackSet::MAXARR) { launch_pack(ps, SFD_PREC_FP32, false, st); ps.narr = 0; }
+            }
+            launch_pack(ps, SFD_PREC_FP32, false, st);
+        } else {
+            CKC(cudaMemcpyAsync(p->d_psi_adj, p->d_psi_all, sizeof(float) * z.psi, cudaMemcpyDeviceToDevice, st));
+        }
     }
     Fields fa = p->f;
     for (int i = 0; i < NPSI; i++)
         fa.psi[i] = p->f.psi[i] ? p->d_psi_adj + (p->f.psi[i] - p->d_psi_all) : nullptr;
+    int rc;
+    if ((rc = prepare_adjoint_params(p))) return rc;
+    for (int k = 0; k < NPAR; k++) fa.p[k] = p->padj[k];
     Grid ga = g;
     ga.ckpt = 1;
+    ga.fhalf = false;   // the adjoint fields are FP32
     AdjFields a = p->a;
     for (int w = 0; w < NW; w++) a.bnd[w] = nullptr;
     LoopKey key;
@@ -669,7 +737,6 @@ int adjoint_ckpt(sfd_plan *p, const PointSet &S, const PointSet &R, unsigned oma
     key.add(p->cfg.precision); key.add(tmax); key.add(tmin); key.add(z.K);
     const float *chk = check_field(a.wr);
     const int64_t nchk = g.nvol * g.nb;
-    int rc;
     if ((rc = arm_unstable(p, st))) return rc;
     CKC(cudaEventRecord(p->ev0, st));
     int rcl = run_loop(p, p->gadj, key.s, st, [&](cudaStream_t s) {
@@ -692,7 +759,7 @@ int adjoint_ckpt(sfd_plan *p, const PointSet &S, const PointSet &R, unsigned oma
                 launch_update_adj(ga, fa, a, true, p->cfg.precision, s);
                 launch_update_adj(ga, fa, a, false, p->cfg.precision, s);
                 if (t % FINITE_CHECK_EVERY == 0 || t == tmin + 1)
-                    launch_finite_check(g, chk, nchk, t, p->d_unstable, s);
+                    launch_finite_check(ga, chk, nchk, t, p->d_unstable, s);
             }
         }
     });
@@ -889,7 +956,7 @@ int check_config(const sfd_config &c)
     if (c.checkpoint < 0) return SFD_ERR_ARG;
     // checkpointed gradients: boundary-saving semantics on P-SV and 3D grids, one shot per launch
     if (c.checkpoint > 0 && (c.back_prop_type == 2 || (c.nd != 2 && c.nd != 3) || c.batch > 1 ||
-                             c.field_precision != 0))
+                             (c.field_precision != 0 && c.hout)))
         return SFD_ERR_UNSUPPORTED;
     // batched shots: P-SV, acoustic and 3D one-cell / 4-cell kernels in FP32,
     // boundary-saving gradients
@@ -978,6 +1045,8 @@ extern "C" int sfd_plan_create(const sfd_config *cfg, sfd_plan **out)
     p->fwd_nb = 0;
     p->d_snap = p->d_seg = nullptr;
     p->d_psi_adj = nullptr;
+    p->d_padj = nullptr;
+    p->padj_valid = false;
     p->snap_bytes = p->seg_bytes = 0;
     p->nseg = 0;
     memset(&p->f, 0, sizeof p->f);
@@ -1040,6 +1109,7 @@ extern "C" int sfd_footprint(const sfd_config *cfg, int gradient, int nsrc, int6
             if (cfg->checkpoint > 0) {   // snapshots, segment store, adjoint CPML memory
                 const CkptSizes z = ckpt_sizes(g, *cfg);
                 b += (int64_t)(z.snap * z.nseg + z.seg) + 4 * std::max<int64_t>(z.psi, 1);
+                if (g.fhalf) b += 4 * npar * 8;   // the adjoint's unscaled moduli and buoyancies
             } else {
                 b += B * (int64_t)(cfg->precision == SFD_PREC_FP32 ? 4 : 2) * nt * g.nbnd * nwave;
             }
@@ -1140,6 +1210,7 @@ extern "C" int sfd_set_model(sfd_plan *p, const float *const *params)
             CKC(cudaMemcpy((void *)p->f.p[k], p->hp[k].data(), sizeof(float) * npar, cudaMemcpyHostToDevice));
     }
     p->model_set = true;
+    p->padj_valid = false;
     p->have_forward = false;
     return SFD_OK;
 }
@@ -1228,8 +1299,9 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
         b = a + shift;
     };
     if (g.fhalf) {
-        if (save_boundaries)
-            return fail(p, SFD_ERR_UNSUPPORTED, "FP16 wave-field storage covers forward modelling only");
+        if (save_boundaries && !(p->cfg.checkpoint > 0 && p->cfg.back_prop_type != 2))
+            return fail(p, SFD_ERR_UNSUPPORTED,
+                        "FP16 wave-field storage covers forward modelling and checkpointed gradients");
         int a, b;
         store_exponents(p->kshift, a, b);
         for (int w = 0; w < NW; w++) p->g.ws.w[w] = std::ldexp(1.0f, w <= VZ ? b : a);
@@ -1387,7 +1459,8 @@ extern "C" int sfd_adjoint_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
     if ((rc = check_batch(p, nshot, shots, sb))) return rc;
     if (p->g.nd == 21 || p->g.nd == 22)
         return fail(p, SFD_ERR_UNSUPPORTED, "the adjoint path covers P-SV and 3D elastic/viscoelastic media");
-    if (p->g.fhalf) return fail(p, SFD_ERR_UNSUPPORTED, "FP16 wave-field storage covers forward modelling only");
+    if (p->g.fhalf && p->cfg.checkpoint <= 0)
+        return fail(p, SFD_ERR_UNSUPPORTED, "FP16 wave-field storage covers forward modelling and checkpointed gradients");
     if (!p->have_forward) return fail(p, SFD_ERR_STATE, "sfd_adjoint needs a preceding sfd_forward with saved boundaries");
     if (nshot != p->fwd_nb) return fail(p, SFD_ERR_STATE, "the adjoint must follow a forward run of the same shots");
     if (p->g.freesurf && p->surf_mu_zero)

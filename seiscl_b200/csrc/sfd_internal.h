@@ -162,9 +162,16 @@ struct sfd_plan {
     int *d_unstable;        // first checked step with a non-finite wave field (INT_MAX: none)
     int *d_fsync;           // fused 3D step: ticket counter + one flag per work unit
     // checkpointed gradients (cfg.checkpoint = K > 0)
-    char *d_snap;           // [nseg] snapshots: wave fields, memory variables (store type), CPML (FP32)
+    char *d_snap;           // [nseg] snapshots: wave fields, memory variables (store type; FP16 wave-field
+                            // storage: the FP16 fields as they are), CPML (FP32)
     char *d_seg;            // [K][wave fields] of the segment being backpropagated (store type)
     float *d_psi_adj;       // the adjoint's CPML memory
+    // FP16 wave-field storage: the parameters the adjoint reads, without the
+    // power-of-two scalings of the moduli and buoyancies (the adjoint fields
+    // are FP32 and unscaled); padj[k] is f.p[k] for the unscaled ones
+    float *d_padj;
+    const float *padj[sfd::NPAR];
+    bool padj_valid;
     size_t snap_bytes, seg_bytes;
     int nseg;
     int batch;              // copies of the per-shot arrays (shots per launch)

@@ -2288,12 +2288,17 @@ __global__ void __launch_bounds__(128, PF ? 3 : 4) k_adjs3d_q4(Grid g, Fields f,
                 gM[j] = -((s3[0].v[j] + s3[1].v[j] + s3[2].v[j]) * (ls[0] + ls[1] + ls[2]));
             }
         }
-        // the new adjoint memory values go to the forward arrays
+        // the new adjoint memory values go to the forward arrays; a
+        // checkpointed adjoint reloads those from a snapshot before they are
+        // read again, so it skips the stores (its forward arrays may also be
+        // FP16)
         if constexpr (L > 0) {
+            if (!g.ckpt) {
 #pragma unroll
-            for (int c = 0; c < 3; c++)
+                for (int c = 0; c < 3; c++)
 #pragma unroll
-                for (int l = 0; l < L; l++) stq(f.r[rid[c]] + l * g.nvol + iv, rr[c][l]);
+                    for (int l = 0; l < L; l++) stq(f.r[rid[c]] + l * g.nvol + iv, rr[c][l]);
+            }
         }
         if (g.abs_type == 2) {
 #pragma unroll
@@ -3184,17 +3189,22 @@ __global__ void __launch_bounds__(256) k_adjs3d(Grid g, Fields f, AdjFields a)
         }
         for (int q = 0; q < 6; q++) ls[q] += g.dt2 * aa[q];
         // the reference stores these into the forward memory variables and
-        // keeps only the last adjoint value of each sum (update_adjs3D.cl:566-583)
+        // keeps only the last adjoint value of each sum (update_adjs3D.cl:566-583);
+        // a checkpointed adjoint skips the stores (dead: the forward arrays are
+        // reloaded from a snapshot before they are read)
         for (int l = 0; l < L; l++) {
-            float el = g.eta[l];
-            float b = 1.0f / (1.0f + el * 0.5f), c = 1.0f - el * 0.5f;
             i64 ir = l * g.nvol + iv;
-            r[RXY][ir] = b * (rr[RXY][ir] * c - el * (dipjp * vxyyxr));
-            r[RYZ][ir] = b * (rr[RYZ][ir] * c - el * (djpkp * vyzzyr));
-            r[RXZ][ir] = b * (rr[RXZ][ir] * c - el * (dipkp * vxzzxr));
-            r[RXX][ir] = b * (rr[RXX][ir] * c - el * (e * vxxyyzzr - d * vyyzzr));
-            r[RYY][ir] = b * (rr[RYY][ir] * c - el * (e * vxxyyzzr - d * vxxzzr));
-            r[RZZ][ir] = b * (rr[RZZ][ir] * c - el * (e * vxxyyzzr - d * vxxyyr));
+            if (!g.ckpt) {
+                float el = g.eta[l];
+                float b = 1.0f / (1.0f + el * 0.5f), c = 1.0f - el * 0.5f;
+                r[RXY][ir] = b * (rr[RXY][ir] * c - el * (dipjp * vxyyxr));
+                r[RYZ][ir] = b * (rr[RYZ][ir] * c - el * (djpkp * vyzzyr));
+                r[RXZ][ir] = b * (rr[RXZ][ir] * c - el * (dipkp * vxzzxr));
+                r[RXX][ir] = b * (rr[RXX][ir] * c - el * (e * vxxyyzzr - d * vyyzzr));
+                r[RYY][ir] = b * (rr[RYY][ir] * c - el * (e * vxxyyzzr - d * vxxzzr));
+                r[RZZ][ir] = b * (rr[RZZ][ir] * c - el * (e * vxxyyzzr - d * vxxyyr));
+            }
+            // after the stores: in the DFT adjoint r and rr are one buffer
             for (int q = 0; q < 6; q++) aa[q] = rr[rid[q]][ir];
         }
         for (int q = 0; q < 6; q++) wr[sid[q]][iv] += ls[q] + g.dt2 * aa[q];
@@ -3680,9 +3690,10 @@ void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st)
     }
 }
 
-// FP32 arrays to T stores (pack) or back (unpack), value times scale; one
-// grid row per array, a grid-stride loop over its elements
-template <class T, bool UNPACK>
+// S arrays (FP32 or FP16 wave fields) to T stores (pack) or FP32 arrays
+// back from T stores (unpack), value times scale; one grid row per array, a
+// grid-stride loop over its elements
+template <class T, bool UNPACK, class S = float>
 __global__ void k_pack(PackSet ps)
 {
     const int q = blockIdx.y;
@@ -3690,18 +3701,22 @@ __global__ void k_pack(PackSet ps)
     const float sc = ps.scale[q];
     for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
         if (UNPACK) ((float *)ps.dst[q])[i] = to_f<T>(((const T *)ps.src[q])[i]) * sc;
-        else ((T *)ps.dst[q])[i] = from_f<T>(((const float *)ps.src[q])[i] * sc);
+        else ((T *)ps.dst[q])[i] = from_f<T>(to_f<S>(((const S *)ps.src[q])[i]) * sc);
     }
 }
 
-void launch_pack(const PackSet &ps, int prec, bool unpack, cudaStream_t st)
+void launch_pack(const PackSet &ps, int prec, bool unpack, cudaStream_t st, bool half_src)
 {
     if (ps.narr <= 0) return;
     i64 nmax = 0;
     for (int q = 0; q < ps.narr; q++) nmax = ps.n[q] > nmax ? ps.n[q] : nmax;
     dim3 gr((unsigned)std::min<i64>((nmax + 255) / 256, 148 * 8), (unsigned)ps.narr);
     if (gr.x == 0) return;
-    if (prec == SFD_PREC_FP16) {
+    if (half_src && !unpack) {
+        if (prec == SFD_PREC_FP16) k_pack<__half, false, __half><<<gr, 256, 0, st>>>(ps);
+        else if (prec == SFD_PREC_BF16) k_pack<__nv_bfloat16, false, __half><<<gr, 256, 0, st>>>(ps);
+        else k_pack<float, false, __half><<<gr, 256, 0, st>>>(ps);
+    } else if (prec == SFD_PREC_FP16) {
         if (unpack) k_pack<__half, true><<<gr, 256, 0, st>>>(ps);
         else k_pack<__half, false><<<gr, 256, 0, st>>>(ps);
     } else if (prec == SFD_PREC_BF16) {

@@ -69,13 +69,14 @@ void launch_movie(const Grid &g, const float *fld, float inv_scale, float *dst, 
 // their FP32 arrays and stores of the saved-boundary precision (FP16 stores
 // scaled by powers of two)
 struct PackSet {
-    const void *src[NW + NR];
-    void *dst[NW + NR];
-    int64_t n[NW + NR];
-    float scale[NW + NR];   // applied to each value on the way
+    static constexpr int MAXARR = NW + NR;
+    const void *src[MAXARR];
+    void *dst[MAXARR];
+    int64_t n[MAXARR];
+    float scale[MAXARR];   // applied to each value on the way
     int narr;
 };
-void launch_pack(const PackSet &ps, int prec, bool unpack, cudaStream_t st);
+void launch_pack(const PackSet &ps, int prec, bool unpack, cudaStream_t st, bool half_src = false);
 
 // DFT gradient (sfd_dft.cu)
 struct DftSet {             // variables transformed by one accumulation launch

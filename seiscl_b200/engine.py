@@ -154,7 +154,8 @@ class Config:
     #                        "register", "tma", "stream", "vector", "fused" ("fast" plus the fused
     #                        one-launch modelling step)
     adjoint_reset_psi: bool = False  # True: the adjoint starts from zeroed CPML memory (not the reference's)
-    field_precision: str = "fp32"  # "fp16": wave fields / memory variables stored in FP16 (3D, 2D P-SV forward)
+    field_precision: str = "fp32"  # "fp16": wave fields / memory variables stored in FP16 (3D, 2D P-SV;
+    #                                forward modelling and checkpointed gradients)
     back_prop_type: int = 1  # 1: boundary-saving backpropagation, 2: DFT gradient at `gradfreqs`
     gradfreqs: Sequence[float] = ()  # DFT gradient frequencies (Hz), back_prop_type 2
     loop_graphs: str = "auto"  # time loops as CUDA graphs: "auto" (from the 2nd run of a loop), "always", "never"

@@ -159,9 +159,10 @@ class SeisCL:
         device: ``with_docker``, ``with_mpi``, ``NP``, ``pref_device_type``,
         ``MPI_NPROC_SHOT``, ``nmax_dev``, ``no_use_GPUs`` (shots are spread
         over ranks by ``seiscl_b200.shots`` instead). ``FP16`` 2 or 3 stores
-        the saved boundaries in FP16 and, for 3D forward runs, the wave fields
-        and memory variables too (power-of-two scaled, as the reference's
-        FP16=2 mode); arithmetic is FP32 in every mode.
+        the saved boundaries in FP16 and, for forward runs of 3D and 2D P-SV
+        grids with L <= 3, the wave fields and memory variables too
+        (power-of-two scaled, as the reference's FP16=2 mode); arithmetic is
+        FP32 in every mode.
 
         ``files`` (no counterpart in the reference, which always uses files):
         True writes and reads the job files as HDF5 in ``workdir``; False
@@ -624,7 +625,8 @@ class SeisCL:
             tmin=self._steps(self.tmin), tmax=self._steps(self.tmax),
             param_type=int(self.param_type), restype=int(self.restype),
             precision="fp16" if int(self.FP16) >= 2 else "fp32",
-            field_precision="fp16" if int(self.FP16) >= 2 and int(self.ND) == 3 and not self.gradout else "fp32",
+            field_precision="fp16" if (int(self.FP16) >= 2 and int(self.ND) in (2, 3) and int(self.L) <= 3
+                                       and not self.gradout) else "fp32",
             back_prop_type=bpt, gradfreqs=freqs if bpt == 2 else (),
             hout=1 if (self.Hout and self.gradout) else 0)
 

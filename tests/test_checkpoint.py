@@ -115,6 +115,48 @@ def test_checkpoint_stores_in_half_precision(prec, cuda_device):
     assert nbytes == engine.footprint(ec, True, 1, 2 * len(acq["rec_pos"]))
 
 
+FP16_FIELD_CASES = [
+    (dict(nd=2, freesurf=1, L=0, abs_type=1, src_type=100, nt=200, seed=119), 25, "fp32"),
+    (dict(nd=2, freesurf=0, L=2, abs_type=1, src_type=100, nt=200, seed=120), 40, "fp16"),
+    (dict(nd=3, freesurf=1, L=0, abs_type=1, src_type=100, nz=36, ny=32, nx=36, nt=100, nab=8, seed=121), 25, "fp32"),
+    (dict(nd=3, freesurf=0, L=2, abs_type=1, src_type=2, nz=36, ny=32, nx=36, nt=100, nab=8, seed=122), 20, "bf16"),
+]
+# relative L2 of the gradient with FP16 wave fields against FP32 wave fields
+# (same checkpointing): the rounding of the stored fields carried through the
+# residuals and the correlation; measured on a B200 1.7e-4 - 5.5e-3
+FP16_FIELD_GRAD_TOL = 1e-2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw,K,prec", FP16_FIELD_CASES,
+                         ids=["2d_fs", "2d_visco_fp16store", "3d_fs", "3d_visco_bf16store"])
+def test_fp16_wave_fields_in_checkpointed_gradient(kw, K, prec, cuda_device):
+    """FP16 wave-field storage in the forward and recomputed runs of a
+    checkpointed gradient (the adjoint fields stay FP32 and read unscaled
+    parameters): the forward seismograms are those of an FP16 modelling run,
+    bit for bit; the gradient is within FP16_FIELD_GRAD_TOL of the one with
+    FP32 wave fields; the plan holds what ``sfd_footprint`` says."""
+    from seiscl_b200 import engine
+
+    cfg, model, acq = make_case(**kw)
+    outs = ["vx", "vy", "vz"] if cfg["nd"] == 3 else ["vx", "vz"]
+    _, g32, _ = _gradient(cfg, model, acq, outs, checkpoint=K, precision=prec)
+    dh, gh, nbytes = _gradient(cfg, model, acq, outs, checkpoint=K, precision=prec, field_precision="fp16")
+    plan = engine.Plan(dataclasses.replace(engine_config(cfg), field_precision="fp16"))
+    plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+    dm = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
+    plan.close()
+    for k in outs:
+        assert np.array_equal(dh[k], dm[k]), k
+    errs = {k: rel_l2(gh[k], g32[k]) for k in ("M", "mu", "rho")}
+    print("FP16 wave fields, checkpointed gradient vs FP32 fields:", errs)
+    for k, e in errs.items():
+        assert np.abs(g32[k]).max() > 0 and np.isfinite(gh[k]).all(), k
+        assert e < FP16_FIELD_GRAD_TOL, (k, e)
+    ec = dataclasses.replace(engine_config(cfg), checkpoint=K, precision=prec, field_precision="fp16")
+    assert nbytes == engine.footprint(ec, True, 1, len(outs) * len(acq["rec_pos"]))
+
+
 def test_checkpoint_configuration_checks():
     from seiscl_b200 import engine
 
@@ -123,7 +165,10 @@ def test_checkpoint_configuration_checks():
     f1 = engine.footprint(ok, True, 1, 20)
     f2 = engine.footprint(dataclasses.replace(ok, checkpoint=50), True, 1, 20)
     assert len({f0, f1, f2}) == 3
+    # FP16 wave fields: snapshots of half the bytes, plus the adjoint's unscaled parameters
+    fh = engine.footprint(dataclasses.replace(ok, field_precision="fp16"), True, 1, 20)
+    assert fh < f1
     for bad in (dict(checkpoint=-1), dict(checkpoint=5, back_prop_type=2), dict(checkpoint=5, ND=22, N=[40, 50]),
-                dict(checkpoint=5, batch=2)):
+                dict(checkpoint=5, batch=2), dict(checkpoint=5, field_precision="fp16", hout=1)):
         with pytest.raises(engine.SeisCLEngineError):
             engine.footprint(dataclasses.replace(ok, **bad), True, 1, 20)
