@@ -15,6 +15,8 @@
 //   boundary  src/savebnd{2D,3D}.cl, src/header_injectbnd.cl
 // Arithmetic is FP32 with FMA; gradients accumulate in FP64.
 #include <algorithm>
+#include <cstdlib>
+#include <utility>
 #include <type_traits>
 
 #include <cuda_bf16.h>
@@ -116,6 +118,16 @@ template <typename T> __device__ __forceinline__ float to_f(T v);
 template <> __device__ __forceinline__ float to_f<float>(float v) { return v; }
 template <> __device__ __forceinline__ float to_f<__half>(__half v) { return __half2float(v); }
 template <> __device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+// Programmatic dependent launch (the 3D modelling loop's kernels, see
+// pdl_enabled): a kernel launched with programmatic stream serialization may
+// be resident before the previous kernel of the stream has finished.
+// pdl_wait returns once that kernel has completed and its stores are
+// visible (at once for an ordinary launch); nothing it writes may be read,
+// and nothing at all written, before it.  pdl_trigger lets the next
+// kernel's CTAs launch once every CTA of this grid has passed it.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 template <typename T> __device__ __forceinline__ T from_f(float v);
 template <> __device__ __forceinline__ float from_f<float>(float v) { return v; }
 template <> __device__ __forceinline__ __half from_f<__half>(float v) { return __float2half_rn(v); }
@@ -842,8 +854,9 @@ __device__ __forceinline__ Q4 ldq_p(const float *p)
 template <int LP>
 __device__ __forceinline__ Q4 ldq_p(const __half *p)
 {
-    static_assert(LP == 0, "FP16 fields are read through the read-only path only");
-    return ldq(p);
+    static_assert(LP == 0 || LP == 1, "FP16 fields are read through the read-only path or plainly");
+    if constexpr (LP == 0) return ldq(p);
+    else return ldq_rw(p);
 }
 
 // forward / backward differences of four cells along a stride (x or y)
@@ -1145,9 +1158,21 @@ __global__ void __launch_bounds__(128) k_v3d_q4(Grid g, Fields f)
 // 256^3 L=2 on a B200.  5 CTAs (102 registers) is slower again, and a
 // component-at-a-time update with 80 registers slower still (0.37 ms): the
 // kernel is bound by the stencil loads each thread keeps in flight.
+// PDL: launched with programmatic stream serialization; the stresses then
+// come through plain loads (see k_s3d_q4_pf)
+// Taking the x planes in the reverse of the stress kernel's order (each
+// kernel starting on the planes the other has just written) was measured
+// and is not faster: 16.96 against 17.00 Gcell/s at 256^3, L=2.
+template <bool PDL = false>
 __global__ void __launch_bounds__(128, 4) k_v3d_q4_b4(Grid g, Fields f)
 {
-    v3d_q4<float, false>(g, f);
+    if constexpr (PDL) {
+        pdl_trigger();
+        pdl_wait();
+    }
+    constexpr bool MB = false;
+    CELL3D_Q4
+    v3d_q4_at<float, PDL ? 1 : 0>(g, f, gz0, gy, gx, iv, ip);
 }
 
 // ------------------------------------- velocity update staged by cp.async
@@ -1693,7 +1718,7 @@ __device__ __forceinline__ void s_shear_q4(const Grid &g, const Fields &f, int g
 // stress update of the quad (gz0..gz0+3, gy, gx); LP: load policy of the
 // velocity reads; surf: free surface folded in (see s_normal_q4); PF: first
 // ask L2 for the quad's per-cell streams
-template <int L, class T, int LP = 0, bool PF = false>
+template <int L, class T, int LP = 0, bool PF = false, bool PDL = false>
 __device__ __forceinline__ void s3d_q4_at(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip,
                                           bool surf = false)
 {
@@ -1713,6 +1738,9 @@ __device__ __forceinline__ void s3d_q4_at(const Grid &g, const Fields &f, int gz
 #pragma unroll
         for (int k = 0; k < np; k++) asm volatile("prefetch.global.L2 [%0];" ::"l"(f.p[pid[k]] + ip));
     }
+    // launched early (programmatic dependent launch): everything the
+    // previous kernels write is read from here on
+    if constexpr (PDL) pdl_wait();
     const T *Vx = fld<T>(f.w[VX]), *Vy = fld<T>(f.w[VY]), *Vz = fld<T>(f.w[VZ]);
     Q4 vzz = dbw_z<F>(ldw<T, LP>(Vz, iv), hc);
     Q4 vyz = dfw_z<F>(ldw<T, LP>(Vy, iv), hc);
@@ -1749,12 +1777,16 @@ __global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f, bool surf)
 // 0.651 ms against 0.695 for k_s3d_q4 (0.571 against 0.601 without
 // absorbing boundary); the prefetch at 4 CTAs per SM gave 0.674, 3 CTAs
 // without it 0.713.
-template <int L, class T>
+// PDL: launched with programmatic stream serialization (launch_pdl).  The
+// velocities then come through plain loads: a read-only-path (ld.global.nc)
+// load counts as invariant, and the compiler may move it above the wait.
+template <int L, class T, bool PDL = false>
 __global__ void __launch_bounds__(128, 3) k_s3d_q4_pf(Grid g, Fields f, bool surf)
 {
     constexpr bool MB = false;
+    if constexpr (PDL) pdl_trigger();
     CELL3D_Q4
-    s3d_q4_at<L, T, 0, true>(g, f, gz0, gy, gx, iv, ip, surf);
+    s3d_q4_at<L, T, PDL ? 1 : 0, true, PDL>(g, f, gz0, gy, gx, iv, ip, surf);
 }
 
 // ------------------------------------------------- fused 3D forward step
@@ -2427,6 +2459,49 @@ __global__ void __launch_bounds__(128, PF ? 3 : 4) k_adjs3d_q4(Grid g, Fields f,
 
 // true when the 4-cell kernels apply to this grid
 static inline bool q4_ok(const Grid &g) { return g.nd == 3 && g.F == 4 && g.nz % 4 == 0; }
+
+// Programmatic dependent launch for the single-shot 3D loop: the velocity
+// and stress kernels, the sources and the receivers are launched with
+// programmatic stream serialization, so each may be resident while the
+// previous one drains its last wave (and the stress kernel asks L2 for its
+// own streams meanwhile); every one of them waits (pdl_wait) before it
+// reads or writes anything the previous kernels touch, and reads those
+// fields with plain loads (a read-only-path load may be hoisted above the
+// wait).  256^3, L=2: 1.008 against 1.015 ms per step.  On unless the
+// environment sets SEISCL_B200_PDL=0.
+static bool pdl_enabled()
+{
+    static const bool on = [] {
+        const char *e = std::getenv("SEISCL_B200_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+static void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args &&...args)
+{
+    cudaLaunchConfig_t c = {};
+    c.gridDim = grid;
+    c.blockDim = block;
+    c.dynamicSmemBytes = 0;
+    c.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    c.attrs = at;
+    c.numAttrs = 1;
+    cudaLaunchKernelEx(&c, kernel, std::forward<Args>(args)...);
+}
+
+// kernel<<<grid, block, 0, st>>>(args...), with programmatic serialization when `pdl`
+template <typename... KArgs, typename... Args>
+static void launch_maybe_pdl(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
+                             Args &&...args)
+{
+    if (pdl) launch_pdl(kernel, grid, block, st, std::forward<Args>(args)...);
+    else kernel<<<grid, block, 0, st>>>(std::forward<Args>(args)...);
+}
 
 template <int F, int L, class T = float, bool MB = false>
 __global__ void __launch_bounds__(256, 2) k_s3d_stream(Grid g, Fields f)
@@ -3306,6 +3381,8 @@ template <class T = float>
 __global__ void k_sources(Fields f, PointSet s, const float *src, int nt_total, int t, int pdir, float dt,
                           int freesurf, int F, WScale ws)
 {
+    pdl_trigger();
+    pdl_wait();
     int gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid < s.n) source_point<T>(f, s, src, nt_total, t, pdir, dt, freesurf, F, ws, gid);
 }
@@ -3344,6 +3421,8 @@ __device__ __forceinline__ void record_point(const Fields &f, const PointSet &r,
 template <class T = float>
 __global__ void k_record(Fields f, PointSet r, float *out, int nt_total, int t, unsigned outmask, int nd, WScale ws)
 {
+    pdl_trigger();
+    pdl_wait();
     int gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid < r.n) record_point<T, false>(f, r, out, nt_total, t, outmask, nd, ws, gid);
 }
@@ -3496,6 +3575,7 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
             // 4, 0.284 for 8 x 2 x 8 and 0.34 for 4 x 8 x 4 quads x y x x
             const dim3 b = q4_block(g, 16, 4, 2), gr = q4_grid(g, b);
             if (g.nb > 1) k_v3d_q4<float, true><<<gr, b, 0, st>>>(g, f);
+            else if (pdl_enabled()) launch_pdl(k_v3d_q4_b4<true>, gr, b, st, g, f);
             else k_v3d_q4_b4<<<gr, b, 0, st>>>(g, f);
             return;
         }
@@ -3518,11 +3598,20 @@ bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_
         if (q4_ok(g)) {
             const dim3 b4 = q4_block(g, 16, 8, 1), g4 = q4_grid(g, b4);
             if (g.kernels == 0 && g.nb == 1 && g.L > 0) {   // with the stream prefetch, as the FP32 default
+                const bool pdl = pdl_enabled();
                 switch (g.L) {
-                case 0: k_s3d_q4_pf<0, __half><<<g4, b4, 0, st>>>(g, f, false); break;
-                case 1: k_s3d_q4_pf<1, __half><<<g4, b4, 0, st>>>(g, f, false); break;
-                case 2: k_s3d_q4_pf<2, __half><<<g4, b4, 0, st>>>(g, f, false); break;
-                default: k_s3d_q4_pf<3, __half><<<g4, b4, 0, st>>>(g, f, false); break;
+                case 0: if (pdl) launch_pdl(k_s3d_q4_pf<0, __half, true>, g4, b4, st, g, f, false);
+                        else k_s3d_q4_pf<0, __half><<<g4, b4, 0, st>>>(g, f, false);
+                        break;
+                case 1: if (pdl) launch_pdl(k_s3d_q4_pf<1, __half, true>, g4, b4, st, g, f, false);
+                        else k_s3d_q4_pf<1, __half><<<g4, b4, 0, st>>>(g, f, false);
+                        break;
+                case 2: if (pdl) launch_pdl(k_s3d_q4_pf<2, __half, true>, g4, b4, st, g, f, false);
+                        else k_s3d_q4_pf<2, __half><<<g4, b4, 0, st>>>(g, f, false);
+                        break;
+                default: if (pdl) launch_pdl(k_s3d_q4_pf<3, __half, true>, g4, b4, st, g, f, false);
+                         else k_s3d_q4_pf<3, __half><<<g4, b4, 0, st>>>(g, f, false);
+                         break;
                 }
                 return false;
             }
@@ -3563,11 +3652,20 @@ bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_
             // streams: 256^3, L=2: 0.654 ms against 0.706; elastic (L=0):
             // 0.376 against 0.366 without it.  kernels 5 keeps k_s3d_q4.
             if (g.nb == 1 && g.kernels == 0 && g.L > 0) {
+                const bool pdl = pdl_enabled();
                 switch (g.L) {
-                case 0: k_s3d_q4_pf<0, float><<<g4, b4, 0, st>>>(g, f, surf); break;
-                case 1: k_s3d_q4_pf<1, float><<<g4, b4, 0, st>>>(g, f, surf); break;
-                case 2: k_s3d_q4_pf<2, float><<<g4, b4, 0, st>>>(g, f, surf); break;
-                default: k_s3d_q4_pf<3, float><<<g4, b4, 0, st>>>(g, f, surf); break;
+                case 0: if (pdl) launch_pdl(k_s3d_q4_pf<0, float, true>, g4, b4, st, g, f, surf);
+                        else k_s3d_q4_pf<0, float><<<g4, b4, 0, st>>>(g, f, surf);
+                        break;
+                case 1: if (pdl) launch_pdl(k_s3d_q4_pf<1, float, true>, g4, b4, st, g, f, surf);
+                        else k_s3d_q4_pf<1, float><<<g4, b4, 0, st>>>(g, f, surf);
+                        break;
+                case 2: if (pdl) launch_pdl(k_s3d_q4_pf<2, float, true>, g4, b4, st, g, f, surf);
+                        else k_s3d_q4_pf<2, float><<<g4, b4, 0, st>>>(g, f, surf);
+                        break;
+                default: if (pdl) launch_pdl(k_s3d_q4_pf<3, float, true>, g4, b4, st, g, f, surf);
+                         else k_s3d_q4_pf<3, float><<<g4, b4, 0, st>>>(g, f, surf);
+                         break;
                 }
                 return surf;
             }
@@ -3803,20 +3901,22 @@ void launch_sources(const Grid &g, const Fields &f, const PointSet &s, const flo
                     int pdir, cudaStream_t st)
 {
     if (s.n == 0) return;
+    const bool pdl = g.nd == 3 && g.nb == 1 && pdl_enabled();
+    const dim3 gr(cdiv(s.n, 128)), b(128);
     if (g.fhalf)
-        k_sources<__half><<<cdiv(s.n, 128), 128, 0, st>>>(f, s, src, nt_total, t, pdir, g.dt, g.freesurf, g.F, g.ws);
+        launch_maybe_pdl(pdl, k_sources<__half>, gr, b, st, f, s, src, nt_total, t, pdir, g.dt, g.freesurf, g.F, g.ws);
     else
-        k_sources<float><<<cdiv(s.n, 128), 128, 0, st>>>(f, s, src, nt_total, t, pdir, g.dt, g.freesurf, g.F, g.ws);
+        launch_maybe_pdl(pdl, k_sources<float>, gr, b, st, f, s, src, nt_total, t, pdir, g.dt, g.freesurf, g.F, g.ws);
 }
 
 void launch_record(const Grid &g, const Fields &f, const PointSet &r, float *out, int nt_total, int t,
                    unsigned outmask, cudaStream_t st)
 {
     if (r.n == 0 || outmask == 0) return;
-    if (g.fhalf)
-        k_record<__half><<<cdiv(r.n, 128), 128, 0, st>>>(f, r, out, nt_total, t, outmask, g.nd, g.ws);
-    else
-        k_record<float><<<cdiv(r.n, 128), 128, 0, st>>>(f, r, out, nt_total, t, outmask, g.nd, g.ws);
+    const bool pdl = g.nd == 3 && g.nb == 1 && pdl_enabled();
+    const dim3 gr(cdiv(r.n, 128)), b(128);
+    if (g.fhalf) launch_maybe_pdl(pdl, k_record<__half>, gr, b, st, f, r, out, nt_total, t, outmask, g.nd, g.ws);
+    else launch_maybe_pdl(pdl, k_record<float>, gr, b, st, f, r, out, nt_total, t, outmask, g.nd, g.ws);
 }
 
 void launch_residuals(const Grid &g, const AdjFields &a, const PointSet &r, const float *res, int nt_total, int t,
