@@ -229,7 +229,7 @@ def build_workload_light(name):
     return w, None, None
 
 
-def algorithmic_bytes(w, state_bytes=4):
+def algorithmic_bytes(w, state_bytes=4, mem_bytes=None):
     """Minimum DRAM bytes of one time step of the two stencil kernels (FP32).
 
     Velocity kernel: read 6 stresses, read+write 3 velocities, read 3
@@ -254,10 +254,11 @@ def algorithmic_bytes(w, state_bytes=4):
         psi_cells_axis = 2 * nab * nz + nx * zlayers
         psi_v = 2 * psi_cells_axis
         psi_s = 2 * psi_cells_axis
-    sb = state_bytes  # bytes per stored wave-field / memory-variable value; parameters and psi stay FP32
+    sb = state_bytes  # bytes per stored wave-field value; parameters and psi stay FP32
+    mb = sb if mem_bytes is None else mem_bytes   # bytes per stored memory-variable value
     v_bytes = n * (sb * (ns + 2 * nv) + 4 * nv) + 8 * psi_v
-    s_bytes = n * (sb * (nv + 2 * ns + 2 * ns * L) + 4 * npar_s) + 8 * psi_s
-    fused = n * (sb * 2 * (nv + ns + ns * L) + 4 * (nv + npar_s)) + 8 * (psi_v + psi_s)
+    s_bytes = n * (sb * (nv + 2 * ns) + mb * 2 * ns * L + 4 * npar_s) + 8 * psi_s
+    fused = n * (sb * 2 * (nv + ns) + mb * 2 * ns * L + 4 * (nv + npar_s)) + 8 * (psi_v + psi_s)
     return dict(v=v_bytes, s=s_bytes, fused=fused, cells=n)
 
 
@@ -409,6 +410,8 @@ def run_gradient(args):
         B = 1   # checkpointed gradients run one shot per launch
     elif args.fields == "fp16":
         raise SystemExit("FP16 wave fields in a gradient need --checkpoint K")
+    if args.fields == "fp16_mem":
+        raise SystemExit("FP16 memory variables cover forward modelling only")
     nuse = (args.warmup + args.steps) * B
     w, true, start, shots = build_gradient_workload(args.workload, nuse, grid=args.grid)
     if args.nt > 0:
@@ -640,8 +643,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="visco3d",
                     choices=sorted(WORKLOADS) + sorted(GRADIENT_WORKLOADS) + ["serving"])
-    ap.add_argument("--fields", default="fp32", choices=["fp32", "fp16"],
-                    help="storage of wave fields and memory variables (arithmetic is FP32 either way)")
+    ap.add_argument("--fields", default="fp32", choices=["fp32", "fp16", "fp16_mem"],
+                    help="storage of wave fields and memory variables (arithmetic is FP32 either way); "
+                         "fp16_mem: memory variables alone in FP16")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: request arrival rate (1/s)")
     ap.add_argument("--workers", type=int, default=4, help="serving: worker threads")
     ap.add_argument("--no-plain", action="store_true", help="serving: skip the plain one-at-a-time arm")
@@ -719,7 +723,7 @@ def main():
     # (velocity + stress + free surface in one launch per step), else the
     # dominant stress update
     kv, ks, ksurf, kfused = plan.bench_kernels(args.kernel_reps)
-    ab = algorithmic_bytes(w, 2 if args.fields == "fp16" else 4)
+    ab = algorithmic_bytes(w, 2 if args.fields == "fp16" else 4, 2 if args.fields != "fp32" else 4)
     peak, peak_kind = measured_peaks()
     s_gbs = ab["s"] / (ks / 1e3) / 1e9
     v_gbs = ab["v"] / (kv / 1e3) / 1e9
@@ -734,7 +738,8 @@ def main():
     skern = "stress update, %s%s (%s)" % ({"vector": "4-cell vectorised", "tma": "TMA-pipelined",
                                            "stream": "streaming", "register": "register-blocked",
                                            "general": "general", "2d": "general 2D"}[fam],
-                                          ", FP16 storage" if args.fields == "fp16" else "", kname)
+                                          {"fp16": ", FP16 storage", "fp16_mem": ", FP16 memory variables"}.get(
+                                              args.fields, ""), kname)
     if fused:
         kname = "k_fused3d_q4<%d>" % w["L"]
         skern = "fused 3D step: velocity, stress, memory variables, free surface (%s)" % kname
@@ -746,7 +751,7 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "traffic_%s.json" % args.workload)
     if os.path.exists(tpath):
         # DRAM bytes per launch of the kernel that ran, from an ncu capture
-        key = kname if args.fields == "fp32" else kname + ",fp16"
+        key = kname if args.fields == "fp32" else kname + "," + args.fields
         traffic = json.load(open(tpath)).get("stress_kernel_bytes_per_launch", {}).get(key)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

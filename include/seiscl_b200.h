@@ -102,7 +102,10 @@ typedef struct sfd_config {
                               scaled by powers of two per shot (forward modelling of 3D
                               and 2D P-SV grids, L <= 3, and the forward and recomputed
                               runs of a checkpointed gradient, whose adjoint fields stay
-                              FP32; arithmetic stays FP32).  No reference counterpart
+                              FP32; arithmetic stays FP32); 2: memory variables alone
+                              in FP16, times a power of two set per shot, wave fields
+                              FP32 (3D viscoelastic forward modelling, FDORDER 8, NZ a
+                              multiple of 4, kernels 0, batch 1).  No reference counterpart
                               in this form: the reference's FP16=2 mode also scales
                               by powers of two (src/assign_modeling_case.c:829-866). */
     int back_prop_type;    /* BACK_PROP_TYPE: 0 or 1 boundary-saving backpropagation,

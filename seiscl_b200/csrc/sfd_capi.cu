@@ -215,6 +215,7 @@ int upload_shot(sfd_plan *p, const sfd_shot *shot, int mask, PointSet &S, PointS
 
 // bytes per stored wave-field / memory-variable value
 size_t wave_elem(const Grid &g) { return g.fhalf ? 2 : sizeof(float); }
+size_t mem_elem(const Grid &g) { return g.fhalf || g.rhalf ? 2 : sizeof(float); }
 
 // CPML memory arrays of a grid (0: unused); returns the floats of their
 // 256-byte aligned spans
@@ -250,7 +251,7 @@ int alloc_model(sfd_plan *p)
     for (int r = 0; r < NR; r++) {
         p->f.r[r] = nullptr;
         if (!is_mem_used(g, r)) continue;
-        p->f.r[r] = (float *)dalloc(p, wave_elem(g) * g.nvol * g.L * p->batch, &e);
+        p->f.r[r] = (float *)dalloc(p, mem_elem(g) * g.nvol * g.L * p->batch, &e);
         if (e) return fail(p, SFD_ERR_MEMORY, "memory-variable allocation failed");
     }
     int64_t tot = psi_sizes(g, p->psi_size);
@@ -324,7 +325,7 @@ int zero_forward_state(sfd_plan *p, cudaStream_t st)
     for (int w = 0; w < NW; w++)
         if (p->f.w[w]) CKC(cudaMemsetAsync(p->f.w[w], 0, wave_elem(g) * g.nvol * nb, st));
     for (int r = 0; r < NR; r++)
-        if (p->f.r[r]) CKC(cudaMemsetAsync(p->f.r[r], 0, wave_elem(g) * g.nvol * g.L * nb, st));
+        if (p->f.r[r]) CKC(cudaMemsetAsync(p->f.r[r], 0, mem_elem(g) * g.nvol * g.L * nb, st));
     int64_t tot = 0;
     for (int i = 0; i < NPSI; i++) tot += psi_span(p->psi_size[i]);
     if (tot) CKC(cudaMemsetAsync(p->d_psi_all, 0, sizeof(float) * tot * nb, st));
@@ -944,7 +945,12 @@ int check_config(const sfd_config &c)
     if (c.precision < 0 || c.precision > 2) return SFD_ERR_ARG;
     if (c.kernels < 0 || c.kernels > 7) return SFD_ERR_ARG;
     if (c.adjoint_reset_psi < 0 || c.adjoint_reset_psi > 1) return SFD_ERR_ARG;
-    if (c.field_precision < 0 || c.field_precision > 1) return SFD_ERR_ARG;
+    if (c.field_precision < 0 || c.field_precision > 2) return SFD_ERR_ARG;
+    // FP16 memory variables with FP32 wave fields: the 4-cell stress kernel
+    // of single-shot 3D viscoelastic modelling
+    if (c.field_precision == 2 && (c.nd != 3 || c.L < 1 || c.L > 3 || c.fdorder != 8 || c.n[0] % 4 ||
+                                   c.kernels != 0 || c.batch > 1 || c.checkpoint > 0 || c.hout))
+        return SFD_ERR_UNSUPPORTED;
     // 16-bit fields: 3D (L <= 3, the 4-cell and streaming kernels) and 2D P-SV
     if (c.field_precision == 1 && ((c.nd != 3 && c.nd != 2) || c.L > 3)) return SFD_ERR_UNSUPPORTED;
     if (c.back_prop_type < 0 || c.back_prop_type > 2) return SFD_ERR_ARG;
@@ -1002,6 +1008,8 @@ void init_grid(const sfd_config &c, Grid &g)
     }
     g.inv_dt = 1.0f / c.dt;
     g.fhalf = c.field_precision == 1;
+    g.rhalf = c.field_precision == 2;
+    g.rsc = g.rsci = 1.0f;
     for (int w = 0; w < NW; w++) g.ws.w[w] = g.bsc[w] = g.bsci[w] = 1.0f;
     g.nbnd = nbnd_cells(g.nd, g.nz, g.ny, g.nx, g.F, g.nab, g.freesurf);
     g.nb = 1;
@@ -1087,7 +1095,8 @@ extern "C" int sfd_footprint(const sfd_config *cfg, int gradient, int nsrc, int6
     int64_t psz[NPSI];
     const int64_t nc = std::max(2 * g.nab, 1);
     const int64_t B = std::max(1, cfg->batch);   // copies of the per-shot arrays
-    int64_t b = B * ((int64_t)wave_elem(g) * g.nvol * (nwave + (int64_t)nmem * g.L) + 4 * psi_sizes(g, psz)) +
+    int64_t b = B * ((int64_t)wave_elem(g) * g.nvol * nwave + (int64_t)mem_elem(g) * g.nvol * nmem * g.L +
+                     4 * psi_sizes(g, psz)) +
                 4 * npar * NPAR + 4 * (3 * NC * nc + nc + 6 * nc);
     // ensure_shot_buffers: source maps and signatures, receiver maps, seismograms and residuals
     const int64_t cs = std::max<int64_t>(nsrc, 16), cr = std::max<int64_t>(nrec_sel, 16);
@@ -1306,6 +1315,16 @@ extern "C" int sfd_forward_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
         store_exponents(p->kshift, a, b);
         for (int w = 0; w < NW; w++) p->g.ws.w[w] = std::ldexp(1.0f, w <= VZ ? b : a);
     }
+    if (g.rhalf) {
+        // FP16 memory variables: stored times the stress scale FP16 wave
+        // fields would take (about 2^4 injected per step for explosive sources)
+        if (save_boundaries)
+            return fail(p, SFD_ERR_UNSUPPORTED, "FP16 memory variables cover forward modelling only");
+        int a, b;
+        store_exponents(p->bshift, a, b);
+        p->g.rsc = std::ldexp(1.0f, a);
+        p->g.rsci = std::ldexp(1.0f, -a);
+    }
     for (int w = 0; w < NW; w++) p->g.bsc[w] = p->g.bsci[w] = 1.0f;
     if (save_boundaries && p->cfg.precision == SFD_PREC_FP16) {
         // without a scale, velocities (~stress / impedance) fall below FP16's range
@@ -1461,6 +1480,7 @@ extern "C" int sfd_adjoint_batch(sfd_plan *p, int nshot, const sfd_shot *shots, 
         return fail(p, SFD_ERR_UNSUPPORTED, "the adjoint path covers P-SV and 3D elastic/viscoelastic media");
     if (p->g.fhalf && p->cfg.checkpoint <= 0)
         return fail(p, SFD_ERR_UNSUPPORTED, "FP16 wave-field storage covers forward modelling and checkpointed gradients");
+    if (p->g.rhalf) return fail(p, SFD_ERR_UNSUPPORTED, "FP16 memory variables cover forward modelling only");
     if (!p->have_forward) return fail(p, SFD_ERR_STATE, "sfd_adjoint needs a preceding sfd_forward with saved boundaries");
     if (nshot != p->fwd_nb) return fail(p, SFD_ERR_STATE, "the adjoint must follow a forward run of the same shots");
     if (p->g.freesurf && p->surf_mu_zero)
@@ -1771,6 +1791,7 @@ extern "C" int64_t sfd_debug_copy(sfd_plan *p, int kind, int id, float *dst, int
     const void *src = nullptr;
     int64_t n = 0;
     if (g.fhalf && kind >= 0 && kind <= 2) return fail(p, SFD_ERR_UNSUPPORTED, "wave fields are stored in FP16");
+    if (g.rhalf && kind == 2) return fail(p, SFD_ERR_UNSUPPORTED, "memory variables are stored in FP16");
     if (kind == 0 && id >= 0 && id < NW) { src = p->f.w[id]; n = g.nvol; }
     else if (kind == 1 && id >= 0 && id < NW) { src = p->a.wr[id]; n = g.nvol; }
     else if (kind == 2 && id >= 0 && id < NR) { src = p->f.r[id]; n = g.nvol * g.L; }
@@ -1798,6 +1819,7 @@ extern "C" int64_t sfd_debug_load(sfd_plan *p, int kind, int id, const float *sr
     if (!p->model_set) return fail(p, SFD_ERR_STATE, "sfd_set_model must be called first");
     const Grid &g = p->g;
     if (g.fhalf) return fail(p, SFD_ERR_UNSUPPORTED, "wave fields are stored in FP16");
+    if (g.rhalf && kind == 2) return fail(p, SFD_ERR_UNSUPPORTED, "memory variables are stored in FP16");
     int rc;
     if (kind == 1 && (rc = alloc_adjoint(p))) return rc;
     void *dst = nullptr;

@@ -57,6 +57,8 @@ struct Grid {
     float eta_b[8], eta_c[8];  // 1/(1+eta/2) and 1-eta/2, FP32 as the kernels would form them
     float inv_dt;           // 1/dt rounded to FP32
     int fhalf;              // 1: wave fields and memory variables stored in FP16 (3D forward)
+    int rhalf;              // 1: memory variables alone stored in FP16, times rsc (3D forward)
+    float rsc, rsci;        // that scale (a power of two, set per shot) and its inverse
     WScale ws;              // storage scale per wave field (all 1 for FP32)
     float bsc[NW], bsci[NW];  // saved-boundary store scale per wave field and its inverse
                               // (powers of two for FP16 stores, 1 otherwise)

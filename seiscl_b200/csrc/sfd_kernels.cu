@@ -859,6 +859,31 @@ __device__ __forceinline__ Q4 ldq_p(const __half *p)
     else return ldq_rw(p);
 }
 
+// memory variables of four cells in storage type TR: with TR FP16 under
+// FP32 wave fields (Grid::rhalf) they are stored times g.rsc
+template <class T, class TR>
+__device__ __forceinline__ Q4 ldr_q(const Grid &g, const TR *p)
+{
+    Q4 r = ldq_rw(p);
+    if constexpr (!std::is_same<T, TR>::value) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) r.v[j] *= g.rsci;
+    }
+    return r;
+}
+template <class T, class TR>
+__device__ __forceinline__ void str_q(const Grid &g, TR *p, const Q4 &q)
+{
+    if constexpr (!std::is_same<T, TR>::value) {
+        Q4 r;
+#pragma unroll
+        for (int j = 0; j < 4; j++) r.v[j] = q.v[j] * g.rsc;
+        stq(p, r);
+    } else {
+        stq(p, q);
+    }
+}
+
 // forward / backward differences of four cells along a stride (x or y)
 template <int F, class T, int LP = 0>
 __device__ __forceinline__ Q4 dfw_q(const T *__restrict__ v, i64 i, i64 st, const float *hc)
@@ -1517,12 +1542,12 @@ __device__ __forceinline__ void cpml_s3d_q4(const Grid &g, const Fields &f, int 
 // forms them) and writes the images szz(F-m) = -szz(F+m) for m = 1..3 and
 // sxz(F-m) = -sxz(F+m-1), syz(F-m) = -syz(F+m-1) for m = 1..4; the quad at
 // gz0 = F+4 writes szz(F-4) = -szz(F+4).
-template <int L, class T>
+template <int L, class T, class TR = T>
 __device__ __forceinline__ void s_normal_q4(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip,
                                             const Q4 &vxx, const Q4 &vyy, const Q4 &vzz, bool surf = false)
 {
     T *const ws[3] = {fld<T>(f.w[SXX]), fld<T>(f.w[SYY]), fld<T>(f.w[SZZ])};
-    T *const wr[3] = {fld<T>(f.r[RXX]), fld<T>(f.r[RYY]), fld<T>(f.r[RZZ])};
+    TR *const wr[3] = {fld<TR>(f.r[RXX]), fld<TR>(f.r[RYY]), fld<TR>(f.r[RZZ])};
     Q4 sq[3];
 #pragma unroll
     for (int q = 0; q < 3; q++) sq[q] = ldq_rw(ws[q] + iv);
@@ -1545,7 +1570,7 @@ __device__ __forceinline__ void s_normal_q4(const Grid &g, const Fields &f, int 
 #pragma unroll
         for (int l = 0; l < L; l++)
 #pragma unroll
-            for (int q = 0; q < 3; q++) rq[q][l] = ldq_rw(wr[q] + l * g.nvol + iv);
+            for (int q = 0; q < 3; q++) rq[q][l] = ldr_q<T>(g, wr[q] + l * g.nvol + iv);
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             float vxxyyzz = vxx.v[j] + vyy.v[j] + vzz.v[j], vyyzz = vyy.v[j] + vzz.v[j];
@@ -1629,18 +1654,18 @@ __device__ __forceinline__ void s_normal_q4(const Grid &g, const Fields &f, int 
 #pragma unroll
         for (int l = 0; l < L; l++)
 #pragma unroll
-            for (int q = 0; q < 3; q++) stq(wr[q] + l * g.nvol + iv, rq[q][l]);
+            for (int q = 0; q < 3; q++) str_q<T>(g, wr[q] + l * g.nvol + iv, rq[q][l]);
     }
 #pragma unroll
     for (int q = 0; q < 3; q++) stq(ws[q] + iv, sq[q]);
 }
 
-template <int L, class T>
+template <int L, class T, class TR = T>
 __device__ __forceinline__ void s_shear_q4(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip,
                                            const Q4 &vxyyx, const Q4 &vyzzy, const Q4 &vxzzx, bool surf = false)
 {
     T *const ws[3] = {fld<T>(f.w[SXY]), fld<T>(f.w[SYZ]), fld<T>(f.w[SXZ])};
-    T *const wr[3] = {fld<T>(f.r[RXY]), fld<T>(f.r[RYZ]), fld<T>(f.r[RXZ])};
+    TR *const wr[3] = {fld<TR>(f.r[RXY]), fld<TR>(f.r[RYZ]), fld<TR>(f.r[RXZ])};
     Q4 sq[3];
 #pragma unroll
     for (int q = 0; q < 3; q++) sq[q] = ldq_rw(ws[q] + iv);
@@ -1659,7 +1684,7 @@ __device__ __forceinline__ void s_shear_q4(const Grid &g, const Fields &f, int g
 #pragma unroll
         for (int l = 0; l < L; l++)
 #pragma unroll
-            for (int q = 0; q < 3; q++) rq[q][l] = ldq_rw(wr[q] + l * g.nvol + iv);
+            for (int q = 0; q < 3; q++) rq[q][l] = ldr_q<T>(g, wr[q] + l * g.nvol + iv);
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const float lmuipkp = qmuipkp.v[j], lmuipjp = qmuipjp.v[j], lmujpkp = qmujpkp.v[j];
@@ -1693,7 +1718,7 @@ __device__ __forceinline__ void s_shear_q4(const Grid &g, const Fields &f, int g
 #pragma unroll
         for (int l = 0; l < L; l++)
 #pragma unroll
-            for (int q = 0; q < 3; q++) stq(wr[q] + l * g.nvol + iv, rq[q][l]);
+            for (int q = 0; q < 3; q++) str_q<T>(g, wr[q] + l * g.nvol + iv, rq[q][l]);
     }
     if (g.abs_type == 2) {
 #pragma unroll
@@ -1718,7 +1743,7 @@ __device__ __forceinline__ void s_shear_q4(const Grid &g, const Fields &f, int g
 // stress update of the quad (gz0..gz0+3, gy, gx); LP: load policy of the
 // velocity reads; surf: free surface folded in (see s_normal_q4); PF: first
 // ask L2 for the quad's per-cell streams
-template <int L, class T, int LP = 0, bool PF = false, bool PDL = false>
+template <int L, class T, int LP = 0, bool PF = false, bool PDL = false, class TR = T>
 __device__ __forceinline__ void s3d_q4_at(const Grid &g, const Fields &f, int gz0, int gy, int gx, i64 iv, i64 ip,
                                           bool surf = false)
 {
@@ -1732,7 +1757,7 @@ __device__ __forceinline__ void s3d_q4_at(const Grid &g, const Fields &f, int gz
         for (int l = 0; l < L; l++)
 #pragma unroll
             for (int q = 0; q < NR; q++)
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(fld<T>(f.r[q]) + l * g.nvol + iv));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(fld<TR>(f.r[q]) + l * g.nvol + iv));
         constexpr int np = L > 0 ? 10 : 5;
         constexpr int pid[10] = {PM, PMU, PMUIPJP, PMUJPKP, PMUIPKP, PTAUP, PTAUS, PTAUSIPJP, PTAUSJPKP, PTAUSIPKP};
 #pragma unroll
@@ -1756,8 +1781,8 @@ __device__ __forceinline__ void s3d_q4_at(const Grid &g, const Fields &f, int gz
         vyzzy.v[j] = vyz.v[j] + vzy.v[j];
         vxzzx.v[j] = vxz.v[j] + vzx.v[j];
     }
-    s_normal_q4<L, T>(g, f, gz0, gy, gx, iv, ip, vxx, vyy, vzz, surf);
-    s_shear_q4<L, T>(g, f, gz0, gy, gx, iv, ip, vxyyx, vyzzy, vxzzx, surf);
+    s_normal_q4<L, T, TR>(g, f, gz0, gy, gx, iv, ip, vxx, vyy, vzz, surf);
+    s_shear_q4<L, T, TR>(g, f, gz0, gy, gx, iv, ip, vxyyx, vyzzy, vxzzx, surf);
 }
 
 // surf: the free surface of the step applied in the same launch (single-shot
@@ -1780,13 +1805,15 @@ __global__ void __launch_bounds__(128, 4) k_s3d_q4(Grid g, Fields f, bool surf)
 // PDL: launched with programmatic stream serialization (launch_pdl).  The
 // velocities then come through plain loads: a read-only-path (ld.global.nc)
 // load counts as invariant, and the compiler may move it above the wait.
-template <int L, class T, bool PDL = false>
+// TR: storage type of the memory variables (FP16 under FP32 wave fields
+// with Grid::rhalf)
+template <int L, class T, bool PDL = false, class TR = T>
 __global__ void __launch_bounds__(128, 3) k_s3d_q4_pf(Grid g, Fields f, bool surf)
 {
     constexpr bool MB = false;
     if constexpr (PDL) pdl_trigger();
     CELL3D_Q4
-    s3d_q4_at<L, T, PDL ? 1 : 0, true, PDL>(g, f, gz0, gy, gx, iv, ip, surf);
+    s3d_q4_at<L, T, PDL ? 1 : 0, true, PDL, TR>(g, f, gz0, gy, gx, iv, ip, surf);
 }
 
 // ------------------------------------------------- fused 3D forward step
@@ -2590,7 +2617,9 @@ __global__ void __launch_bounds__(256, 2) k_s3d_stream(Grid g, Fields f)
 }
 
 // free surface 3D, one thread per (y, x) column (surface3D.cl:39-271)
-template <int F, class T = float>
+// TR: storage type of the memory variables; values are read times
+// g.rsci and stored times g.rsc (1 except with Grid::rhalf)
+template <int F, class T = float, class TR = T>
 __global__ void k_surf3d(Grid g, Fields f, int pdir)
 {
     SHOT_F
@@ -2603,7 +2632,7 @@ __global__ void k_surf3d(Grid g, Fields f, int pdir)
     i64 ip = ((i64)(gx - F) * g.ny + (gy - F)) * g.nz + (gz - F);
     T *sxx = fld<T>(f.w[SXX]), *syy = fld<T>(f.w[SYY]), *szz = fld<T>(f.w[SZZ]), *syz = fld<T>(f.w[SYZ]),
       *sxz = fld<T>(f.w[SXZ]);
-    T *rxx = fld<T>(f.r[RXX]), *ryy = fld<T>(f.r[RYY]), *rzz = fld<T>(f.r[RZZ]);
+    TR *rxx = fld<TR>(f.r[RXX]), *ryy = fld<TR>(f.r[RYY]), *rzz = fld<TR>(f.r[RZZ]);
     stv(szz + iv, 0.0f);
     for (int l = 0; l < L; l++) stv(rzz + l * g.nvol + iv, 0.0f);
 #pragma unroll
@@ -2647,7 +2676,10 @@ __global__ void k_surf3d(Grid g, Fields f, int pdir)
         float gm = M * (1.0f + L * taup);
         float h = -((gm - fm) * (gm - fm) * (vxx + vyy) / gm) - ((gm - fm) * vzz);
         float sumx = 0, sumy = 0;
-        for (int l = 0; l < L; l++) { sumx += ldv(rxx + l * g.nvol + iv); sumy += ldv(ryy + l * g.nvol + iv); }
+        for (int l = 0; l < L; l++) {
+            sumx += ldv(rxx + l * g.nvol + iv) * g.rsci;
+            sumy += ldv(ryy + l * g.nvol + iv) * g.rsci;
+        }
         stv(sxx + iv, ldv(sxx + iv) + pdir * (h - g.dt2 * sumx));
         stv(syy + iv, ldv(syy + iv) + pdir * (h - g.dt2 * sumy));
         float d = 2.0f * mu * taus / g.dt, e = M * taup / g.dt;
@@ -2655,9 +2687,9 @@ __global__ void k_surf3d(Grid g, Fields f, int pdir)
         for (int l = 0; l < L; l++) {
             float b = g.eta[l] / (1.0f + g.eta[l] * 0.5f);
             float hh = b * (((d - e) * ((fm / gm) - 1.0f) * (vxx + vyy)) - ((d - e) * vzz));
-            float rx = ldv(rxx + l * g.nvol + iv) + hh, ry = ldv(ryy + l * g.nvol + iv) + hh;
-            stv(rxx + l * g.nvol + iv, rx);
-            stv(ryy + l * g.nvol + iv, ry);
+            float rx = ldv(rxx + l * g.nvol + iv) * g.rsci + hh, ry = ldv(ryy + l * g.nvol + iv) * g.rsci + hh;
+            stv(rxx + l * g.nvol + iv, rx * g.rsc);
+            stv(ryy + l * g.nvol + iv, ry * g.rsc);
             sumx += rx; sumy += ry;
         }
         stv(sxx + iv, ldv(sxx + iv) + g.dt2 * sumx);
@@ -3592,6 +3624,14 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
     }
 }
 
+// the FP32 stream-prefetch stress kernel; TR: storage type of the memory variables
+template <int L, class TR>
+static void launch_s_pf(const Grid &g, const Fields &f, dim3 g4, dim3 b4, cudaStream_t st, bool surf, bool pdl)
+{
+    if (pdl) launch_pdl(k_s3d_q4_pf<L, float, true, TR>, g4, b4, st, g, f, surf);
+    else k_s3d_q4_pf<L, float, false, TR><<<g4, b4, 0, st>>>(g, f, surf);
+}
+
 bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_surface)
 {
     if (g.fhalf && g.nd == 3 && g.L <= 3) {   // FP16 storage: the vectorised or the streaming kernels
@@ -3654,17 +3694,15 @@ bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_
             if (g.nb == 1 && g.kernels == 0 && g.L > 0) {
                 const bool pdl = pdl_enabled();
                 switch (g.L) {
-                case 0: if (pdl) launch_pdl(k_s3d_q4_pf<0, float, true>, g4, b4, st, g, f, surf);
-                        else k_s3d_q4_pf<0, float><<<g4, b4, 0, st>>>(g, f, surf);
+                case 0: launch_s_pf<0, float>(g, f, g4, b4, st, surf, pdl); break;
+                case 1: if (g.rhalf) launch_s_pf<1, __half>(g, f, g4, b4, st, surf, pdl);
+                        else launch_s_pf<1, float>(g, f, g4, b4, st, surf, pdl);
                         break;
-                case 1: if (pdl) launch_pdl(k_s3d_q4_pf<1, float, true>, g4, b4, st, g, f, surf);
-                        else k_s3d_q4_pf<1, float><<<g4, b4, 0, st>>>(g, f, surf);
+                case 2: if (g.rhalf) launch_s_pf<2, __half>(g, f, g4, b4, st, surf, pdl);
+                        else launch_s_pf<2, float>(g, f, g4, b4, st, surf, pdl);
                         break;
-                case 2: if (pdl) launch_pdl(k_s3d_q4_pf<2, float, true>, g4, b4, st, g, f, surf);
-                        else k_s3d_q4_pf<2, float><<<g4, b4, 0, st>>>(g, f, surf);
-                        break;
-                default: if (pdl) launch_pdl(k_s3d_q4_pf<3, float, true>, g4, b4, st, g, f, surf);
-                         else k_s3d_q4_pf<3, float><<<g4, b4, 0, st>>>(g, f, surf);
+                default: if (g.rhalf) launch_s_pf<3, __half>(g, f, g4, b4, st, surf, pdl);
+                         else launch_s_pf<3, float>(g, f, g4, b4, st, surf, pdl);
                          break;
                 }
                 return surf;
@@ -3781,6 +3819,7 @@ void launch_surface(const Grid &g, const Fields &f, int pdir, cudaStream_t st)
     if (g.nd == 3) {
         dim3 b(32, 4), gr(cdiv(g.ny, 32), cdiv(g.nx, 4), g.nb);
         if (g.fhalf) DISPATCH_F(g.F, k_surf3d<FF, __half><<<gr, b, 0, st>>>(g, f, pdir))
+        else if (g.rhalf) DISPATCH_F(g.F, (k_surf3d<FF, float, __half><<<gr, b, 0, st>>>(g, f, pdir)))
         else DISPATCH_F(g.F, k_surf3d<FF><<<gr, b, 0, st>>>(g, f, pdir))
     } else {
         if (g.fhalf) DISPATCH_F(g.F, k_surf2d<FF, __half><<<dim3(cdiv(g.nx, 128), 1, g.nb), 128, 0, st>>>(g, f, pdir))

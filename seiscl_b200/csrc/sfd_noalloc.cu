@@ -97,7 +97,10 @@ extern "C" int sfd_forward_noalloc(sfd_plan *p, const float *src_pos, const floa
 {
     if (!p) return SFD_ERR_ARG;
     if (!p->model_set) { p->err = "sfd_set_model must be called first"; return SFD_ERR_STATE; }
-    if (p->g.fhalf) { p->err = "sfd_forward_noalloc runs FP32 wave fields only"; return SFD_ERR_UNSUPPORTED; }
+    if (p->g.fhalf || p->g.rhalf) {
+        p->err = "sfd_forward_noalloc runs FP32 wave fields and memory variables only";
+        return SFD_ERR_UNSUPPORTED;
+    }
     if (nsrc < 0 || nrec < 0 || (nsrc && (!src_pos || !src)) || (nrec && !rec_pos)) {
         p->err = "invalid shot arrays";
         return SFD_ERR_ARG;

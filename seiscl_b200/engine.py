@@ -155,7 +155,8 @@ class Config:
     #                        one-launch modelling step)
     adjoint_reset_psi: bool = False  # True: the adjoint starts from zeroed CPML memory (not the reference's)
     field_precision: str = "fp32"  # "fp16": wave fields / memory variables stored in FP16 (3D, 2D P-SV;
-    #                                forward modelling and checkpointed gradients)
+    #                                forward modelling and checkpointed gradients); "fp16_mem": memory
+    #                                variables alone in FP16 (3D viscoelastic forward modelling)
     back_prop_type: int = 1  # 1: boundary-saving backpropagation, 2: DFT gradient at `gradfreqs`
     gradfreqs: Sequence[float] = ()  # DFT gradient frequencies (Hz), back_prop_type 2
     loop_graphs: str = "auto"  # time loops as CUDA graphs: "auto" (from the 2nd run of a loop), "always", "never"
@@ -197,7 +198,7 @@ class Config:
         c.adjoint_reset_psi = 1 if self.adjoint_reset_psi else 0
         c.batch = int(self.batch)
         c.checkpoint = int(self.checkpoint)
-        c.field_precision = {"fp32": 0, "fp16": 1}[self.field_precision]
+        c.field_precision = {"fp32": 0, "fp16": 1, "fp16_mem": 2}[self.field_precision]
         c.back_prop_type = int(self.back_prop_type)
         c.loop_graphs = {"auto": 0, "always": 1, "never": 2}[self.loop_graphs]
         c.hout = int(self.hout)

@@ -4,6 +4,8 @@ import glob
 import os
 import re
 
+import pytest
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -58,6 +60,23 @@ def test_invalid_configs_rejected():
         h = C.c_void_p()
         rc = lib.sfd_plan_create(C.byref(c), C.byref(h))
         assert rc in (-1, -7), bad
+
+
+def test_fp16_memory_variable_configs():
+    """FP16 memory variables under FP32 wave fields: 3D viscoelastic, 8th
+    order, NZ a multiple of 4, default kernels, one shot, no checkpointing;
+    they halve the memory variables' bytes and nothing else."""
+    import dataclasses
+
+    from seiscl_b200.engine import Config, SeisCLEngineError, footprint
+
+    ok = Config(N=[40, 36, 44], ND=3, NT=50, L=2, nab=8, field_precision="fp16_mem")
+    f32, f16 = footprint(dataclasses.replace(ok, field_precision="fp32")), footprint(ok)
+    assert f32 - f16 == (40 + 8) * (36 + 8) * (44 + 8) * 6 * 2 * 2   # padded cells x 6 variables x L x 2 bytes
+    for bad in (dict(ND=2, N=[40, 44]), dict(L=0), dict(FDORDER=4), dict(N=[42, 36, 44]), dict(kernels="general"),
+                dict(batch=2), dict(checkpoint=10)):
+        with pytest.raises(SeisCLEngineError):
+            footprint(dataclasses.replace(ok, **bad))
 
 
 def test_tma_map_cache_is_thread_safe():

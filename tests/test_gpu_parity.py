@@ -325,6 +325,57 @@ def test_fp16_field_storage_against_fp32(kw, cuda_device):
     assert num / den < 1e-3, num / den
 
 
+FP16_MEM_CASES = [
+    dict(nd=3, freesurf=1, L=2, abs_type=1, src_type=2, nz=40, ny=36, nx=44, nt=150, nab=8, seed=84),
+    dict(nd=3, freesurf=0, L=1, abs_type=2, src_type=100, nz=36, ny=30, nx=40, nt=150, nab=8, seed=85),
+    dict(nd=3, freesurf=1, L=3, abs_type=1, src_type=100, nz=44, ny=26, nx=30, nt=150, nab=6, seed=86),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", FP16_MEM_CASES, ids=["force_fs_L2", "taper_L1", "fs_L3"])
+def test_fp16_memory_variables_against_fp32(kw, cuda_device):
+    """Memory variables alone stored in FP16 (times a power of two set per
+    shot), wave fields FP32: within 1e-3 relative L2 of the FP32 run and of
+    the oracle over all outputs; the 4-cell kernels run it (free surface
+    folded into the stress update, and the separate surface kernel of the
+    kernel timings); what needs FP32 memory variables refuses the plan."""
+    import dataclasses
+
+    from oracle.oracle import Oracle
+    from seiscl_b200.engine import Plan, SeisCLEngineError
+
+    cfg, model, acq = make_case(**kw)
+    outs = _outputs(3)
+    res = {}
+    for prec in ("fp32", "fp16_mem"):
+        plan = Plan(dataclasses.replace(engine_config(cfg), field_precision=prec))
+        plan.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+        res[prec] = plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
+        if prec == "fp16_mem":
+            assert plan.kernel_family == "vector"
+            assert np.isfinite(plan.debug_array(0, 0, plan.nvol)).all()   # wave fields stay FP32
+            with pytest.raises(SeisCLEngineError):   # the memory variables are FP16
+                plan.debug_array(2, 0, plan.nvol * cfg["L"])
+            with pytest.raises(SeisCLEngineError):   # forward modelling only
+                plan.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs, save_boundaries=True)
+            assert all(t >= 0 for t in plan.bench_kernels(1))
+    ora = Oracle(cfg)
+    ora.set_model(model["vp"], model["vs"], model["rho"], model["taup"], model["taus"])
+    ref = ora.forward(acq["src_pos"], acq["src"], acq["rec_pos"], outs)
+    ora.close()
+
+    def joint(a, b):
+        num = sum(float(((a[n].astype(np.float64) - b[n]) ** 2).sum()) for n in outs)
+        den = sum(float((b[n].astype(np.float64) ** 2).sum()) for n in outs)
+        assert den > 0
+        return float(np.sqrt(num / den))
+
+    e32, eora = joint(res["fp16_mem"], res["fp32"]), joint(res["fp16_mem"], ref)
+    print("FP16 memory variables: rel L2 %.3g against FP32, %.3g against the oracle" % (e32, eora))
+    assert e32 < 1e-3 and eora < 1e-3, (e32, eora)
+
+
 FP16_2D_CASES = [
     dict(nd=2, freesurf=1, L=0, abs_type=1, src_type=100, nt=300, seed=81),
     dict(nd=2, freesurf=1, L=2, abs_type=1, src_type=2, nt=300, seed=82, fdorder=4),
