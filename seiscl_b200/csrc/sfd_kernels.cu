@@ -2494,7 +2494,9 @@ static inline bool q4_ok(const Grid &g) { return g.nd == 3 && g.F == 4 && g.nz %
 // own streams meanwhile); every one of them waits (pdl_wait) before it
 // reads or writes anything the previous kernels touch, and reads those
 // fields with plain loads (a read-only-path load may be hoisted above the
-// wait).  256^3, L=2: 1.008 against 1.015 ms per step.  On unless the
+// wait).  256^3, L=2: 1.008 against 1.015 ms per step.  The same for the
+// 2D P-SV loop (velocity and fused stress-step kernels, 300 x 400) was
+// slower, 7.17 against 7.39 Gcell/s, and is not done.  On unless the
 // environment sets SEISCL_B200_PDL=0.
 static bool pdl_enabled()
 {
