@@ -1183,21 +1183,20 @@ __global__ void __launch_bounds__(128) k_v3d_q4(Grid g, Fields f)
 // 256^3 L=2 on a B200.  5 CTAs (102 registers) is slower again, and a
 // component-at-a-time update with 80 registers slower still (0.37 ms): the
 // kernel is bound by the stencil loads each thread keeps in flight.
-// PDL: launched with programmatic stream serialization; the stresses then
-// come through plain loads (see k_s3d_q4_pf)
+// TRIG: an ordinary launch that lets the next kernel (the stress update,
+// launched with programmatic stream serialization) launch early.  Launched
+// that way itself, the kernel would have to read the stresses with plain
+// loads (see k_s3d_q4_pf), which cost it more than the overlap gives.
 // Taking the x planes in the reverse of the stress kernel's order (each
 // kernel starting on the planes the other has just written) was measured
 // and is not faster: 16.96 against 17.00 Gcell/s at 256^3, L=2.
-template <bool PDL = false>
+template <bool TRIG = false>
 __global__ void __launch_bounds__(128, 4) k_v3d_q4_b4(Grid g, Fields f)
 {
-    if constexpr (PDL) {
-        pdl_trigger();
-        pdl_wait();
-    }
+    if constexpr (TRIG) pdl_trigger();
     constexpr bool MB = false;
     CELL3D_Q4
-    v3d_q4_at<float, PDL ? 1 : 0>(g, f, gz0, gy, gx, iv, ip);
+    v3d_q4_at<float, 0>(g, f, gz0, gy, gx, iv, ip);
 }
 
 // ------------------------------------- velocity update staged by cp.async
@@ -2487,14 +2486,15 @@ __global__ void __launch_bounds__(128, PF ? 3 : 4) k_adjs3d_q4(Grid g, Fields f,
 // true when the 4-cell kernels apply to this grid
 static inline bool q4_ok(const Grid &g) { return g.nd == 3 && g.F == 4 && g.nz % 4 == 0; }
 
-// Programmatic dependent launch for the single-shot 3D loop: the velocity
-// and stress kernels, the sources and the receivers are launched with
-// programmatic stream serialization, so each may be resident while the
-// previous one drains its last wave (and the stress kernel asks L2 for its
-// own streams meanwhile); every one of them waits (pdl_wait) before it
-// reads or writes anything the previous kernels touch, and reads those
-// fields with plain loads (a read-only-path load may be hoisted above the
-// wait).  256^3, L=2: 1.008 against 1.015 ms per step.  The same for the
+// Programmatic dependent launch for the single-shot 3D loop: the stress
+// kernel, the sources and the receivers are launched with programmatic
+// stream serialization, so each may be resident while the previous one
+// drains its last wave (and the stress kernel asks L2 for its own streams
+// meanwhile); every one of them waits (pdl_wait) before it reads or writes
+// anything the previous kernels touch, and reads those fields with plain
+// loads (a read-only-path load may be hoisted above the wait).  The
+// velocity kernel is an ordinary launch that triggers its dependents
+// early.  256^3, L=2: 1.004 against 1.015 ms per step.  The same for the
 // 2D P-SV loop (velocity and fused stress-step kernels, 300 x 400) was
 // slower, 7.17 against 7.39 Gcell/s, and is not done.  On unless the
 // environment sets SEISCL_B200_PDL=0.
@@ -3609,7 +3609,11 @@ void launch_update_v(const Grid &g, const Fields &f, cudaStream_t st)
             // 4, 0.284 for 8 x 2 x 8 and 0.34 for 4 x 8 x 4 quads x y x x
             const dim3 b = q4_block(g, 16, 4, 2), gr = q4_grid(g, b);
             if (g.nb > 1) k_v3d_q4<float, true><<<gr, b, 0, st>>>(g, f);
-            else if (pdl_enabled()) launch_pdl(k_v3d_q4_b4<true>, gr, b, st, g, f);
+            // an ordinary launch (after the sources, which are complete by
+            // then) that lets the stress kernel launch early; launched with
+            // programmatic serialization itself it would need plain loads:
+            // 1.0062 against 1.0038 ms per step at 256^3, L=2
+            else if (pdl_enabled()) k_v3d_q4_b4<true><<<gr, b, 0, st>>>(g, f);
             else k_v3d_q4_b4<<<gr, b, 0, st>>>(g, f);
             return;
         }
