@@ -223,7 +223,7 @@ def serve_alone(req: Request, max_slots: int = 1, slot_bytes: int = 1 << 30,
 
 
 class Server:
-    """``Server(workers=4)``; ``submit(request) -> Future[Result]``;
+    """``Server(workers=8)``; ``submit(request) -> Future[Result]``;
     ``close()`` drains the queue and stops the workers.
 
     Admission by device memory: every plan the service holds (running or
@@ -239,7 +239,7 @@ class Server:
     captured loops.  ``max_batch``: see ``plan_config``; ``max_slots`` /
     ``slot_bytes``: see ``shot_slots``."""
 
-    def __init__(self, workers: int = 4, plans_per_worker: int = 4, device: Optional[int] = None,
+    def __init__(self, workers: int = 8, plans_per_worker: int = 4, device: Optional[int] = None,
                  memory_budget: Optional[int] = None, footprint=request_footprint, max_slots: int = 1,
                  slot_bytes: int = 1 << 30, max_batch: int = 8):
         self._q: "queue.Queue" = queue.Queue()
