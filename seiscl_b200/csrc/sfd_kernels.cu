@@ -3644,20 +3644,14 @@ bool launch_update_s(const Grid &g, const Fields &f, cudaStream_t st, bool fold_
         if (q4_ok(g)) {
             const dim3 b4 = q4_block(g, 16, 8, 1), g4 = q4_grid(g, b4);
             if (g.kernels == 0 && g.nb == 1 && g.L > 0) {   // with the stream prefetch, as the FP32 default
-                const bool pdl = pdl_enabled();
+                // ordinary launches: with programmatic serialization the FP16
+                // velocities need plain loads, which cost this kernel more than
+                // the overlap gives (0.510 against 0.489 ms at 256^3, L=2)
                 switch (g.L) {
-                case 0: if (pdl) launch_pdl(k_s3d_q4_pf<0, __half, true>, g4, b4, st, g, f, false);
-                        else k_s3d_q4_pf<0, __half><<<g4, b4, 0, st>>>(g, f, false);
-                        break;
-                case 1: if (pdl) launch_pdl(k_s3d_q4_pf<1, __half, true>, g4, b4, st, g, f, false);
-                        else k_s3d_q4_pf<1, __half><<<g4, b4, 0, st>>>(g, f, false);
-                        break;
-                case 2: if (pdl) launch_pdl(k_s3d_q4_pf<2, __half, true>, g4, b4, st, g, f, false);
-                        else k_s3d_q4_pf<2, __half><<<g4, b4, 0, st>>>(g, f, false);
-                        break;
-                default: if (pdl) launch_pdl(k_s3d_q4_pf<3, __half, true>, g4, b4, st, g, f, false);
-                         else k_s3d_q4_pf<3, __half><<<g4, b4, 0, st>>>(g, f, false);
-                         break;
+                case 0: k_s3d_q4_pf<0, __half><<<g4, b4, 0, st>>>(g, f, false); break;
+                case 1: k_s3d_q4_pf<1, __half><<<g4, b4, 0, st>>>(g, f, false); break;
+                case 2: k_s3d_q4_pf<2, __half><<<g4, b4, 0, st>>>(g, f, false); break;
+                default: k_s3d_q4_pf<3, __half><<<g4, b4, 0, st>>>(g, f, false); break;
                 }
                 return false;
             }
